@@ -1,0 +1,330 @@
+"""Benchmark: CloverLeaf3D hydro-cycle throughput (cell-updates/s) on B200.
+
+Workload: the two-state shock of the reference decks (state 1 rho=0.2 e=1.0,
+state 2 rho=1.0 e=2.5 in x<5, y<2, z<2) on [0,10]^3 at 512^3 cells,
+initial/max timestep 0.04, timestep_rise 1.5, field summary every 10 steps.
+A "step" is one full hydro step (hydro.f90:52-72, summaries included).
+
+value      device-resident chunk (native API), inputs already in HBM, steps
+           replayed from CUDA graphs; cells * steps / device time.
+e2e        the same workload through the drop-in C ABI with HOST arrays: the
+           reference control flow calling clover_*_kernel, the first call of
+           each array uploading it and a final copy back of every array, all
+           inside the timed region.
+roofline   dominant kernel group, algorithmic bytes / its event-timed duration
+           (a profiled run of the same steps right after the timed one).
+cpu_baseline  the oracle (C restatement of the reference, OpenMP) on the
+           host cores over a bounded sample of the same problem.
+
+--impl reference times that CPU restatement alone (the Fortran reference
+cannot be compiled on this image: no Fortran compiler).
+Multi-GPU (--gpus N under torchrun): N independent replicas, one chunk per
+GPU (the single-chunk path does not shard); weak scaling, max time over ranks.
+"""
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+STATES = [
+    dict(density=0.2, energy=1.0),
+    dict(density=1.0, energy=2.5, geometry="cuboid", xmin=0.0, xmax=5.0, ymin=0.0, ymax=2.0,
+         zmin=0.0, zmax=2.0),
+]
+
+
+def deck_values(n, steps):
+    return dict(x_cells=n, y_cells=n, z_cells=n, xmin=0.0, ymin=0.0, zmin=0.0, xmax=10.0,
+                ymax=10.0, zmax=10.0, initial_timestep=0.04, max_timestep=0.04,
+                timestep_rise=1.5, end_step=steps, end_time=1.0e6, summary_frequency=10)
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            j = json.load(f)
+        return j.get("hbm_gbs", 6650.0), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.p = None
+        return self
+
+    def __exit__(self, *a):
+        self.lines = []
+        if self.p:
+            self.p.terminate()
+            try:
+                out, _ = self.p.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.p.kill()
+                out, _ = self.p.communicate()
+            self.lines = [l for l in out.splitlines() if l.strip()]
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in getattr(self, "lines", []):
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 8:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for i, n in enumerate(names):
+                if f[4 + i].lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_baseline(n_cells, seconds_target=12.0):
+    """Oracle (OpenMP, all host threads) on a bounded sample of the problem."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_lib as O
+    L = O.load(fast=True)
+    L.oracle_run_timed.restype = ctypes.c_double
+    cores = os.cpu_count() or 1
+    # calibrate on 128^3, then size the sample to about seconds_target
+    d = O.make_deck(dict(deck_values(128, 3), states=STATES))
+    t = L.oracle_run_timed(ctypes.byref(d), 1, 2)
+    rate = 128 ** 3 * 2 / t
+    n = 256 if rate * seconds_target > 256 ** 3 * 2 else 128
+    steps = max(2, min(20, int(rate * seconds_target / n ** 3)))
+    d = O.make_deck(dict(deck_values(n, steps + 1), states=STATES))
+    t = L.oracle_run_timed(ctypes.byref(d), 1, steps)
+    return {"value": n ** 3 * steps / t, "unit": "cell-updates/s", "cores": cores,
+            "kind": "port",
+            "sample": "%d^3 cells x %d steps of the same two-state shock (oracle C restatement, "
+                      "OpenMP %d threads, -O3 x86-64-v3)" % (n, steps, cores)}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_lib as O
+    L = O.load(fast=True)
+    L.oracle_run_timed.restype = ctypes.c_double
+    cores = os.cpu_count() or 1
+    # bounded sample: the configured size when the host holds it, else 256^3
+    n = args.cells
+    need = 31 * (n + 5) ** 3 * 8
+    avail = 0
+    try:
+        with open("/proc/meminfo") as f:
+            for l in f:
+                if l.startswith("MemAvailable"):
+                    avail = int(l.split()[1]) * 1024
+    except OSError:
+        pass
+    if need * 1.5 > avail:
+        n = 256
+    steps = max(1, min(args.steps, 5 if n >= 512 else args.steps))
+    warm = min(args.warmup, 1)
+    d = O.make_deck(dict(deck_values(n, steps + warm + 1), states=STATES))
+    t = L.oracle_run_timed(ctypes.byref(d), warm, steps)
+    v = n ** 3 * steps / t
+    line = {
+        "metric": "cell-updates/s", "value": v, "unit": "cell-updates/s", "impl": "reference",
+        "n_gpus": args.gpus, "steps": steps, "warmup": warm, "ms_per_step": 1000.0 * t / steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic: two-state shock deck generated on the host",
+        "config": {"workload": "two-state shock %d^3 FP64 (%s)" % (
+            n, "configured size" if n == args.cells else "reduced from %d^3: host memory" % args.cells)},
+        "cpu_baseline": {"value": v, "unit": "cell-updates/s", "cores": cores, "kind": "port",
+                         "sample": "%d^3 cells x %d steps after %d warm-up (oracle C restatement of "
+                                   "the reference; the Fortran reference needs a Fortran compiler, "
+                                   "absent on this image)" % (n, steps, warm)},
+        "e2e": {"value": v, "unit": "cell-updates/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def e2e_dropin(C, args, n, steps):
+    """The workload through the drop-in C ABI with host arrays, copies timed."""
+    import numpy as np  # noqa: F401
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    deck = C.Deck.from_values(states=STATES, **deck_values(n, steps))
+    L = C.lib()
+    L.clover_gpu_release()
+    L.clover_gpu_synchronize()
+    t0 = time.perf_counter()
+    di = C.DropIn(deck)  # start(): first sight of every host array uploads it
+    taken = di.run(steps)
+    L.clover_gpu_sync_to_host()  # every array back to the host
+    t1 = time.perf_counter()
+    arrays = ctypes.c_int(0)
+    nbytes = ctypes.c_longlong(0)
+    L.clover_gpu_mirror_stats(ctypes.byref(arrays), ctypes.byref(nbytes))
+    host_bytes = 0
+    nx = n
+    cell = (nx + 4) ** 3 * 8
+    vert = (nx + 5) ** 3 * 8
+    face = (nx + 5) * (nx + 4) ** 2 * 8
+    host_bytes = 8 * cell + 6 * vert + 9 * face + 7 * vert  # 3D arrays of build_field
+    di.close()
+    return {"value": n ** 3 * taken / (t1 - t0), "unit": "cell-updates/s",
+            "h2d_bytes_per_step": host_bytes / taken,
+            "d2h_bytes_per_step": (host_bytes + 8 * taken + 40 * (taken // 10 + 2)) / taken,
+            "seconds": t1 - t0, "steps": taken, "cells": "%d^3" % n}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cells", type=int, default=512)
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+    import torch.distributed as dist
+    import cloverleaf3d_ref_b200 as C
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    n = args.cells
+    prec = C.PRECISION_MIXED if args.precision == "mixed" else C.PRECISION_FP64
+    total = args.warmup + 2 * args.steps + 5
+    deck = C.Deck.from_values(states=STATES, **deck_values(n, total))
+    ch = C.Chunk(deck, prec)
+    stream = torch.cuda.ExternalStream(ch.stream)
+    ch.step(args.warmup)
+    ch.sync()
+    launches = ch.launches_per_step
+
+    # timed region A: graph replay
+    barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        e0.record(stream)
+        ch.step(args.steps)
+        e1.record(stream)
+        e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    torch.cuda.synchronize()
+    barrier()
+    if world > 1:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    clocks = clk.summary()
+
+    # profiled region B: same steps with events around every kernel group
+    ch.profile(True)
+    ch.step(args.steps)
+    groups = ch.profile_report()
+    ch.profile(False)
+    status = ch.status
+    summaries, sum_steps = ch.summaries()
+    ch.close()
+
+    value = world * n ** 3 * args.steps / (ms / 1000.0)
+    peak, peak_kind = load_peaks()
+    top = max(groups, key=lambda g: g["ms"])
+    prof_total_ms = sum(g["ms"] for g in groups)
+    achieved = top["bytes"] / (top["ms"] / 1000.0) / 1e9
+    step_bytes = sum(g["bytes"] for g in groups) / args.steps
+    roofline = {
+        "kernel": top["name"], "bound": "hbm", "achieved": achieved, "peak": peak,
+        "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
+        "traffic": None,
+        "launches": top["launches"], "share": top["ms"] / prof_total_ms,
+        "step_algorithmic_bytes_per_cell": step_bytes / n ** 3,
+        "step_achieved_gbs": step_bytes / (ms / args.steps / 1000.0) / 1e9,
+        "step_frac": step_bytes / (ms / args.steps / 1000.0) / 1e9 / peak,
+        "reference_structured_frac": 2512.0 * n ** 3 / (ms / args.steps / 1000.0) / 1e9 / peak,
+    }
+    per_kernel = {g["name"]: {"ms_per_step": g["ms"] / args.steps,
+                              "gbs": g["bytes"] / max(g["ms"], 1e-9) / 1e6,
+                              "launches_per_step": g["launches"] / args.steps} for g in groups}
+
+    e2e = None
+    if not args.no_e2e and rank == 0:
+        e2e = e2e_dropin(C, args, n, args.steps)
+    cpu = None
+    if not args.no_cpu and rank == 0 and world == 1:
+        cpu = cpu_baseline(n)
+
+    if rank == 0:
+        line = {
+            "metric": "cell-updates/s", "value": value, "unit": "cell-updates/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64" if prec == C.PRECISION_FP64 else "f32/f64 mixed",
+            "data": "synthetic: two-state shock deck generated on the device",
+            "config": {"workload": "two-state shock %d^3, %s, graph-replayed steps" % (
+                n, args.precision), "cells": n ** 3, "parallelism": "replicas only",
+                "l2": "inputs larger than L2 (each field %.2f GB)" % ((n + 5) ** 3 * 8 / 1e9)},
+            "gpu_launches": launches * args.steps + 2 * (args.steps // 10 + 1),
+            "clocks": clocks, "roofline": roofline, "per_kernel": per_kernel,
+            "status": status,
+            "last_summary": {"step": int(sum_steps[-1]), "vol_mass_ie_ke_press":
+                             [float(x) for x in summaries[-1]]},
+        }
+        if e2e:
+            line["e2e"] = e2e
+        if cpu:
+            line["cpu_baseline"] = cpu
+        print(json.dumps(line))
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,382 @@
+"""B200-native CloverLeaf3D hydro cycle.
+
+Python bindings (ctypes) of libclover_b200.so:
+
+* ``Deck``      -- the *clover input deck (parse.f90 / read_input.f90 keys and
+                   defaults), parsed by the library's own reader.
+* ``Chunk``     -- a chunk resident in HBM, stepped on the device from CUDA
+                   graphs (FP64, or FP32 storage with FP64 where conservation
+                   needs it).
+* ``DropIn``    -- the reference's control flow driving the drop-in C ABI
+                   (include/clover_kernels.h) with host arrays.
+* ``abi``       -- the raw ctypes handle of the drop-in entry points.
+
+The library is built in-tree (``cloverleaf3d_ref_b200/libclover_b200.so``,
+``build()``); importing this package never builds or falls back: a missing
+library raises.
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libclover_b200.so")
+CSRC = os.path.join(HERE, "csrc")
+ROOT = os.path.dirname(HERE)
+
+MAX_STATES = 16
+PRECISION_FP64 = 0
+PRECISION_MIXED = 1
+
+# reference field ids, data.f90:55-74
+FIELD_IDS = {
+    "density0": 1, "density1": 2, "energy0": 3, "energy1": 4, "pressure": 5,
+    "viscosity": 6, "soundspeed": 7, "xvel0": 8, "xvel1": 9, "yvel0": 10,
+    "yvel1": 11, "zvel0": 12, "zvel1": 13, "vol_flux_x": 14, "vol_flux_y": 15,
+    "vol_flux_z": 16, "mass_flux_x": 17, "mass_flux_y": 18, "mass_flux_z": 19,
+}
+FIELD_NAMES = sorted(FIELD_IDS, key=FIELD_IDS.get)
+
+STATUS_BITS = {
+    0x1: "cuda_error", 0x2: "bounds", 0x4: "small_dt", 0x8: "no_device",
+    0x10: "bad_arg", 0x20: "timeout",
+}
+
+
+def field_shape(name, nx, ny, nz):
+    """Fortran-order shape of a reference array (build_field.f90:41-146)."""
+    fid = FIELD_IDS[name]
+    if fid <= 7:
+        return (nx + 4, ny + 4, nz + 4)
+    if fid <= 13:
+        return (nx + 5, ny + 5, nz + 5)
+    if fid in (14, 17):
+        return (nx + 5, ny + 4, nz + 4)
+    if fid in (15, 18):
+        return (nx + 4, ny + 5, nz + 4)
+    return (nx + 4, ny + 4, nz + 5)
+
+
+def build(verbose=False):
+    """Compile the CUDA library for sm_100a in-tree."""
+    out = None if verbose else subprocess.DEVNULL
+    subprocess.check_call(["make", "-s", "-C", CSRC, "-j4"], stdout=out)
+
+
+class CloverError(RuntimeError):
+    pass
+
+
+_LIB = None
+
+
+def lib():
+    """The loaded libclover_b200.so (raises if it has not been built)."""
+    global _LIB
+    if _LIB is None:
+        if not os.path.exists(LIB_PATH):
+            raise CloverError(
+                "libclover_b200.so is not built; run cloverleaf3d_ref_b200.build()")
+        _LIB = ctypes.CDLL(LIB_PATH)
+        _declare(_LIB)
+    return _LIB
+
+
+abi = None  # set by _declare
+
+
+class DeckStruct(ctypes.Structure):
+    _fields_ = [
+        ("x_cells", ctypes.c_int), ("y_cells", ctypes.c_int), ("z_cells", ctypes.c_int),
+        ("xmin", ctypes.c_double), ("ymin", ctypes.c_double), ("zmin", ctypes.c_double),
+        ("xmax", ctypes.c_double), ("ymax", ctypes.c_double), ("zmax", ctypes.c_double),
+        ("initial_timestep", ctypes.c_double), ("max_timestep", ctypes.c_double),
+        ("timestep_rise", ctypes.c_double), ("end_time", ctypes.c_double),
+        ("dtmin", ctypes.c_double), ("dtc_safe", ctypes.c_double),
+        ("dtu_safe", ctypes.c_double), ("dtv_safe", ctypes.c_double),
+        ("dtw_safe", ctypes.c_double), ("dtdiv_safe", ctypes.c_double),
+        ("end_step", ctypes.c_int), ("summary_frequency", ctypes.c_int),
+        ("visit_frequency", ctypes.c_int), ("tiles_per_chunk", ctypes.c_int),
+        ("test_problem", ctypes.c_int), ("profiler_on", ctypes.c_int),
+        ("number_of_states", ctypes.c_int),
+        ("state_defined", ctypes.c_int * MAX_STATES),
+        ("state_density", ctypes.c_double * MAX_STATES),
+        ("state_energy", ctypes.c_double * MAX_STATES),
+        ("state_xvel", ctypes.c_double * MAX_STATES),
+        ("state_yvel", ctypes.c_double * MAX_STATES),
+        ("state_zvel", ctypes.c_double * MAX_STATES),
+        ("state_xmin", ctypes.c_double * MAX_STATES),
+        ("state_xmax", ctypes.c_double * MAX_STATES),
+        ("state_ymin", ctypes.c_double * MAX_STATES),
+        ("state_ymax", ctypes.c_double * MAX_STATES),
+        ("state_zmin", ctypes.c_double * MAX_STATES),
+        ("state_zmax", ctypes.c_double * MAX_STATES),
+        ("state_radius", ctypes.c_double * MAX_STATES),
+        ("state_geometry", ctypes.c_int * MAX_STATES),
+    ]
+
+
+def _declare(L):
+    global abi
+    P = ctypes.c_void_p
+    L.clover_deck_parse.argtypes = [ctypes.c_char_p, P, ctypes.c_char_p, ctypes.c_int]
+    L.clover_deck_parse.restype = ctypes.c_int
+    L.clover_deck_defaults.argtypes = [P]
+    L.clover_chunk_create.argtypes = [P, ctypes.c_int]
+    L.clover_chunk_create.restype = P
+    L.clover_last_error.restype = ctypes.c_char_p
+    L.clover_chunk_destroy.argtypes = [P]
+    for n in ("clover_chunk_step",):
+        getattr(L, n).argtypes = [P, ctypes.c_int]
+        getattr(L, n).restype = ctypes.c_int
+    for n in ("clover_chunk_run", "clover_chunk_sync", "clover_chunk_steps",
+              "clover_chunk_status", "clover_chunk_launches_per_step"):
+        getattr(L, n).argtypes = [P]
+        getattr(L, n).restype = ctypes.c_int
+    L.clover_chunk_use_graphs.argtypes = [P, ctypes.c_int]
+    L.clover_chunk_time.argtypes = [P]
+    L.clover_chunk_time.restype = ctypes.c_double
+    L.clover_chunk_dt_history.argtypes = [P, P, ctypes.c_int]
+    L.clover_chunk_dt_history.restype = ctypes.c_int
+    L.clover_chunk_summaries.argtypes = [P, P, P, ctypes.c_int]
+    L.clover_chunk_summaries.restype = ctypes.c_int
+    L.clover_chunk_read_field.argtypes = [P, ctypes.c_int, P]
+    L.clover_chunk_read_field.restype = ctypes.c_int
+    L.clover_chunk_write_field.argtypes = [P, ctypes.c_int, P]
+    L.clover_chunk_write_field.restype = ctypes.c_int
+    L.clover_chunk_stream.argtypes = [P]
+    L.clover_chunk_stream.restype = ctypes.c_size_t
+    L.clover_chunk_device_bytes.argtypes = [P]
+    L.clover_chunk_device_bytes.restype = ctypes.c_longlong
+    L.clover_chunk_profile.argtypes = [P, ctypes.c_int]
+    L.clover_chunk_profile_report.argtypes = [P, P, ctypes.c_int, P, P, P, ctypes.c_int]
+    L.clover_chunk_profile_report.restype = ctypes.c_int
+    L.clover_dropin_create.argtypes = [P]
+    L.clover_dropin_create.restype = P
+    L.clover_dropin_run.argtypes = [P, ctypes.c_int]
+    L.clover_dropin_run.restype = ctypes.c_int
+    L.clover_dropin_dt_history.argtypes = [P, P, ctypes.c_int]
+    L.clover_dropin_dt_history.restype = ctypes.c_int
+    L.clover_dropin_summaries.argtypes = [P, P, P, ctypes.c_int]
+    L.clover_dropin_summaries.restype = ctypes.c_int
+    L.clover_dropin_read_field.argtypes = [P, ctypes.c_int, P, ctypes.c_longlong]
+    L.clover_dropin_read_field.restype = ctypes.c_int
+    L.clover_dropin_destroy.argtypes = [P]
+    L.clover_gpu_status.restype = ctypes.c_int
+    L.clover_gpu_error_string.restype = ctypes.c_char_p
+    L.clover_gpu_invalidate.argtypes = [P]
+    abi = L
+
+
+class Deck:
+    """A parsed *clover deck. Construct from text, a file, or keyword values
+    (``Deck.from_values(x_cells=32, ...,
+    states=[dict(density=0.2, energy=1.0), dict(...)])``)."""
+
+    def __init__(self, struct):
+        self.s = struct
+
+    @classmethod
+    def parse(cls, text):
+        s = DeckStruct()
+        err = ctypes.create_string_buffer(256)
+        rc = lib().clover_deck_parse(text.encode(), ctypes.byref(s), err, 256)
+        if rc != 0:
+            raise CloverError("deck: " + err.value.decode())
+        return cls(s)
+
+    @classmethod
+    def from_file(cls, path):
+        with open(path) as f:
+            return cls.parse(f.read())
+
+    @classmethod
+    def from_values(cls, states, **kw):
+        s = DeckStruct()
+        lib().clover_deck_defaults(ctypes.byref(s))
+        for k, v in kw.items():
+            if not hasattr(s, k):
+                raise CloverError("deck: unknown key %s" % k)
+            setattr(s, k, v)
+        if not 1 <= len(states) <= MAX_STATES:
+            raise CloverError("deck: 1..16 states")
+        s.number_of_states = len(states)
+        geo = {"cuboid": 1, "sphere": 2, "point": 3}
+        for i, st in enumerate(states):
+            s.state_defined[i] = 1
+            for k, v in st.items():
+                if k == "geometry":
+                    s.state_geometry[i] = geo[v]
+                else:
+                    getattr(s, "state_" + k)[i] = v
+        return cls(s)
+
+    def __getattr__(self, k):
+        return getattr(self.s, k)
+
+    def replace(self, **kw):
+        s = DeckStruct.from_buffer_copy(self.s)
+        for k, v in kw.items():
+            setattr(s, k, v)
+        return Deck(s)
+
+    @property
+    def cells(self):
+        return self.s.x_cells * self.s.y_cells * self.s.z_cells
+
+
+class Chunk:
+    """A chunk resident on the current CUDA device (native API)."""
+
+    def __init__(self, deck, precision=PRECISION_FP64):
+        L = lib()
+        self.deck = deck
+        self.precision = precision
+        self.h = L.clover_chunk_create(ctypes.byref(deck.s), precision)
+        if not self.h:
+            raise CloverError("chunk: " + L.clover_last_error().decode())
+
+    def close(self):
+        if self.h:
+            lib().clover_chunk_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def step(self, n):
+        if lib().clover_chunk_step(self.h, n) != 0:
+            raise CloverError("chunk step failed")
+
+    def run(self):
+        return lib().clover_chunk_run(self.h)
+
+    def sync(self):
+        if lib().clover_chunk_sync(self.h) != 0:
+            raise CloverError("chunk sync failed")
+
+    def use_graphs(self, on):
+        lib().clover_chunk_use_graphs(self.h, 1 if on else 0)
+
+    @property
+    def steps(self):
+        return lib().clover_chunk_steps(self.h)
+
+    @property
+    def time(self):
+        return lib().clover_chunk_time(self.h)
+
+    @property
+    def status(self):
+        return lib().clover_chunk_status(self.h)
+
+    @property
+    def stream(self):
+        return lib().clover_chunk_stream(self.h)
+
+    @property
+    def device_bytes(self):
+        return lib().clover_chunk_device_bytes(self.h)
+
+    @property
+    def launches_per_step(self):
+        return lib().clover_chunk_launches_per_step(self.h)
+
+    def profile(self, on):
+        """Profile mode: direct launches bracketed by events per kernel group."""
+        lib().clover_chunk_profile(self.h, 1 if on else 0)
+
+    def profile_report(self, cap=64):
+        """Per kernel group since the last report: ms, algorithmic bytes, launches."""
+        names = ctypes.create_string_buffer(cap * 32)
+        ms = np.zeros(cap)
+        by = np.zeros(cap)
+        la = np.zeros(cap, dtype=np.int32)
+        n = lib().clover_chunk_profile_report(self.h, names, 32, ms.ctypes.data,
+                                              by.ctypes.data, la.ctypes.data, cap)
+        raw = names.raw
+        out = []
+        for i in range(n):
+            nm = raw[i * 32:(i + 1) * 32].split(b"\0")[0].decode()
+            out.append({"name": nm, "ms": float(ms[i]), "bytes": float(by[i]),
+                        "launches": int(la[i])})
+        return out
+
+    def dt_history(self):
+        n = self.steps
+        out = np.zeros(max(n, 1))
+        got = lib().clover_chunk_dt_history(self.h, out.ctypes.data, n)
+        return out[:got]
+
+    def summaries(self, cap=100000):
+        out = np.zeros((cap, 5))
+        st = np.zeros(cap, dtype=np.int32)
+        n = lib().clover_chunk_summaries(self.h, out.ctypes.data, st.ctypes.data, cap)
+        return out[:n], st[:n]
+
+    def field(self, name):
+        s = self.deck.s
+        a = np.zeros(field_shape(name, s.x_cells, s.y_cells, s.z_cells), order="F")
+        if lib().clover_chunk_read_field(self.h, FIELD_IDS[name], a.ctypes.data) != 0:
+            raise CloverError("read_field failed")
+        return a
+
+    def set_field(self, name, a):
+        s = self.deck.s
+        a = np.asfortranarray(a, dtype=np.float64)
+        assert a.shape == field_shape(name, s.x_cells, s.y_cells, s.z_cells)
+        if lib().clover_chunk_write_field(self.h, FIELD_IDS[name], a.ctypes.data) != 0:
+            raise CloverError("write_field failed")
+
+
+class DropIn:
+    """The reference control flow over the drop-in ABI with host arrays."""
+
+    def __init__(self, deck):
+        L = lib()
+        L.clover_gpu_clear_status()
+        self.deck = deck
+        self.h = L.clover_dropin_create(ctypes.byref(deck.s))
+        if not self.h:
+            raise CloverError("drop-in start failed: " + L.clover_gpu_error_string().decode())
+
+    def run(self, max_steps=2 ** 30):
+        n = lib().clover_dropin_run(self.h, max_steps)
+        st = lib().clover_gpu_status()
+        if st & ~0x4:
+            raise CloverError("drop-in: " + lib().clover_gpu_error_string().decode())
+        return n
+
+    def dt_history(self, cap=1 << 20):
+        out = np.zeros(cap)
+        n = lib().clover_dropin_dt_history(self.h, out.ctypes.data, cap)
+        return out[:n]
+
+    def summaries(self, cap=100000):
+        out = np.zeros((cap, 5))
+        st = np.zeros(cap, dtype=np.int32)
+        n = lib().clover_dropin_summaries(self.h, out.ctypes.data, st.ctypes.data, cap)
+        return out[:n], st[:n]
+
+    def field(self, name):
+        s = self.deck.s
+        a = np.zeros(field_shape(name, s.x_cells, s.y_cells, s.z_cells), order="F")
+        if lib().clover_dropin_read_field(self.h, FIELD_IDS[name], a.ctypes.data, a.size) != 0:
+            raise CloverError("drop-in read_field failed")
+        return a
+
+    def close(self):
+        if self.h:
+            lib().clover_dropin_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,1265 @@
+// Hydro-cycle kernels for sm_100a, one family per reference *_kernel.
+//
+// Each kernel computes exactly the elements the reference loop nest computes,
+// over the same index ranges, with the same operation order. The library is
+// built with -fmad=false, so FP64 results are bit-identical to a serial
+// IEEE evaluation of the reference expressions (the reductions excepted,
+// whose order differs). All arithmetic is FP64 whatever the storage type.
+//
+// Threads map one-to-one onto elements: x (the contiguous axis) across the
+// 32 lanes of a warp, y across warps, z across the grid, so every warp load
+// is a coalesced 256-byte row segment of the pitched layout.
+#include <cfloat>
+#include <cstdio>
+
+#include "clover_launch.h"
+
+namespace clover {
+
+namespace {
+
+constexpr int BX = 32, BY = 8;
+
+struct Box {
+  int j0, j1, k0, k1, l0, l1;
+};
+
+inline dim3 grid_of(const Box& b) {
+  int nj = b.j1 - b.j0 + 1, nk = b.k1 - b.k0 + 1, nl = b.l1 - b.l0 + 1;
+  if (nj <= 0 || nk <= 0 || nl <= 0) return dim3(0, 0, 0);
+  return dim3((nj + BX - 1) / BX, (nk + BY - 1) / BY, nl);
+}
+
+inline bool launchable(const dim3& gr) { return gr.x > 0 && gr.y > 0 && gr.z > 0; }
+
+#define BOX_THREAD(b)                                    \
+  const int j = (b).j0 + blockIdx.x * BX + threadIdx.x;  \
+  const int k = (b).k0 + blockIdx.y * BY + threadIdx.y;  \
+  const int l = (b).l0 + blockIdx.z;                     \
+  if (j > (b).j1 || k > (b).k1) return
+
+// 3D element, 1D coordinate arrays
+#define E(a, jj, kk, ll) (a)[off3(g, (jj), (kk), (ll))]
+#define GX(a, jj) (a)[(jj) - g.x_min + 2]
+#define GY(a, kk) (a)[(kk) - g.y_min + 2]
+#define GZ(a, ll) (a)[(ll) - g.z_min + 2]
+
+__device__ __forceinline__ double ld(const double* p) { return __ldg(p); }
+__device__ __forceinline__ double ld(const float* p) { return (double)__ldg(p); }
+#define L(a, jj, kk, ll) ld(&E(a, jj, kk, ll))
+
+template <class T>
+__device__ __forceinline__ T st(double v) { return (T)v; }
+
+__device__ __forceinline__ double fmin2(double a, double b) { return b < a ? b : a; }
+__device__ __forceinline__ double fmax2(double a, double b) { return b > a ? b : a; }
+
+__device__ __forceinline__ double dt_of(double v, const double* p) { return p ? *p : v; }
+
+// ---------------------------------------------------------------------------
+// ideal_gas_kernel.f90:47-58
+template <class S>
+__global__ void __launch_bounds__(BX * BY) k_ideal_gas(Geom g, Box b,
+    const typename S::rho_t* __restrict__ density, const typename S::ene_t* __restrict__ energy,
+    typename S::cs_t* __restrict__ pressure, typename S::cs_t* __restrict__ soundspeed) {
+  BOX_THREAD(b);
+  const double d = L(density, j, k, l);
+  const double v = 1.0 / d;
+  const double p = (1.4 - 1.0) * d * L(energy, j, k, l);
+  const double pressurebyenergy = (1.4 - 1.0) * d;
+  const double pressurebyvolume = -d * p;
+  const double ss2 = v * v * (p * pressurebyenergy - pressurebyvolume);
+  using C = typename S::cs_t;
+  E(pressure, j, k, l) = st<C>(p);
+  E(soundspeed, j, k, l) = st<C>(sqrt(ss2));
+}
+
+// ---------------------------------------------------------------------------
+// viscosity_kernel.f90:71-134
+template <class S>
+__global__ void __launch_bounds__(BX * BY) k_viscosity(Geom g, Box b, GeomArrays ga,
+    const typename S::rho_t* __restrict__ density0, const typename S::cs_t* __restrict__ pressure,
+    typename S::cs_t* __restrict__ viscosity, const typename S::vel_t* __restrict__ xvel0,
+    const typename S::vel_t* __restrict__ yvel0, const typename S::vel_t* __restrict__ zvel0) {
+  BOX_THREAD(b);
+  const double u000 = L(xvel0, j, k, l), u100 = L(xvel0, j + 1, k, l);
+  const double u010 = L(xvel0, j, k + 1, l), u110 = L(xvel0, j + 1, k + 1, l);
+  const double u001 = L(xvel0, j, k, l + 1), u101 = L(xvel0, j + 1, k, l + 1);
+  const double u011 = L(xvel0, j, k + 1, l + 1), u111 = L(xvel0, j + 1, k + 1, l + 1);
+  const double v000 = L(yvel0, j, k, l), v100 = L(yvel0, j + 1, k, l);
+  const double v010 = L(yvel0, j, k + 1, l), v110 = L(yvel0, j + 1, k + 1, l);
+  const double v001 = L(yvel0, j, k, l + 1), v101 = L(yvel0, j + 1, k, l + 1);
+  const double v011 = L(yvel0, j, k + 1, l + 1), v111 = L(yvel0, j + 1, k + 1, l + 1);
+  const double w000 = L(zvel0, j, k, l), w100 = L(zvel0, j + 1, k, l);
+  const double w010 = L(zvel0, j, k + 1, l), w110 = L(zvel0, j + 1, k + 1, l);
+  const double w001 = L(zvel0, j, k, l + 1), w101 = L(zvel0, j + 1, k, l + 1);
+  const double w011 = L(zvel0, j, k + 1, l + 1), w111 = L(zvel0, j + 1, k + 1, l + 1);
+
+  const double ugradx1 = u000 + u010 + u001 + u011;
+  const double ugradx2 = u100 + u110 + u101 + u111;
+  const double ugrady1 = u000 + u100 + u001 + u101;
+  const double ugrady2 = u010 + u110 + u011 + u111;
+  const double ugradz1 = u000 + u100 + u010 + u110;
+  const double ugradz2 = u001 + u101 + u011 + u111;
+
+  const double vgradx1 = v000 + v010 + v001 + v011;
+  const double vgradx2 = v100 + v110 + v101 + v111;
+  const double vgrady1 = v000 + v100 + v001 + v101;
+  const double vgrady2 = v010 + v110 + v011 + v111;
+  const double vgradz1 = v000 + v100 + v010 + v110;
+  const double vgradz2 = v001 + v101 + v011 + v111;
+
+  const double wgradx1 = w000 + w010 + w001 + w011;
+  const double wgradx2 = w100 + w110 + w101 + w111;
+  const double wgrady1 = w000 + w100 + w001 + w101;
+  const double wgrady2 = w010 + w110 + w011 + w111;
+  const double wgradz1 = w000 + w100 + w010 + w110;
+  const double wgradz2 = w001 + w101 + w011 + w111;
+
+  const double cdx = GX(ga.celldx, j), cdy = GY(ga.celldy, k), cdz = GZ(ga.celldz, l);
+  const double div = (E(ga.xarea, j, k, l) * (ugradx2 - ugradx1) +
+                      E(ga.yarea, j, k, l) * (vgrady2 - vgrady1)) +
+                     E(ga.zarea, j, k, l) * (wgradz2 - wgradz1);
+
+  const double xx = 0.25 * (ugradx2 - ugradx1) / cdx;
+  const double yy = 0.25 * (vgrady2 - vgrady1) / cdy;
+  const double zz = 0.25 * (wgradz2 - wgradz1) / cdz;
+  const double xy = 0.25 * (ugrady2 - ugrady1) / cdy + 0.25 * (vgradx2 - vgradx1) / cdx;
+  const double xz = 0.25 * (ugradz2 - ugradz1) / cdz + 0.25 * (wgradx2 - wgradx1) / cdx;
+  const double yz = 0.25 * (vgradz2 - vgradz1) / cdz + 0.25 * (wgrady2 - wgrady1) / cdy;
+
+  double pgradx = (L(pressure, j + 1, k, l) - L(pressure, j - 1, k, l)) / (cdx + GX(ga.celldx, j + 1));
+  double pgrady = (L(pressure, j, k + 1, l) - L(pressure, j, k - 1, l)) / (cdy + GY(ga.celldy, k + 1));
+  double pgradz = (L(pressure, j, k, l + 1) - L(pressure, j, k, l - 1)) / (cdz + GZ(ga.celldz, l + 1));
+
+  const double pgradx2 = pgradx * pgradx;
+  const double pgrady2 = pgrady * pgrady;
+  const double pgradz2 = pgradz * pgradz;
+
+  const double limiter = (xx * pgradx2 + yy * pgrady2 + zz * pgradz2 + xy * pgradx * pgrady +
+                          xz * pgradx * pgradz + yz * pgrady * pgradz) /
+                         fmax2(pgradx2 + pgrady2 + pgradz2, 1.0e-16);
+  double q;
+  if ((limiter > 0.0) || (div >= 0.0)) {
+    q = 0.0;
+  } else {
+    pgradx = copysign(fmax2(1.0e-16, fabs(pgradx)), pgradx);
+    pgrady = copysign(fmax2(1.0e-16, fabs(pgrady)), pgrady);
+    pgradz = copysign(fmax2(1.0e-16, fabs(pgradz)), pgradz);
+    const double pgrad = sqrt(pgradx * pgradx + pgrady * pgrady + pgradz * pgradz);
+    const double xgrad = fabs(cdx * pgrad / pgradx);
+    const double ygrad = fabs(cdy * pgrad / pgrady);
+    const double zgrad = fabs(cdz * pgrad / pgradz);
+    const double grad = fmin2(fmin2(xgrad, ygrad), zgrad);
+    const double grad2 = grad * grad;
+    q = 2.0 * L(density0, j, k, l) * grad2 * limiter * limiter;
+  }
+  E(viscosity, j, k, l) = st<typename S::cs_t>(q);
+}
+
+// ---------------------------------------------------------------------------
+// calc_dt_kernel.f90:102-149 with the minimum of :141-147 folded into an
+// atomic minimum. Doubles are mapped to an order-preserving 64-bit key, so the
+// atomic gives exactly the serial minimum; NaNs never win, as with .LT..
+__host__ __device__ __forceinline__ unsigned long long key_of(double v) {
+#ifdef __CUDA_ARCH__
+  unsigned long long b = (unsigned long long)__double_as_longlong(v);
+#else
+  unsigned long long b;
+  memcpy(&b, &v, sizeof(b));
+#endif
+  return (b >> 63) ? ~b : (b | 0x8000000000000000ull);
+}
+
+template <class S>
+__global__ void __launch_bounds__(BX * BY) k_calc_dt(Geom g, Box b, GeomArrays ga,
+    double g_small, double dtc_safe, double dtu_safe, double dtv_safe, double dtw_safe,
+    double dtdiv_safe, const typename S::rho_t* __restrict__ density0,
+    const typename S::cs_t* __restrict__ viscosity_a, const typename S::cs_t* __restrict__ soundspeed,
+    const typename S::vel_t* __restrict__ xvel0, const typename S::vel_t* __restrict__ yvel0,
+    const typename S::vel_t* __restrict__ zvel0, typename S::wk_t* __restrict__ dt_min,
+    unsigned long long* __restrict__ min_key) {
+  const int j = b.j0 + blockIdx.x * BX + threadIdx.x;
+  const int k = b.k0 + blockIdx.y * BY + threadIdx.y;
+  const int l = b.l0 + blockIdx.z;
+  unsigned long long key = ~0ull;
+  if (j <= b.j1 && k <= b.k1) {
+    const double m = fmin2(fmin2(GX(ga.celldx, j), GY(ga.celldy, k)), GZ(ga.celldz, l));
+    const double ds = 1.0 / (m * m);
+    const double ss = L(soundspeed, j, k, l);
+    double cc = ss * ss;
+    cc = cc + 2.0 * L(viscosity_a, j, k, l) / L(density0, j, k, l);
+    double dtct = ds * cc;
+    dtct = dtc_safe * 1.0 / fmax2(sqrt(dtct), g_small);
+
+    const double vol = E(ga.volume, j, k, l);
+    const double xa = E(ga.xarea, j, k, l);
+    const double du1 = (L(xvel0, j, k, l) + L(xvel0, j, k + 1, l) + L(xvel0, j, k, l + 1) +
+                        L(xvel0, j, k + 1, l + 1)) * xa;
+    const double du2 = (L(xvel0, j + 1, k, l) + L(xvel0, j + 1, k + 1, l) +
+                        L(xvel0, j + 1, k, l + 1) + L(xvel0, j + 1, k + 1, l + 1)) * xa;
+    const double dtut = dtu_safe * 4.0 * vol / fmax2(fmax2(fabs(du1), fabs(du2)), 1.0e-5 * vol);
+
+    const double ya = E(ga.yarea, j, k, l);
+    const double dv1 = (L(yvel0, j, k, l) + L(yvel0, j + 1, k, l) + L(yvel0, j, k, l + 1) +
+                        L(yvel0, j + 1, k, l + 1)) * ya;
+    const double dv2 = (L(yvel0, j, k + 1, l) + L(yvel0, j + 1, k + 1, l) +
+                        L(yvel0, j, k + 1, l + 1) + L(yvel0, j + 1, k + 1, l + 1)) * ya;
+    const double dtvt = dtv_safe * 4.0 * vol / fmax2(fmax2(fabs(dv1), fabs(dv2)), 1.0e-5 * vol);
+
+    const double za = E(ga.zarea, j, k, l);  // both z faces use zarea(j,k,l)
+    const double dw1 = (L(zvel0, j, k, l) + L(zvel0, j, k + 1, l) + L(zvel0, j + 1, k, l) +
+                        L(zvel0, j + 1, k + 1, l)) * za;
+    const double dw2 = (L(zvel0, j, k, l + 1) + L(zvel0, j, k + 1, l + 1) +
+                        L(zvel0, j + 1, k, l + 1) + L(zvel0, j + 1, k + 1, l + 1)) * za;
+    const double dtwt = dtw_safe * 4.0 * vol / fmax2(fmax2(fabs(dw1), fabs(dw2)), 1.0e-5 * vol);
+
+    const double div = du2 - du1 + dv2 - dv1 + dw2 - dw1;
+    const double dtdivt = dtdiv_safe * 4.0 * vol / fmax2(vol * 1.0e-05, fabs(div));
+
+    const double mn = fmin2(fmin2(fmin2(fmin2(dtct, dtut), dtvt), dtwt), dtdivt);
+    if (dt_min) E(dt_min, j, k, l) = st<typename S::wk_t>(mn);
+    if (!(mn != mn)) key = key_of(mn);
+  }
+  // warp then block minimum, one atomic per block
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    unsigned long long other = __shfl_xor_sync(0xffffffffu, key, o);
+    key = other < key ? other : key;
+  }
+  __shared__ unsigned long long wmin[BX * BY / 32];
+  const int lane = threadIdx.x, warp = threadIdx.y;
+  if (lane == 0) wmin[warp] = key;
+  __syncthreads();
+  if (warp == 0) {
+    key = lane < BX * BY / 32 ? wmin[lane] : ~0ull;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      unsigned long long other = __shfl_xor_sync(0xffffffffu, key, o);
+      key = other < key ? other : key;
+    }
+    if (lane == 0 && key != ~0ull) atomicMin(min_key, key);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// PdV_kernel.f90:72-166
+template <class S>
+__global__ void __launch_bounds__(BX * BY) k_pdv(Geom g, Box b, int predict, double dt_val,
+    const double* dt_ptr, GeomArrays ga, const typename S::rho_t* __restrict__ density0,
+    typename S::rho_t* __restrict__ density1, const typename S::ene_t* __restrict__ energy0,
+    typename S::ene_t* __restrict__ energy1, const typename S::cs_t* __restrict__ pressure,
+    const typename S::cs_t* __restrict__ viscosity, const typename S::vel_t* __restrict__ xvel0,
+    const typename S::vel_t* __restrict__ xvel1, const typename S::vel_t* __restrict__ yvel0,
+    const typename S::vel_t* __restrict__ yvel1, const typename S::vel_t* __restrict__ zvel0,
+    const typename S::vel_t* __restrict__ zvel1) {
+  BOX_THREAD(b);
+  const double dt = dt_of(dt_val, dt_ptr);
+  // predictor: the second velocity set is vel0 again and the flux carries *0.5
+  const typename S::vel_t* xb = predict ? xvel0 : xvel1;
+  const typename S::vel_t* yb = predict ? yvel0 : yvel1;
+  const typename S::vel_t* zb = predict ? zvel0 : zvel1;
+#define XF(jj)                                                                            \
+  (E(ga.xarea, jj, k, l) * (L(xvel0, jj, k, l) + L(xvel0, jj, k + 1, l) + L(xvel0, jj, k, l + 1) + \
+                            L(xvel0, jj, k + 1, l + 1) + L(xb, jj, k, l) + L(xb, jj, k + 1, l) +   \
+                            L(xb, jj, k, l + 1) + L(xb, jj, k + 1, l + 1)))
+#define YF(kk)                                                                            \
+  (E(ga.yarea, j, kk, l) * (L(yvel0, j, kk, l) + L(yvel0, j + 1, kk, l) + L(yvel0, j, kk, l + 1) + \
+                            L(yvel0, j + 1, kk, l + 1) + L(yb, j, kk, l) + L(yb, j + 1, kk, l) +   \
+                            L(yb, j, kk, l + 1) + L(yb, j + 1, kk, l + 1)))
+#define ZF(ll)                                                                            \
+  (E(ga.zarea, j, k, ll) * (L(zvel0, j, k, ll) + L(zvel0, j + 1, k, ll) + L(zvel0, j, k + 1, ll) + \
+                            L(zvel0, j + 1, k + 1, ll) + L(zb, j, k, ll) + L(zb, j + 1, k, ll) +   \
+                            L(zb, j, k + 1, ll) + L(zb, j + 1, k + 1, ll)))
+  double left_flux, right_flux, bottom_flux, top_flux, back_flux, front_flux;
+  if (predict) {
+    left_flux = XF(j) * 0.125 * dt * 0.5;
+    right_flux = XF(j + 1) * 0.125 * dt * 0.5;
+    bottom_flux = YF(k) * 0.125 * dt * 0.5;
+    top_flux = YF(k + 1) * 0.125 * dt * 0.5;
+    back_flux = ZF(l) * 0.125 * dt * 0.5;
+    front_flux = ZF(l + 1) * 0.125 * dt * 0.5;
+  } else {
+    left_flux = XF(j) * 0.125 * dt;
+    right_flux = XF(j + 1) * 0.125 * dt;
+    bottom_flux = YF(k) * 0.125 * dt;
+    top_flux = YF(k + 1) * 0.125 * dt;
+    back_flux = ZF(l) * 0.125 * dt;
+    front_flux = ZF(l + 1) * 0.125 * dt;
+  }
+#undef XF
+#undef YF
+#undef ZF
+  const double total_flux = right_flux - left_flux + top_flux - bottom_flux + front_flux - back_flux;
+  const double vol = E(ga.volume, j, k, l);
+  const double vol_change_s = vol / (vol + total_flux);
+  const double recip_volume = 1.0 / vol;
+  const double d0 = L(density0, j, k, l);
+  const double energy_change =
+      (L(pressure, j, k, l) / d0 + L(viscosity, j, k, l) / d0) * total_flux * recip_volume;
+  E(energy1, j, k, l) = st<typename S::ene_t>(L(energy0, j, k, l) - energy_change);
+  E(density1, j, k, l) = st<typename S::rho_t>(d0 * vol_change_s);
+}
+
+// ---------------------------------------------------------------------------
+// revert_kernel.f90:41-61
+template <class S>
+__global__ void __launch_bounds__(BX * BY) k_revert(Geom g, Box b,
+    const typename S::rho_t* __restrict__ density0, typename S::rho_t* __restrict__ density1,
+    const typename S::ene_t* __restrict__ energy0, typename S::ene_t* __restrict__ energy1) {
+  BOX_THREAD(b);
+  E(density1, j, k, l) = E(density0, j, k, l);
+  E(energy1, j, k, l) = E(energy0, j, k, l);
+}
+
+// ---------------------------------------------------------------------------
+// accelerate_kernel.f90:61-109
+template <class S>
+__global__ void __launch_bounds__(BX * BY) k_accelerate(Geom g, Box b, double dt_val,
+    const double* dt_ptr, GeomArrays ga, const typename S::rho_t* __restrict__ density0,
+    const typename S::cs_t* __restrict__ pressure, const typename S::cs_t* __restrict__ viscosity,
+    const typename S::vel_t* __restrict__ xvel0, const typename S::vel_t* __restrict__ yvel0,
+    const typename S::vel_t* __restrict__ zvel0, typename S::vel_t* __restrict__ xvel1,
+    typename S::vel_t* __restrict__ yvel1, typename S::vel_t* __restrict__ zvel1) {
+  BOX_THREAD(b);
+  const double dt = dt_of(dt_val, dt_ptr);
+#define DV(a, bb, c) (L(density0, j + (a), k + (bb), l + (c)) * E(ga.volume, j + (a), k + (bb), l + (c)))
+  const double nodal_mass = (DV(-1, -1, 0) + DV(0, -1, 0) + DV(0, 0, 0) + DV(-1, 0, 0) +
+                             DV(-1, -1, -1) + DV(0, -1, -1) + DV(0, 0, -1) + DV(-1, 0, -1)) * 0.125;
+#undef DV
+  const double stepbymass_s = 0.25 * dt / nodal_mass;
+  const double p000 = L(pressure, j, k, l), p100 = L(pressure, j - 1, k, l);
+  const double p010 = L(pressure, j, k - 1, l), p110 = L(pressure, j - 1, k - 1, l);
+  const double p001 = L(pressure, j, k, l - 1), p101 = L(pressure, j - 1, k, l - 1);
+  const double p011 = L(pressure, j, k - 1, l - 1), p111 = L(pressure, j - 1, k - 1, l - 1);
+  const double q000 = L(viscosity, j, k, l), q100 = L(viscosity, j - 1, k, l);
+  const double q010 = L(viscosity, j, k - 1, l), q110 = L(viscosity, j - 1, k - 1, l);
+  const double q001 = L(viscosity, j, k, l - 1), q101 = L(viscosity, j - 1, k, l - 1);
+  const double q011 = L(viscosity, j, k - 1, l - 1), q111 = L(viscosity, j - 1, k - 1, l - 1);
+  const double xa0 = E(ga.xarea, j, k, l), xa1 = E(ga.xarea, j, k - 1, l);
+  const double xa2 = E(ga.xarea, j, k, l - 1), xa3 = E(ga.xarea, j, k - 1, l - 1);
+  const double ya0 = E(ga.yarea, j, k, l), ya1 = E(ga.yarea, j - 1, k, l);
+  const double ya2 = E(ga.yarea, j, k, l - 1), ya3 = E(ga.yarea, j - 1, k, l - 1);
+  const double za0 = E(ga.zarea, j, k, l), za1 = E(ga.zarea, j, k - 1, l);
+  const double za2 = E(ga.zarea, j - 1, k, l), za3 = E(ga.zarea, j - 1, k - 1, l);
+
+  const double xvel1_s = L(xvel0, j, k, l) -
+      stepbymass_s * (xa0 * (p000 - p100) + xa1 * (p010 - p110) + xa2 * (p001 - p101) +
+                      xa3 * (p011 - p111));
+  const double yvel1_s = L(yvel0, j, k, l) -
+      stepbymass_s * (ya0 * (p000 - p010) + ya1 * (p100 - p110) + ya2 * (p001 - p011) +
+                      ya3 * (p101 - p111));
+  const double zvel1_s = L(zvel0, j, k, l) -
+      stepbymass_s * (za0 * (p000 - p001) + za1 * (p010 - p011) + za2 * (p100 - p101) +
+                      za3 * (p110 - p111));
+  using V = typename S::vel_t;
+  E(xvel1, j, k, l) = st<V>(xvel1_s -
+      stepbymass_s * (xa0 * (q000 - q100) + xa1 * (q010 - q110) + xa2 * (q001 - q101) +
+                      xa3 * (q011 - q111)));
+  E(yvel1, j, k, l) = st<V>(yvel1_s -
+      stepbymass_s * (ya0 * (q000 - q010) + ya1 * (q100 - q110) + ya2 * (q001 - q011) +
+                      ya3 * (q101 - q111)));
+  E(zvel1, j, k, l) = st<V>(zvel1_s -
+      stepbymass_s * (za0 * (q000 - q001) + za1 * (q010 - q011) + za2 * (q100 - q101) +
+                      za3 * (q110 - q111)));
+}
+
+// ---------------------------------------------------------------------------
+// flux_calc_kernel.f90:58-91: one launch over the union of the three face
+// ranges. The z sum repeats zvel0(j+1,k,l) and omits zvel0(j,k+1,l) (:86).
+template <class S>
+__global__ void __launch_bounds__(BX * BY) k_flux_calc(Geom g, Box b, double dt_val,
+    const double* dt_ptr, GeomArrays ga, const typename S::vel_t* __restrict__ xvel0,
+    const typename S::vel_t* __restrict__ yvel0, const typename S::vel_t* __restrict__ zvel0,
+    const typename S::vel_t* __restrict__ xvel1, const typename S::vel_t* __restrict__ yvel1,
+    const typename S::vel_t* __restrict__ zvel1, typename S::vf_t* __restrict__ vol_flux_x,
+    typename S::vf_t* __restrict__ vol_flux_y, typename S::vf_t* __restrict__ vol_flux_z) {
+  BOX_THREAD(b);
+  const double dt = dt_of(dt_val, dt_ptr);
+  using F = typename S::vf_t;
+  const bool jin = j <= g.x_max, kin = k <= g.y_max, lin = l <= g.z_max;
+  if (kin && lin)
+    E(vol_flux_x, j, k, l) = st<F>(0.125 * dt * E(ga.xarea, j, k, l) *
+        (L(xvel0, j, k, l) + L(xvel0, j, k + 1, l) + L(xvel0, j, k, l + 1) + L(xvel0, j, k + 1, l + 1) +
+         L(xvel1, j, k, l) + L(xvel1, j, k + 1, l) + L(xvel1, j, k, l + 1) + L(xvel1, j, k + 1, l + 1)));
+  if (jin && lin)
+    E(vol_flux_y, j, k, l) = st<F>(0.125 * dt * E(ga.yarea, j, k, l) *
+        (L(yvel0, j, k, l) + L(yvel0, j + 1, k, l) + L(yvel0, j, k, l + 1) + L(yvel0, j + 1, k, l + 1) +
+         L(yvel1, j, k, l) + L(yvel1, j + 1, k, l) + L(yvel1, j, k, l + 1) + L(yvel1, j + 1, k, l + 1)));
+  if (jin && kin)
+    E(vol_flux_z, j, k, l) = st<F>(0.125 * dt * E(ga.zarea, j, k, l) *
+        (L(zvel0, j, k, l) + L(zvel0, j + 1, k, l) + L(zvel0, j + 1, k, l) + L(zvel0, j + 1, k + 1, l) +
+         L(zvel1, j, k, l) + L(zvel1, j + 1, k, l) + L(zvel1, j, k + 1, l) + L(zvel1, j + 1, k + 1, l)));
+}
+
+// ---------------------------------------------------------------------------
+// advec_cell_kernel.f90: pre/post volume pass (:97-121, :190-216, :287-311)
+template <class S>
+__global__ void __launch_bounds__(BX * BY) k_cell_vol(Geom g, Box b, int variant, GeomArrays ga,
+    const typename S::vf_t* __restrict__ vfx, const typename S::vf_t* __restrict__ vfy,
+    const typename S::vf_t* __restrict__ vfz, typename S::wk_t* __restrict__ pre_vol,
+    typename S::wk_t* __restrict__ post_vol) {
+  BOX_THREAD(b);
+  const double vol = E(ga.volume, j, k, l);
+  const double fx1 = L(vfx, j + 1, k, l), fx0 = L(vfx, j, k, l);
+  const double fy1 = L(vfy, j, k + 1, l), fy0 = L(vfy, j, k, l);
+  const double fz1 = L(vfz, j, k, l + 1), fz0 = L(vfz, j, k, l);
+  double pre, post;
+  switch (variant) {
+    case 0:  // x, sweep 1
+      pre = vol + (fx1 - fx0 + fy1 - fy0 + fz1 - fz0);
+      post = pre - (fx1 - fx0);
+      break;
+    case 1:  // x, sweep 3
+      pre = vol + fx1 - fx0;
+      post = vol;
+      break;
+    case 2:  // y, sweep 2, advect_x
+      pre = vol + fy1 - fy0 + fz1 - fz0;
+      post = pre - (fy1 - fy0);
+      break;
+    case 3:  // y, sweep 2, not advect_x
+      pre = vol + fy1 - fy0 + fx1 - fx0;
+      post = pre - (fy1 - fy0);
+      break;
+    case 4:  // z, sweep 1
+      pre = vol + (fx1 - fx0 + fy1 - fy0 + fz1 - fz0);
+      post = pre - (fz1 - fz0);
+      break;
+    default:  // z, sweep 3
+      pre = vol + fz1 - fz0;
+      post = vol;
+      break;
+  }
+  using W = typename S::wk_t;
+  E(pre_vol, j, k, l) = st<W>(pre);
+  E(post_vol, j, k, l) = st<W>(post);
+}
+
+__device__ __forceinline__ double cell_limiter(double sig, double sigma3, double sigma4,
+                                               double diffuw, double diffdw) {
+  const double one_by_six = 1.0 / 6.0;
+  if (diffuw * diffdw > 0.0)
+    return (1.0 - sig) * copysign(1.0, diffdw) *
+           fmin2(fmin2(fabs(diffuw), fabs(diffdw)),
+                 one_by_six * (sigma3 * fabs(diffuw) + sigma4 * fabs(diffdw)));
+  return 0.0;
+}
+
+// advec_cell_kernel.f90 flux pass (:125-171 x, :220-266 y, :315-361 z).
+// DIR is the sweep axis; (dj,dk,dl) its unit offset.
+template <class S, int DIR>
+__global__ void __launch_bounds__(BX * BY) k_cell_flux(Geom g, Box b, GeomArrays ga,
+    const typename S::rho_t* __restrict__ density1, const typename S::ene_t* __restrict__ energy1,
+    const typename S::vf_t* __restrict__ vol_flux, typename S::mf_t* __restrict__ mass_flux,
+    const typename S::wk_t* __restrict__ pre_vol, typename S::wk_t* __restrict__ ener_flux) {
+  BOX_THREAD(b);
+  const int i = DIR == 1 ? j : DIR == 2 ? k : l;
+  const int imax = DIR == 1 ? g.x_max : DIR == 2 ? g.y_max : g.z_max;
+  const double* vd = DIR == 1 ? ga.vertexdx : DIR == 2 ? ga.vertexdy : ga.vertexdz;
+  const int vlo = DIR == 1 ? g.x_min : DIR == 2 ? g.y_min : g.z_min;
+  const double vf = L(vol_flux, j, k, l);
+  int upwind, donor, downwind, dif;
+  if (vf > 0.0) {
+    upwind = i - 2; donor = i - 1; downwind = i; dif = donor;
+  } else {
+    upwind = (i + 1 < imax + 2) ? i + 1 : imax + 2;
+    donor = i; downwind = i - 1; dif = upwind;
+  }
+#define AT(a, ii) L(a, DIR == 1 ? (ii) : j, DIR == 2 ? (ii) : k, DIR == 3 ? (ii) : l)
+  const double pv_donor = AT(pre_vol, donor);
+  const double sigmat = fabs(vf) / pv_donor;
+  const double sigma3 = (1.0 + sigmat) * (vd[i - vlo + 2] / vd[dif - vlo + 2]);
+  const double sigma4 = 2.0 - sigmat;
+  const double sigmav = sigmat;
+
+  const double d_donor = AT(density1, donor);
+  double diffuw = d_donor - AT(density1, upwind);
+  double diffdw = AT(density1, downwind) - d_donor;
+  double limiter = cell_limiter(sigmav, sigma3, sigma4, diffuw, diffdw);
+  const double mflux = vf * (d_donor + limiter);
+  E(mass_flux, j, k, l) = st<typename S::mf_t>(mflux);
+
+  const double sigmam = fabs(mflux) / (d_donor * pv_donor);
+  const double e_donor = AT(energy1, donor);
+  diffuw = e_donor - AT(energy1, upwind);
+  diffdw = AT(energy1, downwind) - e_donor;
+  limiter = cell_limiter(sigmam, sigma3, sigma4, diffuw, diffdw);
+  E(ener_flux, j, k, l) = st<typename S::wk_t>(mflux * (e_donor + limiter));
+#undef AT
+}
+
+// advec_cell_kernel.f90 update pass (:175-186 x, :270-281 y, :365-376 z)
+template <class S, int DIR>
+__global__ void __launch_bounds__(BX * BY) k_cell_update(Geom g, Box b,
+    typename S::rho_t* __restrict__ density1, typename S::ene_t* __restrict__ energy1,
+    const typename S::vf_t* __restrict__ vol_flux, const typename S::mf_t* __restrict__ mass_flux,
+    const typename S::wk_t* __restrict__ pre_vol, typename S::wk_t* __restrict__ pre_mass,
+    typename S::wk_t* __restrict__ post_mass, typename S::wk_t* __restrict__ advec_vol,
+    typename S::wk_t* __restrict__ post_ener, const typename S::wk_t* __restrict__ ener_flux) {
+  BOX_THREAD(b);
+  const int j1 = j + (DIR == 1), k1 = k + (DIR == 2), l1 = l + (DIR == 3);
+  const double pv = L(pre_vol, j, k, l);
+  const double pm = L(density1, j, k, l) * pv;
+  const double pom = pm + L(mass_flux, j, k, l) - L(mass_flux, j1, k1, l1);
+  const double poe = (L(energy1, j, k, l) * pm + L(ener_flux, j, k, l) - L(ener_flux, j1, k1, l1)) / pom;
+  const double av = pv + L(vol_flux, j, k, l) - L(vol_flux, j1, k1, l1);
+  using W = typename S::wk_t;
+  if (pre_mass) {
+    E(pre_mass, j, k, l) = st<W>(pm);
+    E(post_mass, j, k, l) = st<W>(pom);
+    E(post_ener, j, k, l) = st<W>(poe);
+    E(advec_vol, j, k, l) = st<W>(av);
+  }
+  E(density1, j, k, l) = st<typename S::rho_t>(pom / av);
+  E(energy1, j, k, l) = st<typename S::ene_t>(poe);
+}
+
+// ---------------------------------------------------------------------------
+// advec_mom_kernel.f90 pre/post volume variants (:95-163)
+template <class S>
+__global__ void __launch_bounds__(BX * BY) k_mom_vol(Geom g, Box b, int variant, GeomArrays ga,
+    const typename S::vf_t* __restrict__ vfx, const typename S::vf_t* __restrict__ vfy,
+    const typename S::vf_t* __restrict__ vfz, typename S::wk_t* __restrict__ pre_vol,
+    typename S::wk_t* __restrict__ post_vol) {
+  BOX_THREAD(b);
+  const double vol = E(ga.volume, j, k, l);
+  const double fx1 = L(vfx, j + 1, k, l), fx0 = L(vfx, j, k, l);
+  const double fy1 = L(vfy, j, k + 1, l), fy0 = L(vfy, j, k, l);
+  const double fz1 = L(vfz, j, k, l + 1), fz0 = L(vfz, j, k, l);
+  double post, pre;
+  switch (variant) {
+    case 0:  // sweep 1, direction x
+      post = vol + fy1 - fy0 + fz1 - fz0;
+      pre = post + fx1 - fx0;
+      break;
+    case 1:  // sweep 1, direction z
+      post = vol + fx1 - fx0 + fy1 - fy0;
+      pre = post + fz1 - fz0;
+      break;
+    case 2:  // sweep 2, advect_x
+      post = vol + fz1 - fz0;
+      pre = post + fy1 - fy0;
+      break;
+    case 3:  // sweep 2, not advect_x
+      post = vol + fx1 - fx0;
+      pre = post + fy1 - fy0;
+      break;
+    case 4:  // sweep 3, direction x
+      post = vol;
+      pre = post + fx1 - fx0;
+      break;
+    default:  // sweep 3, direction z
+      post = vol;
+      pre = post + fz1 - fz0;
+      break;
+  }
+  using W = typename S::wk_t;
+  E(post_vol, j, k, l) = st<W>(post);
+  E(pre_vol, j, k, l) = st<W>(pre);
+}
+
+// node_flux (:166-176 x, :254-263 y, :339-349 z) and node_mass_post
+// (:177-193, :264-279, :350-365) over the union of their ranges.
+template <class S, int DIR>
+__global__ void __launch_bounds__(BX * BY) k_mom_node(Geom g, Box b, Box bflux, Box bmass,
+    const typename S::mf_t* __restrict__ mf, const typename S::rho_t* __restrict__ density1,
+    const typename S::wk_t* __restrict__ post_vol, typename S::wk_t* __restrict__ node_flux,
+    typename S::wk_t* __restrict__ node_mass_post) {
+  BOX_THREAD(b);
+  using W = typename S::wk_t;
+  if (j >= bflux.j0 && j <= bflux.j1 && k >= bflux.k0 && k <= bflux.k1 && l >= bflux.l0 &&
+      l <= bflux.l1) {
+    double nf;
+    if (DIR == 1)
+      nf = 0.125 * (L(mf, j, k - 1, l) + L(mf, j, k, l) + L(mf, j + 1, k - 1, l) + L(mf, j + 1, k, l) +
+                    L(mf, j, k - 1, l - 1) + L(mf, j, k, l - 1) + L(mf, j + 1, k - 1, l - 1) +
+                    L(mf, j + 1, k, l - 1));
+    else if (DIR == 2)
+      nf = 0.125 * (L(mf, j - 1, k, l) + L(mf, j, k, l) + L(mf, j - 1, k + 1, l) + L(mf, j, k + 1, l) +
+                    L(mf, j - 1, k, l - 1) + L(mf, j, k, l - 1) + L(mf, j - 1, k + 1, l - 1) +
+                    L(mf, j, k + 1, l - 1));
+    else
+      nf = 0.125 * (L(mf, j - 1, k, l) + L(mf, j, k, l) + L(mf, j - 1, k, l + 1) + L(mf, j, k, l + 1) +
+                    L(mf, j - 1, k - 1, l) + L(mf, j, k - 1, l) + L(mf, j - 1, k - 1, l + 1) +
+                    L(mf, j, k - 1, l + 1));
+    E(node_flux, j, k, l) = st<W>(nf);
+  }
+  if (j >= bmass.j0 && j <= bmass.j1 && k >= bmass.k0 && k <= bmass.k1 && l >= bmass.l0 &&
+      l <= bmass.l1) {
+#define DP(a, bb, c) (L(density1, j + (a), k + (bb), l + (c)) * L(post_vol, j + (a), k + (bb), l + (c)))
+    const double nm = 0.125 * (DP(0, -1, 0) + DP(0, 0, 0) + DP(-1, -1, 0) + DP(-1, 0, 0) +
+                               DP(0, -1, -1) + DP(0, 0, -1) + DP(-1, -1, -1) + DP(-1, 0, -1));
+#undef DP
+    E(node_mass_post, j, k, l) = st<W>(nm);
+  }
+}
+
+// node_mass_pre (:194-202 x, :280-288 y, :366-374 z)
+template <class S, int DIR>
+__global__ void __launch_bounds__(BX * BY) k_mom_nmpre(Geom g, Box b,
+    const typename S::wk_t* __restrict__ node_flux, const typename S::wk_t* __restrict__ node_mass_post,
+    typename S::wk_t* __restrict__ node_mass_pre) {
+  BOX_THREAD(b);
+  const double prev = DIR == 1 ? L(node_flux, j - 1, k, l)
+                    : DIR == 2 ? L(node_flux, j, k - 1, l) : L(node_flux, j, k, l - 1);
+  E(node_mass_pre, j, k, l) =
+      st<typename S::wk_t>(L(node_mass_post, j, k, l) - prev + L(node_flux, j, k, l));
+}
+
+__device__ __forceinline__ double mom_limiter(double sigma, double width, double celld_dif,
+                                              double vdiffuw, double vdiffdw) {
+  double limiter = 0.0;
+  if (vdiffuw * vdiffdw > 0.0) {
+    const double auw = fabs(vdiffuw);
+    const double adw = fabs(vdiffdw);
+    double wind = 1.0;
+    if (vdiffdw <= 0.0) wind = -1.0;
+    limiter = wind * fmin2(fmin2(width * ((2.0 - sigma) * adw / width +
+                                          (1.0 + sigma) * auw / celld_dif) / 6.0,
+                                 auw),
+                           adw);
+  }
+  return limiter;
+}
+
+// mom_flux (:211-242 x, :295-327 y, :381-413 z)
+template <class S, int DIR>
+__global__ void __launch_bounds__(BX * BY) k_mom_flux(Geom g, Box b, GeomArrays ga,
+    const typename S::vel_t* __restrict__ vel1, const typename S::wk_t* __restrict__ node_flux,
+    const typename S::wk_t* __restrict__ node_mass_pre, typename S::wk_t* __restrict__ mom_flux) {
+  BOX_THREAD(b);
+  const int i = DIR == 1 ? j : DIR == 2 ? k : l;
+  const double nf = L(node_flux, j, k, l);
+  int upwind, donor, downwind, dif;
+  if (nf < 0.0) {
+    upwind = i + 2; donor = i + 1; downwind = i; dif = donor;
+  } else {
+    upwind = i - 1; donor = i; downwind = i + 1; dif = upwind;
+  }
+#define AT(a, ii) L(a, DIR == 1 ? (ii) : j, DIR == 2 ? (ii) : k, DIR == 3 ? (ii) : l)
+  const double sigma = fabs(nf) / AT(node_mass_pre, donor);
+  const double* cd = DIR == 1 ? ga.celldx : DIR == 2 ? ga.celldy : ga.celldz;
+  const int clo = DIR == 1 ? g.x_min : DIR == 2 ? g.y_min : g.z_min;
+  const double width = cd[i - clo + 2];
+  const double v_donor = AT(vel1, donor);
+  const double vdiffuw = v_donor - AT(vel1, upwind);
+  const double vdiffdw = AT(vel1, downwind) - v_donor;
+  const double limiter = mom_limiter(sigma, width, cd[dif - clo + 2], vdiffuw, vdiffdw);
+  const double advec_vel_s = v_donor + (1.0 - sigma) * limiter;
+  E(mom_flux, j, k, l) = st<typename S::wk_t>(advec_vel_s * nf);
+#undef AT
+}
+
+// velocity update (:245-252 x, :330-337 y, :416-423 z)
+template <class S, int DIR>
+__global__ void __launch_bounds__(BX * BY) k_mom_update(Geom g, Box b,
+    typename S::vel_t* __restrict__ vel1, const typename S::wk_t* __restrict__ node_mass_pre,
+    const typename S::wk_t* __restrict__ node_mass_post, const typename S::wk_t* __restrict__ mom_flux) {
+  BOX_THREAD(b);
+  const double prev = DIR == 1 ? L(mom_flux, j - 1, k, l)
+                    : DIR == 2 ? L(mom_flux, j, k - 1, l) : L(mom_flux, j, k, l - 1);
+  E(vel1, j, k, l) = st<typename S::vel_t>(
+      (L(vel1, j, k, l) * L(node_mass_pre, j, k, l) + prev - L(mom_flux, j, k, l)) /
+      L(node_mass_post, j, k, l));
+}
+
+// ---------------------------------------------------------------------------
+// reset_field_kernel.f90:51-98 (cell part over the interior, vertex part over
+// the interior nodes; one launch over the node box)
+template <class S>
+__global__ void __launch_bounds__(BX * BY) k_reset(Geom g, Box b,
+    typename S::rho_t* __restrict__ density0, const typename S::rho_t* __restrict__ density1,
+    typename S::ene_t* __restrict__ energy0, const typename S::ene_t* __restrict__ energy1,
+    typename S::vel_t* __restrict__ xvel0, const typename S::vel_t* __restrict__ xvel1,
+    typename S::vel_t* __restrict__ yvel0, const typename S::vel_t* __restrict__ yvel1,
+    typename S::vel_t* __restrict__ zvel0, const typename S::vel_t* __restrict__ zvel1) {
+  BOX_THREAD(b);
+  if (j <= g.x_max && k <= g.y_max && l <= g.z_max) {
+    E(density0, j, k, l) = E(density1, j, k, l);
+    E(energy0, j, k, l) = E(energy1, j, k, l);
+  }
+  E(xvel0, j, k, l) = E(xvel1, j, k, l);
+  E(yvel0, j, k, l) = E(yvel1, j, k, l);
+  E(zvel0, j, k, l) = E(zvel1, j, k, l);
+}
+
+// ---------------------------------------------------------------------------
+// field_summary_kernel.f90:57-77: a fixed grid of SUM_BLOCKS blocks strides
+// over the interior cells in a fixed assignment; each block tree-reduces its
+// five partials; a one-block pass adds the partials in block order. The
+// result is the same on every run.
+constexpr int SUM_THREADS = 256;
+constexpr int SUM_BLOCKS = 148 * 4;
+
+__device__ __forceinline__ void block_sum5(double v[5], double* sh /*5*SUM_THREADS*/) {
+  const int t = threadIdx.x;
+  for (int q = 0; q < 5; q++) sh[q * SUM_THREADS + t] = v[q];
+  __syncthreads();
+  for (int s = SUM_THREADS / 2; s > 0; s >>= 1) {
+    if (t < s)
+      for (int q = 0; q < 5; q++) sh[q * SUM_THREADS + t] += sh[q * SUM_THREADS + t + s];
+    __syncthreads();
+  }
+  for (int q = 0; q < 5; q++) v[q] = sh[q * SUM_THREADS];
+}
+
+template <class S>
+__global__ void __launch_bounds__(SUM_THREADS) k_summary(Geom g, const double* __restrict__ volume,
+    const typename S::rho_t* __restrict__ density0, const typename S::ene_t* __restrict__ energy0,
+    const typename S::cs_t* __restrict__ pressure, const typename S::vel_t* __restrict__ xvel0,
+    const typename S::vel_t* __restrict__ yvel0, const typename S::vel_t* __restrict__ zvel0,
+    double* __restrict__ partials) {
+  __shared__ double sh[5 * SUM_THREADS];
+  const int nx = g.x_max - g.x_min + 1, ny = g.y_max - g.y_min + 1, nz = g.z_max - g.z_min + 1;
+  const long long n = (long long)nx * ny * nz;
+  double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+  for (long long c = (long long)blockIdx.x * SUM_THREADS + threadIdx.x; c < n;
+       c += (long long)SUM_BLOCKS * SUM_THREADS) {
+    const int j = g.x_min + (int)(c % nx);
+    const long long r = c / nx;
+    const int k = g.y_min + (int)(r % ny);
+    const int l = g.z_min + (int)(r / ny);
+    double vsqrd = 0.0;
+    for (int lv = l; lv <= l + 1; lv++)
+      for (int kv = k; kv <= k + 1; kv++)
+        for (int jv = j; jv <= j + 1; jv++) {
+          const double u = L(xvel0, jv, kv, lv), v = L(yvel0, jv, kv, lv), w = L(zvel0, jv, kv, lv);
+          vsqrd = vsqrd + 0.125 * (u * u + v * v + w * w);
+        }
+    const double cell_vol = E(volume, j, k, l);
+    const double cell_mass = cell_vol * L(density0, j, k, l);
+    acc[0] = acc[0] + cell_vol;
+    acc[1] = acc[1] + cell_mass;
+    acc[2] = acc[2] + cell_mass * L(energy0, j, k, l);
+    acc[3] = acc[3] + cell_mass * 0.5 * vsqrd;
+    acc[4] = acc[4] + cell_vol * L(pressure, j, k, l);
+  }
+  block_sum5(acc, sh);
+  if (threadIdx.x == 0)
+    for (int q = 0; q < 5; q++) partials[blockIdx.x * 5 + q] = acc[q];
+}
+
+__global__ void __launch_bounds__(SUM_THREADS) k_summary_final(const double* __restrict__ partials,
+                                                               double* __restrict__ out5) {
+  __shared__ double sh[5 * SUM_THREADS];
+  double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+  for (int i = threadIdx.x; i < SUM_BLOCKS; i += SUM_THREADS)
+    for (int q = 0; q < 5; q++) acc[q] = acc[q] + partials[i * 5 + q];
+  block_sum5(acc, sh);
+  if (threadIdx.x == 0)
+    for (int q = 0; q < 5; q++) out5[q] = acc[q];
+}
+
+// ---------------------------------------------------------------------------
+// update_halo_kernel.f90:115-1423, table driven. For a face of normal axis A
+// and m = 1..depth:
+//   low face : dst = 1 - m,        src = low_src + m
+//   high face: dst = max + hi_dst + m, src = max + hi_src - m
+// with sign -1 where the reference negates. The two tangential loops run over
+// [min-depth, max+depth+ext] with ext (0 or 1) per field, face and axis.
+struct HaloRule {
+  signed char sign, low_src, hi_dst, hi_src;
+  signed char ext_lo[3], ext_hi[3];  // per axis x,y,z: extent of the low / high face loops
+};
+
+// kind: 0 cell, 1 vertex (comp = velocity component), 2 face (comp = normal)
+inline HaloRule make_rule(int kind, int comp, int face_axis, int field_id) {
+  HaloRule r;
+  for (int a = 0; a < 3; a++) { r.ext_lo[a] = 0; r.ext_hi[a] = 0; }
+  if (kind == 0) {  // :121-590
+    r.sign = 1; r.low_src = 0; r.hi_dst = 0; r.hi_src = 1;
+  } else if (kind == 1) {  // :604-1004
+    r.sign = comp == face_axis ? -1 : 1;
+    r.low_src = 1; r.hi_dst = 1; r.hi_src = 1;
+    for (int a = 0; a < 3; a++) { r.ext_lo[a] = 1; r.ext_hi[a] = 1; }
+  } else {  // :1018-1417
+    if (comp == face_axis) {
+      r.sign = -1; r.low_src = 1; r.hi_dst = 1; r.hi_src = 1;
+    } else {
+      r.sign = 1; r.low_src = 1; r.hi_dst = 0; r.hi_src = 0;
+    }
+    // Tangential extents: the face-normal axis of the field runs one further,
+    // except on the z faces (back/front), which never extend.
+    if (face_axis != 2 && comp != face_axis) { r.ext_lo[comp] = 1; r.ext_hi[comp] = 1; }
+    // vol_flux_z (id 16) on the bottom face stops at z_max+depth (:1297-1303)
+    if (field_id == 16 && face_axis == 1) r.ext_lo[2] = 0;
+  }
+  return r;
+}
+
+struct HaloLaunch {
+  void* f[19];
+  int elem_bytes[19];
+  HaloRule rule[19];
+  int nfields;
+  int ids[19];
+};
+
+template <int AX>
+__global__ void k_halo(Geom g, HaloLaunch h, int depth, int do_low, int do_high) {
+  // tangential axes: y faces (j,l), x faces (k,l), z faces (j,k)
+  const int ta = AX == 0 ? 1 : 0;  // first tangential axis
+  const int tb = AX == 2 ? 1 : 2;  // second tangential axis
+  const int mins[3] = {g.x_min, g.y_min, g.z_min};
+  const int maxs[3] = {g.x_max, g.y_max, g.z_max};
+  const int a = mins[ta] - depth + blockIdx.x * blockDim.x + threadIdx.x;
+  const int bb = mins[tb] - depth + blockIdx.y * blockDim.y + threadIdx.y;
+  if (a > maxs[ta] + 1 + depth || bb > maxs[tb] + 1 + depth) return;
+  const int n = maxs[AX];
+  for (int fi = 0; fi < h.nfields; fi++) {
+    const HaloRule r = h.rule[fi];
+    const int id = h.ids[fi];
+    for (int side = 0; side < 2; side++) {
+      if (side == 0 ? !do_low : !do_high) continue;
+      const signed char* ext = side == 0 ? r.ext_lo : r.ext_hi;
+      if (a > maxs[ta] + depth + ext[ta] || bb > maxs[tb] + depth + ext[tb]) continue;
+      for (int m = 1; m <= depth; m++) {
+        const int dst = side == 0 ? 1 - m : n + r.hi_dst + m;
+        const int src = side == 0 ? r.low_src + m : n + r.hi_src - m;
+        int dj, dk, dl, sj, sk, sl;
+        if (AX == 0) { dj = dst; sj = src; dk = sk = a; dl = sl = bb; }
+        else if (AX == 1) { dk = dst; sk = src; dj = sj = a; dl = sl = bb; }
+        else { dl = dst; sl = src; dj = sj = a; dk = sk = bb; }
+        const long long od = off3(g, dj, dk, dl), os = off3(g, sj, sk, sl);
+        if (h.elem_bytes[fi] == 8) {
+          double* p = (double*)h.f[fi];
+          p[od] = r.sign < 0 ? -p[os] : p[os];
+        } else {
+          float* p = (float*)h.f[fi];
+          p[od] = r.sign < 0 ? -p[os] : p[os];
+        }
+      }
+    }
+    (void)id;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// initialise_chunk_kernel.f90:70-178 and generate_chunk_kernel.f90:98-207
+__global__ void k_init_1d(Geom g, double xmin, double ymin, double zmin, double dx, double dy,
+                          double dz, double* vertexx, double* vertexdx, double* vertexy,
+                          double* vertexdy, double* vertexz, double* vertexdz, double* cellx,
+                          double* celldx, double* celly, double* celldy, double* cellz,
+                          double* celldz) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int jx = g.x_min - 2 + t, ky = g.y_min - 2 + t, lz = g.z_min - 2 + t;
+  // float(j-x_min) is a default REAL; small integers convert exactly
+  auto vx = [&](int j) { return xmin + dx * (double)(float)(j - g.x_min); };
+  auto vy = [&](int k) { return ymin + dy * (double)(float)(k - g.y_min); };
+  auto vz = [&](int l) { return zmin + dz * (double)(float)(l - g.z_min); };
+  if (jx <= g.x_max + 3) { GX(vertexx, jx) = vx(jx); GX(vertexdx, jx) = dx; }
+  if (ky <= g.y_max + 3) { GY(vertexy, ky) = vy(ky); GY(vertexdy, ky) = dy; }
+  if (lz <= g.z_max + 3) { GZ(vertexz, lz) = vz(lz); GZ(vertexdz, lz) = dz; }
+  if (jx <= g.x_max + 2) { GX(cellx, jx) = 0.5 * (vx(jx) + vx(jx + 1)); GX(celldx, jx) = dx; }
+  if (ky <= g.y_max + 2) { GY(celly, ky) = 0.5 * (vy(ky) + vy(ky + 1)); GY(celldy, ky) = dy; }
+  if (lz <= g.z_max + 2) { GZ(cellz, lz) = 0.5 * (vz(lz) + vz(lz + 1)); GZ(celldz, lz) = dz; }
+}
+
+__global__ void __launch_bounds__(BX * BY) k_init_3d(Geom g, Box b, double dx, double dy, double dz,
+    const double* celldx, const double* celldy, const double* celldz, double* volume,
+    double* xarea, double* yarea, double* zarea) {
+  BOX_THREAD(b);
+  E(volume, j, k, l) = dx * dy * dz;
+  E(xarea, j, k, l) = GY(celldy, k) * GZ(celldz, l);
+  E(yarea, j, k, l) = GX(celldx, j) * GZ(celldz, l);
+  E(zarea, j, k, l) = GX(celldx, j) * GY(celldy, k);
+}
+
+template <class S>
+__global__ void __launch_bounds__(BX * BY) k_generate_bg(Geom g, Box b, StateTable st,
+    typename S::rho_t* density0, typename S::ene_t* energy0, typename S::vel_t* xvel0,
+    typename S::vel_t* yvel0, typename S::vel_t* zvel0) {
+  BOX_THREAD(b);
+  E(energy0, j, k, l) = st.energy[0];
+  E(density0, j, k, l) = st.density[0];
+  E(xvel0, j, k, l) = st.xvel[0];
+  E(yvel0, j, k, l) = st.yvel[0];
+  E(zvel0, j, k, l) = st.zvel[0];
+}
+
+template <class S>
+__global__ void __launch_bounds__(BX * BY) k_generate_state(Geom g, Box b, GeomArrays ga, int s,
+    StateTable st, typename S::rho_t* density0, typename S::ene_t* energy0,
+    typename S::vel_t* xvel0, typename S::vel_t* yvel0, typename S::vel_t* zvel0) {
+  BOX_THREAD(b);
+  bool hit = false;
+  if (st.geometry[s] == 1) {
+    hit = GX(ga.vertexx, j + 1) >= st.xmin[s] && GX(ga.vertexx, j) < st.xmax[s] &&
+          GY(ga.vertexy, k + 1) >= st.ymin[s] && GY(ga.vertexy, k) < st.ymax[s] &&
+          GZ(ga.vertexz, l + 1) >= st.zmin[s] && GZ(ga.vertexz, l) < st.zmax[s];
+  } else if (st.geometry[s] == 2) {
+    const double cx = GX(ga.cellx, j) - st.xmin[s], cy = GY(ga.celly, k) - st.ymin[s],
+                 cz = GZ(ga.cellz, l) - st.zmin[s];
+    hit = sqrt(cx * cx + cy * cy + cz * cz) <= st.radius[s];
+  } else if (st.geometry[s] == 3) {
+    hit = GX(ga.vertexx, j) == st.xmin[s] && GY(ga.vertexy, k) == st.ymin[s] &&
+          GZ(ga.vertexz, l) == st.zmin[s];
+  }
+  if (!hit) return;
+  E(energy0, j, k, l) = st.energy[s];
+  E(density0, j, k, l) = st.density[s];
+  // every writer of a node writes the same state's value
+  for (int lt = l; lt <= l + 1; lt++)
+    for (int kt = k; kt <= k + 1; kt++)
+      for (int jt = j; jt <= j + 1; jt++) {
+        E(xvel0, jt, kt, lt) = st.xvel[s];
+        E(yvel0, jt, kt, lt) = st.yvel[s];
+        E(zvel0, jt, kt, lt) = st.zvel[s];
+      }
+}
+
+template <class T>
+__global__ void k_fill(T* p, long long n, T v) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    p[i] = v;
+}
+
+}  // namespace
+
+// ===========================================================================
+// Launchers
+#define LAUNCH(kern, box, ...)                                          \
+  do {                                                                  \
+    const Box _b = (box);                                               \
+    const dim3 _gr = grid_of(_b);                                       \
+    if (launchable(_gr)) kern<<<_gr, dim3(BX, BY), 0, s>>>(g, _b, __VA_ARGS__); \
+  } while (0)
+
+static inline Box interior(const Geom& g) {
+  return Box{g.x_min, g.x_max, g.y_min, g.y_max, g.z_min, g.z_max};
+}
+static inline Box nodes(const Geom& g) {
+  return Box{g.x_min, g.x_max + 1, g.y_min, g.y_max + 1, g.z_min, g.z_max + 1};
+}
+static inline Box halo2(const Geom& g) {
+  return Box{g.x_min - 2, g.x_max + 2, g.y_min - 2, g.y_max + 2, g.z_min - 2, g.z_max + 2};
+}
+
+unsigned long long min_key_of(double v) { return key_of(v); }
+double min_key_value(unsigned long long key) {
+  unsigned long long b = (key >> 63) ? (key & 0x7fffffffffffffffull) : ~key;
+  double v;
+  memcpy(&v, &b, sizeof(v));
+  return v;
+}
+
+template <class S>
+void launch_ideal_gas(const Geom& g, cudaStream_t s, const typename S::rho_t* density,
+                      const typename S::ene_t* energy, typename S::cs_t* pressure,
+                      typename S::cs_t* soundspeed) {
+  LAUNCH(k_ideal_gas<S>, interior(g), density, energy, pressure, soundspeed);
+}
+
+template <class S>
+void launch_viscosity(const Geom& g, cudaStream_t s, const GeomArrays& ga,
+                      const typename S::rho_t* density0, const typename S::cs_t* pressure,
+                      typename S::cs_t* viscosity, const typename S::vel_t* xvel0,
+                      const typename S::vel_t* yvel0, const typename S::vel_t* zvel0) {
+  LAUNCH(k_viscosity<S>, interior(g), ga, density0, pressure, viscosity, xvel0, yvel0, zvel0);
+}
+
+template <class S>
+void launch_calc_dt(const Geom& g, cudaStream_t s, const GeomArrays& ga, double g_small,
+                    double dtc_safe, double dtu_safe, double dtv_safe, double dtw_safe,
+                    double dtdiv_safe, const typename S::rho_t* density0,
+                    const typename S::cs_t* viscosity, const typename S::cs_t* soundspeed,
+                    const typename S::vel_t* xvel0, const typename S::vel_t* yvel0,
+                    const typename S::vel_t* zvel0, typename S::wk_t* dt_min_arr,
+                    unsigned long long* min_key) {
+  LAUNCH(k_calc_dt<S>, interior(g), ga, g_small, dtc_safe, dtu_safe, dtv_safe, dtw_safe,
+         dtdiv_safe, density0, viscosity, soundspeed, xvel0, yvel0, zvel0, dt_min_arr, min_key);
+}
+
+template <class S>
+void launch_pdv(const Geom& g, cudaStream_t s, int predict, double dt_val, const double* dt_ptr,
+                const GeomArrays& ga, const typename S::rho_t* density0,
+                typename S::rho_t* density1, const typename S::ene_t* energy0,
+                typename S::ene_t* energy1, const typename S::cs_t* pressure,
+                const typename S::cs_t* viscosity, const typename S::vel_t* xvel0,
+                const typename S::vel_t* xvel1, const typename S::vel_t* yvel0,
+                const typename S::vel_t* yvel1, const typename S::vel_t* zvel0,
+                const typename S::vel_t* zvel1) {
+  LAUNCH(k_pdv<S>, interior(g), predict, dt_val, dt_ptr, ga, density0, density1, energy0,
+         energy1, pressure, viscosity, xvel0, xvel1, yvel0, yvel1, zvel0, zvel1);
+}
+
+template <class S>
+void launch_revert(const Geom& g, cudaStream_t s, const typename S::rho_t* density0,
+                   typename S::rho_t* density1, const typename S::ene_t* energy0,
+                   typename S::ene_t* energy1) {
+  LAUNCH(k_revert<S>, interior(g), density0, density1, energy0, energy1);
+}
+
+template <class S>
+void launch_accelerate(const Geom& g, cudaStream_t s, double dt_val, const double* dt_ptr,
+                       const GeomArrays& ga, const typename S::rho_t* density0,
+                       const typename S::cs_t* pressure, const typename S::cs_t* viscosity,
+                       const typename S::vel_t* xvel0, const typename S::vel_t* yvel0,
+                       const typename S::vel_t* zvel0, typename S::vel_t* xvel1,
+                       typename S::vel_t* yvel1, typename S::vel_t* zvel1) {
+  LAUNCH(k_accelerate<S>, nodes(g), dt_val, dt_ptr, ga, density0, pressure, viscosity, xvel0,
+         yvel0, zvel0, xvel1, yvel1, zvel1);
+}
+
+template <class S>
+void launch_flux_calc(const Geom& g, cudaStream_t s, double dt_val, const double* dt_ptr,
+                      const GeomArrays& ga, const typename S::vel_t* xvel0,
+                      const typename S::vel_t* yvel0, const typename S::vel_t* zvel0,
+                      const typename S::vel_t* xvel1, const typename S::vel_t* yvel1,
+                      const typename S::vel_t* zvel1, typename S::vf_t* vol_flux_x,
+                      typename S::vf_t* vol_flux_y, typename S::vf_t* vol_flux_z) {
+  LAUNCH(k_flux_calc<S>, nodes(g), dt_val, dt_ptr, ga, xvel0, yvel0, zvel0, xvel1, yvel1,
+         zvel1, vol_flux_x, vol_flux_y, vol_flux_z);
+}
+
+template <class S>
+void launch_advec_cell(const Geom& g, cudaStream_t s, int advect_x, int dir, int sweep,
+                       const GeomArrays& ga, typename S::rho_t* density1,
+                       typename S::ene_t* energy1, typename S::mf_t* mass_flux_x,
+                       const typename S::vf_t* vol_flux_x, typename S::mf_t* mass_flux_y,
+                       const typename S::vf_t* vol_flux_y, typename S::mf_t* mass_flux_z,
+                       const typename S::vf_t* vol_flux_z, typename S::wk_t* const* work) {
+  typename S::wk_t *pre_vol = work[0], *post_vol = work[1], *pre_mass = work[2],
+                   *post_mass = work[3], *advec_vol = work[4], *post_ener = work[5],
+                   *ener_flux = work[6];
+  int variant = -1;
+  if (dir == 1) variant = sweep == 1 ? 0 : sweep == 3 ? 1 : -1;
+  else if (dir == 2) variant = sweep == 2 ? (advect_x ? 2 : 3) : -1;
+  else if (dir == 3) variant = sweep == 1 ? 4 : sweep == 3 ? 5 : -1;
+  if (variant >= 0)
+    LAUNCH(k_cell_vol<S>, halo2(g), variant, ga, vol_flux_x, vol_flux_y, vol_flux_z, pre_vol, post_vol);
+  if (dir == 1) {
+    LAUNCH((k_cell_flux<S, 1>), (Box{g.x_min, g.x_max + 2, g.y_min, g.y_max, g.z_min, g.z_max}),
+           ga, density1, energy1, vol_flux_x, mass_flux_x, pre_vol, ener_flux);
+    LAUNCH((k_cell_update<S, 1>), interior(g), density1, energy1, vol_flux_x, mass_flux_x, pre_vol,
+           pre_mass, post_mass, advec_vol, post_ener, ener_flux);
+  } else if (dir == 2) {
+    LAUNCH((k_cell_flux<S, 2>), (Box{g.x_min, g.x_max, g.y_min, g.y_max + 2, g.z_min, g.z_max + 2}),
+           ga, density1, energy1, vol_flux_y, mass_flux_y, pre_vol, ener_flux);
+    LAUNCH((k_cell_update<S, 2>), interior(g), density1, energy1, vol_flux_y, mass_flux_y, pre_vol,
+           pre_mass, post_mass, advec_vol, post_ener, ener_flux);
+  } else if (dir == 3) {
+    LAUNCH((k_cell_flux<S, 3>), (Box{g.x_min, g.x_max, g.y_min, g.y_max, g.z_min, g.z_max + 2}),
+           ga, density1, energy1, vol_flux_z, mass_flux_z, pre_vol, ener_flux);
+    LAUNCH((k_cell_update<S, 3>), interior(g), density1, energy1, vol_flux_z, mass_flux_z, pre_vol,
+           pre_mass, post_mass, advec_vol, post_ener, ener_flux);
+  }
+}
+
+static inline Box box_union(const Box& a, const Box& b) {
+  return Box{a.j0 < b.j0 ? a.j0 : b.j0, a.j1 > b.j1 ? a.j1 : b.j1,
+             a.k0 < b.k0 ? a.k0 : b.k0, a.k1 > b.k1 ? a.k1 : b.k1,
+             a.l0 < b.l0 ? a.l0 : b.l0, a.l1 > b.l1 ? a.l1 : b.l1};
+}
+
+template <class S>
+void launch_advec_mom(const Geom& g, cudaStream_t s, typename S::vel_t* vel1,
+                      const typename S::mf_t* mass_flux_x, const typename S::vf_t* vol_flux_x,
+                      const typename S::mf_t* mass_flux_y, const typename S::vf_t* vol_flux_y,
+                      const typename S::mf_t* mass_flux_z, const typename S::vf_t* vol_flux_z,
+                      const GeomArrays& ga, const typename S::rho_t* density1,
+                      typename S::wk_t* const* work, int advect_x, int which_vel, int sweep,
+                      int direction) {
+  typename S::wk_t *node_flux = work[0], *node_mass_post = work[1], *node_mass_pre = work[2],
+                   *mom_flux = work[4], *pre_vol = work[5], *post_vol = work[6];
+  int variant = -1;
+  if (sweep == 1 && direction == 1) variant = 0;
+  else if (sweep == 1 && direction == 3) variant = 1;
+  else if (sweep == 2 && advect_x) variant = 2;
+  else if (sweep == 2 && !advect_x) variant = 3;
+  else if (sweep == 3 && direction == 1) variant = 4;
+  else if (sweep == 3 && direction == 3) variant = 5;
+  if (variant >= 0)
+    LAUNCH(k_mom_vol<S>, halo2(g), variant, ga, vol_flux_x, vol_flux_y, vol_flux_z, pre_vol, post_vol);
+  const int x0 = g.x_min, x1 = g.x_max, y0 = g.y_min, y1 = g.y_max, z0 = g.z_min, z1 = g.z_max;
+  if (direction == 1) {
+    if (which_vel == 1) {
+      const Box bf{x0 - 2, x1 + 2, y0, y1 + 1, z0, z1 + 1}, bm{x0 - 1, x1 + 2, y0, y1 + 1, z0, z1 + 1};
+      LAUNCH((k_mom_node<S, 1>), box_union(bf, bm), bf, bm, mass_flux_x, density1, post_vol,
+             node_flux, node_mass_post);
+      LAUNCH((k_mom_nmpre<S, 1>), bm, node_flux, node_mass_post, node_mass_pre);
+    }
+    LAUNCH((k_mom_flux<S, 1>), (Box{x0 - 1, x1 + 1, y0, y1 + 1, z0, z1 + 1}), ga, vel1, node_flux,
+           node_mass_pre, mom_flux);
+  } else if (direction == 2) {
+    if (which_vel == 1) {
+      const Box bf{x0, x1 + 1, y0 - 2, y1 + 2, z0, z1 + 1}, bm{x0, x1 + 1, y0 - 1, y1 + 2, z0, z1 + 1};
+      LAUNCH((k_mom_node<S, 2>), box_union(bf, bm), bf, bm, mass_flux_y, density1, post_vol,
+             node_flux, node_mass_post);
+      LAUNCH((k_mom_nmpre<S, 2>), bm, node_flux, node_mass_post, node_mass_pre);
+    }
+    LAUNCH((k_mom_flux<S, 2>), (Box{x0, x1 + 1, y0 - 1, y1 + 1, z0, z1 + 1}), ga, vel1, node_flux,
+           node_mass_pre, mom_flux);
+  } else if (direction == 3) {
+    if (which_vel == 1) {
+      const Box bf{x0, x1 + 1, y0, y1 + 1, z0 - 2, z1 + 2}, bm{x0, x1 + 1, y0, y1 + 1, z0 - 1, z1 + 2};
+      LAUNCH((k_mom_node<S, 3>), box_union(bf, bm), bf, bm, mass_flux_z, density1, post_vol,
+             node_flux, node_mass_post);
+      LAUNCH((k_mom_nmpre<S, 3>), bm, node_flux, node_mass_post, node_mass_pre);
+    }
+    LAUNCH((k_mom_flux<S, 3>), (Box{x0, x1 + 1, y0, y1 + 1, z0 - 1, z1 + 1}), ga, vel1, node_flux,
+           node_mass_pre, mom_flux);
+  }
+  if (direction == 1)
+    LAUNCH((k_mom_update<S, 1>), nodes(g), vel1, node_mass_pre, node_mass_post, mom_flux);
+  else if (direction == 2)
+    LAUNCH((k_mom_update<S, 2>), nodes(g), vel1, node_mass_pre, node_mass_post, mom_flux);
+  else if (direction == 3)
+    LAUNCH((k_mom_update<S, 3>), nodes(g), vel1, node_mass_pre, node_mass_post, mom_flux);
+}
+
+template <class S>
+void launch_reset_field(const Geom& g, cudaStream_t s, typename S::rho_t* density0,
+                        const typename S::rho_t* density1, typename S::ene_t* energy0,
+                        const typename S::ene_t* energy1, typename S::vel_t* xvel0,
+                        const typename S::vel_t* xvel1, typename S::vel_t* yvel0,
+                        const typename S::vel_t* yvel1, typename S::vel_t* zvel0,
+                        const typename S::vel_t* zvel1) {
+  LAUNCH(k_reset<S>, nodes(g), density0, density1, energy0, energy1, xvel0, xvel1, yvel0, yvel1,
+         zvel0, zvel1);
+}
+
+int summary_partials_len() { return SUM_BLOCKS * 5; }
+
+template <class S>
+void launch_field_summary(const Geom& g, cudaStream_t s, const double* volume,
+                          const typename S::rho_t* density0, const typename S::ene_t* energy0,
+                          const typename S::cs_t* pressure, const typename S::vel_t* xvel0,
+                          const typename S::vel_t* yvel0, const typename S::vel_t* zvel0,
+                          double* partials, double* out5) {
+  k_summary<S><<<SUM_BLOCKS, SUM_THREADS, 0, s>>>(g, volume, density0, energy0, pressure, xvel0,
+                                                  yvel0, zvel0, partials);
+  k_summary_final<<<1, SUM_THREADS, 0, s>>>(partials, out5);
+}
+
+template <class S>
+static int elem_bytes_of(int id) {
+  if (id == 1 || id == 2) return sizeof(typename S::rho_t);
+  if (id == 3 || id == 4) return sizeof(typename S::ene_t);
+  if (id >= 5 && id <= 7) return sizeof(typename S::cs_t);
+  if (id >= 8 && id <= 13) return sizeof(typename S::vel_t);
+  if (id >= 14 && id <= 16) return sizeof(typename S::vf_t);
+  return sizeof(typename S::mf_t);
+}
+
+template <class S>
+void launch_update_halo(const Geom& g, cudaStream_t s, const HaloFields& f, const int* fields,
+                        int depth, const int* external_faces) {
+  // field id -> (kind, component)
+  static const int kind[19] = {0, 0, 0, 0, 0, 0, 0, 1, 1, 1, 1, 1, 1, 2, 2, 2, 2, 2, 2};
+  static const int comp[19] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 1, 1, 2, 2, 0, 1, 2, 0, 1, 2};
+  // faces: 0 left, 1 right, 2 bottom, 3 top, 4 back, 5 front; axis order y, x, z
+  const int axes[3] = {1, 0, 2};
+  for (int ai = 0; ai < 3; ai++) {
+    const int ax = axes[ai];
+    const int lo_face = ax == 0 ? 0 : ax == 1 ? 2 : 4;
+    const int do_low = external_faces[lo_face] ? 1 : 0, do_high = external_faces[lo_face + 1] ? 1 : 0;
+    if (!do_low && !do_high) continue;
+    HaloLaunch h;
+    h.nfields = 0;
+    for (int id = 1; id <= 19; id++) {
+      if (fields[id - 1] != 1) continue;
+      const int i = h.nfields++;
+      h.f[i] = f.f[id - 1];
+      h.ids[i] = id;
+      h.elem_bytes[i] = elem_bytes_of<S>(id);
+      h.rule[i] = make_rule(kind[id - 1], comp[id - 1], ax, id);
+    }
+    if (h.nfields == 0) return;
+    const int mins[3] = {g.x_min, g.y_min, g.z_min}, maxs[3] = {g.x_max, g.y_max, g.z_max};
+    const int ta = ax == 0 ? 1 : 0, tb = ax == 2 ? 1 : 2;
+    const int na = maxs[ta] - mins[ta] + 2 + 2 * depth, nb = maxs[tb] - mins[tb] + 2 + 2 * depth;
+    const dim3 blk(32, 8);
+    const dim3 gr((na + 31) / 32, (nb + 7) / 8);
+    if (ax == 0) k_halo<0><<<gr, blk, 0, s>>>(g, h, depth, do_low, do_high);
+    else if (ax == 1) k_halo<1><<<gr, blk, 0, s>>>(g, h, depth, do_low, do_high);
+    else k_halo<2><<<gr, blk, 0, s>>>(g, h, depth, do_low, do_high);
+  }
+}
+
+void launch_initialise_chunk(const Geom& g, cudaStream_t s, double xmin, double ymin,
+                             double zmin, double dx, double dy, double dz, double* vertexx,
+                             double* vertexdx, double* vertexy, double* vertexdy,
+                             double* vertexz, double* vertexdz, double* cellx, double* celldx,
+                             double* celly, double* celldy, double* cellz, double* celldz,
+                             double* volume, double* xarea, double* yarea, double* zarea) {
+  int n = g.x_max - g.x_min;
+  if (g.y_max - g.y_min > n) n = g.y_max - g.y_min;
+  if (g.z_max - g.z_min > n) n = g.z_max - g.z_min;
+  n += 6;
+  k_init_1d<<<(n + 127) / 128, 128, 0, s>>>(g, xmin, ymin, zmin, dx, dy, dz, vertexx, vertexdx,
+                                            vertexy, vertexdy, vertexz, vertexdz, cellx, celldx,
+                                            celly, celldy, cellz, celldz);
+  LAUNCH(k_init_3d, halo2(g), dx, dy, dz, celldx, celldy, celldz, volume, xarea, yarea, zarea);
+}
+
+template <class S>
+void launch_generate_chunk(const Geom& g, cudaStream_t s, const GeomArrays& ga,
+                           typename S::rho_t* density0, typename S::ene_t* energy0,
+                           typename S::vel_t* xvel0, typename S::vel_t* yvel0,
+                           typename S::vel_t* zvel0, const StateTable& st) {
+  LAUNCH(k_generate_bg<S>, halo2(g), st, density0, energy0, xvel0, yvel0, zvel0);
+  for (int state = 1; state < st.n; state++)
+    LAUNCH(k_generate_state<S>, halo2(g), ga, state, st, density0, energy0, xvel0, yvel0, zvel0);
+}
+
+template <class T>
+void launch_fill(cudaStream_t s, T* p, long long elems, T value) {
+  k_fill<T><<<148 * 8, 256, 0, s>>>(p, elems, value);
+}
+
+#define INST(S)                                                                               \
+  template void launch_ideal_gas<S>(const Geom&, cudaStream_t, const S::rho_t*, const S::ene_t*, \
+                                    S::cs_t*, S::cs_t*);                                      \
+  template void launch_viscosity<S>(const Geom&, cudaStream_t, const GeomArrays&, const S::rho_t*, \
+                                    const S::cs_t*, S::cs_t*, const S::vel_t*, const S::vel_t*, \
+                                    const S::vel_t*);                                         \
+  template void launch_calc_dt<S>(const Geom&, cudaStream_t, const GeomArrays&, double, double, \
+                                  double, double, double, double, const S::rho_t*,             \
+                                  const S::cs_t*, const S::cs_t*, const S::vel_t*,              \
+                                  const S::vel_t*, const S::vel_t*, S::wk_t*,                  \
+                                  unsigned long long*);                                        \
+  template void launch_pdv<S>(const Geom&, cudaStream_t, int, double, const double*,             \
+                              const GeomArrays&, const S::rho_t*, S::rho_t*, const S::ene_t*,  \
+                              S::ene_t*, const S::cs_t*, const S::cs_t*, const S::vel_t*,       \
+                              const S::vel_t*, const S::vel_t*, const S::vel_t*,               \
+                              const S::vel_t*, const S::vel_t*);                               \
+  template void launch_revert<S>(const Geom&, cudaStream_t, const S::rho_t*, S::rho_t*,          \
+                                 const S::ene_t*, S::ene_t*);                                  \
+  template void launch_accelerate<S>(const Geom&, cudaStream_t, double, const double*,           \
+                                     const GeomArrays&, const S::rho_t*, const S::cs_t*,       \
+                                     const S::cs_t*, const S::vel_t*, const S::vel_t*,          \
+                                     const S::vel_t*, S::vel_t*, S::vel_t*, S::vel_t*);        \
+  template void launch_flux_calc<S>(const Geom&, cudaStream_t, double, const double*,            \
+                                    const GeomArrays&, const S::vel_t*, const S::vel_t*,       \
+                                    const S::vel_t*, const S::vel_t*, const S::vel_t*,          \
+                                    const S::vel_t*, S::vf_t*, S::vf_t*, S::vf_t*);            \
+  template void launch_advec_cell<S>(const Geom&, cudaStream_t, int, int, int, const GeomArrays&, \
+                                     S::rho_t*, S::ene_t*, S::mf_t*, const S::vf_t*, S::mf_t*, \
+                                     const S::vf_t*, S::mf_t*, const S::vf_t*, S::wk_t* const*); \
+  template void launch_advec_mom<S>(const Geom&, cudaStream_t, S::vel_t*, const S::mf_t*,        \
+                                    const S::vf_t*, const S::mf_t*, const S::vf_t*,            \
+                                    const S::mf_t*, const S::vf_t*, const GeomArrays&,         \
+                                    const S::rho_t*, S::wk_t* const*, int, int, int, int);     \
+  template void launch_reset_field<S>(const Geom&, cudaStream_t, S::rho_t*, const S::rho_t*,     \
+                                      S::ene_t*, const S::ene_t*, S::vel_t*, const S::vel_t*,  \
+                                      S::vel_t*, const S::vel_t*, S::vel_t*, const S::vel_t*); \
+  template void launch_field_summary<S>(const Geom&, cudaStream_t, const double*,               \
+                                        const S::rho_t*, const S::ene_t*, const S::cs_t*,      \
+                                        const S::vel_t*, const S::vel_t*, const S::vel_t*,     \
+                                        double*, double*);                                     \
+  template void launch_update_halo<S>(const Geom&, cudaStream_t, const HaloFields&, const int*,  \
+                                      int, const int*);                                        \
+  template void launch_generate_chunk<S>(const Geom&, cudaStream_t, const GeomArrays&,          \
+                                         S::rho_t*, S::ene_t*, S::vel_t*, S::vel_t*,           \
+                                         S::vel_t*, const StateTable&);
+
+INST(F64)
+INST(F32Mixed)
+
+template void launch_fill<double>(cudaStream_t, double*, long long, double);
+template void launch_fill<float>(cudaStream_t, float*, long long, float);
+
+}  // namespace clover

@@ -1,0 +1,177 @@
+// Host-side launchers of the hydro-cycle kernels (C++, internal to the
+// library). Every launcher takes device pointers in the chunk layout of
+// clover_layout.cuh, a stream, and the scalar arguments of the reference
+// kernel it replaces. dt is passed either by value (dt_ptr == nullptr) or as a
+// device pointer, so the same kernels serve the drop-in ABI (dt from the
+// caller) and the graph-captured native step (dt computed on the device).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "clover_layout.cuh"
+
+namespace clover {
+
+// Storage policy: FP64 everywhere (the drop-in / parity path).
+struct F64 {
+  using rho_t = double;  // density0, density1
+  using ene_t = double;  // energy0, energy1
+  using cs_t = double;   // pressure, viscosity, soundspeed
+  using vel_t = double;  // xvel0..zvel1
+  using vf_t = double;   // vol_flux_x/y/z
+  using mf_t = double;   // mass_flux_x/y/z
+  using wk_t = double;   // work arrays
+};
+
+// Storage policy of the mixed-precision native path: FP32 storage for the
+// stencilled fields, FP64 kept for density, mass fluxes and work arrays
+// (pre/post volumes, node masses) where conservation needs it. All
+// arithmetic is FP64.
+struct F32Mixed {
+  using rho_t = double;
+  using ene_t = float;
+  using cs_t = float;
+  using vel_t = float;
+  using vf_t = float;
+  using mf_t = double;
+  using wk_t = double;
+};
+
+// Geometry arrays (always FP64).
+struct GeomArrays {
+  const double *volume, *xarea, *yarea, *zarea;
+  const double *cellx, *celly, *cellz;
+  const double *celldx, *celldy, *celldz;
+  const double *vertexx, *vertexy, *vertexz;
+  const double *vertexdx, *vertexdy, *vertexdz;
+};
+
+// The 19 halo-exchangeable fields in reference id order (data.f90:55-74).
+struct HaloFields {
+  void* f[19];
+};
+
+template <class S>
+void launch_ideal_gas(const Geom& g, cudaStream_t s, const typename S::rho_t* density,
+                      const typename S::ene_t* energy, typename S::cs_t* pressure,
+                      typename S::cs_t* soundspeed);
+
+template <class S>
+void launch_viscosity(const Geom& g, cudaStream_t s, const GeomArrays& ga,
+                      const typename S::rho_t* density0, const typename S::cs_t* pressure,
+                      typename S::cs_t* viscosity, const typename S::vel_t* xvel0,
+                      const typename S::vel_t* yvel0, const typename S::vel_t* zvel0);
+
+// Writes dt_min per interior cell (when dt_min_arr != nullptr) and folds the
+// minimum into *min_key (an order-preserving 64-bit key of a double, see
+// clover_kernels.cu); the caller initialises *min_key.
+template <class S>
+void launch_calc_dt(const Geom& g, cudaStream_t s, const GeomArrays& ga, double g_small,
+                    double dtc_safe, double dtu_safe, double dtv_safe, double dtw_safe,
+                    double dtdiv_safe, const typename S::rho_t* density0,
+                    const typename S::cs_t* viscosity, const typename S::cs_t* soundspeed,
+                    const typename S::vel_t* xvel0, const typename S::vel_t* yvel0,
+                    const typename S::vel_t* zvel0, typename S::wk_t* dt_min_arr,
+                    unsigned long long* min_key);
+
+unsigned long long min_key_of(double v);
+double min_key_value(unsigned long long key);
+
+template <class S>
+void launch_pdv(const Geom& g, cudaStream_t s, int predict, double dt_val, const double* dt_ptr,
+                const GeomArrays& ga, const typename S::rho_t* density0,
+                typename S::rho_t* density1, const typename S::ene_t* energy0,
+                typename S::ene_t* energy1, const typename S::cs_t* pressure,
+                const typename S::cs_t* viscosity, const typename S::vel_t* xvel0,
+                const typename S::vel_t* xvel1, const typename S::vel_t* yvel0,
+                const typename S::vel_t* yvel1, const typename S::vel_t* zvel0,
+                const typename S::vel_t* zvel1);
+
+template <class S>
+void launch_revert(const Geom& g, cudaStream_t s, const typename S::rho_t* density0,
+                   typename S::rho_t* density1, const typename S::ene_t* energy0,
+                   typename S::ene_t* energy1);
+
+template <class S>
+void launch_accelerate(const Geom& g, cudaStream_t s, double dt_val, const double* dt_ptr,
+                       const GeomArrays& ga, const typename S::rho_t* density0,
+                       const typename S::cs_t* pressure, const typename S::cs_t* viscosity,
+                       const typename S::vel_t* xvel0, const typename S::vel_t* yvel0,
+                       const typename S::vel_t* zvel0, typename S::vel_t* xvel1,
+                       typename S::vel_t* yvel1, typename S::vel_t* zvel1);
+
+template <class S>
+void launch_flux_calc(const Geom& g, cudaStream_t s, double dt_val, const double* dt_ptr,
+                      const GeomArrays& ga, const typename S::vel_t* xvel0,
+                      const typename S::vel_t* yvel0, const typename S::vel_t* zvel0,
+                      const typename S::vel_t* xvel1, const typename S::vel_t* yvel1,
+                      const typename S::vel_t* zvel1, typename S::vf_t* vol_flux_x,
+                      typename S::vf_t* vol_flux_y, typename S::vf_t* vol_flux_z);
+
+// work: the 7 work arrays (advec_cell_driver.f90:56-62 order).
+template <class S>
+void launch_advec_cell(const Geom& g, cudaStream_t s, int advect_x, int dir, int sweep,
+                       const GeomArrays& ga, typename S::rho_t* density1,
+                       typename S::ene_t* energy1, typename S::mf_t* mass_flux_x,
+                       const typename S::vf_t* vol_flux_x, typename S::mf_t* mass_flux_y,
+                       const typename S::vf_t* vol_flux_y, typename S::mf_t* mass_flux_z,
+                       const typename S::vf_t* vol_flux_z, typename S::wk_t* const* work);
+
+// work: the 7 work arrays (advec_mom_driver.f90:51-57 order).
+template <class S>
+void launch_advec_mom(const Geom& g, cudaStream_t s, typename S::vel_t* vel1,
+                      const typename S::mf_t* mass_flux_x, const typename S::vf_t* vol_flux_x,
+                      const typename S::mf_t* mass_flux_y, const typename S::vf_t* vol_flux_y,
+                      const typename S::mf_t* mass_flux_z, const typename S::vf_t* vol_flux_z,
+                      const GeomArrays& ga, const typename S::rho_t* density1,
+                      typename S::wk_t* const* work, int advect_x, int which_vel, int sweep,
+                      int direction);
+
+template <class S>
+void launch_reset_field(const Geom& g, cudaStream_t s, typename S::rho_t* density0,
+                        const typename S::rho_t* density1, typename S::ene_t* energy0,
+                        const typename S::ene_t* energy1, typename S::vel_t* xvel0,
+                        const typename S::vel_t* xvel1, typename S::vel_t* yvel0,
+                        const typename S::vel_t* yvel1, typename S::vel_t* zvel0,
+                        const typename S::vel_t* zvel1);
+
+// Sums (vol, mass, ie, ke, press) into out5 (device), deterministic order.
+// partials: device scratch of summary_partials_len() doubles.
+int summary_partials_len();
+template <class S>
+void launch_field_summary(const Geom& g, cudaStream_t s, const double* volume,
+                          const typename S::rho_t* density0, const typename S::ene_t* energy0,
+                          const typename S::cs_t* pressure, const typename S::vel_t* xvel0,
+                          const typename S::vel_t* yvel0, const typename S::vel_t* zvel0,
+                          double* partials, double* out5);
+
+// update_halo_kernel: fields[i] != 0 selects field id i+1; all faces external.
+// Element size of every selected field comes from the policy S.
+template <class S>
+void launch_update_halo(const Geom& g, cudaStream_t s, const HaloFields& f, const int* fields,
+                        int depth, const int* external_faces /*6: left..front*/);
+
+// initialise_chunk_kernel + generate_chunk_kernel on the device.
+struct StateTable {
+  int n;
+  double density[16], energy[16], xvel[16], yvel[16], zvel[16];
+  double xmin[16], xmax[16], ymin[16], ymax[16], zmin[16], zmax[16], radius[16];
+  int geometry[16];
+};
+void launch_initialise_chunk(const Geom& g, cudaStream_t s, double xmin, double ymin,
+                             double zmin, double dx, double dy, double dz, double* vertexx,
+                             double* vertexdx, double* vertexy, double* vertexdy,
+                             double* vertexz, double* vertexdz, double* cellx, double* celldx,
+                             double* celly, double* celldy, double* cellz, double* celldz,
+                             double* volume, double* xarea, double* yarea, double* zarea);
+template <class S>
+void launch_generate_chunk(const Geom& g, cudaStream_t s, const GeomArrays& ga,
+                           typename S::rho_t* density0, typename S::ene_t* energy0,
+                           typename S::vel_t* xvel0, typename S::vel_t* yvel0,
+                           typename S::vel_t* zvel0, const StateTable& st);
+
+// Fill every element of an array (size elems after the pad) with a value.
+template <class T>
+void launch_fill(cudaStream_t s, T* base_after_pad, long long elems, T value);
+
+}  // namespace clover

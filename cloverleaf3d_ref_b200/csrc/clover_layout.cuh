@@ -1,0 +1,54 @@
+// Device layout of a CloverLeaf3D chunk in HBM.
+//
+// Every 3D array of a chunk (cell, vertex, face and work arrays) shares one
+// pitched layout: element (j,k,l), j in [x_min-2, x_max+3], k in
+// [y_min-2, y_max+3], l in [z_min-2, z_max+3], sits at
+//   (j - x_min + 2) + (k - y_min + 2) * px + (l - z_min + 2) * pxy
+// with px a multiple of 32 elements and each allocation shifted so that the
+// first interior column (j = x_min) of every row starts on a 128-byte
+// boundary, for 4- and 8-byte elements alike. Cell arrays simply leave their
+// last row/plane/column unused, so a kernel can address every array with one
+// (px, pxy) pair. 1D coordinate arrays are indexed from min-2.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace clover {
+
+struct Geom {
+  int x_min, x_max, y_min, y_max, z_min, z_max;
+  int px;         // row pitch in elements
+  long long pxy;  // plane pitch in elements
+};
+
+// Elements per 128 bytes for a storage type.
+template <class T>
+constexpr int kAlignElems = 128 / (int)sizeof(T);
+
+// Front padding so that element j = x_min (2 after the first) is aligned.
+template <class T>
+constexpr int kFrontPad = kAlignElems<T> - 2;
+
+inline Geom make_geom(int x_min, int x_max, int y_min, int y_max, int z_min, int z_max) {
+  Geom g;
+  g.x_min = x_min; g.x_max = x_max; g.y_min = y_min;
+  g.y_max = y_max; g.z_min = z_min; g.z_max = z_max;
+  const int align = 32;
+  int nxv = x_max - x_min + 6;
+  g.px = (nxv + align - 1) / align * align;
+  g.pxy = (long long)g.px * (y_max - y_min + 6);
+  return g;
+}
+
+// Elements (after the front pad) one 3D array of the chunk occupies.
+inline long long array_elems(const Geom& g) {
+  return g.pxy * (long long)(g.z_max - g.z_min + 6);
+}
+
+__host__ __device__ __forceinline__ long long off3(const Geom& g, int j, int k, int l) {
+  return (long long)(j - g.x_min + 2) + (long long)(k - g.y_min + 2) * g.px +
+         (long long)(l - g.z_min + 2) * g.pxy;
+}
+
+}  // namespace clover

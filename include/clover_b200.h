@@ -1,0 +1,126 @@
+/*
+ * Native API of the B200 hydro-cycle engine: a whole CloverLeaf3D chunk kept
+ * resident in HBM and advanced by the device, with dt, time and the step
+ * count on the GPU and the step replayed from CUDA graphs.
+ *
+ * This is the fast path behind the drop-in ABI of clover_kernels.h: the same
+ * kernels, sequenced as hydro.f90:46-192 sequences the *_kernel calls, but
+ * with no host round trip per step. The deck reader mirrors parse.f90 and
+ * read_input.f90 (same keywords, same defaults).
+ */
+#ifndef CLOVER_B200_H
+#define CLOVER_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CLOVER_MAX_STATES 16
+
+/* The keys of a *clover deck (read_input.f90:38-86 defaults). State bounds
+ * are stored as written in the deck; the nudge by a hundredth of a cell
+ * (read_input.f90:287-303) is applied when a chunk is created. */
+typedef struct clover_deck {
+  int x_cells, y_cells, z_cells;
+  double xmin, ymin, zmin, xmax, ymax, zmax;
+  double initial_timestep, max_timestep, timestep_rise, end_time;
+  double dtmin, dtc_safe, dtu_safe, dtv_safe, dtw_safe, dtdiv_safe;
+  int end_step, summary_frequency, visit_frequency, tiles_per_chunk;
+  int test_problem, profiler_on;
+  int number_of_states;
+  int state_defined[CLOVER_MAX_STATES];
+  double state_density[CLOVER_MAX_STATES], state_energy[CLOVER_MAX_STATES];
+  double state_xvel[CLOVER_MAX_STATES], state_yvel[CLOVER_MAX_STATES];
+  double state_zvel[CLOVER_MAX_STATES];
+  double state_xmin[CLOVER_MAX_STATES], state_xmax[CLOVER_MAX_STATES];
+  double state_ymin[CLOVER_MAX_STATES], state_ymax[CLOVER_MAX_STATES];
+  double state_zmin[CLOVER_MAX_STATES], state_zmax[CLOVER_MAX_STATES];
+  double state_radius[CLOVER_MAX_STATES];
+  int state_geometry[CLOVER_MAX_STATES]; /* 1 cuboid, 2 sphere, 3 point */
+} clover_deck;
+
+/* read_input.f90:38-86 defaults (no states). */
+void clover_deck_defaults(clover_deck *deck);
+/* Parse the text of a deck (the *clover ... *endclover block). Returns 0, or
+ * a nonzero code with a message in err: 1 no states, 2 state defined twice,
+ * 3 bad number, 4 too many states. */
+int clover_deck_parse(const char *text, clover_deck *deck, char *err, int errlen);
+
+typedef struct clover_chunk clover_chunk;
+
+#define CLOVER_PRECISION_FP64 0  /* every field FP64: the parity path */
+#define CLOVER_PRECISION_MIXED 1 /* FP32 storage, FP64 density/mass flux/work */
+
+/* Build the chunk on the current device: allocate, initialise_chunk,
+ * generate_chunk, ideal_gas, the depth-2 halo prime and the step-0 field
+ * summary (start.f90:49-136). NULL on failure (see clover_last_error). */
+clover_chunk *clover_chunk_create(const clover_deck *deck, int precision);
+void clover_chunk_destroy(clover_chunk *c);
+const char *clover_last_error(void);
+
+/* Enqueue n hydro steps (hydro.f90:46-84 minus the end test) on the chunk
+ * stream, with field summaries at the deck's summary_frequency. Returns
+ * immediately. Uses CUDA graphs when enabled (the default). */
+int clover_chunk_step(clover_chunk *c, int n);
+/* The hydro loop of hydro.f90 to completion (end_step or end_time), with
+ * the final field summary. Returns the number of steps taken, or <0 on the
+ * small-timestep error. */
+int clover_chunk_run(clover_chunk *c);
+/* Wait for the chunk stream. */
+int clover_chunk_sync(clover_chunk *c);
+/* 0 = launch kernels directly, 1 = replay captured graphs. */
+void clover_chunk_use_graphs(clover_chunk *c, int on);
+
+/* Host copies of the device records (these synchronise):
+ * steps taken, simulated time, dt of each step, field summaries
+ * (vol, mass, ie, ke, press) with the step each was taken at. */
+int clover_chunk_steps(clover_chunk *c);
+double clover_chunk_time(clover_chunk *c);
+int clover_chunk_dt_history(clover_chunk *c, double *out, int cap);
+int clover_chunk_summaries(clover_chunk *c, double *out5, int *steps, int cap);
+/* Device status bits (CLOVER_STATUS_* of clover_kernels.h). */
+int clover_chunk_status(clover_chunk *c);
+
+/* Copy one field (reference field id 1..19, data.f90:55-74) into a host
+ * array in the reference layout, widening FP32 storage to FP64. */
+int clover_chunk_read_field(clover_chunk *c, int field_id, double *host);
+/* Replace one field from a host array in the reference layout. */
+int clover_chunk_write_field(clover_chunk *c, int field_id, const double *host);
+
+/* The chunk stream (a cudaStream_t), for timing with events on it. */
+uintptr_t clover_chunk_stream(clover_chunk *c);
+/* Device bytes held by the chunk. */
+long long clover_chunk_device_bytes(clover_chunk *c);
+/* Profile mode: when on, steps launch kernels directly and every kernel
+ * group is bracketed by events on the chunk stream. The report returns, per
+ * group (names[i*name_len], NUL-terminated): summed ms, summed algorithmic
+ * bytes (distinct 3D arrays read + written x cells x element size) and
+ * launches since the last report, then resets. Turning it off clears it. */
+void clover_chunk_profile(clover_chunk *c, int on);
+int clover_chunk_profile_report(clover_chunk *c, char *names, int name_len, double *ms,
+                                double *bytes, int *launches, int cap);
+/* Kernel launches one hydro step issues (graph nodes per step). */
+int clover_chunk_launches_per_step(clover_chunk *c);
+
+/* ---- Host driver over the drop-in ABI ----
+ * The reference's own control flow (start.f90, hydro.f90, timestep.f90,
+ * PdV.f90, advection.f90) over host arrays allocated as build_field.f90
+ * allocates them, every kernel call going through clover_kernels.h. One
+ * instance per process (the ABI mirrors one chunk). */
+typedef struct clover_dropin clover_dropin;
+clover_dropin *clover_dropin_create(const clover_deck *deck);
+/* Run the hydro loop to its end (deck end_step/end_time, or max_steps).
+ * Returns the steps taken, negative on the small-timestep error. */
+int clover_dropin_run(clover_dropin *d, int max_steps);
+int clover_dropin_dt_history(clover_dropin *d, double *out, int cap);
+int clover_dropin_summaries(clover_dropin *d, double *out5, int *steps, int cap);
+/* Copy a field (id 1..19) back to the host and out (n elements, reference layout). */
+int clover_dropin_read_field(clover_dropin *d, int field_id, double *out, long long n);
+void clover_dropin_destroy(clover_dropin *d);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

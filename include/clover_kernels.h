@@ -1,0 +1,211 @@
+/*
+ * Drop-in C ABI of the CloverLeaf3D hydro-cycle kernels, B200 (sm_100a).
+ *
+ * Each entry point replaces one Fortran module procedure of the reference
+ * (UK-MAC/CloverLeaf3D_ref) and keeps its argument list and argument order.
+ * Every argument is a pointer, as Fortran passes them by reference; LOGICAL
+ * arguments arrive as int32 (nonzero = .TRUE.). Array arguments point at
+ * element (x_min-2, y_min-2, z_min-2) of a column-major array with the shape
+ * the reference declares for that argument.
+ *
+ * Host arrays are mirrored on the GPU: the first call that sees a host
+ * pointer allocates a device buffer in the chunk layout and copies the array
+ * up; every later call works on the resident copy and the host copy goes
+ * stale. Scalar outputs (calc_dt, field_summary) come back on return.
+ * clover_gpu_sync_to_host() copies every mirrored array back;
+ * clover_gpu_invalidate() marks one host array as changed on the host.
+ * A pointer to device memory is used in place and must already follow the
+ * chunk layout that clover_gpu_layout() describes.
+ *
+ * One chunk with one tile per process: every call must pass the same
+ * x_min..z_max. Calls are asynchronous on one library stream, except those
+ * that return scalars. Not re-entrant. Errors never cross the ABI: they set
+ * bits of clover_gpu_status().
+ */
+#ifndef CLOVER_KERNELS_H
+#define CLOVER_KERNELS_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ideal_gas_kernel_module::ideal_gas_kernel, ideal_gas_kernel.f90:23-64 */
+void clover_ideal_gas_kernel(const int *x_min, const int *x_max, const int *y_min,
+                             const int *y_max, const int *z_min, const int *z_max,
+                             double *density, double *energy, double *pressure,
+                             double *soundspeed);
+
+/* viscosity_kernel_module::viscosity_kernel, viscosity_kernel.f90:28-141 */
+void clover_viscosity_kernel(const int *x_min, const int *x_max, const int *y_min,
+                             const int *y_max, const int *z_min, const int *z_max,
+                             double *xarea, double *yarea, double *zarea, double *celldx,
+                             double *celldy, double *celldz, double *density0,
+                             double *pressure, double *viscosity, double *xvel0,
+                             double *yvel0, double *zvel0);
+
+/* calc_dt_kernel_module::calc_dt_kernel, calc_dt_kernel.f90:28-183.
+ * Synchronises: dt_min_val and the location outputs are host scalars. */
+void clover_calc_dt_kernel(const int *x_min, const int *x_max, const int *y_min,
+                           const int *y_max, const int *z_min, const int *z_max,
+                           const double *g_small, const double *g_big, const double *dtmin,
+                           const double *dtc_safe, const double *dtu_safe,
+                           const double *dtv_safe, const double *dtw_safe,
+                           const double *dtdiv_safe, double *xarea, double *yarea,
+                           double *zarea, double *cellx, double *celly, double *cellz,
+                           double *celldx, double *celldy, double *celldz, double *volume,
+                           double *density0, double *energy0, double *pressure,
+                           double *viscosity_a, double *soundspeed, double *xvel0,
+                           double *yvel0, double *zvel0, double *dt_min, double *dt_min_val,
+                           int *dtl_control, double *xl_pos, double *yl_pos, double *zl_pos,
+                           int *jldt, int *kldt, int *lldt, int *small);
+
+/* PdV_kernel_module::PdV_kernel, PdV_kernel.f90:28-175 */
+void clover_pdv_kernel(const int32_t *predict, const int *x_min, const int *x_max,
+                       const int *y_min, const int *y_max, const int *z_min, const int *z_max,
+                       const double *dt, double *xarea, double *yarea, double *zarea,
+                       double *volume, double *density0, double *density1, double *energy0,
+                       double *energy1, double *pressure, double *viscosity, double *xvel0,
+                       double *xvel1, double *yvel0, double *yvel1, double *zvel0,
+                       double *zvel1);
+
+/* revert_kernel_module::revert_kernel, revert_kernel.f90:23-67 */
+void clover_revert_kernel(const int *x_min, const int *x_max, const int *y_min,
+                          const int *y_max, const int *z_min, const int *z_max,
+                          double *density0, double *density1, double *energy0,
+                          double *energy1);
+
+/* accelerate_kernel_module::accelerate_kernel, accelerate_kernel.f90:27-115 */
+void clover_accelerate_kernel(const int *x_min, const int *x_max, const int *y_min,
+                              const int *y_max, const int *z_min, const int *z_max,
+                              const double *dt, double *xarea, double *yarea, double *zarea,
+                              double *volume, double *density0, double *pressure,
+                              double *viscosity, double *xvel0, double *yvel0, double *zvel0,
+                              double *xvel1, double *yvel1, double *zvel1);
+
+/* flux_calc_kernel_module::flux_calc_kernel, flux_calc_kernel.f90:26-95 */
+void clover_flux_calc_kernel(const int *x_min, const int *x_max, const int *y_min,
+                             const int *y_max, const int *z_min, const int *z_max,
+                             const double *dt, double *xarea, double *yarea, double *zarea,
+                             double *xvel0, double *yvel0, double *zvel0, double *xvel1,
+                             double *yvel1, double *zvel1, double *vol_flux_x,
+                             double *vol_flux_y, double *vol_flux_z);
+
+/* advec_cell_kernel_module::advec_cell_kernel, advec_cell_kernel.f90:30-383 */
+void clover_advec_cell_kernel(const int *x_min, const int *x_max, const int *y_min,
+                              const int *y_max, const int *z_min, const int *z_max,
+                              const int32_t *advect_x, const int *dir, const int *sweep_number,
+                              double *vertexdx, double *vertexdy, double *vertexdz,
+                              double *volume, double *density1, double *energy1,
+                              double *mass_flux_x, double *vol_flux_x, double *mass_flux_y,
+                              double *vol_flux_y, double *mass_flux_z, double *vol_flux_z,
+                              double *pre_vol, double *post_vol, double *pre_mass,
+                              double *post_mass, double *advec_vol, double *post_ener,
+                              double *ener_flux);
+
+/* advec_mom_kernel_mod::advec_mom_kernel, advec_mom_kernel.f90:29-428 */
+void clover_advec_mom_kernel(const int *x_min, const int *x_max, const int *y_min,
+                             const int *y_max, const int *z_min, const int *z_max,
+                             double *vel1, double *mass_flux_x, double *vol_flux_x,
+                             double *mass_flux_y, double *vol_flux_y, double *mass_flux_z,
+                             double *vol_flux_z, double *volume, double *density1,
+                             double *node_flux, double *node_mass_post, double *node_mass_pre,
+                             double *advec_vel, double *mom_flux, double *pre_vol,
+                             double *post_vol, double *celldx, double *celldy, double *celldz,
+                             const int32_t *advect_x, const int *which_vel,
+                             const int *sweep_number, const int *direction);
+
+/* reset_field_kernel_module::reset_field_kernel, reset_field_kernel.f90:27-101 */
+void clover_reset_field_kernel(const int *x_min, const int *x_max, const int *y_min,
+                               const int *y_max, const int *z_min, const int *z_max,
+                               double *density0, double *density1, double *energy0,
+                               double *energy1, double *xvel0, double *xvel1, double *yvel0,
+                               double *yvel1, double *zvel0, double *zvel1);
+
+/* field_summary_kernel_module::field_summary_kernel, field_summary_kernel.f90:26-81.
+ * Synchronises: the five sums are host scalars. */
+void clover_field_summary_kernel(const int *x_min, const int *x_max, const int *y_min,
+                                 const int *y_max, const int *z_min, const int *z_max,
+                                 double *volume, double *density0, double *energy0,
+                                 double *pressure, double *xvel0, double *yvel0, double *zvel0,
+                                 double *vol, double *mass, double *ie, double *ke,
+                                 double *press);
+
+/* update_halo_kernel_module::update_halo_kernel, update_halo_kernel.f90:32-1427.
+ * Reflective copies on the faces where both neighbour entries are -1. */
+void clover_update_halo_kernel(const int *x_min, const int *x_max, const int *y_min,
+                               const int *y_max, const int *z_min, const int *z_max,
+                               const int *chunk_neighbours, const int *tile_neighbours,
+                               double *density0, double *energy0, double *pressure,
+                               double *viscosity, double *soundspeed, double *density1,
+                               double *energy1, double *xvel0, double *yvel0, double *zvel0,
+                               double *xvel1, double *yvel1, double *zvel1,
+                               double *vol_flux_x, double *vol_flux_y, double *vol_flux_z,
+                               double *mass_flux_x, double *mass_flux_y, double *mass_flux_z,
+                               const int *fields, const int *depth);
+
+/* initialise_chunk_kernel_module::initialise_chunk_kernel,
+ * initialise_chunk_kernel.f90:27-182 */
+void clover_initialise_chunk_kernel(const int *x_min, const int *x_max, const int *y_min,
+                                    const int *y_max, const int *z_min, const int *z_max,
+                                    const double *xmin, const double *ymin, const double *zmin,
+                                    const double *dx, const double *dy, const double *dz,
+                                    double *vertexx, double *vertexdx, double *vertexy,
+                                    double *vertexdy, double *vertexz, double *vertexdz,
+                                    double *cellx, double *celldx, double *celly,
+                                    double *celldy, double *cellz, double *celldz,
+                                    double *volume, double *xarea, double *yarea,
+                                    double *zarea);
+
+/* generate_chunk_kernel_module::generate_chunk_kernel, generate_chunk_kernel.f90:27-211
+ * (at most 16 states) */
+void clover_generate_chunk_kernel(const int *x_min, const int *x_max, const int *y_min,
+                                  const int *y_max, const int *z_min, const int *z_max,
+                                  double *vertexx, double *vertexy, double *vertexz,
+                                  double *cellx, double *celly, double *cellz,
+                                  double *density0, double *energy0, double *xvel0,
+                                  double *yvel0, double *zvel0, const int *number_of_states,
+                                  const double *state_density, const double *state_energy,
+                                  const double *state_xvel, const double *state_yvel,
+                                  const double *state_zvel, const double *state_xmin,
+                                  const double *state_xmax, const double *state_ymin,
+                                  const double *state_ymax, const double *state_zmin,
+                                  const double *state_zmax, const double *state_radius,
+                                  const int *state_geometry, const int *g_rect,
+                                  const int *g_circ, const int *g_point);
+
+/* ---- mirror management (no counterpart in the reference: the reference
+ * arrays live in host memory only) ---- */
+
+/* Status bits. */
+#define CLOVER_STATUS_CUDA_ERROR 0x1   /* a CUDA call or launch failed */
+#define CLOVER_STATUS_BOUNDS 0x2       /* a call passed other chunk bounds */
+#define CLOVER_STATUS_SMALL_DT 0x4     /* calc_dt returned small=1 */
+#define CLOVER_STATUS_NO_DEVICE 0x8    /* no CUDA device */
+#define CLOVER_STATUS_BAD_ARG 0x10     /* unsupported argument (e.g. >16 states) */
+#define CLOVER_STATUS_TIMEOUT 0x20     /* a bounded device wait gave up */
+
+int clover_gpu_status(void);
+const char *clover_gpu_error_string(void);
+void clover_gpu_clear_status(void);
+/* Copy every mirrored array back into its host array (waits for the GPU). */
+void clover_gpu_sync_to_host(void);
+/* The host copy of this array changed: upload it again at its next use. */
+void clover_gpu_invalidate(const void *host_array);
+/* Wait for all queued work. */
+void clover_gpu_synchronize(void);
+/* Free every mirror and the library stream. */
+void clover_gpu_release(void);
+/* Chunk layout for device pointers passed in place: element (j,k,l) is at
+ * (j-x_min+2) + (k-y_min+2)*px + (l-z_min+2)*pxy from the pointer. */
+void clover_gpu_layout(const int *x_min, const int *x_max, const int *y_min, const int *y_max,
+                       const int *z_min, const int *z_max, int *px, long long *pxy,
+                       long long *elems);
+/* Number of host arrays currently mirrored, and their total device bytes. */
+void clover_gpu_mirror_stats(int *arrays, long long *bytes);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -208,6 +208,11 @@ int oracle_run(const oracle_deck *deck, int max_steps, double *dt_out, int max_s
                double *summary_out, int *summary_step_out, int *n_summaries,
                double **fields_out);
 
+/* CPU-baseline timing: run warmup + steps steps of the deck and return the
+ * wall seconds of the last `steps` (the step loop including its field
+ * summaries, without set-up). */
+double oracle_run_timed(const oracle_deck *deck, int warmup, int steps);
+
 #ifdef __cplusplus
 }
 #endif

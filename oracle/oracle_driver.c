@@ -9,6 +9,17 @@
 
 #include <stdlib.h>
 #include <string.h>
+#include <time.h>
+
+static double now_s(void) {
+  struct timespec ts;
+  clock_gettime(CLOCK_MONOTONIC, &ts);
+  return (double)ts.tv_sec + 1e-9 * (double)ts.tv_nsec;
+}
+
+/* Wall time of the step loop after `timing_warmup` steps (CPU baseline). */
+static int timing_warmup = -1;
+static double timing_t0 = 0.0, timing_t1 = 0.0;
 
 /* data.f90:30-31: both are default-REAL literals assigned to REAL(8). */
 #define G_SMALL ((double)1.0e-16f)
@@ -270,6 +281,7 @@ int oracle_run(const oracle_deck *dk, int max_steps, double *dt_out, int max_sum
   double time = 0.0, dt = dk->dtinit, dtold = dk->dtinit;
   int step = 0;
   for (;;) {
+    if (step == timing_warmup) timing_t0 = now_s();
     step = step + 1;
     if (timestep(t, dk, &dt, &dtold)) {
       step = -step; /* report_error('timestep','small timestep') */
@@ -299,6 +311,7 @@ int oracle_run(const oracle_deck *dk, int max_steps, double *dt_out, int max_sum
       break;
     }
   }
+  timing_t1 = now_s();
   if (n_summaries) *n_summaries = nsum;
 
   if (fields_out) {
@@ -314,4 +327,12 @@ int oracle_run(const oracle_deck *dk, int max_steps, double *dt_out, int max_sum
   }
   free_field(t);
   return step;
+}
+
+double oracle_run_timed(const oracle_deck *deck, int warmup, int steps) {
+  timing_warmup = warmup;
+  timing_t0 = timing_t1 = 0.0;
+  oracle_run(deck, warmup + steps, NULL, 0, NULL, NULL, NULL, NULL);
+  timing_warmup = -1;
+  return timing_t1 - timing_t0;
 }

@@ -1,0 +1,163 @@
+"""GPU parity: the CUDA kernels against the oracle, through the drop-in C ABI.
+
+FP64 kernels are built without multiply-add contraction and keep the
+reference's operation order, so every array must match the oracle BIT FOR
+BIT after every kernel call; only the field_summary sums (a different
+reduction order) are compared with a tolerance (1e-12 relative).
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+import cloverleaf3d_ref_b200 as C
+import decks
+import hydro_harness as H
+import oracle_lib as O
+
+pytestmark = pytest.mark.gpu
+
+SUMMARY_RTOL = 1e-12
+
+
+@pytest.fixture(autouse=True)
+def fresh_abi():
+    L = C.lib()
+    L.clover_gpu_release()
+    L.clover_gpu_clear_status()
+    yield
+    L.clover_gpu_release()
+    L.clover_gpu_clear_status()
+
+
+def oracle_trace(d, steps):
+    """Run the oracle kernel by kernel, snapshotting every array after each call."""
+    nx, ny, nz = d["x_cells"], d["y_cells"], d["z_cells"]
+    a = H.new_chunk(nx, ny, nz)
+    snaps = []
+    b = H.Backend(O.load(), "oracle_", after=lambda name: snaps.append((name, H.clone(a))))
+    h = H.Hydro(b, a, nx, ny, nz, d)
+    h.start()
+    scal = []
+    for _ in range(steps):
+        h.step()
+        scal.append(h.calc_dt_out)
+    scal.append(tuple(h.field_summary()))
+    return snaps, scal
+
+
+def gpu_lockstep(d, steps, snaps):
+    """Run the same calls through the ABI and compare after each one."""
+    L = C.lib()
+    nx, ny, nz = d["x_cells"], d["y_cells"], d["z_cells"]
+    a = H.new_chunk(nx, ny, nz)
+    idx = [0]
+    mism = []
+
+    def after(name):
+        L.clover_gpu_sync_to_host()
+        assert L.clover_gpu_status() in (0, 4), L.clover_gpu_error_string()
+        ref_name, ref = snaps[idx[0]]
+        assert ref_name == name
+        for k in ref:
+            if not np.array_equal(a[k], ref[k]):
+                bad = np.argwhere(a[k] != ref[k])
+                mism.append((idx[0], name, k, len(bad), tuple(bad[0])))
+        idx[0] += 1
+        if mism:
+            raise AssertionError("first mismatch (call, kernel, array, count, index): %s" % (mism[0],))
+
+    h = H.Hydro(H.Backend(L, "clover_", after=after), a, nx, ny, nz, d)
+    h.start()
+    scal = []
+    for _ in range(steps):
+        h.step()
+        scal.append(h.calc_dt_out)
+    scal.append(tuple(h.field_summary()))
+    return scal
+
+
+@pytest.mark.parametrize("case", ["shock_11x7x6", "mixed_9x8x10", "thin_5x1x3", "tp1_10x2x2"])
+def test_kernel_by_kernel_bitwise(case):
+    d = {
+        "shock_11x7x6": decks.shock(11, 7, 6, 3),
+        "mixed_9x8x10": decks.shock(9, 8, 10, 2, states=decks.MIXED_STATES),
+        "thin_5x1x3": decks.shock(5, 1, 3, 2, states=decks.MIXED_STATES),
+        "tp1_10x2x2": decks.test_problem_1(),
+    }[case]
+    steps = 3 if case != "tp1_10x2x2" else 2
+    snaps, ref_scal = oracle_trace(d, steps)
+    got = gpu_lockstep(d, steps, snaps)
+    for r, g in zip(ref_scal[:-1], got[:-1]):
+        assert r == g  # calc_dt outputs, dt_min_val bitwise
+    np.testing.assert_allclose(got[-1], ref_scal[-1], rtol=SUMMARY_RTOL, atol=0)
+
+
+def run_both(d, steps):
+    r = O.run(d, max_steps=steps, want_fields=True)
+    return r
+
+
+def compare_run(r, dts, sums, sum_steps, fields):
+    assert np.array_equal(dts, r["dt"]), "dt sequence differs"
+    assert np.array_equal(sum_steps, r["summary_steps"])
+    np.testing.assert_allclose(sums, r["summaries"], rtol=SUMMARY_RTOL, atol=0)
+    for n in O.FIELD_NAMES:
+        f = fields(n)
+        if not np.array_equal(f, r["fields"][n]):
+            bad = np.argwhere(f != r["fields"][n])
+            raise AssertionError("%s differs at %d elements, first %s" % (n, len(bad), bad[0]))
+
+
+@pytest.mark.parametrize("case", ["tp1", "shock16", "mixed"])
+def test_dropin_driver_run_bitwise(case):
+    d = {"tp1": decks.test_problem_1(), "shock16": decks.shock(16, 16, 16, 30),
+         "mixed": decks.shock(13, 9, 11, 20, states=decks.MIXED_STATES)}[case]
+    steps = d["end_step"]
+    r = O.run(d, max_steps=steps, want_fields=True)
+    di = C.DropIn(decks.to_deck(d))
+    n = di.run(steps)
+    assert n == r["steps"]
+    sums, sst = di.summaries()
+    compare_run(r, di.dt_history(), sums, sst, di.field)
+    if case == "tp1":
+        ke = sums[-1][3]
+        assert abs(100.0 * (ke / 3.64560737191257) - 100.0) < 0.001
+    di.close()
+
+
+@pytest.mark.parametrize("graphs", [True, False])
+@pytest.mark.parametrize("case", ["tp1", "shock16", "mixed"])
+def test_native_chunk_run_bitwise(case, graphs):
+    d = {"tp1": decks.test_problem_1(), "shock16": decks.shock(16, 16, 16, 30),
+         "mixed": decks.shock(13, 9, 11, 20, states=decks.MIXED_STATES)}[case]
+    r = O.run(d, want_fields=True)
+    ch = C.Chunk(decks.to_deck(d))
+    ch.use_graphs(graphs)
+    n = ch.run()
+    assert n == r["steps"]
+    assert ch.status == 0
+    sums, sst = ch.summaries()
+    compare_run(r, ch.dt_history(), sums, sst, ch.field)
+    ch.close()
+
+
+def test_native_end_time_stop():
+    """hydro.f90:84: the run stops at the first step with time+g_small > end_time."""
+    d = decks.shock(12, 10, 8, 1000, end_time=1.0)
+    r = O.run(d, want_fields=True)
+    ch = C.Chunk(decks.to_deck(d))
+    n = ch.run()
+    assert n == r["steps"]
+    sums, sst = ch.summaries()
+    compare_run(r, ch.dt_history(), sums, sst, ch.field)
+    ch.close()
+
+
+def test_native_known_answer():
+    ch = C.Chunk(decks.to_deck(decks.test_problem_1()))
+    assert ch.run() == 75
+    sums, _ = ch.summaries()
+    ke = sums[-1][3]
+    assert abs(ke / 3.64560737191257 - 1.0) < 1e-13
+    ch.close()

@@ -43,3 +43,16 @@ def test_threads_do_not_change_results():
     assert np.array_equal(a["summaries"], b["summaries"])
     for n in O.FIELD_NAMES:
         assert np.array_equal(a["fields"][n], b["fields"][n]), n
+
+
+def test_reference_index_ranges_in_bounds_on_edge_grids():
+    """ASan/UBSan build of the oracle on 1-cell-thick, 2-cell and odd grids
+    with every state geometry: no out-of-bounds access in any kernel."""
+    import subprocess
+    subprocess.check_call(["make", "-s", "-C", O.ORACLE_DIR, "asan"],
+                          stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+    r = subprocess.run([os.path.join(O.ORACLE_DIR, "_build", "oracle_asan")],
+                       capture_output=True, text=True, env=dict(os.environ, ASAN_OPTIONS="detect_leaks=0"))
+    assert r.returncode == 0, r.stderr[-2000:]
+    assert "runtime error" not in r.stderr and "AddressSanitizer" not in r.stderr
+    assert r.stdout.count("steps 6") == 9
