@@ -136,6 +136,7 @@ def _declare(L):
         getattr(L, n).argtypes = [P]
         getattr(L, n).restype = ctypes.c_int
     L.clover_chunk_use_graphs.argtypes = [P, ctypes.c_int]
+    L.clover_chunk_use_fused.argtypes = [P, ctypes.c_int]
     L.clover_chunk_time.argtypes = [P]
     L.clover_chunk_time.restype = ctypes.c_double
     L.clover_chunk_dt_history.argtypes = [P, P, ctypes.c_int]
@@ -262,6 +263,11 @@ class Chunk:
 
     def use_graphs(self, on):
         lib().clover_chunk_use_graphs(self.h, 1 if on else 0)
+
+    def use_fused(self, on):
+        """Fused kernels (default) or one kernel per reference loop nest; only
+        before the first step."""
+        lib().clover_chunk_use_fused(self.h, 1 if on else 0)
 
     @property
     def steps(self):

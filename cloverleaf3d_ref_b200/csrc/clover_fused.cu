@@ -1,0 +1,825 @@
+// Fused kernels of the native step (clover_native.cu).
+//
+// Every value these kernels produce is computed with the operation order of
+// the reference expression it stands for, so the native step stays bit for
+// bit equal to the drop-in kernels and to the oracle. What changes is the
+// traffic: intermediate arrays that the reference writes and reads back
+// (pre/post volumes, node fluxes and masses, momentum fluxes, the predictor
+// density/energy) live in registers, dead writes are dropped, and passes that
+// read the same inputs are merged.
+//
+//  k_timestep_visc   viscosity with the compression test first: where the
+//                    divergence is non-negative the viscosity is zero whatever
+//                    the limiter, so the thirteen divisions are skipped.
+//  k_pdv_predict_eos PdV predictor + ideal_gas on the predicted state; only
+//                    the pressure is stored (revert then restores time level
+//                    0, and the corrector overwrites density1/energy1).
+//  k_pdv_flux        PdV corrector + flux_calc (shared velocity loads).
+//  k_cell_flux_f     advec_cell face pass with pre_vol from the volume fluxes.
+//  k_cell_update_f   advec_cell update pass, pre_vol recomputed, in place.
+//  k_mom_node_*      node flux, node mass post/pre (one pass, march along the
+//                    sweep axis for y and z sweeps).
+//  k_mom_vel3_*      momentum flux + velocity update for the three components
+//                    (march along the sweep axis for y and z sweeps; the
+//                    updated velocities go to the other buffer of a pair).
+#include "clover_launch.h"
+
+namespace clover {
+namespace {
+
+constexpr int BX = 32, BY = 8;
+
+struct Box {
+  int j0, j1, k0, k1, l0, l1;
+};
+
+inline dim3 grid_of(const Box& b, int march = 1) {
+  int nj = b.j1 - b.j0 + 1, nk = b.k1 - b.k0 + 1, nl = b.l1 - b.l0 + 1;
+  if (nj <= 0 || nk <= 0 || nl <= 0) return dim3(0, 0, 0);
+  return dim3((nj + BX - 1) / BX, (nk + BY - 1) / BY, (nl + march - 1) / march);
+}
+
+#define E(a, jj, kk, ll) (a)[off3(g, (jj), (kk), (ll))]
+#define GX(a, jj) (a)[(jj) - g.x_min + 2]
+#define GY(a, kk) (a)[(kk) - g.y_min + 2]
+#define GZ(a, ll) (a)[(ll) - g.z_min + 2]
+
+__device__ __forceinline__ double ld(const double* p) { return __ldg(p); }
+__device__ __forceinline__ double ld(const float* p) { return (double)__ldg(p); }
+#define L(a, jj, kk, ll) ld(&E(a, jj, kk, ll))
+// the same with the three indices given by one macro (expanded first)
+#define EI(a, idx) EI_(a, idx)
+#define EI_(a, jj, kk, ll) (a)[off3(g, (jj), (kk), (ll))]
+#define LI(a, idx) ld(&EI_(a, idx))
+
+template <class T>
+__device__ __forceinline__ T st(double v) { return (T)v; }
+
+__device__ __forceinline__ double fmin2(double a, double b) { return b < a ? b : a; }
+__device__ __forceinline__ double fmax2(double a, double b) { return b > a ? b : a; }
+
+// ---------------------------------------------------------------------------
+// viscosity_kernel.f90:71-134 with IF((limiter.GT.0.0).OR.(div.GE.0.0)) taken
+// as "div >= 0 -> 0, else limiter > 0 -> 0, else ..." (the same outcome).
+template <class S>
+__global__ void __launch_bounds__(BX * BY) k_timestep_visc(Geom g, Box b, GeomArrays ga,
+    const typename S::rho_t* __restrict__ density0, const typename S::cs_t* __restrict__ pressure,
+    typename S::cs_t* __restrict__ viscosity, const typename S::vel_t* __restrict__ xvel0,
+    const typename S::vel_t* __restrict__ yvel0, const typename S::vel_t* __restrict__ zvel0) {
+  const int j = b.j0 + blockIdx.x * BX + threadIdx.x;
+  const int k = b.k0 + blockIdx.y * BY + threadIdx.y;
+  const int l = b.l0 + blockIdx.z;
+  if (j > b.j1 || k > b.k1) return;
+  const double u000 = L(xvel0, j, k, l), u100 = L(xvel0, j + 1, k, l);
+  const double u010 = L(xvel0, j, k + 1, l), u110 = L(xvel0, j + 1, k + 1, l);
+  const double u001 = L(xvel0, j, k, l + 1), u101 = L(xvel0, j + 1, k, l + 1);
+  const double u011 = L(xvel0, j, k + 1, l + 1), u111 = L(xvel0, j + 1, k + 1, l + 1);
+  const double v000 = L(yvel0, j, k, l), v100 = L(yvel0, j + 1, k, l);
+  const double v010 = L(yvel0, j, k + 1, l), v110 = L(yvel0, j + 1, k + 1, l);
+  const double v001 = L(yvel0, j, k, l + 1), v101 = L(yvel0, j + 1, k, l + 1);
+  const double v011 = L(yvel0, j, k + 1, l + 1), v111 = L(yvel0, j + 1, k + 1, l + 1);
+  const double w000 = L(zvel0, j, k, l), w100 = L(zvel0, j + 1, k, l);
+  const double w010 = L(zvel0, j, k + 1, l), w110 = L(zvel0, j + 1, k + 1, l);
+  const double w001 = L(zvel0, j, k, l + 1), w101 = L(zvel0, j + 1, k, l + 1);
+  const double w011 = L(zvel0, j, k + 1, l + 1), w111 = L(zvel0, j + 1, k + 1, l + 1);
+
+  const double ugradx1 = u000 + u010 + u001 + u011;
+  const double ugradx2 = u100 + u110 + u101 + u111;
+  const double vgrady1 = v000 + v100 + v001 + v101;
+  const double vgrady2 = v010 + v110 + v011 + v111;
+  const double wgradz1 = w000 + w100 + w010 + w110;
+  const double wgradz2 = w001 + w101 + w011 + w111;
+  const double div = (E(ga.xarea, j, k, l) * (ugradx2 - ugradx1) +
+                      E(ga.yarea, j, k, l) * (vgrady2 - vgrady1)) +
+                     E(ga.zarea, j, k, l) * (wgradz2 - wgradz1);
+  double q = 0.0;
+  if (!(div >= 0.0)) {
+    const double ugrady1 = u000 + u100 + u001 + u101;
+    const double ugrady2 = u010 + u110 + u011 + u111;
+    const double ugradz1 = u000 + u100 + u010 + u110;
+    const double ugradz2 = u001 + u101 + u011 + u111;
+    const double vgradx1 = v000 + v010 + v001 + v011;
+    const double vgradx2 = v100 + v110 + v101 + v111;
+    const double vgradz1 = v000 + v100 + v010 + v110;
+    const double vgradz2 = v001 + v101 + v011 + v111;
+    const double wgradx1 = w000 + w010 + w001 + w011;
+    const double wgradx2 = w100 + w110 + w101 + w111;
+    const double wgrady1 = w000 + w100 + w001 + w101;
+    const double wgrady2 = w010 + w110 + w011 + w111;
+    const double cdx = GX(ga.celldx, j), cdy = GY(ga.celldy, k), cdz = GZ(ga.celldz, l);
+    const double xx = 0.25 * (ugradx2 - ugradx1) / cdx;
+    const double yy = 0.25 * (vgrady2 - vgrady1) / cdy;
+    const double zz = 0.25 * (wgradz2 - wgradz1) / cdz;
+    const double xy = 0.25 * (ugrady2 - ugrady1) / cdy + 0.25 * (vgradx2 - vgradx1) / cdx;
+    const double xz = 0.25 * (ugradz2 - ugradz1) / cdz + 0.25 * (wgradx2 - wgradx1) / cdx;
+    const double yz = 0.25 * (vgradz2 - vgradz1) / cdz + 0.25 * (wgrady2 - wgrady1) / cdy;
+    double pgradx = (L(pressure, j + 1, k, l) - L(pressure, j - 1, k, l)) / (cdx + GX(ga.celldx, j + 1));
+    double pgrady = (L(pressure, j, k + 1, l) - L(pressure, j, k - 1, l)) / (cdy + GY(ga.celldy, k + 1));
+    double pgradz = (L(pressure, j, k, l + 1) - L(pressure, j, k, l - 1)) / (cdz + GZ(ga.celldz, l + 1));
+    const double pgradx2 = pgradx * pgradx;
+    const double pgrady2 = pgrady * pgrady;
+    const double pgradz2 = pgradz * pgradz;
+    const double limiter = (xx * pgradx2 + yy * pgrady2 + zz * pgradz2 + xy * pgradx * pgrady +
+                            xz * pgradx * pgradz + yz * pgrady * pgradz) /
+                           fmax2(pgradx2 + pgrady2 + pgradz2, 1.0e-16);
+    if (!(limiter > 0.0)) {
+      pgradx = copysign(fmax2(1.0e-16, fabs(pgradx)), pgradx);
+      pgrady = copysign(fmax2(1.0e-16, fabs(pgrady)), pgrady);
+      pgradz = copysign(fmax2(1.0e-16, fabs(pgradz)), pgradz);
+      const double pgrad = sqrt(pgradx * pgradx + pgrady * pgrady + pgradz * pgradz);
+      const double xgrad = fabs(cdx * pgrad / pgradx);
+      const double ygrad = fabs(cdy * pgrad / pgrady);
+      const double zgrad = fabs(cdz * pgrad / pgradz);
+      const double grad = fmin2(fmin2(xgrad, ygrad), zgrad);
+      const double grad2 = grad * grad;
+      q = 2.0 * L(density0, j, k, l) * grad2 * limiter * limiter;
+    }
+  }
+  E(viscosity, j, k, l) = st<typename S::cs_t>(q);
+}
+
+// ---------------------------------------------------------------------------
+// PdV_kernel.f90:72-118 (predict) followed by ideal_gas_kernel.f90:47-58 on
+// the predicted density1/energy1; the pressure is stored in place (each
+// thread reads and writes only its own cell).
+template <class S>
+__global__ void __launch_bounds__(BX * BY) k_pdv_predict_eos(Geom g, Box b, const double* dt_ptr,
+    GeomArrays ga, const typename S::rho_t* __restrict__ density0,
+    const typename S::ene_t* __restrict__ energy0, typename S::cs_t* __restrict__ pressure,
+    const typename S::cs_t* __restrict__ viscosity, const typename S::vel_t* __restrict__ xvel0,
+    const typename S::vel_t* __restrict__ yvel0, const typename S::vel_t* __restrict__ zvel0) {
+  const int j = b.j0 + blockIdx.x * BX + threadIdx.x;
+  const int k = b.k0 + blockIdx.y * BY + threadIdx.y;
+  const int l = b.l0 + blockIdx.z;
+  if (j > b.j1 || k > b.k1) return;
+  const double dt = *dt_ptr;
+#define XS(jj) (L(xvel0, jj, k, l) + L(xvel0, jj, k + 1, l) + L(xvel0, jj, k, l + 1) + L(xvel0, jj, k + 1, l + 1))
+#define YS(kk) (L(yvel0, j, kk, l) + L(yvel0, j + 1, kk, l) + L(yvel0, j, kk, l + 1) + L(yvel0, j + 1, kk, l + 1))
+#define ZS(ll) (L(zvel0, j, k, ll) + L(zvel0, j + 1, k, ll) + L(zvel0, j, k + 1, ll) + L(zvel0, j + 1, k + 1, ll))
+  // the predictor sums the same four node values twice (vel0 + vel0)
+  double s;
+  s = XS(j);
+  const double left_flux = (E(ga.xarea, j, k, l) * (s + L(xvel0, j, k, l) + L(xvel0, j, k + 1, l) +
+                            L(xvel0, j, k, l + 1) + L(xvel0, j, k + 1, l + 1))) * 0.125 * dt * 0.5;
+  s = XS(j + 1);
+  const double right_flux = (E(ga.xarea, j + 1, k, l) * (s + L(xvel0, j + 1, k, l) + L(xvel0, j + 1, k + 1, l) +
+                             L(xvel0, j + 1, k, l + 1) + L(xvel0, j + 1, k + 1, l + 1))) * 0.125 * dt * 0.5;
+  s = YS(k);
+  const double bottom_flux = (E(ga.yarea, j, k, l) * (s + L(yvel0, j, k, l) + L(yvel0, j + 1, k, l) +
+                              L(yvel0, j, k, l + 1) + L(yvel0, j + 1, k, l + 1))) * 0.125 * dt * 0.5;
+  s = YS(k + 1);
+  const double top_flux = (E(ga.yarea, j, k + 1, l) * (s + L(yvel0, j, k + 1, l) + L(yvel0, j + 1, k + 1, l) +
+                           L(yvel0, j, k + 1, l + 1) + L(yvel0, j + 1, k + 1, l + 1))) * 0.125 * dt * 0.5;
+  s = ZS(l);
+  const double back_flux = (E(ga.zarea, j, k, l) * (s + L(zvel0, j, k, l) + L(zvel0, j + 1, k, l) +
+                            L(zvel0, j, k + 1, l) + L(zvel0, j + 1, k + 1, l))) * 0.125 * dt * 0.5;
+  s = ZS(l + 1);
+  const double front_flux = (E(ga.zarea, j, k, l + 1) * (s + L(zvel0, j, k, l + 1) + L(zvel0, j + 1, k, l + 1) +
+                             L(zvel0, j, k + 1, l + 1) + L(zvel0, j + 1, k + 1, l + 1))) * 0.125 * dt * 0.5;
+#undef XS
+#undef YS
+#undef ZS
+  const double total_flux = right_flux - left_flux + top_flux - bottom_flux + front_flux - back_flux;
+  const double vol = E(ga.volume, j, k, l);
+  const double vol_change_s = vol / (vol + total_flux);
+  const double recip_volume = 1.0 / vol;
+  const double d0 = L(density0, j, k, l);
+  const double energy_change =
+      (L(pressure, j, k, l) / d0 + L(viscosity, j, k, l) / d0) * total_flux * recip_volume;
+  using R = typename S::rho_t;
+  using En = typename S::ene_t;
+  // the predicted state goes through the storage types, as it would in memory
+  const double e1 = (double)st<En>(L(energy0, j, k, l) - energy_change);
+  const double d1 = (double)st<R>(d0 * vol_change_s);
+  E(pressure, j, k, l) = st<typename S::cs_t>((1.4 - 1.0) * d1 * e1);
+}
+
+// ---------------------------------------------------------------------------
+// PdV_kernel.f90:120-166 (corrector) + flux_calc_kernel.f90:58-91 over the
+// node box [min, max+1]^3: cells in the interior run the corrector, faces in
+// the flux ranges get their volume flux.
+template <class S>
+__global__ void __launch_bounds__(BX * BY) k_pdv_flux(Geom g, Box b, const double* dt_ptr,
+    GeomArrays ga, const typename S::rho_t* __restrict__ density0,
+    typename S::rho_t* __restrict__ density1, const typename S::ene_t* __restrict__ energy0,
+    typename S::ene_t* __restrict__ energy1, const typename S::cs_t* __restrict__ pressure,
+    const typename S::cs_t* __restrict__ viscosity, const typename S::vel_t* __restrict__ xvel0,
+    const typename S::vel_t* __restrict__ xvel1, const typename S::vel_t* __restrict__ yvel0,
+    const typename S::vel_t* __restrict__ yvel1, const typename S::vel_t* __restrict__ zvel0,
+    const typename S::vel_t* __restrict__ zvel1, typename S::vf_t* __restrict__ vol_flux_x,
+    typename S::vf_t* __restrict__ vol_flux_y, typename S::vf_t* __restrict__ vol_flux_z) {
+  const int j = b.j0 + blockIdx.x * BX + threadIdx.x;
+  const int k = b.k0 + blockIdx.y * BY + threadIdx.y;
+  const int l = b.l0 + blockIdx.z;
+  if (j > b.j1 || k > b.k1) return;
+  const double dt = *dt_ptr;
+  const bool jin = j <= g.x_max, kin = k <= g.y_max, lin = l <= g.z_max;
+  using F = typename S::vf_t;
+  // face sums of the node velocities, reference order (vel0 x4 then vel1 x4)
+  auto xsum = [&](int jj) {
+    return L(xvel0, jj, k, l) + L(xvel0, jj, k + 1, l) + L(xvel0, jj, k, l + 1) +
+           L(xvel0, jj, k + 1, l + 1) + L(xvel1, jj, k, l) + L(xvel1, jj, k + 1, l) +
+           L(xvel1, jj, k, l + 1) + L(xvel1, jj, k + 1, l + 1);
+  };
+  auto ysum = [&](int kk) {
+    return L(yvel0, j, kk, l) + L(yvel0, j + 1, kk, l) + L(yvel0, j, kk, l + 1) +
+           L(yvel0, j + 1, kk, l + 1) + L(yvel1, j, kk, l) + L(yvel1, j + 1, kk, l) +
+           L(yvel1, j, kk, l + 1) + L(yvel1, j + 1, kk, l + 1);
+  };
+  auto zsum = [&](int ll) {
+    return L(zvel0, j, k, ll) + L(zvel0, j + 1, k, ll) + L(zvel0, j, k + 1, ll) +
+           L(zvel0, j + 1, k + 1, ll) + L(zvel1, j, k, ll) + L(zvel1, j + 1, k, ll) +
+           L(zvel1, j, k + 1, ll) + L(zvel1, j + 1, k + 1, ll);
+  };
+  double sx = 0, sy = 0, sz = 0;
+  if (kin && lin) {
+    sx = xsum(j);
+    E(vol_flux_x, j, k, l) = st<F>(0.125 * dt * E(ga.xarea, j, k, l) * sx);
+  }
+  if (jin && lin) {
+    sy = ysum(k);
+    E(vol_flux_y, j, k, l) = st<F>(0.125 * dt * E(ga.yarea, j, k, l) * sy);
+  }
+  if (jin && kin) {
+    // flux_calc_kernel.f90:86 repeats zvel0(j+1,k,l) and omits zvel0(j,k+1,l)
+    const double bz = L(zvel0, j, k, l) + L(zvel0, j + 1, k, l) + L(zvel0, j + 1, k, l) +
+                      L(zvel0, j + 1, k + 1, l) + L(zvel1, j, k, l) + L(zvel1, j + 1, k, l) +
+                      L(zvel1, j, k + 1, l) + L(zvel1, j + 1, k + 1, l);
+    E(vol_flux_z, j, k, l) = st<F>(0.125 * dt * E(ga.zarea, j, k, l) * bz);
+    sz = zsum(l);
+  }
+  if (!(jin && kin && lin)) return;
+  const double left_flux = (E(ga.xarea, j, k, l) * sx) * 0.125 * dt;
+  const double right_flux = (E(ga.xarea, j + 1, k, l) * xsum(j + 1)) * 0.125 * dt;
+  const double bottom_flux = (E(ga.yarea, j, k, l) * sy) * 0.125 * dt;
+  const double top_flux = (E(ga.yarea, j, k + 1, l) * ysum(k + 1)) * 0.125 * dt;
+  const double back_flux = (E(ga.zarea, j, k, l) * sz) * 0.125 * dt;
+  const double front_flux = (E(ga.zarea, j, k, l + 1) * zsum(l + 1)) * 0.125 * dt;
+  const double total_flux = right_flux - left_flux + top_flux - bottom_flux + front_flux - back_flux;
+  const double vol = E(ga.volume, j, k, l);
+  const double vol_change_s = vol / (vol + total_flux);
+  const double recip_volume = 1.0 / vol;
+  const double d0 = L(density0, j, k, l);
+  const double energy_change =
+      (L(pressure, j, k, l) / d0 + L(viscosity, j, k, l) / d0) * total_flux * recip_volume;
+  E(energy1, j, k, l) = st<typename S::ene_t>(L(energy0, j, k, l) - energy_change);
+  E(density1, j, k, l) = st<typename S::rho_t>(d0 * vol_change_s);
+}
+
+// ---------------------------------------------------------------------------
+// advec_cell pre_vol (advec_cell_kernel.f90:97-121, :190-216, :287-311),
+// the variants of launch_advec_cell in clover_kernels.cu.
+template <class S>
+__device__ __forceinline__ double cell_pre_vol(const Geom& g, int variant, const GeomArrays& ga,
+    const typename S::vf_t* vfx, const typename S::vf_t* vfy, const typename S::vf_t* vfz,
+    int j, int k, int l) {
+  const double vol = E(ga.volume, j, k, l);
+  switch (variant) {
+    case 0:
+    case 4: {
+      const double fx1 = L(vfx, j + 1, k, l), fx0 = L(vfx, j, k, l);
+      const double fy1 = L(vfy, j, k + 1, l), fy0 = L(vfy, j, k, l);
+      const double fz1 = L(vfz, j, k, l + 1), fz0 = L(vfz, j, k, l);
+      return vol + (fx1 - fx0 + fy1 - fy0 + fz1 - fz0);
+    }
+    case 1:
+      return vol + L(vfx, j + 1, k, l) - L(vfx, j, k, l);
+    case 2:
+      return vol + L(vfy, j, k + 1, l) - L(vfy, j, k, l) + L(vfz, j, k, l + 1) - L(vfz, j, k, l);
+    case 3:
+      return vol + L(vfy, j, k + 1, l) - L(vfy, j, k, l) + L(vfx, j + 1, k, l) - L(vfx, j, k, l);
+    default:
+      return vol + L(vfz, j, k, l + 1) - L(vfz, j, k, l);
+  }
+}
+
+__device__ __forceinline__ double cell_limiter(double sig, double sigma3, double sigma4,
+                                               double diffuw, double diffdw) {
+  const double one_by_six = 1.0 / 6.0;
+  if (diffuw * diffdw > 0.0)
+    return (1.0 - sig) * copysign(1.0, diffdw) *
+           fmin2(fmin2(fabs(diffuw), fabs(diffdw)),
+                 one_by_six * (sigma3 * fabs(diffuw) + sigma4 * fabs(diffdw)));
+  return 0.0;
+}
+
+// advec_cell face pass (:125-171, :220-266, :315-361) with pre_vol(donor)
+// computed from the volume fluxes instead of read from a work array.
+template <class S, int DIR>
+__global__ void __launch_bounds__(BX * BY) k_cell_flux_f(Geom g, Box b, int variant, GeomArrays ga,
+    const typename S::rho_t* __restrict__ density1, const typename S::ene_t* __restrict__ energy1,
+    const typename S::vf_t* __restrict__ vfx, const typename S::vf_t* __restrict__ vfy,
+    const typename S::vf_t* __restrict__ vfz, typename S::mf_t* __restrict__ mass_flux,
+    typename S::wk_t* __restrict__ ener_flux) {
+  const int j = b.j0 + blockIdx.x * BX + threadIdx.x;
+  const int k = b.k0 + blockIdx.y * BY + threadIdx.y;
+  const int l = b.l0 + blockIdx.z;
+  if (j > b.j1 || k > b.k1) return;
+  const typename S::vf_t* vf_d = DIR == 1 ? vfx : DIR == 2 ? vfy : vfz;
+  const int i = DIR == 1 ? j : DIR == 2 ? k : l;
+  const int imax = DIR == 1 ? g.x_max : DIR == 2 ? g.y_max : g.z_max;
+  const double* vd = DIR == 1 ? ga.vertexdx : DIR == 2 ? ga.vertexdy : ga.vertexdz;
+  const int vlo = DIR == 1 ? g.x_min : DIR == 2 ? g.y_min : g.z_min;
+  const double vf = L(vf_d, j, k, l);
+  int upwind, donor, downwind, dif;
+  if (vf > 0.0) {
+    upwind = i - 2; donor = i - 1; downwind = i; dif = donor;
+  } else {
+    upwind = (i + 1 < imax + 2) ? i + 1 : imax + 2;
+    donor = i; downwind = i - 1; dif = upwind;
+  }
+#define AT(a, ii) L(a, DIR == 1 ? (ii) : j, DIR == 2 ? (ii) : k, DIR == 3 ? (ii) : l)
+  const double pv_donor = cell_pre_vol<S>(g, variant, ga, vfx, vfy, vfz, DIR == 1 ? donor : j,
+                                          DIR == 2 ? donor : k, DIR == 3 ? donor : l);
+  const double sigmat = fabs(vf) / pv_donor;
+  const double sigma3 = (1.0 + sigmat) * (vd[i - vlo + 2] / vd[dif - vlo + 2]);
+  const double sigma4 = 2.0 - sigmat;
+  const double d_donor = AT(density1, donor);
+  double diffuw = d_donor - AT(density1, upwind);
+  double diffdw = AT(density1, downwind) - d_donor;
+  double limiter = cell_limiter(sigmat, sigma3, sigma4, diffuw, diffdw);
+  const double mflux = vf * (d_donor + limiter);
+  E(mass_flux, j, k, l) = st<typename S::mf_t>(mflux);
+  const double sigmam = fabs(mflux) / (d_donor * pv_donor);
+  const double e_donor = AT(energy1, donor);
+  diffuw = e_donor - AT(energy1, upwind);
+  diffdw = AT(energy1, downwind) - e_donor;
+  limiter = cell_limiter(sigmam, sigma3, sigma4, diffuw, diffdw);
+  E(ener_flux, j, k, l) = st<typename S::wk_t>(mflux * (e_donor + limiter));
+#undef AT
+}
+
+// advec_cell update pass, in place (each thread reads and writes its own cell).
+template <class S, int DIR>
+__global__ void __launch_bounds__(BX * BY) k_cell_update_f(Geom g, Box b, int variant, GeomArrays ga,
+    typename S::rho_t* __restrict__ density1, typename S::ene_t* __restrict__ energy1,
+    const typename S::vf_t* __restrict__ vfx, const typename S::vf_t* __restrict__ vfy,
+    const typename S::vf_t* __restrict__ vfz, const typename S::mf_t* __restrict__ mass_flux,
+    const typename S::wk_t* __restrict__ ener_flux) {
+  const int j = b.j0 + blockIdx.x * BX + threadIdx.x;
+  const int k = b.k0 + blockIdx.y * BY + threadIdx.y;
+  const int l = b.l0 + blockIdx.z;
+  if (j > b.j1 || k > b.k1) return;
+  const typename S::vf_t* vf_d = DIR == 1 ? vfx : DIR == 2 ? vfy : vfz;
+  const int j1 = j + (DIR == 1), k1 = k + (DIR == 2), l1 = l + (DIR == 3);
+  const double pv = cell_pre_vol<S>(g, variant, ga, vfx, vfy, vfz, j, k, l);
+  const double pm = L(density1, j, k, l) * pv;
+  const double pom = pm + L(mass_flux, j, k, l) - L(mass_flux, j1, k1, l1);
+  const double poe = (L(energy1, j, k, l) * pm + L(ener_flux, j, k, l) - L(ener_flux, j1, k1, l1)) / pom;
+  const double av = pv + L(vf_d, j, k, l) - L(vf_d, j1, k1, l1);
+  E(density1, j, k, l) = st<typename S::rho_t>(pom / av);
+  E(energy1, j, k, l) = st<typename S::ene_t>(poe);
+}
+
+// ---------------------------------------------------------------------------
+// advec_mom post_vol (advec_mom_kernel.f90:95-163); pre_vol is not needed by
+// the node masses, only post_vol.
+template <class S>
+__device__ __forceinline__ double mom_post_vol(const Geom& g, int variant, const GeomArrays& ga,
+    const typename S::vf_t* vfx, const typename S::vf_t* vfy, const typename S::vf_t* vfz,
+    int j, int k, int l) {
+  const double vol = E(ga.volume, j, k, l);
+  switch (variant) {
+    case 0:
+      return vol + L(vfy, j, k + 1, l) - L(vfy, j, k, l) + L(vfz, j, k, l + 1) - L(vfz, j, k, l);
+    case 1:
+      return vol + L(vfx, j + 1, k, l) - L(vfx, j, k, l) + L(vfy, j, k + 1, l) - L(vfy, j, k, l);
+    case 2:
+      return vol + L(vfz, j, k, l + 1) - L(vfz, j, k, l);
+    case 3:
+      return vol + L(vfx, j + 1, k, l) - L(vfx, j, k, l);
+    default:
+      return vol;
+  }
+}
+
+// The reference's node-flux sum for direction DIR at node (j,k,l).
+template <class S, int DIR>
+__device__ __forceinline__ double node_flux_at(const Geom& g, const typename S::mf_t* mf, int j,
+                                               int k, int l) {
+  if (DIR == 1)
+    return 0.125 * (L(mf, j, k - 1, l) + L(mf, j, k, l) + L(mf, j + 1, k - 1, l) + L(mf, j + 1, k, l) +
+                    L(mf, j, k - 1, l - 1) + L(mf, j, k, l - 1) + L(mf, j + 1, k - 1, l - 1) +
+                    L(mf, j + 1, k, l - 1));
+  if (DIR == 2)
+    return 0.125 * (L(mf, j - 1, k, l) + L(mf, j, k, l) + L(mf, j - 1, k + 1, l) + L(mf, j, k + 1, l) +
+                    L(mf, j - 1, k, l - 1) + L(mf, j, k, l - 1) + L(mf, j - 1, k + 1, l - 1) +
+                    L(mf, j, k + 1, l - 1));
+  return 0.125 * (L(mf, j - 1, k, l) + L(mf, j, k, l) + L(mf, j - 1, k, l + 1) + L(mf, j, k, l + 1) +
+                  L(mf, j - 1, k - 1, l) + L(mf, j, k - 1, l) + L(mf, j - 1, k - 1, l + 1) +
+                  L(mf, j, k - 1, l + 1));
+}
+
+// Node mass post (reference order of the eight cells) from cell products P.
+__device__ __forceinline__ double node_mass_sum(double p_0m0, double p_000, double p_mm0,
+                                                double p_m00, double p_0mm, double p_00m,
+                                                double p_mmm, double p_m0m) {
+  return 0.125 * (p_0m0 + p_000 + p_mm0 + p_m00 + p_0mm + p_00m + p_mmm + p_m0m);
+}
+
+template <class S>
+__device__ __forceinline__ double cell_product(const Geom& g, int variant, const GeomArrays& ga,
+    const typename S::rho_t* density1, const typename S::vf_t* vfx, const typename S::vf_t* vfy,
+    const typename S::vf_t* vfz, int j, int k, int l) {
+  return L(density1, j, k, l) * mom_post_vol<S>(g, variant, ga, vfx, vfy, vfz, j, k, l);
+}
+
+// Node pass for direction x: one thread per node computes node_flux(j),
+// node_mass_post(j) and node_mass_pre(j) (node_flux(j-1) recomputed).
+// Ranges: node_flux j in [x_min-2, x_max+2], masses j in [x_min-1, x_max+2],
+// k in [y_min, y_max+1], l in [z_min, z_max+1].
+template <class S>
+__global__ void __launch_bounds__(BX * BY) k_mom_node_x(Geom g, Box b, int variant, GeomArrays ga,
+    const typename S::mf_t* __restrict__ mf, const typename S::rho_t* __restrict__ density1,
+    const typename S::vf_t* __restrict__ vfx, const typename S::vf_t* __restrict__ vfy,
+    const typename S::vf_t* __restrict__ vfz, typename S::wk_t* __restrict__ node_flux,
+    typename S::wk_t* __restrict__ node_mass_post, typename S::wk_t* __restrict__ node_mass_pre) {
+  const int j = b.j0 + blockIdx.x * BX + threadIdx.x;
+  const int k = b.k0 + blockIdx.y * BY + threadIdx.y;
+  const int l = b.l0 + blockIdx.z;
+  if (j > b.j1 || k > b.k1) return;
+  using W = typename S::wk_t;
+  const double nf = node_flux_at<S, 1>(g, mf, j, k, l);
+  E(node_flux, j, k, l) = st<W>(nf);
+  if (j < g.x_min - 1) return;
+  auto P = [&](int jj, int kk, int ll) {
+    return cell_product<S>(g, variant, ga, density1, vfx, vfy, vfz, jj, kk, ll);
+  };
+  const double nmp = node_mass_sum(P(j, k - 1, l), P(j, k, l), P(j - 1, k - 1, l), P(j - 1, k, l),
+                                   P(j, k - 1, l - 1), P(j, k, l - 1), P(j - 1, k - 1, l - 1),
+                                   P(j - 1, k, l - 1));
+  E(node_mass_post, j, k, l) = st<W>(nmp);
+  const double nf_prev = node_flux_at<S, 1>(g, mf, j - 1, k, l);
+  E(node_mass_pre, j, k, l) = st<W>(nmp - nf_prev + nf);
+}
+
+// Node pass for direction y or z, marching along the sweep axis: thread
+// (j, c) walks p over the sweep range carrying the previous node flux and the
+// previous plane of cell products.
+// DIR 2: p = k, c = l; DIR 3: p = l, c = k.
+template <class S, int DIR>
+__global__ void __launch_bounds__(BX * BY) k_mom_node_march(Geom g, int jlo, int jhi, int clo,
+    int chi, int plo, int phi, int seg, int variant, GeomArrays ga,
+    const typename S::mf_t* __restrict__ mf, const typename S::rho_t* __restrict__ density1,
+    const typename S::vf_t* __restrict__ vfx, const typename S::vf_t* __restrict__ vfy,
+    const typename S::vf_t* __restrict__ vfz, typename S::wk_t* __restrict__ node_flux,
+    typename S::wk_t* __restrict__ node_mass_post, typename S::wk_t* __restrict__ node_mass_pre) {
+  const int j = jlo + blockIdx.x * BX + threadIdx.x;
+  const int c = clo + blockIdx.y * BY + threadIdx.y;
+  if (j > jhi || c > chi) return;
+  const int p0 = plo + blockIdx.z * seg;
+  int p1 = p0 + seg - 1;
+  if (p1 > phi) p1 = phi;
+  using W = typename S::wk_t;
+  // (j,k,l) of the node at march index p
+#define IDX(p) (DIR == 2 ? j : j), (DIR == 2 ? (p) : c), (DIR == 2 ? c : (p))
+  auto P = [&](int jj, int kk, int ll) {
+    return cell_product<S>(g, variant, ga, density1, vfx, vfy, vfz, jj, kk, ll);
+  };
+  // node flux of the node before the segment and the plane of products
+  // below the first node (cells at march index p0-1)
+  double nf_prev = 0.0;
+  if (p0 - 1 >= plo) nf_prev = node_flux_at<S, DIR>(g, mf, IDX(p0 - 1));
+  // Plane products: the node at (j,k,l) uses cells (j-1..j, k-1..k, l-1..l).
+  // Along the march the "lower" plane of node p is the upper plane of p-1.
+  double q_a = 0.0, q_b = 0.0, q_c = 0.0, q_d = 0.0;  // lower-plane products
+  // The first segment starts at the first node-flux index, whose node mass is
+  // not computed: its lower plane (one below the arrays) is not loaded.
+  if (p0 - 1 >= plo) {
+    const int p = p0;
+    if (DIR == 3) {  // lower plane l-1: P(j,k-1,l-1), P(j,k,l-1), P(j-1,k-1,l-1), P(j-1,k,l-1)
+      q_a = P(j, c - 1, p - 1); q_b = P(j, c, p - 1); q_c = P(j - 1, c - 1, p - 1); q_d = P(j - 1, c, p - 1);
+    } else {  // lower plane k-1: P(j,k-1,l), P(j-1,k-1,l), P(j,k-1,l-1), P(j-1,k-1,l-1)
+      q_a = P(j, p - 1, c); q_b = P(j - 1, p - 1, c); q_c = P(j, p - 1, c - 1); q_d = P(j - 1, p - 1, c - 1);
+    }
+  }
+  for (int p = p0; p <= p1; p++) {
+    const double nf = node_flux_at<S, DIR>(g, mf, IDX(p));
+    EI(node_flux, IDX(p)) = st<W>(nf);
+    double u_a, u_b, u_c, u_d;  // upper-plane products
+    double nmp;
+    if (DIR == 3) {  // upper plane l: P(j,k-1,l), P(j,k,l), P(j-1,k-1,l), P(j-1,k,l)
+      u_a = P(j, c - 1, p); u_b = P(j, c, p); u_c = P(j - 1, c - 1, p); u_d = P(j - 1, c, p);
+      nmp = node_mass_sum(u_a, u_b, u_c, u_d, q_a, q_b, q_c, q_d);
+    } else {  // upper plane k: P(j,k,l), P(j-1,k,l), P(j,k,l-1), P(j-1,k,l-1)
+      u_a = P(j, p, c); u_b = P(j - 1, p, c); u_c = P(j, p, c - 1); u_d = P(j - 1, p, c - 1);
+      // order: P(j,k-1,l) P(j,k,l) P(j-1,k-1,l) P(j-1,k,l) P(j,k-1,l-1) P(j,k,l-1) P(j-1,k-1,l-1) P(j-1,k,l-1)
+      nmp = node_mass_sum(q_a, u_a, q_b, u_b, q_c, u_c, q_d, u_d);
+    }
+    if (p >= plo + 1) {  // node masses run from one node after the flux range start
+      EI(node_mass_post, IDX(p)) = st<W>(nmp);
+      EI(node_mass_pre, IDX(p)) = st<W>(nmp - nf_prev + nf);
+    }
+    nf_prev = nf;
+    q_a = u_a; q_b = u_b; q_c = u_c; q_d = u_d;
+  }
+#undef IDX
+}
+
+__device__ __forceinline__ double mom_limiter(double sigma, double width, double celld_dif,
+                                              double vdiffuw, double vdiffdw) {
+  double limiter = 0.0;
+  if (vdiffuw * vdiffdw > 0.0) {
+    const double auw = fabs(vdiffuw);
+    const double adw = fabs(vdiffdw);
+    double wind = 1.0;
+    if (vdiffdw <= 0.0) wind = -1.0;
+    limiter = wind * fmin2(fmin2(width * ((2.0 - sigma) * adw / width +
+                                          (1.0 + sigma) * auw / celld_dif) / 6.0,
+                                 auw),
+                           adw);
+  }
+  return limiter;
+}
+
+// Momentum flux at node i (advec_mom_kernel.f90:211-242 and the y/z forms)
+// from the velocity window v(i-1..i+2).
+__device__ __forceinline__ double mom_flux_at(double nf, double nmpre_i, double nmpre_ip1,
+                                              double vm1, double v0, double vp1, double vp2,
+                                              double width, double cd_m1, double cd_p1) {
+  double v_upwind, v_donor, v_downwind, nm_donor, cd_dif;
+  if (nf < 0.0) {
+    v_upwind = vp2; v_donor = vp1; v_downwind = v0; nm_donor = nmpre_ip1; cd_dif = cd_p1;
+  } else {
+    v_upwind = vm1; v_donor = v0; v_downwind = vp1; nm_donor = nmpre_i; cd_dif = cd_m1;
+  }
+  const double sigma = fabs(nf) / nm_donor;
+  const double vdiffuw = v_donor - v_upwind;
+  const double vdiffdw = v_downwind - v_donor;
+  const double limiter = mom_limiter(sigma, width, cd_dif, vdiffuw, vdiffdw);
+  const double advec_vel_s = v_donor + (1.0 - sigma) * limiter;
+  return advec_vel_s * nf;
+}
+
+// Velocity pass for direction x: one thread per node updates the three
+// velocities (mom_flux at j-1 and j computed in the thread).
+template <class S>
+__global__ void __launch_bounds__(BX * BY) k_mom_vel3_x(Geom g, Box b, GeomArrays ga,
+    const typename S::wk_t* __restrict__ node_flux, const typename S::wk_t* __restrict__ node_mass_post,
+    const typename S::wk_t* __restrict__ node_mass_pre, const typename S::vel_t* __restrict__ u_in,
+    const typename S::vel_t* __restrict__ v_in, const typename S::vel_t* __restrict__ w_in,
+    typename S::vel_t* __restrict__ u_out, typename S::vel_t* __restrict__ v_out,
+    typename S::vel_t* __restrict__ w_out) {
+  const int j = b.j0 + blockIdx.x * BX + threadIdx.x;
+  const int k = b.k0 + blockIdx.y * BY + threadIdx.y;
+  const int l = b.l0 + blockIdx.z;
+  if (j > b.j1 || k > b.k1) return;
+  const double nf_m = L(node_flux, j - 1, k, l), nf_0 = L(node_flux, j, k, l);
+  const double pre_m = L(node_mass_pre, j - 1, k, l), pre_0 = L(node_mass_pre, j, k, l),
+               pre_p = L(node_mass_pre, j + 1, k, l);
+  const double post_0 = L(node_mass_post, j, k, l);
+  const double w_m = GX(ga.celldx, j - 1), w_0 = GX(ga.celldx, j);
+  const double cd_m2 = GX(ga.celldx, j - 2), cd_p1 = GX(ga.celldx, j + 1);
+  using V = typename S::vel_t;
+  const typename S::vel_t* in[3] = {u_in, v_in, w_in};
+  typename S::vel_t* out[3] = {u_out, v_out, w_out};
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    const double vm2 = L(in[c], j - 2, k, l), vm1 = L(in[c], j - 1, k, l), v0 = L(in[c], j, k, l),
+                 vp1 = L(in[c], j + 1, k, l), vp2 = L(in[c], j + 2, k, l);
+    // mom_flux(j-1): donor j-1 (dif j-2) or j (dif j)
+    const double mf_m = mom_flux_at(nf_m, pre_m, pre_0, vm2, vm1, v0, vp1, w_m, cd_m2, w_0);
+    const double mf_0 = mom_flux_at(nf_0, pre_0, pre_p, vm1, v0, vp1, vp2, w_0, w_m, cd_p1);
+    E(out[c], j, k, l) = st<V>((v0 * pre_0 + mf_m - mf_0) / post_0);
+  }
+}
+
+// Velocity pass for direction y or z, marching along the sweep axis with the
+// previous momentum fluxes and the velocity window in registers.
+template <class S, int DIR>
+__global__ void __launch_bounds__(BX * BY) k_mom_vel3_march(Geom g, int jlo, int jhi, int clo,
+    int chi, int plo, int phi, int seg, GeomArrays ga,
+    const typename S::wk_t* __restrict__ node_flux, const typename S::wk_t* __restrict__ node_mass_post,
+    const typename S::wk_t* __restrict__ node_mass_pre, const typename S::vel_t* __restrict__ u_in,
+    const typename S::vel_t* __restrict__ v_in, const typename S::vel_t* __restrict__ w_in,
+    typename S::vel_t* __restrict__ u_out, typename S::vel_t* __restrict__ v_out,
+    typename S::vel_t* __restrict__ w_out) {
+  const int j = jlo + blockIdx.x * BX + threadIdx.x;
+  const int c = clo + blockIdx.y * BY + threadIdx.y;
+  if (j > jhi || c > chi) return;
+  const int p0 = plo + blockIdx.z * seg;
+  int p1 = p0 + seg - 1;
+  if (p1 > phi) p1 = phi;
+#define IDX(p) j, (DIR == 2 ? (p) : c), (DIR == 2 ? c : (p))
+  const double* cd = DIR == 2 ? ga.celldy : ga.celldz;
+  const int cdlo = DIR == 2 ? g.y_min : g.z_min;
+#define CD(p) cd[(p) - cdlo + 2]
+  using V = typename S::vel_t;
+  const typename S::vel_t* in[3] = {u_in, v_in, w_in};
+  typename S::vel_t* out[3] = {u_out, v_out, w_out};
+  // window at node p: v(p-2), v(p-1), v(p), v(p+1) ; loaded v(p+2) each step
+  double vw[3][4];
+  double mf_prev[3];
+  double nf_m = LI(node_flux, IDX(p0 - 1));
+  double pre_m = LI(node_mass_pre, IDX(p0 - 1));
+  double pre_0 = LI(node_mass_pre, IDX(p0));
+#pragma unroll
+  for (int q = 0; q < 3; q++) {
+    vw[q][0] = LI(in[q], IDX(p0 - 2));
+    vw[q][1] = LI(in[q], IDX(p0 - 1));
+    vw[q][2] = LI(in[q], IDX(p0));
+    vw[q][3] = LI(in[q], IDX(p0 + 1));
+    // mom_flux(p0-1)
+    mf_prev[q] = mom_flux_at(nf_m, pre_m, pre_0, vw[q][0], vw[q][1], vw[q][2], vw[q][3],
+                             CD(p0 - 1), CD(p0 - 2), CD(p0));
+  }
+  for (int p = p0; p <= p1; p++) {
+    const double nf_0 = LI(node_flux, IDX(p));
+    const double pre_p = LI(node_mass_pre, IDX(p + 1));
+    const double post_0 = LI(node_mass_post, IDX(p));
+    const double w_0 = CD(p), cd_m1 = CD(p - 1), cd_p1 = CD(p + 1);
+#pragma unroll
+    for (int q = 0; q < 3; q++) {
+      const double vp2 = LI(in[q], IDX(p + 2));
+      const double mf_0 = mom_flux_at(nf_0, pre_0, pre_p, vw[q][1], vw[q][2], vw[q][3], vp2, w_0,
+                                      cd_m1, cd_p1);
+      EI(out[q], IDX(p)) = st<V>((vw[q][2] * pre_0 + mf_prev[q] - mf_0) / post_0);
+      mf_prev[q] = mf_0;
+      vw[q][0] = vw[q][1];
+      vw[q][1] = vw[q][2];
+      vw[q][2] = vw[q][3];
+      vw[q][3] = vp2;
+    }
+    pre_0 = pre_p;
+  }
+#undef CD
+#undef IDX
+}
+
+// Copy the halo shell of three vertex arrays (every node outside
+// [min, max+1]^3) from one buffer of a pair to the other.
+template <class T>
+__global__ void k_vert_shell_copy(Geom g, const T* __restrict__ a_in, const T* __restrict__ b_in,
+                                  const T* __restrict__ c_in, T* __restrict__ a_out,
+                                  T* __restrict__ b_out, T* __restrict__ c_out) {
+  const int j = g.x_min - 2 + blockIdx.x * BX + threadIdx.x;
+  const int k = g.y_min - 2 + blockIdx.y * BY + threadIdx.y;
+  const int l = g.z_min - 2 + blockIdx.z;
+  if (j > g.x_max + 3 || k > g.y_max + 3) return;
+  const bool inside = j >= g.x_min && j <= g.x_max + 1 && k >= g.y_min && k <= g.y_max + 1 &&
+                      l >= g.z_min && l <= g.z_max + 1;
+  if (inside) return;
+  const long long o = off3(g, j, k, l);
+  a_out[o] = a_in[o];
+  b_out[o] = b_in[o];
+  c_out[o] = c_in[o];
+}
+
+}  // namespace
+
+// ===========================================================================
+#define LAUNCH(kern, box, ...)                                                 \
+  do {                                                                         \
+    const Box _b = (box);                                                      \
+    const dim3 _gr = grid_of(_b);                                              \
+    if (_gr.x && _gr.y && _gr.z) kern<<<_gr, dim3(BX, BY), 0, s>>>(g, _b, __VA_ARGS__); \
+  } while (0)
+
+template <class S>
+void launch_timestep_visc(const Geom& g, cudaStream_t s, const GeomArrays& ga,
+                          const typename S::rho_t* density0, const typename S::cs_t* pressure,
+                          typename S::cs_t* viscosity, const typename S::vel_t* xvel0,
+                          const typename S::vel_t* yvel0, const typename S::vel_t* zvel0) {
+  LAUNCH(k_timestep_visc<S>, (Box{g.x_min, g.x_max, g.y_min, g.y_max, g.z_min, g.z_max}), ga,
+         density0, pressure, viscosity, xvel0, yvel0, zvel0);
+}
+
+template <class S>
+void launch_pdv_predict_eos(const Geom& g, cudaStream_t s, const double* dt_ptr,
+                            const GeomArrays& ga, const typename S::rho_t* density0,
+                            const typename S::ene_t* energy0, typename S::cs_t* pressure,
+                            const typename S::cs_t* viscosity, const typename S::vel_t* xvel0,
+                            const typename S::vel_t* yvel0, const typename S::vel_t* zvel0) {
+  LAUNCH(k_pdv_predict_eos<S>, (Box{g.x_min, g.x_max, g.y_min, g.y_max, g.z_min, g.z_max}),
+         dt_ptr, ga, density0, energy0, pressure, viscosity, xvel0, yvel0, zvel0);
+}
+
+template <class S>
+void launch_pdv_flux(const Geom& g, cudaStream_t s, const double* dt_ptr, const GeomArrays& ga,
+                     const typename S::rho_t* density0, typename S::rho_t* density1,
+                     const typename S::ene_t* energy0, typename S::ene_t* energy1,
+                     const typename S::cs_t* pressure, const typename S::cs_t* viscosity,
+                     const typename S::vel_t* xvel0, const typename S::vel_t* xvel1,
+                     const typename S::vel_t* yvel0, const typename S::vel_t* yvel1,
+                     const typename S::vel_t* zvel0, const typename S::vel_t* zvel1,
+                     typename S::vf_t* vol_flux_x, typename S::vf_t* vol_flux_y,
+                     typename S::vf_t* vol_flux_z) {
+  LAUNCH(k_pdv_flux<S>, (Box{g.x_min, g.x_max + 1, g.y_min, g.y_max + 1, g.z_min, g.z_max + 1}),
+         dt_ptr, ga, density0, density1, energy0, energy1, pressure, viscosity, xvel0, xvel1,
+         yvel0, yvel1, zvel0, zvel1, vol_flux_x, vol_flux_y, vol_flux_z);
+}
+
+template <class S>
+void launch_advec_cell_fused(const Geom& g, cudaStream_t s, int advect_x, int dir, int sweep,
+                             const GeomArrays& ga, typename S::rho_t* density1,
+                             typename S::ene_t* energy1, typename S::mf_t* mass_flux_x,
+                             const typename S::vf_t* vol_flux_x, typename S::mf_t* mass_flux_y,
+                             const typename S::vf_t* vol_flux_y, typename S::mf_t* mass_flux_z,
+                             const typename S::vf_t* vol_flux_z, typename S::wk_t* ener_flux) {
+  int variant = 0;
+  if (dir == 1) variant = sweep == 1 ? 0 : 1;
+  else if (dir == 2) variant = advect_x ? 2 : 3;
+  else variant = sweep == 1 ? 4 : 5;
+  const Box in{g.x_min, g.x_max, g.y_min, g.y_max, g.z_min, g.z_max};
+  if (dir == 1) {
+    LAUNCH((k_cell_flux_f<S, 1>), (Box{g.x_min, g.x_max + 2, g.y_min, g.y_max, g.z_min, g.z_max}),
+           variant, ga, density1, energy1, vol_flux_x, vol_flux_y, vol_flux_z, mass_flux_x, ener_flux);
+    LAUNCH((k_cell_update_f<S, 1>), in, variant, ga, density1, energy1, vol_flux_x, vol_flux_y,
+           vol_flux_z, mass_flux_x, ener_flux);
+  } else if (dir == 2) {
+    LAUNCH((k_cell_flux_f<S, 2>), (Box{g.x_min, g.x_max, g.y_min, g.y_max + 2, g.z_min, g.z_max + 2}),
+           variant, ga, density1, energy1, vol_flux_x, vol_flux_y, vol_flux_z, mass_flux_y, ener_flux);
+    LAUNCH((k_cell_update_f<S, 2>), in, variant, ga, density1, energy1, vol_flux_x, vol_flux_y,
+           vol_flux_z, mass_flux_y, ener_flux);
+  } else {
+    LAUNCH((k_cell_flux_f<S, 3>), (Box{g.x_min, g.x_max, g.y_min, g.y_max, g.z_min, g.z_max + 2}),
+           variant, ga, density1, energy1, vol_flux_x, vol_flux_y, vol_flux_z, mass_flux_z, ener_flux);
+    LAUNCH((k_cell_update_f<S, 3>), in, variant, ga, density1, energy1, vol_flux_x, vol_flux_y,
+           vol_flux_z, mass_flux_z, ener_flux);
+  }
+}
+
+constexpr int kMarchSeg = 32;
+
+template <class S>
+void launch_advec_mom_fused(const Geom& g, cudaStream_t s, int advect_x, int sweep, int dir,
+                            const GeomArrays& ga, const typename S::rho_t* density1,
+                            const typename S::mf_t* mass_flux_x, const typename S::mf_t* mass_flux_y,
+                            const typename S::mf_t* mass_flux_z, const typename S::vf_t* vol_flux_x,
+                            const typename S::vf_t* vol_flux_y, const typename S::vf_t* vol_flux_z,
+                            typename S::wk_t* node_flux, typename S::wk_t* node_mass_post,
+                            typename S::wk_t* node_mass_pre, typename S::vel_t* const* vel_in,
+                            typename S::vel_t* const* vel_out) {
+  int variant;
+  if (sweep == 1 && dir == 1) variant = 0;
+  else if (sweep == 1 && dir == 3) variant = 1;
+  else if (sweep == 2 && advect_x) variant = 2;
+  else if (sweep == 2) variant = 3;
+  else variant = 4;  // sweep 3: post_vol = volume
+  const int x0 = g.x_min, x1 = g.x_max, y0 = g.y_min, y1 = g.y_max, z0 = g.z_min, z1 = g.z_max;
+  if (dir == 1) {
+    LAUNCH(k_mom_node_x<S>, (Box{x0 - 2, x1 + 2, y0, y1 + 1, z0, z1 + 1}), variant, ga, mass_flux_x,
+           density1, vol_flux_x, vol_flux_y, vol_flux_z, node_flux, node_mass_post, node_mass_pre);
+    LAUNCH(k_mom_vel3_x<S>, (Box{x0, x1 + 1, y0, y1 + 1, z0, z1 + 1}), ga, node_flux,
+           node_mass_post, node_mass_pre, vel_in[0], vel_in[1], vel_in[2], vel_out[0], vel_out[1],
+           vel_out[2]);
+  } else {
+    // node pass: march index from min-2 (flux) to max+2; masses from min-1
+    const int plo = (dir == 2 ? y0 : z0) - 2, phi = (dir == 2 ? y1 : z1) + 2;
+    const int clo = dir == 2 ? z0 : y0, chi = (dir == 2 ? z1 : y1) + 1;
+    const int nseg = (phi - plo + 1 + kMarchSeg - 1) / kMarchSeg;
+    const dim3 gr((x1 + 1 - x0 + 1 + BX - 1) / BX, (chi - clo + 1 + BY - 1) / BY, nseg);
+    const int ulo = (dir == 2 ? y0 : z0), uhi = (dir == 2 ? y1 : z1) + 1;
+    const int useg = (uhi - ulo + 1 + kMarchSeg - 1) / kMarchSeg;
+    const dim3 gv((x1 + 1 - x0 + 1 + BX - 1) / BX, (chi - clo + 1 + BY - 1) / BY, useg);
+    if (dir == 2) {
+      k_mom_node_march<S, 2><<<gr, dim3(BX, BY), 0, s>>>(g, x0, x1 + 1, clo, chi, plo, phi, kMarchSeg,
+          variant, ga, mass_flux_y, density1, vol_flux_x, vol_flux_y, vol_flux_z, node_flux,
+          node_mass_post, node_mass_pre);
+      k_mom_vel3_march<S, 2><<<gv, dim3(BX, BY), 0, s>>>(g, x0, x1 + 1, clo, chi, ulo, uhi, kMarchSeg,
+          ga, node_flux, node_mass_post, node_mass_pre, vel_in[0], vel_in[1], vel_in[2],
+          vel_out[0], vel_out[1], vel_out[2]);
+    } else {
+      k_mom_node_march<S, 3><<<gr, dim3(BX, BY), 0, s>>>(g, x0, x1 + 1, clo, chi, plo, phi, kMarchSeg,
+          variant, ga, mass_flux_z, density1, vol_flux_x, vol_flux_y, vol_flux_z, node_flux,
+          node_mass_post, node_mass_pre);
+      k_mom_vel3_march<S, 3><<<gv, dim3(BX, BY), 0, s>>>(g, x0, x1 + 1, clo, chi, ulo, uhi, kMarchSeg,
+          ga, node_flux, node_mass_post, node_mass_pre, vel_in[0], vel_in[1], vel_in[2],
+          vel_out[0], vel_out[1], vel_out[2]);
+    }
+  }
+  // the updated buffers take the halo shell of the inputs
+  const dim3 gs((g.x_max - g.x_min + 6 + BX - 1) / BX, (g.y_max - g.y_min + 6 + BY - 1) / BY,
+                g.z_max - g.z_min + 6);
+  k_vert_shell_copy<typename S::vel_t><<<gs, dim3(BX, BY), 0, s>>>(
+      g, vel_in[0], vel_in[1], vel_in[2], vel_out[0], vel_out[1], vel_out[2]);
+}
+
+#define INSTF(S)                                                                               \
+  template void launch_timestep_visc<S>(const Geom&, cudaStream_t, const GeomArrays&,          \
+                                        const S::rho_t*, const S::cs_t*, S::cs_t*,             \
+                                        const S::vel_t*, const S::vel_t*, const S::vel_t*);    \
+  template void launch_pdv_predict_eos<S>(const Geom&, cudaStream_t, const double*,            \
+                                          const GeomArrays&, const S::rho_t*, const S::ene_t*, \
+                                          S::cs_t*, const S::cs_t*, const S::vel_t*,           \
+                                          const S::vel_t*, const S::vel_t*);                   \
+  template void launch_pdv_flux<S>(const Geom&, cudaStream_t, const double*, const GeomArrays&, \
+                                   const S::rho_t*, S::rho_t*, const S::ene_t*, S::ene_t*,     \
+                                   const S::cs_t*, const S::cs_t*, const S::vel_t*,            \
+                                   const S::vel_t*, const S::vel_t*, const S::vel_t*,          \
+                                   const S::vel_t*, const S::vel_t*, S::vf_t*, S::vf_t*,       \
+                                   S::vf_t*);                                                  \
+  template void launch_advec_cell_fused<S>(const Geom&, cudaStream_t, int, int, int,           \
+                                           const GeomArrays&, S::rho_t*, S::ene_t*, S::mf_t*,  \
+                                           const S::vf_t*, S::mf_t*, const S::vf_t*, S::mf_t*, \
+                                           const S::vf_t*, S::wk_t*);                          \
+  template void launch_advec_mom_fused<S>(const Geom&, cudaStream_t, int, int, int,            \
+                                          const GeomArrays&, const S::rho_t*, const S::mf_t*,  \
+                                          const S::mf_t*, const S::mf_t*, const S::vf_t*,      \
+                                          const S::vf_t*, const S::vf_t*, S::wk_t*, S::wk_t*,  \
+                                          S::wk_t*, S::vel_t* const*, S::vel_t* const*);
+
+INSTF(F64)
+INSTF(F32Mixed)
+
+}  // namespace clover

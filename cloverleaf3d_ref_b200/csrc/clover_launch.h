@@ -170,6 +170,47 @@ void launch_generate_chunk(const Geom& g, cudaStream_t s, const GeomArrays& ga,
                            typename S::vel_t* xvel0, typename S::vel_t* yvel0,
                            typename S::vel_t* zvel0, const StateTable& st);
 
+// ---- fused kernels of the native step (clover_fused.cu) ----
+template <class S>
+void launch_timestep_visc(const Geom& g, cudaStream_t s, const GeomArrays& ga,
+                          const typename S::rho_t* density0, const typename S::cs_t* pressure,
+                          typename S::cs_t* viscosity, const typename S::vel_t* xvel0,
+                          const typename S::vel_t* yvel0, const typename S::vel_t* zvel0);
+template <class S>
+void launch_pdv_predict_eos(const Geom& g, cudaStream_t s, const double* dt_ptr,
+                            const GeomArrays& ga, const typename S::rho_t* density0,
+                            const typename S::ene_t* energy0, typename S::cs_t* pressure,
+                            const typename S::cs_t* viscosity, const typename S::vel_t* xvel0,
+                            const typename S::vel_t* yvel0, const typename S::vel_t* zvel0);
+template <class S>
+void launch_pdv_flux(const Geom& g, cudaStream_t s, const double* dt_ptr, const GeomArrays& ga,
+                     const typename S::rho_t* density0, typename S::rho_t* density1,
+                     const typename S::ene_t* energy0, typename S::ene_t* energy1,
+                     const typename S::cs_t* pressure, const typename S::cs_t* viscosity,
+                     const typename S::vel_t* xvel0, const typename S::vel_t* xvel1,
+                     const typename S::vel_t* yvel0, const typename S::vel_t* yvel1,
+                     const typename S::vel_t* zvel0, const typename S::vel_t* zvel1,
+                     typename S::vf_t* vol_flux_x, typename S::vf_t* vol_flux_y,
+                     typename S::vf_t* vol_flux_z);
+template <class S>
+void launch_advec_cell_fused(const Geom& g, cudaStream_t s, int advect_x, int dir, int sweep,
+                             const GeomArrays& ga, typename S::rho_t* density1,
+                             typename S::ene_t* energy1, typename S::mf_t* mass_flux_x,
+                             const typename S::vf_t* vol_flux_x, typename S::mf_t* mass_flux_y,
+                             const typename S::vf_t* vol_flux_y, typename S::mf_t* mass_flux_z,
+                             const typename S::vf_t* vol_flux_z, typename S::wk_t* ener_flux);
+// All three velocities of one sweep; vel_in/vel_out are the two buffers of
+// each velocity pair (the shell outside [min,max+1]^3 is copied across).
+template <class S>
+void launch_advec_mom_fused(const Geom& g, cudaStream_t s, int advect_x, int sweep, int dir,
+                            const GeomArrays& ga, const typename S::rho_t* density1,
+                            const typename S::mf_t* mass_flux_x, const typename S::mf_t* mass_flux_y,
+                            const typename S::mf_t* mass_flux_z, const typename S::vf_t* vol_flux_x,
+                            const typename S::vf_t* vol_flux_y, const typename S::vf_t* vol_flux_z,
+                            typename S::wk_t* node_flux, typename S::wk_t* node_mass_post,
+                            typename S::wk_t* node_mass_pre, typename S::vel_t* const* vel_in,
+                            typename S::vel_t* const* vel_out);
+
 // Fill every element of an array (size elems after the pad) with a value.
 template <class T>
 void launch_fill(cudaStream_t s, T* base_after_pad, long long elems, T value);

@@ -105,6 +105,7 @@ struct Chunk : ChunkBase {
   En *energy0, *energy1;
   C *pressure, *viscosity, *soundspeed;
   V *xvel0, *xvel1, *yvel0, *yvel1, *zvel0, *zvel1;
+  V* vel1b[3];  // second buffer of each time-level-1 velocity (fused step)
   VF *vol_flux_x, *vol_flux_y, *vol_flux_z;
   MF *mass_flux_x, *mass_flux_y, *mass_flux_z;
   W* work[7];
@@ -124,6 +125,7 @@ struct Chunk : ChunkBase {
   int host_step = 0;     // steps enqueued
   bool advect_x = true;  // start.f90:99
   bool use_graphs = true;
+  bool fused = true;  // fused kernels (clover_fused.cu) instead of one kernel per reference pass
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
   int launches_per_step = 0;
   int ext[6] = {1, 1, 1, 1, 1, 1};
@@ -176,19 +178,28 @@ struct Chunk : ChunkBase {
     return (double)(g.x_max - g.x_min + 1) * (g.y_max - g.y_min + 1) * (g.z_max - g.z_min + 1);
   }
 
-  HaloFields halo_fields() {
+  // time-level-1 velocity c (0 x, 1 y, 2 z) in buffer b of its pair
+  V* vel1(int c, int b) const {
+    V* a[3] = {xvel1, yvel1, zvel1};
+    return b ? vel1b[c] : a[c];
+  }
+  // the buffer holding time level 1 velocities after `steps` fused steps:
+  // each step flips the pair three times (one per sweep)
+  int vel1_buffer(int steps) const { return fused ? steps % 2 : 0; }
+
+  HaloFields halo_fields(int vb) {
     HaloFields h;
     void* f[19] = {density0, density1, energy0, energy1, pressure, viscosity, soundspeed,
-                   xvel0, xvel1, yvel0, yvel1, zvel0, zvel1, vol_flux_x, vol_flux_y,
-                   vol_flux_z, mass_flux_x, mass_flux_y, mass_flux_z};
+                   xvel0, vel1(0, vb), yvel0, vel1(1, vb), zvel0, vel1(2, vb), vol_flux_x,
+                   vol_flux_y, vol_flux_z, mass_flux_x, mass_flux_y, mass_flux_z};
     for (int i = 0; i < 19; i++) h.f[i] = f[i];
     return h;
   }
 
-  void halo(std::initializer_list<int> ids, int depth) {
+  void halo(std::initializer_list<int> ids, int depth, int vb = 0) {
     int fields[19] = {0};
     for (int id : ids) fields[id - 1] = 1;
-    launch_update_halo<S>(g, stream, halo_fields(), fields, depth, ext);
+    launch_update_halo<S>(g, stream, halo_fields(vb), fields, depth, ext);
   }
 
   bool create(const clover_deck& d) {
@@ -210,6 +221,7 @@ struct Chunk : ChunkBase {
     chk(yvel1 = alloc_field<V>(g, owned, bytes, stream));
     chk(zvel0 = alloc_field<V>(g, owned, bytes, stream));
     chk(zvel1 = alloc_field<V>(g, owned, bytes, stream));
+    for (int c3 = 0; c3 < 3; c3++) chk(vel1b[c3] = alloc_field<V>(g, owned, bytes, stream));
     chk(vol_flux_x = alloc_field<VF>(g, owned, bytes, stream));
     chk(vol_flux_y = alloc_field<VF>(g, owned, bytes, stream));
     chk(vol_flux_z = alloc_field<VF>(g, owned, bytes, stream));
@@ -319,8 +331,98 @@ struct Chunk : ChunkBase {
     sum_steps.push_back(step);
   }
 
+  // One hydro step with the fused kernels (same results, bit for bit).
+  void enqueue_step_fused(bool ax) {
+    const double* dtp = &sc->dt;
+    const double n = cells();
+    const double R8 = sizeof(R), E8 = sizeof(En), C8 = sizeof(C), V8 = sizeof(V),
+                 VF8 = sizeof(VF), MF8 = sizeof(MF), W8 = sizeof(W), G8 = sizeof(double);
+    int vc = ax ? 0 : 1;  // buffer of the velocity pairs at the start of this step
+    // timestep.f90:56-126
+    k_dt_prepare<<<1, 1, 0, stream>>>(sc, min_key_of(kGBig));
+    pbeg();
+    launch_ideal_gas<S>(g, stream, density0, energy0, pressure, soundspeed);
+    pend("ideal_gas", n * (R8 + E8 + 2 * C8));
+    pbeg();
+    halo({5, 3, 1, 8, 10}, 1, vc);
+    pend("update_halo", 0);
+    pbeg();
+    launch_timestep_visc<S>(g, stream, ga, density0, pressure, viscosity, xvel0, yvel0, zvel0);
+    pend("viscosity", n * (3 * V8 + 3 * G8 + C8));
+    pbeg();
+    halo({6}, 1, vc);
+    pend("update_halo", 0);
+    pbeg();
+    launch_calc_dt<S>(g, stream, ga, kGSmall, deck.dtc_safe, deck.dtu_safe, deck.dtv_safe,
+                      deck.dtw_safe, deck.dtdiv_safe, density0, viscosity, soundspeed, xvel0,
+                      yvel0, zvel0, (W*)nullptr, &sc->key);
+    k_dt_finalize<<<1, 1, 0, stream>>>(sc, dt_hist, deck.timestep_rise, deck.max_timestep,
+                                       deck.dtmin);
+    pend("calc_dt", n * (4 * G8 + R8 + 2 * C8 + 3 * V8));
+    // PdV.f90:50-107: predictor + EOS on the predicted state; revert is implied
+    pbeg();
+    launch_pdv_predict_eos<S>(g, stream, dtp, ga, density0, energy0, pressure, viscosity, xvel0,
+                              yvel0, zvel0);
+    pend("pdv", n * (4 * G8 + R8 + E8 + 3 * C8 + 3 * V8));
+    pbeg();
+    halo({5}, 1, vc);
+    pend("update_halo", 0);
+    pbeg();
+    launch_accelerate<S>(g, stream, 0.0, dtp, ga, density0, pressure, viscosity, xvel0, yvel0,
+                         zvel0, vel1(0, vc), vel1(1, vc), vel1(2, vc));
+    pend("accelerate", n * (4 * G8 + R8 + 2 * C8 + 6 * V8));
+    pbeg();
+    launch_pdv_flux<S>(g, stream, dtp, ga, density0, density1, energy0, energy1, pressure,
+                       viscosity, xvel0, vel1(0, vc), yvel0, vel1(1, vc), zvel0, vel1(2, vc),
+                       vol_flux_x, vol_flux_y, vol_flux_z);
+    pend("pdv_flux", n * (4 * G8 + 2 * R8 + 2 * E8 + 2 * C8 + 6 * V8 + 3 * VF8));
+    // advection.f90:43-179
+    const int axi = ax ? 1 : 0;
+    auto sweep = [&](int sweep_number, int dir, bool pre_halo) {
+      if (pre_halo) {
+        pbeg();
+        halo({4, 2, 14, 15, 16}, 2, vc);
+        pend("update_halo", 0);
+      }
+      // volume fluxes read for pre_vol: all three on sweep 1, two on the y sweep,
+      // the sweep direction only on sweep 3
+      const double nvf = sweep_number == 1 ? 3 : sweep_number == 2 ? 2 : 1;
+      pbeg();
+      launch_advec_cell_fused<S>(g, stream, axi, dir, sweep_number, ga, density1, energy1,
+                                 mass_flux_x, vol_flux_x, mass_flux_y, vol_flux_y, mass_flux_z,
+                                 vol_flux_z, work[6]);
+      pend("advec_cell", n * ((G8 + nvf * VF8 + R8 + E8 + MF8 + W8) +
+                              (G8 + nvf * VF8 + 2 * R8 + 2 * E8 + MF8 + W8)));
+      pbeg();
+      halo({2, 4, 9, 11, 13, 17, 18, 19}, 2, vc);
+      pend("update_halo", 0);
+      // post_vol reads two volume fluxes on sweep 1, one on sweep 2, none on sweep 3
+      const double npv = sweep_number == 1 ? 2 : sweep_number == 2 ? 1 : 0;
+      V* vin[3] = {vel1(0, vc), vel1(1, vc), vel1(2, vc)};
+      V* vout[3] = {vel1(0, vc ^ 1), vel1(1, vc ^ 1), vel1(2, vc ^ 1)};
+      pbeg();
+      launch_advec_mom_fused<S>(g, stream, axi, sweep_number, dir, ga, density1, mass_flux_x,
+                                mass_flux_y, mass_flux_z, vol_flux_x, vol_flux_y, vol_flux_z,
+                                work[0], work[1], work[2], vin, vout);
+      pend("advec_mom", n * ((MF8 + R8 + G8 + npv * VF8 + 3 * W8) + (3 * W8 + 6 * V8)));
+      vc ^= 1;
+    };
+    sweep(1, ax ? 1 : 3, true);
+    sweep(2, 2, true);
+    sweep(3, ax ? 3 : 1, false);
+    pbeg();
+    launch_reset_field<S>(g, stream, density0, density1, energy0, energy1, xvel0, vel1(0, vc),
+                          yvel0, vel1(1, vc), zvel0, vel1(2, vc));
+    pend("reset_field", n * (2 * R8 + 2 * E8 + 6 * V8));
+    k_step_end<<<1, 1, 0, stream>>>(sc);
+  }
+
   // One hydro step, hydro.f90:52-68 (timestep .. time = time + dt).
   void enqueue_step(bool ax) {
+    if (fused) {
+      enqueue_step_fused(ax);
+      return;
+    }
     const double* dtp = &sc->dt;
     const double n = cells();
     const double R8 = sizeof(R), E8 = sizeof(En), C8 = sizeof(C), V8 = sizeof(V),
@@ -483,9 +585,10 @@ struct Chunk : ChunkBase {
 
   int read_field(int id, double* host, bool write) {
     if (id < 1 || id > 19) return -1;
+    const int vb = vel1_buffer(host_step);
     void* f[19] = {density0, density1, energy0, energy1, pressure, viscosity, soundspeed,
-                   xvel0, xvel1, yvel0, yvel1, zvel0, zvel1, vol_flux_x, vol_flux_y,
-                   vol_flux_z, mass_flux_x, mass_flux_y, mass_flux_z};
+                   xvel0, vel1(0, vb), yvel0, vel1(1, vb), zvel0, vel1(2, vb), vol_flux_x,
+                   vol_flux_y, vol_flux_z, mass_flux_x, mass_flux_y, mass_flux_z};
     const int eb[19] = {(int)sizeof(R), (int)sizeof(R), (int)sizeof(En), (int)sizeof(En),
                         (int)sizeof(C), (int)sizeof(C), (int)sizeof(C), (int)sizeof(V),
                         (int)sizeof(V), (int)sizeof(V), (int)sizeof(V), (int)sizeof(V),
@@ -837,6 +940,16 @@ uintptr_t clover_chunk_stream(clover_chunk* c) {
   return (uintptr_t)(c->f64 ? c->f64->stream : c->mixed->stream);
 }
 long long clover_chunk_device_bytes(clover_chunk* c) { return DISPATCH(c, bytes); }
+void clover_chunk_use_fused(clover_chunk* c, int on) {
+  // only between runs: the velocity buffers of a fused step alternate per step
+  if (c->f64) {
+    if (c->f64->host_step == 0) { c->f64->fused = on != 0; for (auto& gr : c->f64->graph) if (gr) { cudaGraphExecDestroy(gr); gr = nullptr; } }
+  } else if (c->mixed->host_step == 0) {
+    c->mixed->fused = on != 0;
+    for (auto& gr : c->mixed->graph) if (gr) { cudaGraphExecDestroy(gr); gr = nullptr; }
+  }
+}
+
 void clover_chunk_profile(clover_chunk* c, int on) {
   if (c->f64) { c->f64->prof_collect(); c->f64->profile = on != 0; if (!on) c->f64->prof_acc.clear(); }
   else { c->mixed->prof_collect(); c->mixed->profile = on != 0; if (!on) c->mixed->prof_acc.clear(); }

@@ -72,6 +72,9 @@ int clover_chunk_run(clover_chunk *c);
 int clover_chunk_sync(clover_chunk *c);
 /* 0 = launch kernels directly, 1 = replay captured graphs. */
 void clover_chunk_use_graphs(clover_chunk *c, int on);
+/* 1 (default) = the fused kernels, 0 = one kernel per reference loop nest.
+ * Both give the same results bit for bit. Only before the first step. */
+void clover_chunk_use_fused(clover_chunk *c, int on);
 
 /* Host copies of the device records (these synchronise):
  * steps taken, simulated time, dt of each step, field summaries

@@ -5,6 +5,7 @@
  * hydro.f90:46-192 with the phase drivers timestep.f90:56-126,
  * PdV.f90:50-107, advection.f90:43-179 and field_summary.f90:55-113.
  */
+#define _POSIX_C_SOURCE 199309L
 #include "clover_oracle.h"
 
 #include <stdlib.h>

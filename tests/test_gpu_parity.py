@@ -126,13 +126,19 @@ def test_dropin_driver_run_bitwise(case):
     di.close()
 
 
+@pytest.mark.parametrize("fused", [True, False])
 @pytest.mark.parametrize("graphs", [True, False])
-@pytest.mark.parametrize("case", ["tp1", "shock16", "mixed"])
-def test_native_chunk_run_bitwise(case, graphs):
+@pytest.mark.parametrize("case", ["tp1", "shock16", "mixed", "thin"])
+def test_native_chunk_run_bitwise(case, graphs, fused):
+    """The native step (fused kernels or one kernel per reference pass, graph
+    replay or direct launches) against the oracle: dt and every array of the
+    19 fields bit for bit, summaries to 1e-12."""
     d = {"tp1": decks.test_problem_1(), "shock16": decks.shock(16, 16, 16, 30),
-         "mixed": decks.shock(13, 9, 11, 20, states=decks.MIXED_STATES)}[case]
+         "mixed": decks.shock(13, 9, 11, 20, states=decks.MIXED_STATES),
+         "thin": decks.shock(7, 1, 5, 9, states=decks.MIXED_STATES)}[case]
     r = O.run(d, want_fields=True)
     ch = C.Chunk(decks.to_deck(d))
+    ch.use_fused(fused)
     ch.use_graphs(graphs)
     n = ch.run()
     assert n == r["steps"]
@@ -160,4 +166,17 @@ def test_native_known_answer():
     sums, _ = ch.summaries()
     ke = sums[-1][3]
     assert abs(ke / 3.64560737191257 - 1.0) < 1e-13
+    ch.close()
+
+
+def test_native_fused_long_run_bitwise():
+    """A longer fused run on an uneven grid (several segments of the marching
+    kernels along every axis) stays bit-identical."""
+    d = decks.shock(40, 37, 70, 40, states=decks.MIXED_STATES)
+    r = O.run(d, want_fields=True)
+    ch = C.Chunk(decks.to_deck(d))
+    n = ch.run()
+    assert n == r["steps"]
+    sums, sst = ch.summaries()
+    compare_run(r, ch.dt_history(), sums, sst, ch.field)
     ch.close()
