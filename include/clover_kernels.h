@@ -132,6 +132,31 @@ void clover_field_summary_kernel(const int *x_min, const int *x_max, const int *
                                  double *vol, double *mass, double *ie, double *ke,
                                  double *press);
 
+/* field_summary for callers that cannot let the library allocate device
+ * memory. No counterpart in the reference. Meant for a host code whose GPU
+ * memory is all owned by its own pool allocator or held under a fixed budget,
+ * where a cudaMalloc made inside the library could fail or fragment that
+ * pool. It allocates nothing: the arrays are the caller's DEVICE arrays in
+ * the chunk layout of clover_gpu_layout() (host arrays are rejected), the
+ * five sums come back in host scalars, and the reduction scratch is a fixed
+ * 160 KiB file-scope device array that every GPU loading the library holds
+ * until the process exits. At most CLOVER_NOALLOC_MAX_Z_CELLS cells along z
+ * (larger grids return CLOVER_STATUS_BAD_ARG with a message on stderr).
+ * Runs on the legacy default stream and returns when the sums are on the
+ * host; 0 on success, else a CLOVER_STATUS_* bit. The first call on a device
+ * looks up the scratch address (once per device); make that first call
+ * before any stream capture. All calls share the one scratch array: calls
+ * that overlap on the GPU race. Sums agree with clover_field_summary_kernel
+ * to rounding (a different, fixed reduction order). */
+#define CLOVER_NOALLOC_MAX_Z_CELLS 4096
+int clover_field_summary_kernel_noalloc(const int *x_min, const int *x_max, const int *y_min,
+                                        const int *y_max, const int *z_min, const int *z_max,
+                                        const double *volume, const double *density0,
+                                        const double *energy0, const double *pressure,
+                                        const double *xvel0, const double *yvel0,
+                                        const double *zvel0, double *vol, double *mass,
+                                        double *ie, double *ke, double *press);
+
 /* update_halo_kernel_module::update_halo_kernel, update_halo_kernel.f90:32-1427.
  * Reflective copies on the faces where both neighbour entries are -1. */
 void clover_update_halo_kernel(const int *x_min, const int *x_max, const int *y_min,
