@@ -172,6 +172,54 @@ def run_reference(args):
     return 0
 
 
+def mixed_leg(C, torch, deck, args, fp64_ms, fp64_sums, fp64_steps, barrier, world, dist):
+    """The same workload with FP32 storage (FP64 density, mass fluxes, work
+    arrays and arithmetic): timed the same way, and its field summaries
+    compared with the FP64 run's at the same steps."""
+    import numpy as np
+    n = args.cells
+    ch = C.Chunk(deck, C.PRECISION_MIXED)
+    stream = torch.cuda.ExternalStream(ch.stream)
+    ch.step(args.warmup)
+    ch.sync()
+    barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    ch.step(args.steps)
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    barrier()
+    if world > 1:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    ch.profile(True)
+    ch.step(args.steps)
+    groups = ch.profile_report()
+    ch.profile(False)
+    sums, steps = ch.summaries()
+    nbytes = ch.device_bytes
+    ch.close()
+    m = min(len(sums), len(fp64_sums))
+    assert np.array_equal(steps[:m], fp64_steps[:m])
+    rel = np.abs(sums[:m] - fp64_sums[:m]) / np.abs(fp64_sums[:m])
+    step_bytes = sum(g["bytes"] for g in groups) / args.steps
+    return {
+        "value": world * n ** 3 * args.steps / (ms / 1000.0), "unit": "cell-updates/s",
+        "ms_per_step": ms / args.steps, "speedup_vs_fp64": fp64_ms / ms,
+        "dtype": "f32 storage (f64 density, mass flux, work arrays, arithmetic)",
+        "device_gb": nbytes / 1e9,
+        "step_algorithmic_bytes_per_cell": step_bytes / n ** 3,
+        "step_achieved_gbs": step_bytes / (ms / args.steps / 1000.0) / 1e9,
+        "summary_steps_compared": int(m),
+        "max_rel_err_vs_fp64": dict(zip(["vol", "mass", "ie", "ke", "press"],
+                                        [float(x) for x in rel.max(axis=0)])),
+    }
+
+
 def e2e_dropin(C, args, n, steps):
     """The workload through the drop-in C ABI with host arrays, copies timed."""
     import numpy as np  # noqa: F401
@@ -211,6 +259,7 @@ def main():
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-mixed", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -293,6 +342,10 @@ def main():
                               "gbs": g["bytes"] / max(g["ms"], 1e-9) / 1e6,
                               "launches_per_step": g["launches"] / args.steps} for g in groups}
 
+    mixed = None
+    if prec == C.PRECISION_FP64 and not args.no_mixed:
+        mixed = mixed_leg(C, torch, deck, args, ms, summaries, sum_steps, barrier, world, dist)
+
     e2e = None
     if not args.no_e2e and rank == 0:
         e2e = e2e_dropin(C, args, n, args.steps)
@@ -316,6 +369,8 @@ def main():
             "last_summary": {"step": int(sum_steps[-1]), "vol_mass_ie_ke_press":
                              [float(x) for x in summaries[-1]]},
         }
+        if mixed:
+            line["mixed_fp32"] = mixed
         if e2e:
             line["e2e"] = e2e
         if cpu:

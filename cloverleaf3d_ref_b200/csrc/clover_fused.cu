@@ -15,13 +15,17 @@
 //                    the pressure is stored (revert then restores time level
 //                    0, and the corrector overwrites density1/energy1).
 //  k_pdv_flux        PdV corrector + flux_calc (shared velocity loads).
-//  k_cell_flux_f     advec_cell face pass with pre_vol from the volume fluxes.
-//  k_cell_update_f   advec_cell update pass, pre_vol recomputed, in place.
-//  k_mom_node_*      node flux, node mass post/pre (one pass, march along the
-//                    sweep axis for y and z sweeps).
-//  k_mom_vel3_*      momentum flux + velocity update for the three components
-//                    (march along the sweep axis for y and z sweeps; the
-//                    updated velocities go to the other buffer of a pair).
+//  k_cell_flux_f     advec_cell x face pass with pre_vol from the volume fluxes.
+//  k_cell_update_f   advec_cell x update pass, pre_vol recomputed, in place.
+//  k_cell_sweep_march  the whole y or z cell sweep in one pass, each thread
+//                    marching its column with the stencil in registers.
+//  k_mom_sweep_x     the whole x momentum sweep (three velocities) in one pass:
+//                    neighbouring nodes along x through warp shuffles, the
+//                    previous z plane in registers.
+//  k_mom_node_march / k_mom_vel3_march  y and z momentum sweeps: node pass and
+//                    velocity pass, each marching along the sweep axis with the
+//                    previous node's values in registers.
+//  Updated velocities go to the other buffer of each velocity pair.
 #include "clover_launch.h"
 
 namespace clover {
@@ -62,7 +66,7 @@ __device__ __forceinline__ double fmax2(double a, double b) { return b > a ? b :
 // viscosity_kernel.f90:71-134 with IF((limiter.GT.0.0).OR.(div.GE.0.0)) taken
 // as "div >= 0 -> 0, else limiter > 0 -> 0, else ..." (the same outcome).
 template <class S>
-__global__ void __launch_bounds__(BX * BY) k_timestep_visc(Geom g, Box b, GeomArrays ga,
+__global__ void __launch_bounds__(BX * BY, 4) k_timestep_visc(Geom g, Box b, GeomArrays ga,
     const typename S::rho_t* __restrict__ density0, const typename S::cs_t* __restrict__ pressure,
     typename S::cs_t* __restrict__ viscosity, const typename S::vel_t* __restrict__ xvel0,
     const typename S::vel_t* __restrict__ yvel0, const typename S::vel_t* __restrict__ zvel0) {
@@ -424,41 +428,12 @@ __device__ __forceinline__ double cell_product(const Geom& g, int variant, const
   return L(density1, j, k, l) * mom_post_vol<S>(g, variant, ga, vfx, vfy, vfz, j, k, l);
 }
 
-// Node pass for direction x: one thread per node computes node_flux(j),
-// node_mass_post(j) and node_mass_pre(j) (node_flux(j-1) recomputed).
-// Ranges: node_flux j in [x_min-2, x_max+2], masses j in [x_min-1, x_max+2],
-// k in [y_min, y_max+1], l in [z_min, z_max+1].
-template <class S>
-__global__ void __launch_bounds__(BX * BY) k_mom_node_x(Geom g, Box b, int variant, GeomArrays ga,
-    const typename S::mf_t* __restrict__ mf, const typename S::rho_t* __restrict__ density1,
-    const typename S::vf_t* __restrict__ vfx, const typename S::vf_t* __restrict__ vfy,
-    const typename S::vf_t* __restrict__ vfz, typename S::wk_t* __restrict__ node_flux,
-    typename S::wk_t* __restrict__ node_mass_post, typename S::wk_t* __restrict__ node_mass_pre) {
-  const int j = b.j0 + blockIdx.x * BX + threadIdx.x;
-  const int k = b.k0 + blockIdx.y * BY + threadIdx.y;
-  const int l = b.l0 + blockIdx.z;
-  if (j > b.j1 || k > b.k1) return;
-  using W = typename S::wk_t;
-  const double nf = node_flux_at<S, 1>(g, mf, j, k, l);
-  E(node_flux, j, k, l) = st<W>(nf);
-  if (j < g.x_min - 1) return;
-  auto P = [&](int jj, int kk, int ll) {
-    return cell_product<S>(g, variant, ga, density1, vfx, vfy, vfz, jj, kk, ll);
-  };
-  const double nmp = node_mass_sum(P(j, k - 1, l), P(j, k, l), P(j - 1, k - 1, l), P(j - 1, k, l),
-                                   P(j, k - 1, l - 1), P(j, k, l - 1), P(j - 1, k - 1, l - 1),
-                                   P(j - 1, k, l - 1));
-  E(node_mass_post, j, k, l) = st<W>(nmp);
-  const double nf_prev = node_flux_at<S, 1>(g, mf, j - 1, k, l);
-  E(node_mass_pre, j, k, l) = st<W>(nmp - nf_prev + nf);
-}
-
 // Node pass for direction y or z, marching along the sweep axis: thread
 // (j, c) walks p over the sweep range carrying the previous node flux and the
 // previous plane of cell products.
 // DIR 2: p = k, c = l; DIR 3: p = l, c = k.
 template <class S, int DIR>
-__global__ void __launch_bounds__(BX * BY) k_mom_node_march(Geom g, int jlo, int jhi, int clo,
+__global__ void __launch_bounds__(BX * BY, 4) k_mom_node_march(Geom g, int jlo, int jhi, int clo,
     int chi, int plo, int phi, int seg, int variant, GeomArrays ga,
     const typename S::mf_t* __restrict__ mf, const typename S::rho_t* __restrict__ density1,
     const typename S::vf_t* __restrict__ vfx, const typename S::vf_t* __restrict__ vfy,
@@ -551,43 +526,10 @@ __device__ __forceinline__ double mom_flux_at(double nf, double nmpre_i, double 
   return advec_vel_s * nf;
 }
 
-// Velocity pass for direction x: one thread per node updates the three
-// velocities (mom_flux at j-1 and j computed in the thread).
-template <class S>
-__global__ void __launch_bounds__(BX * BY) k_mom_vel3_x(Geom g, Box b, GeomArrays ga,
-    const typename S::wk_t* __restrict__ node_flux, const typename S::wk_t* __restrict__ node_mass_post,
-    const typename S::wk_t* __restrict__ node_mass_pre, const typename S::vel_t* __restrict__ u_in,
-    const typename S::vel_t* __restrict__ v_in, const typename S::vel_t* __restrict__ w_in,
-    typename S::vel_t* __restrict__ u_out, typename S::vel_t* __restrict__ v_out,
-    typename S::vel_t* __restrict__ w_out) {
-  const int j = b.j0 + blockIdx.x * BX + threadIdx.x;
-  const int k = b.k0 + blockIdx.y * BY + threadIdx.y;
-  const int l = b.l0 + blockIdx.z;
-  if (j > b.j1 || k > b.k1) return;
-  const double nf_m = L(node_flux, j - 1, k, l), nf_0 = L(node_flux, j, k, l);
-  const double pre_m = L(node_mass_pre, j - 1, k, l), pre_0 = L(node_mass_pre, j, k, l),
-               pre_p = L(node_mass_pre, j + 1, k, l);
-  const double post_0 = L(node_mass_post, j, k, l);
-  const double w_m = GX(ga.celldx, j - 1), w_0 = GX(ga.celldx, j);
-  const double cd_m2 = GX(ga.celldx, j - 2), cd_p1 = GX(ga.celldx, j + 1);
-  using V = typename S::vel_t;
-  const typename S::vel_t* in[3] = {u_in, v_in, w_in};
-  typename S::vel_t* out[3] = {u_out, v_out, w_out};
-#pragma unroll
-  for (int c = 0; c < 3; c++) {
-    const double vm2 = L(in[c], j - 2, k, l), vm1 = L(in[c], j - 1, k, l), v0 = L(in[c], j, k, l),
-                 vp1 = L(in[c], j + 1, k, l), vp2 = L(in[c], j + 2, k, l);
-    // mom_flux(j-1): donor j-1 (dif j-2) or j (dif j)
-    const double mf_m = mom_flux_at(nf_m, pre_m, pre_0, vm2, vm1, v0, vp1, w_m, cd_m2, w_0);
-    const double mf_0 = mom_flux_at(nf_0, pre_0, pre_p, vm1, v0, vp1, vp2, w_0, w_m, cd_p1);
-    E(out[c], j, k, l) = st<V>((v0 * pre_0 + mf_m - mf_0) / post_0);
-  }
-}
-
 // Velocity pass for direction y or z, marching along the sweep axis with the
 // previous momentum fluxes and the velocity window in registers.
 template <class S, int DIR>
-__global__ void __launch_bounds__(BX * BY) k_mom_vel3_march(Geom g, int jlo, int jhi, int clo,
+__global__ void __launch_bounds__(BX * BY, 3) k_mom_vel3_march(Geom g, int jlo, int jhi, int clo,
     int chi, int plo, int phi, int seg, GeomArrays ga,
     const typename S::wk_t* __restrict__ node_flux, const typename S::wk_t* __restrict__ node_mass_post,
     const typename S::wk_t* __restrict__ node_mass_pre, const typename S::vel_t* __restrict__ u_in,
@@ -623,14 +565,27 @@ __global__ void __launch_bounds__(BX * BY) k_mom_vel3_march(Geom g, int jlo, int
     mf_prev[q] = mom_flux_at(nf_m, pre_m, pre_0, vw[q][0], vw[q][1], vw[q][2], vw[q][3],
                              CD(p0 - 1), CD(p0 - 2), CD(p0));
   }
+  // loads of node p are issued one node ahead of their use
+  double nf_0 = LI(node_flux, IDX(p0));
+  double pre_p = LI(node_mass_pre, IDX(p0 + 1));
+  double post_0 = LI(node_mass_post, IDX(p0));
+  double vn[3];
+#pragma unroll
+  for (int q = 0; q < 3; q++) vn[q] = LI(in[q], IDX(p0 + 2));
   for (int p = p0; p <= p1; p++) {
-    const double nf_0 = LI(node_flux, IDX(p));
-    const double pre_p = LI(node_mass_pre, IDX(p + 1));
-    const double post_0 = LI(node_mass_post, IDX(p));
+    const bool more = p < p1;
+    double nf_n = 0.0, pre_n = 0.0, post_n = 0.0, vn_n[3] = {0.0, 0.0, 0.0};
+    if (more) {
+      nf_n = LI(node_flux, IDX(p + 1));
+      pre_n = LI(node_mass_pre, IDX(p + 2));
+      post_n = LI(node_mass_post, IDX(p + 1));
+#pragma unroll
+      for (int q = 0; q < 3; q++) vn_n[q] = LI(in[q], IDX(p + 3));
+    }
     const double w_0 = CD(p), cd_m1 = CD(p - 1), cd_p1 = CD(p + 1);
 #pragma unroll
     for (int q = 0; q < 3; q++) {
-      const double vp2 = LI(in[q], IDX(p + 2));
+      const double vp2 = vn[q];
       const double mf_0 = mom_flux_at(nf_0, pre_0, pre_p, vw[q][1], vw[q][2], vw[q][3], vp2, w_0,
                                       cd_m1, cd_p1);
       EI(out[q], IDX(p)) = st<V>((vw[q][2] * pre_0 + mf_prev[q] - mf_0) / post_0);
@@ -639,11 +594,183 @@ __global__ void __launch_bounds__(BX * BY) k_mom_vel3_march(Geom g, int jlo, int
       vw[q][1] = vw[q][2];
       vw[q][2] = vw[q][3];
       vw[q][3] = vp2;
+      vn[q] = vn_n[q];
     }
     pre_0 = pre_p;
+    nf_0 = nf_n;
+    pre_p = pre_n;
+    post_0 = post_n;
   }
 #undef CD
 #undef IDX
+}
+
+// ---------------------------------------------------------------------------
+// advec_cell sweep along y or z as ONE pass: thread (j, c) walks its whole
+// column along the sweep axis p (k for DIR 2, l for DIR 3) from the first face
+// to the last, holding the old density/energy of cells p-2..p+1 and the
+// pre-volumes of cells p-1, p in registers, so the donor/upwind selection
+// needs no dependent loads; cell p-1 is updated as soon as face p is known
+// (in place: no other thread reads this column's density or energy).
+// Faces p in [pmin, pmax+2] (c up to chi), cells p in [pmin, pmax] (c <= cmax).
+template <class S, int DIR>
+__global__ void __launch_bounds__(BX * BY, 3) k_cell_sweep_march(Geom g, int jlo, int jhi,
+    int clo, int chi, int cmax, int variant, GeomArrays ga,
+    typename S::rho_t* __restrict__ density1, typename S::ene_t* __restrict__ energy1,
+    const typename S::vf_t* __restrict__ vfx, const typename S::vf_t* __restrict__ vfy,
+    const typename S::vf_t* __restrict__ vfz, typename S::mf_t* __restrict__ mass_flux) {
+  const int j = jlo + blockIdx.x * BX + threadIdx.x;
+  const int c = clo + blockIdx.y * BY + threadIdx.y;
+  if (j > jhi || c > chi) return;
+#define IDX(p) j, (DIR == 2 ? (p) : c), (DIR == 2 ? c : (p))
+  const typename S::vf_t* vf_d = DIR == 2 ? vfy : vfz;
+  const int pmin = DIR == 2 ? g.y_min : g.z_min;
+  const int pmax = DIR == 2 ? g.y_max : g.z_max;
+  const double* vd = DIR == 2 ? ga.vertexdy : ga.vertexdz;
+#define VD(p) vd[(p) - pmin + 2]
+  const bool update = c <= cmax;
+  using R = typename S::rho_t;
+  using En = typename S::ene_t;
+  using MF = typename S::mf_t;
+  auto prevol = [&](int p) {
+    return cell_pre_vol<S>(g, variant, ga, vfx, vfy, vfz, IDX(p));
+  };
+  // window: d0..d3 = density1(p-2..p+1), e0..e3 = energy1(p-2..p+1), old values
+  double d0 = LI(density1, IDX(pmin - 2)), d1 = LI(density1, IDX(pmin - 1));
+  double d2 = LI(density1, IDX(pmin)), d3;
+  double e0 = LI(energy1, IDX(pmin - 2)), e1 = LI(energy1, IDX(pmin - 1));
+  double e2 = LI(energy1, IDX(pmin)), e3;
+  double pv_m = prevol(pmin - 1), pv_0;  // pre_vol(p-1), pre_vol(p)
+  double vf_prev = 0.0, mf_prev = 0.0, ef_prev = 0.0;
+  for (int p = pmin; p <= pmax + 2; p++) {
+    // cell p+1 is read by face p (the upwind index clamps to pmax+2 at the top)
+    const int pn = p + 1 <= pmax + 2 ? p + 1 : pmax + 2;
+    d3 = LI(density1, IDX(pn));
+    e3 = LI(energy1, IDX(pn));
+    pv_0 = prevol(p);
+    const double vf = LI(vf_d, IDX(p));
+    // advec_cell_kernel.f90:226-264 (y) / :321-359 (z) at face p
+    double d_up, d_don, d_dn, e_up, e_don, e_dn, pv_don;
+    int dif;
+    if (vf > 0.0) {  // upwind p-2, donor p-1, downwind p
+      d_up = d0; d_don = d1; d_dn = d2; e_up = e0; e_don = e1; e_dn = e2; pv_don = pv_m;
+      dif = p - 1;
+    } else {  // upwind min(p+1, pmax+2), donor p, downwind p-1
+      d_up = d3; d_don = d2; d_dn = d1; e_up = e3; e_don = e2; e_dn = e1; pv_don = pv_0;
+      dif = p + 1 < pmax + 2 ? p + 1 : pmax + 2;
+    }
+    const double sigmat = fabs(vf) / pv_don;
+    const double sigma3 = (1.0 + sigmat) * (VD(p) / VD(dif));
+    const double sigma4 = 2.0 - sigmat;
+    double diffuw = d_don - d_up;
+    double diffdw = d_dn - d_don;
+    double limiter = cell_limiter(sigmat, sigma3, sigma4, diffuw, diffdw);
+    const double mflux = vf * (d_don + limiter);
+    EI(mass_flux, IDX(p)) = st<MF>(mflux);
+    const double mf_stored = (double)st<MF>(mflux);
+    const double sigmam = fabs(mflux) / (d_don * pv_don);
+    diffuw = e_don - e_up;
+    diffdw = e_dn - e_don;
+    limiter = cell_limiter(sigmam, sigma3, sigma4, diffuw, diffdw);
+    const double eflux = (double)st<typename S::wk_t>(mflux * (e_don + limiter));
+    // advec_cell_kernel.f90:270-281 (y) / :365-376 (z) for cell p-1
+    if (update && p - 1 >= pmin && p - 1 <= pmax) {
+      const double pm = d1 * pv_m;
+      const double pom = pm + mf_prev - mf_stored;
+      const double poe = (e1 * pm + ef_prev - eflux) / pom;
+      const double av = pv_m + vf_prev - vf;
+      EI(density1, IDX(p - 1)) = st<R>(pom / av);
+      EI(energy1, IDX(p - 1)) = st<En>(poe);
+    }
+    vf_prev = vf;
+    mf_prev = mf_stored;
+    ef_prev = eflux;
+    d0 = d1; d1 = d2; d2 = d3;
+    e0 = e1; e1 = e2; e2 = e3;
+    pv_m = pv_0;
+  }
+#undef VD
+#undef IDX
+}
+
+// ---------------------------------------------------------------------------
+// advec_mom x sweep as ONE pass for the three velocities. Lane L of a warp
+// holds node j = j0 - 2 + L of row k and walks l over a segment; node_flux(j)
+// and the cell masses density1*post_vol of column j come from loads, the
+// values of column j-1 / node j+1 from the neighbouring lanes (shuffles), and
+// the plane l-1 terms from the previous step. Lanes 1..31 form node masses,
+// lanes 1..30 momentum fluxes, lanes 2..30 update (29 nodes per warp). Sums
+// and the momentum limiter keep the reference order
+// (advec_mom_kernel.f90:166-252).
+template <class S>
+__global__ void __launch_bounds__(BX * BY, 3) k_mom_sweep_x(Geom g, int seg, int variant,
+    GeomArrays ga, const typename S::mf_t* __restrict__ mfx,
+    const typename S::rho_t* __restrict__ density1, const typename S::vf_t* __restrict__ vfx,
+    const typename S::vf_t* __restrict__ vfy, const typename S::vf_t* __restrict__ vfz,
+    const typename S::vel_t* __restrict__ u_in, const typename S::vel_t* __restrict__ v_in,
+    const typename S::vel_t* __restrict__ w_in, typename S::vel_t* __restrict__ u_out,
+    typename S::vel_t* __restrict__ v_out, typename S::vel_t* __restrict__ w_out) {
+  const int lane = threadIdx.x;
+  const int j = g.x_min - 2 + blockIdx.x * 29 + lane;  // node of this lane
+  const int k = g.y_min + blockIdx.y * BY + threadIdx.y;
+  const int l0 = g.z_min + blockIdx.z * seg;
+  int l1 = l0 + seg - 1;
+  if (l1 > g.z_max + 1) l1 = g.z_max + 1;
+  const bool row = k <= g.y_max + 1;                // every lane of a row stays for the shuffles
+  const bool has_nf = row && j <= g.x_max + 2;     // node_flux range j in [x_min-2, x_max+2]
+  const bool has_mf = row && lane >= 1 && lane <= 30 && j >= g.x_min - 1 && j <= g.x_max + 1;
+  const bool has_up = row && lane >= 2 && lane <= 30 && j >= g.x_min && j <= g.x_max + 1;
+  auto P = [&](int kk, int ll) {
+    return cell_product<S>(g, variant, ga, density1, vfx, vfy, vfz, j, kk, ll);
+  };
+  using V = typename S::vel_t;
+  const typename S::vel_t* in[3] = {u_in, v_in, w_in};
+  typename S::vel_t* out[3] = {u_out, v_out, w_out};
+  const double cd_0 = has_nf ? GX(ga.celldx, j) : 1.0;
+  const double cd_m1 = has_mf ? GX(ga.celldx, j - 1) : 1.0;
+  const double cd_p1 = has_mf ? GX(ga.celldx, j + 1) : 1.0;
+  // plane l-1 terms: mass fluxes at (j, k-1), (j, k), (j+1, k-1), (j+1, k); cell
+  // masses at (j, k-1), (j, k)
+  double fm_a = 0.0, fm_b = 0.0, fm_c = 0.0, fm_d = 0.0, pm_a = 0.0, pm_b = 0.0;
+  if (has_nf) {
+    fm_a = L(mfx, j, k - 1, l0 - 1); fm_b = L(mfx, j, k, l0 - 1);
+    fm_c = L(mfx, j + 1, k - 1, l0 - 1); fm_d = L(mfx, j + 1, k, l0 - 1);
+    pm_a = P(k - 1, l0 - 1); pm_b = P(k, l0 - 1);
+  }
+  for (int l = l0; l <= l1; l++) {
+    double f_a = 0.0, f_b = 0.0, f_c = 0.0, f_d = 0.0, p_a = 0.0, p_b = 0.0;
+    if (has_nf) {
+      f_a = L(mfx, j, k - 1, l); f_b = L(mfx, j, k, l);
+      f_c = L(mfx, j + 1, k - 1, l); f_d = L(mfx, j + 1, k, l);
+      p_a = P(k - 1, l); p_b = P(k, l);
+    }
+    // node_flux(j): mfx(j,k-1,l) mfx(j,k,l) mfx(j+1,k-1,l) mfx(j+1,k,l) then l-1
+    const double nf = 0.125 * (f_a + f_b + f_c + f_d + fm_a + fm_b + fm_c + fm_d);
+    // cell masses of column j-1 from the lane below
+    const double q_a = __shfl_up_sync(0xffffffffu, p_a, 1);
+    const double q_b = __shfl_up_sync(0xffffffffu, p_b, 1);
+    const double qm_a = __shfl_up_sync(0xffffffffu, pm_a, 1);
+    const double qm_b = __shfl_up_sync(0xffffffffu, pm_b, 1);
+    // P(j,k-1,l) P(j,k,l) P(j-1,k-1,l) P(j-1,k,l) P(j,k-1,l-1) P(j,k,l-1) P(j-1,k-1,l-1) P(j-1,k,l-1)
+    const double nmp = node_mass_sum(p_a, p_b, q_a, q_b, pm_a, pm_b, qm_a, qm_b);
+    const double nf_m = __shfl_up_sync(0xffffffffu, nf, 1);
+    const double nmpre = nmp - nf_m + nf;
+    const double nmpre_p = __shfl_down_sync(0xffffffffu, nmpre, 1);
+#pragma unroll
+    for (int q = 0; q < 3; q++) {
+      double mf = 0.0, v0 = 0.0;
+      if (has_mf) {
+        const double vm1 = L(in[q], j - 1, k, l);
+        v0 = L(in[q], j, k, l);
+        const double vp1 = L(in[q], j + 1, k, l), vp2 = L(in[q], j + 2, k, l);
+        mf = mom_flux_at(nf, nmpre, nmpre_p, vm1, v0, vp1, vp2, cd_0, cd_m1, cd_p1);
+      }
+      const double mf_m = __shfl_up_sync(0xffffffffu, mf, 1);
+      if (has_up) E(out[q], j, k, l) = st<V>((v0 * nmpre + mf_m - mf) / nmp);
+    }
+    fm_a = f_a; fm_b = f_b; fm_c = f_c; fm_d = f_d;
+    pm_a = p_a; pm_b = p_b;
+  }
 }
 
 // Copy the halo shell of three vertex arrays (every node outside
@@ -727,23 +854,25 @@ void launch_advec_cell_fused(const Geom& g, cudaStream_t s, int advect_x, int di
     LAUNCH((k_cell_update_f<S, 1>), in, variant, ga, density1, energy1, vol_flux_x, vol_flux_y,
            vol_flux_z, mass_flux_x, ener_flux);
   } else if (dir == 2) {
-    LAUNCH((k_cell_flux_f<S, 2>), (Box{g.x_min, g.x_max, g.y_min, g.y_max + 2, g.z_min, g.z_max + 2}),
-           variant, ga, density1, energy1, vol_flux_x, vol_flux_y, vol_flux_z, mass_flux_y, ener_flux);
-    LAUNCH((k_cell_update_f<S, 2>), in, variant, ga, density1, energy1, vol_flux_x, vol_flux_y,
-           vol_flux_z, mass_flux_y, ener_flux);
+    // one pass; faces run over l up to z_max+2, cells update for l <= z_max
+    const int clo = g.z_min, chi = g.z_max + 2;
+    const dim3 gr((g.x_max - g.x_min + 1 + BX - 1) / BX, (chi - clo + 1 + BY - 1) / BY, 1);
+    k_cell_sweep_march<S, 2><<<gr, dim3(BX, BY), 0, s>>>(g, g.x_min, g.x_max, clo, chi, g.z_max,
+        variant, ga, density1, energy1, vol_flux_x, vol_flux_y, vol_flux_z, mass_flux_y);
   } else {
-    LAUNCH((k_cell_flux_f<S, 3>), (Box{g.x_min, g.x_max, g.y_min, g.y_max, g.z_min, g.z_max + 2}),
-           variant, ga, density1, energy1, vol_flux_x, vol_flux_y, vol_flux_z, mass_flux_z, ener_flux);
-    LAUNCH((k_cell_update_f<S, 3>), in, variant, ga, density1, energy1, vol_flux_x, vol_flux_y,
-           vol_flux_z, mass_flux_z, ener_flux);
+    const int clo = g.y_min, chi = g.y_max;
+    const dim3 gr((g.x_max - g.x_min + 1 + BX - 1) / BX, (chi - clo + 1 + BY - 1) / BY, 1);
+    k_cell_sweep_march<S, 3><<<gr, dim3(BX, BY), 0, s>>>(g, g.x_min, g.x_max, clo, chi, g.y_max,
+        variant, ga, density1, energy1, vol_flux_x, vol_flux_y, vol_flux_z, mass_flux_z);
   }
+  (void)in;
 }
 
 constexpr int kMarchSeg = 32;
 
 template <class S>
 void launch_advec_mom_fused(const Geom& g, cudaStream_t s, int advect_x, int sweep, int dir,
-                            const GeomArrays& ga, const typename S::rho_t* density1,
+                            double vol, const GeomArrays& ga, const typename S::rho_t* density1,
                             const typename S::mf_t* mass_flux_x, const typename S::mf_t* mass_flux_y,
                             const typename S::mf_t* mass_flux_z, const typename S::vf_t* vol_flux_x,
                             const typename S::vf_t* vol_flux_y, const typename S::vf_t* vol_flux_z,
@@ -758,13 +887,15 @@ void launch_advec_mom_fused(const Geom& g, cudaStream_t s, int advect_x, int swe
   else variant = 4;  // sweep 3: post_vol = volume
   const int x0 = g.x_min, x1 = g.x_max, y0 = g.y_min, y1 = g.y_max, z0 = g.z_min, z1 = g.z_max;
   if (dir == 1) {
-    LAUNCH(k_mom_node_x<S>, (Box{x0 - 2, x1 + 2, y0, y1 + 1, z0, z1 + 1}), variant, ga, mass_flux_x,
-           density1, vol_flux_x, vol_flux_y, vol_flux_z, node_flux, node_mass_post, node_mass_pre);
-    LAUNCH(k_mom_vel3_x<S>, (Box{x0, x1 + 1, y0, y1 + 1, z0, z1 + 1}), ga, node_flux,
-           node_mass_post, node_mass_pre, vel_in[0], vel_in[1], vel_in[2], vel_out[0], vel_out[1],
-           vel_out[2]);
+    // one pass: 29 nodes per warp along x, segments of kMarchSeg planes along z
+    const int nseg = (z1 + 1 - z0 + 1 + kMarchSeg - 1) / kMarchSeg;
+    const dim3 gx((x1 + 1 - x0 + 1 + 28) / 29, (y1 + 1 - y0 + 1 + BY - 1) / BY, nseg);
+    k_mom_sweep_x<S><<<gx, dim3(BX, BY), 0, s>>>(g, kMarchSeg, variant, ga, mass_flux_x, density1,
+        vol_flux_x, vol_flux_y, vol_flux_z, vel_in[0], vel_in[1], vel_in[2], vel_out[0],
+        vel_out[1], vel_out[2]);
   } else {
-    // node pass: march index from min-2 (flux) to max+2; masses from min-1
+    // node pass then velocity pass, each marching along the sweep axis in
+    // segments: node flux from min-2, node masses from min-1, updates min..max+1
     const int plo = (dir == 2 ? y0 : z0) - 2, phi = (dir == 2 ? y1 : z1) + 2;
     const int clo = dir == 2 ? z0 : y0, chi = (dir == 2 ? z1 : y1) + 1;
     const int nseg = (phi - plo + 1 + kMarchSeg - 1) / kMarchSeg;
@@ -787,6 +918,7 @@ void launch_advec_mom_fused(const Geom& g, cudaStream_t s, int advect_x, int swe
           ga, node_flux, node_mass_post, node_mass_pre, vel_in[0], vel_in[1], vel_in[2],
           vel_out[0], vel_out[1], vel_out[2]);
     }
+    (void)vol;
   }
   // the updated buffers take the halo shell of the inputs
   const dim3 gs((g.x_max - g.x_min + 6 + BX - 1) / BX, (g.y_max - g.y_min + 6 + BY - 1) / BY,
@@ -813,7 +945,7 @@ void launch_advec_mom_fused(const Geom& g, cudaStream_t s, int advect_x, int swe
                                            const GeomArrays&, S::rho_t*, S::ene_t*, S::mf_t*,  \
                                            const S::vf_t*, S::mf_t*, const S::vf_t*, S::mf_t*, \
                                            const S::vf_t*, S::wk_t*);                          \
-  template void launch_advec_mom_fused<S>(const Geom&, cudaStream_t, int, int, int,            \
+  template void launch_advec_mom_fused<S>(const Geom&, cudaStream_t, int, int, int, double,    \
                                           const GeomArrays&, const S::rho_t*, const S::mf_t*,  \
                                           const S::mf_t*, const S::mf_t*, const S::vf_t*,      \
                                           const S::vf_t*, const S::vf_t*, S::wk_t*, S::wk_t*,  \

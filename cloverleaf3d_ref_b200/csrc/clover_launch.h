@@ -24,15 +24,17 @@ struct F64 {
 };
 
 // Storage policy of the mixed-precision native path: FP32 storage for the
-// stencilled fields, FP64 kept for density, mass fluxes and work arrays
-// (pre/post volumes, node masses) where conservation needs it. All
-// arithmetic is FP64.
+// stencilled fields (energy, pressure, viscosity, sound speed, velocities),
+// FP64 kept where conservation needs it: density, mass fluxes, work arrays
+// (pre/post volumes, node masses) and the volume fluxes, whose differences
+// form the pre/post volumes and must cancel against the PdV volume change
+// for mass to be conserved. All arithmetic is FP64.
 struct F32Mixed {
   using rho_t = double;
   using ene_t = float;
   using cs_t = float;
   using vel_t = float;
-  using vf_t = float;
+  using vf_t = double;
   using mf_t = double;
   using wk_t = double;
 };
@@ -201,9 +203,10 @@ void launch_advec_cell_fused(const Geom& g, cudaStream_t s, int advect_x, int di
                              const typename S::vf_t* vol_flux_z, typename S::wk_t* ener_flux);
 // All three velocities of one sweep; vel_in/vel_out are the two buffers of
 // each velocity pair (the shell outside [min,max+1]^3 is copied across).
+// vol: the uniform cell volume of the chunk (dx*dy*dz).
 template <class S>
 void launch_advec_mom_fused(const Geom& g, cudaStream_t s, int advect_x, int sweep, int dir,
-                            const GeomArrays& ga, const typename S::rho_t* density1,
+                            double vol, const GeomArrays& ga, const typename S::rho_t* density1,
                             const typename S::mf_t* mass_flux_x, const typename S::mf_t* mass_flux_y,
                             const typename S::mf_t* mass_flux_z, const typename S::vf_t* vol_flux_x,
                             const typename S::vf_t* vol_flux_y, const typename S::vf_t* vol_flux_z,

@@ -122,6 +122,7 @@ struct Chunk : ChunkBase {
   std::vector<int> sum_steps;  // host: step of each recorded summary
   double* partials = nullptr;
 
+  double cell_volume = 0.0;  // dx*dy*dz, the volume of every cell (initialise_chunk)
   int host_step = 0;     // steps enqueued
   bool advect_x = true;  // start.f90:99
   bool use_graphs = true;
@@ -283,6 +284,7 @@ struct Chunk : ChunkBase {
     const double xmin = d.xmin + dx * (double)(float)0;
     const double ymin = d.ymin + dy * (double)(float)0;
     const double zmin = d.zmin + dz * (double)(float)0;
+    cell_volume = dx * dy * dz;  // initialise_chunk_kernel.f90:155
     launch_initialise_chunk(g, stream, xmin, ymin, zmin, dx, dy, dz, vertexx, vertexdx, vertexy,
                             vertexdy, vertexz, vertexdz, cellx, celldx, celly, celldy, cellz,
                             celldz, volume, xarea, yarea, zarea);
@@ -391,8 +393,12 @@ struct Chunk : ChunkBase {
       launch_advec_cell_fused<S>(g, stream, axi, dir, sweep_number, ga, density1, energy1,
                                  mass_flux_x, vol_flux_x, mass_flux_y, vol_flux_y, mass_flux_z,
                                  vol_flux_z, work[6]);
-      pend("advec_cell", n * ((G8 + nvf * VF8 + R8 + E8 + MF8 + W8) +
-                              (G8 + nvf * VF8 + 2 * R8 + 2 * E8 + MF8 + W8)));
+      // x: face pass + update pass; y, z: one marching pass (in place)
+      if (dir == 1)
+        pend("advec_cell_x", n * ((G8 + nvf * VF8 + R8 + E8 + MF8 + W8) +
+                                  (G8 + nvf * VF8 + 2 * R8 + 2 * E8 + MF8 + W8)));
+      else
+        pend("advec_cell_yz", n * (G8 + nvf * VF8 + 2 * R8 + 2 * E8 + MF8));
       pbeg();
       halo({2, 4, 9, 11, 13, 17, 18, 19}, 2, vc);
       pend("update_halo", 0);
@@ -401,10 +407,14 @@ struct Chunk : ChunkBase {
       V* vin[3] = {vel1(0, vc), vel1(1, vc), vel1(2, vc)};
       V* vout[3] = {vel1(0, vc ^ 1), vel1(1, vc ^ 1), vel1(2, vc ^ 1)};
       pbeg();
-      launch_advec_mom_fused<S>(g, stream, axi, sweep_number, dir, ga, density1, mass_flux_x,
+      launch_advec_mom_fused<S>(g, stream, axi, sweep_number, dir, cell_volume, ga, density1, mass_flux_x,
                                 mass_flux_y, mass_flux_z, vol_flux_x, vol_flux_y, vol_flux_z,
                                 work[0], work[1], work[2], vin, vout);
-      pend("advec_mom", n * ((MF8 + R8 + G8 + npv * VF8 + 3 * W8) + (3 * W8 + 6 * V8)));
+      // x: node pass + velocity pass; y, z: one marching pass
+      if (dir == 1)  // one pass
+        pend("advec_mom_x", n * (MF8 + R8 + G8 + npv * VF8 + 6 * V8));
+      else  // node pass + velocity pass
+        pend("advec_mom_yz", n * ((MF8 + R8 + G8 + npv * VF8 + 3 * W8) + (3 * W8 + 6 * V8)));
       vc ^= 1;
     };
     sweep(1, ax ? 1 : 3, true);
