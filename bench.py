@@ -15,6 +15,12 @@ roofline   dominant kernel group, algorithmic bytes / its event-timed duration
            (a profiled run of the same steps right after the timed one).
 cpu_baseline  the oracle (C restatement of the reference, OpenMP) on the
            host cores over a bounded sample of the same problem.
+ensemble   batched decks (seeded draws of the same problem with drawn sizes,
+           region, densities and energies): 64 decks of 24..128 cells per
+           axis for 150 steps (FP64 and mixed) and 512 decks of 16..48 cells
+           per axis for 100 steps (mixed, with its FP64 twin for the errors),
+           each autotuned and graph-replayed, against the same decks run one
+           after another as single chunks (graph-replayed too).
 
 --impl reference times that CPU restatement alone (the Fortran reference
 cannot be compiled on this image: no Fortran compiler).
@@ -220,6 +226,91 @@ def mixed_leg(C, torch, deck, args, fp64_ms, fp64_sums, fp64_steps, barrier, wor
     }
 
 
+def timed_steps(torch, obj, steps):
+    """Device time (ms) of obj.step(steps) with events on obj's stream."""
+    stream = torch.cuda.ExternalStream(obj.stream)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    obj.step(steps)
+    e1.record(stream)
+    e1.synchronize()
+    return e0.elapsed_time(e1)
+
+
+def ensemble_leg(C, torch, name, n_decks, cells, steps, seed, precisions, seq_decks, warm=3):
+    """One ensemble configuration: per precision, the batched run (autotuned,
+    then warm steps, then the rest of the steps timed); then the same decks
+    one after another as single chunks (the first seq_decks of them, the
+    rate scaled by their cells), and the per-deck summary error of the mixed
+    run against the FP64 run at every summary step."""
+    import numpy as np
+    decks = C.draw_decks(n_decks, seed, cells=cells, end_step=steps, summary_frequency=10)
+    total = sum(d.cells for d in decks)
+    timed = steps - warm
+    out = {"decks": n_decks, "cells_per_axis": list(cells), "steps": steps, "seed": seed,
+           "total_cells": total}
+    sums = {}
+    for prec in precisions:
+        key = "fp64" if prec == C.PRECISION_FP64 else "mixed"
+        ens = C.Ensemble(decks, prec)
+        t0 = time.perf_counter()
+        ens.autotune(1)
+        tune_s = time.perf_counter() - t0
+        ens.step(warm)
+        ens.sync()
+        ms = timed_steps(torch, ens, timed)
+        assert ens.run() == steps
+        bad = [d for d in range(n_decks) if ens.deck_status(d) != 0]
+        sums[key] = [ens.deck_summaries(d)[0] for d in range(n_decks)]
+        sched = ens.schedule()
+        out[key] = {
+            "value": total * timed / (ms / 1000.0), "unit": "cell-updates/s",
+            "ms_per_step": ms / timed, "autotune_s": tune_s,
+            "graph_nodes_per_step": ens.launches_per_step, "device_gb": ens.device_bytes / 1e9,
+            "decks_with_status": bad,
+            "schedule": {"launches": len(sched),
+                         "order_counts": [sum(1 for x in sched if x["order"] == o)
+                                          for o in range(3)],
+                         "grid_div_counts": {str(v): sum(1 for x in sched if x["grid_div"] == v)
+                                             for v in sorted({x["grid_div"] for x in sched})},
+                         "segs": sorted({x["seg"] for x in sched if x["seg"] > 0})},
+        }
+        ens.close()
+    # the same decks one after another (single chunks, graph replay)
+    prec = precisions[0]
+    key = "fp64" if prec == C.PRECISION_FP64 else "mixed"
+    sample = decks[:seq_decks]
+    seq_ms = 0.0
+    for d in sample:
+        ch = C.Chunk(d, prec)
+        ch.step(warm)
+        ch.sync()
+        seq_ms += timed_steps(torch, ch, timed)
+        ch.close()
+    seq_cells = sum(d.cells for d in sample)
+    seq_value = seq_cells * timed / (seq_ms / 1000.0)
+    out["sequential"] = {"precision": key, "value": seq_value, "unit": "cell-updates/s",
+                         "decks_timed": len(sample),
+                         "sample": "first %d of %d decks, rate over their cells" % (
+                             len(sample), n_decks)}
+    out["speedup_vs_sequential"] = out[key]["value"] / seq_value
+    if "fp64" in sums and "mixed" in sums:
+        errs = []
+        for a, b in zip(sums["mixed"], sums["fp64"]):
+            scale = np.maximum(np.abs(b), 1e-300)
+            errs.append(np.abs(a - b) / scale)
+        e = np.stack(errs)  # deck, summary, quantity
+        last = e[:, -1, :]
+        out["mixed_rel_err_vs_fp64"] = {
+            "at_last_summary_max_over_decks": dict(zip(
+                ["vol", "mass", "ie", "ke", "press"], [float(x) for x in last.max(axis=0)])),
+            "all_summaries_max_over_decks_excluding_ke_at_step0": float(
+                max(e[:, :, [0, 1, 2, 4]].max(), e[:, 1:, 3].max() if e.shape[1] > 1 else 0.0)),
+        }
+    return out
+
+
 def e2e_dropin(C, args, n, steps):
     """The workload through the drop-in C ABI with host arrays, copies timed."""
     import numpy as np  # noqa: F401
@@ -249,6 +340,17 @@ def e2e_dropin(C, args, n, steps):
             "seconds": t1 - t0, "steps": taken, "cells": "%d^3" % n}
 
 
+def ensembles(C, torch):
+    """The two ensemble configurations (64 decks FP64 + mixed; 512 small decks
+    mixed with its FP64 twin)."""
+    return {
+        "decks64": ensemble_leg(C, torch, "decks64", 64, (24, 128), 150, 2024,
+                                [C.PRECISION_FP64, C.PRECISION_MIXED], 64),
+        "decks512": ensemble_leg(C, torch, "decks512", 512, (16, 48), 100, 4048,
+                                 [C.PRECISION_MIXED, C.PRECISION_FP64], 64),
+    }
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -260,6 +362,9 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-mixed", action="store_true")
+    ap.add_argument("--no-ensemble", action="store_true")
+    ap.add_argument("--ensemble-only", action="store_true",
+                    help="only the ensemble legs (a separate JSON line)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -283,6 +388,11 @@ def main():
     def barrier():
         if world > 1:
             dist.barrier()
+
+    if args.ensemble_only:
+        if rank == 0:
+            print(json.dumps({"ensemble": ensembles(C, torch)}))
+        return 0
 
     n = args.cells
     prec = C.PRECISION_MIXED if args.precision == "mixed" else C.PRECISION_FP64
@@ -352,6 +462,9 @@ def main():
     cpu = None
     if not args.no_cpu and rank == 0 and world == 1:
         cpu = cpu_baseline(n)
+    ens = None
+    if not args.no_ensemble and rank == 0 and world == 1:
+        ens = ensembles(C, torch)
 
     if rank == 0:
         line = {
@@ -375,6 +488,8 @@ def main():
             line["e2e"] = e2e
         if cpu:
             line["cpu_baseline"] = cpu
+        if ens:
+            line["ensemble"] = ens
         print(json.dumps(line))
     if world > 1:
         dist.destroy_process_group()

@@ -7,6 +7,11 @@ Python bindings (ctypes) of libclover_b200.so:
 * ``Chunk``     -- a chunk resident in HBM, stepped on the device from CUDA
                    graphs (FP64, or FP32 storage with FP64 where conservation
                    needs it).
+* ``Ensemble``  -- many independent decks of any sizes advanced together,
+                   each with its own dt, every kernel of the step launched
+                   once over all decks (autotuned schedules, CUDA graphs).
+* ``draw_decks`` -- seeded ensemble decks: the two-state shock problem with
+                   drawn sizes, region and densities/energies.
 * ``DropIn``    -- the reference's control flow driving the drop-in C ABI
                    (include/clover_kernels.h) with host arrays.
 * ``abi``       -- the raw ctypes handle of the drop-in entry points.
@@ -154,6 +159,25 @@ def _declare(L):
     L.clover_chunk_profile.argtypes = [P, ctypes.c_int]
     L.clover_chunk_profile_report.argtypes = [P, P, ctypes.c_int, P, P, P, ctypes.c_int]
     L.clover_chunk_profile_report.restype = ctypes.c_int
+    L.clover_ensemble_create.argtypes = [P, ctypes.c_int, ctypes.c_int]
+    L.clover_ensemble_create.restype = P
+    for n in ("clover_ensemble_decks", "clover_ensemble_reset"):
+        getattr(L, n).argtypes = [P]
+        getattr(L, n).restype = ctypes.c_int
+    L.clover_ensemble_autotune.argtypes = [P, ctypes.c_int]
+    L.clover_ensemble_autotune.restype = ctypes.c_int
+    L.clover_ensemble_schedule.argtypes = [P, ctypes.c_char_p, ctypes.c_int]
+    L.clover_ensemble_schedule.restype = ctypes.c_int
+    L.clover_ensemble_status.argtypes = [P, ctypes.c_int]
+    L.clover_ensemble_status.restype = ctypes.c_int
+    L.clover_ensemble_time.argtypes = [P, ctypes.c_int]
+    L.clover_ensemble_time.restype = ctypes.c_double
+    L.clover_ensemble_dt_history.argtypes = [P, ctypes.c_int, P, ctypes.c_int]
+    L.clover_ensemble_dt_history.restype = ctypes.c_int
+    L.clover_ensemble_summaries.argtypes = [P, ctypes.c_int, P, P, ctypes.c_int]
+    L.clover_ensemble_summaries.restype = ctypes.c_int
+    L.clover_ensemble_read_field.argtypes = [P, ctypes.c_int, ctypes.c_int, P]
+    L.clover_ensemble_read_field.restype = ctypes.c_int
     L.clover_dropin_create.argtypes = [P]
     L.clover_dropin_create.restype = P
     L.clover_dropin_run.argtypes = [P, ctypes.c_int]
@@ -338,6 +362,121 @@ class Chunk:
         assert a.shape == field_shape(name, s.x_cells, s.y_cells, s.z_cells)
         if lib().clover_chunk_write_field(self.h, FIELD_IDS[name], a.ctypes.data) != 0:
             raise CloverError("write_field failed")
+
+
+class Ensemble(Chunk):
+    """Independent decks advanced together on the current CUDA device.
+
+    Every deck keeps its own dt, time and calc_dt reduction; the decks share
+    end_step, summary_frequency and calc_dt's safety factors. ``step``,
+    ``run``, ``sync``, ``profile`` and ``use_graphs`` act on all decks; the
+    per-deck results take a deck index."""
+
+    def __init__(self, decks, precision=PRECISION_FP64):
+        L = lib()
+        self.decks = list(decks)
+        self.deck = self.decks[0]
+        self.precision = precision
+        arr = (DeckStruct * len(self.decks))(*[d.s for d in self.decks])
+        self._arr = arr
+        self.h = L.clover_ensemble_create(ctypes.cast(arr, ctypes.c_void_p), len(self.decks),
+                                          precision)
+        if not self.h:
+            raise CloverError("ensemble: " + L.clover_last_error().decode())
+
+    def __len__(self):
+        return len(self.decks)
+
+    @property
+    def cells(self):
+        return sum(d.cells for d in self.decks)
+
+    def autotune(self, trial_steps=2):
+        """Pick each batched launch's schedule by timing candidates; the
+        decks are set back to step 0 afterwards."""
+        n = lib().clover_ensemble_autotune(self.h, trial_steps)
+        if n < 0:
+            raise CloverError("ensemble autotune failed")
+        return n
+
+    def reset(self):
+        if lib().clover_ensemble_reset(self.h) != 0:
+            raise CloverError("ensemble reset failed")
+
+    def schedule(self):
+        """The schedule in use: one dict per batched launch."""
+        n = lib().clover_ensemble_schedule(self.h, None, 0)
+        buf = ctypes.create_string_buffer(n + 1)
+        lib().clover_ensemble_schedule(self.h, buf, n + 1)
+        out = []
+        for line in buf.value.decode().splitlines():
+            key, order, div, seg, blocks, items = (int(x) for x in line.split())
+            out.append({"key": key, "order": order, "grid_div": div, "seg": seg,
+                        "blocks": blocks, "items": items})
+        return out
+
+    def deck_status(self, d):
+        return lib().clover_ensemble_status(self.h, d)
+
+    def deck_time(self, d):
+        return lib().clover_ensemble_time(self.h, d)
+
+    def deck_dt_history(self, d):
+        n = self.steps
+        out = np.zeros(max(n, 1))
+        got = lib().clover_ensemble_dt_history(self.h, d, out.ctypes.data, n)
+        if got < 0:
+            raise CloverError("bad deck index")
+        return out[:got]
+
+    def deck_summaries(self, d, cap=100000):
+        out = np.zeros((cap, 5))
+        st = np.zeros(cap, dtype=np.int32)
+        n = lib().clover_ensemble_summaries(self.h, d, out.ctypes.data, st.ctypes.data, cap)
+        if n < 0:
+            raise CloverError("bad deck index")
+        return out[:n], st[:n]
+
+    def deck_field(self, d, name):
+        s = self.decks[d].s
+        a = np.zeros(field_shape(name, s.x_cells, s.y_cells, s.z_cells), order="F")
+        if lib().clover_ensemble_read_field(self.h, d, FIELD_IDS[name], a.ctypes.data) != 0:
+            raise CloverError("read_field failed")
+        return a
+
+    def field(self, name):
+        return self.deck_field(0, name)
+
+    def set_field(self, name, a):
+        raise CloverError("ensembles are set up from their decks only")
+
+
+def draw_decks(n, seed, cells=(24, 128), end_step=150, summary_frequency=10):
+    """Seeded ensemble decks of the two-state shock problem on [0,10]^3.
+
+    Per deck: cells per axis uniform in cells (inclusive, independent per
+    axis); a high-state cuboid [0,u]x[0,v]x[0,w] with u, v, w uniform in
+    [1,6]; background density lognormal(ln 0.2, 0.3), region density
+    lognormal(ln 1.0, 0.3), both energies uniform in [0.5, 3.0]; zero
+    velocity; dt 0.04 initial and maximum, rise 1.5; end_time far beyond
+    end_step * 0.04 so that every deck runs end_step steps."""
+    rng = np.random.default_rng(seed)
+    out = []
+    lo, hi = cells
+    for _ in range(n):
+        nx, ny, nz = (int(v) for v in rng.integers(lo, hi + 1, size=3))
+        u, v, w = (float(x) for x in rng.uniform(1.0, 6.0, size=3))
+        rho_bg = float(rng.lognormal(np.log(0.2), 0.3))
+        rho_hi = float(rng.lognormal(np.log(1.0), 0.3))
+        e_bg, e_hi = (float(x) for x in rng.uniform(0.5, 3.0, size=2))
+        out.append(Deck.from_values(
+            [dict(density=rho_bg, energy=e_bg),
+             dict(density=rho_hi, energy=e_hi, geometry="cuboid", xmin=0.0, xmax=u,
+                  ymin=0.0, ymax=v, zmin=0.0, zmax=w)],
+            x_cells=nx, y_cells=ny, z_cells=nz, xmin=0.0, xmax=10.0, ymin=0.0, ymax=10.0,
+            zmin=0.0, zmax=10.0, initial_timestep=0.04, timestep_rise=1.5, max_timestep=0.04,
+            end_step=end_step, end_time=1.0e6, summary_frequency=summary_frequency))
+    return out
 
 
 class DropIn:

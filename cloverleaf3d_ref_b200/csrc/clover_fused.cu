@@ -43,10 +43,54 @@ inline dim3 grid_of(const Box& b, int march = 1) {
   return dim3((nj + BX - 1) / BX, (nk + BY - 1) / BY, (nl + march - 1) / march);
 }
 
+// Index ranges of the kernels, from a chunk's geometry (device: per tile of
+// a mapped kernel; host: the tile grid of a launch).
+__host__ __device__ inline Box interior(const Geom& g) {
+  return Box{g.x_min, g.x_max, g.y_min, g.y_max, g.z_min, g.z_max};
+}
+__host__ __device__ inline Box nodes(const Geom& g) {
+  return Box{g.x_min, g.x_max + 1, g.y_min, g.y_max + 1, g.z_min, g.z_max + 1};
+}
+// x faces of the x cell sweep: j to x_max+2 over the interior rows
+template <int DIR>
+__host__ __device__ inline Box cell_flux_box(const Geom& g) {
+  static_assert(DIR == 1, "the fused face pass serves the x sweep");
+  return Box{g.x_min, g.x_max + 2, g.y_min, g.y_max, g.z_min, g.z_max};
+}
+
+// A marching kernel's threads cover j in [jlo, jhi] and the cross axis c in
+// [clo, chi] and walk the sweep axis p over [plo, phi] (cell sweeps: faces
+// from the sweep axis minimum to its maximum+2, cells updated for c <= cmax).
+struct MarchRange {
+  int jlo, jhi, clo, chi, plo, phi, cmax;
+};
+// advec_mom y/z node pass: node fluxes from min-2 to max+2 along the sweep
+template <int DIR>
+__host__ __device__ inline MarchRange mom_node_range(const Geom& g) {
+  const int pmin = DIR == 2 ? g.y_min : g.z_min, pmax = DIR == 2 ? g.y_max : g.z_max;
+  const int cmin = DIR == 2 ? g.z_min : g.y_min, cmx = DIR == 2 ? g.z_max : g.y_max;
+  return MarchRange{g.x_min, g.x_max + 1, cmin, cmx + 1, pmin - 2, pmax + 2, cmx + 1};
+}
+// advec_mom y/z velocity pass: nodes min..max+1 along the sweep
+template <int DIR>
+__host__ __device__ inline MarchRange mom_vel_range(const Geom& g) {
+  const int pmin = DIR == 2 ? g.y_min : g.z_min, pmax = DIR == 2 ? g.y_max : g.z_max;
+  const int cmin = DIR == 2 ? g.z_min : g.y_min, cmx = DIR == 2 ? g.z_max : g.y_max;
+  return MarchRange{g.x_min, g.x_max + 1, cmin, cmx + 1, pmin, pmax + 1, cmx + 1};
+}
+// advec_cell y sweep: columns l in [z_min, z_max+2] (the reference's y face
+// range), cells updated for l <= z_max; z sweep: rows k in [y_min, y_max]
+template <int DIR>
+__host__ __device__ inline MarchRange cell_sweep_range(const Geom& g) {
+  if (DIR == 2)
+    return MarchRange{g.x_min, g.x_max, g.z_min, g.z_max + 2, g.y_min, g.y_max + 2, g.z_max};
+  return MarchRange{g.x_min, g.x_max, g.y_min, g.y_max, g.z_min, g.z_max + 2, g.y_max};
+}
+
 #define E(a, jj, kk, ll) (a)[off3(g, (jj), (kk), (ll))]
-#define GX(a, jj) (a)[(jj) - g.x_min + 2]
-#define GY(a, kk) (a)[(kk) - g.y_min + 2]
-#define GZ(a, ll) (a)[(ll) - g.z_min + 2]
+#define GX(a, jj) (a)[g.o1 + (jj) - g.x_min + 2]
+#define GY(a, kk) (a)[g.o1 + (kk) - g.y_min + 2]
+#define GZ(a, ll) (a)[g.o1 + (ll) - g.z_min + 2]
 
 __device__ __forceinline__ double ld(const double* p) { return __ldg(p); }
 __device__ __forceinline__ double ld(const float* p) { return (double)__ldg(p); }
@@ -65,14 +109,16 @@ __device__ __forceinline__ double fmax2(double a, double b) { return b > a ? b :
 // ---------------------------------------------------------------------------
 // viscosity_kernel.f90:71-134 with IF((limiter.GT.0.0).OR.(div.GE.0.0)) taken
 // as "div >= 0 -> 0, else limiter > 0 -> 0, else ..." (the same outcome).
-template <class S>
-__global__ void __launch_bounds__(BX * BY, 4) k_timestep_visc(Geom g, Box b, GeomArrays ga,
+template <class S, class M>
+__global__ void __launch_bounds__(BX * BY, 4) k_timestep_visc(M m, GeomArrays ga,
     const typename S::rho_t* __restrict__ density0, const typename S::cs_t* __restrict__ pressure,
     typename S::cs_t* __restrict__ viscosity, const typename S::vel_t* __restrict__ xvel0,
     const typename S::vel_t* __restrict__ yvel0, const typename S::vel_t* __restrict__ zvel0) {
-  const int j = b.j0 + blockIdx.x * BX + threadIdx.x;
-  const int k = b.k0 + blockIdx.y * BY + threadIdx.y;
-  const int l = b.l0 + blockIdx.z;
+  m.run([&](const Geom& g, const Tile& t) {
+  const Box b = interior(g);
+  const int j = b.j0 + t.x * BX + threadIdx.x;
+  const int k = b.k0 + t.y * BY + threadIdx.y;
+  const int l = b.l0 + t.z;
   if (j > b.j1 || k > b.k1) return;
   const double u000 = L(xvel0, j, k, l), u100 = L(xvel0, j + 1, k, l);
   const double u010 = L(xvel0, j, k + 1, l), u110 = L(xvel0, j + 1, k + 1, l);
@@ -140,23 +186,26 @@ __global__ void __launch_bounds__(BX * BY, 4) k_timestep_visc(Geom g, Box b, Geo
     }
   }
   E(viscosity, j, k, l) = st<typename S::cs_t>(q);
+  });
 }
 
 // ---------------------------------------------------------------------------
 // PdV_kernel.f90:72-118 (predict) followed by ideal_gas_kernel.f90:47-58 on
 // the predicted density1/energy1; the pressure is stored in place (each
 // thread reads and writes only its own cell).
-template <class S>
-__global__ void __launch_bounds__(BX * BY) k_pdv_predict_eos(Geom g, Box b, const double* dt_ptr,
+template <class S, class M>
+__global__ void __launch_bounds__(BX * BY) k_pdv_predict_eos(M m, const double* dt_ptr,
     GeomArrays ga, const typename S::rho_t* __restrict__ density0,
     const typename S::ene_t* __restrict__ energy0, typename S::cs_t* __restrict__ pressure,
     const typename S::cs_t* __restrict__ viscosity, const typename S::vel_t* __restrict__ xvel0,
     const typename S::vel_t* __restrict__ yvel0, const typename S::vel_t* __restrict__ zvel0) {
-  const int j = b.j0 + blockIdx.x * BX + threadIdx.x;
-  const int k = b.k0 + blockIdx.y * BY + threadIdx.y;
-  const int l = b.l0 + blockIdx.z;
+  m.run([&](const Geom& g, const Tile& t) {
+  const Box b = interior(g);
+  const int j = b.j0 + t.x * BX + threadIdx.x;
+  const int k = b.k0 + t.y * BY + threadIdx.y;
+  const int l = b.l0 + t.z;
   if (j > b.j1 || k > b.k1) return;
-  const double dt = *dt_ptr;
+  const double dt = dt_ptr[(long long)t.d * kScalarStride];
 #define XS(jj) (L(xvel0, jj, k, l) + L(xvel0, jj, k + 1, l) + L(xvel0, jj, k, l + 1) + L(xvel0, jj, k + 1, l + 1))
 #define YS(kk) (L(yvel0, j, kk, l) + L(yvel0, j + 1, kk, l) + L(yvel0, j, kk, l + 1) + L(yvel0, j + 1, kk, l + 1))
 #define ZS(ll) (L(zvel0, j, k, ll) + L(zvel0, j + 1, k, ll) + L(zvel0, j, k + 1, ll) + L(zvel0, j + 1, k + 1, ll))
@@ -196,14 +245,15 @@ __global__ void __launch_bounds__(BX * BY) k_pdv_predict_eos(Geom g, Box b, cons
   const double e1 = (double)st<En>(L(energy0, j, k, l) - energy_change);
   const double d1 = (double)st<R>(d0 * vol_change_s);
   E(pressure, j, k, l) = st<typename S::cs_t>((1.4 - 1.0) * d1 * e1);
+  });
 }
 
 // ---------------------------------------------------------------------------
 // PdV_kernel.f90:120-166 (corrector) + flux_calc_kernel.f90:58-91 over the
 // node box [min, max+1]^3: cells in the interior run the corrector, faces in
 // the flux ranges get their volume flux.
-template <class S>
-__global__ void __launch_bounds__(BX * BY) k_pdv_flux(Geom g, Box b, const double* dt_ptr,
+template <class S, class M>
+__global__ void __launch_bounds__(BX * BY, 5) k_pdv_flux(M m, const double* dt_ptr,
     GeomArrays ga, const typename S::rho_t* __restrict__ density0,
     typename S::rho_t* __restrict__ density1, const typename S::ene_t* __restrict__ energy0,
     typename S::ene_t* __restrict__ energy1, const typename S::cs_t* __restrict__ pressure,
@@ -212,11 +262,13 @@ __global__ void __launch_bounds__(BX * BY) k_pdv_flux(Geom g, Box b, const doubl
     const typename S::vel_t* __restrict__ yvel1, const typename S::vel_t* __restrict__ zvel0,
     const typename S::vel_t* __restrict__ zvel1, typename S::vf_t* __restrict__ vol_flux_x,
     typename S::vf_t* __restrict__ vol_flux_y, typename S::vf_t* __restrict__ vol_flux_z) {
-  const int j = b.j0 + blockIdx.x * BX + threadIdx.x;
-  const int k = b.k0 + blockIdx.y * BY + threadIdx.y;
-  const int l = b.l0 + blockIdx.z;
+  m.run([&](const Geom& g, const Tile& t) {
+  const Box b = nodes(g);
+  const int j = b.j0 + t.x * BX + threadIdx.x;
+  const int k = b.k0 + t.y * BY + threadIdx.y;
+  const int l = b.l0 + t.z;
   if (j > b.j1 || k > b.k1) return;
-  const double dt = *dt_ptr;
+  const double dt = dt_ptr[(long long)t.d * kScalarStride];
   const bool jin = j <= g.x_max, kin = k <= g.y_max, lin = l <= g.z_max;
   using F = typename S::vf_t;
   // face sums of the node velocities, reference order (vel0 x4 then vel1 x4)
@@ -268,6 +320,7 @@ __global__ void __launch_bounds__(BX * BY) k_pdv_flux(Geom g, Box b, const doubl
       (L(pressure, j, k, l) / d0 + L(viscosity, j, k, l) / d0) * total_flux * recip_volume;
   E(energy1, j, k, l) = st<typename S::ene_t>(L(energy0, j, k, l) - energy_change);
   E(density1, j, k, l) = st<typename S::rho_t>(d0 * vol_change_s);
+  });
 }
 
 // ---------------------------------------------------------------------------
@@ -309,15 +362,17 @@ __device__ __forceinline__ double cell_limiter(double sig, double sigma3, double
 
 // advec_cell face pass (:125-171, :220-266, :315-361) with pre_vol(donor)
 // computed from the volume fluxes instead of read from a work array.
-template <class S, int DIR>
-__global__ void __launch_bounds__(BX * BY) k_cell_flux_f(Geom g, Box b, int variant, GeomArrays ga,
+template <class S, int DIR, class M>
+__global__ void __launch_bounds__(BX * BY) k_cell_flux_f(M m, int variant, GeomArrays ga,
     const typename S::rho_t* __restrict__ density1, const typename S::ene_t* __restrict__ energy1,
     const typename S::vf_t* __restrict__ vfx, const typename S::vf_t* __restrict__ vfy,
     const typename S::vf_t* __restrict__ vfz, typename S::mf_t* __restrict__ mass_flux,
     typename S::wk_t* __restrict__ ener_flux) {
-  const int j = b.j0 + blockIdx.x * BX + threadIdx.x;
-  const int k = b.k0 + blockIdx.y * BY + threadIdx.y;
-  const int l = b.l0 + blockIdx.z;
+  m.run([&](const Geom& g, const Tile& t) {
+  const Box b = cell_flux_box<DIR>(g);
+  const int j = b.j0 + t.x * BX + threadIdx.x;
+  const int k = b.k0 + t.y * BY + threadIdx.y;
+  const int l = b.l0 + t.z;
   if (j > b.j1 || k > b.k1) return;
   const typename S::vf_t* vf_d = DIR == 1 ? vfx : DIR == 2 ? vfy : vfz;
   const int i = DIR == 1 ? j : DIR == 2 ? k : l;
@@ -336,7 +391,7 @@ __global__ void __launch_bounds__(BX * BY) k_cell_flux_f(Geom g, Box b, int vari
   const double pv_donor = cell_pre_vol<S>(g, variant, ga, vfx, vfy, vfz, DIR == 1 ? donor : j,
                                           DIR == 2 ? donor : k, DIR == 3 ? donor : l);
   const double sigmat = fabs(vf) / pv_donor;
-  const double sigma3 = (1.0 + sigmat) * (vd[i - vlo + 2] / vd[dif - vlo + 2]);
+  const double sigma3 = (1.0 + sigmat) * (vd[g.o1 + i - vlo + 2] / vd[g.o1 + dif - vlo + 2]);
   const double sigma4 = 2.0 - sigmat;
   const double d_donor = AT(density1, donor);
   double diffuw = d_donor - AT(density1, upwind);
@@ -351,18 +406,21 @@ __global__ void __launch_bounds__(BX * BY) k_cell_flux_f(Geom g, Box b, int vari
   limiter = cell_limiter(sigmam, sigma3, sigma4, diffuw, diffdw);
   E(ener_flux, j, k, l) = st<typename S::wk_t>(mflux * (e_donor + limiter));
 #undef AT
+  });
 }
 
 // advec_cell update pass, in place (each thread reads and writes its own cell).
-template <class S, int DIR>
-__global__ void __launch_bounds__(BX * BY) k_cell_update_f(Geom g, Box b, int variant, GeomArrays ga,
+template <class S, int DIR, class M>
+__global__ void __launch_bounds__(BX * BY) k_cell_update_f(M m, int variant, GeomArrays ga,
     typename S::rho_t* __restrict__ density1, typename S::ene_t* __restrict__ energy1,
     const typename S::vf_t* __restrict__ vfx, const typename S::vf_t* __restrict__ vfy,
     const typename S::vf_t* __restrict__ vfz, const typename S::mf_t* __restrict__ mass_flux,
     const typename S::wk_t* __restrict__ ener_flux) {
-  const int j = b.j0 + blockIdx.x * BX + threadIdx.x;
-  const int k = b.k0 + blockIdx.y * BY + threadIdx.y;
-  const int l = b.l0 + blockIdx.z;
+  m.run([&](const Geom& g, const Tile& t) {
+  const Box b = interior(g);
+  const int j = b.j0 + t.x * BX + threadIdx.x;
+  const int k = b.k0 + t.y * BY + threadIdx.y;
+  const int l = b.l0 + t.z;
   if (j > b.j1 || k > b.k1) return;
   const typename S::vf_t* vf_d = DIR == 1 ? vfx : DIR == 2 ? vfy : vfz;
   const int j1 = j + (DIR == 1), k1 = k + (DIR == 2), l1 = l + (DIR == 3);
@@ -373,6 +431,7 @@ __global__ void __launch_bounds__(BX * BY) k_cell_update_f(Geom g, Box b, int va
   const double av = pv + L(vf_d, j, k, l) - L(vf_d, j1, k1, l1);
   E(density1, j, k, l) = st<typename S::rho_t>(pom / av);
   E(energy1, j, k, l) = st<typename S::ene_t>(poe);
+  });
 }
 
 // ---------------------------------------------------------------------------
@@ -432,17 +491,20 @@ __device__ __forceinline__ double cell_product(const Geom& g, int variant, const
 // (j, c) walks p over the sweep range carrying the previous node flux and the
 // previous plane of cell products.
 // DIR 2: p = k, c = l; DIR 3: p = l, c = k.
-template <class S, int DIR>
-__global__ void __launch_bounds__(BX * BY, 4) k_mom_node_march(Geom g, int jlo, int jhi, int clo,
-    int chi, int plo, int phi, int seg, int variant, GeomArrays ga,
+template <class S, int DIR, class M>
+__global__ void __launch_bounds__(BX * BY, 4) k_mom_node_march(M m, int variant, GeomArrays ga,
     const typename S::mf_t* __restrict__ mf, const typename S::rho_t* __restrict__ density1,
     const typename S::vf_t* __restrict__ vfx, const typename S::vf_t* __restrict__ vfy,
     const typename S::vf_t* __restrict__ vfz, typename S::wk_t* __restrict__ node_flux,
     typename S::wk_t* __restrict__ node_mass_post, typename S::wk_t* __restrict__ node_mass_pre) {
-  const int j = jlo + blockIdx.x * BX + threadIdx.x;
-  const int c = clo + blockIdx.y * BY + threadIdx.y;
+  m.run([&](const Geom& g, const Tile& t) {
+  const MarchRange r = mom_node_range<DIR>(g);
+  const int jlo = r.jlo, jhi = r.jhi, clo = r.clo, chi = r.chi, plo = r.plo, phi = r.phi;
+  const int seg = m.seg;
+  const int j = jlo + t.x * BX + threadIdx.x;
+  const int c = clo + t.y * BY + threadIdx.y;
   if (j > jhi || c > chi) return;
-  const int p0 = plo + blockIdx.z * seg;
+  const int p0 = plo + t.z * seg;
   int p1 = p0 + seg - 1;
   if (p1 > phi) p1 = phi;
   using W = typename S::wk_t;
@@ -489,6 +551,7 @@ __global__ void __launch_bounds__(BX * BY, 4) k_mom_node_march(Geom g, int jlo, 
     q_a = u_a; q_b = u_b; q_c = u_c; q_d = u_d;
   }
 #undef IDX
+  });
 }
 
 __device__ __forceinline__ double mom_limiter(double sigma, double width, double celld_dif,
@@ -528,24 +591,27 @@ __device__ __forceinline__ double mom_flux_at(double nf, double nmpre_i, double 
 
 // Velocity pass for direction y or z, marching along the sweep axis with the
 // previous momentum fluxes and the velocity window in registers.
-template <class S, int DIR>
-__global__ void __launch_bounds__(BX * BY, 3) k_mom_vel3_march(Geom g, int jlo, int jhi, int clo,
-    int chi, int plo, int phi, int seg, GeomArrays ga,
+template <class S, int DIR, class M>
+__global__ void __launch_bounds__(BX * BY, 3) k_mom_vel3_march(M m, GeomArrays ga,
     const typename S::wk_t* __restrict__ node_flux, const typename S::wk_t* __restrict__ node_mass_post,
     const typename S::wk_t* __restrict__ node_mass_pre, const typename S::vel_t* __restrict__ u_in,
     const typename S::vel_t* __restrict__ v_in, const typename S::vel_t* __restrict__ w_in,
     typename S::vel_t* __restrict__ u_out, typename S::vel_t* __restrict__ v_out,
     typename S::vel_t* __restrict__ w_out) {
-  const int j = jlo + blockIdx.x * BX + threadIdx.x;
-  const int c = clo + blockIdx.y * BY + threadIdx.y;
+  m.run([&](const Geom& g, const Tile& t) {
+  const MarchRange r = mom_vel_range<DIR>(g);
+  const int jlo = r.jlo, jhi = r.jhi, clo = r.clo, chi = r.chi, plo = r.plo, phi = r.phi;
+  const int seg = m.seg;
+  const int j = jlo + t.x * BX + threadIdx.x;
+  const int c = clo + t.y * BY + threadIdx.y;
   if (j > jhi || c > chi) return;
-  const int p0 = plo + blockIdx.z * seg;
+  const int p0 = plo + t.z * seg;
   int p1 = p0 + seg - 1;
   if (p1 > phi) p1 = phi;
 #define IDX(p) j, (DIR == 2 ? (p) : c), (DIR == 2 ? c : (p))
   const double* cd = DIR == 2 ? ga.celldy : ga.celldz;
   const int cdlo = DIR == 2 ? g.y_min : g.z_min;
-#define CD(p) cd[(p) - cdlo + 2]
+#define CD(p) cd[g.o1 + (p) - cdlo + 2]
   using V = typename S::vel_t;
   const typename S::vel_t* in[3] = {u_in, v_in, w_in};
   typename S::vel_t* out[3] = {u_out, v_out, w_out};
@@ -603,6 +669,7 @@ __global__ void __launch_bounds__(BX * BY, 3) k_mom_vel3_march(Geom g, int jlo, 
   }
 #undef CD
 #undef IDX
+  });
 }
 
 // ---------------------------------------------------------------------------
@@ -613,21 +680,23 @@ __global__ void __launch_bounds__(BX * BY, 3) k_mom_vel3_march(Geom g, int jlo, 
 // needs no dependent loads; cell p-1 is updated as soon as face p is known
 // (in place: no other thread reads this column's density or energy).
 // Faces p in [pmin, pmax+2] (c up to chi), cells p in [pmin, pmax] (c <= cmax).
-template <class S, int DIR>
-__global__ void __launch_bounds__(BX * BY, 3) k_cell_sweep_march(Geom g, int jlo, int jhi,
-    int clo, int chi, int cmax, int variant, GeomArrays ga,
+template <class S, int DIR, class M>
+__global__ void __launch_bounds__(BX * BY, 3) k_cell_sweep_march(M m, int variant, GeomArrays ga,
     typename S::rho_t* __restrict__ density1, typename S::ene_t* __restrict__ energy1,
     const typename S::vf_t* __restrict__ vfx, const typename S::vf_t* __restrict__ vfy,
     const typename S::vf_t* __restrict__ vfz, typename S::mf_t* __restrict__ mass_flux) {
-  const int j = jlo + blockIdx.x * BX + threadIdx.x;
-  const int c = clo + blockIdx.y * BY + threadIdx.y;
+  m.run([&](const Geom& g, const Tile& t) {
+  const MarchRange r = cell_sweep_range<DIR>(g);
+  const int jlo = r.jlo, jhi = r.jhi, clo = r.clo, chi = r.chi, cmax = r.cmax;
+  const int j = jlo + t.x * BX + threadIdx.x;
+  const int c = clo + t.y * BY + threadIdx.y;
   if (j > jhi || c > chi) return;
 #define IDX(p) j, (DIR == 2 ? (p) : c), (DIR == 2 ? c : (p))
   const typename S::vf_t* vf_d = DIR == 2 ? vfy : vfz;
   const int pmin = DIR == 2 ? g.y_min : g.z_min;
   const int pmax = DIR == 2 ? g.y_max : g.z_max;
   const double* vd = DIR == 2 ? ga.vertexdy : ga.vertexdz;
-#define VD(p) vd[(p) - pmin + 2]
+#define VD(p) vd[g.o1 + (p) - pmin + 2]
   const bool update = c <= cmax;
   using R = typename S::rho_t;
   using En = typename S::ene_t;
@@ -691,6 +760,7 @@ __global__ void __launch_bounds__(BX * BY, 3) k_cell_sweep_march(Geom g, int jlo
   }
 #undef VD
 #undef IDX
+  });
 }
 
 // ---------------------------------------------------------------------------
@@ -702,18 +772,20 @@ __global__ void __launch_bounds__(BX * BY, 3) k_cell_sweep_march(Geom g, int jlo
 // lanes 1..30 momentum fluxes, lanes 2..30 update (29 nodes per warp). Sums
 // and the momentum limiter keep the reference order
 // (advec_mom_kernel.f90:166-252).
-template <class S>
-__global__ void __launch_bounds__(BX * BY, 3) k_mom_sweep_x(Geom g, int seg, int variant,
+template <class S, class M>
+__global__ void __launch_bounds__(BX * BY, 3) k_mom_sweep_x(M m, int variant,
     GeomArrays ga, const typename S::mf_t* __restrict__ mfx,
     const typename S::rho_t* __restrict__ density1, const typename S::vf_t* __restrict__ vfx,
     const typename S::vf_t* __restrict__ vfy, const typename S::vf_t* __restrict__ vfz,
     const typename S::vel_t* __restrict__ u_in, const typename S::vel_t* __restrict__ v_in,
     const typename S::vel_t* __restrict__ w_in, typename S::vel_t* __restrict__ u_out,
     typename S::vel_t* __restrict__ v_out, typename S::vel_t* __restrict__ w_out) {
+  m.run([&](const Geom& g, const Tile& t) {
+  const int seg = m.seg;
   const int lane = threadIdx.x;
-  const int j = g.x_min - 2 + blockIdx.x * 29 + lane;  // node of this lane
-  const int k = g.y_min + blockIdx.y * BY + threadIdx.y;
-  const int l0 = g.z_min + blockIdx.z * seg;
+  const int j = g.x_min - 2 + t.x * 29 + lane;  // node of this lane
+  const int k = g.y_min + t.y * BY + threadIdx.y;
+  const int l0 = g.z_min + t.z * seg;
   int l1 = l0 + seg - 1;
   if (l1 > g.z_max + 1) l1 = g.z_max + 1;
   const bool row = k <= g.y_max + 1;                // every lane of a row stays for the shuffles
@@ -771,17 +843,19 @@ __global__ void __launch_bounds__(BX * BY, 3) k_mom_sweep_x(Geom g, int seg, int
     fm_a = f_a; fm_b = f_b; fm_c = f_c; fm_d = f_d;
     pm_a = p_a; pm_b = p_b;
   }
+  });
 }
 
 // Copy the halo shell of three vertex arrays (every node outside
 // [min, max+1]^3) from one buffer of a pair to the other.
-template <class T>
-__global__ void k_vert_shell_copy(Geom g, const T* __restrict__ a_in, const T* __restrict__ b_in,
+template <class T, class M>
+__global__ void k_vert_shell_copy(M m, const T* __restrict__ a_in, const T* __restrict__ b_in,
                                   const T* __restrict__ c_in, T* __restrict__ a_out,
                                   T* __restrict__ b_out, T* __restrict__ c_out) {
-  const int j = g.x_min - 2 + blockIdx.x * BX + threadIdx.x;
-  const int k = g.y_min - 2 + blockIdx.y * BY + threadIdx.y;
-  const int l = g.z_min - 2 + blockIdx.z;
+  m.run([&](const Geom& g, const Tile& t) {
+  const int j = g.x_min - 2 + t.x * BX + threadIdx.x;
+  const int k = g.y_min - 2 + t.y * BY + threadIdx.y;
+  const int l = g.z_min - 2 + t.z;
   if (j > g.x_max + 3 || k > g.y_max + 3) return;
   const bool inside = j >= g.x_min && j <= g.x_max + 1 && k >= g.y_min && k <= g.y_max + 1 &&
                       l >= g.z_min && l <= g.z_max + 1;
@@ -790,39 +864,71 @@ __global__ void k_vert_shell_copy(Geom g, const T* __restrict__ a_in, const T* _
   a_out[o] = a_in[o];
   b_out[o] = b_in[o];
   c_out[o] = c_in[o];
+  });
+}
+
+
+// ===========================================================================
+// Tile grids of the launches (aux: segment length of a marching kernel)
+constexpr int kMarchSeg = 32;
+
+dim3 grid_interior(const Geom& g, int) { return grid_of(interior(g)); }
+dim3 grid_nodes(const Geom& g, int) { return grid_of(nodes(g)); }
+dim3 grid_cell_flux_x(const Geom& g, int) { return grid_of(cell_flux_box<1>(g)); }
+template <int DIR>
+dim3 grid_cell_sweep(const Geom& g, int) {
+  const MarchRange r = cell_sweep_range<DIR>(g);
+  return dim3((r.jhi - r.jlo + 1 + BX - 1) / BX, (r.chi - r.clo + 1 + BY - 1) / BY, 1);
+}
+template <int DIR>
+dim3 grid_mom_node(const Geom& g, int seg) {
+  const MarchRange r = mom_node_range<DIR>(g);
+  return dim3((r.jhi - r.jlo + 1 + BX - 1) / BX, (r.chi - r.clo + 1 + BY - 1) / BY,
+              (r.phi - r.plo + 1 + seg - 1) / seg);
+}
+template <int DIR>
+dim3 grid_mom_vel(const Geom& g, int seg) {
+  const MarchRange r = mom_vel_range<DIR>(g);
+  return dim3((r.jhi - r.jlo + 1 + BX - 1) / BX, (r.chi - r.clo + 1 + BY - 1) / BY,
+              (r.phi - r.plo + 1 + seg - 1) / seg);
+}
+// 29 nodes per warp along x, rows of 8 along y, segments of seg planes along z
+dim3 grid_mom_sweep_x(const Geom& g, int seg) {
+  return dim3((g.x_max + 1 - g.x_min + 1 + 28) / 29, (g.y_max + 1 - g.y_min + 1 + BY - 1) / BY,
+              (g.z_max + 1 - g.z_min + 1 + seg - 1) / seg);
+}
+dim3 grid_shell(const Geom& g, int) {
+  return dim3((g.x_max - g.x_min + 6 + BX - 1) / BX, (g.y_max - g.y_min + 6 + BY - 1) / BY,
+              g.z_max - g.z_min + 6);
 }
 
 }  // namespace
 
-// ===========================================================================
-#define LAUNCH(kern, box, ...)                                                 \
-  do {                                                                         \
-    const Box _b = (box);                                                      \
-    const dim3 _gr = grid_of(_b);                                              \
-    if (_gr.x && _gr.y && _gr.z) kern<<<_gr, dim3(BX, BY), 0, s>>>(g, _b, __VA_ARGS__); \
-  } while (0)
+const dim3 kBlk(BX, BY);
 
 template <class S>
-void launch_timestep_visc(const Geom& g, cudaStream_t s, const GeomArrays& ga,
+void launch_timestep_visc(const Target& tg, cudaStream_t s, const GeomArrays& ga,
                           const typename S::rho_t* density0, const typename S::cs_t* pressure,
                           typename S::cs_t* viscosity, const typename S::vel_t* xvel0,
                           const typename S::vel_t* yvel0, const typename S::vel_t* zvel0) {
-  LAUNCH(k_timestep_visc<S>, (Box{g.x_min, g.x_max, g.y_min, g.y_max, g.z_min, g.z_max}), ga,
-         density0, pressure, viscosity, xvel0, yvel0, zvel0);
+  launch_mapped(tg, s, kKeyTimestepVisc, grid_interior, 0, false, kBlk,
+                k_timestep_visc<S, MapSingle>, k_timestep_visc<S, MapBatch>, ga, density0,
+                pressure, viscosity, xvel0, yvel0, zvel0);
 }
 
 template <class S>
-void launch_pdv_predict_eos(const Geom& g, cudaStream_t s, const double* dt_ptr,
+void launch_pdv_predict_eos(const Target& tg, cudaStream_t s, const double* dt_ptr,
                             const GeomArrays& ga, const typename S::rho_t* density0,
                             const typename S::ene_t* energy0, typename S::cs_t* pressure,
                             const typename S::cs_t* viscosity, const typename S::vel_t* xvel0,
                             const typename S::vel_t* yvel0, const typename S::vel_t* zvel0) {
-  LAUNCH(k_pdv_predict_eos<S>, (Box{g.x_min, g.x_max, g.y_min, g.y_max, g.z_min, g.z_max}),
-         dt_ptr, ga, density0, energy0, pressure, viscosity, xvel0, yvel0, zvel0);
+  launch_mapped(tg, s, kKeyPdvPredict, grid_interior, 0, false, kBlk,
+                k_pdv_predict_eos<S, MapSingle>, k_pdv_predict_eos<S, MapBatch>, dt_ptr, ga,
+                density0, energy0, pressure, viscosity, xvel0, yvel0, zvel0);
 }
 
 template <class S>
-void launch_pdv_flux(const Geom& g, cudaStream_t s, const double* dt_ptr, const GeomArrays& ga,
+void launch_pdv_flux(const Target& tg, cudaStream_t s, const double* dt_ptr, const GeomArrays& ga,
                      const typename S::rho_t* density0, typename S::rho_t* density1,
                      const typename S::ene_t* energy0, typename S::ene_t* energy1,
                      const typename S::cs_t* pressure, const typename S::cs_t* viscosity,
@@ -831,13 +937,14 @@ void launch_pdv_flux(const Geom& g, cudaStream_t s, const double* dt_ptr, const 
                      const typename S::vel_t* zvel0, const typename S::vel_t* zvel1,
                      typename S::vf_t* vol_flux_x, typename S::vf_t* vol_flux_y,
                      typename S::vf_t* vol_flux_z) {
-  LAUNCH(k_pdv_flux<S>, (Box{g.x_min, g.x_max + 1, g.y_min, g.y_max + 1, g.z_min, g.z_max + 1}),
-         dt_ptr, ga, density0, density1, energy0, energy1, pressure, viscosity, xvel0, xvel1,
-         yvel0, yvel1, zvel0, zvel1, vol_flux_x, vol_flux_y, vol_flux_z);
+  launch_mapped(tg, s, kKeyPdvFlux, grid_nodes, 0, false, kBlk, k_pdv_flux<S, MapSingle>,
+                k_pdv_flux<S, MapBatch>, dt_ptr, ga, density0, density1, energy0, energy1,
+                pressure, viscosity, xvel0, xvel1, yvel0, yvel1, zvel0, zvel1, vol_flux_x,
+                vol_flux_y, vol_flux_z);
 }
 
 template <class S>
-void launch_advec_cell_fused(const Geom& g, cudaStream_t s, int advect_x, int dir, int sweep,
+void launch_advec_cell_fused(const Target& tg, cudaStream_t s, int advect_x, int dir, int sweep,
                              const GeomArrays& ga, typename S::rho_t* density1,
                              typename S::ene_t* energy1, typename S::mf_t* mass_flux_x,
                              const typename S::vf_t* vol_flux_x, typename S::mf_t* mass_flux_y,
@@ -847,31 +954,28 @@ void launch_advec_cell_fused(const Geom& g, cudaStream_t s, int advect_x, int di
   if (dir == 1) variant = sweep == 1 ? 0 : 1;
   else if (dir == 2) variant = advect_x ? 2 : 3;
   else variant = sweep == 1 ? 4 : 5;
-  const Box in{g.x_min, g.x_max, g.y_min, g.y_max, g.z_min, g.z_max};
   if (dir == 1) {
-    LAUNCH((k_cell_flux_f<S, 1>), (Box{g.x_min, g.x_max + 2, g.y_min, g.y_max, g.z_min, g.z_max}),
-           variant, ga, density1, energy1, vol_flux_x, vol_flux_y, vol_flux_z, mass_flux_x, ener_flux);
-    LAUNCH((k_cell_update_f<S, 1>), in, variant, ga, density1, energy1, vol_flux_x, vol_flux_y,
-           vol_flux_z, mass_flux_x, ener_flux);
+    // face pass, then the update pass
+    launch_mapped(tg, s, kKeyCellFluxX, grid_cell_flux_x, 0, false, kBlk,
+                  k_cell_flux_f<S, 1, MapSingle>, k_cell_flux_f<S, 1, MapBatch>, variant, ga,
+                  density1, energy1, vol_flux_x, vol_flux_y, vol_flux_z, mass_flux_x, ener_flux);
+    launch_mapped(tg, s, kKeyCellUpdateX, grid_interior, 0, false, kBlk,
+                  k_cell_update_f<S, 1, MapSingle>, k_cell_update_f<S, 1, MapBatch>, variant, ga,
+                  density1, energy1, vol_flux_x, vol_flux_y, vol_flux_z, mass_flux_x, ener_flux);
   } else if (dir == 2) {
-    // one pass; faces run over l up to z_max+2, cells update for l <= z_max
-    const int clo = g.z_min, chi = g.z_max + 2;
-    const dim3 gr((g.x_max - g.x_min + 1 + BX - 1) / BX, (chi - clo + 1 + BY - 1) / BY, 1);
-    k_cell_sweep_march<S, 2><<<gr, dim3(BX, BY), 0, s>>>(g, g.x_min, g.x_max, clo, chi, g.z_max,
-        variant, ga, density1, energy1, vol_flux_x, vol_flux_y, vol_flux_z, mass_flux_y);
+    // one marching pass, in place
+    launch_mapped(tg, s, kKeyCellSweep | 2u, grid_cell_sweep<2>, 0, false, kBlk,
+                  k_cell_sweep_march<S, 2, MapSingle>, k_cell_sweep_march<S, 2, MapBatch>,
+                  variant, ga, density1, energy1, vol_flux_x, vol_flux_y, vol_flux_z, mass_flux_y);
   } else {
-    const int clo = g.y_min, chi = g.y_max;
-    const dim3 gr((g.x_max - g.x_min + 1 + BX - 1) / BX, (chi - clo + 1 + BY - 1) / BY, 1);
-    k_cell_sweep_march<S, 3><<<gr, dim3(BX, BY), 0, s>>>(g, g.x_min, g.x_max, clo, chi, g.y_max,
-        variant, ga, density1, energy1, vol_flux_x, vol_flux_y, vol_flux_z, mass_flux_z);
+    launch_mapped(tg, s, kKeyCellSweep | 3u, grid_cell_sweep<3>, 0, false, kBlk,
+                  k_cell_sweep_march<S, 3, MapSingle>, k_cell_sweep_march<S, 3, MapBatch>,
+                  variant, ga, density1, energy1, vol_flux_x, vol_flux_y, vol_flux_z, mass_flux_z);
   }
-  (void)in;
 }
 
-constexpr int kMarchSeg = 32;
-
 template <class S>
-void launch_advec_mom_fused(const Geom& g, cudaStream_t s, int advect_x, int sweep, int dir,
+void launch_advec_mom_fused(const Target& tg, cudaStream_t s, int advect_x, int sweep, int dir,
                             double vol, const GeomArrays& ga, const typename S::rho_t* density1,
                             const typename S::mf_t* mass_flux_x, const typename S::mf_t* mass_flux_y,
                             const typename S::mf_t* mass_flux_z, const typename S::vf_t* vol_flux_x,
@@ -885,67 +989,59 @@ void launch_advec_mom_fused(const Geom& g, cudaStream_t s, int advect_x, int swe
   else if (sweep == 2 && advect_x) variant = 2;
   else if (sweep == 2) variant = 3;
   else variant = 4;  // sweep 3: post_vol = volume
-  const int x0 = g.x_min, x1 = g.x_max, y0 = g.y_min, y1 = g.y_max, z0 = g.z_min, z1 = g.z_max;
+  (void)vol;
   if (dir == 1) {
-    // one pass: 29 nodes per warp along x, segments of kMarchSeg planes along z
-    const int nseg = (z1 + 1 - z0 + 1 + kMarchSeg - 1) / kMarchSeg;
-    const dim3 gx((x1 + 1 - x0 + 1 + 28) / 29, (y1 + 1 - y0 + 1 + BY - 1) / BY, nseg);
-    k_mom_sweep_x<S><<<gx, dim3(BX, BY), 0, s>>>(g, kMarchSeg, variant, ga, mass_flux_x, density1,
-        vol_flux_x, vol_flux_y, vol_flux_z, vel_in[0], vel_in[1], vel_in[2], vel_out[0],
-        vel_out[1], vel_out[2]);
+    // one pass for the three velocities
+    launch_mapped(tg, s, kKeyMomSweepX, grid_mom_sweep_x, kMarchSeg, true, kBlk,
+                  k_mom_sweep_x<S, MapSingle>, k_mom_sweep_x<S, MapBatch>, variant, ga,
+                  mass_flux_x, density1, vol_flux_x, vol_flux_y, vol_flux_z, vel_in[0],
+                  vel_in[1], vel_in[2], vel_out[0], vel_out[1], vel_out[2]);
+  } else if (dir == 2) {
+    // node pass then velocity pass, each marching along y in segments
+    launch_mapped(tg, s, kKeyMomNode | 2u, grid_mom_node<2>, kMarchSeg, true, kBlk,
+                  k_mom_node_march<S, 2, MapSingle>, k_mom_node_march<S, 2, MapBatch>, variant,
+                  ga, mass_flux_y, density1, vol_flux_x, vol_flux_y, vol_flux_z, node_flux,
+                  node_mass_post, node_mass_pre);
+    launch_mapped(tg, s, kKeyMomVel3 | 2u, grid_mom_vel<2>, kMarchSeg, true, kBlk,
+                  k_mom_vel3_march<S, 2, MapSingle>, k_mom_vel3_march<S, 2, MapBatch>, ga,
+                  node_flux, node_mass_post, node_mass_pre, vel_in[0], vel_in[1], vel_in[2],
+                  vel_out[0], vel_out[1], vel_out[2]);
   } else {
-    // node pass then velocity pass, each marching along the sweep axis in
-    // segments: node flux from min-2, node masses from min-1, updates min..max+1
-    const int plo = (dir == 2 ? y0 : z0) - 2, phi = (dir == 2 ? y1 : z1) + 2;
-    const int clo = dir == 2 ? z0 : y0, chi = (dir == 2 ? z1 : y1) + 1;
-    const int nseg = (phi - plo + 1 + kMarchSeg - 1) / kMarchSeg;
-    const dim3 gr((x1 + 1 - x0 + 1 + BX - 1) / BX, (chi - clo + 1 + BY - 1) / BY, nseg);
-    const int ulo = (dir == 2 ? y0 : z0), uhi = (dir == 2 ? y1 : z1) + 1;
-    const int useg = (uhi - ulo + 1 + kMarchSeg - 1) / kMarchSeg;
-    const dim3 gv((x1 + 1 - x0 + 1 + BX - 1) / BX, (chi - clo + 1 + BY - 1) / BY, useg);
-    if (dir == 2) {
-      k_mom_node_march<S, 2><<<gr, dim3(BX, BY), 0, s>>>(g, x0, x1 + 1, clo, chi, plo, phi, kMarchSeg,
-          variant, ga, mass_flux_y, density1, vol_flux_x, vol_flux_y, vol_flux_z, node_flux,
-          node_mass_post, node_mass_pre);
-      k_mom_vel3_march<S, 2><<<gv, dim3(BX, BY), 0, s>>>(g, x0, x1 + 1, clo, chi, ulo, uhi, kMarchSeg,
-          ga, node_flux, node_mass_post, node_mass_pre, vel_in[0], vel_in[1], vel_in[2],
-          vel_out[0], vel_out[1], vel_out[2]);
-    } else {
-      k_mom_node_march<S, 3><<<gr, dim3(BX, BY), 0, s>>>(g, x0, x1 + 1, clo, chi, plo, phi, kMarchSeg,
-          variant, ga, mass_flux_z, density1, vol_flux_x, vol_flux_y, vol_flux_z, node_flux,
-          node_mass_post, node_mass_pre);
-      k_mom_vel3_march<S, 3><<<gv, dim3(BX, BY), 0, s>>>(g, x0, x1 + 1, clo, chi, ulo, uhi, kMarchSeg,
-          ga, node_flux, node_mass_post, node_mass_pre, vel_in[0], vel_in[1], vel_in[2],
-          vel_out[0], vel_out[1], vel_out[2]);
-    }
-    (void)vol;
+    launch_mapped(tg, s, kKeyMomNode | 3u, grid_mom_node<3>, kMarchSeg, true, kBlk,
+                  k_mom_node_march<S, 3, MapSingle>, k_mom_node_march<S, 3, MapBatch>, variant,
+                  ga, mass_flux_z, density1, vol_flux_x, vol_flux_y, vol_flux_z, node_flux,
+                  node_mass_post, node_mass_pre);
+    launch_mapped(tg, s, kKeyMomVel3 | 3u, grid_mom_vel<3>, kMarchSeg, true, kBlk,
+                  k_mom_vel3_march<S, 3, MapSingle>, k_mom_vel3_march<S, 3, MapBatch>, ga,
+                  node_flux, node_mass_post, node_mass_pre, vel_in[0], vel_in[1], vel_in[2],
+                  vel_out[0], vel_out[1], vel_out[2]);
   }
   // the updated buffers take the halo shell of the inputs
-  const dim3 gs((g.x_max - g.x_min + 6 + BX - 1) / BX, (g.y_max - g.y_min + 6 + BY - 1) / BY,
-                g.z_max - g.z_min + 6);
-  k_vert_shell_copy<typename S::vel_t><<<gs, dim3(BX, BY), 0, s>>>(
-      g, vel_in[0], vel_in[1], vel_in[2], vel_out[0], vel_out[1], vel_out[2]);
+  using V = typename S::vel_t;
+  launch_mapped(tg, s, kKeyShellCopy, grid_shell, 0, false, kBlk, k_vert_shell_copy<V, MapSingle>,
+                k_vert_shell_copy<V, MapBatch>, vel_in[0], vel_in[1], vel_in[2], vel_out[0],
+                vel_out[1], vel_out[2]);
 }
 
 #define INSTF(S)                                                                               \
-  template void launch_timestep_visc<S>(const Geom&, cudaStream_t, const GeomArrays&,          \
+  template void launch_timestep_visc<S>(const Target&, cudaStream_t, const GeomArrays&,          \
                                         const S::rho_t*, const S::cs_t*, S::cs_t*,             \
                                         const S::vel_t*, const S::vel_t*, const S::vel_t*);    \
-  template void launch_pdv_predict_eos<S>(const Geom&, cudaStream_t, const double*,            \
+  template void launch_pdv_predict_eos<S>(const Target&, cudaStream_t, const double*,            \
                                           const GeomArrays&, const S::rho_t*, const S::ene_t*, \
                                           S::cs_t*, const S::cs_t*, const S::vel_t*,           \
                                           const S::vel_t*, const S::vel_t*);                   \
-  template void launch_pdv_flux<S>(const Geom&, cudaStream_t, const double*, const GeomArrays&, \
+  template void launch_pdv_flux<S>(const Target&, cudaStream_t, const double*, const GeomArrays&, \
                                    const S::rho_t*, S::rho_t*, const S::ene_t*, S::ene_t*,     \
                                    const S::cs_t*, const S::cs_t*, const S::vel_t*,            \
                                    const S::vel_t*, const S::vel_t*, const S::vel_t*,          \
                                    const S::vel_t*, const S::vel_t*, S::vf_t*, S::vf_t*,       \
                                    S::vf_t*);                                                  \
-  template void launch_advec_cell_fused<S>(const Geom&, cudaStream_t, int, int, int,           \
+  template void launch_advec_cell_fused<S>(const Target&, cudaStream_t, int, int, int,           \
                                            const GeomArrays&, S::rho_t*, S::ene_t*, S::mf_t*,  \
                                            const S::vf_t*, S::mf_t*, const S::vf_t*, S::mf_t*, \
                                            const S::vf_t*, S::wk_t*);                          \
-  template void launch_advec_mom_fused<S>(const Geom&, cudaStream_t, int, int, int, double,    \
+  template void launch_advec_mom_fused<S>(const Target&, cudaStream_t, int, int, int, double,    \
                                           const GeomArrays&, const S::rho_t*, const S::mf_t*,  \
                                           const S::mf_t*, const S::mf_t*, const S::vf_t*,      \
                                           const S::vf_t*, const S::vf_t*, S::wk_t*, S::wk_t*,  \

@@ -32,17 +32,37 @@ inline dim3 grid_of(const Box& b) {
 
 inline bool launchable(const dim3& gr) { return gr.x > 0 && gr.y > 0 && gr.z > 0; }
 
+__host__ __device__ inline Box interior(const Geom& g) {
+  return Box{g.x_min, g.x_max, g.y_min, g.y_max, g.z_min, g.z_max};
+}
+__host__ __device__ inline Box nodes(const Geom& g) {
+  return Box{g.x_min, g.x_max + 1, g.y_min, g.y_max + 1, g.z_min, g.z_max + 1};
+}
+__host__ __device__ inline Box halo2(const Geom& g) {
+  return Box{g.x_min - 2, g.x_max + 2, g.y_min - 2, g.y_max + 2, g.z_min - 2, g.z_max + 2};
+}
+inline dim3 grid_interior(const Geom& g, int) { return grid_of(interior(g)); }
+inline dim3 grid_nodes(const Geom& g, int) { return grid_of(nodes(g)); }
+
 #define BOX_THREAD(b)                                    \
   const int j = (b).j0 + blockIdx.x * BX + threadIdx.x;  \
   const int k = (b).k0 + blockIdx.y * BY + threadIdx.y;  \
   const int l = (b).l0 + blockIdx.z;                     \
   if (j > (b).j1 || k > (b).k1) return
 
+// the same for tile t of a mapped kernel (clover_sched.cuh)
+#define TILE_THREAD(box, t)                            \
+  const Box b = (box);                                 \
+  const int j = b.j0 + (t).x * BX + threadIdx.x;       \
+  const int k = b.k0 + (t).y * BY + threadIdx.y;       \
+  const int l = b.l0 + (t).z;                          \
+  if (j > b.j1 || k > b.k1) return
+
 // 3D element, 1D coordinate arrays
 #define E(a, jj, kk, ll) (a)[off3(g, (jj), (kk), (ll))]
-#define GX(a, jj) (a)[(jj) - g.x_min + 2]
-#define GY(a, kk) (a)[(kk) - g.y_min + 2]
-#define GZ(a, ll) (a)[(ll) - g.z_min + 2]
+#define GX(a, jj) (a)[g.o1 + (jj) - g.x_min + 2]
+#define GY(a, kk) (a)[g.o1 + (kk) - g.y_min + 2]
+#define GZ(a, ll) (a)[g.o1 + (ll) - g.z_min + 2]
 
 __device__ __forceinline__ double ld(const double* p) { return __ldg(p); }
 __device__ __forceinline__ double ld(const float* p) { return (double)__ldg(p); }
@@ -58,11 +78,12 @@ __device__ __forceinline__ double dt_of(double v, const double* p) { return p ? 
 
 // ---------------------------------------------------------------------------
 // ideal_gas_kernel.f90:47-58
-template <class S>
-__global__ void __launch_bounds__(BX * BY) k_ideal_gas(Geom g, Box b,
+template <class S, class M>
+__global__ void __launch_bounds__(BX * BY) k_ideal_gas(M m,
     const typename S::rho_t* __restrict__ density, const typename S::ene_t* __restrict__ energy,
     typename S::cs_t* __restrict__ pressure, typename S::cs_t* __restrict__ soundspeed) {
-  BOX_THREAD(b);
+  m.run([&](const Geom& g, const Tile& t) {
+  TILE_THREAD(interior(g), t);
   const double d = L(density, j, k, l);
   const double v = 1.0 / d;
   const double p = (1.4 - 1.0) * d * L(energy, j, k, l);
@@ -72,6 +93,7 @@ __global__ void __launch_bounds__(BX * BY) k_ideal_gas(Geom g, Box b,
   using C = typename S::cs_t;
   E(pressure, j, k, l) = st<C>(p);
   E(soundspeed, j, k, l) = st<C>(sqrt(ss2));
+  });
 }
 
 // ---------------------------------------------------------------------------
@@ -171,17 +193,20 @@ __host__ __device__ __forceinline__ unsigned long long key_of(double v) {
   return (b >> 63) ? ~b : (b | 0x8000000000000000ull);
 }
 
-template <class S>
-__global__ void __launch_bounds__(BX * BY) k_calc_dt(Geom g, Box b, GeomArrays ga,
+template <class S, class M>
+__global__ void __launch_bounds__(BX * BY) k_calc_dt(M m, GeomArrays ga,
     double g_small, double dtc_safe, double dtu_safe, double dtv_safe, double dtw_safe,
     double dtdiv_safe, const typename S::rho_t* __restrict__ density0,
     const typename S::cs_t* __restrict__ viscosity_a, const typename S::cs_t* __restrict__ soundspeed,
     const typename S::vel_t* __restrict__ xvel0, const typename S::vel_t* __restrict__ yvel0,
     const typename S::vel_t* __restrict__ zvel0, typename S::wk_t* __restrict__ dt_min,
     unsigned long long* __restrict__ min_key) {
-  const int j = b.j0 + blockIdx.x * BX + threadIdx.x;
-  const int k = b.k0 + blockIdx.y * BY + threadIdx.y;
-  const int l = b.l0 + blockIdx.z;
+  __shared__ unsigned long long wmin[BX * BY / 32];
+  m.run([&](const Geom& g, const Tile& t) {
+  const Box b = interior(g);
+  const int j = b.j0 + t.x * BX + threadIdx.x;
+  const int k = b.k0 + t.y * BY + threadIdx.y;
+  const int l = b.l0 + t.z;
   unsigned long long key = ~0ull;
   if (j <= b.j1 && k <= b.k1) {
     const double m = fmin2(fmin2(GX(ga.celldx, j), GY(ga.celldy, k)), GZ(ga.celldz, l));
@@ -227,7 +252,6 @@ __global__ void __launch_bounds__(BX * BY) k_calc_dt(Geom g, Box b, GeomArrays g
     unsigned long long other = __shfl_xor_sync(0xffffffffu, key, o);
     key = other < key ? other : key;
   }
-  __shared__ unsigned long long wmin[BX * BY / 32];
   const int lane = threadIdx.x, warp = threadIdx.y;
   if (lane == 0) wmin[warp] = key;
   __syncthreads();
@@ -238,8 +262,9 @@ __global__ void __launch_bounds__(BX * BY) k_calc_dt(Geom g, Box b, GeomArrays g
       unsigned long long other = __shfl_xor_sync(0xffffffffu, key, o);
       key = other < key ? other : key;
     }
-    if (lane == 0 && key != ~0ull) atomicMin(min_key, key);
+    if (lane == 0 && key != ~0ull) atomicMin(min_key + (long long)t.d * kScalarStride, key);
   }
+  });
 }
 
 // ---------------------------------------------------------------------------
@@ -314,15 +339,16 @@ __global__ void __launch_bounds__(BX * BY) k_revert(Geom g, Box b,
 
 // ---------------------------------------------------------------------------
 // accelerate_kernel.f90:61-109
-template <class S>
-__global__ void __launch_bounds__(BX * BY) k_accelerate(Geom g, Box b, double dt_val,
+template <class S, class M>
+__global__ void __launch_bounds__(BX * BY) k_accelerate(M m, double dt_val,
     const double* dt_ptr, GeomArrays ga, const typename S::rho_t* __restrict__ density0,
     const typename S::cs_t* __restrict__ pressure, const typename S::cs_t* __restrict__ viscosity,
     const typename S::vel_t* __restrict__ xvel0, const typename S::vel_t* __restrict__ yvel0,
     const typename S::vel_t* __restrict__ zvel0, typename S::vel_t* __restrict__ xvel1,
     typename S::vel_t* __restrict__ yvel1, typename S::vel_t* __restrict__ zvel1) {
-  BOX_THREAD(b);
-  const double dt = dt_of(dt_val, dt_ptr);
+  m.run([&](const Geom& g, const Tile& t) {
+  TILE_THREAD(nodes(g), t);
+  const double dt = dt_ptr ? dt_ptr[(long long)t.d * kScalarStride] : dt_val;
 #define DV(a, bb, c) (L(density0, j + (a), k + (bb), l + (c)) * E(ga.volume, j + (a), k + (bb), l + (c)))
   const double nodal_mass = (DV(-1, -1, 0) + DV(0, -1, 0) + DV(0, 0, 0) + DV(-1, 0, 0) +
                              DV(-1, -1, -1) + DV(0, -1, -1) + DV(0, 0, -1) + DV(-1, 0, -1)) * 0.125;
@@ -362,6 +388,7 @@ __global__ void __launch_bounds__(BX * BY) k_accelerate(Geom g, Box b, double dt
   E(zvel1, j, k, l) = st<V>(zvel1_s -
       stepbymass_s * (za0 * (q000 - q001) + za1 * (q010 - q011) + za2 * (q100 - q101) +
                       za3 * (q110 - q111)));
+  });
 }
 
 // ---------------------------------------------------------------------------
@@ -469,7 +496,7 @@ __global__ void __launch_bounds__(BX * BY) k_cell_flux(Geom g, Box b, GeomArrays
 #define AT(a, ii) L(a, DIR == 1 ? (ii) : j, DIR == 2 ? (ii) : k, DIR == 3 ? (ii) : l)
   const double pv_donor = AT(pre_vol, donor);
   const double sigmat = fabs(vf) / pv_donor;
-  const double sigma3 = (1.0 + sigmat) * (vd[i - vlo + 2] / vd[dif - vlo + 2]);
+  const double sigma3 = (1.0 + sigmat) * (vd[g.o1 + i - vlo + 2] / vd[g.o1 + dif - vlo + 2]);
   const double sigma4 = 2.0 - sigmat;
   const double sigmav = sigmat;
 
@@ -641,11 +668,11 @@ __global__ void __launch_bounds__(BX * BY) k_mom_flux(Geom g, Box b, GeomArrays 
   const double sigma = fabs(nf) / AT(node_mass_pre, donor);
   const double* cd = DIR == 1 ? ga.celldx : DIR == 2 ? ga.celldy : ga.celldz;
   const int clo = DIR == 1 ? g.x_min : DIR == 2 ? g.y_min : g.z_min;
-  const double width = cd[i - clo + 2];
+  const double width = cd[g.o1 + i - clo + 2];
   const double v_donor = AT(vel1, donor);
   const double vdiffuw = v_donor - AT(vel1, upwind);
   const double vdiffdw = AT(vel1, downwind) - v_donor;
-  const double limiter = mom_limiter(sigma, width, cd[dif - clo + 2], vdiffuw, vdiffdw);
+  const double limiter = mom_limiter(sigma, width, cd[g.o1 + dif - clo + 2], vdiffuw, vdiffdw);
   const double advec_vel_s = v_donor + (1.0 - sigma) * limiter;
   E(mom_flux, j, k, l) = st<typename S::wk_t>(advec_vel_s * nf);
 #undef AT
@@ -667,14 +694,15 @@ __global__ void __launch_bounds__(BX * BY) k_mom_update(Geom g, Box b,
 // ---------------------------------------------------------------------------
 // reset_field_kernel.f90:51-98 (cell part over the interior, vertex part over
 // the interior nodes; one launch over the node box)
-template <class S>
-__global__ void __launch_bounds__(BX * BY) k_reset(Geom g, Box b,
+template <class S, class M>
+__global__ void __launch_bounds__(BX * BY) k_reset(M m,
     typename S::rho_t* __restrict__ density0, const typename S::rho_t* __restrict__ density1,
     typename S::ene_t* __restrict__ energy0, const typename S::ene_t* __restrict__ energy1,
     typename S::vel_t* __restrict__ xvel0, const typename S::vel_t* __restrict__ xvel1,
     typename S::vel_t* __restrict__ yvel0, const typename S::vel_t* __restrict__ yvel1,
     typename S::vel_t* __restrict__ zvel0, const typename S::vel_t* __restrict__ zvel1) {
-  BOX_THREAD(b);
+  m.run([&](const Geom& g, const Tile& t) {
+  TILE_THREAD(nodes(g), t);
   if (j <= g.x_max && k <= g.y_max && l <= g.z_max) {
     E(density0, j, k, l) = E(density1, j, k, l);
     E(energy0, j, k, l) = E(energy1, j, k, l);
@@ -682,6 +710,7 @@ __global__ void __launch_bounds__(BX * BY) k_reset(Geom g, Box b,
   E(xvel0, j, k, l) = E(xvel1, j, k, l);
   E(yvel0, j, k, l) = E(yvel1, j, k, l);
   E(zvel0, j, k, l) = E(zvel1, j, k, l);
+  });
 }
 
 // ---------------------------------------------------------------------------
@@ -704,6 +733,29 @@ __device__ __forceinline__ void block_sum5(double v[5], double* sh /*5*SUM_THREA
   for (int q = 0; q < 5; q++) v[q] = sh[q * SUM_THREADS];
 }
 
+// field_summary_kernel.f90:60-75 for cell (j,k,l), added to acc[5]
+template <class S>
+__device__ __forceinline__ void summary_cell(const Geom& g, int j, int k, int l,
+    const double* __restrict__ volume, const typename S::rho_t* __restrict__ density0,
+    const typename S::ene_t* __restrict__ energy0, const typename S::cs_t* __restrict__ pressure,
+    const typename S::vel_t* __restrict__ xvel0, const typename S::vel_t* __restrict__ yvel0,
+    const typename S::vel_t* __restrict__ zvel0, double acc[5]) {
+  double vsqrd = 0.0;
+  for (int lv = l; lv <= l + 1; lv++)
+    for (int kv = k; kv <= k + 1; kv++)
+      for (int jv = j; jv <= j + 1; jv++) {
+        const double u = L(xvel0, jv, kv, lv), v = L(yvel0, jv, kv, lv), w = L(zvel0, jv, kv, lv);
+        vsqrd = vsqrd + 0.125 * (u * u + v * v + w * w);
+      }
+  const double cell_vol = E(volume, j, k, l);
+  const double cell_mass = cell_vol * L(density0, j, k, l);
+  acc[0] = acc[0] + cell_vol;
+  acc[1] = acc[1] + cell_mass;
+  acc[2] = acc[2] + cell_mass * L(energy0, j, k, l);
+  acc[3] = acc[3] + cell_mass * 0.5 * vsqrd;
+  acc[4] = acc[4] + cell_vol * L(pressure, j, k, l);
+}
+
 template <class S>
 __global__ void __launch_bounds__(SUM_THREADS) k_summary(Geom g, const double* __restrict__ volume,
     const typename S::rho_t* __restrict__ density0, const typename S::ene_t* __restrict__ energy0,
@@ -720,20 +772,7 @@ __global__ void __launch_bounds__(SUM_THREADS) k_summary(Geom g, const double* _
     const long long r = c / nx;
     const int k = g.y_min + (int)(r % ny);
     const int l = g.z_min + (int)(r / ny);
-    double vsqrd = 0.0;
-    for (int lv = l; lv <= l + 1; lv++)
-      for (int kv = k; kv <= k + 1; kv++)
-        for (int jv = j; jv <= j + 1; jv++) {
-          const double u = L(xvel0, jv, kv, lv), v = L(yvel0, jv, kv, lv), w = L(zvel0, jv, kv, lv);
-          vsqrd = vsqrd + 0.125 * (u * u + v * v + w * w);
-        }
-    const double cell_vol = E(volume, j, k, l);
-    const double cell_mass = cell_vol * L(density0, j, k, l);
-    acc[0] = acc[0] + cell_vol;
-    acc[1] = acc[1] + cell_mass;
-    acc[2] = acc[2] + cell_mass * L(energy0, j, k, l);
-    acc[3] = acc[3] + cell_mass * 0.5 * vsqrd;
-    acc[4] = acc[4] + cell_vol * L(pressure, j, k, l);
+    summary_cell<S>(g, j, k, l, volume, density0, energy0, pressure, xvel0, yvel0, zvel0, acc);
   }
   block_sum5(acc, sh);
   if (threadIdx.x == 0)
@@ -749,6 +788,45 @@ __global__ void __launch_bounds__(SUM_THREADS) k_summary_final(const double* __r
   block_sum5(acc, sh);
   if (threadIdx.x == 0)
     for (int q = 0; q < 5; q++) out5[q] = acc[q];
+}
+
+// Per-deck summaries of an ensemble: tile z = one z plane of one deck, its
+// cells strided over the block in a fixed order and tree-reduced.
+template <class S, class M>
+__global__ void __launch_bounds__(SUM_THREADS) k_summary_plane(M m,
+    const int* __restrict__ plane_base, const double* __restrict__ volume,
+    const typename S::rho_t* __restrict__ density0, const typename S::ene_t* __restrict__ energy0,
+    const typename S::cs_t* __restrict__ pressure, const typename S::vel_t* __restrict__ xvel0,
+    const typename S::vel_t* __restrict__ yvel0, const typename S::vel_t* __restrict__ zvel0,
+    double* __restrict__ partials) {
+  __shared__ double sh[5 * SUM_THREADS];
+  m.run([&](const Geom& g, const Tile& t) {
+    const int nx = g.x_max - g.x_min + 1, ny = g.y_max - g.y_min + 1;
+    const int l = g.z_min + t.z;
+    double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    for (int c = threadIdx.x; c < nx * ny; c += SUM_THREADS)
+      summary_cell<S>(g, g.x_min + c % nx, g.y_min + c / nx, l, volume, density0, energy0,
+                      pressure, xvel0, yvel0, zvel0, acc);
+    block_sum5(acc, sh);
+    if (threadIdx.x == 0) {
+      double* o = partials + 5 * ((long long)plane_base[t.d] + t.z);
+      for (int q = 0; q < 5; q++) o[q] = acc[q];
+    }
+  });
+}
+
+// One block per deck: its plane partials added in plane order.
+__global__ void __launch_bounds__(SUM_THREADS) k_summary_decks(const int* __restrict__ plane_base,
+    const double* __restrict__ partials, double* __restrict__ out) {
+  __shared__ double sh[5 * SUM_THREADS];
+  const int d = blockIdx.x;
+  const int p0 = plane_base[d], p1 = plane_base[d + 1];
+  double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+  for (int i = p0 + (int)threadIdx.x; i < p1; i += SUM_THREADS)
+    for (int q = 0; q < 5; q++) acc[q] = acc[q] + partials[i * 5 + q];
+  block_sum5(acc, sh);
+  if (threadIdx.x == 0)
+    for (int q = 0; q < 5; q++) out[d * 5 + q] = acc[q];
 }
 
 // ---------------------------------------------------------------------------
@@ -796,15 +874,16 @@ struct HaloLaunch {
   int ids[19];
 };
 
-template <int AX>
-__global__ void k_halo(Geom g, HaloLaunch h, int depth, int do_low, int do_high) {
+template <int AX, class M>
+__global__ void k_halo(M m, HaloLaunch h, int depth, int do_low, int do_high) {
+  m.run([&](const Geom& g, const Tile& t) {
   // tangential axes: y faces (j,l), x faces (k,l), z faces (j,k)
   const int ta = AX == 0 ? 1 : 0;  // first tangential axis
   const int tb = AX == 2 ? 1 : 2;  // second tangential axis
   const int mins[3] = {g.x_min, g.y_min, g.z_min};
   const int maxs[3] = {g.x_max, g.y_max, g.z_max};
-  const int a = mins[ta] - depth + blockIdx.x * blockDim.x + threadIdx.x;
-  const int bb = mins[tb] - depth + blockIdx.y * blockDim.y + threadIdx.y;
+  const int a = mins[ta] - depth + t.x * blockDim.x + threadIdx.x;
+  const int bb = mins[tb] - depth + t.y * blockDim.y + threadIdx.y;
   if (a > maxs[ta] + 1 + depth || bb > maxs[tb] + 1 + depth) return;
   const int n = maxs[AX];
   for (int fi = 0; fi < h.nfields; fi++) {
@@ -833,6 +912,17 @@ __global__ void k_halo(Geom g, HaloLaunch h, int depth, int do_low, int do_high)
     }
     (void)id;
   }
+  });
+}
+
+// tile grid of the halo update of the faces normal to AX (32 x 8 tiles over
+// the two tangential axes, each extended by depth)
+template <int AX>
+dim3 grid_halo(const Geom& g, int depth) {
+  const int mins[3] = {g.x_min, g.y_min, g.z_min}, maxs[3] = {g.x_max, g.y_max, g.z_max};
+  const int ta = AX == 0 ? 1 : 0, tb = AX == 2 ? 1 : 2;
+  const int na = maxs[ta] - mins[ta] + 2 + 2 * depth, nb = maxs[tb] - mins[tb] + 2 + 2 * depth;
+  return dim3((na + 31) / 32, (nb + 7) / 8, 1);
 }
 
 // ---------------------------------------------------------------------------
@@ -927,15 +1017,6 @@ __global__ void k_fill(T* p, long long n, T v) {
     if (launchable(_gr)) kern<<<_gr, dim3(BX, BY), 0, s>>>(g, _b, __VA_ARGS__); \
   } while (0)
 
-static inline Box interior(const Geom& g) {
-  return Box{g.x_min, g.x_max, g.y_min, g.y_max, g.z_min, g.z_max};
-}
-static inline Box nodes(const Geom& g) {
-  return Box{g.x_min, g.x_max + 1, g.y_min, g.y_max + 1, g.z_min, g.z_max + 1};
-}
-static inline Box halo2(const Geom& g) {
-  return Box{g.x_min - 2, g.x_max + 2, g.y_min - 2, g.y_max + 2, g.z_min - 2, g.z_max + 2};
-}
 
 unsigned long long min_key_of(double v) { return key_of(v); }
 double min_key_value(unsigned long long key) {
@@ -946,10 +1027,12 @@ double min_key_value(unsigned long long key) {
 }
 
 template <class S>
-void launch_ideal_gas(const Geom& g, cudaStream_t s, const typename S::rho_t* density,
+void launch_ideal_gas(const Target& tg, cudaStream_t s, const typename S::rho_t* density,
                       const typename S::ene_t* energy, typename S::cs_t* pressure,
                       typename S::cs_t* soundspeed) {
-  LAUNCH(k_ideal_gas<S>, interior(g), density, energy, pressure, soundspeed);
+  launch_mapped(tg, s, kKeyIdealGas, grid_interior, 0, false, dim3(BX, BY),
+                k_ideal_gas<S, MapSingle>, k_ideal_gas<S, MapBatch>, density, energy, pressure,
+                soundspeed);
 }
 
 template <class S>
@@ -961,15 +1044,17 @@ void launch_viscosity(const Geom& g, cudaStream_t s, const GeomArrays& ga,
 }
 
 template <class S>
-void launch_calc_dt(const Geom& g, cudaStream_t s, const GeomArrays& ga, double g_small,
+void launch_calc_dt(const Target& tg, cudaStream_t s, const GeomArrays& ga, double g_small,
                     double dtc_safe, double dtu_safe, double dtv_safe, double dtw_safe,
                     double dtdiv_safe, const typename S::rho_t* density0,
                     const typename S::cs_t* viscosity, const typename S::cs_t* soundspeed,
                     const typename S::vel_t* xvel0, const typename S::vel_t* yvel0,
                     const typename S::vel_t* zvel0, typename S::wk_t* dt_min_arr,
                     unsigned long long* min_key) {
-  LAUNCH(k_calc_dt<S>, interior(g), ga, g_small, dtc_safe, dtu_safe, dtv_safe, dtw_safe,
-         dtdiv_safe, density0, viscosity, soundspeed, xvel0, yvel0, zvel0, dt_min_arr, min_key);
+  launch_mapped(tg, s, kKeyCalcDt, grid_interior, 0, false, dim3(BX, BY), k_calc_dt<S, MapSingle>,
+                k_calc_dt<S, MapBatch>, ga, g_small, dtc_safe, dtu_safe, dtv_safe, dtw_safe,
+                dtdiv_safe, density0, viscosity, soundspeed, xvel0, yvel0, zvel0, dt_min_arr,
+                min_key);
 }
 
 template <class S>
@@ -993,14 +1078,15 @@ void launch_revert(const Geom& g, cudaStream_t s, const typename S::rho_t* densi
 }
 
 template <class S>
-void launch_accelerate(const Geom& g, cudaStream_t s, double dt_val, const double* dt_ptr,
+void launch_accelerate(const Target& tg, cudaStream_t s, double dt_val, const double* dt_ptr,
                        const GeomArrays& ga, const typename S::rho_t* density0,
                        const typename S::cs_t* pressure, const typename S::cs_t* viscosity,
                        const typename S::vel_t* xvel0, const typename S::vel_t* yvel0,
                        const typename S::vel_t* zvel0, typename S::vel_t* xvel1,
                        typename S::vel_t* yvel1, typename S::vel_t* zvel1) {
-  LAUNCH(k_accelerate<S>, nodes(g), dt_val, dt_ptr, ga, density0, pressure, viscosity, xvel0,
-         yvel0, zvel0, xvel1, yvel1, zvel1);
+  launch_mapped(tg, s, kKeyAccelerate, grid_nodes, 0, false, dim3(BX, BY),
+                k_accelerate<S, MapSingle>, k_accelerate<S, MapBatch>, dt_val, dt_ptr, ga,
+                density0, pressure, viscosity, xvel0, yvel0, zvel0, xvel1, yvel1, zvel1);
 }
 
 template <class S>
@@ -1111,14 +1197,15 @@ void launch_advec_mom(const Geom& g, cudaStream_t s, typename S::vel_t* vel1,
 }
 
 template <class S>
-void launch_reset_field(const Geom& g, cudaStream_t s, typename S::rho_t* density0,
+void launch_reset_field(const Target& tg, cudaStream_t s, typename S::rho_t* density0,
                         const typename S::rho_t* density1, typename S::ene_t* energy0,
                         const typename S::ene_t* energy1, typename S::vel_t* xvel0,
                         const typename S::vel_t* xvel1, typename S::vel_t* yvel0,
                         const typename S::vel_t* yvel1, typename S::vel_t* zvel0,
                         const typename S::vel_t* zvel1) {
-  LAUNCH(k_reset<S>, nodes(g), density0, density1, energy0, energy1, xvel0, xvel1, yvel0, yvel1,
-         zvel0, zvel1);
+  launch_mapped(tg, s, kKeyReset, grid_nodes, 0, false, dim3(BX, BY), k_reset<S, MapSingle>,
+                k_reset<S, MapBatch>, density0, density1, energy0, energy1, xvel0, xvel1, yvel0,
+                yvel1, zvel0, zvel1);
 }
 
 int summary_partials_len() { return SUM_BLOCKS * 5; }
@@ -1134,6 +1221,22 @@ void launch_field_summary(const Geom& g, cudaStream_t s, const double* volume,
   k_summary_final<<<1, SUM_THREADS, 0, s>>>(partials, out5);
 }
 
+inline dim3 grid_planes(const Geom& g, int) { return dim3(1, 1, g.z_max - g.z_min + 1); }
+
+template <class S>
+void launch_field_summary_batch(BatchPlan* plan, int n_decks, cudaStream_t s,
+                                const int* plane_base, const double* volume,
+                                const typename S::rho_t* density0, const typename S::ene_t* energy0,
+                                const typename S::cs_t* pressure, const typename S::vel_t* xvel0,
+                                const typename S::vel_t* yvel0, const typename S::vel_t* zvel0,
+                                double* partials, double* out) {
+  launch_mapped(Target(plan), s, kKeySummary, grid_planes, 0, false, dim3(SUM_THREADS),
+                k_summary_plane<S, MapSingle>, k_summary_plane<S, MapBatch>, plane_base, volume,
+                density0, energy0, pressure, xvel0, yvel0, zvel0, partials);
+  if (n_decks > 0)
+    k_summary_decks<<<n_decks, SUM_THREADS, 0, s>>>(plane_base, partials, out);
+}
+
 template <class S>
 static int elem_bytes_of(int id) {
   if (id == 1 || id == 2) return sizeof(typename S::rho_t);
@@ -1145,7 +1248,7 @@ static int elem_bytes_of(int id) {
 }
 
 template <class S>
-void launch_update_halo(const Geom& g, cudaStream_t s, const HaloFields& f, const int* fields,
+void launch_update_halo(const Target& tg, cudaStream_t s, const HaloFields& f, const int* fields,
                         int depth, const int* external_faces) {
   // field id -> (kind, component)
   static const int kind[19] = {0, 0, 0, 0, 0, 0, 0, 1, 1, 1, 1, 1, 1, 2, 2, 2, 2, 2, 2};
@@ -1168,14 +1271,17 @@ void launch_update_halo(const Geom& g, cudaStream_t s, const HaloFields& f, cons
       h.rule[i] = make_rule(kind[id - 1], comp[id - 1], ax, id);
     }
     if (h.nfields == 0) return;
-    const int mins[3] = {g.x_min, g.y_min, g.z_min}, maxs[3] = {g.x_max, g.y_max, g.z_max};
-    const int ta = ax == 0 ? 1 : 0, tb = ax == 2 ? 1 : 2;
-    const int na = maxs[ta] - mins[ta] + 2 + 2 * depth, nb = maxs[tb] - mins[tb] + 2 + 2 * depth;
     const dim3 blk(32, 8);
-    const dim3 gr((na + 31) / 32, (nb + 7) / 8);
-    if (ax == 0) k_halo<0><<<gr, blk, 0, s>>>(g, h, depth, do_low, do_high);
-    else if (ax == 1) k_halo<1><<<gr, blk, 0, s>>>(g, h, depth, do_low, do_high);
-    else k_halo<2><<<gr, blk, 0, s>>>(g, h, depth, do_low, do_high);
+    const unsigned key = kKeyHalo | (unsigned)(ax << 4) | (unsigned)depth;
+    if (ax == 0)
+      launch_mapped(tg, s, key, grid_halo<0>, depth, false, blk, k_halo<0, MapSingle>,
+                    k_halo<0, MapBatch>, h, depth, do_low, do_high);
+    else if (ax == 1)
+      launch_mapped(tg, s, key, grid_halo<1>, depth, false, blk, k_halo<1, MapSingle>,
+                    k_halo<1, MapBatch>, h, depth, do_low, do_high);
+    else
+      launch_mapped(tg, s, key, grid_halo<2>, depth, false, blk, k_halo<2, MapSingle>,
+                    k_halo<2, MapBatch>, h, depth, do_low, do_high);
   }
 }
 
@@ -1211,12 +1317,12 @@ void launch_fill(cudaStream_t s, T* p, long long elems, T value) {
 }
 
 #define INST(S)                                                                               \
-  template void launch_ideal_gas<S>(const Geom&, cudaStream_t, const S::rho_t*, const S::ene_t*, \
+  template void launch_ideal_gas<S>(const Target&, cudaStream_t, const S::rho_t*, const S::ene_t*, \
                                     S::cs_t*, S::cs_t*);                                      \
   template void launch_viscosity<S>(const Geom&, cudaStream_t, const GeomArrays&, const S::rho_t*, \
                                     const S::cs_t*, S::cs_t*, const S::vel_t*, const S::vel_t*, \
                                     const S::vel_t*);                                         \
-  template void launch_calc_dt<S>(const Geom&, cudaStream_t, const GeomArrays&, double, double, \
+  template void launch_calc_dt<S>(const Target&, cudaStream_t, const GeomArrays&, double, double, \
                                   double, double, double, double, const S::rho_t*,             \
                                   const S::cs_t*, const S::cs_t*, const S::vel_t*,              \
                                   const S::vel_t*, const S::vel_t*, S::wk_t*,                  \
@@ -1228,7 +1334,7 @@ void launch_fill(cudaStream_t s, T* p, long long elems, T value) {
                               const S::vel_t*, const S::vel_t*);                               \
   template void launch_revert<S>(const Geom&, cudaStream_t, const S::rho_t*, S::rho_t*,          \
                                  const S::ene_t*, S::ene_t*);                                  \
-  template void launch_accelerate<S>(const Geom&, cudaStream_t, double, const double*,           \
+  template void launch_accelerate<S>(const Target&, cudaStream_t, double, const double*,           \
                                      const GeomArrays&, const S::rho_t*, const S::cs_t*,       \
                                      const S::cs_t*, const S::vel_t*, const S::vel_t*,          \
                                      const S::vel_t*, S::vel_t*, S::vel_t*, S::vel_t*);        \
@@ -1243,14 +1349,18 @@ void launch_fill(cudaStream_t s, T* p, long long elems, T value) {
                                     const S::vf_t*, const S::mf_t*, const S::vf_t*,            \
                                     const S::mf_t*, const S::vf_t*, const GeomArrays&,         \
                                     const S::rho_t*, S::wk_t* const*, int, int, int, int);     \
-  template void launch_reset_field<S>(const Geom&, cudaStream_t, S::rho_t*, const S::rho_t*,     \
+  template void launch_reset_field<S>(const Target&, cudaStream_t, S::rho_t*, const S::rho_t*,     \
                                       S::ene_t*, const S::ene_t*, S::vel_t*, const S::vel_t*,  \
                                       S::vel_t*, const S::vel_t*, S::vel_t*, const S::vel_t*); \
   template void launch_field_summary<S>(const Geom&, cudaStream_t, const double*,               \
                                         const S::rho_t*, const S::ene_t*, const S::cs_t*,      \
                                         const S::vel_t*, const S::vel_t*, const S::vel_t*,     \
                                         double*, double*);                                     \
-  template void launch_update_halo<S>(const Geom&, cudaStream_t, const HaloFields&, const int*,  \
+  template void launch_field_summary_batch<S>(BatchPlan*, int, cudaStream_t, const int*,        \
+                                              const double*, const S::rho_t*, const S::ene_t*, \
+                                              const S::cs_t*, const S::vel_t*, const S::vel_t*, \
+                                              const S::vel_t*, double*, double*);              \
+  template void launch_update_halo<S>(const Target&, cudaStream_t, const HaloFields&, const int*,  \
                                       int, const int*);                                        \
   template void launch_generate_chunk<S>(const Geom&, cudaStream_t, const GeomArrays&,          \
                                          S::rho_t*, S::ene_t*, S::vel_t*, S::vel_t*,           \

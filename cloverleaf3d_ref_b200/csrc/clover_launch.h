@@ -4,13 +4,95 @@
 // kernel it replaces. dt is passed either by value (dt_ptr == nullptr) or as a
 // device pointer, so the same kernels serve the drop-in ABI (dt from the
 // caller) and the graph-captured native step (dt computed on the device).
+//
+// The launchers of the native step take a Target: one chunk (a Geom, which
+// may carry offsets into shared allocations) or every deck of an ensemble's
+// BatchPlan, in which case the same kernels run over all decks in one
+// persistent launch (clover_sched.cuh, clover_batch.cu).
 #pragma once
 
 #include <cuda_runtime.h>
 
+#include <utility>
+
 #include "clover_layout.cuh"
+#include "clover_sched.cuh"
 
 namespace clover {
+
+// Device-resident state of one deck of a native run (timestep.f90 and
+// hydro.f90 scalars, the calc_dt reduction key, the status word and the
+// deck's timestep controls). Kernels find deck d's copy kScalarStride
+// doubles after deck 0's.
+struct DevScalars {
+  double dt, dtold, time;
+  unsigned long long key;
+  int step;
+  int status;
+  int dt_cap;
+  int pad;
+  double dtrise, dtmax, dtmin, pad2;
+};
+constexpr int kScalarStride = (int)(sizeof(DevScalars) / sizeof(double));
+static_assert(sizeof(DevScalars) % sizeof(double) == 0, "deck scalars stride");
+
+// ---- batched launches over the decks of an ensemble ----
+struct BatchPlan;  // clover_batch.cu
+
+// One deck's tile grid for a launch; aux is the segment length of a marching
+// kernel or the depth of a halo update.
+using GridFn = dim3 (*)(const Geom& g, int aux);
+
+struct BatchLaunch {
+  const int4* items;  // (deck, tile x, y, z), in schedule order
+  const Geom* decks;
+  int n;              // items
+  int grid;           // blocks to launch (0: nothing to launch)
+  int aux;            // segment length / depth the schedule was built for
+};
+
+// The schedule of one batched launch. key names the launch (kernel and the
+// variant that fixes its grid); seg_tunable says whether aux is a segment
+// length the plan may choose. Builds the schedule on first use (not while a
+// stream is being captured).
+BatchLaunch batch_launch(BatchPlan* plan, unsigned key, GridFn grid_fn, int aux, bool seg_tunable,
+                         const void* kernel, int threads);
+void batch_mark(BatchPlan* plan, unsigned key, cudaStream_t s, bool begin);
+
+struct Target {
+  Geom g;
+  BatchPlan* plan;
+  Target(const Geom& g_) : g(g_), plan(nullptr) {}
+  explicit Target(BatchPlan* p) : g(), plan(p) {}
+};
+
+// Launch kernel ks over one chunk (grid from grid_fn) or kb over the plan's
+// schedule; both get the map first and then args.
+template <class... P, class... A>
+inline void launch_mapped(const Target& tg, cudaStream_t s, unsigned key, GridFn grid_fn, int aux,
+                          bool seg_tunable, dim3 blk, void (*ks)(MapSingle, P...),
+                          void (*kb)(MapBatch, P...), A&&... args) {
+  if (!tg.plan) {
+    const dim3 gr = grid_fn(tg.g, aux);
+    if (gr.x && gr.y && gr.z) ks<<<gr, blk, 0, s>>>(MapSingle{tg.g, aux}, std::forward<A>(args)...);
+    return;
+  }
+  const BatchLaunch bl = batch_launch(tg.plan, key, grid_fn, aux, seg_tunable, (const void*)kb,
+                                      (int)(blk.x * blk.y * blk.z));
+  if (bl.grid <= 0) return;
+  batch_mark(tg.plan, key, s, true);
+  kb<<<bl.grid, blk, 0, s>>>(MapBatch{bl.items, bl.decks, bl.n, bl.aux}, std::forward<A>(args)...);
+  batch_mark(tg.plan, key, s, false);
+}
+
+// Launch keys: kernel id in the high bits, the variant fixing the grid low.
+enum : unsigned {
+  kKeyIdealGas = 1u << 8, kKeyCalcDt = 2u << 8, kKeyReset = 3u << 8, kKeyHalo = 4u << 8,
+  kKeyTimestepVisc = 5u << 8, kKeyPdvPredict = 6u << 8, kKeyPdvFlux = 7u << 8,
+  kKeyCellFluxX = 8u << 8, kKeyCellUpdateX = 9u << 8, kKeyCellSweep = 10u << 8,
+  kKeyMomSweepX = 11u << 8, kKeyMomNode = 12u << 8, kKeyMomVel3 = 13u << 8,
+  kKeyShellCopy = 14u << 8, kKeySummary = 15u << 8, kKeyAccelerate = 16u << 8
+};
 
 // Storage policy: FP64 everywhere (the drop-in / parity path).
 struct F64 {
@@ -54,7 +136,7 @@ struct HaloFields {
 };
 
 template <class S>
-void launch_ideal_gas(const Geom& g, cudaStream_t s, const typename S::rho_t* density,
+void launch_ideal_gas(const Target& tg, cudaStream_t s, const typename S::rho_t* density,
                       const typename S::ene_t* energy, typename S::cs_t* pressure,
                       typename S::cs_t* soundspeed);
 
@@ -66,9 +148,11 @@ void launch_viscosity(const Geom& g, cudaStream_t s, const GeomArrays& ga,
 
 // Writes dt_min per interior cell (when dt_min_arr != nullptr) and folds the
 // minimum into *min_key (an order-preserving 64-bit key of a double, see
-// clover_kernels.cu); the caller initialises *min_key.
+// clover_kernels.cu); the caller initialises *min_key. Over a plan, deck d
+// folds into min_key[d * kScalarStride]; dt_ptr arguments are read the same
+// way (deck d's dt at dt_ptr[d * kScalarStride]).
 template <class S>
-void launch_calc_dt(const Geom& g, cudaStream_t s, const GeomArrays& ga, double g_small,
+void launch_calc_dt(const Target& tg, cudaStream_t s, const GeomArrays& ga, double g_small,
                     double dtc_safe, double dtu_safe, double dtv_safe, double dtw_safe,
                     double dtdiv_safe, const typename S::rho_t* density0,
                     const typename S::cs_t* viscosity, const typename S::cs_t* soundspeed,
@@ -95,7 +179,7 @@ void launch_revert(const Geom& g, cudaStream_t s, const typename S::rho_t* densi
                    typename S::ene_t* energy1);
 
 template <class S>
-void launch_accelerate(const Geom& g, cudaStream_t s, double dt_val, const double* dt_ptr,
+void launch_accelerate(const Target& tg, cudaStream_t s, double dt_val, const double* dt_ptr,
                        const GeomArrays& ga, const typename S::rho_t* density0,
                        const typename S::cs_t* pressure, const typename S::cs_t* viscosity,
                        const typename S::vel_t* xvel0, const typename S::vel_t* yvel0,
@@ -130,12 +214,24 @@ void launch_advec_mom(const Geom& g, cudaStream_t s, typename S::vel_t* vel1,
                       int direction);
 
 template <class S>
-void launch_reset_field(const Geom& g, cudaStream_t s, typename S::rho_t* density0,
+void launch_reset_field(const Target& tg, cudaStream_t s, typename S::rho_t* density0,
                         const typename S::rho_t* density1, typename S::ene_t* energy0,
                         const typename S::ene_t* energy1, typename S::vel_t* xvel0,
                         const typename S::vel_t* xvel1, typename S::vel_t* yvel0,
                         const typename S::vel_t* yvel1, typename S::vel_t* zvel0,
                         const typename S::vel_t* zvel1);
+
+// Per-deck sums of a plan's decks: out holds 5 doubles per deck. Each deck
+// sums its z planes (one block each, a fixed tree order) into
+// partials[(plane_base[d] + plane) * 5 ...], then one block per deck adds its
+// planes in order. plane_base: device array of the decks' first plane index.
+template <class S>
+void launch_field_summary_batch(BatchPlan* plan, int n_decks, cudaStream_t s,
+                                const int* plane_base, const double* volume,
+                                const typename S::rho_t* density0, const typename S::ene_t* energy0,
+                                const typename S::cs_t* pressure, const typename S::vel_t* xvel0,
+                                const typename S::vel_t* yvel0, const typename S::vel_t* zvel0,
+                                double* partials, double* out);
 
 // Sums (vol, mass, ie, ke, press) into out5 (device), deterministic order.
 // partials: device scratch of summary_partials_len() doubles.
@@ -150,7 +246,7 @@ void launch_field_summary(const Geom& g, cudaStream_t s, const double* volume,
 // update_halo_kernel: fields[i] != 0 selects field id i+1; all faces external.
 // Element size of every selected field comes from the policy S.
 template <class S>
-void launch_update_halo(const Geom& g, cudaStream_t s, const HaloFields& f, const int* fields,
+void launch_update_halo(const Target& tg, cudaStream_t s, const HaloFields& f, const int* fields,
                         int depth, const int* external_faces /*6: left..front*/);
 
 // initialise_chunk_kernel + generate_chunk_kernel on the device.
@@ -174,18 +270,18 @@ void launch_generate_chunk(const Geom& g, cudaStream_t s, const GeomArrays& ga,
 
 // ---- fused kernels of the native step (clover_fused.cu) ----
 template <class S>
-void launch_timestep_visc(const Geom& g, cudaStream_t s, const GeomArrays& ga,
+void launch_timestep_visc(const Target& tg, cudaStream_t s, const GeomArrays& ga,
                           const typename S::rho_t* density0, const typename S::cs_t* pressure,
                           typename S::cs_t* viscosity, const typename S::vel_t* xvel0,
                           const typename S::vel_t* yvel0, const typename S::vel_t* zvel0);
 template <class S>
-void launch_pdv_predict_eos(const Geom& g, cudaStream_t s, const double* dt_ptr,
+void launch_pdv_predict_eos(const Target& tg, cudaStream_t s, const double* dt_ptr,
                             const GeomArrays& ga, const typename S::rho_t* density0,
                             const typename S::ene_t* energy0, typename S::cs_t* pressure,
                             const typename S::cs_t* viscosity, const typename S::vel_t* xvel0,
                             const typename S::vel_t* yvel0, const typename S::vel_t* zvel0);
 template <class S>
-void launch_pdv_flux(const Geom& g, cudaStream_t s, const double* dt_ptr, const GeomArrays& ga,
+void launch_pdv_flux(const Target& tg, cudaStream_t s, const double* dt_ptr, const GeomArrays& ga,
                      const typename S::rho_t* density0, typename S::rho_t* density1,
                      const typename S::ene_t* energy0, typename S::ene_t* energy1,
                      const typename S::cs_t* pressure, const typename S::cs_t* viscosity,
@@ -195,7 +291,7 @@ void launch_pdv_flux(const Geom& g, cudaStream_t s, const double* dt_ptr, const 
                      typename S::vf_t* vol_flux_x, typename S::vf_t* vol_flux_y,
                      typename S::vf_t* vol_flux_z);
 template <class S>
-void launch_advec_cell_fused(const Geom& g, cudaStream_t s, int advect_x, int dir, int sweep,
+void launch_advec_cell_fused(const Target& tg, cudaStream_t s, int advect_x, int dir, int sweep,
                              const GeomArrays& ga, typename S::rho_t* density1,
                              typename S::ene_t* energy1, typename S::mf_t* mass_flux_x,
                              const typename S::vf_t* vol_flux_x, typename S::mf_t* mass_flux_y,
@@ -205,7 +301,7 @@ void launch_advec_cell_fused(const Geom& g, cudaStream_t s, int advect_x, int di
 // each velocity pair (the shell outside [min,max+1]^3 is copied across).
 // vol: the uniform cell volume of the chunk (dx*dy*dz).
 template <class S>
-void launch_advec_mom_fused(const Geom& g, cudaStream_t s, int advect_x, int sweep, int dir,
+void launch_advec_mom_fused(const Target& tg, cudaStream_t s, int advect_x, int sweep, int dir,
                             double vol, const GeomArrays& ga, const typename S::rho_t* density1,
                             const typename S::mf_t* mass_flux_x, const typename S::mf_t* mass_flux_y,
                             const typename S::mf_t* mass_flux_z, const typename S::vf_t* vol_flux_x,

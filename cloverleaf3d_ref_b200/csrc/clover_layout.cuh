@@ -9,6 +9,10 @@
 // boundary, for 4- and 8-byte elements alike. Cell arrays simply leave their
 // last row/plane/column unused, so a kernel can address every array with one
 // (px, pxy) pair. 1D coordinate arrays are indexed from min-2.
+//
+// Several chunks (the decks of an ensemble) can share one allocation per
+// array: deck d then starts o3 elements into every 3D allocation and o1
+// elements into every 1D allocation. A single chunk has o3 = o1 = 0.
 #pragma once
 
 #include <cstdint>
@@ -19,7 +23,9 @@ namespace clover {
 struct Geom {
   int x_min, x_max, y_min, y_max, z_min, z_max;
   int px;         // row pitch in elements
+  int o1;         // offset of this chunk in the shared 1D allocations
   long long pxy;  // plane pitch in elements
+  long long o3;   // offset of this chunk in the shared 3D allocations
 };
 
 // Elements per 128 bytes for a storage type.
@@ -38,6 +44,8 @@ inline Geom make_geom(int x_min, int x_max, int y_min, int y_max, int z_min, int
   int nxv = x_max - x_min + 6;
   g.px = (nxv + align - 1) / align * align;
   g.pxy = (long long)g.px * (y_max - y_min + 6);
+  g.o1 = 0;
+  g.o3 = 0;
   return g;
 }
 
@@ -47,8 +55,17 @@ inline long long array_elems(const Geom& g) {
 }
 
 __host__ __device__ __forceinline__ long long off3(const Geom& g, int j, int k, int l) {
-  return (long long)(j - g.x_min + 2) + (long long)(k - g.y_min + 2) * g.px +
+  return g.o3 + (long long)(j - g.x_min + 2) + (long long)(k - g.y_min + 2) * g.px +
          (long long)(l - g.z_min + 2) * g.pxy;
+}
+
+// Elements of one 1D coordinate array (any axis) of a chunk, rounded so that
+// the next chunk's arrays start on a 256-byte boundary.
+inline int array1d_elems(const Geom& g) {
+  int n = g.x_max - g.x_min;
+  if (g.y_max - g.y_min > n) n = g.y_max - g.y_min;
+  if (g.z_max - g.z_min > n) n = g.z_max - g.z_min;
+  return (n + 6 + 31) / 32 * 32;
 }
 
 }  // namespace clover

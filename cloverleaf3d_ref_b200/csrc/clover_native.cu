@@ -1,16 +1,22 @@
 // Native chunk: the whole hydro cycle resident in HBM, dt/time/step on the
 // device, one step replayed from a CUDA graph (one graph per sweep order).
+// The same object holds an ensemble: many independent decks whose arrays
+// share one allocation per field (each deck at its own offset), every
+// kernel of the step launched once over all decks through a BatchPlan
+// schedule, each deck with its own dt, time and calc_dt reduction.
 // Also the deck reader (parse.f90 + read_input.f90 semantics).
 #include <cctype>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <map>
 #include <string>
 #include <vector>
 
 #include "../../include/clover_b200.h"
 #include "../../include/clover_kernels.h"
+#include "clover_batch.h"
 #include "clover_launch.h"
 
 namespace clover {
@@ -22,59 +28,64 @@ std::string g_last_error;
 const double kGSmall = (double)1.0e-16f;
 const double kGBig = (double)1.0e+21f;
 
-// Device-resident step state.
-struct DevScalars {
-  double dt, dtold, time;
-  unsigned long long key;
-  int step;
-  int status;
-  int dt_cap;
-  int pad;
-};
+// One thread per deck: the key of the calc_dt reduction starts at g_big.
+__global__ void k_dt_prepare(DevScalars* sc, int nd, unsigned long long init) {
+  const int d = blockIdx.x * blockDim.x + threadIdx.x;
+  if (d < nd) sc[d].key = init;
+}
 
-__global__ void k_dt_prepare(DevScalars* sc, unsigned long long init) { sc->key = init; }
-
-// timestep.f90:90-126 after the calc_dt reduction
-__global__ void k_dt_finalize(DevScalars* sc, double* dt_hist, double dtrise, double dtmax,
-                              double dtmin) {
+// timestep.f90:90-126 after the calc_dt reduction, one thread per deck
+__global__ void k_dt_finalize(DevScalars* scs, int nd, double* dt_hist) {
+  const int d = blockIdx.x * blockDim.x + threadIdx.x;
+  if (d >= nd) return;
+  DevScalars* sc = scs + d;
   unsigned long long key = sc->key;
   unsigned long long b = (key >> 63) ? (key & 0x7fffffffffffffffull) : ~key;
   const double dtlp = __longlong_as_double((long long)b);
   double dt = kGBig;
   if (dtlp <= dt) dt = dtlp;
   double m = dt;
-  const double r = sc->dtold * dtrise;
+  const double r = sc->dtold * sc->dtrise;
   if (r < m) m = r;
-  if (dtmax < m) m = dtmax;
+  if (sc->dtmax < m) m = sc->dtmax;
   dt = m;
-  if (dt < dtmin) sc->status |= CLOVER_STATUS_SMALL_DT;
+  if (dt < sc->dtmin) sc->status |= CLOVER_STATUS_SMALL_DT;
   sc->dt = dt;
   sc->dtold = dt;
   const int s = sc->step;
-  if (s < sc->dt_cap) dt_hist[s] = dt;
+  if (s < sc->dt_cap) dt_hist[(long long)d * sc->dt_cap + s] = dt;
   sc->step = s + 1;
 }
 
-// hydro.f90:68
-__global__ void k_step_end(DevScalars* sc) { sc->time = sc->time + sc->dt; }
+// hydro.f90:68, one thread per deck
+__global__ void k_step_end(DevScalars* sc, int nd) {
+  const int d = blockIdx.x * blockDim.x + threadIdx.x;
+  if (d < nd) sc[d].time = sc[d].time + sc[d].dt;
+}
 
+struct Owned {
+  void* p;
+  size_t bytes;
+};
+
+// One 3D array for all decks (elems after the front pad), zeroed.
 template <class T>
-T* alloc_field(const Geom& g, std::vector<void*>& owned, long long& bytes, cudaStream_t s) {
+T* alloc_field(long long elems, std::vector<Owned>& owned, long long& bytes, cudaStream_t s) {
   void* raw = nullptr;
-  const size_t n = (size_t)(array_elems(g) + kFrontPad<T>) * sizeof(T);
+  const size_t n = (size_t)(elems + kFrontPad<T>) * sizeof(T);
   if (cudaMalloc(&raw, n) != cudaSuccess) return nullptr;
   cudaMemsetAsync(raw, 0, n, s);
-  owned.push_back(raw);
+  owned.push_back(Owned{raw, n});
   bytes += (long long)n;
   return (T*)raw + kFrontPad<T>;
 }
 
-double* alloc_1d(int n, std::vector<void*>& owned, long long& bytes, cudaStream_t s) {
+double* alloc_1d(long long n, std::vector<Owned>& owned, long long& bytes, cudaStream_t s) {
   void* raw = nullptr;
   const size_t sz = (size_t)(n + 32) * sizeof(double);
   if (cudaMalloc(&raw, sz) != cudaSuccess) return nullptr;
   cudaMemsetAsync(raw, 0, sz, s);
-  owned.push_back(raw);
+  owned.push_back(Owned{raw, sz});
   bytes += (long long)sz;
   return (double*)raw;
 }
@@ -95,10 +106,16 @@ struct Chunk : ChunkBase {
   using MF = typename S::mf_t;
   using W = typename S::wk_t;
 
-  clover_deck deck;
-  Geom g;
+  clover_deck deck;                // deck 0: summary cadence and end step of all decks
+  Geom g;                          // deck 0's geometry (the whole chunk when nd == 1)
+  std::vector<clover_deck> decks;  // every deck
+  std::vector<Geom> geoms;         // every deck, with its offsets in the shared arrays
+  int nd = 1;
+  BatchPlan* plan = nullptr;       // ensemble: the schedules of the batched launches
+  Target tg{Geom{}};               // where the step's launchers run
+  bool warm[2] = {false, false};   // a step of each sweep order ran since the schedules changed
   cudaStream_t stream = nullptr;
-  std::vector<void*> owned;
+  std::vector<Owned> owned;
   long long bytes = 0;
 
   R *density0, *density1;
@@ -121,6 +138,7 @@ struct Chunk : ChunkBase {
   int sum_cap = 0;
   std::vector<int> sum_steps;  // host: step of each recorded summary
   double* partials = nullptr;
+  int* plane_base = nullptr;  // ensemble: first summary plane of each deck (nd + 1)
 
   double cell_volume = 0.0;  // dx*dy*dz, the volume of every cell (initialise_chunk)
   int host_step = 0;     // steps enqueued
@@ -176,7 +194,10 @@ struct Chunk : ChunkBase {
     prof_pending.clear();
   }
   double cells() const {
-    return (double)(g.x_max - g.x_min + 1) * (g.y_max - g.y_min + 1) * (g.z_max - g.z_min + 1);
+    double n = 0.0;
+    for (const Geom& q : geoms)
+      n += (double)(q.x_max - q.x_min + 1) * (q.y_max - q.y_min + 1) * (q.z_max - q.z_min + 1);
+    return n;
   }
 
   // time-level-1 velocity c (0 x, 1 y, 2 z) in buffer b of its pair
@@ -200,53 +221,70 @@ struct Chunk : ChunkBase {
   void halo(std::initializer_list<int> ids, int depth, int vb = 0) {
     int fields[19] = {0};
     for (int id : ids) fields[id - 1] = 1;
-    launch_update_halo<S>(g, stream, halo_fields(vb), fields, depth, ext);
+    launch_update_halo<S>(tg, stream, halo_fields(vb), fields, depth, ext);
   }
 
-  bool create(const clover_deck& d) {
-    deck = d;
-    g = make_geom(1, d.x_cells, 1, d.y_cells, 1, d.z_cells);
+  int deck_blocks() const { return (nd + 127) / 128; }
+
+  // Allocate the shared arrays of the decks (batched: launch every kernel
+  // over all decks through a plan, even for one deck) and set them up.
+  bool create(const clover_deck* ds, int n, bool batched) {
+    decks.assign(ds, ds + n);
+    nd = n;
+    deck = decks[0];
+    long long total3 = 0, total1 = 0;
+    for (int d = 0; d < nd; d++) {
+      Geom q = make_geom(1, decks[d].x_cells, 1, decks[d].y_cells, 1, decks[d].z_cells);
+      q.o3 = total3;
+      q.o1 = (int)total1;
+      total3 += array_elems(q);
+      total1 += array1d_elems(q);
+      geoms.push_back(q);
+    }
+    g = geoms[0];
     if (cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking) != cudaSuccess) return false;
+    if (batched) {
+      plan = new BatchPlan;
+      if (!plan->init(geoms)) {
+        g_last_error = "device allocation failed";
+        return false;
+      }
+      tg = Target(plan);
+      fused = true;  // the batched step is the fused one
+    } else {
+      tg = Target(g);
+    }
     bool ok = true;
     auto chk = [&](const void* p) { ok = ok && p != nullptr; };
-    chk(density0 = alloc_field<R>(g, owned, bytes, stream));
-    chk(density1 = alloc_field<R>(g, owned, bytes, stream));
-    chk(energy0 = alloc_field<En>(g, owned, bytes, stream));
-    chk(energy1 = alloc_field<En>(g, owned, bytes, stream));
-    chk(pressure = alloc_field<C>(g, owned, bytes, stream));
-    chk(viscosity = alloc_field<C>(g, owned, bytes, stream));
-    chk(soundspeed = alloc_field<C>(g, owned, bytes, stream));
-    chk(xvel0 = alloc_field<V>(g, owned, bytes, stream));
-    chk(xvel1 = alloc_field<V>(g, owned, bytes, stream));
-    chk(yvel0 = alloc_field<V>(g, owned, bytes, stream));
-    chk(yvel1 = alloc_field<V>(g, owned, bytes, stream));
-    chk(zvel0 = alloc_field<V>(g, owned, bytes, stream));
-    chk(zvel1 = alloc_field<V>(g, owned, bytes, stream));
-    for (int c3 = 0; c3 < 3; c3++) chk(vel1b[c3] = alloc_field<V>(g, owned, bytes, stream));
-    chk(vol_flux_x = alloc_field<VF>(g, owned, bytes, stream));
-    chk(vol_flux_y = alloc_field<VF>(g, owned, bytes, stream));
-    chk(vol_flux_z = alloc_field<VF>(g, owned, bytes, stream));
-    chk(mass_flux_x = alloc_field<MF>(g, owned, bytes, stream));
-    chk(mass_flux_y = alloc_field<MF>(g, owned, bytes, stream));
-    chk(mass_flux_z = alloc_field<MF>(g, owned, bytes, stream));
-    for (int i = 0; i < 7; i++) chk(work[i] = alloc_field<W>(g, owned, bytes, stream));
-    chk(volume = alloc_field<double>(g, owned, bytes, stream));
-    chk(xarea = alloc_field<double>(g, owned, bytes, stream));
-    chk(yarea = alloc_field<double>(g, owned, bytes, stream));
-    chk(zarea = alloc_field<double>(g, owned, bytes, stream));
-    const int nx = d.x_cells, ny = d.y_cells, nz = d.z_cells;
-    chk(cellx = alloc_1d(nx + 4, owned, bytes, stream));
-    chk(celly = alloc_1d(ny + 4, owned, bytes, stream));
-    chk(cellz = alloc_1d(nz + 4, owned, bytes, stream));
-    chk(celldx = alloc_1d(nx + 4, owned, bytes, stream));
-    chk(celldy = alloc_1d(ny + 4, owned, bytes, stream));
-    chk(celldz = alloc_1d(nz + 4, owned, bytes, stream));
-    chk(vertexx = alloc_1d(nx + 5, owned, bytes, stream));
-    chk(vertexy = alloc_1d(ny + 5, owned, bytes, stream));
-    chk(vertexz = alloc_1d(nz + 5, owned, bytes, stream));
-    chk(vertexdx = alloc_1d(nx + 5, owned, bytes, stream));
-    chk(vertexdy = alloc_1d(ny + 5, owned, bytes, stream));
-    chk(vertexdz = alloc_1d(nz + 5, owned, bytes, stream));
+    const long long e3 = total3;
+    chk(density0 = alloc_field<R>(e3, owned, bytes, stream));
+    chk(density1 = alloc_field<R>(e3, owned, bytes, stream));
+    chk(energy0 = alloc_field<En>(e3, owned, bytes, stream));
+    chk(energy1 = alloc_field<En>(e3, owned, bytes, stream));
+    chk(pressure = alloc_field<C>(e3, owned, bytes, stream));
+    chk(viscosity = alloc_field<C>(e3, owned, bytes, stream));
+    chk(soundspeed = alloc_field<C>(e3, owned, bytes, stream));
+    chk(xvel0 = alloc_field<V>(e3, owned, bytes, stream));
+    chk(xvel1 = alloc_field<V>(e3, owned, bytes, stream));
+    chk(yvel0 = alloc_field<V>(e3, owned, bytes, stream));
+    chk(yvel1 = alloc_field<V>(e3, owned, bytes, stream));
+    chk(zvel0 = alloc_field<V>(e3, owned, bytes, stream));
+    chk(zvel1 = alloc_field<V>(e3, owned, bytes, stream));
+    for (int c3 = 0; c3 < 3; c3++) chk(vel1b[c3] = alloc_field<V>(e3, owned, bytes, stream));
+    chk(vol_flux_x = alloc_field<VF>(e3, owned, bytes, stream));
+    chk(vol_flux_y = alloc_field<VF>(e3, owned, bytes, stream));
+    chk(vol_flux_z = alloc_field<VF>(e3, owned, bytes, stream));
+    chk(mass_flux_x = alloc_field<MF>(e3, owned, bytes, stream));
+    chk(mass_flux_y = alloc_field<MF>(e3, owned, bytes, stream));
+    chk(mass_flux_z = alloc_field<MF>(e3, owned, bytes, stream));
+    for (int i = 0; i < 7; i++) chk(work[i] = alloc_field<W>(e3, owned, bytes, stream));
+    chk(volume = alloc_field<double>(e3, owned, bytes, stream));
+    chk(xarea = alloc_field<double>(e3, owned, bytes, stream));
+    chk(yarea = alloc_field<double>(e3, owned, bytes, stream));
+    chk(zarea = alloc_field<double>(e3, owned, bytes, stream));
+    double** one_d[12] = {&cellx, &celly, &cellz, &celldx, &celldy, &celldz,
+                          &vertexx, &vertexy, &vertexz, &vertexdx, &vertexdy, &vertexdz};
+    for (double** a : one_d) chk(*a = alloc_1d(total1, owned, bytes, stream));
     if (!ok) {
       g_last_error = "device allocation failed";
       return false;
@@ -254,70 +292,181 @@ struct Chunk : ChunkBase {
     ga = GeomArrays{volume, xarea, yarea, zarea, cellx, celly, cellz, celldx, celldy, celldz,
                     vertexx, vertexy, vertexz, vertexdx, vertexdy, vertexdz};
 
-    dt_cap = d.end_step < (1 << 22) ? d.end_step + 16 : (1 << 22);
-    sum_cap = dt_cap / (d.summary_frequency > 0 ? d.summary_frequency : dt_cap) + 8;
+    dt_cap = deck.end_step < (1 << 22) ? deck.end_step + 16 : (1 << 22);
+    sum_cap = dt_cap / (deck.summary_frequency > 0 ? deck.summary_frequency : dt_cap) + 8;
+    int planes = 0;
+    std::vector<int> pb(nd + 1, 0);
+    for (int d = 0; d < nd; d++) {
+      pb[d] = planes;
+      planes += geoms[d].z_max - geoms[d].z_min + 1;
+    }
+    pb[nd] = planes;
     void* p = nullptr;
-    ok = cudaMalloc(&p, sizeof(DevScalars)) == cudaSuccess;
+    ok = cudaMalloc(&p, (size_t)nd * sizeof(DevScalars)) == cudaSuccess;
     sc = (DevScalars*)p;
-    ok = ok && cudaMalloc(&p, (size_t)dt_cap * sizeof(double)) == cudaSuccess;
+    ok = ok && cudaMalloc(&p, (size_t)nd * dt_cap * sizeof(double)) == cudaSuccess;
     dt_hist = (double*)p;
-    ok = ok && cudaMalloc(&p, (size_t)sum_cap * 5 * sizeof(double)) == cudaSuccess;
+    ok = ok && cudaMalloc(&p, (size_t)nd * sum_cap * 5 * sizeof(double)) == cudaSuccess;
     sum_hist = (double*)p;
-    ok = ok && cudaMalloc(&p, (size_t)summary_partials_len() * sizeof(double)) == cudaSuccess;
+    const size_t np = plan ? (size_t)planes * 5 : (size_t)summary_partials_len();
+    ok = ok && cudaMalloc(&p, np * sizeof(double)) == cudaSuccess;
     partials = (double*)p;
+    if (ok && plan) {
+      ok = cudaMalloc(&p, pb.size() * sizeof(int)) == cudaSuccess;
+      plane_base = (int*)p;
+      ok = ok && cudaMemcpy(plane_base, pb.data(), pb.size() * sizeof(int),
+                            cudaMemcpyHostToDevice) == cudaSuccess;
+    }
     if (!ok) {
       g_last_error = "device allocation failed";
       return false;
     }
-    DevScalars h{};
-    h.dt = d.initial_timestep;     // start.f90:51-52
-    h.dtold = d.initial_timestep;
-    h.time = 0.0;
-    h.step = 0;
-    h.dt_cap = dt_cap;
-    cudaMemcpyAsync(sc, &h, sizeof(h), cudaMemcpyHostToDevice, stream);
-
-    // initialise_chunk.f90:38-46
+    const clover_deck& d = deck;
     const double dx = (d.xmax - d.xmin) / (double)(float)d.x_cells;
     const double dy = (d.ymax - d.ymin) / (double)(float)d.y_cells;
     const double dz = (d.zmax - d.zmin) / (double)(float)d.z_cells;
-    const double xmin = d.xmin + dx * (double)(float)0;
-    const double ymin = d.ymin + dy * (double)(float)0;
-    const double zmin = d.zmin + dz * (double)(float)0;
-    cell_volume = dx * dy * dz;  // initialise_chunk_kernel.f90:155
-    launch_initialise_chunk(g, stream, xmin, ymin, zmin, dx, dy, dz, vertexx, vertexdx, vertexy,
-                            vertexdy, vertexz, vertexdz, cellx, celldx, celly, celldy, cellz,
-                            celldz, volume, xarea, yarea, zarea);
-    // read_input.f90:293-303 nudge, then generate_chunk
-    StateTable st;
-    st.n = d.number_of_states;
-    for (int i = 0; i < st.n; i++) {
-      st.density[i] = d.state_density[i]; st.energy[i] = d.state_energy[i];
-      st.xvel[i] = d.state_xvel[i]; st.yvel[i] = d.state_yvel[i]; st.zvel[i] = d.state_zvel[i];
-      st.xmin[i] = d.state_xmin[i]; st.xmax[i] = d.state_xmax[i];
-      st.ymin[i] = d.state_ymin[i]; st.ymax[i] = d.state_ymax[i];
-      st.zmin[i] = d.state_zmin[i]; st.zmax[i] = d.state_zmax[i];
-      st.radius[i] = d.state_radius[i];
-      st.geometry[i] = d.state_geometry[i];
-      if (i >= 1) {
-        st.xmin[i] = st.xmin[i] + (dx / 100.0);
-        st.ymin[i] = st.ymin[i] + (dy / 100.0);
-        st.zmin[i] = st.zmin[i] + (dz / 100.0);
-        st.xmax[i] = st.xmax[i] - (dx / 100.0);
-        st.ymax[i] = st.ymax[i] - (dy / 100.0);
-        st.zmax[i] = st.zmax[i] - (dz / 100.0);
-      }
+    cell_volume = dx * dy * dz;  // initialise_chunk_kernel.f90:155 (deck 0)
+    return initial_state();
+  }
+
+  // start.f90:49-136 for every deck on the device: scalars, geometry,
+  // generated state, EOS, halos and the step-0 summary. The arrays must hold
+  // zeros (fresh allocation or reset()).
+  bool initial_state() {
+    std::vector<DevScalars> h(nd);
+    for (int i = 0; i < nd; i++) {
+      h[i] = DevScalars{};
+      h[i].dt = decks[i].initial_timestep;     // start.f90:51-52
+      h[i].dtold = decks[i].initial_timestep;
+      h[i].time = 0.0;
+      h[i].step = 0;
+      h[i].dt_cap = dt_cap;
+      h[i].dtrise = decks[i].timestep_rise;
+      h[i].dtmax = decks[i].max_timestep;
+      h[i].dtmin = decks[i].dtmin;
     }
-    launch_generate_chunk<S>(g, stream, ga, density0, energy0, xvel0, yvel0, zvel0, st);
+    cudaMemcpyAsync(sc, h.data(), (size_t)nd * sizeof(DevScalars), cudaMemcpyHostToDevice, stream);
+    cudaStreamSynchronize(stream);  // h is released at return
+    for (int i = 0; i < nd; i++) {
+      const clover_deck& d = decks[i];
+      const Geom& q = geoms[i];
+      // initialise_chunk.f90:38-46
+      const double dx = (d.xmax - d.xmin) / (double)(float)d.x_cells;
+      const double dy = (d.ymax - d.ymin) / (double)(float)d.y_cells;
+      const double dz = (d.zmax - d.zmin) / (double)(float)d.z_cells;
+      const double xmin = d.xmin + dx * (double)(float)0;
+      const double ymin = d.ymin + dy * (double)(float)0;
+      const double zmin = d.zmin + dz * (double)(float)0;
+      launch_initialise_chunk(q, stream, xmin, ymin, zmin, dx, dy, dz, vertexx, vertexdx,
+                              vertexy, vertexdy, vertexz, vertexdz, cellx, celldx, celly, celldy,
+                              cellz, celldz, volume, xarea, yarea, zarea);
+      // read_input.f90:293-303 nudge, then generate_chunk
+      StateTable st;
+      st.n = d.number_of_states;
+      for (int k = 0; k < st.n; k++) {
+        st.density[k] = d.state_density[k]; st.energy[k] = d.state_energy[k];
+        st.xvel[k] = d.state_xvel[k]; st.yvel[k] = d.state_yvel[k]; st.zvel[k] = d.state_zvel[k];
+        st.xmin[k] = d.state_xmin[k]; st.xmax[k] = d.state_xmax[k];
+        st.ymin[k] = d.state_ymin[k]; st.ymax[k] = d.state_ymax[k];
+        st.zmin[k] = d.state_zmin[k]; st.zmax[k] = d.state_zmax[k];
+        st.radius[k] = d.state_radius[k];
+        st.geometry[k] = d.state_geometry[k];
+        if (k >= 1) {
+          st.xmin[k] = st.xmin[k] + (dx / 100.0);
+          st.ymin[k] = st.ymin[k] + (dy / 100.0);
+          st.zmin[k] = st.zmin[k] + (dz / 100.0);
+          st.xmax[k] = st.xmax[k] - (dx / 100.0);
+          st.ymax[k] = st.ymax[k] - (dy / 100.0);
+          st.zmax[k] = st.zmax[k] - (dz / 100.0);
+        }
+      }
+      launch_generate_chunk<S>(q, stream, ga, density0, energy0, xvel0, yvel0, zvel0, st);
+    }
     // start.f90:109-136
-    launch_ideal_gas<S>(g, stream, density0, energy0, pressure, soundspeed);
+    launch_ideal_gas<S>(tg, stream, density0, energy0, pressure, soundspeed);
     halo({1, 3, 5, 6, 2, 4, 8, 10, 12, 9, 11, 13}, 2);
+    host_step = 0;
+    advect_x = true;
+    sum_steps.clear();
     summary(0);
-    if (cudaStreamSynchronize(stream) != cudaSuccess || cudaGetLastError() != cudaSuccess) {
+    if (cudaStreamSynchronize(stream) != cudaSuccess || cudaGetLastError() != cudaSuccess ||
+        (plan && plan->failed)) {
       g_last_error = "chunk set-up failed on the device";
       return false;
     }
     return true;
+  }
+
+  // Zero every array and set the decks up again (after autotuning, whose
+  // trial steps advance the state). The schedules stay; the graphs are
+  // captured again.
+  bool reset() {
+    cudaStreamSynchronize(stream);
+    for (auto& gr : graph)
+      if (gr) { cudaGraphExecDestroy(gr); gr = nullptr; }
+    for (const Owned& o : owned) cudaMemsetAsync(o.p, 0, o.bytes, stream);
+    warm[0] = warm[1] = false;
+    return initial_state();
+  }
+
+  // The autotuner: per batched launch (key), the item order and grid size,
+  // then the segment length of the marching kernels, that run fastest. Each
+  // candidate runs one untimed and trial_steps timed eager steps with every
+  // batched launch bracketed by events; the fastest candidate per key is
+  // kept. Trial steps advance the decks, so the ensemble is reset to its
+  // initial state afterwards. Results do not depend on the schedule.
+  int autotune(int trial_steps) {
+    if (!plan) return -1;
+    if (trial_steps < 1) trial_steps = 1;
+    const bool prof = profile;
+    profile = false;
+    plan->timing = true;
+    std::map<unsigned, std::pair<double, SchedCfg>> best;
+    auto trial = [&](SchedCfg c) {
+      plan->trial = c;
+      plan->trial_active = true;
+      step(1);
+      cudaStreamSynchronize(stream);
+      plan->collect_marks();
+      step(trial_steps);
+      for (auto& kv : plan->collect_marks()) {
+        const SchedCfg eff = plan->cfg_for(kv.first);
+        auto it = best.find(kv.first);
+        if (it == best.end() || kv.second < it->second.first) best[kv.first] = {kv.second, eff};
+      }
+    };
+    const int orders[3] = {0, 1, 2}, divs[4] = {0, 1, 2, 4}, segs[4] = {8, 16, 32, 64};
+    for (int o : orders)
+      for (int dv : divs) trial(SchedCfg{o, dv, -1});
+    for (auto& kv : best) plan->tuned[kv.first] = kv.second.second;
+    for (int sg : segs) trial(SchedCfg{-1, -1, sg});
+    for (auto& kv : best) plan->tuned[kv.first] = kv.second.second;
+    plan->trial_active = false;
+    plan->timing = false;
+    profile = prof;
+    const bool ok = reset() && !plan->failed;
+    return ok ? (int)plan->tuned.size() : -1;
+  }
+
+  // One line per batched launch: key, order, grid divisor, segment, blocks,
+  // items.
+  std::string schedule_report() const {
+    std::string out;
+    if (!plan) return out;
+    for (auto& kv : plan->seg_tunable) {
+      const SchedCfg c = plan->cfg_for(kv.first);
+      int grid = 0, n = 0, a = 0;
+      for (auto& e : plan->cache)
+        if ((unsigned)e.first[0] == kv.first && e.first[1] == c.order && e.first[2] == c.grid_div &&
+            (!kv.second || c.seg <= 0 || e.first[3] == c.seg)) {
+          grid = e.second.grid; n = e.second.n; a = e.second.aux;
+        }
+      char line[160];
+      snprintf(line, sizeof(line), "%u %d %d %d %d %d\n", kv.first, c.order, c.grid_div,
+               kv.second ? a : 0, grid, n);
+      out += line;
+    }
+    return out;
   }
 
   // field_summary.f90:55-108, recorded at the given step
@@ -325,9 +474,14 @@ struct Chunk : ChunkBase {
     const int idx = (int)sum_steps.size();
     if (idx >= sum_cap) return;
     pbeg();
-    launch_ideal_gas<S>(g, stream, density0, energy0, pressure, soundspeed);
-    launch_field_summary<S>(g, stream, volume, density0, energy0, pressure, xvel0, yvel0, zvel0,
-                            partials, sum_hist + 5 * idx);
+    launch_ideal_gas<S>(tg, stream, density0, energy0, pressure, soundspeed);
+    if (plan)
+      launch_field_summary_batch<S>(plan, nd, stream, plane_base, volume, density0, energy0,
+                                    pressure, xvel0, yvel0, zvel0, partials,
+                                    sum_hist + (size_t)5 * nd * idx);
+    else
+      launch_field_summary<S>(g, stream, volume, density0, energy0, pressure, xvel0, yvel0,
+                              zvel0, partials, sum_hist + 5 * idx);
     pend("field_summary", cells() * (2 * sizeof(R) + 2 * sizeof(En) + 3 * sizeof(C) +
                                      sizeof(double) + 3 * sizeof(V)));
     sum_steps.push_back(step);
@@ -341,40 +495,39 @@ struct Chunk : ChunkBase {
                  VF8 = sizeof(VF), MF8 = sizeof(MF), W8 = sizeof(W), G8 = sizeof(double);
     int vc = ax ? 0 : 1;  // buffer of the velocity pairs at the start of this step
     // timestep.f90:56-126
-    k_dt_prepare<<<1, 1, 0, stream>>>(sc, min_key_of(kGBig));
+    k_dt_prepare<<<deck_blocks(), 128, 0, stream>>>(sc, nd, min_key_of(kGBig));
     pbeg();
-    launch_ideal_gas<S>(g, stream, density0, energy0, pressure, soundspeed);
+    launch_ideal_gas<S>(tg, stream, density0, energy0, pressure, soundspeed);
     pend("ideal_gas", n * (R8 + E8 + 2 * C8));
     pbeg();
     halo({5, 3, 1, 8, 10}, 1, vc);
     pend("update_halo", 0);
     pbeg();
-    launch_timestep_visc<S>(g, stream, ga, density0, pressure, viscosity, xvel0, yvel0, zvel0);
+    launch_timestep_visc<S>(tg, stream, ga, density0, pressure, viscosity, xvel0, yvel0, zvel0);
     pend("viscosity", n * (3 * V8 + 3 * G8 + C8));
     pbeg();
     halo({6}, 1, vc);
     pend("update_halo", 0);
     pbeg();
-    launch_calc_dt<S>(g, stream, ga, kGSmall, deck.dtc_safe, deck.dtu_safe, deck.dtv_safe,
+    launch_calc_dt<S>(tg, stream, ga, kGSmall, deck.dtc_safe, deck.dtu_safe, deck.dtv_safe,
                       deck.dtw_safe, deck.dtdiv_safe, density0, viscosity, soundspeed, xvel0,
                       yvel0, zvel0, (W*)nullptr, &sc->key);
-    k_dt_finalize<<<1, 1, 0, stream>>>(sc, dt_hist, deck.timestep_rise, deck.max_timestep,
-                                       deck.dtmin);
+    k_dt_finalize<<<deck_blocks(), 128, 0, stream>>>(sc, nd, dt_hist);
     pend("calc_dt", n * (4 * G8 + R8 + 2 * C8 + 3 * V8));
     // PdV.f90:50-107: predictor + EOS on the predicted state; revert is implied
     pbeg();
-    launch_pdv_predict_eos<S>(g, stream, dtp, ga, density0, energy0, pressure, viscosity, xvel0,
+    launch_pdv_predict_eos<S>(tg, stream, dtp, ga, density0, energy0, pressure, viscosity, xvel0,
                               yvel0, zvel0);
     pend("pdv", n * (4 * G8 + R8 + E8 + 3 * C8 + 3 * V8));
     pbeg();
     halo({5}, 1, vc);
     pend("update_halo", 0);
     pbeg();
-    launch_accelerate<S>(g, stream, 0.0, dtp, ga, density0, pressure, viscosity, xvel0, yvel0,
+    launch_accelerate<S>(tg, stream, 0.0, dtp, ga, density0, pressure, viscosity, xvel0, yvel0,
                          zvel0, vel1(0, vc), vel1(1, vc), vel1(2, vc));
     pend("accelerate", n * (4 * G8 + R8 + 2 * C8 + 6 * V8));
     pbeg();
-    launch_pdv_flux<S>(g, stream, dtp, ga, density0, density1, energy0, energy1, pressure,
+    launch_pdv_flux<S>(tg, stream, dtp, ga, density0, density1, energy0, energy1, pressure,
                        viscosity, xvel0, vel1(0, vc), yvel0, vel1(1, vc), zvel0, vel1(2, vc),
                        vol_flux_x, vol_flux_y, vol_flux_z);
     pend("pdv_flux", n * (4 * G8 + 2 * R8 + 2 * E8 + 2 * C8 + 6 * V8 + 3 * VF8));
@@ -390,7 +543,7 @@ struct Chunk : ChunkBase {
       // the sweep direction only on sweep 3
       const double nvf = sweep_number == 1 ? 3 : sweep_number == 2 ? 2 : 1;
       pbeg();
-      launch_advec_cell_fused<S>(g, stream, axi, dir, sweep_number, ga, density1, energy1,
+      launch_advec_cell_fused<S>(tg, stream, axi, dir, sweep_number, ga, density1, energy1,
                                  mass_flux_x, vol_flux_x, mass_flux_y, vol_flux_y, mass_flux_z,
                                  vol_flux_z, work[6]);
       // x: face pass + update pass; y, z: one marching pass (in place)
@@ -407,7 +560,7 @@ struct Chunk : ChunkBase {
       V* vin[3] = {vel1(0, vc), vel1(1, vc), vel1(2, vc)};
       V* vout[3] = {vel1(0, vc ^ 1), vel1(1, vc ^ 1), vel1(2, vc ^ 1)};
       pbeg();
-      launch_advec_mom_fused<S>(g, stream, axi, sweep_number, dir, cell_volume, ga, density1, mass_flux_x,
+      launch_advec_mom_fused<S>(tg, stream, axi, sweep_number, dir, cell_volume, ga, density1, mass_flux_x,
                                 mass_flux_y, mass_flux_z, vol_flux_x, vol_flux_y, vol_flux_z,
                                 work[0], work[1], work[2], vin, vout);
       // x: node pass + velocity pass; y, z: one marching pass
@@ -421,15 +574,15 @@ struct Chunk : ChunkBase {
     sweep(2, 2, true);
     sweep(3, ax ? 3 : 1, false);
     pbeg();
-    launch_reset_field<S>(g, stream, density0, density1, energy0, energy1, xvel0, vel1(0, vc),
+    launch_reset_field<S>(tg, stream, density0, density1, energy0, energy1, xvel0, vel1(0, vc),
                           yvel0, vel1(1, vc), zvel0, vel1(2, vc));
     pend("reset_field", n * (2 * R8 + 2 * E8 + 6 * V8));
-    k_step_end<<<1, 1, 0, stream>>>(sc);
+    k_step_end<<<deck_blocks(), 128, 0, stream>>>(sc, nd);
   }
 
   // One hydro step, hydro.f90:52-68 (timestep .. time = time + dt).
   void enqueue_step(bool ax) {
-    if (fused) {
+    if (fused || plan) {
       enqueue_step_fused(ax);
       return;
     }
@@ -438,7 +591,7 @@ struct Chunk : ChunkBase {
     const double R8 = sizeof(R), E8 = sizeof(En), C8 = sizeof(C), V8 = sizeof(V),
                  VF8 = sizeof(VF), MF8 = sizeof(MF), W8 = sizeof(W), G8 = sizeof(double);
     // timestep.f90:56-126
-    k_dt_prepare<<<1, 1, 0, stream>>>(sc, min_key_of(kGBig));
+    k_dt_prepare<<<1, 128, 0, stream>>>(sc, 1, min_key_of(kGBig));
     pbeg();
     launch_ideal_gas<S>(g, stream, density0, energy0, pressure, soundspeed);
     pend("ideal_gas", n * (R8 + E8 + 2 * C8));
@@ -455,8 +608,7 @@ struct Chunk : ChunkBase {
     launch_calc_dt<S>(g, stream, ga, kGSmall, deck.dtc_safe, deck.dtu_safe, deck.dtv_safe,
                       deck.dtw_safe, deck.dtdiv_safe, density0, viscosity, soundspeed, xvel0,
                       yvel0, zvel0, (W*)nullptr, &sc->key);
-    k_dt_finalize<<<1, 1, 0, stream>>>(sc, dt_hist, deck.timestep_rise, deck.max_timestep,
-                                       deck.dtmin);
+    k_dt_finalize<<<1, 128, 0, stream>>>(sc, 1, dt_hist);
     pend("calc_dt", n * (4 * G8 + R8 + 2 * C8 + 3 * V8));
     // PdV.f90:50-107 (predictor), accelerate, PdV (corrector), flux_calc
     pbeg();
@@ -524,10 +676,13 @@ struct Chunk : ChunkBase {
     launch_reset_field<S>(g, stream, density0, density1, energy0, energy1, xvel0, xvel1, yvel0,
                           yvel1, zvel0, zvel1);
     pend("reset_field", n * (2 * R8 + 2 * E8 + 6 * V8));
-    k_step_end<<<1, 1, 0, stream>>>(sc);
+    k_step_end<<<1, 128, 0, stream>>>(sc, 1);
   }
 
+  // An ensemble's schedules are built by eager steps (one per sweep order)
+  // before its graphs are captured: a capture cannot allocate them.
   bool capture_graphs() {
+    if (plan && !(warm[0] && warm[1])) return false;
     for (int i = 0; i < 2; i++) {
       if (graph[i]) continue;
       cudaGraph_t gr;
@@ -535,9 +690,18 @@ struct Chunk : ChunkBase {
         return false;
       const bool prof = profile;
       profile = false;
+      if (plan) {
+        plan->capturing = true;
+        plan->missing = false;
+      }
       enqueue_step(i == 0);
       profile = prof;
+      if (plan) plan->capturing = false;
       if (cudaStreamEndCapture(stream, &gr) != cudaSuccess) return false;
+      if (plan && plan->missing) {
+        cudaGraphDestroy(gr);
+        return false;
+      }
       size_t n = 0;
       cudaGraphGetNodes(gr, nullptr, &n);
       launches_per_step = (int)n;
@@ -548,16 +712,18 @@ struct Chunk : ChunkBase {
   }
 
   int step(int n) {
-    const bool graphs = use_graphs && !profile;
-    if (graphs && !capture_graphs()) {
-      cudaGetLastError();
-      use_graphs = false;
-    }
     for (int i = 0; i < n; i++) {
-      if (graphs && use_graphs)
+      bool graphs = use_graphs && !profile && !(plan && plan->timing);
+      if (graphs && !graph[advect_x ? 0 : 1] && !capture_graphs()) {
+        cudaGetLastError();
+        if (!plan) use_graphs = false;  // an ensemble captures once it is warm
+        graphs = false;
+      }
+      if (graphs)
         cudaGraphLaunch(graph[advect_x ? 0 : 1], stream);
       else
         enqueue_step(advect_x);
+      if (plan && !plan->failed) warm[advect_x ? 0 : 1] = true;
       advect_x = !advect_x;
       host_step++;
       if (deck.summary_frequency != 0 && host_step % deck.summary_frequency == 0)
@@ -566,9 +732,9 @@ struct Chunk : ChunkBase {
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
   }
 
-  DevScalars scalars() {
+  DevScalars scalars(int d = 0) {
     DevScalars h{};
-    cudaMemcpyAsync(&h, sc, sizeof(h), cudaMemcpyDeviceToHost, stream);
+    cudaMemcpyAsync(&h, sc + d, sizeof(h), cudaMemcpyDeviceToHost, stream);
     cudaStreamSynchronize(stream);
     return h;
   }
@@ -576,6 +742,16 @@ struct Chunk : ChunkBase {
   // hydro.f90:46-98 with the end test; runs in batches that cannot overshoot
   // end_time, since dt <= max_timestep.
   int run() {
+    if (plan) {
+      // every deck advances deck 0's end_step steps (no per-deck end_time)
+      if (host_step < deck.end_step && step(deck.end_step - host_step) != 0) return -1000000000;
+      int bad = 0;
+      for (int d = 0; d < nd; d++) bad |= scalars(d).status & CLOVER_STATUS_SMALL_DT;
+      if (bad) return -host_step;
+      summary(host_step);  // the final summary (hydro.f90:87)
+      cudaStreamSynchronize(stream);
+      return host_step;
+    }
     for (;;) {
       DevScalars h = scalars();
       if (h.status & CLOVER_STATUS_SMALL_DT) return -host_step;
@@ -593,8 +769,9 @@ struct Chunk : ChunkBase {
     }
   }
 
-  int read_field(int id, double* host, bool write) {
-    if (id < 1 || id > 19) return -1;
+  int read_field(int id, double* host, bool write, int deck_index = 0) {
+    if (id < 1 || id > 19 || deck_index < 0 || deck_index >= nd) return -1;
+    const Geom& g = geoms[deck_index];
     const int vb = vel1_buffer(host_step);
     void* f[19] = {density0, density1, energy0, energy1, pressure, viscosity, soundspeed,
                    xvel0, vel1(0, vb), yvel0, vel1(1, vb), zvel0, vel1(2, vb), vol_flux_x,
@@ -614,8 +791,8 @@ struct Chunk : ChunkBase {
     std::vector<char> stage((size_t)hx * hy * hz * e);
     cudaMemcpy3DParms q = {};
     cudaPitchedPtr hp = make_cudaPitchedPtr(stage.data(), (size_t)hx * e, (size_t)hx * e, hy);
-    cudaPitchedPtr dp = make_cudaPitchedPtr(f[id - 1], (size_t)g.px * e, (size_t)hx * e,
-                                            (size_t)(g.pxy / g.px));
+    cudaPitchedPtr dp = make_cudaPitchedPtr((char*)f[id - 1] + g.o3 * e, (size_t)g.px * e,
+                                            (size_t)hx * e, (size_t)(g.pxy / g.px));
     q.extent = make_cudaExtent((size_t)hx * e, hy, hz);
     if (write) {
       for (size_t i = 0; i < (size_t)hx * hy * hz; i++) {
@@ -640,7 +817,9 @@ struct Chunk : ChunkBase {
     for (auto e : ev_pool) cudaEventDestroy(e);
     for (int i = 0; i < 2; i++)
       if (graph[i]) cudaGraphExecDestroy(graph[i]);
-    for (void* p : owned) cudaFree(p);
+    for (const Owned& o : owned) cudaFree(o.p);
+    delete plan;
+    cudaFree(plane_base);
     cudaFree(sc);
     cudaFree(dt_hist);
     cudaFree(sum_hist);
@@ -884,10 +1063,10 @@ clover_chunk* clover_chunk_create(const clover_deck* deck, int precision) {
   bool ok;
   if (precision == CLOVER_PRECISION_MIXED) {
     c->mixed = new Chunk<F32Mixed>;
-    ok = c->mixed->create(*deck);
+    ok = c->mixed->create(deck, 1, false);
   } else {
     c->f64 = new Chunk<F64>;
-    ok = c->f64->create(*deck);
+    ok = c->f64->create(deck, 1, false);
   }
   if (!ok) {
     if (g_last_error.empty()) g_last_error = "chunk creation failed";
@@ -930,6 +1109,8 @@ int clover_chunk_dt_history(clover_chunk* c, double* out, int cap) {
 }
 
 int clover_chunk_summaries(clover_chunk* c, double* out5, int* steps, int cap) {
+  if (c->f64 ? c->f64->plan != nullptr : c->mixed->plan != nullptr)
+    return clover_ensemble_summaries(c, 0, out5, steps, cap);
   clover_chunk_sync(c);
   const std::vector<int>& ss = c->f64 ? c->f64->sum_steps : c->mixed->sum_steps;
   const double* src = c->f64 ? c->f64->sum_hist : c->mixed->sum_hist;
@@ -988,6 +1169,110 @@ int clover_chunk_launches_per_step(clover_chunk* c) {
   if (c->f64) { c->f64->capture_graphs(); return c->f64->launches_per_step; }
   c->mixed->capture_graphs();
   return c->mixed->launches_per_step;
+}
+
+// ---- ensembles ----
+clover_chunk* clover_ensemble_create(const clover_deck* decks, int n_decks, int precision) {
+  g_last_error.clear();
+  if (!decks || n_decks < 1) {
+    g_last_error = "an ensemble needs at least one deck";
+    return nullptr;
+  }
+  for (int i = 0; i < n_decks; i++) {
+    const clover_deck& d = decks[i];
+    if (d.number_of_states < 1 || d.number_of_states > CLOVER_MAX_STATES) {
+      g_last_error = "deck needs 1..16 states";
+      return nullptr;
+    }
+    if (d.x_cells < 1 || d.y_cells < 1 || d.z_cells < 1) {
+      g_last_error = "deck needs at least one cell per axis";
+      return nullptr;
+    }
+    // one step sequence for all decks: calc_dt's safety factors, the step
+    // count and the summary cadence are shared
+    const clover_deck& a = decks[0];
+    if (d.end_step != a.end_step || d.summary_frequency != a.summary_frequency ||
+        d.dtc_safe != a.dtc_safe || d.dtu_safe != a.dtu_safe || d.dtv_safe != a.dtv_safe ||
+        d.dtw_safe != a.dtw_safe || d.dtdiv_safe != a.dtdiv_safe) {
+      g_last_error = "ensemble decks must share end_step, summary_frequency and the dt safety factors";
+      return nullptr;
+    }
+  }
+  clover_chunk* c = new clover_chunk;
+  c->precision = precision;
+  bool ok;
+  if (precision == CLOVER_PRECISION_MIXED) {
+    c->mixed = new Chunk<F32Mixed>;
+    ok = c->mixed->create(decks, n_decks, true);
+  } else {
+    c->f64 = new Chunk<F64>;
+    ok = c->f64->create(decks, n_decks, true);
+  }
+  if (!ok) {
+    if (g_last_error.empty()) g_last_error = "ensemble creation failed";
+    clover_chunk_destroy(c);
+    return nullptr;
+  }
+  return c;
+}
+
+int clover_ensemble_decks(clover_chunk* c) { return DISPATCH(c, nd); }
+
+int clover_ensemble_autotune(clover_chunk* c, int trial_steps) {
+  return DISPATCH(c, autotune(trial_steps));
+}
+
+int clover_ensemble_reset(clover_chunk* c) { return DISPATCH(c, reset()) ? 0 : -1; }
+
+int clover_ensemble_schedule(clover_chunk* c, char* buf, int len) {
+  const std::string r = DISPATCH(c, schedule_report());
+  if (buf && len > 0) snprintf(buf, (size_t)len, "%s", r.c_str());
+  return (int)r.size();
+}
+
+int clover_ensemble_status(clover_chunk* c, int deck) {
+  if (deck < 0 || deck >= DISPATCH(c, nd)) return -1;
+  return DISPATCH(c, scalars(deck)).status;
+}
+
+double clover_ensemble_time(clover_chunk* c, int deck) {
+  if (deck < 0 || deck >= DISPATCH(c, nd)) return -1.0;
+  return DISPATCH(c, scalars(deck)).time;
+}
+
+int clover_ensemble_dt_history(clover_chunk* c, int deck, double* out, int cap) {
+  const int nd = DISPATCH(c, nd);
+  if (deck < 0 || deck >= nd) return -1;
+  DevScalars h = DISPATCH(c, scalars(deck));
+  const int dcap = c->f64 ? c->f64->dt_cap : c->mixed->dt_cap;
+  int n = h.step < cap ? h.step : cap;
+  if (n > dcap) n = dcap;
+  const double* src = (c->f64 ? c->f64->dt_hist : c->mixed->dt_hist) + (size_t)deck * dcap;
+  if (n > 0 && cudaMemcpy(out, src, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess)
+    return -1;
+  return n;
+}
+
+int clover_ensemble_summaries(clover_chunk* c, int deck, double* out5, int* steps, int cap) {
+  const int nd = DISPATCH(c, nd);
+  if (deck < 0 || deck >= nd) return -1;
+  clover_chunk_sync(c);
+  const std::vector<int>& ss = c->f64 ? c->f64->sum_steps : c->mixed->sum_steps;
+  const double* src = c->f64 ? c->f64->sum_hist : c->mixed->sum_hist;
+  const bool batched = c->f64 ? c->f64->plan != nullptr : c->mixed->plan != nullptr;
+  int n = (int)ss.size() < cap ? (int)ss.size() : cap;
+  for (int i = 0; i < n; i++) {
+    // batched summaries hold all decks per record; a single chunk one deck
+    const double* rec = src + (batched ? (size_t)5 * ((size_t)i * nd + deck) : (size_t)5 * i);
+    if (cudaMemcpy(out5 + 5 * i, rec, 5 * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess)
+      return -1;
+    steps[i] = ss[i];
+  }
+  return n;
+}
+
+int clover_ensemble_read_field(clover_chunk* c, int deck, int id, double* host) {
+  return DISPATCH(c, read_field(id, host, false, deck));
 }
 
 }  // extern "C"

@@ -107,6 +107,36 @@ int clover_chunk_profile_report(clover_chunk *c, char *names, int name_len, doub
 /* Kernel launches one hydro step issues (graph nodes per step). */
 int clover_chunk_launches_per_step(clover_chunk *c);
 
+/* ---- Ensembles: many independent decks advanced together ----
+ * No counterpart in the reference (which runs one deck per job). The decks
+ * of an ensemble may differ in size, states and timestep controls; each
+ * keeps its own dt, time and calc_dt reduction, and nothing synchronises
+ * one deck with another. Their arrays share one device allocation per
+ * field, and every kernel of the (fused) step runs once over all decks: a
+ * persistent grid of blocks walks a schedule of (deck, tile) items. The
+ * decks must share end_step, summary_frequency and calc_dt's safety factors
+ * (one step sequence); end_time is not applied per deck.
+ * clover_chunk_step/run/sync/stream/profile/use_graphs work on ensembles
+ * (run advances every deck end_step steps); the per-deck results come from
+ * the clover_ensemble_* calls. */
+clover_chunk *clover_ensemble_create(const clover_deck *decks, int n_decks, int precision);
+int clover_ensemble_decks(clover_chunk *c);
+/* Time candidate schedules (item order, grid size, marching segment length)
+ * per batched launch over trial_steps steps each, keep the fastest, then
+ * reset the ensemble to its initial state. Returns the number of launches
+ * tuned, -1 on error. */
+int clover_ensemble_autotune(clover_chunk *c, int trial_steps);
+/* Set every deck up again (step 0); the tuned schedules stay. */
+int clover_ensemble_reset(clover_chunk *c);
+/* The schedule in use, one line per launch: key order grid_div seg blocks
+ * items. Returns the length of the full text. */
+int clover_ensemble_schedule(clover_chunk *c, char *buf, int len);
+int clover_ensemble_status(clover_chunk *c, int deck);
+double clover_ensemble_time(clover_chunk *c, int deck);
+int clover_ensemble_dt_history(clover_chunk *c, int deck, double *out, int cap);
+int clover_ensemble_summaries(clover_chunk *c, int deck, double *out5, int *steps, int cap);
+int clover_ensemble_read_field(clover_chunk *c, int deck, int field_id, double *host);
+
 /* ---- Host driver over the drop-in ABI ----
  * The reference's own control flow (start.f90, hydro.f90, timestep.f90,
  * PdV.f90, advection.f90) over host arrays allocated as build_field.f90
