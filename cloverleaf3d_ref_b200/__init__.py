@@ -166,6 +166,8 @@ def _declare(L):
         getattr(L, n).restype = ctypes.c_int
     L.clover_ensemble_autotune.argtypes = [P, ctypes.c_int]
     L.clover_ensemble_autotune.restype = ctypes.c_int
+    L.clover_ensemble_set_schedule.argtypes = [P, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+    L.clover_ensemble_set_schedule.restype = ctypes.c_int
     L.clover_ensemble_schedule.argtypes = [P, ctypes.c_char_p, ctypes.c_int]
     L.clover_ensemble_schedule.restype = ctypes.c_int
     L.clover_ensemble_status.argtypes = [P, ctypes.c_int]
@@ -402,6 +404,11 @@ class Ensemble(Chunk):
     def reset(self):
         if lib().clover_ensemble_reset(self.h) != 0:
             raise CloverError("ensemble reset failed")
+
+    def set_schedule(self, order=0, grid_div=1, seg=0):
+        """One schedule for every batched launch (replaces tuned ones)."""
+        if lib().clover_ensemble_set_schedule(self.h, order, grid_div, seg) != 0:
+            raise CloverError("bad schedule")
 
     def schedule(self):
         """The schedule in use: one dict per batched launch."""

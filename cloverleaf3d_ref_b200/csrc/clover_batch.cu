@@ -27,7 +27,10 @@ namespace clover {
 
 BatchPlan::~BatchPlan() {
   for (auto& kv : cache) cudaFree(kv.second.items);
-  for (auto& m : marks) { cudaEventDestroy(m.a); cudaEventDestroy(m.b); }
+  for (auto& m : marks) {
+    cudaEventDestroy(m.a);
+    if (m.b) cudaEventDestroy(m.b);
+  }
   for (auto e : ev_pool) cudaEventDestroy(e);
   cudaFree(d_decks);
 }
@@ -39,8 +42,12 @@ bool BatchPlan::init(const std::vector<Geom>& geoms) {
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   if (sms <= 0) sms = 148;
   if (cudaMalloc(&d_decks, decks.size() * sizeof(Geom)) != cudaSuccess) return false;
-  return cudaMemcpy(d_decks, decks.data(), decks.size() * sizeof(Geom), cudaMemcpyHostToDevice) ==
-         cudaSuccess;
+  // a copy from pageable memory may still be in flight when cudaMemcpy
+  // returns, and the kernels run on non-blocking streams: wait for it
+  if (cudaMemcpy(d_decks, decks.data(), decks.size() * sizeof(Geom), cudaMemcpyHostToDevice) !=
+      cudaSuccess)
+    return false;
+  return cudaDeviceSynchronize() == cudaSuccess;
 }
 
 SchedCfg BatchPlan::cfg_for(unsigned key) const {
@@ -84,8 +91,8 @@ std::vector<int4> BatchPlan::make_items(GridFn grid_fn, int aux, int order) cons
   return items;
 }
 
-BatchLaunch batch_launch(BatchPlan* plan, unsigned key, GridFn grid_fn, int aux, bool seg_tunable,
-                         const void* kernel, int threads) {
+BatchLaunch batch_launch(BatchPlan* plan, cudaStream_t s, unsigned key, GridFn grid_fn, int aux,
+                         bool seg_tunable, const void* kernel, int threads) {
   BatchLaunch out{nullptr, plan->d_decks, 0, 0, aux};
   plan->seg_tunable[key] = seg_tunable;
   const SchedCfg c = plan->cfg_for(key);
@@ -115,7 +122,15 @@ BatchLaunch batch_launch(BatchPlan* plan, unsigned key, GridFn grid_fn, int aux,
         plan->failed = true;
         return out;
       }
-      cudaMemcpy(e.items, items.data(), items.size() * sizeof(int4), cudaMemcpyHostToDevice);
+      // ordered before the launch on its stream, and complete before the
+      // host vector goes away
+      if (cudaMemcpyAsync(e.items, items.data(), items.size() * sizeof(int4),
+                          cudaMemcpyHostToDevice, s) != cudaSuccess ||
+          cudaStreamSynchronize(s) != cudaSuccess) {
+        cudaFree(e.items);
+        plan->failed = true;
+        return out;
+      }
     }
     it = plan->cache.emplace(id, e).first;
   }

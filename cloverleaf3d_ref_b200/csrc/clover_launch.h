@@ -54,9 +54,9 @@ struct BatchLaunch {
 // The schedule of one batched launch. key names the launch (kernel and the
 // variant that fixes its grid); seg_tunable says whether aux is a segment
 // length the plan may choose. Builds the schedule on first use (not while a
-// stream is being captured).
-BatchLaunch batch_launch(BatchPlan* plan, unsigned key, GridFn grid_fn, int aux, bool seg_tunable,
-                         const void* kernel, int threads);
+// stream is being captured): its upload is ordered on s and waited for.
+BatchLaunch batch_launch(BatchPlan* plan, cudaStream_t s, unsigned key, GridFn grid_fn, int aux,
+                         bool seg_tunable, const void* kernel, int threads);
 void batch_mark(BatchPlan* plan, unsigned key, cudaStream_t s, bool begin);
 
 struct Target {
@@ -77,7 +77,7 @@ inline void launch_mapped(const Target& tg, cudaStream_t s, unsigned key, GridFn
     if (gr.x && gr.y && gr.z) ks<<<gr, blk, 0, s>>>(MapSingle{tg.g, aux}, std::forward<A>(args)...);
     return;
   }
-  const BatchLaunch bl = batch_launch(tg.plan, key, grid_fn, aux, seg_tunable, (const void*)kb,
+  const BatchLaunch bl = batch_launch(tg.plan, s, key, grid_fn, aux, seg_tunable, (const void*)kb,
                                       (int)(blk.x * blk.y * blk.z));
   if (bl.grid <= 0) return;
   batch_mark(tg.plan, key, s, true);

@@ -314,8 +314,10 @@ struct Chunk : ChunkBase {
     if (ok && plan) {
       ok = cudaMalloc(&p, pb.size() * sizeof(int)) == cudaSuccess;
       plane_base = (int*)p;
-      ok = ok && cudaMemcpy(plane_base, pb.data(), pb.size() * sizeof(int),
-                            cudaMemcpyHostToDevice) == cudaSuccess;
+      // on the chunk's stream and waited for: pb is released at return
+      ok = ok && cudaMemcpyAsync(plane_base, pb.data(), pb.size() * sizeof(int),
+                                 cudaMemcpyHostToDevice, stream) == cudaSuccess &&
+           cudaStreamSynchronize(stream) == cudaSuccess;
     }
     if (!ok) {
       g_last_error = "device allocation failed";
@@ -394,6 +396,14 @@ struct Chunk : ChunkBase {
       g_last_error = "chunk set-up failed on the device";
       return false;
     }
+    return true;
+  }
+
+  bool drop_graphs() {
+    cudaStreamSynchronize(stream);
+    for (auto& gr : graph)
+      if (gr) { cudaGraphExecDestroy(gr); gr = nullptr; }
+    warm[0] = warm[1] = false;
     return true;
   }
 
@@ -1223,6 +1233,15 @@ int clover_ensemble_autotune(clover_chunk* c, int trial_steps) {
 }
 
 int clover_ensemble_reset(clover_chunk* c) { return DISPATCH(c, reset()) ? 0 : -1; }
+
+int clover_ensemble_set_schedule(clover_chunk* c, int order, int grid_div, int seg) {
+  BatchPlan* plan = c->f64 ? c->f64->plan : c->mixed->plan;
+  if (!plan || order < 0 || order > 2 || grid_div < 0 || seg < 0) return -1;
+  plan->tuned.clear();
+  plan->fallback = SchedCfg{order, grid_div, seg};
+  // the graphs hold the old schedule: capture again after eager steps
+  return DISPATCH(c, drop_graphs()) ? 0 : -1;
+}
 
 int clover_ensemble_schedule(clover_chunk* c, char* buf, int len) {
   const std::string r = DISPATCH(c, schedule_report());

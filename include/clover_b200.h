@@ -128,6 +128,11 @@ int clover_ensemble_decks(clover_chunk *c);
 int clover_ensemble_autotune(clover_chunk *c, int trial_steps);
 /* Set every deck up again (step 0); the tuned schedules stay. */
 int clover_ensemble_reset(clover_chunk *c);
+/* One schedule for every batched launch instead of the tuned ones: item
+ * order (0 deck order, 1 largest deck first, 2 round robin), grid_div (0 one
+ * block per item, n: resident blocks / n), seg (marching segment length, 0
+ * the default). */
+int clover_ensemble_set_schedule(clover_chunk *c, int order, int grid_div, int seg);
 /* The schedule in use, one line per launch: key order grid_div seg blocks
  * items. Returns the length of the full text. */
 int clover_ensemble_schedule(clover_chunk *c, char *buf, int len);

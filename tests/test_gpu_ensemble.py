@@ -125,6 +125,30 @@ def test_mixed_ensemble_matches_mixed_chunks_and_fp64():
     fp64.close()
 
 
+@pytest.mark.parametrize("sched", [(0, 0, 0), (0, 1, 0), (2, 2, 16), (1, 4, 8)])
+def test_large_decks_every_schedule_bitwise(sched):
+    """Decks large enough that every block of a persistent grid walks many
+    items (and item lists take a while to upload), under one block per item,
+    full and partial persistent grids, every item order and several segment
+    lengths: each deck equals the same deck run alone."""
+    ds = C.draw_decks(4, seed=31, cells=(56, 96), end_step=4, summary_frequency=2)
+    ens = C.Ensemble(ds)
+    ens.set_schedule(*sched)
+    ens.step(4)
+    ens.sync()
+    for i, d in enumerate(ds):
+        ch = C.Chunk(d)
+        ch.step(4)
+        assert np.array_equal(ens.deck_dt_history(i), ch.dt_history())
+        for n in O.FIELD_NAMES:
+            assert np.array_equal(ens.deck_field(i, n), ch.field(n)), (i, n)
+        a, _ = ens.deck_summaries(i)
+        b, _ = ch.summaries()
+        np.testing.assert_allclose(a, b, rtol=SUMMARY_RTOL, atol=0)
+        ch.close()
+    ens.close()
+
+
 def test_deck_status_is_per_deck():
     """A deck whose dtmin lies above its dt is flagged; the others are not."""
     ds = C.draw_decks(3, seed=2, cells=(6, 12), end_step=4, summary_frequency=2)
