@@ -8,9 +8,10 @@
 // density/energy) live in registers, dead writes are dropped, and passes that
 // read the same inputs are merged.
 //
-//  k_timestep_visc   viscosity with the compression test first: where the
+//  k_visc_dt         viscosity with the compression test first (where the
 //                    divergence is non-negative the viscosity is zero whatever
-//                    the limiter, so the thirteen divisions are skipped.
+//                    the limiter, so its thirteen divisions are skipped), then
+//                    calc_dt on the same cell and the per-deck minimum.
 //  k_pdv_predict_eos PdV predictor + ideal_gas on the predicted state; only
 //                    the pressure is stored (revert then restores time level
 //                    0, and the corrector overwrites density1/energy1).
@@ -18,7 +19,8 @@
 //  k_cell_flux_f     advec_cell x face pass with pre_vol from the volume fluxes.
 //  k_cell_update_f   advec_cell x update pass, pre_vol recomputed, in place.
 //  k_cell_sweep_march  the whole y or z cell sweep in one pass, each thread
-//                    marching its column with the stencil in registers.
+//                    marching a segment of a column with the stencil in
+//                    registers (the segments of a column share a block).
 //  k_mom_sweep_x     the whole x momentum sweep (three velocities) in one pass:
 //                    neighbouring nodes along x through warp shuffles, the
 //                    previous z plane in registers.
@@ -107,19 +109,28 @@ __device__ __forceinline__ double fmin2(double a, double b) { return b < a ? b :
 __device__ __forceinline__ double fmax2(double a, double b) { return b > a ? b : a; }
 
 // ---------------------------------------------------------------------------
-// viscosity_kernel.f90:71-134 with IF((limiter.GT.0.0).OR.(div.GE.0.0)) taken
-// as "div >= 0 -> 0, else limiter > 0 -> 0, else ..." (the same outcome).
+// viscosity_kernel.f90:71-134 followed by calc_dt_kernel.f90:102-149 on the
+// same cell: both read the cell's 24 corner velocities, its face areas and
+// density, and calc_dt reads the viscosity of its own cell only, so it needs
+// no halo of the viscosity just computed. The viscosity's
+// IF((limiter.GT.0.0).OR.(div.GE.0.0)) is taken as "div >= 0 -> 0, else
+// limiter > 0 -> 0, else ..." (the same outcome). The cell minimum folds into
+// deck d's key at min_key[d * kScalarStride] (warp, block, one atomic).
 template <class S, class M>
-__global__ void __launch_bounds__(BX * BY, 4) k_timestep_visc(M m, GeomArrays ga,
+__global__ void __launch_bounds__(BX * BY, 3) k_visc_dt(M m, GeomArrays ga, double g_small,
+    double dtc_safe, double dtu_safe, double dtv_safe, double dtw_safe, double dtdiv_safe,
     const typename S::rho_t* __restrict__ density0, const typename S::cs_t* __restrict__ pressure,
-    typename S::cs_t* __restrict__ viscosity, const typename S::vel_t* __restrict__ xvel0,
-    const typename S::vel_t* __restrict__ yvel0, const typename S::vel_t* __restrict__ zvel0) {
+    typename S::cs_t* __restrict__ viscosity, const typename S::cs_t* __restrict__ soundspeed,
+    const typename S::vel_t* __restrict__ xvel0, const typename S::vel_t* __restrict__ yvel0,
+    const typename S::vel_t* __restrict__ zvel0, unsigned long long* __restrict__ min_key) {
+  __shared__ unsigned long long wmin[BX * BY / 32];
   m.run([&](const Geom& g, const Tile& t) {
   const Box b = interior(g);
   const int j = b.j0 + t.x * BX + threadIdx.x;
   const int k = b.k0 + t.y * BY + threadIdx.y;
   const int l = b.l0 + t.z;
-  if (j > b.j1 || k > b.k1) return;
+  unsigned long long key = ~0ull;
+  if (j <= b.j1 && k <= b.k1) {
   const double u000 = L(xvel0, j, k, l), u100 = L(xvel0, j + 1, k, l);
   const double u010 = L(xvel0, j, k + 1, l), u110 = L(xvel0, j + 1, k + 1, l);
   const double u001 = L(xvel0, j, k, l + 1), u101 = L(xvel0, j + 1, k, l + 1);
@@ -139,9 +150,9 @@ __global__ void __launch_bounds__(BX * BY, 4) k_timestep_visc(M m, GeomArrays ga
   const double vgrady2 = v010 + v110 + v011 + v111;
   const double wgradz1 = w000 + w100 + w010 + w110;
   const double wgradz2 = w001 + w101 + w011 + w111;
-  const double div = (E(ga.xarea, j, k, l) * (ugradx2 - ugradx1) +
-                      E(ga.yarea, j, k, l) * (vgrady2 - vgrady1)) +
-                     E(ga.zarea, j, k, l) * (wgradz2 - wgradz1);
+  const double xa = E(ga.xarea, j, k, l), ya = E(ga.yarea, j, k, l), za = E(ga.zarea, j, k, l);
+  const double div = (xa * (ugradx2 - ugradx1) + ya * (vgrady2 - vgrady1)) +
+                     za * (wgradz2 - wgradz1);
   double q = 0.0;
   if (!(div >= 0.0)) {
     const double ugrady1 = u000 + u100 + u001 + u101;
@@ -185,7 +196,50 @@ __global__ void __launch_bounds__(BX * BY, 4) k_timestep_visc(M m, GeomArrays ga
       q = 2.0 * L(density0, j, k, l) * grad2 * limiter * limiter;
     }
   }
-  E(viscosity, j, k, l) = st<typename S::cs_t>(q);
+  using C = typename S::cs_t;
+  E(viscosity, j, k, l) = st<C>(q);
+  // calc_dt_kernel.f90:102-149 (the viscosity as stored)
+  const double visc = (double)st<C>(q);
+  const double d0 = L(density0, j, k, l);
+  const double mcd = fmin2(fmin2(GX(ga.celldx, j), GY(ga.celldy, k)), GZ(ga.celldz, l));
+  const double ds = 1.0 / (mcd * mcd);
+  const double ss = L(soundspeed, j, k, l);
+  double cc = ss * ss;
+  cc = cc + 2.0 * visc / d0;
+  double dtct = ds * cc;
+  dtct = dtc_safe * 1.0 / fmax2(sqrt(dtct), g_small);
+  const double vol = E(ga.volume, j, k, l);
+  const double du1 = ugradx1 * xa, du2 = ugradx2 * xa;
+  const double dtut = dtu_safe * 4.0 * vol / fmax2(fmax2(fabs(du1), fabs(du2)), 1.0e-5 * vol);
+  const double dv1 = vgrady1 * ya, dv2 = vgrady2 * ya;
+  const double dtvt = dtv_safe * 4.0 * vol / fmax2(fmax2(fabs(dv1), fabs(dv2)), 1.0e-5 * vol);
+  // both z faces use zarea(j,k,l); its sums add (j,k+1) before (j+1,k)
+  const double dw1 = (w000 + w010 + w100 + w110) * za;
+  const double dw2 = (w001 + w011 + w101 + w111) * za;
+  const double dtwt = dtw_safe * 4.0 * vol / fmax2(fmax2(fabs(dw1), fabs(dw2)), 1.0e-5 * vol);
+  const double dvg = du2 - du1 + dv2 - dv1 + dw2 - dw1;
+  const double dtdivt = dtdiv_safe * 4.0 * vol / fmax2(vol * 1.0e-05, fabs(dvg));
+  const double mn = fmin2(fmin2(fmin2(fmin2(dtct, dtut), dtvt), dtwt), dtdivt);
+  if (!(mn != mn)) key = key_of(mn);
+  }
+  // warp then block minimum, one atomic per block
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    unsigned long long other = __shfl_xor_sync(0xffffffffu, key, o);
+    key = other < key ? other : key;
+  }
+  const int lane = threadIdx.x, warp = threadIdx.y;
+  if (lane == 0) wmin[warp] = key;
+  __syncthreads();
+  if (warp == 0) {
+    key = lane < BX * BY / 32 ? wmin[lane] : ~0ull;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      unsigned long long other = __shfl_xor_sync(0xffffffffu, key, o);
+      key = other < key ? other : key;
+    }
+    if (lane == 0 && key != ~0ull) atomicMin(min_key + (long long)t.d * kScalarStride, key);
+  }
   });
 }
 
@@ -673,31 +727,56 @@ __global__ void __launch_bounds__(BX * BY, 3) k_mom_vel3_march(M m, GeomArrays g
 }
 
 // ---------------------------------------------------------------------------
-// advec_cell sweep along y or z as ONE pass: thread (j, c) walks its whole
-// column along the sweep axis p (k for DIR 2, l for DIR 3) from the first face
-// to the last, holding the old density/energy of cells p-2..p+1 and the
-// pre-volumes of cells p-1, p in registers, so the donor/upwind selection
-// needs no dependent loads; cell p-1 is updated as soon as face p is known
-// (in place: no other thread reads this column's density or energy).
-// Faces p in [pmin, pmax+2] (c up to chi), cells p in [pmin, pmax] (c <= cmax).
+// advec_cell sweep along y or z as ONE pass. A block holds 32 columns j of
+// one cross-axis index c and splits the sweep axis p (k for DIR 2, l for
+// DIR 3) into BY segments, one per threadIdx.y. Each thread walks its segment
+// [c0, c1] face by face, holding the old density/energy of cells p-2..p+1
+// and the pre-volumes of cells p-1, p in registers, so the donor/upwind
+// selection needs no dependent loads, and updates cell p-1 in place as soon
+// as face p is known. The faces at a segment's ends read two old cells of
+// each neighbouring segment, which those segments overwrite: every thread
+// reads them (c0-2, c0-1, c1+1, c1+2) before the block's barrier, and only
+// then does any thread write. Faces p in [pmin, pmax+2] (c up to chi), cells p
+// in [pmin, pmax] (c <= cmax); face c1+1 is computed by both neighbours and
+// stored by the segment that starts there.
 template <class S, int DIR, class M>
 __global__ void __launch_bounds__(BX * BY, 3) k_cell_sweep_march(M m, int variant, GeomArrays ga,
     typename S::rho_t* __restrict__ density1, typename S::ene_t* __restrict__ energy1,
     const typename S::vf_t* __restrict__ vfx, const typename S::vf_t* __restrict__ vfy,
     const typename S::vf_t* __restrict__ vfz, typename S::mf_t* __restrict__ mass_flux) {
+  // old density/energy of cells c1+1, c1+2 of each thread's segment
+  __shared__ double s_end[4][BY][BX];
   m.run([&](const Geom& g, const Tile& t) {
   const MarchRange r = cell_sweep_range<DIR>(g);
-  const int jlo = r.jlo, jhi = r.jhi, clo = r.clo, chi = r.chi, cmax = r.cmax;
-  const int j = jlo + t.x * BX + threadIdx.x;
-  const int c = clo + t.y * BY + threadIdx.y;
-  if (j > jhi || c > chi) return;
-#define IDX(p) j, (DIR == 2 ? (p) : c), (DIR == 2 ? c : (p))
-  const typename S::vf_t* vf_d = DIR == 2 ? vfy : vfz;
+  const int j = r.jlo + t.x * BX + threadIdx.x;
+  const int c = r.clo + t.y;
   const int pmin = DIR == 2 ? g.y_min : g.z_min;
   const int pmax = DIR == 2 ? g.y_max : g.z_max;
+  const int len = (pmax - pmin + 1 + BY - 1) / BY;  // cells per segment
+  const int c0 = pmin + (int)threadIdx.y * len;
+  const int c1 = c0 + len - 1 < pmax ? c0 + len - 1 : pmax;
+  const bool active = j <= r.jhi && c <= r.chi && c0 <= pmax;
+  const bool last = c1 == pmax;  // this segment also walks the faces pmax+1, pmax+2
+#define IDX(p) j, (DIR == 2 ? (p) : c), (DIR == 2 ? c : (p))
+  const int top = pmax + 2;
+  // old values at the segment's ends (cells of the neighbouring segments)
+  double d0 = 0.0, d1 = 0.0, e0 = 0.0, e1 = 0.0;
+  const int ty = threadIdx.y, tx = threadIdx.x;
+  if (active) {
+    d0 = LI(density1, IDX(c0 - 2)); d1 = LI(density1, IDX(c0 - 1));
+    e0 = LI(energy1, IDX(c0 - 2)); e1 = LI(energy1, IDX(c0 - 1));
+    const int q1 = c1 + 1 < top ? c1 + 1 : top, q2 = c1 + 2 < top ? c1 + 2 : top;
+    s_end[0][ty][tx] = LI(density1, IDX(q1));
+    s_end[1][ty][tx] = LI(density1, IDX(q2));
+    s_end[2][ty][tx] = LI(energy1, IDX(q1));
+    s_end[3][ty][tx] = LI(energy1, IDX(q2));
+  }
+  __syncthreads();
+  if (!active) return;
+  const typename S::vf_t* vf_d = DIR == 2 ? vfy : vfz;
   const double* vd = DIR == 2 ? ga.vertexdy : ga.vertexdz;
 #define VD(p) vd[g.o1 + (p) - pmin + 2]
-  const bool update = c <= cmax;
+  const bool update = c <= r.cmax;
   using R = typename S::rho_t;
   using En = typename S::ene_t;
   using MF = typename S::mf_t;
@@ -705,17 +784,23 @@ __global__ void __launch_bounds__(BX * BY, 3) k_cell_sweep_march(M m, int varian
     return cell_pre_vol<S>(g, variant, ga, vfx, vfy, vfz, IDX(p));
   };
   // window: d0..d3 = density1(p-2..p+1), e0..e3 = energy1(p-2..p+1), old values
-  double d0 = LI(density1, IDX(pmin - 2)), d1 = LI(density1, IDX(pmin - 1));
-  double d2 = LI(density1, IDX(pmin)), d3;
-  double e0 = LI(energy1, IDX(pmin - 2)), e1 = LI(energy1, IDX(pmin - 1));
-  double e2 = LI(energy1, IDX(pmin)), e3;
-  double pv_m = prevol(pmin - 1), pv_0;  // pre_vol(p-1), pre_vol(p)
+  double d2 = LI(density1, IDX(c0)), d3;
+  double e2 = LI(energy1, IDX(c0)), e3;
+  double pv_m = prevol(c0 - 1), pv_0;  // pre_vol(p-1), pre_vol(p)
   double vf_prev = 0.0, mf_prev = 0.0, ef_prev = 0.0;
-  for (int p = pmin; p <= pmax + 2; p++) {
-    // cell p+1 is read by face p (the upwind index clamps to pmax+2 at the top)
-    const int pn = p + 1 <= pmax + 2 ? p + 1 : pmax + 2;
-    d3 = LI(density1, IDX(pn));
-    e3 = LI(energy1, IDX(pn));
+  const int pend = last ? top : c1 + 1;
+  for (int p = c0; p <= pend; p++) {
+    // cell p+1 is read by face p (the upwind index clamps to pmax+2 at the top);
+    // beyond c1 it comes from the values read before the barrier
+    const int pn = p + 1 <= top ? p + 1 : top;
+    if (pn <= c1) {
+      d3 = LI(density1, IDX(pn));
+      e3 = LI(energy1, IDX(pn));
+    } else {
+      const int w = pn == c1 + 1 ? 0 : 1;
+      d3 = s_end[w][ty][tx];
+      e3 = s_end[2 + w][ty][tx];
+    }
     pv_0 = prevol(p);
     const double vf = LI(vf_d, IDX(p));
     // advec_cell_kernel.f90:226-264 (y) / :321-359 (z) at face p
@@ -726,7 +811,7 @@ __global__ void __launch_bounds__(BX * BY, 3) k_cell_sweep_march(M m, int varian
       dif = p - 1;
     } else {  // upwind min(p+1, pmax+2), donor p, downwind p-1
       d_up = d3; d_don = d2; d_dn = d1; e_up = e3; e_don = e2; e_dn = e1; pv_don = pv_0;
-      dif = p + 1 < pmax + 2 ? p + 1 : pmax + 2;
+      dif = p + 1 < top ? p + 1 : top;
     }
     const double sigmat = fabs(vf) / pv_don;
     const double sigma3 = (1.0 + sigmat) * (VD(p) / VD(dif));
@@ -735,7 +820,7 @@ __global__ void __launch_bounds__(BX * BY, 3) k_cell_sweep_march(M m, int varian
     double diffdw = d_dn - d_don;
     double limiter = cell_limiter(sigmat, sigma3, sigma4, diffuw, diffdw);
     const double mflux = vf * (d_don + limiter);
-    EI(mass_flux, IDX(p)) = st<MF>(mflux);
+    if (p <= c1 || last) EI(mass_flux, IDX(p)) = st<MF>(mflux);
     const double mf_stored = (double)st<MF>(mflux);
     const double sigmam = fabs(mflux) / (d_don * pv_don);
     diffuw = e_don - e_up;
@@ -743,7 +828,7 @@ __global__ void __launch_bounds__(BX * BY, 3) k_cell_sweep_march(M m, int varian
     limiter = cell_limiter(sigmam, sigma3, sigma4, diffuw, diffdw);
     const double eflux = (double)st<typename S::wk_t>(mflux * (e_don + limiter));
     // advec_cell_kernel.f90:270-281 (y) / :365-376 (z) for cell p-1
-    if (update && p - 1 >= pmin && p - 1 <= pmax) {
+    if (update && p - 1 >= c0 && p - 1 <= c1) {
       const double pm = d1 * pv_m;
       const double pom = pm + mf_prev - mf_stored;
       const double poe = (e1 * pm + ef_prev - eflux) / pom;
@@ -875,10 +960,11 @@ constexpr int kMarchSeg = 32;
 dim3 grid_interior(const Geom& g, int) { return grid_of(interior(g)); }
 dim3 grid_nodes(const Geom& g, int) { return grid_of(nodes(g)); }
 dim3 grid_cell_flux_x(const Geom& g, int) { return grid_of(cell_flux_box<1>(g)); }
+// 32 columns j of one cross-axis index per block, BY segments along the sweep
 template <int DIR>
 dim3 grid_cell_sweep(const Geom& g, int) {
   const MarchRange r = cell_sweep_range<DIR>(g);
-  return dim3((r.jhi - r.jlo + 1 + BX - 1) / BX, (r.chi - r.clo + 1 + BY - 1) / BY, 1);
+  return dim3((r.jhi - r.jlo + 1 + BX - 1) / BX, r.chi - r.clo + 1, 1);
 }
 template <int DIR>
 dim3 grid_mom_node(const Geom& g, int seg) {
@@ -907,13 +993,17 @@ dim3 grid_shell(const Geom& g, int) {
 const dim3 kBlk(BX, BY);
 
 template <class S>
-void launch_timestep_visc(const Target& tg, cudaStream_t s, const GeomArrays& ga,
-                          const typename S::rho_t* density0, const typename S::cs_t* pressure,
-                          typename S::cs_t* viscosity, const typename S::vel_t* xvel0,
-                          const typename S::vel_t* yvel0, const typename S::vel_t* zvel0) {
-  launch_mapped(tg, s, kKeyTimestepVisc, grid_interior, 0, false, kBlk,
-                k_timestep_visc<S, MapSingle>, k_timestep_visc<S, MapBatch>, ga, density0,
-                pressure, viscosity, xvel0, yvel0, zvel0);
+void launch_visc_dt(const Target& tg, cudaStream_t s, const GeomArrays& ga, double g_small,
+                    double dtc_safe, double dtu_safe, double dtv_safe, double dtw_safe,
+                    double dtdiv_safe, const typename S::rho_t* density0,
+                    const typename S::cs_t* pressure, typename S::cs_t* viscosity,
+                    const typename S::cs_t* soundspeed, const typename S::vel_t* xvel0,
+                    const typename S::vel_t* yvel0, const typename S::vel_t* zvel0,
+                    unsigned long long* min_key) {
+  launch_mapped(tg, s, kKeyTimestepVisc, grid_interior, 0, false, kBlk, k_visc_dt<S, MapSingle>,
+                k_visc_dt<S, MapBatch>, ga, g_small, dtc_safe, dtu_safe, dtv_safe, dtw_safe,
+                dtdiv_safe, density0, pressure, viscosity, soundspeed, xvel0, yvel0, zvel0,
+                min_key);
 }
 
 template <class S>
@@ -1024,9 +1114,10 @@ void launch_advec_mom_fused(const Target& tg, cudaStream_t s, int advect_x, int 
 }
 
 #define INSTF(S)                                                                               \
-  template void launch_timestep_visc<S>(const Target&, cudaStream_t, const GeomArrays&,          \
-                                        const S::rho_t*, const S::cs_t*, S::cs_t*,             \
-                                        const S::vel_t*, const S::vel_t*, const S::vel_t*);    \
+  template void launch_visc_dt<S>(const Target&, cudaStream_t, const GeomArrays&, double, double,  \
+                                  double, double, double, double, const S::rho_t*,             \
+                                  const S::cs_t*, S::cs_t*, const S::cs_t*, const S::vel_t*,    \
+                                  const S::vel_t*, const S::vel_t*, unsigned long long*);      \
   template void launch_pdv_predict_eos<S>(const Target&, cudaStream_t, const double*,            \
                                           const GeomArrays&, const S::rho_t*, const S::ene_t*, \
                                           S::cs_t*, const S::cs_t*, const S::vel_t*,           \

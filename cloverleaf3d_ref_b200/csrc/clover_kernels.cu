@@ -183,15 +183,6 @@ __global__ void __launch_bounds__(BX * BY) k_viscosity(Geom g, Box b, GeomArrays
 // calc_dt_kernel.f90:102-149 with the minimum of :141-147 folded into an
 // atomic minimum. Doubles are mapped to an order-preserving 64-bit key, so the
 // atomic gives exactly the serial minimum; NaNs never win, as with .LT..
-__host__ __device__ __forceinline__ unsigned long long key_of(double v) {
-#ifdef __CUDA_ARCH__
-  unsigned long long b = (unsigned long long)__double_as_longlong(v);
-#else
-  unsigned long long b;
-  memcpy(&b, &v, sizeof(b));
-#endif
-  return (b >> 63) ? ~b : (b | 0x8000000000000000ull);
-}
 
 template <class S, class M>
 __global__ void __launch_bounds__(BX * BY) k_calc_dt(M m, GeomArrays ga,

@@ -13,6 +13,7 @@
 
 #include <cuda_runtime.h>
 
+#include <cstring>
 #include <utility>
 
 #include "clover_layout.cuh"
@@ -160,6 +161,18 @@ void launch_calc_dt(const Target& tg, cudaStream_t s, const GeomArrays& ga, doub
                     const typename S::vel_t* zvel0, typename S::wk_t* dt_min_arr,
                     unsigned long long* min_key);
 
+// Doubles mapped to an order-preserving 64-bit key: an atomic minimum over
+// keys gives exactly the serial minimum of the values (NaNs are skipped by
+// the callers, as the reference's .LT. skips them).
+__host__ __device__ __forceinline__ unsigned long long key_of(double v) {
+#ifdef __CUDA_ARCH__
+  unsigned long long b = (unsigned long long)__double_as_longlong(v);
+#else
+  unsigned long long b;
+  memcpy(&b, &v, sizeof(b));
+#endif
+  return (b >> 63) ? ~b : (b | 0x8000000000000000ull);
+}
 unsigned long long min_key_of(double v);
 double min_key_value(unsigned long long key);
 
@@ -269,11 +282,16 @@ void launch_generate_chunk(const Geom& g, cudaStream_t s, const GeomArrays& ga,
                            typename S::vel_t* zvel0, const StateTable& st);
 
 // ---- fused kernels of the native step (clover_fused.cu) ----
+// viscosity and calc_dt of every interior cell in one pass; the cell minimum
+// folds into min_key (per deck over a plan).
 template <class S>
-void launch_timestep_visc(const Target& tg, cudaStream_t s, const GeomArrays& ga,
-                          const typename S::rho_t* density0, const typename S::cs_t* pressure,
-                          typename S::cs_t* viscosity, const typename S::vel_t* xvel0,
-                          const typename S::vel_t* yvel0, const typename S::vel_t* zvel0);
+void launch_visc_dt(const Target& tg, cudaStream_t s, const GeomArrays& ga, double g_small,
+                    double dtc_safe, double dtu_safe, double dtv_safe, double dtw_safe,
+                    double dtdiv_safe, const typename S::rho_t* density0,
+                    const typename S::cs_t* pressure, typename S::cs_t* viscosity,
+                    const typename S::cs_t* soundspeed, const typename S::vel_t* xvel0,
+                    const typename S::vel_t* yvel0, const typename S::vel_t* zvel0,
+                    unsigned long long* min_key);
 template <class S>
 void launch_pdv_predict_eos(const Target& tg, cudaStream_t s, const double* dt_ptr,
                             const GeomArrays& ga, const typename S::rho_t* density0,

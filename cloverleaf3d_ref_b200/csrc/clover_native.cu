@@ -513,17 +513,14 @@ struct Chunk : ChunkBase {
     halo({5, 3, 1, 8, 10}, 1, vc);
     pend("update_halo", 0);
     pbeg();
-    launch_timestep_visc<S>(tg, stream, ga, density0, pressure, viscosity, xvel0, yvel0, zvel0);
-    pend("viscosity", n * (3 * V8 + 3 * G8 + C8));
-    pbeg();
-    halo({6}, 1, vc);
-    pend("update_halo", 0);
-    pbeg();
-    launch_calc_dt<S>(tg, stream, ga, kGSmall, deck.dtc_safe, deck.dtu_safe, deck.dtv_safe,
-                      deck.dtw_safe, deck.dtdiv_safe, density0, viscosity, soundspeed, xvel0,
-                      yvel0, zvel0, (W*)nullptr, &sc->key);
+    launch_visc_dt<S>(tg, stream, ga, kGSmall, deck.dtc_safe, deck.dtu_safe, deck.dtv_safe,
+                      deck.dtw_safe, deck.dtdiv_safe, density0, pressure, viscosity, soundspeed,
+                      xvel0, yvel0, zvel0, &sc->key);
     k_dt_finalize<<<deck_blocks(), 128, 0, stream>>>(sc, nd, dt_hist);
-    pend("calc_dt", n * (4 * G8 + R8 + 2 * C8 + 3 * V8));
+    pend("viscosity_calc_dt", n * (3 * V8 + 4 * G8 + R8 + 3 * C8));
+    pbeg();
+    halo({6}, 1, vc);  // read by accelerate at its neighbours
+    pend("update_halo", 0);
     // PdV.f90:50-107: predictor + EOS on the predicted state; revert is implied
     pbeg();
     launch_pdv_predict_eos<S>(tg, stream, dtp, ga, density0, energy0, pressure, viscosity, xvel0,
