@@ -541,10 +541,13 @@ __device__ __forceinline__ double cell_product(const Geom& g, int variant, const
   return L(density1, j, k, l) * mom_post_vol<S>(g, variant, ga, vfx, vfy, vfz, j, k, l);
 }
 
-// Node pass for direction y or z, marching along the sweep axis: thread
-// (j, c) walks p over the sweep range carrying the previous node flux and the
-// previous plane of cell products.
-// DIR 2: p = k, c = l; DIR 3: p = l, c = k.
+// Node pass for direction y or z, marching along the sweep axis p: thread
+// (j, c) walks a segment of p carrying the mass fluxes of plane p and the cell
+// products of the plane below. Lane L of a warp holds column j = jlo-1+31t+L:
+// the values at column j-1 (mass fluxes and cell products) come from lane
+// L-1, so lane 0 only serves lane 1 and lanes 1..31 store nodes.
+// DIR 2: p = k, c = l; DIR 3: p = l, c = k. Sums keep the reference order
+// (advec_mom_kernel.f90:166-190 and the y/z forms).
 template <class S, int DIR, class M>
 __global__ void __launch_bounds__(BX * BY, 4) k_mom_node_march(M m, int variant, GeomArrays ga,
     const typename S::mf_t* __restrict__ mf, const typename S::rho_t* __restrict__ density1,
@@ -553,75 +556,82 @@ __global__ void __launch_bounds__(BX * BY, 4) k_mom_node_march(M m, int variant,
     typename S::wk_t* __restrict__ node_mass_post, typename S::wk_t* __restrict__ node_mass_pre) {
   m.run([&](const Geom& g, const Tile& t) {
   const MarchRange r = mom_node_range<DIR>(g);
-  const int jlo = r.jlo, jhi = r.jhi, clo = r.clo, chi = r.chi, plo = r.plo, phi = r.phi;
+  const int plo = r.plo, phi = r.phi;
   const int seg = m.seg;
-  const int j = jlo + t.x * BX + threadIdx.x;
-  const int c = clo + t.y * BY + threadIdx.y;
-  if (j > jhi || c > chi) return;
+  const int lane = threadIdx.x;
+  const int j = r.jlo - 1 + t.x * 31 + lane;
+  const int c = r.clo + t.y * BY + threadIdx.y;
+  if (c > r.chi) return;  // the whole warp: c depends on the row only
+  const bool lds = j <= r.jhi;            // lanes that load (lane 0 holds column j-1 of lane 1)
+  const bool own = lds && lane >= 1;      // lanes that store
   const int p0 = plo + t.z * seg;
   int p1 = p0 + seg - 1;
   if (p1 > phi) p1 = phi;
+  const unsigned full = 0xffffffffu;
   using W = typename S::wk_t;
-  // (j,k,l) of the node at march index p
-#define IDX(p) (DIR == 2 ? j : j), (DIR == 2 ? (p) : c), (DIR == 2 ? c : (p))
+  // (j,k,l) of the node at march index p, and the same with c-1
+#define IDX(p) j, (DIR == 2 ? (p) : c), (DIR == 2 ? c : (p))
+#define IDXM(p) j, (DIR == 2 ? (p) : c - 1), (DIR == 2 ? c - 1 : (p))
   auto P = [&](int jj, int kk, int ll) {
     return cell_product<S>(g, variant, ga, density1, vfx, vfy, vfz, jj, kk, ll);
   };
-  // node flux of the node before the segment and the plane of products
-  // below the first node (cells at march index p0-1)
+  auto up = [&](double v) { return __shfl_up_sync(full, v, 1); };
+  // mass fluxes of plane p at (j, c) and (j, c-1); the node flux of node p
+  // adds, in the reference order, (j-1,c,p) (j,c,p) (j-1,c,p+1) (j,c,p+1)
+  // (j-1,c-1,p) (j,c-1,p) (j-1,c-1,p+1) (j,c-1,p+1)
+  double a0 = 0.0, b0 = 0.0;
+  if (lds) { a0 = LI(mf, IDX(p0)); b0 = LI(mf, IDXM(p0)); }
+  double a0m = up(a0), b0m = up(b0);
+  // node flux of the node before the segment and the plane of products below
+  // the first node (cells at march index p0-1); the first segment starts at
+  // the first node-flux index, whose node mass is not computed
   double nf_prev = 0.0;
-  if (p0 - 1 >= plo) nf_prev = node_flux_at<S, DIR>(g, mf, IDX(p0 - 1));
-  // Plane products: the node at (j,k,l) uses cells (j-1..j, k-1..k, l-1..l).
-  // Along the march the "lower" plane of node p is the upper plane of p-1.
   double q_a = 0.0, q_b = 0.0, q_c = 0.0, q_d = 0.0;  // lower-plane products
-  // The first segment starts at the first node-flux index, whose node mass is
-  // not computed: its lower plane (one below the arrays) is not loaded.
   if (p0 - 1 >= plo) {
+    double am = 0.0, bm = 0.0;
+    if (lds) { am = LI(mf, IDX(p0 - 1)); bm = LI(mf, IDXM(p0 - 1)); }
+    const double amm = up(am), bmm = up(bm);
+    nf_prev = 0.125 * (amm + am + a0m + a0 + bmm + bm + b0m + b0);
     const int p = p0;
+    double x0 = 0.0, x1 = 0.0;
     if (DIR == 3) {  // lower plane l-1: P(j,k-1,l-1), P(j,k,l-1), P(j-1,k-1,l-1), P(j-1,k,l-1)
-      q_a = P(j, c - 1, p - 1); q_b = P(j, c, p - 1); q_c = P(j - 1, c - 1, p - 1); q_d = P(j - 1, c, p - 1);
+      if (lds) { x0 = P(j, c - 1, p - 1); x1 = P(j, c, p - 1); }
+      q_a = x0; q_b = x1; q_c = up(x0); q_d = up(x1);
     } else {  // lower plane k-1: P(j,k-1,l), P(j-1,k-1,l), P(j,k-1,l-1), P(j-1,k-1,l-1)
-      q_a = P(j, p - 1, c); q_b = P(j - 1, p - 1, c); q_c = P(j, p - 1, c - 1); q_d = P(j - 1, p - 1, c - 1);
+      if (lds) { x0 = P(j, p - 1, c); x1 = P(j, p - 1, c - 1); }
+      q_a = x0; q_b = up(x0); q_c = x1; q_d = up(x1);
     }
   }
   for (int p = p0; p <= p1; p++) {
-    const double nf = node_flux_at<S, DIR>(g, mf, IDX(p));
-    EI(node_flux, IDX(p)) = st<W>(nf);
+    double a1 = 0.0, b1 = 0.0;
+    if (lds) { a1 = LI(mf, IDX(p + 1)); b1 = LI(mf, IDXM(p + 1)); }
+    const double a1m = up(a1), b1m = up(b1);
+    const double nf = 0.125 * (a0m + a0 + a1m + a1 + b0m + b0 + b1m + b1);
+    if (own) EI(node_flux, IDX(p)) = st<W>(nf);
     double u_a, u_b, u_c, u_d;  // upper-plane products
     double nmp;
+    double x0 = 0.0, x1 = 0.0;
     if (DIR == 3) {  // upper plane l: P(j,k-1,l), P(j,k,l), P(j-1,k-1,l), P(j-1,k,l)
-      u_a = P(j, c - 1, p); u_b = P(j, c, p); u_c = P(j - 1, c - 1, p); u_d = P(j - 1, c, p);
+      if (lds) { x0 = P(j, c - 1, p); x1 = P(j, c, p); }
+      u_a = x0; u_b = x1; u_c = up(x0); u_d = up(x1);
       nmp = node_mass_sum(u_a, u_b, u_c, u_d, q_a, q_b, q_c, q_d);
     } else {  // upper plane k: P(j,k,l), P(j-1,k,l), P(j,k,l-1), P(j-1,k,l-1)
-      u_a = P(j, p, c); u_b = P(j - 1, p, c); u_c = P(j, p, c - 1); u_d = P(j - 1, p, c - 1);
+      if (lds) { x0 = P(j, p, c); x1 = P(j, p, c - 1); }
+      u_a = x0; u_b = up(x0); u_c = x1; u_d = up(x1);
       // order: P(j,k-1,l) P(j,k,l) P(j-1,k-1,l) P(j-1,k,l) P(j,k-1,l-1) P(j,k,l-1) P(j-1,k-1,l-1) P(j-1,k,l-1)
       nmp = node_mass_sum(q_a, u_a, q_b, u_b, q_c, u_c, q_d, u_d);
     }
-    if (p >= plo + 1) {  // node masses run from one node after the flux range start
+    if (own && p >= plo + 1) {  // node masses run from one node after the flux range start
       EI(node_mass_post, IDX(p)) = st<W>(nmp);
       EI(node_mass_pre, IDX(p)) = st<W>(nmp - nf_prev + nf);
     }
     nf_prev = nf;
     q_a = u_a; q_b = u_b; q_c = u_c; q_d = u_d;
+    a0 = a1; b0 = b1; a0m = a1m; b0m = b1m;
   }
+#undef IDXM
 #undef IDX
   });
-}
-
-__device__ __forceinline__ double mom_limiter(double sigma, double width, double celld_dif,
-                                              double vdiffuw, double vdiffdw) {
-  double limiter = 0.0;
-  if (vdiffuw * vdiffdw > 0.0) {
-    const double auw = fabs(vdiffuw);
-    const double adw = fabs(vdiffdw);
-    double wind = 1.0;
-    if (vdiffdw <= 0.0) wind = -1.0;
-    limiter = wind * fmin2(fmin2(width * ((2.0 - sigma) * adw / width +
-                                          (1.0 + sigma) * auw / celld_dif) / 6.0,
-                                 auw),
-                           adw);
-  }
-  return limiter;
 }
 
 // Momentum flux at node i (advec_mom_kernel.f90:211-242 and the y/z forms)
@@ -638,7 +648,17 @@ __device__ __forceinline__ double mom_flux_at(double nf, double nmpre_i, double 
   const double sigma = fabs(nf) / nm_donor;
   const double vdiffuw = v_donor - v_upwind;
   const double vdiffdw = v_downwind - v_donor;
-  const double limiter = mom_limiter(sigma, width, cd_dif, vdiffuw, vdiffdw);
+  double limiter = 0.0;
+  if (vdiffuw * vdiffdw > 0.0) {
+    const double auw = fabs(vdiffuw);
+    const double adw = fabs(vdiffdw);
+    double wind = 1.0;
+    if (vdiffdw <= 0.0) wind = -1.0;
+    limiter = wind * fmin2(fmin2(width * ((2.0 - sigma) * adw / width +
+                                          (1.0 + sigma) * auw / cd_dif) / 6.0,
+                                 auw),
+                           adw);
+  }
   const double advec_vel_s = v_donor + (1.0 - sigma) * limiter;
   return advec_vel_s * nf;
 }
@@ -901,14 +921,11 @@ __global__ void __launch_bounds__(BX * BY, 3) k_mom_sweep_x(M m, int variant,
       f_c = L(mfx, j + 1, k - 1, l); f_d = L(mfx, j + 1, k, l);
       p_a = P(k - 1, l); p_b = P(k, l);
     }
-    // node_flux(j): mfx(j,k-1,l) mfx(j,k,l) mfx(j+1,k-1,l) mfx(j+1,k,l) then l-1
     const double nf = 0.125 * (f_a + f_b + f_c + f_d + fm_a + fm_b + fm_c + fm_d);
-    // cell masses of column j-1 from the lane below
     const double q_a = __shfl_up_sync(0xffffffffu, p_a, 1);
     const double q_b = __shfl_up_sync(0xffffffffu, p_b, 1);
     const double qm_a = __shfl_up_sync(0xffffffffu, pm_a, 1);
     const double qm_b = __shfl_up_sync(0xffffffffu, pm_b, 1);
-    // P(j,k-1,l) P(j,k,l) P(j-1,k-1,l) P(j-1,k,l) P(j,k-1,l-1) P(j,k,l-1) P(j-1,k-1,l-1) P(j-1,k,l-1)
     const double nmp = node_mass_sum(p_a, p_b, q_a, q_b, pm_a, pm_b, qm_a, qm_b);
     const double nf_m = __shfl_up_sync(0xffffffffu, nf, 1);
     const double nmpre = nmp - nf_m + nf;
@@ -966,10 +983,11 @@ dim3 grid_cell_sweep(const Geom& g, int) {
   const MarchRange r = cell_sweep_range<DIR>(g);
   return dim3((r.jhi - r.jlo + 1 + BX - 1) / BX, r.chi - r.clo + 1, 1);
 }
+// 31 nodes per warp along x (lane 0 holds the column below), rows of 8, segments
 template <int DIR>
 dim3 grid_mom_node(const Geom& g, int seg) {
   const MarchRange r = mom_node_range<DIR>(g);
-  return dim3((r.jhi - r.jlo + 1 + BX - 1) / BX, (r.chi - r.clo + 1 + BY - 1) / BY,
+  return dim3((r.jhi - r.jlo + 1 + 30) / 31, (r.chi - r.clo + 1 + BY - 1) / BY,
               (r.phi - r.plo + 1 + seg - 1) / seg);
 }
 template <int DIR>
