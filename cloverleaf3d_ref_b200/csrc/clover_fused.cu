@@ -34,6 +34,7 @@ namespace clover {
 namespace {
 
 constexpr int BX = 32, BY = 8;
+constexpr int kViscCellsZ = 2;  // cells along z per thread of k_visc_dt
 
 struct Box {
   int j0, j1, k0, k1, l0, l1;
@@ -128,9 +129,13 @@ __global__ void __launch_bounds__(BX * BY, 3) k_visc_dt(M m, GeomArrays ga, doub
   const Box b = interior(g);
   const int j = b.j0 + t.x * BX + threadIdx.x;
   const int k = b.k0 + t.y * BY + threadIdx.y;
-  const int l = b.l0 + t.z;
   unsigned long long key = ~0ull;
-  if (j <= b.j1 && k <= b.k1) {
+  // kViscCellsZ cells along z per thread, unrolled so that the loads of one
+  // cell are in flight with the arithmetic of the other
+#pragma unroll
+  for (int iz = 0; iz < kViscCellsZ; iz++) {
+  const int l = b.l0 + t.z * kViscCellsZ + iz;
+  if (j <= b.j1 && k <= b.k1 && l <= b.l1) {
   const double u000 = L(xvel0, j, k, l), u100 = L(xvel0, j + 1, k, l);
   const double u010 = L(xvel0, j, k + 1, l), u110 = L(xvel0, j + 1, k + 1, l);
   const double u001 = L(xvel0, j, k, l + 1), u101 = L(xvel0, j + 1, k, l + 1);
@@ -220,7 +225,11 @@ __global__ void __launch_bounds__(BX * BY, 3) k_visc_dt(M m, GeomArrays ga, doub
   const double dvg = du2 - du1 + dv2 - dv1 + dw2 - dw1;
   const double dtdivt = dtdiv_safe * 4.0 * vol / fmax2(vol * 1.0e-05, fabs(dvg));
   const double mn = fmin2(fmin2(fmin2(fmin2(dtct, dtut), dtvt), dtwt), dtdivt);
-  if (!(mn != mn)) key = key_of(mn);
+  if (!(mn != mn)) {
+    const unsigned long long kc = key_of(mn);
+    key = kc < key ? kc : key;
+  }
+  }
   }
   // warp then block minimum, one atomic per block
 #pragma unroll
@@ -976,6 +985,7 @@ constexpr int kMarchSeg = 32;
 
 dim3 grid_interior(const Geom& g, int) { return grid_of(interior(g)); }
 dim3 grid_nodes(const Geom& g, int) { return grid_of(nodes(g)); }
+dim3 grid_visc(const Geom& g, int) { return grid_of(interior(g), kViscCellsZ); }
 dim3 grid_cell_flux_x(const Geom& g, int) { return grid_of(cell_flux_box<1>(g)); }
 // 32 columns j of one cross-axis index per block, BY segments along the sweep
 template <int DIR>
@@ -1018,7 +1028,7 @@ void launch_visc_dt(const Target& tg, cudaStream_t s, const GeomArrays& ga, doub
                     const typename S::cs_t* soundspeed, const typename S::vel_t* xvel0,
                     const typename S::vel_t* yvel0, const typename S::vel_t* zvel0,
                     unsigned long long* min_key) {
-  launch_mapped(tg, s, kKeyTimestepVisc, grid_interior, 0, false, kBlk, k_visc_dt<S, MapSingle>,
+  launch_mapped(tg, s, kKeyTimestepVisc, grid_visc, 0, false, kBlk, k_visc_dt<S, MapSingle>,
                 k_visc_dt<S, MapBatch>, ga, g_small, dtc_safe, dtu_safe, dtv_safe, dtw_safe,
                 dtdiv_safe, density0, pressure, viscosity, soundspeed, xvel0, yvel0, zvel0,
                 min_key);
