@@ -178,6 +178,37 @@ def run_reference(args):
     return 0
 
 
+def rel_err(a, b):
+    """|a - b| / |b| per element; 0 where both are 0 (the kinetic energy at
+    step 0 of a deck at rest)."""
+    import numpy as np
+    d = np.abs(a - b)
+    s = np.abs(b)
+    return np.where(s > 0, d / np.where(s > 0, s, 1.0), np.where(d > 0, np.inf, 0.0))
+
+
+def accuracy_leg(C, n, steps):
+    """The FP64 and the mixed-precision chunk run the same deck for `steps`
+    steps (summary every 10); the relative error of every summary quantity at
+    every summary step, the bar being 1e-5 after 200 steps."""
+    deck = C.Deck.from_values(states=STATES, **deck_values(n, steps))
+    out = {}
+    for name, prec in (("fp64", C.PRECISION_FP64), ("mixed", C.PRECISION_MIXED)):
+        ch = C.Chunk(deck, prec)
+        assert ch.run() == steps
+        out[name] = ch.summaries()
+        ch.close()
+    (a, st), (b, _) = out["fp64"], out["mixed"]
+    rel = rel_err(b, a)
+    names = ["vol", "mass", "ie", "ke", "press"]
+    return {
+        "steps": steps, "cells": "%d^3" % n, "summary_steps": [int(x) for x in st],
+        "rel_err_per_summary": {q: [float(x) for x in rel[:, i]] for i, q in enumerate(names)},
+        "max_rel_err": {q: float(rel[:, i].max()) for i, q in enumerate(names)},
+        "within_1e-5": bool(rel.max() <= 1e-5),
+    }
+
+
 def mixed_leg(C, torch, deck, args, fp64_ms, fp64_sums, fp64_steps, barrier, world, dist):
     """The same workload with FP32 storage (FP64 density, mass fluxes, work
     arrays and arithmetic): timed the same way, and its field summaries
@@ -211,7 +242,7 @@ def mixed_leg(C, torch, deck, args, fp64_ms, fp64_sums, fp64_steps, barrier, wor
     ch.close()
     m = min(len(sums), len(fp64_sums))
     assert np.array_equal(steps[:m], fp64_steps[:m])
-    rel = np.abs(sums[:m] - fp64_sums[:m]) / np.abs(fp64_sums[:m])
+    rel = rel_err(sums[:m], fp64_sums[:m])
     step_bytes = sum(g["bytes"] for g in groups) / args.steps
     return {
         "value": world * n ** 3 * args.steps / (ms / 1000.0), "unit": "cell-updates/s",
@@ -238,7 +269,7 @@ def timed_steps(torch, obj, steps):
     return e0.elapsed_time(e1)
 
 
-def ensemble_leg(C, torch, name, n_decks, cells, steps, seed, precisions, seq_decks, warm=3):
+def ensemble_leg(C, torch, n_decks, cells, steps, seed, precisions, seq_decks, warm=3):
     """One ensemble configuration: per precision, the batched run (autotuned,
     then warm steps, then the rest of the steps timed); then the same decks
     one after another as single chunks (the first seq_decks of them, the
@@ -296,11 +327,7 @@ def ensemble_leg(C, torch, name, n_decks, cells, steps, seed, precisions, seq_de
                              len(sample), n_decks)}
     out["speedup_vs_sequential"] = out[key]["value"] / seq_value
     if "fp64" in sums and "mixed" in sums:
-        errs = []
-        for a, b in zip(sums["mixed"], sums["fp64"]):
-            scale = np.maximum(np.abs(b), 1e-300)
-            errs.append(np.abs(a - b) / scale)
-        e = np.stack(errs)  # deck, summary, quantity
+        e = np.stack([rel_err(a, b) for a, b in zip(sums["mixed"], sums["fp64"])])  # deck, summary, quantity
         last = e[:, -1, :]
         out["mixed_rel_err_vs_fp64"] = {
             "at_last_summary_max_over_decks": dict(zip(
@@ -344,9 +371,9 @@ def ensembles(C, torch):
     """The two ensemble configurations (64 decks FP64 + mixed; 512 small decks
     mixed with its FP64 twin)."""
     return {
-        "decks64": ensemble_leg(C, torch, "decks64", 64, (24, 128), 150, 2024,
+        "decks64": ensemble_leg(C, torch, 64, (24, 128), 150, 2024,
                                 [C.PRECISION_FP64, C.PRECISION_MIXED], 64),
-        "decks512": ensemble_leg(C, torch, "decks512", 512, (16, 48), 100, 4048,
+        "decks512": ensemble_leg(C, torch, 512, (16, 48), 100, 4048,
                                  [C.PRECISION_MIXED, C.PRECISION_FP64], 64),
     }
 
@@ -363,6 +390,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--no-ensemble", action="store_true")
+    ap.add_argument("--no-accuracy", action="store_true",
+                    help="skip the 200-step FP64 vs mixed comparison")
     ap.add_argument("--ensemble-only", action="store_true",
                     help="only the ensemble legs (a separate JSON line)")
     args = ap.parse_args()
@@ -455,6 +484,8 @@ def main():
     mixed = None
     if prec == C.PRECISION_FP64 and not args.no_mixed:
         mixed = mixed_leg(C, torch, deck, args, ms, summaries, sum_steps, barrier, world, dist)
+        if not args.no_accuracy and rank == 0:
+            mixed["accuracy_200_steps"] = accuracy_leg(C, n, 200)
 
     e2e = None
     if not args.no_e2e and rank == 0:
