@@ -906,6 +906,62 @@ __global__ void k_halo(M m, HaloLaunch h, int depth, int do_low, int do_high) {
   });
 }
 
+// The x faces, one copy per thread: task = ((row * nfields + field) * 2 +
+// side) * depth + m - 1 over the rows (k, l) of the face, so that the copies
+// are all in flight at once (a row's halo cells lie in different sectors;
+// the y and z faces are coalesced along x instead). On an axis shorter than
+// three cells the high side reads cells the low side writes: there one thread
+// per row does the row's copies in the reference order.
+template <class M>
+__global__ void k_halo_x(M m, HaloLaunch h, int depth, int do_low, int do_high) {
+  m.run([&](const Geom& g, const Tile& t) {
+  const int na = g.y_max - g.y_min + 2 + 2 * depth;  // k in [y_min-depth, y_max+1+depth]
+  const int nb = g.z_max - g.z_min + 2 + 2 * depth;  // l likewise
+  const int per_row = h.nfields * 2 * depth;
+  const long long task = (long long)t.x * (BX * BY) + threadIdx.y * BX + threadIdx.x;
+  if (task >= (long long)na * nb * per_row) return;
+  const long long row = task / per_row;
+  int rem = (int)(task % per_row);
+  const int a = g.y_min - depth + (int)(row % na);
+  const int bb = g.z_min - depth + (int)(row / na);
+  const int n = g.x_max - g.x_min + 1;
+  auto copy = [&](int fi, int side, int mm) {
+    if (side == 0 ? !do_low : !do_high) return;
+    const HaloRule r = h.rule[fi];
+    const signed char* ext = side == 0 ? r.ext_lo : r.ext_hi;
+    if (a > g.y_max + depth + ext[1] || bb > g.z_max + depth + ext[2]) return;
+    const int dst = side == 0 ? 1 - mm : n + r.hi_dst + mm;
+    const int src = side == 0 ? r.low_src + mm : n + r.hi_src - mm;
+    const long long od = off3(g, dst, a, bb), os = off3(g, src, a, bb);
+    if (h.elem_bytes[fi] == 8) {
+      double* p = (double*)h.f[fi];
+      p[od] = r.sign < 0 ? -p[os] : p[os];
+    } else {
+      float* p = (float*)h.f[fi];
+      p[od] = r.sign < 0 ? -p[os] : p[os];
+    }
+  };
+  if (n < 3) {
+    if (rem != 0) return;
+    for (int fi = 0; fi < h.nfields; fi++)
+      for (int side = 0; side < 2; side++)
+        for (int mm = 1; mm <= depth; mm++) copy(fi, side, mm);
+    return;
+  }
+  const int mm = rem % depth + 1;
+  rem /= depth;
+  copy(rem / 2, rem % 2, mm);
+  });
+}
+
+// tasks of k_halo_x in blocks of BX * BY; aux = tasks per row (fields * 2 * depth)
+dim3 grid_halo_x_tasks(const Geom& g, int per_row, int depth) {
+  const long long na = g.y_max - g.y_min + 2 + 2 * depth, nb = g.z_max - g.z_min + 2 + 2 * depth;
+  return dim3((unsigned)((na * nb * per_row + BX * BY - 1) / (BX * BY)), 1, 1);
+}
+template <int D>
+dim3 grid_halo_x(const Geom& g, int per_row) { return grid_halo_x_tasks(g, per_row, D); }
+
 // tile grid of the halo update of the faces normal to AX (32 x 8 tiles over
 // the two tangential axes, each extended by depth)
 template <int AX>
@@ -1264,9 +1320,16 @@ void launch_update_halo(const Target& tg, cudaStream_t s, const HaloFields& f, c
     if (h.nfields == 0) return;
     const dim3 blk(32, 8);
     const unsigned key = kKeyHalo | (unsigned)(ax << 4) | (unsigned)depth;
-    if (ax == 0)
-      launch_mapped(tg, s, key, grid_halo<0>, depth, false, blk, k_halo<0, MapSingle>,
-                    k_halo<0, MapBatch>, h, depth, do_low, do_high);
+    if (ax == 0) {
+      const int per_row = h.nfields * 2 * depth;
+      const unsigned kx = kKeyHaloX | (unsigned)per_row;
+      if (depth == 1)
+        launch_mapped(tg, s, kx, grid_halo_x<1>, per_row, false, blk, k_halo_x<MapSingle>,
+                      k_halo_x<MapBatch>, h, depth, do_low, do_high);
+      else
+        launch_mapped(tg, s, kx, grid_halo_x<2>, per_row, false, blk, k_halo_x<MapSingle>,
+                      k_halo_x<MapBatch>, h, depth, do_low, do_high);
+    }
     else if (ax == 1)
       launch_mapped(tg, s, key, grid_halo<1>, depth, false, blk, k_halo<1, MapSingle>,
                     k_halo<1, MapBatch>, h, depth, do_low, do_high);

@@ -92,7 +92,8 @@ enum : unsigned {
   kKeyTimestepVisc = 5u << 8, kKeyPdvPredict = 6u << 8, kKeyPdvFlux = 7u << 8,
   kKeyCellFluxX = 8u << 8, kKeyCellUpdateX = 9u << 8, kKeyCellSweep = 10u << 8,
   kKeyMomSweepX = 11u << 8, kKeyMomNode = 12u << 8, kKeyMomVel3 = 13u << 8,
-  kKeyShellCopy = 14u << 8, kKeySummary = 15u << 8, kKeyAccelerate = 16u << 8
+  kKeyShellCopy = 14u << 8, kKeySummary = 15u << 8, kKeyAccelerate = 16u << 8,
+  kKeyHaloX = 17u << 8
 };
 
 // Storage policy: FP64 everywhere (the drop-in / parity path).
