@@ -156,6 +156,15 @@ def _declare(L):
     L.clover_chunk_stream.restype = ctypes.c_size_t
     L.clover_chunk_device_bytes.argtypes = [P]
     L.clover_chunk_device_bytes.restype = ctypes.c_longlong
+    L.clover_chunk_set_visit_dir.argtypes = [P, ctypes.c_char_p]
+    L.clover_chunk_set_visit_dir.restype = ctypes.c_int
+    L.clover_chunk_visit.argtypes = [P]
+    L.clover_chunk_visit.restype = ctypes.c_int
+    L.clover_format_e12_4.argtypes = [ctypes.c_double, ctypes.c_char_p]
+    L.clover_chunk_checkpoint.argtypes = [P, ctypes.c_char_p]
+    L.clover_chunk_checkpoint.restype = ctypes.c_int
+    L.clover_chunk_restore.argtypes = [P, ctypes.c_char_p]
+    L.clover_chunk_restore.restype = ctypes.c_int
     L.clover_chunk_profile.argtypes = [P, ctypes.c_int]
     L.clover_chunk_profile_report.argtypes = [P, P, ctypes.c_int, P, P, P, ctypes.c_int]
     L.clover_chunk_profile_report.restype = ctypes.c_int
@@ -358,6 +367,41 @@ class Chunk:
             raise CloverError("read_field failed")
         return a
 
+    def set_visit_dir(self, path):
+        """Directory of the VTK output (clover.visit and clover.*.vtk)."""
+        lib().clover_chunk_set_visit_dir(self.h, os.fsencode(path))
+
+    def visit(self):
+        """Write the current step as VTK (visit.f90) and wait for the file."""
+        if lib().clover_chunk_visit(self.h) != 0:
+            raise CloverError("visit failed: " + lib().clover_last_error().decode())
+
+    def checkpoint(self, path):
+        """Write the whole device state (every array, dt/time/step, the dt and
+        summary histories) to path."""
+        rc = lib().clover_chunk_checkpoint(self.h, os.fsencode(path))
+        if rc != 0:
+            raise CloverError("checkpoint failed (%d)" % rc)
+
+    def restore(self, path):
+        """Replace the device state by a checkpoint of a chunk made from the
+        same deck(s) and precision; stepping on continues bit for bit."""
+        rc = lib().clover_chunk_restore(self.h, os.fsencode(path))
+        if rc != 0:
+            raise CloverError("restore failed (%d): %s" % (rc, lib().clover_last_error().decode()))
+
+    def dump_fields(self, path):
+        """Every field in the reference layout (FP64, Fortran order) to an .npz."""
+        np.savez(path, **{n: self.field(n) for n in FIELD_NAMES})
+
+    def write_summary_log(self, path):
+        """The recorded field summaries, one line per summary step, %.17g."""
+        sums, steps = self.summaries()
+        with open(path, "w") as f:
+            f.write("step vol mass ie ke press\n")
+            for st, row in zip(steps, sums):
+                f.write("%d %s\n" % (st, " ".join("%.17g" % x for x in row)))
+
     def set_field(self, name, a):
         s = self.deck.s
         a = np.asfortranarray(a, dtype=np.float64)
@@ -454,8 +498,25 @@ class Ensemble(Chunk):
     def field(self, name):
         return self.deck_field(0, name)
 
+    def dump_fields(self, path, deck=0):
+        np.savez(path, **{n: self.deck_field(deck, n) for n in FIELD_NAMES})
+
+    def write_summary_log(self, path, deck=0):
+        sums, steps = self.deck_summaries(deck)
+        with open(path, "w") as f:
+            f.write("step vol mass ie ke press\n")
+            for st, row in zip(steps, sums):
+                f.write("%d %s\n" % (st, " ".join("%.17g" % x for x in row)))
+
     def set_field(self, name, a):
         raise CloverError("ensembles are set up from their decks only")
+
+
+def format_e12_4(v):
+    """A value as the reference's VTK files print it (Fortran E12.4)."""
+    out = ctypes.create_string_buffer(13)
+    lib().clover_format_e12_4(float(v), out)
+    return out.value.decode()
 
 
 def draw_decks(n, seed, cells=(24, 128), end_step=150, summary_frequency=10):

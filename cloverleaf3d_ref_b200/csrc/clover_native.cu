@@ -16,8 +16,11 @@
 
 #include "../../include/clover_b200.h"
 #include "../../include/clover_kernels.h"
+#include <thread>
+
 #include "clover_batch.h"
 #include "clover_launch.h"
+#include "clover_visit.h"
 
 namespace clover {
 namespace {
@@ -391,12 +394,190 @@ struct Chunk : ChunkBase {
     advect_x = true;
     sum_steps.clear();
     summary(0);
+    // start.f90:138: written before the first step (so that the output
+    // directory can be set after creation)
+    visit_pending = deck.visit_frequency != 0;
     if (cudaStreamSynchronize(stream) != cudaSuccess || cudaGetLastError() != cudaSuccess ||
         (plan && plan->failed)) {
       g_last_error = "chunk set-up failed on the device";
       return false;
     }
     return true;
+  }
+
+  // Checkpoint file: a header (format tag, precision, decks, step state and
+  // the sizes of every device allocation), the device scalars, dt and summary
+  // histories, then every device allocation byte for byte. A restore needs a
+  // chunk made from the same decks and precision; it replaces the whole
+  // device state, so the continued run is bit-identical to an uninterrupted
+  // one.
+  struct CkptHeader {
+    char tag[8];
+    int version, precision, nd, host_step, advect_x, fused, n_owned, n_sum, dt_cap, sum_cap;
+  };
+  static constexpr const char* kCkptTag = "CLVCKPT";
+
+  CkptHeader ckpt_header() const {
+    CkptHeader h{};
+    memcpy(h.tag, kCkptTag, 8);
+    h.version = 1;
+    h.precision = sizeof(V) == 8 ? CLOVER_PRECISION_FP64 : CLOVER_PRECISION_MIXED;
+    h.nd = nd;
+    h.host_step = host_step;
+    h.advect_x = advect_x ? 1 : 0;
+    h.fused = fused ? 1 : 0;
+    h.n_owned = (int)owned.size();
+    h.n_sum = (int)sum_steps.size();
+    h.dt_cap = dt_cap;
+    h.sum_cap = sum_cap;
+    return h;
+  }
+
+  // device <-> file through a bounded host buffer
+  static bool dev_to_file(FILE* f, const void* d, size_t n, std::vector<char>& buf) {
+    for (size_t o = 0; o < n; o += buf.size()) {
+      const size_t c = n - o < buf.size() ? n - o : buf.size();
+      if (cudaMemcpy(buf.data(), (const char*)d + o, c, cudaMemcpyDeviceToHost) != cudaSuccess)
+        return false;
+      if (fwrite(buf.data(), 1, c, f) != c) return false;
+    }
+    return true;
+  }
+  static bool file_to_dev(FILE* f, void* d, size_t n, std::vector<char>& buf) {
+    for (size_t o = 0; o < n; o += buf.size()) {
+      const size_t c = n - o < buf.size() ? n - o : buf.size();
+      if (fread(buf.data(), 1, c, f) != c) return false;
+      if (cudaMemcpy((char*)d + o, buf.data(), c, cudaMemcpyHostToDevice) != cudaSuccess)
+        return false;
+    }
+    return true;
+  }
+
+  int checkpoint(const char* path) {
+    if (cudaStreamSynchronize(stream) != cudaSuccess) return -1;
+    FILE* f = fopen(path, "wb");
+    if (!f) return -2;
+    const CkptHeader h = ckpt_header();
+    bool ok = fwrite(&h, sizeof(h), 1, f) == 1;
+    ok = ok && fwrite(decks.data(), sizeof(clover_deck), (size_t)nd, f) == (size_t)nd;
+    for (const Owned& o : owned) ok = ok && fwrite(&o.bytes, sizeof(o.bytes), 1, f) == 1;
+    if (h.n_sum > 0)
+      ok = ok && fwrite(sum_steps.data(), sizeof(int), (size_t)h.n_sum, f) == (size_t)h.n_sum;
+    std::vector<char> buf((size_t)64 << 20);
+    ok = ok && dev_to_file(f, sc, (size_t)nd * sizeof(DevScalars), buf);
+    ok = ok && dev_to_file(f, dt_hist, (size_t)nd * dt_cap * sizeof(double), buf);
+    ok = ok && dev_to_file(f, sum_hist, (size_t)nd * sum_cap * 5 * sizeof(double), buf);
+    for (const Owned& o : owned) ok = ok && dev_to_file(f, o.p, o.bytes, buf);
+    ok = (fclose(f) == 0) && ok;
+    return ok ? 0 : -3;
+  }
+
+  int restore(const char* path) {
+    if (cudaStreamSynchronize(stream) != cudaSuccess) return -1;
+    FILE* f = fopen(path, "rb");
+    if (!f) return -2;
+    CkptHeader h{};
+    const CkptHeader mine = ckpt_header();
+    bool ok = fread(&h, sizeof(h), 1, f) == 1 && memcmp(h.tag, kCkptTag, 8) == 0 &&
+              h.version == 1 && h.precision == mine.precision && h.nd == nd &&
+              h.n_owned == mine.n_owned && h.dt_cap == dt_cap && h.sum_cap == sum_cap &&
+              h.n_sum >= 0 && h.n_sum <= sum_cap;
+    std::vector<clover_deck> ds(ok ? (size_t)nd : 0);
+    ok = ok && fread(ds.data(), sizeof(clover_deck), (size_t)nd, f) == (size_t)nd &&
+         memcmp(ds.data(), decks.data(), (size_t)nd * sizeof(clover_deck)) == 0;
+    for (const Owned& o : owned) {
+      size_t b = 0;
+      ok = ok && fread(&b, sizeof(b), 1, f) == 1 && b == o.bytes;
+    }
+    std::vector<int> ss(ok ? (size_t)h.n_sum : 0);
+    if (ok && h.n_sum > 0) ok = fread(ss.data(), sizeof(int), (size_t)h.n_sum, f) == (size_t)h.n_sum;
+    if (!ok) {
+      fclose(f);
+      g_last_error = "checkpoint does not match this chunk (decks, precision or sizes)";
+      return -4;
+    }
+    std::vector<char> buf((size_t)64 << 20);
+    ok = file_to_dev(f, sc, (size_t)nd * sizeof(DevScalars), buf);
+    ok = ok && file_to_dev(f, dt_hist, (size_t)nd * dt_cap * sizeof(double), buf);
+    ok = ok && file_to_dev(f, sum_hist, (size_t)nd * sum_cap * 5 * sizeof(double), buf);
+    for (const Owned& o : owned) ok = ok && file_to_dev(f, o.p, o.bytes, buf);
+    fclose(f);
+    if (!ok) {
+      g_last_error = "checkpoint read failed";
+      return -5;
+    }
+    drop_graphs();
+    host_step = h.host_step;
+    advect_x = h.advect_x != 0;
+    fused = h.fused != 0;
+    sum_steps = ss;
+    return 0;
+  }
+
+  // visit.f90: ideal_gas, the halos of pressure and the velocities, the
+  // viscosity, then the fields of every deck copied to the host and written
+  // as VTK by a writer thread (the previous frame's writer is joined first).
+  // None of this changes the run: each step recomputes these fields.
+  std::string visit_dir = ".";
+  bool visit_pending = false;  // the step-0 frame is still to be written
+  std::thread visit_writer;
+  bool visit_first = true;
+  std::string visit_error;
+  bool visit_failed = false;
+
+  void visit_join() {
+    if (visit_writer.joinable()) visit_writer.join();
+  }
+
+  int visit() {
+    launch_ideal_gas<S>(tg, stream, density0, energy0, pressure, soundspeed);
+    halo({5, 8, 10, 12}, 1, vel1_buffer(host_step));
+    for (int d = 0; d < nd; d++)
+      launch_viscosity<S>(geoms[d], stream, ga, density0, pressure, viscosity, xvel0, yvel0, zvel0);
+    if (cudaStreamSynchronize(stream) != cudaSuccess) return -1;
+    VisitFrame fr;
+    fr.dir = visit_dir;
+    fr.step = host_step;
+    fr.first = visit_first;
+    for (int d = 0; d < nd; d++) {
+      const Geom& q = geoms[d];
+      VisitChunk c;
+      c.chunk = d + 1;
+      c.nx = q.x_max - q.x_min + 1;
+      c.ny = q.y_max - q.y_min + 1;
+      c.nz = q.z_max - q.z_min + 1;
+      const size_t nc = (size_t)(c.nx + 4) * (c.ny + 4) * (c.nz + 4);
+      const size_t nv = (size_t)(c.nx + 5) * (c.ny + 5) * (c.nz + 5);
+      std::vector<double>* f[7] = {&c.density0, &c.energy0, &c.pressure, &c.viscosity,
+                                   &c.xvel0, &c.yvel0, &c.zvel0};
+      const int ids[7] = {1, 3, 5, 6, 8, 10, 12};
+      for (int i = 0; i < 7; i++) {
+        f[i]->resize(i < 4 ? nc : nv);
+        if (read_field(ids[i], f[i]->data(), false, d) != 0) return -1;
+      }
+      const int n1[3] = {c.nx + 1, c.ny + 1, c.nz + 1};
+      const double* v1[3] = {vertexx, vertexy, vertexz};
+      std::vector<double>* h1[3] = {&c.vertexx, &c.vertexy, &c.vertexz};
+      for (int a = 0; a < 3; a++) {
+        h1[a]->resize(n1[a]);
+        // vertex j = min (index 2 from min-2) .. max+1
+        if (cudaMemcpy(h1[a]->data(), v1[a] + q.o1 + 2, (size_t)n1[a] * sizeof(double),
+                       cudaMemcpyDeviceToHost) != cudaSuccess)
+          return -1;
+      }
+      fr.chunks.push_back(std::move(c));
+    }
+    visit_join();
+    if (visit_failed) return -2;
+    visit_first = false;
+    visit_writer = std::thread([this, fr]() {
+      std::string err;
+      if (!write_visit_frame(fr, &err)) {
+        visit_error = err;
+        visit_failed = true;
+      }
+    });
+    return 0;
   }
 
   bool drop_graphs() {
@@ -719,6 +900,10 @@ struct Chunk : ChunkBase {
   }
 
   int step(int n) {
+    if (visit_pending && n > 0) {
+      visit_pending = false;
+      if (visit() != 0) return -1;
+    }
     for (int i = 0; i < n; i++) {
       bool graphs = use_graphs && !profile && !(plan && plan->timing);
       if (graphs && !graph[advect_x ? 0 : 1] && !capture_graphs()) {
@@ -735,6 +920,8 @@ struct Chunk : ChunkBase {
       host_step++;
       if (deck.summary_frequency != 0 && host_step % deck.summary_frequency == 0)
         summary(host_step);
+      // hydro.f90:73-75
+      if (deck.visit_frequency != 0 && host_step % deck.visit_frequency == 0) visit();
     }
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
   }
@@ -756,7 +943,9 @@ struct Chunk : ChunkBase {
       for (int d = 0; d < nd; d++) bad |= scalars(d).status & CLOVER_STATUS_SMALL_DT;
       if (bad) return -host_step;
       summary(host_step);  // the final summary (hydro.f90:87)
+      if (deck.visit_frequency != 0) visit();  // hydro.f90:88
       cudaStreamSynchronize(stream);
+      visit_join();
       return host_step;
     }
     for (;;) {
@@ -764,7 +953,9 @@ struct Chunk : ChunkBase {
       if (h.status & CLOVER_STATUS_SMALL_DT) return -host_step;
       if (host_step > 0 && (h.time + kGSmall > deck.end_time || host_step >= deck.end_step)) {
         summary(host_step);  // the final summary (hydro.f90:87)
+        if (deck.visit_frequency != 0) visit();  // hydro.f90:88
         cudaStreamSynchronize(stream);
+        visit_join();
         return host_step;
       }
       int batch = deck.end_step - host_step;
@@ -819,6 +1010,7 @@ struct Chunk : ChunkBase {
   }
 
   ~Chunk() {
+    visit_join();
     if (stream) cudaStreamSynchronize(stream);
     prof_collect();
     for (auto e : ev_pool) cudaEventDestroy(e);
@@ -1289,6 +1481,30 @@ int clover_ensemble_summaries(clover_chunk* c, int deck, double* out5, int* step
 
 int clover_ensemble_read_field(clover_chunk* c, int deck, int id, double* host) {
   return DISPATCH(c, read_field(id, host, false, deck));
+}
+
+int clover_chunk_set_visit_dir(clover_chunk* c, const char* dir) {
+  if (!dir) return -1;
+  if (c->f64) c->f64->visit_dir = dir;
+  else c->mixed->visit_dir = dir;
+  return 0;
+}
+
+int clover_chunk_visit(clover_chunk* c) {
+  if (c->f64) c->f64->visit_pending = false; else c->mixed->visit_pending = false;
+  const int rc = DISPATCH(c, visit());
+  if (c->f64) c->f64->visit_join(); else c->mixed->visit_join();
+  const bool failed = c->f64 ? c->f64->visit_failed : c->mixed->visit_failed;
+  if (failed) g_last_error = c->f64 ? c->f64->visit_error : c->mixed->visit_error;
+  return rc != 0 ? rc : (failed ? -2 : 0);
+}
+
+int clover_chunk_checkpoint(clover_chunk* c, const char* path) {
+  return DISPATCH(c, checkpoint(path));
+}
+
+int clover_chunk_restore(clover_chunk* c, const char* path) {
+  return DISPATCH(c, restore(path));
 }
 
 }  // extern "C"

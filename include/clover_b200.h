@@ -107,6 +107,27 @@ int clover_chunk_profile_report(clover_chunk *c, char *names, int name_len, doub
 /* Kernel launches one hydro step issues (graph nodes per step). */
 int clover_chunk_launches_per_step(clover_chunk *c);
 
+/* VTK output as visit.f90 writes it (legacy ASCII rectilinear grids of
+ * density, energy, pressure, viscosity and the node velocities, Fortran
+ * E12.4, plus the clover.visit index) into dir (default "."). With a deck's
+ * visit_frequency set, a run writes at step 0 (when the first step is
+ * enqueued), every visit_frequency steps and at the end, a writer thread formatting each frame while the GPU steps
+ * on; clover_chunk_visit writes the current step and waits for the file.
+ * Ensembles write one file per deck (chunk number = deck + 1). */
+int clover_chunk_set_visit_dir(clover_chunk *c, const char *dir);
+int clover_chunk_visit(clover_chunk *c);
+/* E12.4 formatting of one value into out (13 bytes), for tests. */
+int clover_format_e12_4(double v, char *out13);
+
+/* Checkpoint / restart of a chunk or ensemble (no counterpart in the
+ * reference, which restarts from the deck only). The file holds every device
+ * array of the chunk byte for byte plus the step state (dt, time, step, the dt
+ * and summary histories); restoring it into a chunk made from the same decks
+ * and precision continues bit for bit as if the run had not stopped. 0 on
+ * success; negative on I/O errors or a checkpoint that does not match. */
+int clover_chunk_checkpoint(clover_chunk *c, const char *path);
+int clover_chunk_restore(clover_chunk *c, const char *path);
+
 /* ---- Ensembles: many independent decks advanced together ----
  * No counterpart in the reference (which runs one deck per job). The decks
  * of an ensemble may differ in size, states and timestep controls; each
