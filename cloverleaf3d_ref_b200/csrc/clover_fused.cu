@@ -108,6 +108,13 @@ __device__ __forceinline__ T st(double v) { return (T)v; }
 
 __device__ __forceinline__ double fmin2(double a, double b) { return b < a ? b : a; }
 __device__ __forceinline__ double fmax2(double a, double b) { return b > a ? b : a; }
+__device__ __forceinline__ float fmin2(float a, float b) { return b < a ? b : a; }
+__device__ __forceinline__ float fmax2(float a, float b) { return b > a ? b : a; }
+// a value of the momentum arithmetic type A from storage
+template <class A>
+__device__ __forceinline__ A lda(const double* p) { return (A)__ldg(p); }
+template <class A>
+__device__ __forceinline__ A lda(const float* p) { return (A)__ldg(p); }
 
 // ---------------------------------------------------------------------------
 // viscosity_kernel.f90:71-134 followed by calc_dt_kernel.f90:102-149 on the
@@ -645,30 +652,30 @@ __global__ void __launch_bounds__(BX * BY, 4) k_mom_node_march(M m, int variant,
 
 // Momentum flux at node i (advec_mom_kernel.f90:211-242 and the y/z forms)
 // from the velocity window v(i-1..i+2).
-__device__ __forceinline__ double mom_flux_at(double nf, double nmpre_i, double nmpre_ip1,
-                                              double vm1, double v0, double vp1, double vp2,
-                                              double width, double cd_m1, double cd_p1) {
-  double v_upwind, v_donor, v_downwind, nm_donor, cd_dif;
-  if (nf < 0.0) {
+template <class A>
+__device__ __forceinline__ A mom_flux_at(A nf, A nmpre_i, A nmpre_ip1, A vm1, A v0, A vp1, A vp2,
+                                         A width, A cd_m1, A cd_p1) {
+  A v_upwind, v_donor, v_downwind, nm_donor, cd_dif;
+  if (nf < A(0.0)) {
     v_upwind = vp2; v_donor = vp1; v_downwind = v0; nm_donor = nmpre_ip1; cd_dif = cd_p1;
   } else {
     v_upwind = vm1; v_donor = v0; v_downwind = vp1; nm_donor = nmpre_i; cd_dif = cd_m1;
   }
-  const double sigma = fabs(nf) / nm_donor;
-  const double vdiffuw = v_donor - v_upwind;
-  const double vdiffdw = v_downwind - v_donor;
-  double limiter = 0.0;
-  if (vdiffuw * vdiffdw > 0.0) {
-    const double auw = fabs(vdiffuw);
-    const double adw = fabs(vdiffdw);
-    double wind = 1.0;
-    if (vdiffdw <= 0.0) wind = -1.0;
-    limiter = wind * fmin2(fmin2(width * ((2.0 - sigma) * adw / width +
-                                          (1.0 + sigma) * auw / cd_dif) / 6.0,
+  const A sigma = fabs(nf) / nm_donor;
+  const A vdiffuw = v_donor - v_upwind;
+  const A vdiffdw = v_downwind - v_donor;
+  A limiter = A(0.0);
+  if (vdiffuw * vdiffdw > A(0.0)) {
+    const A auw = fabs(vdiffuw);
+    const A adw = fabs(vdiffdw);
+    A wind = A(1.0);
+    if (vdiffdw <= A(0.0)) wind = A(-1.0);
+    limiter = wind * fmin2(fmin2(width * ((A(2.0) - sigma) * adw / width +
+                                          (A(1.0) + sigma) * auw / cd_dif) / A(6.0),
                                  auw),
                            adw);
   }
-  const double advec_vel_s = v_donor + (1.0 - sigma) * limiter;
+  const A advec_vel_s = v_donor + (A(1.0) - sigma) * limiter;
   return advec_vel_s * nf;
 }
 
@@ -696,47 +703,49 @@ __global__ void __launch_bounds__(BX * BY, 3) k_mom_vel3_march(M m, GeomArrays g
   const int cdlo = DIR == 2 ? g.y_min : g.z_min;
 #define CD(p) cd[g.o1 + (p) - cdlo + 2]
   using V = typename S::vel_t;
+  using A = typename S::arith_t;  // arithmetic of the flux and update
+#define LA(a, idx) lda<A>(&EI_(a, idx))
   const typename S::vel_t* in[3] = {u_in, v_in, w_in};
   typename S::vel_t* out[3] = {u_out, v_out, w_out};
   // window at node p: v(p-2), v(p-1), v(p), v(p+1) ; loaded v(p+2) each step
-  double vw[3][4];
-  double mf_prev[3];
-  double nf_m = LI(node_flux, IDX(p0 - 1));
-  double pre_m = LI(node_mass_pre, IDX(p0 - 1));
-  double pre_0 = LI(node_mass_pre, IDX(p0));
+  A vw[3][4];
+  A mf_prev[3];
+  A nf_m = LA(node_flux, IDX(p0 - 1));
+  A pre_m = LA(node_mass_pre, IDX(p0 - 1));
+  A pre_0 = LA(node_mass_pre, IDX(p0));
 #pragma unroll
   for (int q = 0; q < 3; q++) {
-    vw[q][0] = LI(in[q], IDX(p0 - 2));
-    vw[q][1] = LI(in[q], IDX(p0 - 1));
-    vw[q][2] = LI(in[q], IDX(p0));
-    vw[q][3] = LI(in[q], IDX(p0 + 1));
+    vw[q][0] = LA(in[q], IDX(p0 - 2));
+    vw[q][1] = LA(in[q], IDX(p0 - 1));
+    vw[q][2] = LA(in[q], IDX(p0));
+    vw[q][3] = LA(in[q], IDX(p0 + 1));
     // mom_flux(p0-1)
-    mf_prev[q] = mom_flux_at(nf_m, pre_m, pre_0, vw[q][0], vw[q][1], vw[q][2], vw[q][3],
-                             CD(p0 - 1), CD(p0 - 2), CD(p0));
+    mf_prev[q] = mom_flux_at<A>(nf_m, pre_m, pre_0, vw[q][0], vw[q][1], vw[q][2], vw[q][3],
+                                (A)CD(p0 - 1), (A)CD(p0 - 2), (A)CD(p0));
   }
   // loads of node p are issued one node ahead of their use
-  double nf_0 = LI(node_flux, IDX(p0));
-  double pre_p = LI(node_mass_pre, IDX(p0 + 1));
-  double post_0 = LI(node_mass_post, IDX(p0));
-  double vn[3];
+  A nf_0 = LA(node_flux, IDX(p0));
+  A pre_p = LA(node_mass_pre, IDX(p0 + 1));
+  A post_0 = LA(node_mass_post, IDX(p0));
+  A vn[3];
 #pragma unroll
-  for (int q = 0; q < 3; q++) vn[q] = LI(in[q], IDX(p0 + 2));
+  for (int q = 0; q < 3; q++) vn[q] = LA(in[q], IDX(p0 + 2));
   for (int p = p0; p <= p1; p++) {
     const bool more = p < p1;
-    double nf_n = 0.0, pre_n = 0.0, post_n = 0.0, vn_n[3] = {0.0, 0.0, 0.0};
+    A nf_n = A(0.0), pre_n = A(0.0), post_n = A(0.0), vn_n[3] = {A(0.0), A(0.0), A(0.0)};
     if (more) {
-      nf_n = LI(node_flux, IDX(p + 1));
-      pre_n = LI(node_mass_pre, IDX(p + 2));
-      post_n = LI(node_mass_post, IDX(p + 1));
+      nf_n = LA(node_flux, IDX(p + 1));
+      pre_n = LA(node_mass_pre, IDX(p + 2));
+      post_n = LA(node_mass_post, IDX(p + 1));
 #pragma unroll
-      for (int q = 0; q < 3; q++) vn_n[q] = LI(in[q], IDX(p + 3));
+      for (int q = 0; q < 3; q++) vn_n[q] = LA(in[q], IDX(p + 3));
     }
-    const double w_0 = CD(p), cd_m1 = CD(p - 1), cd_p1 = CD(p + 1);
+    const A w_0 = (A)CD(p), cd_m1 = (A)CD(p - 1), cd_p1 = (A)CD(p + 1);
 #pragma unroll
     for (int q = 0; q < 3; q++) {
-      const double vp2 = vn[q];
-      const double mf_0 = mom_flux_at(nf_0, pre_0, pre_p, vw[q][1], vw[q][2], vw[q][3], vp2, w_0,
-                                      cd_m1, cd_p1);
+      const A vp2 = vn[q];
+      const A mf_0 = mom_flux_at<A>(nf_0, pre_0, pre_p, vw[q][1], vw[q][2], vw[q][3], vp2, w_0,
+                                    cd_m1, cd_p1);
       EI(out[q], IDX(p)) = st<V>((vw[q][2] * pre_0 + mf_prev[q] - mf_0) / post_0);
       mf_prev[q] = mf_0;
       vw[q][0] = vw[q][1];
@@ -750,6 +759,7 @@ __global__ void __launch_bounds__(BX * BY, 3) k_mom_vel3_march(M m, GeomArrays g
     pre_p = pre_n;
     post_0 = post_n;
   }
+#undef LA
 #undef CD
 #undef IDX
   });
@@ -939,17 +949,20 @@ __global__ void __launch_bounds__(BX * BY, 3) k_mom_sweep_x(M m, int variant,
     const double nf_m = __shfl_up_sync(0xffffffffu, nf, 1);
     const double nmpre = nmp - nf_m + nf;
     const double nmpre_p = __shfl_down_sync(0xffffffffu, nmpre, 1);
+    // flux and update in the momentum arithmetic A (node masses are FP64)
+    using A = typename S::arith_t;
 #pragma unroll
     for (int q = 0; q < 3; q++) {
-      double mf = 0.0, v0 = 0.0;
+      A mf = A(0.0), v0 = A(0.0);
       if (has_mf) {
-        const double vm1 = L(in[q], j - 1, k, l);
-        v0 = L(in[q], j, k, l);
-        const double vp1 = L(in[q], j + 1, k, l), vp2 = L(in[q], j + 2, k, l);
-        mf = mom_flux_at(nf, nmpre, nmpre_p, vm1, v0, vp1, vp2, cd_0, cd_m1, cd_p1);
+        const A vm1 = lda<A>(&E(in[q], j - 1, k, l));
+        v0 = lda<A>(&E(in[q], j, k, l));
+        const A vp1 = lda<A>(&E(in[q], j + 1, k, l)), vp2 = lda<A>(&E(in[q], j + 2, k, l));
+        mf = mom_flux_at<A>((A)nf, (A)nmpre, (A)nmpre_p, vm1, v0, vp1, vp2, (A)cd_0, (A)cd_m1,
+                            (A)cd_p1);
       }
-      const double mf_m = __shfl_up_sync(0xffffffffu, mf, 1);
-      if (has_up) E(out[q], j, k, l) = st<V>((v0 * nmpre + mf_m - mf) / nmp);
+      const A mf_m = __shfl_up_sync(0xffffffffu, mf, 1);
+      if (has_up) E(out[q], j, k, l) = st<V>((v0 * (A)nmpre + mf_m - mf) / (A)nmp);
     }
     fm_a = f_a; fm_b = f_b; fm_c = f_c; fm_d = f_d;
     pm_a = p_a; pm_b = p_b;

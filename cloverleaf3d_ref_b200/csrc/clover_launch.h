@@ -105,6 +105,7 @@ struct F64 {
   using vf_t = double;   // vol_flux_x/y/z
   using mf_t = double;   // mass_flux_x/y/z
   using wk_t = double;   // work arrays
+  using arith_t = double;  // arithmetic of the stencils the mixed path runs in FP32
 };
 
 // Storage policy of the mixed-precision native path: FP32 storage for the
@@ -112,7 +113,8 @@ struct F64 {
 // FP64 kept where conservation needs it: density, mass fluxes, work arrays
 // (pre/post volumes, node masses) and the volume fluxes, whose differences
 // form the pre/post volumes and must cancel against the PdV volume change
-// for mass to be conserved. All arithmetic is FP64.
+// for mass to be conserved. The momentum advection's flux limiter and
+// velocity update run in FP32 (arith_t); all other arithmetic is FP64.
 struct F32Mixed {
   using rho_t = double;
   using ene_t = float;
@@ -121,6 +123,7 @@ struct F32Mixed {
   using vf_t = double;
   using mf_t = double;
   using wk_t = double;
+  using arith_t = float;  // momentum flux and update, accelerate (node and cell masses stay FP64)
 };
 
 // Geometry arrays (always FP64).
