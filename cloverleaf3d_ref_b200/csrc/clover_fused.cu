@@ -133,6 +133,14 @@ __global__ void __launch_bounds__(BX * BY, 3) k_visc_dt(M m, GeomArrays ga, doub
     const typename S::vel_t* __restrict__ zvel0, unsigned long long* __restrict__ min_key) {
   __shared__ unsigned long long wmin[BX * BY / 32];
   m.run([&](const Geom& g, const Tile& t) {
+  // viscosity and dt criteria in the policy's arithmetic (FP64, or FP32 in
+  // the mixed path); the minimum folds as a double key
+  using A = typename S::arith_t;
+#define LA(a, jj, kk, ll) lda<A>(&E(a, jj, kk, ll))
+#define EGA(a, jj, kk, ll) ((A)E(a, jj, kk, ll))
+#define AG(G, a, i) ((A)G(a, i))
+  const A a_gs = (A)g_small, a_dtc = (A)dtc_safe, a_dtu = (A)dtu_safe, a_dtv = (A)dtv_safe;
+  const A a_dtw = (A)dtw_safe, a_dtdiv = (A)dtdiv_safe;
   const Box b = interior(g);
   const int j = b.j0 + t.x * BX + threadIdx.x;
   const int k = b.k0 + t.y * BY + threadIdx.y;
@@ -143,95 +151,95 @@ __global__ void __launch_bounds__(BX * BY, 3) k_visc_dt(M m, GeomArrays ga, doub
   for (int iz = 0; iz < kViscCellsZ; iz++) {
   const int l = b.l0 + t.z * kViscCellsZ + iz;
   if (j <= b.j1 && k <= b.k1 && l <= b.l1) {
-  const double u000 = L(xvel0, j, k, l), u100 = L(xvel0, j + 1, k, l);
-  const double u010 = L(xvel0, j, k + 1, l), u110 = L(xvel0, j + 1, k + 1, l);
-  const double u001 = L(xvel0, j, k, l + 1), u101 = L(xvel0, j + 1, k, l + 1);
-  const double u011 = L(xvel0, j, k + 1, l + 1), u111 = L(xvel0, j + 1, k + 1, l + 1);
-  const double v000 = L(yvel0, j, k, l), v100 = L(yvel0, j + 1, k, l);
-  const double v010 = L(yvel0, j, k + 1, l), v110 = L(yvel0, j + 1, k + 1, l);
-  const double v001 = L(yvel0, j, k, l + 1), v101 = L(yvel0, j + 1, k, l + 1);
-  const double v011 = L(yvel0, j, k + 1, l + 1), v111 = L(yvel0, j + 1, k + 1, l + 1);
-  const double w000 = L(zvel0, j, k, l), w100 = L(zvel0, j + 1, k, l);
-  const double w010 = L(zvel0, j, k + 1, l), w110 = L(zvel0, j + 1, k + 1, l);
-  const double w001 = L(zvel0, j, k, l + 1), w101 = L(zvel0, j + 1, k, l + 1);
-  const double w011 = L(zvel0, j, k + 1, l + 1), w111 = L(zvel0, j + 1, k + 1, l + 1);
+  const A u000 = LA(xvel0, j, k, l), u100 = LA(xvel0, j + 1, k, l);
+  const A u010 = LA(xvel0, j, k + 1, l), u110 = LA(xvel0, j + 1, k + 1, l);
+  const A u001 = LA(xvel0, j, k, l + 1), u101 = LA(xvel0, j + 1, k, l + 1);
+  const A u011 = LA(xvel0, j, k + 1, l + 1), u111 = LA(xvel0, j + 1, k + 1, l + 1);
+  const A v000 = LA(yvel0, j, k, l), v100 = LA(yvel0, j + 1, k, l);
+  const A v010 = LA(yvel0, j, k + 1, l), v110 = LA(yvel0, j + 1, k + 1, l);
+  const A v001 = LA(yvel0, j, k, l + 1), v101 = LA(yvel0, j + 1, k, l + 1);
+  const A v011 = LA(yvel0, j, k + 1, l + 1), v111 = LA(yvel0, j + 1, k + 1, l + 1);
+  const A w000 = LA(zvel0, j, k, l), w100 = LA(zvel0, j + 1, k, l);
+  const A w010 = LA(zvel0, j, k + 1, l), w110 = LA(zvel0, j + 1, k + 1, l);
+  const A w001 = LA(zvel0, j, k, l + 1), w101 = LA(zvel0, j + 1, k, l + 1);
+  const A w011 = LA(zvel0, j, k + 1, l + 1), w111 = LA(zvel0, j + 1, k + 1, l + 1);
 
-  const double ugradx1 = u000 + u010 + u001 + u011;
-  const double ugradx2 = u100 + u110 + u101 + u111;
-  const double vgrady1 = v000 + v100 + v001 + v101;
-  const double vgrady2 = v010 + v110 + v011 + v111;
-  const double wgradz1 = w000 + w100 + w010 + w110;
-  const double wgradz2 = w001 + w101 + w011 + w111;
-  const double xa = E(ga.xarea, j, k, l), ya = E(ga.yarea, j, k, l), za = E(ga.zarea, j, k, l);
-  const double div = (xa * (ugradx2 - ugradx1) + ya * (vgrady2 - vgrady1)) +
+  const A ugradx1 = u000 + u010 + u001 + u011;
+  const A ugradx2 = u100 + u110 + u101 + u111;
+  const A vgrady1 = v000 + v100 + v001 + v101;
+  const A vgrady2 = v010 + v110 + v011 + v111;
+  const A wgradz1 = w000 + w100 + w010 + w110;
+  const A wgradz2 = w001 + w101 + w011 + w111;
+  const A xa = EGA(ga.xarea, j, k, l), ya = EGA(ga.yarea, j, k, l), za = EGA(ga.zarea, j, k, l);
+  const A div = (xa * (ugradx2 - ugradx1) + ya * (vgrady2 - vgrady1)) +
                      za * (wgradz2 - wgradz1);
-  double q = 0.0;
-  if (!(div >= 0.0)) {
-    const double ugrady1 = u000 + u100 + u001 + u101;
-    const double ugrady2 = u010 + u110 + u011 + u111;
-    const double ugradz1 = u000 + u100 + u010 + u110;
-    const double ugradz2 = u001 + u101 + u011 + u111;
-    const double vgradx1 = v000 + v010 + v001 + v011;
-    const double vgradx2 = v100 + v110 + v101 + v111;
-    const double vgradz1 = v000 + v100 + v010 + v110;
-    const double vgradz2 = v001 + v101 + v011 + v111;
-    const double wgradx1 = w000 + w010 + w001 + w011;
-    const double wgradx2 = w100 + w110 + w101 + w111;
-    const double wgrady1 = w000 + w100 + w001 + w101;
-    const double wgrady2 = w010 + w110 + w011 + w111;
-    const double cdx = GX(ga.celldx, j), cdy = GY(ga.celldy, k), cdz = GZ(ga.celldz, l);
-    const double xx = 0.25 * (ugradx2 - ugradx1) / cdx;
-    const double yy = 0.25 * (vgrady2 - vgrady1) / cdy;
-    const double zz = 0.25 * (wgradz2 - wgradz1) / cdz;
-    const double xy = 0.25 * (ugrady2 - ugrady1) / cdy + 0.25 * (vgradx2 - vgradx1) / cdx;
-    const double xz = 0.25 * (ugradz2 - ugradz1) / cdz + 0.25 * (wgradx2 - wgradx1) / cdx;
-    const double yz = 0.25 * (vgradz2 - vgradz1) / cdz + 0.25 * (wgrady2 - wgrady1) / cdy;
-    double pgradx = (L(pressure, j + 1, k, l) - L(pressure, j - 1, k, l)) / (cdx + GX(ga.celldx, j + 1));
-    double pgrady = (L(pressure, j, k + 1, l) - L(pressure, j, k - 1, l)) / (cdy + GY(ga.celldy, k + 1));
-    double pgradz = (L(pressure, j, k, l + 1) - L(pressure, j, k, l - 1)) / (cdz + GZ(ga.celldz, l + 1));
-    const double pgradx2 = pgradx * pgradx;
-    const double pgrady2 = pgrady * pgrady;
-    const double pgradz2 = pgradz * pgradz;
-    const double limiter = (xx * pgradx2 + yy * pgrady2 + zz * pgradz2 + xy * pgradx * pgrady +
+  A q = A(A(0.0));
+  if (!(div >= A(0.0))) {
+    const A ugrady1 = u000 + u100 + u001 + u101;
+    const A ugrady2 = u010 + u110 + u011 + u111;
+    const A ugradz1 = u000 + u100 + u010 + u110;
+    const A ugradz2 = u001 + u101 + u011 + u111;
+    const A vgradx1 = v000 + v010 + v001 + v011;
+    const A vgradx2 = v100 + v110 + v101 + v111;
+    const A vgradz1 = v000 + v100 + v010 + v110;
+    const A vgradz2 = v001 + v101 + v011 + v111;
+    const A wgradx1 = w000 + w010 + w001 + w011;
+    const A wgradx2 = w100 + w110 + w101 + w111;
+    const A wgrady1 = w000 + w100 + w001 + w101;
+    const A wgrady2 = w010 + w110 + w011 + w111;
+    const A cdx = AG(GX, ga.celldx, j), cdy = AG(GY, ga.celldy, k), cdz = AG(GZ, ga.celldz, l);
+    const A xx = A(0.25) * (ugradx2 - ugradx1) / cdx;
+    const A yy = A(0.25) * (vgrady2 - vgrady1) / cdy;
+    const A zz = A(0.25) * (wgradz2 - wgradz1) / cdz;
+    const A xy = A(0.25) * (ugrady2 - ugrady1) / cdy + A(0.25) * (vgradx2 - vgradx1) / cdx;
+    const A xz = A(0.25) * (ugradz2 - ugradz1) / cdz + A(0.25) * (wgradx2 - wgradx1) / cdx;
+    const A yz = A(0.25) * (vgradz2 - vgradz1) / cdz + A(0.25) * (wgrady2 - wgrady1) / cdy;
+    A pgradx = (LA(pressure, j + 1, k, l) - LA(pressure, j - 1, k, l)) / (cdx + AG(GX, ga.celldx, j + 1));
+    A pgrady = (LA(pressure, j, k + 1, l) - LA(pressure, j, k - 1, l)) / (cdy + AG(GY, ga.celldy, k + 1));
+    A pgradz = (LA(pressure, j, k, l + 1) - LA(pressure, j, k, l - 1)) / (cdz + AG(GZ, ga.celldz, l + 1));
+    const A pgradx2 = pgradx * pgradx;
+    const A pgrady2 = pgrady * pgrady;
+    const A pgradz2 = pgradz * pgradz;
+    const A limiter = (xx * pgradx2 + yy * pgrady2 + zz * pgradz2 + xy * pgradx * pgrady +
                             xz * pgradx * pgradz + yz * pgrady * pgradz) /
-                           fmax2(pgradx2 + pgrady2 + pgradz2, 1.0e-16);
-    if (!(limiter > 0.0)) {
-      pgradx = copysign(fmax2(1.0e-16, fabs(pgradx)), pgradx);
-      pgrady = copysign(fmax2(1.0e-16, fabs(pgrady)), pgrady);
-      pgradz = copysign(fmax2(1.0e-16, fabs(pgradz)), pgradz);
-      const double pgrad = sqrt(pgradx * pgradx + pgrady * pgrady + pgradz * pgradz);
-      const double xgrad = fabs(cdx * pgrad / pgradx);
-      const double ygrad = fabs(cdy * pgrad / pgrady);
-      const double zgrad = fabs(cdz * pgrad / pgradz);
-      const double grad = fmin2(fmin2(xgrad, ygrad), zgrad);
-      const double grad2 = grad * grad;
-      q = 2.0 * L(density0, j, k, l) * grad2 * limiter * limiter;
+                           fmax2(pgradx2 + pgrady2 + pgradz2, A(1.0e-16));
+    if (!(limiter > A(0.0))) {
+      pgradx = copysign(fmax2(A(1.0e-16), fabs(pgradx)), pgradx);
+      pgrady = copysign(fmax2(A(1.0e-16), fabs(pgrady)), pgrady);
+      pgradz = copysign(fmax2(A(1.0e-16), fabs(pgradz)), pgradz);
+      const A pgrad = sqrt(pgradx * pgradx + pgrady * pgrady + pgradz * pgradz);
+      const A xgrad = fabs(cdx * pgrad / pgradx);
+      const A ygrad = fabs(cdy * pgrad / pgrady);
+      const A zgrad = fabs(cdz * pgrad / pgradz);
+      const A grad = fmin2(fmin2(xgrad, ygrad), zgrad);
+      const A grad2 = grad * grad;
+      q = A(2.0) * LA(density0, j, k, l) * grad2 * limiter * limiter;
     }
   }
   using C = typename S::cs_t;
-  E(viscosity, j, k, l) = st<C>(q);
+  E(viscosity, j, k, l) = st<C>((double)q);
   // calc_dt_kernel.f90:102-149 (the viscosity as stored)
-  const double visc = (double)st<C>(q);
-  const double d0 = L(density0, j, k, l);
-  const double mcd = fmin2(fmin2(GX(ga.celldx, j), GY(ga.celldy, k)), GZ(ga.celldz, l));
-  const double ds = 1.0 / (mcd * mcd);
-  const double ss = L(soundspeed, j, k, l);
-  double cc = ss * ss;
-  cc = cc + 2.0 * visc / d0;
-  double dtct = ds * cc;
-  dtct = dtc_safe * 1.0 / fmax2(sqrt(dtct), g_small);
-  const double vol = E(ga.volume, j, k, l);
-  const double du1 = ugradx1 * xa, du2 = ugradx2 * xa;
-  const double dtut = dtu_safe * 4.0 * vol / fmax2(fmax2(fabs(du1), fabs(du2)), 1.0e-5 * vol);
-  const double dv1 = vgrady1 * ya, dv2 = vgrady2 * ya;
-  const double dtvt = dtv_safe * 4.0 * vol / fmax2(fmax2(fabs(dv1), fabs(dv2)), 1.0e-5 * vol);
+  const A visc = (A)st<C>((double)q);
+  const A d0 = LA(density0, j, k, l);
+  const A mcd = fmin2(fmin2(AG(GX, ga.celldx, j), AG(GY, ga.celldy, k)), AG(GZ, ga.celldz, l));
+  const A ds = A(1.0) / (mcd * mcd);
+  const A ss = LA(soundspeed, j, k, l);
+  A cc = ss * ss;
+  cc = cc + A(2.0) * visc / d0;
+  A dtct = ds * cc;
+  dtct = a_dtc * A(1.0) / fmax2(sqrt(dtct), a_gs);
+  const A vol = EGA(ga.volume, j, k, l);
+  const A du1 = ugradx1 * xa, du2 = ugradx2 * xa;
+  const A dtut = a_dtu * A(4.0) * vol / fmax2(fmax2(fabs(du1), fabs(du2)), A(1.0e-5) * vol);
+  const A dv1 = vgrady1 * ya, dv2 = vgrady2 * ya;
+  const A dtvt = a_dtv * A(4.0) * vol / fmax2(fmax2(fabs(dv1), fabs(dv2)), A(1.0e-5) * vol);
   // both z faces use zarea(j,k,l); its sums add (j,k+1) before (j+1,k)
-  const double dw1 = (w000 + w010 + w100 + w110) * za;
-  const double dw2 = (w001 + w011 + w101 + w111) * za;
-  const double dtwt = dtw_safe * 4.0 * vol / fmax2(fmax2(fabs(dw1), fabs(dw2)), 1.0e-5 * vol);
-  const double dvg = du2 - du1 + dv2 - dv1 + dw2 - dw1;
-  const double dtdivt = dtdiv_safe * 4.0 * vol / fmax2(vol * 1.0e-05, fabs(dvg));
-  const double mn = fmin2(fmin2(fmin2(fmin2(dtct, dtut), dtvt), dtwt), dtdivt);
+  const A dw1 = (w000 + w010 + w100 + w110) * za;
+  const A dw2 = (w001 + w011 + w101 + w111) * za;
+  const A dtwt = a_dtw * A(4.0) * vol / fmax2(fmax2(fabs(dw1), fabs(dw2)), A(1.0e-5) * vol);
+  const A dvg = du2 - du1 + dv2 - dv1 + dw2 - dw1;
+  const A dtdivt = a_dtdiv * A(4.0) * vol / fmax2(vol * A(1.0e-05), fabs(dvg));
+  const A mn = fmin2(fmin2(fmin2(fmin2(dtct, dtut), dtvt), dtwt), dtdivt);
   if (!(mn != mn)) {
     const unsigned long long kc = key_of(mn);
     key = kc < key ? kc : key;
@@ -256,6 +264,9 @@ __global__ void __launch_bounds__(BX * BY, 3) k_visc_dt(M m, GeomArrays ga, doub
     }
     if (lane == 0 && key != ~0ull) atomicMin(min_key + (long long)t.d * kScalarStride, key);
   }
+#undef AG
+#undef EGA
+#undef LA
   });
 }
 

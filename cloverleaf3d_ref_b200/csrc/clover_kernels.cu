@@ -344,31 +344,38 @@ __global__ void __launch_bounds__(BX * BY) k_accelerate(M m, double dt_val,
   const double nodal_mass = (DV(-1, -1, 0) + DV(0, -1, 0) + DV(0, 0, 0) + DV(-1, 0, 0) +
                              DV(-1, -1, -1) + DV(0, -1, -1) + DV(0, 0, -1) + DV(-1, 0, -1)) * 0.125;
 #undef DV
-  const double stepbymass_s = 0.25 * dt / nodal_mass;
-  const double p000 = L(pressure, j, k, l), p100 = L(pressure, j - 1, k, l);
-  const double p010 = L(pressure, j, k - 1, l), p110 = L(pressure, j - 1, k - 1, l);
-  const double p001 = L(pressure, j, k, l - 1), p101 = L(pressure, j - 1, k, l - 1);
-  const double p011 = L(pressure, j, k - 1, l - 1), p111 = L(pressure, j - 1, k - 1, l - 1);
-  const double q000 = L(viscosity, j, k, l), q100 = L(viscosity, j - 1, k, l);
-  const double q010 = L(viscosity, j, k - 1, l), q110 = L(viscosity, j - 1, k - 1, l);
-  const double q001 = L(viscosity, j, k, l - 1), q101 = L(viscosity, j - 1, k, l - 1);
-  const double q011 = L(viscosity, j, k - 1, l - 1), q111 = L(viscosity, j - 1, k - 1, l - 1);
-  const double xa0 = E(ga.xarea, j, k, l), xa1 = E(ga.xarea, j, k - 1, l);
-  const double xa2 = E(ga.xarea, j, k, l - 1), xa3 = E(ga.xarea, j, k - 1, l - 1);
-  const double ya0 = E(ga.yarea, j, k, l), ya1 = E(ga.yarea, j - 1, k, l);
-  const double ya2 = E(ga.yarea, j, k, l - 1), ya3 = E(ga.yarea, j - 1, k, l - 1);
-  const double za0 = E(ga.zarea, j, k, l), za1 = E(ga.zarea, j, k - 1, l);
-  const double za2 = E(ga.zarea, j - 1, k, l), za3 = E(ga.zarea, j - 1, k - 1, l);
+  const double stepbymass_d = 0.25 * dt / nodal_mass;
+  // the pressure and viscosity gradients and the update in the policy's
+  // arithmetic (FP64, or FP32 in the mixed path; the nodal mass stays FP64)
+  using A = typename S::arith_t;
+  const A stepbymass_s = (A)stepbymass_d;
+  auto la = [](const auto* p) { return (A)__ldg(p); };
+#define LA(a, jj, kk, ll) la(&E(a, jj, kk, ll))
+  const A p000 = LA(pressure, j, k, l), p100 = LA(pressure, j - 1, k, l);
+  const A p010 = LA(pressure, j, k - 1, l), p110 = LA(pressure, j - 1, k - 1, l);
+  const A p001 = LA(pressure, j, k, l - 1), p101 = LA(pressure, j - 1, k, l - 1);
+  const A p011 = LA(pressure, j, k - 1, l - 1), p111 = LA(pressure, j - 1, k - 1, l - 1);
+  const A q000 = LA(viscosity, j, k, l), q100 = LA(viscosity, j - 1, k, l);
+  const A q010 = LA(viscosity, j, k - 1, l), q110 = LA(viscosity, j - 1, k - 1, l);
+  const A q001 = LA(viscosity, j, k, l - 1), q101 = LA(viscosity, j - 1, k, l - 1);
+  const A q011 = LA(viscosity, j, k - 1, l - 1), q111 = LA(viscosity, j - 1, k - 1, l - 1);
+  const A xa0 = LA(ga.xarea, j, k, l), xa1 = LA(ga.xarea, j, k - 1, l);
+  const A xa2 = LA(ga.xarea, j, k, l - 1), xa3 = LA(ga.xarea, j, k - 1, l - 1);
+  const A ya0 = LA(ga.yarea, j, k, l), ya1 = LA(ga.yarea, j - 1, k, l);
+  const A ya2 = LA(ga.yarea, j, k, l - 1), ya3 = LA(ga.yarea, j - 1, k, l - 1);
+  const A za0 = LA(ga.zarea, j, k, l), za1 = LA(ga.zarea, j, k - 1, l);
+  const A za2 = LA(ga.zarea, j - 1, k, l), za3 = LA(ga.zarea, j - 1, k - 1, l);
 
-  const double xvel1_s = L(xvel0, j, k, l) -
+  const A xvel1_s = LA(xvel0, j, k, l) -
       stepbymass_s * (xa0 * (p000 - p100) + xa1 * (p010 - p110) + xa2 * (p001 - p101) +
                       xa3 * (p011 - p111));
-  const double yvel1_s = L(yvel0, j, k, l) -
+  const A yvel1_s = LA(yvel0, j, k, l) -
       stepbymass_s * (ya0 * (p000 - p010) + ya1 * (p100 - p110) + ya2 * (p001 - p011) +
                       ya3 * (p101 - p111));
-  const double zvel1_s = L(zvel0, j, k, l) -
+  const A zvel1_s = LA(zvel0, j, k, l) -
       stepbymass_s * (za0 * (p000 - p001) + za1 * (p010 - p011) + za2 * (p100 - p101) +
                       za3 * (p110 - p111));
+#undef LA
   using V = typename S::vel_t;
   E(xvel1, j, k, l) = st<V>(xvel1_s -
       stepbymass_s * (xa0 * (q000 - q100) + xa1 * (q010 - q110) + xa2 * (q001 - q101) +
