@@ -286,46 +286,53 @@ __global__ void __launch_bounds__(BX * BY) k_pdv_predict_eos(M m, const double* 
   const int k = b.k0 + t.y * BY + threadIdx.y;
   const int l = b.l0 + t.z;
   if (j > b.j1 || k > b.k1) return;
-  const double dt = dt_ptr[(long long)t.d * kScalarStride];
-#define XS(jj) (L(xvel0, jj, k, l) + L(xvel0, jj, k + 1, l) + L(xvel0, jj, k, l + 1) + L(xvel0, jj, k + 1, l + 1))
-#define YS(kk) (L(yvel0, j, kk, l) + L(yvel0, j + 1, kk, l) + L(yvel0, j, kk, l + 1) + L(yvel0, j + 1, kk, l + 1))
-#define ZS(ll) (L(zvel0, j, k, ll) + L(zvel0, j + 1, k, ll) + L(zvel0, j, k + 1, ll) + L(zvel0, j + 1, k + 1, ll))
+  // predictor and EOS in the policy's arithmetic (FP64, or FP32 in the mixed
+  // path: only the pressure, stored in FP32 there, comes out of it)
+  using A = typename S::arith_t;
+#define LA(a, jj, kk, ll) lda<A>(&E(a, jj, kk, ll))
+#define EGA(a, jj, kk, ll) ((A)E(a, jj, kk, ll))
+  const A dt = (A)dt_ptr[(long long)t.d * kScalarStride];
+#define XS(jj) (LA(xvel0, jj, k, l) + LA(xvel0, jj, k + 1, l) + LA(xvel0, jj, k, l + 1) + LA(xvel0, jj, k + 1, l + 1))
+#define YS(kk) (LA(yvel0, j, kk, l) + LA(yvel0, j + 1, kk, l) + LA(yvel0, j, kk, l + 1) + LA(yvel0, j + 1, kk, l + 1))
+#define ZS(ll) (LA(zvel0, j, k, ll) + LA(zvel0, j + 1, k, ll) + LA(zvel0, j, k + 1, ll) + LA(zvel0, j + 1, k + 1, ll))
   // the predictor sums the same four node values twice (vel0 + vel0)
-  double s;
+  A s;
   s = XS(j);
-  const double left_flux = (E(ga.xarea, j, k, l) * (s + L(xvel0, j, k, l) + L(xvel0, j, k + 1, l) +
-                            L(xvel0, j, k, l + 1) + L(xvel0, j, k + 1, l + 1))) * 0.125 * dt * 0.5;
+  const A left_flux = (EGA(ga.xarea, j, k, l) * (s + LA(xvel0, j, k, l) + LA(xvel0, j, k + 1, l) +
+                            LA(xvel0, j, k, l + 1) + LA(xvel0, j, k + 1, l + 1))) * A(0.125) * dt * A(0.5);
   s = XS(j + 1);
-  const double right_flux = (E(ga.xarea, j + 1, k, l) * (s + L(xvel0, j + 1, k, l) + L(xvel0, j + 1, k + 1, l) +
-                             L(xvel0, j + 1, k, l + 1) + L(xvel0, j + 1, k + 1, l + 1))) * 0.125 * dt * 0.5;
+  const A right_flux = (EGA(ga.xarea, j + 1, k, l) * (s + LA(xvel0, j + 1, k, l) + LA(xvel0, j + 1, k + 1, l) +
+                             LA(xvel0, j + 1, k, l + 1) + LA(xvel0, j + 1, k + 1, l + 1))) * A(0.125) * dt * A(0.5);
   s = YS(k);
-  const double bottom_flux = (E(ga.yarea, j, k, l) * (s + L(yvel0, j, k, l) + L(yvel0, j + 1, k, l) +
-                              L(yvel0, j, k, l + 1) + L(yvel0, j + 1, k, l + 1))) * 0.125 * dt * 0.5;
+  const A bottom_flux = (EGA(ga.yarea, j, k, l) * (s + LA(yvel0, j, k, l) + LA(yvel0, j + 1, k, l) +
+                              LA(yvel0, j, k, l + 1) + LA(yvel0, j + 1, k, l + 1))) * A(0.125) * dt * A(0.5);
   s = YS(k + 1);
-  const double top_flux = (E(ga.yarea, j, k + 1, l) * (s + L(yvel0, j, k + 1, l) + L(yvel0, j + 1, k + 1, l) +
-                           L(yvel0, j, k + 1, l + 1) + L(yvel0, j + 1, k + 1, l + 1))) * 0.125 * dt * 0.5;
+  const A top_flux = (EGA(ga.yarea, j, k + 1, l) * (s + LA(yvel0, j, k + 1, l) + LA(yvel0, j + 1, k + 1, l) +
+                           LA(yvel0, j, k + 1, l + 1) + LA(yvel0, j + 1, k + 1, l + 1))) * A(0.125) * dt * A(0.5);
   s = ZS(l);
-  const double back_flux = (E(ga.zarea, j, k, l) * (s + L(zvel0, j, k, l) + L(zvel0, j + 1, k, l) +
-                            L(zvel0, j, k + 1, l) + L(zvel0, j + 1, k + 1, l))) * 0.125 * dt * 0.5;
+  const A back_flux = (EGA(ga.zarea, j, k, l) * (s + LA(zvel0, j, k, l) + LA(zvel0, j + 1, k, l) +
+                            LA(zvel0, j, k + 1, l) + LA(zvel0, j + 1, k + 1, l))) * A(0.125) * dt * A(0.5);
   s = ZS(l + 1);
-  const double front_flux = (E(ga.zarea, j, k, l + 1) * (s + L(zvel0, j, k, l + 1) + L(zvel0, j + 1, k, l + 1) +
-                             L(zvel0, j, k + 1, l + 1) + L(zvel0, j + 1, k + 1, l + 1))) * 0.125 * dt * 0.5;
+  const A front_flux = (EGA(ga.zarea, j, k, l + 1) * (s + LA(zvel0, j, k, l + 1) + LA(zvel0, j + 1, k, l + 1) +
+                             LA(zvel0, j, k + 1, l + 1) + LA(zvel0, j + 1, k + 1, l + 1))) * A(0.125) * dt * A(0.5);
 #undef XS
 #undef YS
 #undef ZS
-  const double total_flux = right_flux - left_flux + top_flux - bottom_flux + front_flux - back_flux;
-  const double vol = E(ga.volume, j, k, l);
-  const double vol_change_s = vol / (vol + total_flux);
-  const double recip_volume = 1.0 / vol;
-  const double d0 = L(density0, j, k, l);
-  const double energy_change =
-      (L(pressure, j, k, l) / d0 + L(viscosity, j, k, l) / d0) * total_flux * recip_volume;
+  const A total_flux = right_flux - left_flux + top_flux - bottom_flux + front_flux - back_flux;
+  const A vol = EGA(ga.volume, j, k, l);
+  const A vol_change_s = vol / (vol + total_flux);
+  const A recip_volume = A(1.0) / vol;
+  const A d0 = LA(density0, j, k, l);
+  const A energy_change =
+      (LA(pressure, j, k, l) / d0 + LA(viscosity, j, k, l) / d0) * total_flux * recip_volume;
   using R = typename S::rho_t;
   using En = typename S::ene_t;
   // the predicted state goes through the storage types, as it would in memory
-  const double e1 = (double)st<En>(L(energy0, j, k, l) - energy_change);
-  const double d1 = (double)st<R>(d0 * vol_change_s);
-  E(pressure, j, k, l) = st<typename S::cs_t>((1.4 - 1.0) * d1 * e1);
+  const A e1 = (A)st<En>((double)(LA(energy0, j, k, l) - energy_change));
+  const A d1 = (A)st<R>((double)(d0 * vol_change_s));
+  E(pressure, j, k, l) = st<typename S::cs_t>((double)((A(1.4) - A(1.0)) * d1 * e1));
+#undef EGA
+#undef LA
   });
 }
 

@@ -84,15 +84,18 @@ __global__ void __launch_bounds__(BX * BY) k_ideal_gas(M m,
     typename S::cs_t* __restrict__ pressure, typename S::cs_t* __restrict__ soundspeed) {
   m.run([&](const Geom& g, const Tile& t) {
   TILE_THREAD(interior(g), t);
-  const double d = L(density, j, k, l);
-  const double v = 1.0 / d;
-  const double p = (1.4 - 1.0) * d * L(energy, j, k, l);
-  const double pressurebyenergy = (1.4 - 1.0) * d;
-  const double pressurebyvolume = -d * p;
-  const double ss2 = v * v * (p * pressurebyenergy - pressurebyvolume);
+  // in the policy's arithmetic (FP64, or FP32 where pressure and sound speed
+  // are stored in FP32)
+  using A = typename S::arith_t;
+  const A d = (A)L(density, j, k, l);
+  const A v = A(1.0) / d;
+  const A p = (A(1.4) - A(1.0)) * d * (A)L(energy, j, k, l);
+  const A pressurebyenergy = (A(1.4) - A(1.0)) * d;
+  const A pressurebyvolume = -d * p;
+  const A ss2 = v * v * (p * pressurebyenergy - pressurebyvolume);
   using C = typename S::cs_t;
-  E(pressure, j, k, l) = st<C>(p);
-  E(soundspeed, j, k, l) = st<C>(sqrt(ss2));
+  E(pressure, j, k, l) = st<C>((double)p);
+  E(soundspeed, j, k, l) = st<C>((double)sqrt(ss2));
   });
 }
 
