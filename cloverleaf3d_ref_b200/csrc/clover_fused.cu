@@ -16,8 +16,9 @@
 //                    the pressure is stored (revert then restores time level
 //                    0, and the corrector overwrites density1/energy1).
 //  k_pdv_flux        PdV corrector + flux_calc (shared velocity loads).
-//  k_cell_flux_f     advec_cell x face pass with pre_vol from the volume fluxes.
-//  k_cell_update_f   advec_cell x update pass, pre_vol recomputed, in place.
+//  k_cell_sweep_x    the whole x cell sweep in one pass (neighbouring cells by
+//                    warp shuffles), out of place into the other buffer of the
+//                    density1/energy1 pair.
 //  k_cell_sweep_march  the whole y or z cell sweep in one pass, each thread
 //                    marching a segment of a column with the stencil in
 //                    registers (the segments of a column share a block).
@@ -53,12 +54,6 @@ __host__ __device__ inline Box interior(const Geom& g) {
 }
 __host__ __device__ inline Box nodes(const Geom& g) {
   return Box{g.x_min, g.x_max + 1, g.y_min, g.y_max + 1, g.z_min, g.z_max + 1};
-}
-// x faces of the x cell sweep: j to x_max+2 over the interior rows
-template <int DIR>
-__host__ __device__ inline Box cell_flux_box(const Geom& g) {
-  static_assert(DIR == 1, "the fused face pass serves the x sweep");
-  return Box{g.x_min, g.x_max + 2, g.y_min, g.y_max, g.z_min, g.z_max};
 }
 
 // A marching kernel's threads cover j in [jlo, jhi] and the cross axis c in
@@ -448,77 +443,103 @@ __device__ __forceinline__ double cell_limiter(double sig, double sigma3, double
   return 0.0;
 }
 
-// advec_cell face pass (:125-171, :220-266, :315-361) with pre_vol(donor)
-// computed from the volume fluxes instead of read from a work array.
-template <class S, int DIR, class M>
-__global__ void __launch_bounds__(BX * BY) k_cell_flux_f(M m, int variant, GeomArrays ga,
-    const typename S::rho_t* __restrict__ density1, const typename S::ene_t* __restrict__ energy1,
+// advec_cell x sweep as ONE pass (advec_cell_kernel.f90:125-185), out of
+// place. Lane L of a warp holds cell c = x_min-2+28t+L of a row: its old
+// density, energy, pre-volume, volume flux and vertexdx are loaded once, the
+// neighbours c-2..c+1 come from the lanes around it, lanes 2..30 form the
+// face c fluxes and lanes 2..29 own cell c (28 per warp): they store the
+// fluxes of face c and update cell c from faces c and c+1 into the output
+// arrays, so no thread reads a value another one writes.
+template <class S, class M>
+__global__ void __launch_bounds__(BX * BY) k_cell_sweep_x(M m, int variant, GeomArrays ga,
+    const typename S::rho_t* __restrict__ d_in, const typename S::ene_t* __restrict__ e_in,
+    typename S::rho_t* __restrict__ d_out, typename S::ene_t* __restrict__ e_out,
     const typename S::vf_t* __restrict__ vfx, const typename S::vf_t* __restrict__ vfy,
-    const typename S::vf_t* __restrict__ vfz, typename S::mf_t* __restrict__ mass_flux,
-    typename S::wk_t* __restrict__ ener_flux) {
+    const typename S::vf_t* __restrict__ vfz, typename S::mf_t* __restrict__ mass_flux) {
   m.run([&](const Geom& g, const Tile& t) {
-  const Box b = cell_flux_box<DIR>(g);
-  const int j = b.j0 + t.x * BX + threadIdx.x;
-  const int k = b.k0 + t.y * BY + threadIdx.y;
-  const int l = b.l0 + t.z;
-  if (j > b.j1 || k > b.k1) return;
-  const typename S::vf_t* vf_d = DIR == 1 ? vfx : DIR == 2 ? vfy : vfz;
-  const int i = DIR == 1 ? j : DIR == 2 ? k : l;
-  const int imax = DIR == 1 ? g.x_max : DIR == 2 ? g.y_max : g.z_max;
-  const double* vd = DIR == 1 ? ga.vertexdx : DIR == 2 ? ga.vertexdy : ga.vertexdz;
-  const int vlo = DIR == 1 ? g.x_min : DIR == 2 ? g.y_min : g.z_min;
-  const double vf = L(vf_d, j, k, l);
-  int upwind, donor, downwind, dif;
-  if (vf > 0.0) {
-    upwind = i - 2; donor = i - 1; downwind = i; dif = donor;
-  } else {
-    upwind = (i + 1 < imax + 2) ? i + 1 : imax + 2;
-    donor = i; downwind = i - 1; dif = upwind;
+  const int lane = threadIdx.x;
+  const int c = g.x_min - 2 + t.x * 28 + lane;
+  const int k = g.y_min + t.y * BY + threadIdx.y;
+  const int l = g.z_min + t.z;
+  const bool row = k <= g.y_max;  // every lane of a row stays for the shuffles
+  const bool lds = row && c <= g.x_max + 2;
+  const int top = g.x_max + 2;
+  const unsigned full = 0xffffffffu;
+  double d = 0.0, e = 0.0, pv = 0.0, vf = 0.0, vd = 1.0;
+  if (lds) {
+    d = L(d_in, c, k, l);
+    e = L(e_in, c, k, l);
+    pv = cell_pre_vol<S>(g, variant, ga, vfx, vfy, vfz, c, k, l);
+    vf = L(vfx, c, k, l);
+    vd = GX(ga.vertexdx, c);
   }
-#define AT(a, ii) L(a, DIR == 1 ? (ii) : j, DIR == 2 ? (ii) : k, DIR == 3 ? (ii) : l)
-  const double pv_donor = cell_pre_vol<S>(g, variant, ga, vfx, vfy, vfz, DIR == 1 ? donor : j,
-                                          DIR == 2 ? donor : k, DIR == 3 ? donor : l);
-  const double sigmat = fabs(vf) / pv_donor;
-  const double sigma3 = (1.0 + sigmat) * (vd[g.o1 + i - vlo + 2] / vd[g.o1 + dif - vlo + 2]);
-  const double sigma4 = 2.0 - sigmat;
-  const double d_donor = AT(density1, donor);
-  double diffuw = d_donor - AT(density1, upwind);
-  double diffdw = AT(density1, downwind) - d_donor;
-  double limiter = cell_limiter(sigmat, sigma3, sigma4, diffuw, diffdw);
-  const double mflux = vf * (d_donor + limiter);
-  E(mass_flux, j, k, l) = st<typename S::mf_t>(mflux);
-  const double sigmam = fabs(mflux) / (d_donor * pv_donor);
-  const double e_donor = AT(energy1, donor);
-  diffuw = e_donor - AT(energy1, upwind);
-  diffdw = AT(energy1, downwind) - e_donor;
-  limiter = cell_limiter(sigmam, sigma3, sigma4, diffuw, diffdw);
-  E(ener_flux, j, k, l) = st<typename S::wk_t>(mflux * (e_donor + limiter));
-#undef AT
+  const double d_m2 = __shfl_up_sync(full, d, 2), d_m1 = __shfl_up_sync(full, d, 1);
+  const double d_p1 = __shfl_down_sync(full, d, 1);
+  const double e_m2 = __shfl_up_sync(full, e, 2), e_m1 = __shfl_up_sync(full, e, 1);
+  const double e_p1 = __shfl_down_sync(full, e, 1);
+  const double pv_m1 = __shfl_up_sync(full, pv, 1);
+  const double vd_m1 = __shfl_up_sync(full, vd, 1), vd_p1 = __shfl_down_sync(full, vd, 1);
+  const bool face = lds && lane >= 2 && lane <= 30 && c >= g.x_min;
+  using MF = typename S::mf_t;
+  double mf_st = 0.0, ef = 0.0;
+  if (face) {
+    // advec_cell_kernel.f90:131-169 at face c; the upwind index clamps to x_max+2
+    double d_up, d_don, d_dn, e_up, e_don, e_dn, pv_don, vd_dif;
+    if (vf > 0.0) {  // upwind c-2, donor c-1, downwind c
+      d_up = d_m2; d_don = d_m1; d_dn = d; e_up = e_m2; e_don = e_m1; e_dn = e;
+      pv_don = pv_m1; vd_dif = vd_m1;
+    } else {  // upwind min(c+1, x_max+2), donor c, downwind c-1
+      const bool clamp = c + 1 > top;
+      d_up = clamp ? d : d_p1; d_don = d; d_dn = d_m1;
+      e_up = clamp ? e : e_p1; e_don = e; e_dn = e_m1;
+      pv_don = pv; vd_dif = clamp ? vd : vd_p1;
+    }
+    const double sigmat = fabs(vf) / pv_don;
+    const double sigma3 = (1.0 + sigmat) * (vd / vd_dif);
+    const double sigma4 = 2.0 - sigmat;
+    double diffuw = d_don - d_up;
+    double diffdw = d_dn - d_don;
+    double limiter = cell_limiter(sigmat, sigma3, sigma4, diffuw, diffdw);
+    const double mflux = vf * (d_don + limiter);
+    mf_st = (double)st<MF>(mflux);
+    if (lane <= 29) E(mass_flux, c, k, l) = st<MF>(mflux);
+    const double sigmam = fabs(mflux) / (d_don * pv_don);
+    diffuw = e_don - e_up;
+    diffdw = e_dn - e_don;
+    limiter = cell_limiter(sigmam, sigma3, sigma4, diffuw, diffdw);
+    ef = (double)st<typename S::wk_t>(mflux * (e_don + limiter));
+  }
+  // advec_cell_kernel.f90:173-185 for cell c from faces c and c+1
+  const double mf_p = __shfl_down_sync(full, mf_st, 1);
+  const double ef_p = __shfl_down_sync(full, ef, 1);
+  const double vf_p = __shfl_down_sync(full, vf, 1);
+  if (face && lane <= 29 && c <= g.x_max) {
+    const double pm = d * pv;
+    const double pom = pm + mf_st - mf_p;
+    const double poe = (e * pm + ef - ef_p) / pom;
+    const double av = pv + vf - vf_p;
+    E(d_out, c, k, l) = st<typename S::rho_t>(pom / av);
+    E(e_out, c, k, l) = st<typename S::ene_t>(poe);
+  }
   });
 }
 
-// advec_cell update pass, in place (each thread reads and writes its own cell).
-template <class S, int DIR, class M>
-__global__ void __launch_bounds__(BX * BY) k_cell_update_f(M m, int variant, GeomArrays ga,
-    typename S::rho_t* __restrict__ density1, typename S::ene_t* __restrict__ energy1,
-    const typename S::vf_t* __restrict__ vfx, const typename S::vf_t* __restrict__ vfy,
-    const typename S::vf_t* __restrict__ vfz, const typename S::mf_t* __restrict__ mass_flux,
-    const typename S::wk_t* __restrict__ ener_flux) {
+// Copy the cells of two cell arrays outside the interior (the halo shell
+// [min-2, max+2]^3 minus [min, max]^3) from one buffer to the other.
+template <class R, class En, class M>
+__global__ void k_cell_shell_copy(M m, const R* __restrict__ a_in, const En* __restrict__ b_in,
+                                  R* __restrict__ a_out, En* __restrict__ b_out) {
   m.run([&](const Geom& g, const Tile& t) {
-  const Box b = interior(g);
-  const int j = b.j0 + t.x * BX + threadIdx.x;
-  const int k = b.k0 + t.y * BY + threadIdx.y;
-  const int l = b.l0 + t.z;
-  if (j > b.j1 || k > b.k1) return;
-  const typename S::vf_t* vf_d = DIR == 1 ? vfx : DIR == 2 ? vfy : vfz;
-  const int j1 = j + (DIR == 1), k1 = k + (DIR == 2), l1 = l + (DIR == 3);
-  const double pv = cell_pre_vol<S>(g, variant, ga, vfx, vfy, vfz, j, k, l);
-  const double pm = L(density1, j, k, l) * pv;
-  const double pom = pm + L(mass_flux, j, k, l) - L(mass_flux, j1, k1, l1);
-  const double poe = (L(energy1, j, k, l) * pm + L(ener_flux, j, k, l) - L(ener_flux, j1, k1, l1)) / pom;
-  const double av = pv + L(vf_d, j, k, l) - L(vf_d, j1, k1, l1);
-  E(density1, j, k, l) = st<typename S::rho_t>(pom / av);
-  E(energy1, j, k, l) = st<typename S::ene_t>(poe);
+  const int j = g.x_min - 2 + t.x * BX + threadIdx.x;
+  const int k = g.y_min - 2 + t.y * BY + threadIdx.y;
+  const int l = g.z_min - 2 + t.z;
+  if (j > g.x_max + 2 || k > g.y_max + 2) return;
+  const bool inside = j >= g.x_min && j <= g.x_max && k >= g.y_min && k <= g.y_max &&
+                      l >= g.z_min && l <= g.z_max;
+  if (inside) return;
+  const long long o = off3(g, j, k, l);
+  a_out[o] = a_in[o];
+  b_out[o] = b_in[o];
   });
 }
 
@@ -1017,7 +1038,15 @@ constexpr int kMarchSeg = 32;
 dim3 grid_interior(const Geom& g, int) { return grid_of(interior(g)); }
 dim3 grid_nodes(const Geom& g, int) { return grid_of(nodes(g)); }
 dim3 grid_visc(const Geom& g, int) { return grid_of(interior(g), kViscCellsZ); }
-dim3 grid_cell_flux_x(const Geom& g, int) { return grid_of(cell_flux_box<1>(g)); }
+// 28 cells per warp along x (faces x_min..x_max+2), rows of 8, one plane
+dim3 grid_cell_sweep_x(const Geom& g, int) {
+  return dim3((g.x_max + 2 - g.x_min + 1 + 27) / 28, (g.y_max - g.y_min + 1 + BY - 1) / BY,
+              g.z_max - g.z_min + 1);
+}
+dim3 grid_cell_shell(const Geom& g, int) {
+  return dim3((g.x_max - g.x_min + 5 + BX - 1) / BX, (g.y_max - g.y_min + 5 + BY - 1) / BY,
+              g.z_max - g.z_min + 5);
+}
 // 32 columns j of one cross-axis index per block, BY segments along the sweep
 template <int DIR>
 dim3 grid_cell_sweep(const Geom& g, int) {
@@ -1103,14 +1132,9 @@ void launch_advec_cell_fused(const Target& tg, cudaStream_t s, int advect_x, int
   if (dir == 1) variant = sweep == 1 ? 0 : 1;
   else if (dir == 2) variant = advect_x ? 2 : 3;
   else variant = sweep == 1 ? 4 : 5;
+  (void)ener_flux;
   if (dir == 1) {
-    // face pass, then the update pass
-    launch_mapped(tg, s, kKeyCellFluxX, grid_cell_flux_x, 0, false, kBlk,
-                  k_cell_flux_f<S, 1, MapSingle>, k_cell_flux_f<S, 1, MapBatch>, variant, ga,
-                  density1, energy1, vol_flux_x, vol_flux_y, vol_flux_z, mass_flux_x, ener_flux);
-    launch_mapped(tg, s, kKeyCellUpdateX, grid_interior, 0, false, kBlk,
-                  k_cell_update_f<S, 1, MapSingle>, k_cell_update_f<S, 1, MapBatch>, variant, ga,
-                  density1, energy1, vol_flux_x, vol_flux_y, vol_flux_z, mass_flux_x, ener_flux);
+    return;  // the x sweep is out of place: launch_advec_cell_x
   } else if (dir == 2) {
     // one marching pass, in place
     launch_mapped(tg, s, kKeyCellSweep | 2u, grid_cell_sweep<2>, 0, false, kBlk,
@@ -1121,6 +1145,25 @@ void launch_advec_cell_fused(const Target& tg, cudaStream_t s, int advect_x, int
                   k_cell_sweep_march<S, 3, MapSingle>, k_cell_sweep_march<S, 3, MapBatch>,
                   variant, ga, density1, energy1, vol_flux_x, vol_flux_y, vol_flux_z, mass_flux_z);
   }
+}
+
+template <class S>
+void launch_advec_cell_x(const Target& tg, cudaStream_t s, int sweep, const GeomArrays& ga,
+                         const typename S::rho_t* density1_in, const typename S::ene_t* energy1_in,
+                         typename S::rho_t* density1_out, typename S::ene_t* energy1_out,
+                         const typename S::vf_t* vol_flux_x, const typename S::vf_t* vol_flux_y,
+                         const typename S::vf_t* vol_flux_z, typename S::mf_t* mass_flux_x) {
+  const int variant = sweep == 1 ? 0 : 1;
+  launch_mapped(tg, s, kKeyCellSweepX, grid_cell_sweep_x, 0, false, kBlk,
+                k_cell_sweep_x<S, MapSingle>, k_cell_sweep_x<S, MapBatch>, variant, ga,
+                density1_in, energy1_in, density1_out, energy1_out, vol_flux_x, vol_flux_y,
+                vol_flux_z, mass_flux_x);
+  // the cells the sweep does not update keep their values in the output pair
+  using R = typename S::rho_t;
+  using En = typename S::ene_t;
+  launch_mapped(tg, s, kKeyCellShell, grid_cell_shell, 0, false, kBlk,
+                k_cell_shell_copy<R, En, MapSingle>, k_cell_shell_copy<R, En, MapBatch>,
+                density1_in, energy1_in, density1_out, energy1_out);
 }
 
 template <class S>
@@ -1191,6 +1234,10 @@ void launch_advec_mom_fused(const Target& tg, cudaStream_t s, int advect_x, int 
                                            const GeomArrays&, S::rho_t*, S::ene_t*, S::mf_t*,  \
                                            const S::vf_t*, S::mf_t*, const S::vf_t*, S::mf_t*, \
                                            const S::vf_t*, S::wk_t*);                          \
+  template void launch_advec_cell_x<S>(const Target&, cudaStream_t, int, const GeomArrays&,      \
+                                       const S::rho_t*, const S::ene_t*, S::rho_t*, S::ene_t*,  \
+                                       const S::vf_t*, const S::vf_t*, const S::vf_t*,          \
+                                       S::mf_t*);                                               \
   template void launch_advec_mom_fused<S>(const Target&, cudaStream_t, int, int, int, double,    \
                                           const GeomArrays&, const S::rho_t*, const S::mf_t*,  \
                                           const S::mf_t*, const S::mf_t*, const S::vf_t*,      \

@@ -90,7 +90,7 @@ inline void launch_mapped(const Target& tg, cudaStream_t s, unsigned key, GridFn
 enum : unsigned {
   kKeyIdealGas = 1u << 8, kKeyCalcDt = 2u << 8, kKeyReset = 3u << 8, kKeyHalo = 4u << 8,
   kKeyTimestepVisc = 5u << 8, kKeyPdvPredict = 6u << 8, kKeyPdvFlux = 7u << 8,
-  kKeyCellFluxX = 8u << 8, kKeyCellUpdateX = 9u << 8, kKeyCellSweep = 10u << 8,
+  kKeyCellSweepX = 8u << 8, kKeyCellShell = 9u << 8, kKeyCellSweep = 10u << 8,
   kKeyMomSweepX = 11u << 8, kKeyMomNode = 12u << 8, kKeyMomVel3 = 13u << 8,
   kKeyShellCopy = 14u << 8, kKeySummary = 15u << 8, kKeyAccelerate = 16u << 8,
   kKeyHaloX = 17u << 8
@@ -319,6 +319,14 @@ void launch_advec_cell_fused(const Target& tg, cudaStream_t s, int advect_x, int
                              const typename S::vf_t* vol_flux_x, typename S::mf_t* mass_flux_y,
                              const typename S::vf_t* vol_flux_y, typename S::mf_t* mass_flux_z,
                              const typename S::vf_t* vol_flux_z, typename S::wk_t* ener_flux);
+// The x cell sweep out of place: density1/energy1 in one buffer pair, the
+// updated values (and a copy of every cell outside the interior) in the other.
+template <class S>
+void launch_advec_cell_x(const Target& tg, cudaStream_t s, int sweep, const GeomArrays& ga,
+                         const typename S::rho_t* density1_in, const typename S::ene_t* energy1_in,
+                         typename S::rho_t* density1_out, typename S::ene_t* energy1_out,
+                         const typename S::vf_t* vol_flux_x, const typename S::vf_t* vol_flux_y,
+                         const typename S::vf_t* vol_flux_z, typename S::mf_t* mass_flux_x);
 // All three velocities of one sweep; vel_in/vel_out are the two buffers of
 // each velocity pair (the shell outside [min,max+1]^3 is copied across).
 // vol: the uniform cell volume of the chunk (dx*dy*dz).

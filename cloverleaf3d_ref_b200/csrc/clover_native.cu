@@ -126,6 +126,8 @@ struct Chunk : ChunkBase {
   C *pressure, *viscosity, *soundspeed;
   V *xvel0, *xvel1, *yvel0, *yvel1, *zvel0, *zvel1;
   V* vel1b[3];  // second buffer of each time-level-1 velocity (fused step)
+  R* rho1b;     // second buffer of density1 and energy1 (the fused x cell sweep
+  En* e1b;      // writes out of place)
   VF *vol_flux_x, *vol_flux_y, *vol_flux_z;
   MF *mass_flux_x, *mass_flux_y, *mass_flux_z;
   W* work[7];
@@ -211,20 +213,25 @@ struct Chunk : ChunkBase {
   // the buffer holding time level 1 velocities after `steps` fused steps:
   // each step flips the pair three times (one per sweep)
   int vel1_buffer(int steps) const { return fused ? steps % 2 : 0; }
+  // density1/energy1 pair b, and the buffer holding them after `steps` fused
+  // steps (the x cell sweep flips it once per step)
+  R* rho1(int b) const { return b ? rho1b : density1; }
+  En* ene1(int b) const { return b ? e1b : energy1; }
+  int cell_buffer(int steps) const { return fused ? steps % 2 : 0; }
 
-  HaloFields halo_fields(int vb) {
+  HaloFields halo_fields(int vb, int cb) {
     HaloFields h;
-    void* f[19] = {density0, density1, energy0, energy1, pressure, viscosity, soundspeed,
+    void* f[19] = {density0, rho1(cb), energy0, ene1(cb), pressure, viscosity, soundspeed,
                    xvel0, vel1(0, vb), yvel0, vel1(1, vb), zvel0, vel1(2, vb), vol_flux_x,
                    vol_flux_y, vol_flux_z, mass_flux_x, mass_flux_y, mass_flux_z};
     for (int i = 0; i < 19; i++) h.f[i] = f[i];
     return h;
   }
 
-  void halo(std::initializer_list<int> ids, int depth, int vb = 0) {
+  void halo(std::initializer_list<int> ids, int depth, int vb = 0, int cb = 0) {
     int fields[19] = {0};
     for (int id : ids) fields[id - 1] = 1;
-    launch_update_halo<S>(tg, stream, halo_fields(vb), fields, depth, ext);
+    launch_update_halo<S>(tg, stream, halo_fields(vb, cb), fields, depth, ext);
   }
 
   int deck_blocks() const { return (nd + 127) / 128; }
@@ -274,6 +281,8 @@ struct Chunk : ChunkBase {
     chk(zvel0 = alloc_field<V>(e3, owned, bytes, stream));
     chk(zvel1 = alloc_field<V>(e3, owned, bytes, stream));
     for (int c3 = 0; c3 < 3; c3++) chk(vel1b[c3] = alloc_field<V>(e3, owned, bytes, stream));
+    chk(rho1b = alloc_field<R>(e3, owned, bytes, stream));
+    chk(e1b = alloc_field<En>(e3, owned, bytes, stream));
     chk(vol_flux_x = alloc_field<VF>(e3, owned, bytes, stream));
     chk(vol_flux_y = alloc_field<VF>(e3, owned, bytes, stream));
     chk(vol_flux_z = alloc_field<VF>(e3, owned, bytes, stream));
@@ -531,7 +540,7 @@ struct Chunk : ChunkBase {
 
   int visit() {
     launch_ideal_gas<S>(tg, stream, density0, energy0, pressure, soundspeed);
-    halo({5, 8, 10, 12}, 1, vel1_buffer(host_step));
+    halo({5, 8, 10, 12}, 1, vel1_buffer(host_step), cell_buffer(host_step));
     for (int d = 0; d < nd; d++)
       launch_viscosity<S>(geoms[d], stream, ga, density0, pressure, viscosity, xvel0, yvel0, zvel0);
     if (cudaStreamSynchronize(stream) != cudaSuccess) return -1;
@@ -685,13 +694,14 @@ struct Chunk : ChunkBase {
     const double R8 = sizeof(R), E8 = sizeof(En), C8 = sizeof(C), V8 = sizeof(V),
                  VF8 = sizeof(VF), MF8 = sizeof(MF), W8 = sizeof(W), G8 = sizeof(double);
     int vc = ax ? 0 : 1;  // buffer of the velocity pairs at the start of this step
+    int cb = ax ? 0 : 1;  // buffer of the density1/energy1 pair at the start of this step
     // timestep.f90:56-126
     k_dt_prepare<<<deck_blocks(), 128, 0, stream>>>(sc, nd, min_key_of(kGBig));
     pbeg();
     launch_ideal_gas<S>(tg, stream, density0, energy0, pressure, soundspeed);
     pend("ideal_gas", n * (R8 + E8 + 2 * C8));
     pbeg();
-    halo({5, 3, 1, 8, 10}, 1, vc);
+    halo({5, 3, 1, 8, 10}, 1, vc, cb);
     pend("update_halo", 0);
     pbeg();
     launch_visc_dt<S>(tg, stream, ga, kGSmall, deck.dtc_safe, deck.dtu_safe, deck.dtv_safe,
@@ -700,7 +710,7 @@ struct Chunk : ChunkBase {
     k_dt_finalize<<<deck_blocks(), 128, 0, stream>>>(sc, nd, dt_hist);
     pend("viscosity_calc_dt", n * (3 * V8 + 4 * G8 + R8 + 3 * C8));
     pbeg();
-    halo({6}, 1, vc);  // read by accelerate at its neighbours
+    halo({6}, 1, vc, cb);  // read by accelerate at its neighbours
     pend("update_halo", 0);
     // PdV.f90:50-107: predictor + EOS on the predicted state; revert is implied
     pbeg();
@@ -708,14 +718,14 @@ struct Chunk : ChunkBase {
                               yvel0, zvel0);
     pend("pdv", n * (4 * G8 + R8 + E8 + 3 * C8 + 3 * V8));
     pbeg();
-    halo({5}, 1, vc);
+    halo({5}, 1, vc, cb);
     pend("update_halo", 0);
     pbeg();
     launch_accelerate<S>(tg, stream, 0.0, dtp, ga, density0, pressure, viscosity, xvel0, yvel0,
                          zvel0, vel1(0, vc), vel1(1, vc), vel1(2, vc));
     pend("accelerate", n * (4 * G8 + R8 + 2 * C8 + 6 * V8));
     pbeg();
-    launch_pdv_flux<S>(tg, stream, dtp, ga, density0, density1, energy0, energy1, pressure,
+    launch_pdv_flux<S>(tg, stream, dtp, ga, density0, rho1(cb), energy0, ene1(cb), pressure,
                        viscosity, xvel0, vel1(0, vc), yvel0, vel1(1, vc), zvel0, vel1(2, vc),
                        vol_flux_x, vol_flux_y, vol_flux_z);
     pend("pdv_flux", n * (4 * G8 + 2 * R8 + 2 * E8 + 2 * C8 + 6 * V8 + 3 * VF8));
@@ -724,35 +734,39 @@ struct Chunk : ChunkBase {
     auto sweep = [&](int sweep_number, int dir, bool pre_halo) {
       if (pre_halo) {
         pbeg();
-        halo({4, 2, 14, 15, 16}, 2, vc);
+        halo({4, 2, 14, 15, 16}, 2, vc, cb);
         pend("update_halo", 0);
       }
       // volume fluxes read for pre_vol: all three on sweep 1, two on the y sweep,
       // the sweep direction only on sweep 3
       const double nvf = sweep_number == 1 ? 3 : sweep_number == 2 ? 2 : 1;
       pbeg();
-      launch_advec_cell_fused<S>(tg, stream, axi, dir, sweep_number, ga, density1, energy1,
-                                 mass_flux_x, vol_flux_x, mass_flux_y, vol_flux_y, mass_flux_z,
-                                 vol_flux_z, work[6]);
-      // x: face pass + update pass; y, z: one marching pass (in place)
-      if (dir == 1)
-        pend("advec_cell_x", n * ((G8 + nvf * VF8 + R8 + E8 + MF8 + W8) +
-                                  (G8 + nvf * VF8 + 2 * R8 + 2 * E8 + MF8 + W8)));
-      else
+      if (dir == 1) {
+        // one pass, out of place into the other buffer of the pair
+        launch_advec_cell_x<S>(tg, stream, sweep_number, ga, rho1(cb), ene1(cb), rho1(cb ^ 1),
+                               ene1(cb ^ 1), vol_flux_x, vol_flux_y, vol_flux_z, mass_flux_x);
+        cb ^= 1;
+        pend("advec_cell_x", n * (G8 + nvf * VF8 + 2 * R8 + 2 * E8 + MF8));
+      } else {
+        // one marching pass, in place
+        launch_advec_cell_fused<S>(tg, stream, axi, dir, sweep_number, ga, rho1(cb), ene1(cb),
+                                   mass_flux_x, vol_flux_x, mass_flux_y, vol_flux_y,
+                                   mass_flux_z, vol_flux_z, work[6]);
         pend("advec_cell_yz", n * (G8 + nvf * VF8 + 2 * R8 + 2 * E8 + MF8));
+      }
       pbeg();
-      halo({2, 4, 9, 11, 13, 17, 18, 19}, 2, vc);
+      halo({2, 4, 9, 11, 13, 17, 18, 19}, 2, vc, cb);
       pend("update_halo", 0);
       // post_vol reads two volume fluxes on sweep 1, one on sweep 2, none on sweep 3
       const double npv = sweep_number == 1 ? 2 : sweep_number == 2 ? 1 : 0;
       V* vin[3] = {vel1(0, vc), vel1(1, vc), vel1(2, vc)};
       V* vout[3] = {vel1(0, vc ^ 1), vel1(1, vc ^ 1), vel1(2, vc ^ 1)};
       pbeg();
-      launch_advec_mom_fused<S>(tg, stream, axi, sweep_number, dir, cell_volume, ga, density1, mass_flux_x,
+      launch_advec_mom_fused<S>(tg, stream, axi, sweep_number, dir, cell_volume, ga, rho1(cb), mass_flux_x,
                                 mass_flux_y, mass_flux_z, vol_flux_x, vol_flux_y, vol_flux_z,
                                 work[0], work[1], work[2], vin, vout);
-      // x: node pass + velocity pass; y, z: one marching pass
-      if (dir == 1)  // one pass
+      // x: one pass; y, z: node pass + velocity pass
+      if (dir == 1)
         pend("advec_mom_x", n * (MF8 + R8 + G8 + npv * VF8 + 6 * V8));
       else  // node pass + velocity pass
         pend("advec_mom_yz", n * ((MF8 + R8 + G8 + npv * VF8 + 3 * W8) + (3 * W8 + 6 * V8)));
@@ -762,7 +776,7 @@ struct Chunk : ChunkBase {
     sweep(2, 2, true);
     sweep(3, ax ? 3 : 1, false);
     pbeg();
-    launch_reset_field<S>(tg, stream, density0, density1, energy0, energy1, xvel0, vel1(0, vc),
+    launch_reset_field<S>(tg, stream, density0, rho1(cb), energy0, ene1(cb), xvel0, vel1(0, vc),
                           yvel0, vel1(1, vc), zvel0, vel1(2, vc));
     pend("reset_field", n * (2 * R8 + 2 * E8 + 6 * V8));
     k_step_end<<<deck_blocks(), 128, 0, stream>>>(sc, nd);
@@ -970,8 +984,8 @@ struct Chunk : ChunkBase {
   int read_field(int id, double* host, bool write, int deck_index = 0) {
     if (id < 1 || id > 19 || deck_index < 0 || deck_index >= nd) return -1;
     const Geom& g = geoms[deck_index];
-    const int vb = vel1_buffer(host_step);
-    void* f[19] = {density0, density1, energy0, energy1, pressure, viscosity, soundspeed,
+    const int vb = vel1_buffer(host_step), cb = cell_buffer(host_step);
+    void* f[19] = {density0, rho1(cb), energy0, ene1(cb), pressure, viscosity, soundspeed,
                    xvel0, vel1(0, vb), yvel0, vel1(1, vb), zvel0, vel1(2, vb), vol_flux_x,
                    vol_flux_y, vol_flux_z, mass_flux_x, mass_flux_y, mass_flux_z};
     const int eb[19] = {(int)sizeof(R), (int)sizeof(R), (int)sizeof(En), (int)sizeof(En),
