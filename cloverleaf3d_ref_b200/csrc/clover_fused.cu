@@ -47,6 +47,28 @@ inline dim3 grid_of(const Box& b, int march = 1) {
   return dim3((nj + BX - 1) / BX, (nk + BY - 1) / BY, (nl + march - 1) / march);
 }
 
+// The thread's (j, k) in tile t of box b: 32 x 8 tiles for one chunk; for a
+// batch, tile t.x holds the 256 consecutive cells t.x*256.. of the box's
+// (j, k) plane in row order (MapBatch::kFlat). False outside the box.
+template <class M>
+__device__ __forceinline__ bool tile_jk(const Box& b, const Tile& t, int& j, int& k) {
+  if (M::kFlat) {
+    const int nj = b.j1 - b.j0 + 1, nk = b.k1 - b.k0 + 1;
+    const int i = t.x * (BX * BY) + (int)threadIdx.y * BX + (int)threadIdx.x;
+    j = b.j0 + i % nj;
+    k = b.k0 + i / nj;
+    return i < nj * nk;
+  }
+  j = b.j0 + t.x * BX + (int)threadIdx.x;
+  k = b.k0 + t.y * BY + (int)threadIdx.y;
+  return j <= b.j1 && k <= b.k1;
+}
+inline dim3 grid_flat(const Box& b, int zdiv = 1) {
+  const long long nj = b.j1 - b.j0 + 1, nk = b.k1 - b.k0 + 1, nl = b.l1 - b.l0 + 1;
+  if (nj <= 0 || nk <= 0 || nl <= 0) return dim3(0, 0, 0);
+  return dim3((unsigned)((nj * nk + BX * BY - 1) / (BX * BY)), 1, (unsigned)((nl + zdiv - 1) / zdiv));
+}
+
 // Index ranges of the kernels, from a chunk's geometry (device: per tile of
 // a mapped kernel; host: the tile grid of a launch).
 __host__ __device__ inline Box interior(const Geom& g) {
@@ -137,15 +159,15 @@ __global__ void __launch_bounds__(BX * BY, 3) k_visc_dt(M m, GeomArrays ga, doub
   const A a_gs = (A)g_small, a_dtc = (A)dtc_safe, a_dtu = (A)dtu_safe, a_dtv = (A)dtv_safe;
   const A a_dtw = (A)dtw_safe, a_dtdiv = (A)dtdiv_safe;
   const Box b = interior(g);
-  const int j = b.j0 + t.x * BX + threadIdx.x;
-  const int k = b.k0 + t.y * BY + threadIdx.y;
+  int j, k;
+  const bool in_jk = tile_jk<M>(b, t, j, k);
   unsigned long long key = ~0ull;
   // kViscCellsZ cells along z per thread, unrolled so that the loads of one
   // cell are in flight with the arithmetic of the other
 #pragma unroll
   for (int iz = 0; iz < kViscCellsZ; iz++) {
   const int l = b.l0 + t.z * kViscCellsZ + iz;
-  if (j <= b.j1 && k <= b.k1 && l <= b.l1) {
+  if (in_jk && l <= b.l1) {
   const A u000 = LA(xvel0, j, k, l), u100 = LA(xvel0, j + 1, k, l);
   const A u010 = LA(xvel0, j, k + 1, l), u110 = LA(xvel0, j + 1, k + 1, l);
   const A u001 = LA(xvel0, j, k, l + 1), u101 = LA(xvel0, j + 1, k, l + 1);
@@ -277,10 +299,9 @@ __global__ void __launch_bounds__(BX * BY) k_pdv_predict_eos(M m, const double* 
     const typename S::vel_t* __restrict__ yvel0, const typename S::vel_t* __restrict__ zvel0) {
   m.run([&](const Geom& g, const Tile& t) {
   const Box b = interior(g);
-  const int j = b.j0 + t.x * BX + threadIdx.x;
-  const int k = b.k0 + t.y * BY + threadIdx.y;
+  int j, k;
+  if (!tile_jk<M>(b, t, j, k)) return;
   const int l = b.l0 + t.z;
-  if (j > b.j1 || k > b.k1) return;
   // predictor and EOS in the policy's arithmetic (FP64, or FP32 in the mixed
   // path: only the pressure, stored in FP32 there, comes out of it)
   using A = typename S::arith_t;
@@ -347,10 +368,9 @@ __global__ void __launch_bounds__(BX * BY, 5) k_pdv_flux(M m, const double* dt_p
     typename S::vf_t* __restrict__ vol_flux_y, typename S::vf_t* __restrict__ vol_flux_z) {
   m.run([&](const Geom& g, const Tile& t) {
   const Box b = nodes(g);
-  const int j = b.j0 + t.x * BX + threadIdx.x;
-  const int k = b.k0 + t.y * BY + threadIdx.y;
+  int j, k;
+  if (!tile_jk<M>(b, t, j, k)) return;
   const int l = b.l0 + t.z;
-  if (j > b.j1 || k > b.k1) return;
   const double dt = dt_ptr[(long long)t.d * kScalarStride];
   const bool jin = j <= g.x_max, kin = k <= g.y_max, lin = l <= g.z_max;
   using F = typename S::vf_t;
@@ -530,10 +550,9 @@ template <class R, class En, class M>
 __global__ void k_cell_shell_copy(M m, const R* __restrict__ a_in, const En* __restrict__ b_in,
                                   R* __restrict__ a_out, En* __restrict__ b_out) {
   m.run([&](const Geom& g, const Tile& t) {
-  const int j = g.x_min - 2 + t.x * BX + threadIdx.x;
-  const int k = g.y_min - 2 + t.y * BY + threadIdx.y;
+  int j, k;
+  if (!tile_jk<M>(Box{g.x_min - 2, g.x_max + 2, g.y_min - 2, g.y_max + 2, 0, 0}, t, j, k)) return;
   const int l = g.z_min - 2 + t.z;
-  if (j > g.x_max + 2 || k > g.y_max + 2) return;
   const bool inside = j >= g.x_min && j <= g.x_max && k >= g.y_min && k <= g.y_max &&
                       l >= g.z_min && l <= g.z_max;
   if (inside) return;
@@ -1016,10 +1035,9 @@ __global__ void k_vert_shell_copy(M m, const T* __restrict__ a_in, const T* __re
                                   const T* __restrict__ c_in, T* __restrict__ a_out,
                                   T* __restrict__ b_out, T* __restrict__ c_out) {
   m.run([&](const Geom& g, const Tile& t) {
-  const int j = g.x_min - 2 + t.x * BX + threadIdx.x;
-  const int k = g.y_min - 2 + t.y * BY + threadIdx.y;
+  int j, k;
+  if (!tile_jk<M>(Box{g.x_min - 2, g.x_max + 3, g.y_min - 2, g.y_max + 3, 0, 0}, t, j, k)) return;
   const int l = g.z_min - 2 + t.z;
-  if (j > g.x_max + 3 || k > g.y_max + 3) return;
   const bool inside = j >= g.x_min && j <= g.x_max + 1 && k >= g.y_min && k <= g.y_max + 1 &&
                       l >= g.z_min && l <= g.z_max + 1;
   if (inside) return;
@@ -1038,6 +1056,10 @@ constexpr int kMarchSeg = 32;
 dim3 grid_interior(const Geom& g, int) { return grid_of(interior(g)); }
 dim3 grid_nodes(const Geom& g, int) { return grid_of(nodes(g)); }
 dim3 grid_visc(const Geom& g, int) { return grid_of(interior(g), kViscCellsZ); }
+// the same laid out for a batch (tile_jk)
+dim3 grid_interior_flat(const Geom& g, int) { return grid_flat(interior(g)); }
+dim3 grid_nodes_flat(const Geom& g, int) { return grid_flat(nodes(g)); }
+dim3 grid_visc_flat(const Geom& g, int) { return grid_flat(interior(g), kViscCellsZ); }
 // 28 cells per warp along x (faces x_min..x_max+2), rows of 8, one plane
 dim3 grid_cell_sweep_x(const Geom& g, int) {
   return dim3((g.x_max + 2 - g.x_min + 1 + 27) / 28, (g.y_max - g.y_min + 1 + BY - 1) / BY,
@@ -1046,6 +1068,12 @@ dim3 grid_cell_sweep_x(const Geom& g, int) {
 dim3 grid_cell_shell(const Geom& g, int) {
   return dim3((g.x_max - g.x_min + 5 + BX - 1) / BX, (g.y_max - g.y_min + 5 + BY - 1) / BY,
               g.z_max - g.z_min + 5);
+}
+dim3 grid_cell_shell_flat(const Geom& g, int) {
+  return grid_flat(Box{g.x_min - 2, g.x_max + 2, g.y_min - 2, g.y_max + 2, g.z_min - 2, g.z_max + 2});
+}
+dim3 grid_shell_flat(const Geom& g, int) {
+  return grid_flat(Box{g.x_min - 2, g.x_max + 3, g.y_min - 2, g.y_max + 3, g.z_min - 2, g.z_max + 3});
 }
 // 32 columns j of one cross-axis index per block, BY segments along the sweep
 template <int DIR>
@@ -1088,7 +1116,7 @@ void launch_visc_dt(const Target& tg, cudaStream_t s, const GeomArrays& ga, doub
                     const typename S::cs_t* soundspeed, const typename S::vel_t* xvel0,
                     const typename S::vel_t* yvel0, const typename S::vel_t* zvel0,
                     unsigned long long* min_key) {
-  launch_mapped(tg, s, kKeyTimestepVisc, grid_visc, 0, false, kBlk, k_visc_dt<S, MapSingle>,
+  launch_mapped2(tg, s, kKeyTimestepVisc, grid_visc, grid_visc_flat, 0, false, kBlk, k_visc_dt<S, MapSingle>,
                 k_visc_dt<S, MapBatch>, ga, g_small, dtc_safe, dtu_safe, dtv_safe, dtw_safe,
                 dtdiv_safe, density0, pressure, viscosity, soundspeed, xvel0, yvel0, zvel0,
                 min_key);
@@ -1100,7 +1128,7 @@ void launch_pdv_predict_eos(const Target& tg, cudaStream_t s, const double* dt_p
                             const typename S::ene_t* energy0, typename S::cs_t* pressure,
                             const typename S::cs_t* viscosity, const typename S::vel_t* xvel0,
                             const typename S::vel_t* yvel0, const typename S::vel_t* zvel0) {
-  launch_mapped(tg, s, kKeyPdvPredict, grid_interior, 0, false, kBlk,
+  launch_mapped2(tg, s, kKeyPdvPredict, grid_interior, grid_interior_flat, 0, false, kBlk,
                 k_pdv_predict_eos<S, MapSingle>, k_pdv_predict_eos<S, MapBatch>, dt_ptr, ga,
                 density0, energy0, pressure, viscosity, xvel0, yvel0, zvel0);
 }
@@ -1115,7 +1143,7 @@ void launch_pdv_flux(const Target& tg, cudaStream_t s, const double* dt_ptr, con
                      const typename S::vel_t* zvel0, const typename S::vel_t* zvel1,
                      typename S::vf_t* vol_flux_x, typename S::vf_t* vol_flux_y,
                      typename S::vf_t* vol_flux_z) {
-  launch_mapped(tg, s, kKeyPdvFlux, grid_nodes, 0, false, kBlk, k_pdv_flux<S, MapSingle>,
+  launch_mapped2(tg, s, kKeyPdvFlux, grid_nodes, grid_nodes_flat, 0, false, kBlk, k_pdv_flux<S, MapSingle>,
                 k_pdv_flux<S, MapBatch>, dt_ptr, ga, density0, density1, energy0, energy1,
                 pressure, viscosity, xvel0, xvel1, yvel0, yvel1, zvel0, zvel1, vol_flux_x,
                 vol_flux_y, vol_flux_z);
@@ -1161,7 +1189,7 @@ void launch_advec_cell_x(const Target& tg, cudaStream_t s, int sweep, const Geom
   // the cells the sweep does not update keep their values in the output pair
   using R = typename S::rho_t;
   using En = typename S::ene_t;
-  launch_mapped(tg, s, kKeyCellShell, grid_cell_shell, 0, false, kBlk,
+  launch_mapped2(tg, s, kKeyCellShell, grid_cell_shell, grid_cell_shell_flat, 0, false, kBlk,
                 k_cell_shell_copy<R, En, MapSingle>, k_cell_shell_copy<R, En, MapBatch>,
                 density1_in, energy1_in, density1_out, energy1_out);
 }
@@ -1210,7 +1238,7 @@ void launch_advec_mom_fused(const Target& tg, cudaStream_t s, int advect_x, int 
   }
   // the updated buffers take the halo shell of the inputs
   using V = typename S::vel_t;
-  launch_mapped(tg, s, kKeyShellCopy, grid_shell, 0, false, kBlk, k_vert_shell_copy<V, MapSingle>,
+  launch_mapped2(tg, s, kKeyShellCopy, grid_shell, grid_shell_flat, 0, false, kBlk, k_vert_shell_copy<V, MapSingle>,
                 k_vert_shell_copy<V, MapBatch>, vel_in[0], vel_in[1], vel_in[2], vel_out[0],
                 vel_out[1], vel_out[2]);
 }

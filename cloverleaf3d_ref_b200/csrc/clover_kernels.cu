@@ -50,13 +50,39 @@ inline dim3 grid_nodes(const Geom& g, int) { return grid_of(nodes(g)); }
   const int l = (b).l0 + blockIdx.z;                     \
   if (j > (b).j1 || k > (b).k1) return
 
+// The thread's (j, k) in tile t of box b: 32 x 8 tiles for one chunk; for a
+// batch, tile t.x holds the 256 consecutive cells t.x*256.. of the box's
+// (j, k) plane in row order (MapBatch::kFlat). False outside the box.
+template <class M>
+__device__ __forceinline__ bool tile_jk(const Box& b, const Tile& t, int& j, int& k) {
+  if (M::kFlat) {
+    const int nj = b.j1 - b.j0 + 1, nk = b.k1 - b.k0 + 1;
+    const int i = t.x * (BX * BY) + (int)threadIdx.y * BX + (int)threadIdx.x;
+    j = b.j0 + i % nj;
+    k = b.k0 + i / nj;
+    return i < nj * nk;
+  }
+  j = b.j0 + t.x * BX + (int)threadIdx.x;
+  k = b.k0 + t.y * BY + (int)threadIdx.y;
+  return j <= b.j1 && k <= b.k1;
+}
+// flattened tile grid of a box for a batch: 256 cells of the (j, k) plane per
+// tile, planes along z
+inline dim3 grid_flat(const Box& b, int zdiv = 1) {
+  const long long nj = b.j1 - b.j0 + 1, nk = b.k1 - b.k0 + 1, nl = b.l1 - b.l0 + 1;
+  if (nj <= 0 || nk <= 0 || nl <= 0) return dim3(0, 0, 0);
+  return dim3((unsigned)((nj * nk + BX * BY - 1) / (BX * BY)), 1, (unsigned)((nl + zdiv - 1) / zdiv));
+}
+
+inline dim3 grid_interior_flat(const Geom& g, int) { return grid_flat(interior(g)); }
+inline dim3 grid_nodes_flat(const Geom& g, int) { return grid_flat(nodes(g)); }
+
 // the same for tile t of a mapped kernel (clover_sched.cuh)
 #define TILE_THREAD(box, t)                            \
   const Box b = (box);                                 \
-  const int j = b.j0 + (t).x * BX + threadIdx.x;       \
-  const int k = b.k0 + (t).y * BY + threadIdx.y;       \
-  const int l = b.l0 + (t).z;                          \
-  if (j > b.j1 || k > b.k1) return
+  int j, k;                                            \
+  if (!tile_jk<M>(b, (t), j, k)) return;               \
+  const int l = b.l0 + (t).z
 
 // 3D element, 1D coordinate arrays
 #define E(a, jj, kk, ll) (a)[off3(g, (jj), (kk), (ll))]
@@ -1087,7 +1113,7 @@ template <class S>
 void launch_ideal_gas(const Target& tg, cudaStream_t s, const typename S::rho_t* density,
                       const typename S::ene_t* energy, typename S::cs_t* pressure,
                       typename S::cs_t* soundspeed) {
-  launch_mapped(tg, s, kKeyIdealGas, grid_interior, 0, false, dim3(BX, BY),
+  launch_mapped2(tg, s, kKeyIdealGas, grid_interior, grid_interior_flat, 0, false, dim3(BX, BY),
                 k_ideal_gas<S, MapSingle>, k_ideal_gas<S, MapBatch>, density, energy, pressure,
                 soundspeed);
 }
@@ -1141,7 +1167,7 @@ void launch_accelerate(const Target& tg, cudaStream_t s, double dt_val, const do
                        const typename S::vel_t* xvel0, const typename S::vel_t* yvel0,
                        const typename S::vel_t* zvel0, typename S::vel_t* xvel1,
                        typename S::vel_t* yvel1, typename S::vel_t* zvel1) {
-  launch_mapped(tg, s, kKeyAccelerate, grid_nodes, 0, false, dim3(BX, BY),
+  launch_mapped2(tg, s, kKeyAccelerate, grid_nodes, grid_nodes_flat, 0, false, dim3(BX, BY),
                 k_accelerate<S, MapSingle>, k_accelerate<S, MapBatch>, dt_val, dt_ptr, ga,
                 density0, pressure, viscosity, xvel0, yvel0, zvel0, xvel1, yvel1, zvel1);
 }
@@ -1260,7 +1286,7 @@ void launch_reset_field(const Target& tg, cudaStream_t s, typename S::rho_t* den
                         const typename S::vel_t* xvel1, typename S::vel_t* yvel0,
                         const typename S::vel_t* yvel1, typename S::vel_t* zvel0,
                         const typename S::vel_t* zvel1) {
-  launch_mapped(tg, s, kKeyReset, grid_nodes, 0, false, dim3(BX, BY), k_reset<S, MapSingle>,
+  launch_mapped2(tg, s, kKeyReset, grid_nodes, grid_nodes_flat, 0, false, dim3(BX, BY), k_reset<S, MapSingle>,
                 k_reset<S, MapBatch>, density0, density1, energy0, energy1, xvel0, xvel1, yvel0,
                 yvel1, zvel0, zvel1);
 }

@@ -86,6 +86,20 @@ inline void launch_mapped(const Target& tg, cudaStream_t s, unsigned key, GridFn
   batch_mark(tg.plan, key, s, false);
 }
 
+// The same with another grid function for the batched launch (kernels whose
+// tiles a batch lays out differently, e.g. flattened (j, k) planes).
+template <class... P, class... A>
+inline void launch_mapped2(const Target& tg, cudaStream_t s, unsigned key, GridFn grid_single,
+                           GridFn grid_batch, int aux, bool seg_tunable, dim3 blk,
+                           void (*ks)(MapSingle, P...), void (*kb)(MapBatch, P...),
+                           A&&... args) {
+  if (!tg.plan) {
+    launch_mapped(tg, s, key, grid_single, aux, seg_tunable, blk, ks, kb, std::forward<A>(args)...);
+    return;
+  }
+  launch_mapped(tg, s, key, grid_batch, aux, seg_tunable, blk, ks, kb, std::forward<A>(args)...);
+}
+
 // Launch keys: kernel id in the high bits, the variant fixing the grid low.
 enum : unsigned {
   kKeyIdealGas = 1u << 8, kKeyCalcDt = 2u << 8, kKeyReset = 3u << 8, kKeyHalo = 4u << 8,

@@ -25,6 +25,7 @@ struct Tile {
 };
 
 struct MapSingle {
+  static constexpr bool kFlat = false;  // box kernels use 32 x 8 tiles of (j, k)
   Geom g;
   int seg;
   template <class F>
@@ -34,6 +35,9 @@ struct MapSingle {
 };
 
 struct MapBatch {
+  // box kernels take 256 consecutive cells of a deck's (j, k) plane per tile,
+  // so that decks whose x extent is not a multiple of 32 fill every lane
+  static constexpr bool kFlat = true;
   const int4* __restrict__ items;  // (deck, tile x, tile y, tile z)
   const Geom* __restrict__ decks;  // per deck geometry and offsets
   int n;                           // number of items
