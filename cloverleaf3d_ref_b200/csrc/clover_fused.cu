@@ -750,9 +750,8 @@ __global__ void __launch_bounds__(BX * BY, 3) k_mom_vel3_march(M m, GeomArrays g
   const MarchRange r = mom_vel_range<DIR>(g);
   const int jlo = r.jlo, jhi = r.jhi, clo = r.clo, chi = r.chi, plo = r.plo, phi = r.phi;
   const int seg = m.seg;
-  const int j = jlo + t.x * BX + threadIdx.x;
-  const int c = clo + t.y * BY + threadIdx.y;
-  if (j > jhi || c > chi) return;
+  int j, c;
+  if (!tile_jk<M>(Box{jlo, jhi, clo, chi, 0, 0}, t, j, c)) return;
   const int p0 = plo + t.z * seg;
   int p1 = p0 + seg - 1;
   if (p1 > phi) p1 = phi;
@@ -845,14 +844,27 @@ __global__ void __launch_bounds__(BX * BY, 3) k_cell_sweep_march(M m, int varian
   __shared__ double s_end[4][BY][BX];
   m.run([&](const Geom& g, const Tile& t) {
   const MarchRange r = cell_sweep_range<DIR>(g);
-  const int j = r.jlo + t.x * BX + threadIdx.x;
-  const int c = r.clo + t.y;
+  // one chunk: 32 columns j of one cross index c per block; a batch: 32
+  // consecutive columns of the deck's (j, c) plane in row order
+  int j, c;
+  bool col;
+  if (M::kFlat) {
+    const int nj = r.jhi - r.jlo + 1, nc = r.chi - r.clo + 1;
+    const int i = t.x * BX + (int)threadIdx.x;
+    j = r.jlo + i % nj;
+    c = r.clo + i / nj;
+    col = i < nj * nc;
+  } else {
+    j = r.jlo + t.x * BX + (int)threadIdx.x;
+    c = r.clo + t.y;
+    col = j <= r.jhi && c <= r.chi;
+  }
   const int pmin = DIR == 2 ? g.y_min : g.z_min;
   const int pmax = DIR == 2 ? g.y_max : g.z_max;
   const int len = (pmax - pmin + 1 + BY - 1) / BY;  // cells per segment
   const int c0 = pmin + (int)threadIdx.y * len;
   const int c1 = c0 + len - 1 < pmax ? c0 + len - 1 : pmax;
-  const bool active = j <= r.jhi && c <= r.chi && c0 <= pmax;
+  const bool active = col && c0 <= pmax;
   const bool last = c1 == pmax;  // this segment also walks the faces pmax+1, pmax+2
 #define IDX(p) j, (DIR == 2 ? (p) : c), (DIR == 2 ? c : (p))
   const int top = pmax + 2;
@@ -1089,6 +1101,18 @@ dim3 grid_mom_node(const Geom& g, int seg) {
               (r.phi - r.plo + 1 + seg - 1) / seg);
 }
 template <int DIR>
+dim3 grid_cell_sweep_flat(const Geom& g, int) {
+  const MarchRange r = cell_sweep_range<DIR>(g);
+  const long long n = (long long)(r.jhi - r.jlo + 1) * (r.chi - r.clo + 1);
+  return dim3((unsigned)((n + BX - 1) / BX), 1, 1);
+}
+template <int DIR>
+dim3 grid_mom_vel_flat(const Geom& g, int seg) {
+  const MarchRange r = mom_vel_range<DIR>(g);
+  const long long n = (long long)(r.jhi - r.jlo + 1) * (r.chi - r.clo + 1);
+  return dim3((unsigned)((n + BX * BY - 1) / (BX * BY)), 1, (r.phi - r.plo + 1 + seg - 1) / seg);
+}
+template <int DIR>
 dim3 grid_mom_vel(const Geom& g, int seg) {
   const MarchRange r = mom_vel_range<DIR>(g);
   return dim3((r.jhi - r.jlo + 1 + BX - 1) / BX, (r.chi - r.clo + 1 + BY - 1) / BY,
@@ -1165,11 +1189,13 @@ void launch_advec_cell_fused(const Target& tg, cudaStream_t s, int advect_x, int
     return;  // the x sweep is out of place: launch_advec_cell_x
   } else if (dir == 2) {
     // one marching pass, in place
-    launch_mapped(tg, s, kKeyCellSweep | 2u, grid_cell_sweep<2>, 0, false, kBlk,
+    launch_mapped2(tg, s, kKeyCellSweep | 2u, grid_cell_sweep<2>, grid_cell_sweep_flat<2>, 0,
+                   false, kBlk,
                   k_cell_sweep_march<S, 2, MapSingle>, k_cell_sweep_march<S, 2, MapBatch>,
                   variant, ga, density1, energy1, vol_flux_x, vol_flux_y, vol_flux_z, mass_flux_y);
   } else {
-    launch_mapped(tg, s, kKeyCellSweep | 3u, grid_cell_sweep<3>, 0, false, kBlk,
+    launch_mapped2(tg, s, kKeyCellSweep | 3u, grid_cell_sweep<3>, grid_cell_sweep_flat<3>, 0,
+                   false, kBlk,
                   k_cell_sweep_march<S, 3, MapSingle>, k_cell_sweep_march<S, 3, MapBatch>,
                   variant, ga, density1, energy1, vol_flux_x, vol_flux_y, vol_flux_z, mass_flux_z);
   }
@@ -1222,7 +1248,8 @@ void launch_advec_mom_fused(const Target& tg, cudaStream_t s, int advect_x, int 
                   k_mom_node_march<S, 2, MapSingle>, k_mom_node_march<S, 2, MapBatch>, variant,
                   ga, mass_flux_y, density1, vol_flux_x, vol_flux_y, vol_flux_z, node_flux,
                   node_mass_post, node_mass_pre);
-    launch_mapped(tg, s, kKeyMomVel3 | 2u, grid_mom_vel<2>, kMarchSeg, true, kBlk,
+    launch_mapped2(tg, s, kKeyMomVel3 | 2u, grid_mom_vel<2>, grid_mom_vel_flat<2>, kMarchSeg,
+                   true, kBlk,
                   k_mom_vel3_march<S, 2, MapSingle>, k_mom_vel3_march<S, 2, MapBatch>, ga,
                   node_flux, node_mass_post, node_mass_pre, vel_in[0], vel_in[1], vel_in[2],
                   vel_out[0], vel_out[1], vel_out[2]);
@@ -1231,7 +1258,8 @@ void launch_advec_mom_fused(const Target& tg, cudaStream_t s, int advect_x, int 
                   k_mom_node_march<S, 3, MapSingle>, k_mom_node_march<S, 3, MapBatch>, variant,
                   ga, mass_flux_z, density1, vol_flux_x, vol_flux_y, vol_flux_z, node_flux,
                   node_mass_post, node_mass_pre);
-    launch_mapped(tg, s, kKeyMomVel3 | 3u, grid_mom_vel<3>, kMarchSeg, true, kBlk,
+    launch_mapped2(tg, s, kKeyMomVel3 | 3u, grid_mom_vel<3>, grid_mom_vel_flat<3>, kMarchSeg,
+                   true, kBlk,
                   k_mom_vel3_march<S, 3, MapSingle>, k_mom_vel3_march<S, 3, MapBatch>, ga,
                   node_flux, node_mass_post, node_mass_pre, vel_in[0], vel_in[1], vel_in[2],
                   vel_out[0], vel_out[1], vel_out[2]);
