@@ -909,9 +909,10 @@ __global__ void k_halo(M m, HaloLaunch h, int depth, int do_low, int do_high) {
   const int tb = AX == 2 ? 1 : 2;  // second tangential axis
   const int mins[3] = {g.x_min, g.y_min, g.z_min};
   const int maxs[3] = {g.x_max, g.y_max, g.z_max};
-  const int a = mins[ta] - depth + t.x * blockDim.x + threadIdx.x;
-  const int bb = mins[tb] - depth + t.y * blockDim.y + threadIdx.y;
-  if (a > maxs[ta] + 1 + depth || bb > maxs[tb] + 1 + depth) return;
+  int a, bb;
+  if (!tile_jk<M>(Box{mins[ta] - depth, maxs[ta] + 1 + depth, mins[tb] - depth,
+                      maxs[tb] + 1 + depth, 0, 0}, t, a, bb))
+    return;
   const int n = maxs[AX];
   for (int fi = 0; fi < h.nfields; fi++) {
     const HaloRule r = h.rule[fi];
@@ -1000,6 +1001,13 @@ dim3 grid_halo_x(const Geom& g, int per_row) { return grid_halo_x_tasks(g, per_r
 
 // tile grid of the halo update of the faces normal to AX (32 x 8 tiles over
 // the two tangential axes, each extended by depth)
+template <int AX>
+dim3 grid_halo_flat(const Geom& g, int depth) {
+  const int mins[3] = {g.x_min, g.y_min, g.z_min}, maxs[3] = {g.x_max, g.y_max, g.z_max};
+  const int ta = AX == 0 ? 1 : 0, tb = AX == 2 ? 1 : 2;
+  return grid_flat(Box{mins[ta] - depth, maxs[ta] + 1 + depth, mins[tb] - depth,
+                       maxs[tb] + 1 + depth, 0, 0});
+}
 template <int AX>
 dim3 grid_halo(const Geom& g, int depth) {
   const int mins[3] = {g.x_min, g.y_min, g.z_min}, maxs[3] = {g.x_max, g.y_max, g.z_max};
@@ -1367,11 +1375,11 @@ void launch_update_halo(const Target& tg, cudaStream_t s, const HaloFields& f, c
                       k_halo_x<MapBatch>, h, depth, do_low, do_high);
     }
     else if (ax == 1)
-      launch_mapped(tg, s, key, grid_halo<1>, depth, false, blk, k_halo<1, MapSingle>,
-                    k_halo<1, MapBatch>, h, depth, do_low, do_high);
+      launch_mapped2(tg, s, key, grid_halo<1>, grid_halo_flat<1>, depth, false, blk,
+                     k_halo<1, MapSingle>, k_halo<1, MapBatch>, h, depth, do_low, do_high);
     else
-      launch_mapped(tg, s, key, grid_halo<2>, depth, false, blk, k_halo<2, MapSingle>,
-                    k_halo<2, MapBatch>, h, depth, do_low, do_high);
+      launch_mapped2(tg, s, key, grid_halo<2>, grid_halo_flat<2>, depth, false, blk,
+                     k_halo<2, MapSingle>, k_halo<2, MapBatch>, h, depth, do_low, do_high);
   }
 }
 
