@@ -187,7 +187,7 @@ __global__ void __launch_bounds__(BX * BY, 3) k_visc_dt(M m, GeomArrays ga, doub
   const A vgrady2 = v010 + v110 + v011 + v111;
   const A wgradz1 = w000 + w100 + w010 + w110;
   const A wgradz2 = w001 + w101 + w011 + w111;
-  const A xa = EGA(ga.xarea, j, k, l), ya = EGA(ga.yarea, j, k, l), za = EGA(ga.zarea, j, k, l);
+  const A xa = (A)g.xa, ya = (A)g.ya, za = (A)g.za;
   const A div = (xa * (ugradx2 - ugradx1) + ya * (vgrady2 - vgrady1)) +
                      za * (wgradz2 - wgradz1);
   A q = A(A(0.0));
@@ -245,7 +245,7 @@ __global__ void __launch_bounds__(BX * BY, 3) k_visc_dt(M m, GeomArrays ga, doub
   cc = cc + A(2.0) * visc / d0;
   A dtct = ds * cc;
   dtct = a_dtc * A(1.0) / fmax2(sqrt(dtct), a_gs);
-  const A vol = EGA(ga.volume, j, k, l);
+  const A vol = (A)g.vol;
   const A du1 = ugradx1 * xa, du2 = ugradx2 * xa;
   const A dtut = a_dtu * A(4.0) * vol / fmax2(fmax2(fabs(du1), fabs(du2)), A(1.0e-5) * vol);
   const A dv1 = vgrady1 * ya, dv2 = vgrady2 * ya;
@@ -314,28 +314,28 @@ __global__ void __launch_bounds__(BX * BY) k_pdv_predict_eos(M m, const double* 
   // the predictor sums the same four node values twice (vel0 + vel0)
   A s;
   s = XS(j);
-  const A left_flux = (EGA(ga.xarea, j, k, l) * (s + LA(xvel0, j, k, l) + LA(xvel0, j, k + 1, l) +
+  const A left_flux = ((A)g.xa * (s + LA(xvel0, j, k, l) + LA(xvel0, j, k + 1, l) +
                             LA(xvel0, j, k, l + 1) + LA(xvel0, j, k + 1, l + 1))) * A(0.125) * dt * A(0.5);
   s = XS(j + 1);
-  const A right_flux = (EGA(ga.xarea, j + 1, k, l) * (s + LA(xvel0, j + 1, k, l) + LA(xvel0, j + 1, k + 1, l) +
+  const A right_flux = ((A)g.xa * (s + LA(xvel0, j + 1, k, l) + LA(xvel0, j + 1, k + 1, l) +
                              LA(xvel0, j + 1, k, l + 1) + LA(xvel0, j + 1, k + 1, l + 1))) * A(0.125) * dt * A(0.5);
   s = YS(k);
-  const A bottom_flux = (EGA(ga.yarea, j, k, l) * (s + LA(yvel0, j, k, l) + LA(yvel0, j + 1, k, l) +
+  const A bottom_flux = ((A)g.ya * (s + LA(yvel0, j, k, l) + LA(yvel0, j + 1, k, l) +
                               LA(yvel0, j, k, l + 1) + LA(yvel0, j + 1, k, l + 1))) * A(0.125) * dt * A(0.5);
   s = YS(k + 1);
-  const A top_flux = (EGA(ga.yarea, j, k + 1, l) * (s + LA(yvel0, j, k + 1, l) + LA(yvel0, j + 1, k + 1, l) +
+  const A top_flux = ((A)g.ya * (s + LA(yvel0, j, k + 1, l) + LA(yvel0, j + 1, k + 1, l) +
                            LA(yvel0, j, k + 1, l + 1) + LA(yvel0, j + 1, k + 1, l + 1))) * A(0.125) * dt * A(0.5);
   s = ZS(l);
-  const A back_flux = (EGA(ga.zarea, j, k, l) * (s + LA(zvel0, j, k, l) + LA(zvel0, j + 1, k, l) +
+  const A back_flux = ((A)g.za * (s + LA(zvel0, j, k, l) + LA(zvel0, j + 1, k, l) +
                             LA(zvel0, j, k + 1, l) + LA(zvel0, j + 1, k + 1, l))) * A(0.125) * dt * A(0.5);
   s = ZS(l + 1);
-  const A front_flux = (EGA(ga.zarea, j, k, l + 1) * (s + LA(zvel0, j, k, l + 1) + LA(zvel0, j + 1, k, l + 1) +
+  const A front_flux = ((A)g.za * (s + LA(zvel0, j, k, l + 1) + LA(zvel0, j + 1, k, l + 1) +
                              LA(zvel0, j, k + 1, l + 1) + LA(zvel0, j + 1, k + 1, l + 1))) * A(0.125) * dt * A(0.5);
 #undef XS
 #undef YS
 #undef ZS
   const A total_flux = right_flux - left_flux + top_flux - bottom_flux + front_flux - back_flux;
-  const A vol = EGA(ga.volume, j, k, l);
+  const A vol = (A)g.vol;
   const A vol_change_s = vol / (vol + total_flux);
   const A recip_volume = A(1.0) / vol;
   const A d0 = LA(density0, j, k, l);
@@ -393,29 +393,29 @@ __global__ void __launch_bounds__(BX * BY, 5) k_pdv_flux(M m, const double* dt_p
   double sx = 0, sy = 0, sz = 0;
   if (kin && lin) {
     sx = xsum(j);
-    E(vol_flux_x, j, k, l) = st<F>(0.125 * dt * E(ga.xarea, j, k, l) * sx);
+    E(vol_flux_x, j, k, l) = st<F>(0.125 * dt * g.xa * sx);
   }
   if (jin && lin) {
     sy = ysum(k);
-    E(vol_flux_y, j, k, l) = st<F>(0.125 * dt * E(ga.yarea, j, k, l) * sy);
+    E(vol_flux_y, j, k, l) = st<F>(0.125 * dt * g.ya * sy);
   }
   if (jin && kin) {
     // flux_calc_kernel.f90:86 repeats zvel0(j+1,k,l) and omits zvel0(j,k+1,l)
     const double bz = L(zvel0, j, k, l) + L(zvel0, j + 1, k, l) + L(zvel0, j + 1, k, l) +
                       L(zvel0, j + 1, k + 1, l) + L(zvel1, j, k, l) + L(zvel1, j + 1, k, l) +
                       L(zvel1, j, k + 1, l) + L(zvel1, j + 1, k + 1, l);
-    E(vol_flux_z, j, k, l) = st<F>(0.125 * dt * E(ga.zarea, j, k, l) * bz);
+    E(vol_flux_z, j, k, l) = st<F>(0.125 * dt * g.za * bz);
     sz = zsum(l);
   }
   if (!(jin && kin && lin)) return;
-  const double left_flux = (E(ga.xarea, j, k, l) * sx) * 0.125 * dt;
-  const double right_flux = (E(ga.xarea, j + 1, k, l) * xsum(j + 1)) * 0.125 * dt;
-  const double bottom_flux = (E(ga.yarea, j, k, l) * sy) * 0.125 * dt;
-  const double top_flux = (E(ga.yarea, j, k + 1, l) * ysum(k + 1)) * 0.125 * dt;
-  const double back_flux = (E(ga.zarea, j, k, l) * sz) * 0.125 * dt;
-  const double front_flux = (E(ga.zarea, j, k, l + 1) * zsum(l + 1)) * 0.125 * dt;
+  const double left_flux = (g.xa * sx) * 0.125 * dt;
+  const double right_flux = (g.xa * xsum(j + 1)) * 0.125 * dt;
+  const double bottom_flux = (g.ya * sy) * 0.125 * dt;
+  const double top_flux = (g.ya * ysum(k + 1)) * 0.125 * dt;
+  const double back_flux = (g.za * sz) * 0.125 * dt;
+  const double front_flux = (g.za * zsum(l + 1)) * 0.125 * dt;
   const double total_flux = right_flux - left_flux + top_flux - bottom_flux + front_flux - back_flux;
-  const double vol = E(ga.volume, j, k, l);
+  const double vol = g.vol;
   const double vol_change_s = vol / (vol + total_flux);
   const double recip_volume = 1.0 / vol;
   const double d0 = L(density0, j, k, l);
@@ -433,7 +433,7 @@ template <class S>
 __device__ __forceinline__ double cell_pre_vol(const Geom& g, int variant, const GeomArrays& ga,
     const typename S::vf_t* vfx, const typename S::vf_t* vfy, const typename S::vf_t* vfz,
     int j, int k, int l) {
-  const double vol = E(ga.volume, j, k, l);
+  const double vol = g.vol;
   switch (variant) {
     case 0:
     case 4: {
@@ -569,7 +569,7 @@ template <class S>
 __device__ __forceinline__ double mom_post_vol(const Geom& g, int variant, const GeomArrays& ga,
     const typename S::vf_t* vfx, const typename S::vf_t* vfy, const typename S::vf_t* vfz,
     int j, int k, int l) {
-  const double vol = E(ga.volume, j, k, l);
+  const double vol = g.vol;
   switch (variant) {
     case 0:
       return vol + L(vfy, j, k + 1, l) - L(vfy, j, k, l) + L(vfz, j, k, l + 1) - L(vfz, j, k, l);
@@ -1229,6 +1229,12 @@ void launch_advec_mom_fused(const Target& tg, cudaStream_t s, int advect_x, int 
                             typename S::wk_t* node_flux, typename S::wk_t* node_mass_post,
                             typename S::wk_t* node_mass_pre, typename S::vel_t* const* vel_in,
                             typename S::vel_t* const* vel_out) {
+  // the node arrays of the y/z sweeps live in three work arrays, as nd_t
+  using ND = typename S::wk_t;
+  static_assert(sizeof(ND) <= sizeof(typename S::wk_t), "node arrays fit the work arrays");
+  ND* nd_flux = reinterpret_cast<ND*>(node_flux);
+  ND* nd_post = reinterpret_cast<ND*>(node_mass_post);
+  ND* nd_pre = reinterpret_cast<ND*>(node_mass_pre);
   int variant;
   if (sweep == 1 && dir == 1) variant = 0;
   else if (sweep == 1 && dir == 3) variant = 1;

@@ -358,8 +358,10 @@ __global__ void __launch_bounds__(BX * BY) k_revert(Geom g, Box b,
 }
 
 // ---------------------------------------------------------------------------
-// accelerate_kernel.f90:61-109
-template <class S, class M>
+// accelerate_kernel.f90:61-109. UM: the cell volume and face areas come from
+// the chunk's uniform-mesh constants (Geom::vol, xa, ya, za) instead of the
+// arrays.
+template <class S, class M, bool UM>
 __global__ void __launch_bounds__(BX * BY) k_accelerate(M m, double dt_val,
     const double* dt_ptr, GeomArrays ga, const typename S::rho_t* __restrict__ density0,
     const typename S::cs_t* __restrict__ pressure, const typename S::cs_t* __restrict__ viscosity,
@@ -369,7 +371,7 @@ __global__ void __launch_bounds__(BX * BY) k_accelerate(M m, double dt_val,
   m.run([&](const Geom& g, const Tile& t) {
   TILE_THREAD(nodes(g), t);
   const double dt = dt_ptr ? dt_ptr[(long long)t.d * kScalarStride] : dt_val;
-#define DV(a, bb, c) (L(density0, j + (a), k + (bb), l + (c)) * E(ga.volume, j + (a), k + (bb), l + (c)))
+#define DV(a, bb, c) (L(density0, j + (a), k + (bb), l + (c)) * (UM ? g.vol : E(ga.volume, j + (a), k + (bb), l + (c))))
   const double nodal_mass = (DV(-1, -1, 0) + DV(0, -1, 0) + DV(0, 0, 0) + DV(-1, 0, 0) +
                              DV(-1, -1, -1) + DV(0, -1, -1) + DV(0, 0, -1) + DV(-1, 0, -1)) * 0.125;
 #undef DV
@@ -388,12 +390,14 @@ __global__ void __launch_bounds__(BX * BY) k_accelerate(M m, double dt_val,
   const A q010 = LA(viscosity, j, k - 1, l), q110 = LA(viscosity, j - 1, k - 1, l);
   const A q001 = LA(viscosity, j, k, l - 1), q101 = LA(viscosity, j - 1, k, l - 1);
   const A q011 = LA(viscosity, j, k - 1, l - 1), q111 = LA(viscosity, j - 1, k - 1, l - 1);
-  const A xa0 = LA(ga.xarea, j, k, l), xa1 = LA(ga.xarea, j, k - 1, l);
-  const A xa2 = LA(ga.xarea, j, k, l - 1), xa3 = LA(ga.xarea, j, k - 1, l - 1);
-  const A ya0 = LA(ga.yarea, j, k, l), ya1 = LA(ga.yarea, j - 1, k, l);
-  const A ya2 = LA(ga.yarea, j, k, l - 1), ya3 = LA(ga.yarea, j - 1, k, l - 1);
-  const A za0 = LA(ga.zarea, j, k, l), za1 = LA(ga.zarea, j, k - 1, l);
-  const A za2 = LA(ga.zarea, j - 1, k, l), za3 = LA(ga.zarea, j - 1, k - 1, l);
+#define AR(a, c, jj, kk, ll) (UM ? (A)g.c : LA(ga.a, jj, kk, ll))
+  const A xa0 = AR(xarea, xa, j, k, l), xa1 = AR(xarea, xa, j, k - 1, l);
+  const A xa2 = AR(xarea, xa, j, k, l - 1), xa3 = AR(xarea, xa, j, k - 1, l - 1);
+  const A ya0 = AR(yarea, ya, j, k, l), ya1 = AR(yarea, ya, j - 1, k, l);
+  const A ya2 = AR(yarea, ya, j, k, l - 1), ya3 = AR(yarea, ya, j - 1, k, l - 1);
+  const A za0 = AR(zarea, za, j, k, l), za1 = AR(zarea, za, j, k - 1, l);
+  const A za2 = AR(zarea, za, j - 1, k, l), za3 = AR(zarea, za, j - 1, k - 1, l);
+#undef AR
 
   const A xvel1_s = LA(xvel0, j, k, l) -
       stepbymass_s * (xa0 * (p000 - p100) + xa1 * (p010 - p110) + xa2 * (p001 - p101) +
@@ -1174,10 +1178,17 @@ void launch_accelerate(const Target& tg, cudaStream_t s, double dt_val, const do
                        const typename S::cs_t* pressure, const typename S::cs_t* viscosity,
                        const typename S::vel_t* xvel0, const typename S::vel_t* yvel0,
                        const typename S::vel_t* zvel0, typename S::vel_t* xvel1,
-                       typename S::vel_t* yvel1, typename S::vel_t* zvel1) {
-  launch_mapped2(tg, s, kKeyAccelerate, grid_nodes, grid_nodes_flat, 0, false, dim3(BX, BY),
-                k_accelerate<S, MapSingle>, k_accelerate<S, MapBatch>, dt_val, dt_ptr, ga,
-                density0, pressure, viscosity, xvel0, yvel0, zvel0, xvel1, yvel1, zvel1);
+                       typename S::vel_t* yvel1, typename S::vel_t* zvel1, bool uniform_mesh) {
+  if (uniform_mesh)
+    launch_mapped2(tg, s, kKeyAccelerate, grid_nodes, grid_nodes_flat, 0, false, dim3(BX, BY),
+                   k_accelerate<S, MapSingle, true>, k_accelerate<S, MapBatch, true>, dt_val,
+                   dt_ptr, ga, density0, pressure, viscosity, xvel0, yvel0, zvel0, xvel1, yvel1,
+                   zvel1);
+  else
+    launch_mapped2(tg, s, kKeyAccelerate, grid_nodes, grid_nodes_flat, 0, false, dim3(BX, BY),
+                   k_accelerate<S, MapSingle, false>, k_accelerate<S, MapBatch, false>, dt_val,
+                   dt_ptr, ga, density0, pressure, viscosity, xvel0, yvel0, zvel0, xvel1, yvel1,
+                   zvel1);
 }
 
 template <class S>
@@ -1435,7 +1446,7 @@ void launch_fill(cudaStream_t s, T* p, long long elems, T value) {
   template void launch_accelerate<S>(const Target&, cudaStream_t, double, const double*,           \
                                      const GeomArrays&, const S::rho_t*, const S::cs_t*,       \
                                      const S::cs_t*, const S::vel_t*, const S::vel_t*,          \
-                                     const S::vel_t*, S::vel_t*, S::vel_t*, S::vel_t*);        \
+                                     const S::vel_t*, S::vel_t*, S::vel_t*, S::vel_t*, bool);  \
   template void launch_flux_calc<S>(const Geom&, cudaStream_t, double, const double*,            \
                                     const GeomArrays&, const S::vel_t*, const S::vel_t*,       \
                                     const S::vel_t*, const S::vel_t*, const S::vel_t*,          \

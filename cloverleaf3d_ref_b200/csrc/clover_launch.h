@@ -215,7 +215,8 @@ void launch_accelerate(const Target& tg, cudaStream_t s, double dt_val, const do
                        const typename S::cs_t* pressure, const typename S::cs_t* viscosity,
                        const typename S::vel_t* xvel0, const typename S::vel_t* yvel0,
                        const typename S::vel_t* zvel0, typename S::vel_t* xvel1,
-                       typename S::vel_t* yvel1, typename S::vel_t* zvel1);
+                       typename S::vel_t* yvel1, typename S::vel_t* zvel1,
+                       bool uniform_mesh = false);  // volume and areas from Geom::vol, xa, ya, za
 
 template <class S>
 void launch_flux_calc(const Geom& g, cudaStream_t s, double dt_val, const double* dt_ptr,

@@ -26,6 +26,13 @@ struct Geom {
   int o1;         // offset of this chunk in the shared 1D allocations
   long long pxy;  // plane pitch in elements
   long long o3;   // offset of this chunk in the shared 3D allocations
+  // Cell volume and face areas of the chunk's uniform mesh: every element of
+  // the volume, xarea, yarea and zarea arrays holds these values
+  // (initialise_chunk_kernel.f90:113-175: volume = dx*dy*dz, xarea =
+  // celldy*celldz = dy*dz, yarea = dx*dz, zarea = dx*dy). The native step
+  // kernels read them here instead of streaming four 3D arrays; the drop-in
+  // kernels, whose callers own the arrays, read the arrays.
+  double vol, xa, ya, za;
 };
 
 // Elements per 128 bytes for a storage type.
@@ -46,6 +53,7 @@ inline Geom make_geom(int x_min, int x_max, int y_min, int y_max, int z_min, int
   g.pxy = (long long)g.px * (y_max - y_min + 6);
   g.o1 = 0;
   g.o3 = 0;
+  g.vol = g.xa = g.ya = g.za = 0.0;
   return g;
 }
 

@@ -244,7 +244,16 @@ struct Chunk : ChunkBase {
     deck = decks[0];
     long long total3 = 0, total1 = 0;
     for (int d = 0; d < nd; d++) {
-      Geom q = make_geom(1, decks[d].x_cells, 1, decks[d].y_cells, 1, decks[d].z_cells);
+      const clover_deck& dk = decks[d];
+      Geom q = make_geom(1, dk.x_cells, 1, dk.y_cells, 1, dk.z_cells);
+      // initialise_chunk.f90:38-46 and initialise_chunk_kernel.f90:113-175
+      const double dx = (dk.xmax - dk.xmin) / (double)(float)dk.x_cells;
+      const double dy = (dk.ymax - dk.ymin) / (double)(float)dk.y_cells;
+      const double dz = (dk.zmax - dk.zmin) / (double)(float)dk.z_cells;
+      q.vol = dx * dy * dz;
+      q.xa = dy * dz;
+      q.ya = dx * dz;
+      q.za = dx * dy;
       q.o3 = total3;
       q.o1 = (int)total1;
       total3 += array_elems(q);
@@ -692,7 +701,7 @@ struct Chunk : ChunkBase {
     const double* dtp = &sc->dt;
     const double n = cells();
     const double R8 = sizeof(R), E8 = sizeof(En), C8 = sizeof(C), V8 = sizeof(V),
-                 VF8 = sizeof(VF), MF8 = sizeof(MF), W8 = sizeof(W), G8 = sizeof(double);
+                 VF8 = sizeof(VF), MF8 = sizeof(MF), W8 = sizeof(W);
     int vc = ax ? 0 : 1;  // buffer of the velocity pairs at the start of this step
     int cb = ax ? 0 : 1;  // buffer of the density1/energy1 pair at the start of this step
     // timestep.f90:56-126
@@ -708,7 +717,7 @@ struct Chunk : ChunkBase {
                       deck.dtw_safe, deck.dtdiv_safe, density0, pressure, viscosity, soundspeed,
                       xvel0, yvel0, zvel0, &sc->key);
     k_dt_finalize<<<deck_blocks(), 128, 0, stream>>>(sc, nd, dt_hist);
-    pend("viscosity_calc_dt", n * (3 * V8 + 4 * G8 + R8 + 3 * C8));
+    pend("viscosity_calc_dt", n * (3 * V8 + R8 + 3 * C8));
     pbeg();
     halo({6}, 1, vc, cb);  // read by accelerate at its neighbours
     pend("update_halo", 0);
@@ -716,19 +725,19 @@ struct Chunk : ChunkBase {
     pbeg();
     launch_pdv_predict_eos<S>(tg, stream, dtp, ga, density0, energy0, pressure, viscosity, xvel0,
                               yvel0, zvel0);
-    pend("pdv", n * (4 * G8 + R8 + E8 + 3 * C8 + 3 * V8));
+    pend("pdv", n * (R8 + E8 + 3 * C8 + 3 * V8));
     pbeg();
     halo({5}, 1, vc, cb);
     pend("update_halo", 0);
     pbeg();
     launch_accelerate<S>(tg, stream, 0.0, dtp, ga, density0, pressure, viscosity, xvel0, yvel0,
-                         zvel0, vel1(0, vc), vel1(1, vc), vel1(2, vc));
-    pend("accelerate", n * (4 * G8 + R8 + 2 * C8 + 6 * V8));
+                         zvel0, vel1(0, vc), vel1(1, vc), vel1(2, vc), true);
+    pend("accelerate", n * (R8 + 2 * C8 + 6 * V8));
     pbeg();
     launch_pdv_flux<S>(tg, stream, dtp, ga, density0, rho1(cb), energy0, ene1(cb), pressure,
                        viscosity, xvel0, vel1(0, vc), yvel0, vel1(1, vc), zvel0, vel1(2, vc),
                        vol_flux_x, vol_flux_y, vol_flux_z);
-    pend("pdv_flux", n * (4 * G8 + 2 * R8 + 2 * E8 + 2 * C8 + 6 * V8 + 3 * VF8));
+    pend("pdv_flux", n * (2 * R8 + 2 * E8 + 2 * C8 + 6 * V8 + 3 * VF8));
     // advection.f90:43-179
     const int axi = ax ? 1 : 0;
     auto sweep = [&](int sweep_number, int dir, bool pre_halo) {
@@ -746,13 +755,13 @@ struct Chunk : ChunkBase {
         launch_advec_cell_x<S>(tg, stream, sweep_number, ga, rho1(cb), ene1(cb), rho1(cb ^ 1),
                                ene1(cb ^ 1), vol_flux_x, vol_flux_y, vol_flux_z, mass_flux_x);
         cb ^= 1;
-        pend("advec_cell_x", n * (G8 + nvf * VF8 + 2 * R8 + 2 * E8 + MF8));
+        pend("advec_cell_x", n * (nvf * VF8 + 2 * R8 + 2 * E8 + MF8));
       } else {
         // one marching pass, in place
         launch_advec_cell_fused<S>(tg, stream, axi, dir, sweep_number, ga, rho1(cb), ene1(cb),
                                    mass_flux_x, vol_flux_x, mass_flux_y, vol_flux_y,
                                    mass_flux_z, vol_flux_z, work[6]);
-        pend("advec_cell_yz", n * (G8 + nvf * VF8 + 2 * R8 + 2 * E8 + MF8));
+        pend("advec_cell_yz", n * (nvf * VF8 + 2 * R8 + 2 * E8 + MF8));
       }
       pbeg();
       halo({2, 4, 9, 11, 13, 17, 18, 19}, 2, vc, cb);
@@ -767,9 +776,9 @@ struct Chunk : ChunkBase {
                                 work[0], work[1], work[2], vin, vout);
       // x: one pass; y, z: node pass + velocity pass
       if (dir == 1)
-        pend("advec_mom_x", n * (MF8 + R8 + G8 + npv * VF8 + 6 * V8));
+        pend("advec_mom_x", n * (MF8 + R8 + npv * VF8 + 6 * V8));
       else  // node pass + velocity pass
-        pend("advec_mom_yz", n * ((MF8 + R8 + G8 + npv * VF8 + 3 * W8) + (3 * W8 + 6 * V8)));
+        pend("advec_mom_yz", n * ((MF8 + R8 + npv * VF8 + 3 * W8) + (3 * W8 + 6 * V8)));
       vc ^= 1;
     };
     sweep(1, ax ? 1 : 3, true);

@@ -39,7 +39,12 @@ void format_e12_4(double v, char out[13]) {
   else
     snprintf(body, sizeof(body), "%s0.%s%c%03d", neg ? "-" : "", digits, e < 0 ? '-' : '+',
              e < 0 ? -e : e);
-  snprintf(out, 13, "%12s", body);
+  // right-align in 12 characters (the body is at most 11: "-0.dddd+eee")
+  size_t n = strlen(body);
+  if (n > 12) n = 12;
+  memset(out, ' ', 12);
+  memcpy(out + 12 - n, body, n);
+  out[12] = '\0';
 }
 
 namespace {
