@@ -521,13 +521,15 @@ __global__ void __launch_bounds__(BX * BY) k_cell_sweep_x(M m, int variant, Geom
     double diffdw = d_dn - d_don;
     double limiter = cell_limiter(sigmat, sigma3, sigma4, diffuw, diffdw);
     const double mflux = vf * (d_don + limiter);
-    mf_st = (double)st<MF>(mflux);
+    // the cell update takes the FP64 face fluxes; the stored mass flux
+    // (mf_t) feeds only the momentum sweep
+    mf_st = mflux;
     if (lane <= 29) E(mass_flux, c, k, l) = st<MF>(mflux);
     const double sigmam = fabs(mflux) / (d_don * pv_don);
     diffuw = e_don - e_up;
     diffdw = e_dn - e_don;
     limiter = cell_limiter(sigmam, sigma3, sigma4, diffuw, diffdw);
-    ef = (double)st<typename S::wk_t>(mflux * (e_don + limiter));
+    ef = mflux * (e_don + limiter);
   }
   // advec_cell_kernel.f90:173-185 for cell c from faces c and c+1
   const double mf_p = __shfl_down_sync(full, mf_st, 1);
@@ -626,8 +628,8 @@ template <class S, int DIR, class M>
 __global__ void __launch_bounds__(BX * BY, 4) k_mom_node_march(M m, int variant, GeomArrays ga,
     const typename S::mf_t* __restrict__ mf, const typename S::rho_t* __restrict__ density1,
     const typename S::vf_t* __restrict__ vfx, const typename S::vf_t* __restrict__ vfy,
-    const typename S::vf_t* __restrict__ vfz, typename S::wk_t* __restrict__ node_flux,
-    typename S::wk_t* __restrict__ node_mass_post, typename S::wk_t* __restrict__ node_mass_pre) {
+    const typename S::vf_t* __restrict__ vfz, typename S::nd_t* __restrict__ node_flux,
+    typename S::nd_t* __restrict__ node_mass_post, typename S::nd_t* __restrict__ node_mass_pre) {
   m.run([&](const Geom& g, const Tile& t) {
   const MarchRange r = mom_node_range<DIR>(g);
   const int plo = r.plo, phi = r.phi;
@@ -642,7 +644,7 @@ __global__ void __launch_bounds__(BX * BY, 4) k_mom_node_march(M m, int variant,
   int p1 = p0 + seg - 1;
   if (p1 > phi) p1 = phi;
   const unsigned full = 0xffffffffu;
-  using W = typename S::wk_t;
+  using W = typename S::nd_t;
   // (j,k,l) of the node at march index p, and the same with c-1
 #define IDX(p) j, (DIR == 2 ? (p) : c), (DIR == 2 ? c : (p))
 #define IDXM(p) j, (DIR == 2 ? (p) : c - 1), (DIR == 2 ? c - 1 : (p))
@@ -741,8 +743,8 @@ __device__ __forceinline__ A mom_flux_at(A nf, A nmpre_i, A nmpre_ip1, A vm1, A 
 // previous momentum fluxes and the velocity window in registers.
 template <class S, int DIR, class M>
 __global__ void __launch_bounds__(BX * BY, 3) k_mom_vel3_march(M m, GeomArrays ga,
-    const typename S::wk_t* __restrict__ node_flux, const typename S::wk_t* __restrict__ node_mass_post,
-    const typename S::wk_t* __restrict__ node_mass_pre, const typename S::vel_t* __restrict__ u_in,
+    const typename S::nd_t* __restrict__ node_flux, const typename S::nd_t* __restrict__ node_mass_post,
+    const typename S::nd_t* __restrict__ node_mass_pre, const typename S::vel_t* __restrict__ u_in,
     const typename S::vel_t* __restrict__ v_in, const typename S::vel_t* __restrict__ w_in,
     typename S::vel_t* __restrict__ u_out, typename S::vel_t* __restrict__ v_out,
     typename S::vel_t* __restrict__ w_out) {
@@ -930,12 +932,12 @@ __global__ void __launch_bounds__(BX * BY, 3) k_cell_sweep_march(M m, int varian
     double limiter = cell_limiter(sigmat, sigma3, sigma4, diffuw, diffdw);
     const double mflux = vf * (d_don + limiter);
     if (p <= c1 || last) EI(mass_flux, IDX(p)) = st<MF>(mflux);
-    const double mf_stored = (double)st<MF>(mflux);
+    const double mf_stored = mflux;  // FP64 in the cell update; mf_t storage feeds the momentum sweep
     const double sigmam = fabs(mflux) / (d_don * pv_don);
     diffuw = e_don - e_up;
     diffdw = e_dn - e_don;
     limiter = cell_limiter(sigmam, sigma3, sigma4, diffuw, diffdw);
-    const double eflux = (double)st<typename S::wk_t>(mflux * (e_don + limiter));
+    const double eflux = mflux * (e_don + limiter);
     // advec_cell_kernel.f90:270-281 (y) / :365-376 (z) for cell p-1
     if (update && p - 1 >= c0 && p - 1 <= c1) {
       const double pm = d1 * pv_m;
@@ -1230,7 +1232,7 @@ void launch_advec_mom_fused(const Target& tg, cudaStream_t s, int advect_x, int 
                             typename S::wk_t* node_mass_pre, typename S::vel_t* const* vel_in,
                             typename S::vel_t* const* vel_out) {
   // the node arrays of the y/z sweeps live in three work arrays, as nd_t
-  using ND = typename S::wk_t;
+  using ND = typename S::nd_t;
   static_assert(sizeof(ND) <= sizeof(typename S::wk_t), "node arrays fit the work arrays");
   ND* nd_flux = reinterpret_cast<ND*>(node_flux);
   ND* nd_post = reinterpret_cast<ND*>(node_mass_post);
@@ -1252,22 +1254,22 @@ void launch_advec_mom_fused(const Target& tg, cudaStream_t s, int advect_x, int 
     // node pass then velocity pass, each marching along y in segments
     launch_mapped(tg, s, kKeyMomNode | 2u, grid_mom_node<2>, kMarchSeg, true, kBlk,
                   k_mom_node_march<S, 2, MapSingle>, k_mom_node_march<S, 2, MapBatch>, variant,
-                  ga, mass_flux_y, density1, vol_flux_x, vol_flux_y, vol_flux_z, node_flux,
-                  node_mass_post, node_mass_pre);
+                  ga, mass_flux_y, density1, vol_flux_x, vol_flux_y, vol_flux_z, nd_flux,
+                  nd_post, nd_pre);
     launch_mapped2(tg, s, kKeyMomVel3 | 2u, grid_mom_vel<2>, grid_mom_vel_flat<2>, kMarchSeg,
                    true, kBlk,
                   k_mom_vel3_march<S, 2, MapSingle>, k_mom_vel3_march<S, 2, MapBatch>, ga,
-                  node_flux, node_mass_post, node_mass_pre, vel_in[0], vel_in[1], vel_in[2],
+                  nd_flux, nd_post, nd_pre, vel_in[0], vel_in[1], vel_in[2],
                   vel_out[0], vel_out[1], vel_out[2]);
   } else {
     launch_mapped(tg, s, kKeyMomNode | 3u, grid_mom_node<3>, kMarchSeg, true, kBlk,
                   k_mom_node_march<S, 3, MapSingle>, k_mom_node_march<S, 3, MapBatch>, variant,
-                  ga, mass_flux_z, density1, vol_flux_x, vol_flux_y, vol_flux_z, node_flux,
-                  node_mass_post, node_mass_pre);
+                  ga, mass_flux_z, density1, vol_flux_x, vol_flux_y, vol_flux_z, nd_flux,
+                  nd_post, nd_pre);
     launch_mapped2(tg, s, kKeyMomVel3 | 3u, grid_mom_vel<3>, grid_mom_vel_flat<3>, kMarchSeg,
                    true, kBlk,
                   k_mom_vel3_march<S, 3, MapSingle>, k_mom_vel3_march<S, 3, MapBatch>, ga,
-                  node_flux, node_mass_post, node_mass_pre, vel_in[0], vel_in[1], vel_in[2],
+                  nd_flux, nd_post, nd_pre, vel_in[0], vel_in[1], vel_in[2],
                   vel_out[0], vel_out[1], vel_out[2]);
   }
   // the updated buffers take the halo shell of the inputs

@@ -119,24 +119,32 @@ struct F64 {
   using vf_t = double;   // vol_flux_x/y/z
   using mf_t = double;   // mass_flux_x/y/z
   using wk_t = double;   // work arrays
+  using nd_t = double;   // node flux and node masses of the y/z momentum sweeps
   using arith_t = double;  // arithmetic of the stencils the mixed path runs in FP32
 };
 
 // Storage policy of the mixed-precision native path: FP32 storage for the
 // stencilled fields (energy, pressure, viscosity, sound speed, velocities),
-// FP64 kept where conservation needs it: density, mass fluxes, work arrays
-// (pre/post volumes, node masses) and the volume fluxes, whose differences
-// form the pre/post volumes and must cancel against the PdV volume change
-// for mass to be conserved. The momentum advection's flux limiter and
-// velocity update run in FP32 (arith_t); all other arithmetic is FP64.
+// FP64 kept where conservation needs it: density, the work arrays (pre/post
+// volumes) and the volume fluxes, whose differences form the pre/post volumes
+// and must cancel against the PdV volume change for mass to be conserved.
+// The cell sweeps update mass and energy from their FP64 face fluxes; the
+// mass flux is stored in FP32 (mf_t) for the momentum sweep, which forms its
+// node fluxes and node masses from it in FP64. The y/z momentum sweeps hand
+// those node values to the velocity pass, which reads them in the FP32
+// arithmetic: they are stored as FP32 (nd_t), the rounding the velocity pass
+// would apply. The momentum advection's flux limiter and velocity update,
+// accelerate's gradients and the EOS/viscosity/dt stencils run in FP32
+// (arith_t); all other arithmetic is FP64.
 struct F32Mixed {
   using rho_t = double;
   using ene_t = float;
   using cs_t = float;
   using vel_t = float;
   using vf_t = double;
-  using mf_t = double;
+  using mf_t = float;
   using wk_t = double;
+  using nd_t = float;
   using arith_t = float;  // momentum flux and update, accelerate (node and cell masses stay FP64)
 };
 

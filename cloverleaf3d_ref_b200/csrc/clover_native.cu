@@ -108,6 +108,7 @@ struct Chunk : ChunkBase {
   using VF = typename S::vf_t;
   using MF = typename S::mf_t;
   using W = typename S::wk_t;
+  using ND = typename S::nd_t;
 
   clover_deck deck;                // deck 0: summary cadence and end step of all decks
   Geom g;                          // deck 0's geometry (the whole chunk when nd == 1)
@@ -701,7 +702,7 @@ struct Chunk : ChunkBase {
     const double* dtp = &sc->dt;
     const double n = cells();
     const double R8 = sizeof(R), E8 = sizeof(En), C8 = sizeof(C), V8 = sizeof(V),
-                 VF8 = sizeof(VF), MF8 = sizeof(MF), W8 = sizeof(W);
+                 VF8 = sizeof(VF), MF8 = sizeof(MF), N8 = sizeof(ND);
     int vc = ax ? 0 : 1;  // buffer of the velocity pairs at the start of this step
     int cb = ax ? 0 : 1;  // buffer of the density1/energy1 pair at the start of this step
     // timestep.f90:56-126
@@ -778,7 +779,7 @@ struct Chunk : ChunkBase {
       if (dir == 1)
         pend("advec_mom_x", n * (MF8 + R8 + npv * VF8 + 6 * V8));
       else  // node pass + velocity pass
-        pend("advec_mom_yz", n * ((MF8 + R8 + npv * VF8 + 3 * W8) + (3 * W8 + 6 * V8)));
+        pend("advec_mom_yz", n * ((MF8 + R8 + npv * VF8 + 3 * N8) + (3 * N8 + 6 * V8)));
       vc ^= 1;
     };
     sweep(1, ax ? 1 : 3, true);

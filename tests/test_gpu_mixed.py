@@ -1,7 +1,10 @@
 """GPU: the FP32-storage mixed-precision path against the FP64 path.
 
-FP32 storage for energy, pressure, viscosity, sound speed, velocities and
-volume fluxes; FP64 for density, mass fluxes, work arrays and all arithmetic.
+FP32 storage for energy, pressure, viscosity, sound speed, velocities, mass
+fluxes and the momentum sweep's node values, FP32 arithmetic in the EOS,
+viscosity, dt, PdV predictor, accelerate and momentum stencils; FP64 for
+density, volume fluxes, pre/post volumes, the cell mass/energy update and the
+node masses.
 Bar: every field_summary quantity within 1e-5 relative of FP64 at every
 summary step; total mass equal to FP64's to 1e-8 relative, and on a deck
 where FP64 conserves mass, conserved to 1e-12 relative itself.
@@ -37,8 +40,9 @@ def test_mixed_summaries_within_1e5_of_fp64(fused):
     assert n32 == n64 and np.array_equal(st32, st64)
     rel = np.abs(s32 - s64) / np.maximum(np.abs(s64), 1e-300)
     assert rel.max() < SUMMARY_RTOL, rel.max(axis=0)
-    # Mass is carried in FP64 (density, mass fluxes), so the mixed run conserves
-    # it as well as FP64 does; on this 3D deck FP64 itself drifts ~1e-4 (the
+    # Mass is carried in FP64 (density, the cell sweeps' face fluxes), so the
+    # mixed run conserves it as well as FP64 does; on this 3D deck FP64 itself
+    # drifts ~1e-4 (the
     # reference's z volume flux in flux_calc is not the PdV one), and the
     # mixed run's drift follows FP64's to ~1e-9 relative.
     assert np.all(np.abs(s32[:, 1] / s64[:, 1] - 1) < 1e-8)
