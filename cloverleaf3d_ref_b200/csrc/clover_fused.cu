@@ -711,17 +711,32 @@ __global__ void __launch_bounds__(BX * BY, 4) k_mom_node_march(M m, int variant,
 }
 
 // Momentum flux at node i (advec_mom_kernel.f90:211-242 and the y/z forms)
-// from the velocity window v(i-1..i+2).
+// from the velocity window v(i-1..i+2). The donor side, the Courant number
+// sigma and the limiter's cell widths depend on the node only, so they are
+// formed once per node (MomNodeTerms) for the three velocity components.
 template <class A>
-__device__ __forceinline__ A mom_flux_at(A nf, A nmpre_i, A nmpre_ip1, A vm1, A v0, A vp1, A vp2,
-                                         A width, A cd_m1, A cd_p1) {
-  A v_upwind, v_donor, v_downwind, nm_donor, cd_dif;
-  if (nf < A(0.0)) {
-    v_upwind = vp2; v_donor = vp1; v_downwind = v0; nm_donor = nmpre_ip1; cd_dif = cd_p1;
-  } else {
-    v_upwind = vm1; v_donor = v0; v_downwind = vp1; nm_donor = nmpre_i; cd_dif = cd_m1;
-  }
-  const A sigma = fabs(nf) / nm_donor;
+struct MomNodeTerms {
+  bool neg;  // node flux < 0: the donor is node i+1
+  A nf, sigma, width, cd_dif;
+};
+
+template <class A>
+__device__ __forceinline__ MomNodeTerms<A> mom_node_terms(A nf, A nmpre_i, A nmpre_ip1, A width,
+                                                          A cd_m1, A cd_p1) {
+  MomNodeTerms<A> t;
+  t.neg = nf < A(0.0);
+  t.nf = nf;
+  t.sigma = fabs(nf) / (t.neg ? nmpre_ip1 : nmpre_i);
+  t.width = width;
+  t.cd_dif = t.neg ? cd_p1 : cd_m1;
+  return t;
+}
+
+template <class A>
+__device__ __forceinline__ A mom_flux_v(const MomNodeTerms<A>& t, A vm1, A v0, A vp1, A vp2) {
+  const A v_upwind = t.neg ? vp2 : vm1;
+  const A v_donor = t.neg ? vp1 : v0;
+  const A v_downwind = t.neg ? v0 : vp1;
   const A vdiffuw = v_donor - v_upwind;
   const A vdiffdw = v_downwind - v_donor;
   A limiter = A(0.0);
@@ -730,13 +745,21 @@ __device__ __forceinline__ A mom_flux_at(A nf, A nmpre_i, A nmpre_ip1, A vm1, A 
     const A adw = fabs(vdiffdw);
     A wind = A(1.0);
     if (vdiffdw <= A(0.0)) wind = A(-1.0);
+    const A width = t.width, sigma = t.sigma;
     limiter = wind * fmin2(fmin2(width * ((A(2.0) - sigma) * adw / width +
-                                          (A(1.0) + sigma) * auw / cd_dif) / A(6.0),
+                                          (A(1.0) + sigma) * auw / t.cd_dif) / A(6.0),
                                  auw),
                            adw);
   }
-  const A advec_vel_s = v_donor + (A(1.0) - sigma) * limiter;
-  return advec_vel_s * nf;
+  const A advec_vel_s = v_donor + (A(1.0) - t.sigma) * limiter;
+  return advec_vel_s * t.nf;
+}
+
+template <class A>
+__device__ __forceinline__ A mom_flux_at(A nf, A nmpre_i, A nmpre_ip1, A vm1, A v0, A vp1, A vp2,
+                                         A width, A cd_m1, A cd_p1) {
+  return mom_flux_v<A>(mom_node_terms<A>(nf, nmpre_i, nmpre_ip1, width, cd_m1, cd_p1), vm1, v0,
+                       vp1, vp2);
 }
 
 // Velocity pass for direction y or z, marching along the sweep axis with the
@@ -772,15 +795,18 @@ __global__ void __launch_bounds__(BX * BY, 3) k_mom_vel3_march(M m, GeomArrays g
   A nf_m = LA(node_flux, IDX(p0 - 1));
   A pre_m = LA(node_mass_pre, IDX(p0 - 1));
   A pre_0 = LA(node_mass_pre, IDX(p0));
-#pragma unroll
-  for (int q = 0; q < 3; q++) {
-    vw[q][0] = LA(in[q], IDX(p0 - 2));
-    vw[q][1] = LA(in[q], IDX(p0 - 1));
-    vw[q][2] = LA(in[q], IDX(p0));
-    vw[q][3] = LA(in[q], IDX(p0 + 1));
+  {
     // mom_flux(p0-1)
-    mf_prev[q] = mom_flux_at<A>(nf_m, pre_m, pre_0, vw[q][0], vw[q][1], vw[q][2], vw[q][3],
-                                (A)CD(p0 - 1), (A)CD(p0 - 2), (A)CD(p0));
+    const MomNodeTerms<A> nt =
+        mom_node_terms<A>(nf_m, pre_m, pre_0, (A)CD(p0 - 1), (A)CD(p0 - 2), (A)CD(p0));
+#pragma unroll
+    for (int q = 0; q < 3; q++) {
+      vw[q][0] = LA(in[q], IDX(p0 - 2));
+      vw[q][1] = LA(in[q], IDX(p0 - 1));
+      vw[q][2] = LA(in[q], IDX(p0));
+      vw[q][3] = LA(in[q], IDX(p0 + 1));
+      mf_prev[q] = mom_flux_v<A>(nt, vw[q][0], vw[q][1], vw[q][2], vw[q][3]);
+    }
   }
   // loads of node p are issued one node ahead of their use
   A nf_0 = LA(node_flux, IDX(p0));
@@ -799,12 +825,12 @@ __global__ void __launch_bounds__(BX * BY, 3) k_mom_vel3_march(M m, GeomArrays g
 #pragma unroll
       for (int q = 0; q < 3; q++) vn_n[q] = LA(in[q], IDX(p + 3));
     }
-    const A w_0 = (A)CD(p), cd_m1 = (A)CD(p - 1), cd_p1 = (A)CD(p + 1);
+    const MomNodeTerms<A> nt =
+        mom_node_terms<A>(nf_0, pre_0, pre_p, (A)CD(p), (A)CD(p - 1), (A)CD(p + 1));
 #pragma unroll
     for (int q = 0; q < 3; q++) {
       const A vp2 = vn[q];
-      const A mf_0 = mom_flux_at<A>(nf_0, pre_0, pre_p, vw[q][1], vw[q][2], vw[q][3], vp2, w_0,
-                                    cd_m1, cd_p1);
+      const A mf_0 = mom_flux_v<A>(nt, vw[q][1], vw[q][2], vw[q][3], vp2);
       EI(out[q], IDX(p)) = st<V>((vw[q][2] * pre_0 + mf_prev[q] - mf_0) / post_0);
       mf_prev[q] = mf_0;
       vw[q][0] = vw[q][1];
@@ -1023,6 +1049,8 @@ __global__ void __launch_bounds__(BX * BY, 3) k_mom_sweep_x(M m, int variant,
     const double nmpre_p = __shfl_down_sync(0xffffffffu, nmpre, 1);
     // flux and update in the momentum arithmetic A (node masses are FP64)
     using A = typename S::arith_t;
+    const MomNodeTerms<A> nt =
+        mom_node_terms<A>((A)nf, (A)nmpre, (A)nmpre_p, (A)cd_0, (A)cd_m1, (A)cd_p1);
 #pragma unroll
     for (int q = 0; q < 3; q++) {
       A mf = A(0.0), v0 = A(0.0);
@@ -1030,8 +1058,7 @@ __global__ void __launch_bounds__(BX * BY, 3) k_mom_sweep_x(M m, int variant,
         const A vm1 = lda<A>(&E(in[q], j - 1, k, l));
         v0 = lda<A>(&E(in[q], j, k, l));
         const A vp1 = lda<A>(&E(in[q], j + 1, k, l)), vp2 = lda<A>(&E(in[q], j + 2, k, l));
-        mf = mom_flux_at<A>((A)nf, (A)nmpre, (A)nmpre_p, vm1, v0, vp1, vp2, (A)cd_0, (A)cd_m1,
-                            (A)cd_p1);
+        mf = mom_flux_v<A>(nt, vm1, v0, vp1, vp2);
       }
       const A mf_m = __shfl_up_sync(0xffffffffu, mf, 1);
       if (has_up) E(out[q], j, k, l) = st<V>((v0 * (A)nmpre + mf_m - mf) / (A)nmp);
@@ -1256,21 +1283,19 @@ void launch_advec_mom_fused(const Target& tg, cudaStream_t s, int advect_x, int 
                   k_mom_node_march<S, 2, MapSingle>, k_mom_node_march<S, 2, MapBatch>, variant,
                   ga, mass_flux_y, density1, vol_flux_x, vol_flux_y, vol_flux_z, nd_flux,
                   nd_post, nd_pre);
-    launch_mapped2(tg, s, kKeyMomVel3 | 2u, grid_mom_vel<2>, grid_mom_vel_flat<2>, kMarchSeg,
-                   true, kBlk,
-                  k_mom_vel3_march<S, 2, MapSingle>, k_mom_vel3_march<S, 2, MapBatch>, ga,
-                  nd_flux, nd_post, nd_pre, vel_in[0], vel_in[1], vel_in[2],
-                  vel_out[0], vel_out[1], vel_out[2]);
+    launch_mapped2(tg, s, kKeyMomVel3 | 2u, grid_mom_vel<2>, grid_mom_vel_flat<2>,
+                   kMarchSeg, true, kBlk, k_mom_vel3_march<S, 2, MapSingle>,
+                   k_mom_vel3_march<S, 2, MapBatch>, ga, nd_flux, nd_post, nd_pre, vel_in[0],
+                   vel_in[1], vel_in[2], vel_out[0], vel_out[1], vel_out[2]);
   } else {
     launch_mapped(tg, s, kKeyMomNode | 3u, grid_mom_node<3>, kMarchSeg, true, kBlk,
                   k_mom_node_march<S, 3, MapSingle>, k_mom_node_march<S, 3, MapBatch>, variant,
                   ga, mass_flux_z, density1, vol_flux_x, vol_flux_y, vol_flux_z, nd_flux,
                   nd_post, nd_pre);
-    launch_mapped2(tg, s, kKeyMomVel3 | 3u, grid_mom_vel<3>, grid_mom_vel_flat<3>, kMarchSeg,
-                   true, kBlk,
-                  k_mom_vel3_march<S, 3, MapSingle>, k_mom_vel3_march<S, 3, MapBatch>, ga,
-                  nd_flux, nd_post, nd_pre, vel_in[0], vel_in[1], vel_in[2],
-                  vel_out[0], vel_out[1], vel_out[2]);
+    launch_mapped2(tg, s, kKeyMomVel3 | 3u, grid_mom_vel<3>, grid_mom_vel_flat<3>,
+                   kMarchSeg, true, kBlk, k_mom_vel3_march<S, 3, MapSingle>,
+                   k_mom_vel3_march<S, 3, MapBatch>, ga, nd_flux, nd_post, nd_pre, vel_in[0],
+                   vel_in[1], vel_in[2], vel_out[0], vel_out[1], vel_out[2]);
   }
   // the updated buffers take the halo shell of the inputs
   using V = typename S::vel_t;
