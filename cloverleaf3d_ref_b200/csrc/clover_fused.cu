@@ -29,6 +29,8 @@
 //                    velocity pass, each marching along the sweep axis with the
 //                    previous node's values in registers.
 //  Updated velocities go to the other buffer of each velocity pair.
+#include <type_traits>
+
 #include "clover_launch.h"
 
 namespace clover {
@@ -470,8 +472,8 @@ __device__ __forceinline__ double cell_limiter(double sig, double sigma3, double
 // face c fluxes and lanes 2..29 own cell c (28 per warp): they store the
 // fluxes of face c and update cell c from faces c and c+1 into the output
 // arrays, so no thread reads a value another one writes.
-template <class S, class M>
-__global__ void __launch_bounds__(BX * BY) k_cell_sweep_x(M m, int variant, GeomArrays ga,
+template <class S, int VAR, class M>
+__global__ void __launch_bounds__(BX * BY) k_cell_sweep_x(M m, GeomArrays ga,
     const typename S::rho_t* __restrict__ d_in, const typename S::ene_t* __restrict__ e_in,
     typename S::rho_t* __restrict__ d_out, typename S::ene_t* __restrict__ e_out,
     const typename S::vf_t* __restrict__ vfx, const typename S::vf_t* __restrict__ vfy,
@@ -489,7 +491,7 @@ __global__ void __launch_bounds__(BX * BY) k_cell_sweep_x(M m, int variant, Geom
   if (lds) {
     d = L(d_in, c, k, l);
     e = L(e_in, c, k, l);
-    pv = cell_pre_vol<S>(g, variant, ga, vfx, vfy, vfz, c, k, l);
+    pv = cell_pre_vol<S>(g, VAR, ga, vfx, vfy, vfz, c, k, l);
     vf = L(vfx, c, k, l);
     vd = GX(ga.vertexdx, c);
   }
@@ -624,8 +626,8 @@ __device__ __forceinline__ double cell_product(const Geom& g, int variant, const
 // L-1, so lane 0 only serves lane 1 and lanes 1..31 store nodes.
 // DIR 2: p = k, c = l; DIR 3: p = l, c = k. Sums keep the reference order
 // (advec_mom_kernel.f90:166-190 and the y/z forms).
-template <class S, int DIR, class M>
-__global__ void __launch_bounds__(BX * BY, 4) k_mom_node_march(M m, int variant, GeomArrays ga,
+template <class S, int DIR, int VAR, class M>
+__global__ void __launch_bounds__(BX * BY, 4) k_mom_node_march(M m, GeomArrays ga,
     const typename S::mf_t* __restrict__ mf, const typename S::rho_t* __restrict__ density1,
     const typename S::vf_t* __restrict__ vfx, const typename S::vf_t* __restrict__ vfy,
     const typename S::vf_t* __restrict__ vfz, typename S::nd_t* __restrict__ node_flux,
@@ -649,7 +651,7 @@ __global__ void __launch_bounds__(BX * BY, 4) k_mom_node_march(M m, int variant,
 #define IDX(p) j, (DIR == 2 ? (p) : c), (DIR == 2 ? c : (p))
 #define IDXM(p) j, (DIR == 2 ? (p) : c - 1), (DIR == 2 ? c - 1 : (p))
   auto P = [&](int jj, int kk, int ll) {
-    return cell_product<S>(g, variant, ga, density1, vfx, vfy, vfz, jj, kk, ll);
+    return cell_product<S>(g, VAR, ga, density1, vfx, vfy, vfz, jj, kk, ll);
   };
   auto up = [&](double v) { return __shfl_up_sync(full, v, 1); };
   // mass fluxes of plane p at (j, c) and (j, c-1); the node flux of node p
@@ -808,23 +810,13 @@ __global__ void __launch_bounds__(BX * BY, 3) k_mom_vel3_march(M m, GeomArrays g
       mf_prev[q] = mom_flux_v<A>(nt, vw[q][0], vw[q][1], vw[q][2], vw[q][3]);
     }
   }
-  // loads of node p are issued one node ahead of their use
-  A nf_0 = LA(node_flux, IDX(p0));
-  A pre_p = LA(node_mass_pre, IDX(p0 + 1));
-  A post_0 = LA(node_mass_post, IDX(p0));
-  A vn[3];
-#pragma unroll
-  for (int q = 0; q < 3; q++) vn[q] = LA(in[q], IDX(p0 + 2));
   for (int p = p0; p <= p1; p++) {
-    const bool more = p < p1;
-    A nf_n = A(0.0), pre_n = A(0.0), post_n = A(0.0), vn_n[3] = {A(0.0), A(0.0), A(0.0)};
-    if (more) {
-      nf_n = LA(node_flux, IDX(p + 1));
-      pre_n = LA(node_mass_pre, IDX(p + 2));
-      post_n = LA(node_mass_post, IDX(p + 1));
+    const A nf_0 = LA(node_flux, IDX(p));
+    const A pre_p = LA(node_mass_pre, IDX(p + 1));
+    const A post_0 = LA(node_mass_post, IDX(p));
+    A vn[3];
 #pragma unroll
-      for (int q = 0; q < 3; q++) vn_n[q] = LA(in[q], IDX(p + 3));
-    }
+    for (int q = 0; q < 3; q++) vn[q] = LA(in[q], IDX(p + 2));
     const MomNodeTerms<A> nt =
         mom_node_terms<A>(nf_0, pre_0, pre_p, (A)CD(p), (A)CD(p - 1), (A)CD(p + 1));
 #pragma unroll
@@ -837,12 +829,8 @@ __global__ void __launch_bounds__(BX * BY, 3) k_mom_vel3_march(M m, GeomArrays g
       vw[q][1] = vw[q][2];
       vw[q][2] = vw[q][3];
       vw[q][3] = vp2;
-      vn[q] = vn_n[q];
     }
     pre_0 = pre_p;
-    nf_0 = nf_n;
-    pre_p = pre_n;
-    post_0 = post_n;
   }
 #undef LA
 #undef CD
@@ -863,8 +851,8 @@ __global__ void __launch_bounds__(BX * BY, 3) k_mom_vel3_march(M m, GeomArrays g
 // then does any thread write. Faces p in [pmin, pmax+2] (c up to chi), cells p
 // in [pmin, pmax] (c <= cmax); face c1+1 is computed by both neighbours and
 // stored by the segment that starts there.
-template <class S, int DIR, class M>
-__global__ void __launch_bounds__(BX * BY, 3) k_cell_sweep_march(M m, int variant, GeomArrays ga,
+template <class S, int DIR, int VAR, class M>
+__global__ void __launch_bounds__(BX * BY, 3) k_cell_sweep_march(M m, GeomArrays ga,
     typename S::rho_t* __restrict__ density1, typename S::ene_t* __restrict__ energy1,
     const typename S::vf_t* __restrict__ vfx, const typename S::vf_t* __restrict__ vfy,
     const typename S::vf_t* __restrict__ vfz, typename S::mf_t* __restrict__ mass_flux) {
@@ -918,7 +906,7 @@ __global__ void __launch_bounds__(BX * BY, 3) k_cell_sweep_march(M m, int varian
   using En = typename S::ene_t;
   using MF = typename S::mf_t;
   auto prevol = [&](int p) {
-    return cell_pre_vol<S>(g, variant, ga, vfx, vfy, vfz, IDX(p));
+    return cell_pre_vol<S>(g, VAR, ga, vfx, vfy, vfz, IDX(p));
   };
   // window: d0..d3 = density1(p-2..p+1), e0..e3 = energy1(p-2..p+1), old values
   double d2 = LI(density1, IDX(c0)), d3;
@@ -994,8 +982,8 @@ __global__ void __launch_bounds__(BX * BY, 3) k_cell_sweep_march(M m, int varian
 // lanes 1..30 momentum fluxes, lanes 2..30 update (29 nodes per warp). Sums
 // and the momentum limiter keep the reference order
 // (advec_mom_kernel.f90:166-252).
-template <class S, class M>
-__global__ void __launch_bounds__(BX * BY, 3) k_mom_sweep_x(M m, int variant,
+template <class S, int VAR, class M>
+__global__ void __launch_bounds__(BX * BY, 3) k_mom_sweep_x(M m,
     GeomArrays ga, const typename S::mf_t* __restrict__ mfx,
     const typename S::rho_t* __restrict__ density1, const typename S::vf_t* __restrict__ vfx,
     const typename S::vf_t* __restrict__ vfy, const typename S::vf_t* __restrict__ vfz,
@@ -1015,7 +1003,7 @@ __global__ void __launch_bounds__(BX * BY, 3) k_mom_sweep_x(M m, int variant,
   const bool has_mf = row && lane >= 1 && lane <= 30 && j >= g.x_min - 1 && j <= g.x_max + 1;
   const bool has_up = row && lane >= 2 && lane <= 30 && j >= g.x_min && j <= g.x_max + 1;
   auto P = [&](int kk, int ll) {
-    return cell_product<S>(g, variant, ga, density1, vfx, vfy, vfz, j, kk, ll);
+    return cell_product<S>(g, VAR, ga, density1, vfx, vfy, vfz, j, kk, ll);
   };
   using V = typename S::vel_t;
   const typename S::vel_t* in[3] = {u_in, v_in, w_in};
@@ -1209,24 +1197,31 @@ void launch_advec_cell_fused(const Target& tg, cudaStream_t s, int advect_x, int
                              const typename S::vf_t* vol_flux_x, typename S::mf_t* mass_flux_y,
                              const typename S::vf_t* vol_flux_y, typename S::mf_t* mass_flux_z,
                              const typename S::vf_t* vol_flux_z, typename S::wk_t* ener_flux) {
-  int variant = 0;
-  if (dir == 1) variant = sweep == 1 ? 0 : 1;
-  else if (dir == 2) variant = advect_x ? 2 : 3;
-  else variant = sweep == 1 ? 4 : 5;
   (void)ener_flux;
-  if (dir == 1) {
-    return;  // the x sweep is out of place: launch_advec_cell_x
-  } else if (dir == 2) {
-    // one marching pass, in place
-    launch_mapped2(tg, s, kKeyCellSweep | 2u, grid_cell_sweep<2>, grid_cell_sweep_flat<2>, 0,
-                   false, kBlk,
-                  k_cell_sweep_march<S, 2, MapSingle>, k_cell_sweep_march<S, 2, MapBatch>,
-                  variant, ga, density1, energy1, vol_flux_x, vol_flux_y, vol_flux_z, mass_flux_y);
+  // pre_vol variant (the sweep's volume-flux terms) as a kernel template
+  // argument: y is sweep 2 (2: after x, 3: after z); z is sweep 1 (4) or 3 (5)
+  if (dir == 1) return;  // the x sweep is out of place: launch_advec_cell_x
+  auto sweep_y = [&](auto var) {
+    constexpr int V = decltype(var)::value;
+    launch_mapped2(tg, s, kKeyCellSweep | 2u | (V << 4), grid_cell_sweep<2>,
+                   grid_cell_sweep_flat<2>, 0, false, kBlk,
+                   k_cell_sweep_march<S, 2, V, MapSingle>, k_cell_sweep_march<S, 2, V, MapBatch>,
+                   ga, density1, energy1, vol_flux_x, vol_flux_y, vol_flux_z, mass_flux_y);
+  };
+  auto sweep_z = [&](auto var) {
+    constexpr int V = decltype(var)::value;
+    launch_mapped2(tg, s, kKeyCellSweep | 3u | (V << 4), grid_cell_sweep<3>,
+                   grid_cell_sweep_flat<3>, 0, false, kBlk,
+                   k_cell_sweep_march<S, 3, V, MapSingle>, k_cell_sweep_march<S, 3, V, MapBatch>,
+                   ga, density1, energy1, vol_flux_x, vol_flux_y, vol_flux_z, mass_flux_z);
+  };
+  // one marching pass, in place
+  if (dir == 2) {
+    if (advect_x) sweep_y(std::integral_constant<int, 2>{});
+    else sweep_y(std::integral_constant<int, 3>{});
   } else {
-    launch_mapped2(tg, s, kKeyCellSweep | 3u, grid_cell_sweep<3>, grid_cell_sweep_flat<3>, 0,
-                   false, kBlk,
-                  k_cell_sweep_march<S, 3, MapSingle>, k_cell_sweep_march<S, 3, MapBatch>,
-                  variant, ga, density1, energy1, vol_flux_x, vol_flux_y, vol_flux_z, mass_flux_z);
+    if (sweep == 1) sweep_z(std::integral_constant<int, 4>{});
+    else sweep_z(std::integral_constant<int, 5>{});
   }
 }
 
@@ -1236,11 +1231,17 @@ void launch_advec_cell_x(const Target& tg, cudaStream_t s, int sweep, const Geom
                          typename S::rho_t* density1_out, typename S::ene_t* energy1_out,
                          const typename S::vf_t* vol_flux_x, const typename S::vf_t* vol_flux_y,
                          const typename S::vf_t* vol_flux_z, typename S::mf_t* mass_flux_x) {
-  const int variant = sweep == 1 ? 0 : 1;
-  launch_mapped(tg, s, kKeyCellSweepX, grid_cell_sweep_x, 0, false, kBlk,
-                k_cell_sweep_x<S, MapSingle>, k_cell_sweep_x<S, MapBatch>, variant, ga,
-                density1_in, energy1_in, density1_out, energy1_out, vol_flux_x, vol_flux_y,
-                vol_flux_z, mass_flux_x);
+  // pre_vol variant: 0 on sweep 1 (all three flux differences), 1 on sweep 3
+  if (sweep == 1)
+    launch_mapped(tg, s, kKeyCellSweepX, grid_cell_sweep_x, 0, false, kBlk,
+                  k_cell_sweep_x<S, 0, MapSingle>, k_cell_sweep_x<S, 0, MapBatch>, ga,
+                  density1_in, energy1_in, density1_out, energy1_out, vol_flux_x, vol_flux_y,
+                  vol_flux_z, mass_flux_x);
+  else
+    launch_mapped(tg, s, kKeyCellSweepX | (1u << 4), grid_cell_sweep_x, 0, false, kBlk,
+                  k_cell_sweep_x<S, 1, MapSingle>, k_cell_sweep_x<S, 1, MapBatch>, ga,
+                  density1_in, energy1_in, density1_out, energy1_out, vol_flux_x, vol_flux_y,
+                  vol_flux_z, mass_flux_x);
   // the cells the sweep does not update keep their values in the output pair
   using R = typename S::rho_t;
   using En = typename S::ene_t;
@@ -1264,38 +1265,40 @@ void launch_advec_mom_fused(const Target& tg, cudaStream_t s, int advect_x, int 
   ND* nd_flux = reinterpret_cast<ND*>(node_flux);
   ND* nd_post = reinterpret_cast<ND*>(node_mass_post);
   ND* nd_pre = reinterpret_cast<ND*>(node_mass_pre);
-  int variant;
-  if (sweep == 1 && dir == 1) variant = 0;
-  else if (sweep == 1 && dir == 3) variant = 1;
-  else if (sweep == 2 && advect_x) variant = 2;
-  else if (sweep == 2) variant = 3;
-  else variant = 4;  // sweep 3: post_vol = volume
   (void)vol;
+  // post_vol variant (mom_post_vol) as a kernel template argument: x is sweep
+  // 1 (0) or 3 (4); y is sweep 2 (2: after x, 3: after z); z is sweep 1 (1) or 3 (4)
+  auto node_vel = [&](auto dir_c, auto var) {
+    constexpr int D = decltype(dir_c)::value, V = decltype(var)::value;
+    // node pass then velocity pass, each marching along the sweep axis in segments
+    launch_mapped(tg, s, kKeyMomNode | D | (V << 4), grid_mom_node<D>, kMarchSeg, true, kBlk,
+                  k_mom_node_march<S, D, V, MapSingle>, k_mom_node_march<S, D, V, MapBatch>, ga,
+                  D == 2 ? mass_flux_y : mass_flux_z, density1, vol_flux_x, vol_flux_y,
+                  vol_flux_z, nd_flux, nd_post, nd_pre);
+    launch_mapped2(tg, s, kKeyMomVel3 | D, grid_mom_vel<D>, grid_mom_vel_flat<D>, kMarchSeg,
+                   true, kBlk, k_mom_vel3_march<S, D, MapSingle>, k_mom_vel3_march<S, D, MapBatch>,
+                   ga, nd_flux, nd_post, nd_pre, vel_in[0], vel_in[1], vel_in[2], vel_out[0],
+                   vel_out[1], vel_out[2]);
+  };
+  using I2 = std::integral_constant<int, 2>;
+  using I3 = std::integral_constant<int, 3>;
   if (dir == 1) {
     // one pass for the three velocities
-    launch_mapped(tg, s, kKeyMomSweepX, grid_mom_sweep_x, kMarchSeg, true, kBlk,
-                  k_mom_sweep_x<S, MapSingle>, k_mom_sweep_x<S, MapBatch>, variant, ga,
-                  mass_flux_x, density1, vol_flux_x, vol_flux_y, vol_flux_z, vel_in[0],
-                  vel_in[1], vel_in[2], vel_out[0], vel_out[1], vel_out[2]);
+    auto sweep_x = [&](auto var) {
+      constexpr int V = decltype(var)::value;
+      launch_mapped(tg, s, kKeyMomSweepX | (V << 4), grid_mom_sweep_x, kMarchSeg, true, kBlk,
+                    k_mom_sweep_x<S, V, MapSingle>, k_mom_sweep_x<S, V, MapBatch>, ga,
+                    mass_flux_x, density1, vol_flux_x, vol_flux_y, vol_flux_z, vel_in[0],
+                    vel_in[1], vel_in[2], vel_out[0], vel_out[1], vel_out[2]);
+    };
+    if (sweep == 1) sweep_x(std::integral_constant<int, 0>{});
+    else sweep_x(std::integral_constant<int, 4>{});
   } else if (dir == 2) {
-    // node pass then velocity pass, each marching along y in segments
-    launch_mapped(tg, s, kKeyMomNode | 2u, grid_mom_node<2>, kMarchSeg, true, kBlk,
-                  k_mom_node_march<S, 2, MapSingle>, k_mom_node_march<S, 2, MapBatch>, variant,
-                  ga, mass_flux_y, density1, vol_flux_x, vol_flux_y, vol_flux_z, nd_flux,
-                  nd_post, nd_pre);
-    launch_mapped2(tg, s, kKeyMomVel3 | 2u, grid_mom_vel<2>, grid_mom_vel_flat<2>,
-                   kMarchSeg, true, kBlk, k_mom_vel3_march<S, 2, MapSingle>,
-                   k_mom_vel3_march<S, 2, MapBatch>, ga, nd_flux, nd_post, nd_pre, vel_in[0],
-                   vel_in[1], vel_in[2], vel_out[0], vel_out[1], vel_out[2]);
+    if (advect_x) node_vel(I2{}, std::integral_constant<int, 2>{});
+    else node_vel(I2{}, std::integral_constant<int, 3>{});
   } else {
-    launch_mapped(tg, s, kKeyMomNode | 3u, grid_mom_node<3>, kMarchSeg, true, kBlk,
-                  k_mom_node_march<S, 3, MapSingle>, k_mom_node_march<S, 3, MapBatch>, variant,
-                  ga, mass_flux_z, density1, vol_flux_x, vol_flux_y, vol_flux_z, nd_flux,
-                  nd_post, nd_pre);
-    launch_mapped2(tg, s, kKeyMomVel3 | 3u, grid_mom_vel<3>, grid_mom_vel_flat<3>,
-                   kMarchSeg, true, kBlk, k_mom_vel3_march<S, 3, MapSingle>,
-                   k_mom_vel3_march<S, 3, MapBatch>, ga, nd_flux, nd_post, nd_pre, vel_in[0],
-                   vel_in[1], vel_in[2], vel_out[0], vel_out[1], vel_out[2]);
+    if (sweep == 1) node_vel(I3{}, std::integral_constant<int, 1>{});
+    else node_vel(I3{}, std::integral_constant<int, 4>{});
   }
   // the updated buffers take the halo shell of the inputs
   using V = typename S::vel_t;
