@@ -376,21 +376,27 @@ __global__ void __launch_bounds__(BX * BY, 5) k_pdv_flux(M m, const double* dt_p
   const double dt = dt_ptr[(long long)t.d * kScalarStride];
   const bool jin = j <= g.x_max, kin = k <= g.y_max, lin = l <= g.z_max;
   using F = typename S::vf_t;
-  // face sums of the node velocities, reference order (vel0 x4 then vel1 x4)
+  // face sums of the node velocities, reference order (vel0 x4 then vel1 x4),
+  // in the policy's arithmetic: FP64, or in the mixed path the FP32 sum of
+  // the FP32 velocities, widened once per face (the fluxes, the corrector and
+  // its volume change stay FP64, and the corrector and the volume fluxes see
+  // the same face sums, as in FP64)
+  using A = typename S::arith_t;
+#define LA(a, jj, kk, ll) lda<A>(&E(a, jj, kk, ll))
   auto xsum = [&](int jj) {
-    return L(xvel0, jj, k, l) + L(xvel0, jj, k + 1, l) + L(xvel0, jj, k, l + 1) +
-           L(xvel0, jj, k + 1, l + 1) + L(xvel1, jj, k, l) + L(xvel1, jj, k + 1, l) +
-           L(xvel1, jj, k, l + 1) + L(xvel1, jj, k + 1, l + 1);
+    return (double)(LA(xvel0, jj, k, l) + LA(xvel0, jj, k + 1, l) + LA(xvel0, jj, k, l + 1) +
+                    LA(xvel0, jj, k + 1, l + 1) + LA(xvel1, jj, k, l) + LA(xvel1, jj, k + 1, l) +
+                    LA(xvel1, jj, k, l + 1) + LA(xvel1, jj, k + 1, l + 1));
   };
   auto ysum = [&](int kk) {
-    return L(yvel0, j, kk, l) + L(yvel0, j + 1, kk, l) + L(yvel0, j, kk, l + 1) +
-           L(yvel0, j + 1, kk, l + 1) + L(yvel1, j, kk, l) + L(yvel1, j + 1, kk, l) +
-           L(yvel1, j, kk, l + 1) + L(yvel1, j + 1, kk, l + 1);
+    return (double)(LA(yvel0, j, kk, l) + LA(yvel0, j + 1, kk, l) + LA(yvel0, j, kk, l + 1) +
+                    LA(yvel0, j + 1, kk, l + 1) + LA(yvel1, j, kk, l) + LA(yvel1, j + 1, kk, l) +
+                    LA(yvel1, j, kk, l + 1) + LA(yvel1, j + 1, kk, l + 1));
   };
   auto zsum = [&](int ll) {
-    return L(zvel0, j, k, ll) + L(zvel0, j + 1, k, ll) + L(zvel0, j, k + 1, ll) +
-           L(zvel0, j + 1, k + 1, ll) + L(zvel1, j, k, ll) + L(zvel1, j + 1, k, ll) +
-           L(zvel1, j, k + 1, ll) + L(zvel1, j + 1, k + 1, ll);
+    return (double)(LA(zvel0, j, k, ll) + LA(zvel0, j + 1, k, ll) + LA(zvel0, j, k + 1, ll) +
+                    LA(zvel0, j + 1, k + 1, ll) + LA(zvel1, j, k, ll) + LA(zvel1, j + 1, k, ll) +
+                    LA(zvel1, j, k + 1, ll) + LA(zvel1, j + 1, k + 1, ll));
   };
   double sx = 0, sy = 0, sz = 0;
   if (kin && lin) {
@@ -403,9 +409,10 @@ __global__ void __launch_bounds__(BX * BY, 5) k_pdv_flux(M m, const double* dt_p
   }
   if (jin && kin) {
     // flux_calc_kernel.f90:86 repeats zvel0(j+1,k,l) and omits zvel0(j,k+1,l)
-    const double bz = L(zvel0, j, k, l) + L(zvel0, j + 1, k, l) + L(zvel0, j + 1, k, l) +
-                      L(zvel0, j + 1, k + 1, l) + L(zvel1, j, k, l) + L(zvel1, j + 1, k, l) +
-                      L(zvel1, j, k + 1, l) + L(zvel1, j + 1, k + 1, l);
+    const double bz = (double)(LA(zvel0, j, k, l) + LA(zvel0, j + 1, k, l) +
+                               LA(zvel0, j + 1, k, l) + LA(zvel0, j + 1, k + 1, l) +
+                               LA(zvel1, j, k, l) + LA(zvel1, j + 1, k, l) +
+                               LA(zvel1, j, k + 1, l) + LA(zvel1, j + 1, k + 1, l));
     E(vol_flux_z, j, k, l) = st<F>(0.125 * dt * g.za * bz);
     sz = zsum(l);
   }
@@ -425,6 +432,7 @@ __global__ void __launch_bounds__(BX * BY, 5) k_pdv_flux(M m, const double* dt_p
       (L(pressure, j, k, l) / d0 + L(viscosity, j, k, l) / d0) * total_flux * recip_volume;
   E(energy1, j, k, l) = st<typename S::ene_t>(L(energy0, j, k, l) - energy_change);
   E(density1, j, k, l) = st<typename S::rho_t>(d0 * vol_change_s);
+#undef LA
   });
 }
 
