@@ -1065,26 +1065,58 @@ __global__ void __launch_bounds__(BX * BY, 3) k_mom_sweep_x(M m,
   });
 }
 
-// Copy the halo shell of three vertex arrays (every node outside
-// [min, max+1]^3) from one buffer of a pair to the other.
-template <class T, class M>
-__global__ void k_vert_shell_copy(M m, const T* __restrict__ a_in, const T* __restrict__ b_in,
-                                  const T* __restrict__ c_in, T* __restrict__ a_out,
-                                  T* __restrict__ b_out, T* __restrict__ c_out) {
-  m.run([&](const Geom& g, const Tile& t) {
-  int j, k;
-  if (!tile_jk<M>(Box{g.x_min - 2, g.x_max + 3, g.y_min - 2, g.y_max + 3, 0, 0}, t, j, k)) return;
-  const int l = g.z_min - 2 + t.z;
-  const bool inside = j >= g.x_min && j <= g.x_max + 1 && k >= g.y_min && k <= g.y_max + 1 &&
-                      l >= g.z_min && l <= g.z_max + 1;
-  if (inside) return;
-  const long long o = off3(g, j, k, l);
+// Copy the halo shell of three vertex arrays (every node of [min-2, max+3]^3
+// outside [min, max+1]^3) from one buffer of a pair to the other, touching
+// the shell only: k_vert_shell_planes takes the four halo planes l whole
+// (tile z 0..3: z_min-2, z_min-1, z_max+2, z_max+3), k_vert_shell_ring the
+// ring of each interior plane (the four shell rows k whole, then the four
+// shell columns j of each interior row).
+template <class T>
+__device__ __forceinline__ void copy3_at(long long o, const T* __restrict__ a_in,
+                                         const T* __restrict__ b_in, const T* __restrict__ c_in,
+                                         T* __restrict__ a_out, T* __restrict__ b_out,
+                                         T* __restrict__ c_out) {
   a_out[o] = a_in[o];
   b_out[o] = b_in[o];
   c_out[o] = c_in[o];
+}
+
+template <class T, class M>
+__global__ void k_vert_shell_planes(M m, const T* __restrict__ a_in, const T* __restrict__ b_in,
+                                    const T* __restrict__ c_in, T* __restrict__ a_out,
+                                    T* __restrict__ b_out, T* __restrict__ c_out) {
+  m.run([&](const Geom& g, const Tile& t) {
+  int j, k;
+  if (!tile_jk<M>(Box{g.x_min - 2, g.x_max + 3, g.y_min - 2, g.y_max + 3, 0, 0}, t, j, k)) return;
+  const int l = t.z < 2 ? g.z_min - 2 + t.z : g.z_max + t.z;
+  copy3_at(off3(g, j, k, l), a_in, b_in, c_in, a_out, b_out, c_out);
   });
 }
 
+template <class T, class M>
+__global__ void k_vert_shell_ring(M m, const T* __restrict__ a_in, const T* __restrict__ b_in,
+                                  const T* __restrict__ c_in, T* __restrict__ a_out,
+                                  T* __restrict__ b_out, T* __restrict__ c_out) {
+  m.run([&](const Geom& g, const Tile& t) {
+  const int w = g.x_max - g.x_min + 6;        // nodes of a shell row
+  const int rows = g.y_max - g.y_min + 2;     // interior rows k in [y_min, y_max+1]
+  const int e = t.x * (BX * BY) + (int)threadIdx.y * BX + (int)threadIdx.x;
+  const int l = g.z_min + t.z;                // interior planes [z_min, z_max+1]
+  int j, k;
+  if (e < 4 * w) {
+    const int r = e / w;
+    j = g.x_min - 2 + e % w;
+    k = r < 2 ? g.y_min - 2 + r : g.y_max + r;
+  } else {
+    const int f = e - 4 * w;
+    if (f >= 4 * rows) return;
+    const int c = f % 4;
+    k = g.y_min + f / 4;
+    j = c < 2 ? g.x_min - 2 + c : g.x_max + c;
+  }
+  copy3_at(off3(g, j, k, l), a_in, b_in, c_in, a_out, b_out, c_out);
+  });
+}
 
 // ===========================================================================
 // Tile grids of the launches (aux: segment length of a marching kernel)
@@ -1109,8 +1141,20 @@ dim3 grid_cell_shell(const Geom& g, int) {
 dim3 grid_cell_shell_flat(const Geom& g, int) {
   return grid_flat(Box{g.x_min - 2, g.x_max + 2, g.y_min - 2, g.y_max + 2, g.z_min - 2, g.z_max + 2});
 }
-dim3 grid_shell_flat(const Geom& g, int) {
-  return grid_flat(Box{g.x_min - 2, g.x_max + 3, g.y_min - 2, g.y_max + 3, g.z_min - 2, g.z_max + 3});
+// the vertex shell: four whole halo planes, and the ring of each interior plane
+dim3 grid_shell_planes_flat(const Geom& g, int) {
+  dim3 d = grid_flat(Box{g.x_min - 2, g.x_max + 3, g.y_min - 2, g.y_max + 3, 0, 0});
+  d.z = 4;
+  return d;
+}
+dim3 grid_shell_planes(const Geom& g, int) {
+  dim3 d = grid_of(Box{g.x_min - 2, g.x_max + 3, g.y_min - 2, g.y_max + 3, 0, 0});
+  d.z = 4;
+  return d;
+}
+dim3 grid_shell_ring(const Geom& g, int) {
+  const int ring = 4 * (g.x_max - g.x_min + 6) + 4 * (g.y_max - g.y_min + 2);
+  return dim3((ring + BX * BY - 1) / (BX * BY), 1, g.z_max - g.z_min + 2);
 }
 // 32 columns j of one cross-axis index per block, BY segments along the sweep
 template <int DIR>
@@ -1147,10 +1191,6 @@ dim3 grid_mom_vel(const Geom& g, int seg) {
 dim3 grid_mom_sweep_x(const Geom& g, int seg) {
   return dim3((g.x_max + 1 - g.x_min + 1 + 28) / 29, (g.y_max + 1 - g.y_min + 1 + BY - 1) / BY,
               (g.z_max + 1 - g.z_min + 1 + seg - 1) / seg);
-}
-dim3 grid_shell(const Geom& g, int) {
-  return dim3((g.x_max - g.x_min + 6 + BX - 1) / BX, (g.y_max - g.y_min + 6 + BY - 1) / BY,
-              g.z_max - g.z_min + 6);
 }
 
 }  // namespace
@@ -1238,7 +1278,8 @@ void launch_advec_cell_x(const Target& tg, cudaStream_t s, int sweep, const Geom
                          const typename S::rho_t* density1_in, const typename S::ene_t* energy1_in,
                          typename S::rho_t* density1_out, typename S::ene_t* energy1_out,
                          const typename S::vf_t* vol_flux_x, const typename S::vf_t* vol_flux_y,
-                         const typename S::vf_t* vol_flux_z, typename S::mf_t* mass_flux_x) {
+                         const typename S::vf_t* vol_flux_z, typename S::mf_t* mass_flux_x,
+                         bool copy_shell) {
   // pre_vol variant: 0 on sweep 1 (all three flux differences), 1 on sweep 3
   if (sweep == 1)
     launch_mapped(tg, s, kKeyCellSweepX, grid_cell_sweep_x, 0, false, kBlk,
@@ -1251,11 +1292,13 @@ void launch_advec_cell_x(const Target& tg, cudaStream_t s, int sweep, const Geom
                   density1_in, energy1_in, density1_out, energy1_out, vol_flux_x, vol_flux_y,
                   vol_flux_z, mass_flux_x);
   // the cells the sweep does not update keep their values in the output pair
-  using R = typename S::rho_t;
-  using En = typename S::ene_t;
-  launch_mapped2(tg, s, kKeyCellShell, grid_cell_shell, grid_cell_shell_flat, 0, false, kBlk,
-                k_cell_shell_copy<R, En, MapSingle>, k_cell_shell_copy<R, En, MapBatch>,
-                density1_in, energy1_in, density1_out, energy1_out);
+  if (copy_shell) {
+    using R = typename S::rho_t;
+    using En = typename S::ene_t;
+    launch_mapped2(tg, s, kKeyCellShell, grid_cell_shell, grid_cell_shell_flat, 0, false, kBlk,
+                   k_cell_shell_copy<R, En, MapSingle>, k_cell_shell_copy<R, En, MapBatch>,
+                   density1_in, energy1_in, density1_out, energy1_out);
+  }
 }
 
 template <class S>
@@ -1266,7 +1309,7 @@ void launch_advec_mom_fused(const Target& tg, cudaStream_t s, int advect_x, int 
                             const typename S::vf_t* vol_flux_y, const typename S::vf_t* vol_flux_z,
                             typename S::wk_t* node_flux, typename S::wk_t* node_mass_post,
                             typename S::wk_t* node_mass_pre, typename S::vel_t* const* vel_in,
-                            typename S::vel_t* const* vel_out) {
+                            typename S::vel_t* const* vel_out, bool copy_shell) {
   // the node arrays of the y/z sweeps live in three work arrays, as nd_t
   using ND = typename S::nd_t;
   static_assert(sizeof(ND) <= sizeof(typename S::wk_t), "node arrays fit the work arrays");
@@ -1309,10 +1352,15 @@ void launch_advec_mom_fused(const Target& tg, cudaStream_t s, int advect_x, int 
     else node_vel(I3{}, std::integral_constant<int, 4>{});
   }
   // the updated buffers take the halo shell of the inputs
-  using V = typename S::vel_t;
-  launch_mapped2(tg, s, kKeyShellCopy, grid_shell, grid_shell_flat, 0, false, kBlk, k_vert_shell_copy<V, MapSingle>,
-                k_vert_shell_copy<V, MapBatch>, vel_in[0], vel_in[1], vel_in[2], vel_out[0],
-                vel_out[1], vel_out[2]);
+  if (copy_shell) {
+    using V = typename S::vel_t;
+    launch_mapped2(tg, s, kKeyShellCopy, grid_shell_planes, grid_shell_planes_flat, 0, false,
+                   kBlk, k_vert_shell_planes<V, MapSingle>, k_vert_shell_planes<V, MapBatch>,
+                   vel_in[0], vel_in[1], vel_in[2], vel_out[0], vel_out[1], vel_out[2]);
+    launch_mapped(tg, s, kKeyShellCopy | 1u, grid_shell_ring, 0, false, kBlk,
+                  k_vert_shell_ring<V, MapSingle>, k_vert_shell_ring<V, MapBatch>, vel_in[0],
+                  vel_in[1], vel_in[2], vel_out[0], vel_out[1], vel_out[2]);
+  }
 }
 
 #define INSTF(S)                                                                               \
@@ -1337,12 +1385,12 @@ void launch_advec_mom_fused(const Target& tg, cudaStream_t s, int advect_x, int 
   template void launch_advec_cell_x<S>(const Target&, cudaStream_t, int, const GeomArrays&,      \
                                        const S::rho_t*, const S::ene_t*, S::rho_t*, S::ene_t*,  \
                                        const S::vf_t*, const S::vf_t*, const S::vf_t*,          \
-                                       S::mf_t*);                                               \
+                                       S::mf_t*, bool);                                         \
   template void launch_advec_mom_fused<S>(const Target&, cudaStream_t, int, int, int, double,    \
                                           const GeomArrays&, const S::rho_t*, const S::mf_t*,  \
                                           const S::mf_t*, const S::mf_t*, const S::vf_t*,      \
                                           const S::vf_t*, const S::vf_t*, S::wk_t*, S::wk_t*,  \
-                                          S::wk_t*, S::vel_t* const*, S::vel_t* const*);
+                                          S::wk_t*, S::vel_t* const*, S::vel_t* const*, bool);
 
 INSTF(F64)
 INSTF(F32Mixed)

@@ -343,15 +343,20 @@ void launch_advec_cell_fused(const Target& tg, cudaStream_t s, int advect_x, int
                              const typename S::vf_t* vol_flux_y, typename S::mf_t* mass_flux_z,
                              const typename S::vf_t* vol_flux_z, typename S::wk_t* ener_flux);
 // The x cell sweep out of place: density1/energy1 in one buffer pair, the
-// updated values (and a copy of every cell outside the interior) in the other.
+// updated values in the other, and with copy_shell a copy of every cell
+// outside the interior (left out where a depth-2 halo update of density1 and
+// energy1 follows, which rewrites all of them from the interior).
 template <class S>
 void launch_advec_cell_x(const Target& tg, cudaStream_t s, int sweep, const GeomArrays& ga,
                          const typename S::rho_t* density1_in, const typename S::ene_t* energy1_in,
                          typename S::rho_t* density1_out, typename S::ene_t* energy1_out,
                          const typename S::vf_t* vol_flux_x, const typename S::vf_t* vol_flux_y,
-                         const typename S::vf_t* vol_flux_z, typename S::mf_t* mass_flux_x);
+                         const typename S::vf_t* vol_flux_z, typename S::mf_t* mass_flux_x,
+                         bool copy_shell);
 // All three velocities of one sweep; vel_in/vel_out are the two buffers of
-// each velocity pair (the shell outside [min,max+1]^3 is copied across).
+// each velocity pair, and with copy_shell the shell outside [min,max+1]^3 is
+// copied across (left out where a depth-2 halo update of the velocities
+// comes before the next read of the shell).
 // vol: the uniform cell volume of the chunk (dx*dy*dz).
 template <class S>
 void launch_advec_mom_fused(const Target& tg, cudaStream_t s, int advect_x, int sweep, int dir,
@@ -361,7 +366,7 @@ void launch_advec_mom_fused(const Target& tg, cudaStream_t s, int advect_x, int 
                             const typename S::vf_t* vol_flux_y, const typename S::vf_t* vol_flux_z,
                             typename S::wk_t* node_flux, typename S::wk_t* node_mass_post,
                             typename S::wk_t* node_mass_pre, typename S::vel_t* const* vel_in,
-                            typename S::vel_t* const* vel_out);
+                            typename S::vel_t* const* vel_out, bool copy_shell);
 
 // Fill every element of an array (size elems after the pad) with a value.
 template <class T>

@@ -151,6 +151,17 @@ struct Chunk : ChunkBase {
   bool advect_x = true;  // start.f90:99
   bool use_graphs = true;
   bool fused = true;  // fused kernels (clover_fused.cu) instead of one kernel per reference pass
+  // Every axis of every deck has at least three cells. A repeated halo update
+  // of a cell field, a vertex velocity or a z-face flux, whose values have
+  // not changed since its last update at the same depth, then rewrites every
+  // halo cell with the value it holds (update_halo_kernel.f90 is idempotent
+  // for those fields on such grids; not for the x- and y-face fluxes, whose
+  // far halo corners keep values read before a later face pass wrote them),
+  // so the fused step leaves such repeats out. A depth-2 update of those
+  // fields also rewrites every halo cell from the interior whatever it held,
+  // so the shell copies of the out-of-place sweeps are left out where one
+  // follows before the shell is read.
+  bool halo_repeat_free = false;
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
   int launches_per_step = 0;
   int ext[6] = {1, 1, 1, 1, 1, 1};
@@ -262,6 +273,10 @@ struct Chunk : ChunkBase {
       geoms.push_back(q);
     }
     g = geoms[0];
+    halo_repeat_free = true;
+    for (int d = 0; d < nd; d++)
+      if (decks[d].x_cells < 3 || decks[d].y_cells < 3 || decks[d].z_cells < 3)
+        halo_repeat_free = false;
     if (cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking) != cudaSuccess) return false;
     if (batched) {
       plan = new BatchPlan;
@@ -744,7 +759,10 @@ struct Chunk : ChunkBase {
     auto sweep = [&](int sweep_number, int dir, bool pre_halo) {
       if (pre_halo) {
         pbeg();
-        halo({4, 2, 14, 15, 16}, 2, vc, cb);
+        // before sweep 2, density1 and energy1 (updated after sweep 1) and
+        // vol_flux_z (updated before sweep 1) have not changed since
+        if (sweep_number == 2 && halo_repeat_free) halo({14, 15}, 2, vc, cb);
+        else halo({4, 2, 14, 15, 16}, 2, vc, cb);
         pend("update_halo", 0);
       }
       // volume fluxes read for pre_vol: all three on sweep 1, two on the y sweep,
@@ -753,8 +771,10 @@ struct Chunk : ChunkBase {
       pbeg();
       if (dir == 1) {
         // one pass, out of place into the other buffer of the pair
+        // the post-sweep depth-2 halo update rewrites the output pair's shell
         launch_advec_cell_x<S>(tg, stream, sweep_number, ga, rho1(cb), ene1(cb), rho1(cb ^ 1),
-                               ene1(cb ^ 1), vol_flux_x, vol_flux_y, vol_flux_z, mass_flux_x);
+                               ene1(cb ^ 1), vol_flux_x, vol_flux_y, vol_flux_z, mass_flux_x,
+                               !halo_repeat_free);
         cb ^= 1;
         pend("advec_cell_x", n * (nvf * VF8 + 2 * R8 + 2 * E8 + MF8));
       } else {
@@ -765,16 +785,22 @@ struct Chunk : ChunkBase {
         pend("advec_cell_yz", n * (nvf * VF8 + 2 * R8 + 2 * E8 + MF8));
       }
       pbeg();
-      halo({2, 4, 9, 11, 13, 17, 18, 19}, 2, vc, cb);
+      // mass_flux_z changes only in the z sweep and is updated right after it
+      if (dir != 3 && halo_repeat_free) halo({2, 4, 9, 11, 13, 17, 18}, 2, vc, cb);
+      else halo({2, 4, 9, 11, 13, 17, 18, 19}, 2, vc, cb);
       pend("update_halo", 0);
       // post_vol reads two volume fluxes on sweep 1, one on sweep 2, none on sweep 3
       const double npv = sweep_number == 1 ? 2 : sweep_number == 2 ? 1 : 0;
       V* vin[3] = {vel1(0, vc), vel1(1, vc), vel1(2, vc)};
       V* vout[3] = {vel1(0, vc ^ 1), vel1(1, vc ^ 1), vel1(2, vc ^ 1)};
       pbeg();
-      launch_advec_mom_fused<S>(tg, stream, axi, sweep_number, dir, cell_volume, ga, rho1(cb), mass_flux_x,
-                                mass_flux_y, mass_flux_z, vol_flux_x, vol_flux_y, vol_flux_z,
-                                work[0], work[1], work[2], vin, vout);
+      // after sweeps 1 and 2 the next post-sweep depth-2 halo update rewrites
+      // the velocities' shell before anything reads it; after sweep 3 the
+      // shell carries the step's final halo values
+      launch_advec_mom_fused<S>(tg, stream, axi, sweep_number, dir, cell_volume, ga, rho1(cb),
+                                mass_flux_x, mass_flux_y, mass_flux_z, vol_flux_x, vol_flux_y,
+                                vol_flux_z, work[0], work[1], work[2], vin, vout,
+                                sweep_number == 3 || !halo_repeat_free);
       // x: one pass; y, z: node pass + velocity pass
       if (dir == 1)
         pend("advec_mom_x", n * (MF8 + R8 + npv * VF8 + 6 * V8));

@@ -56,3 +56,82 @@ def test_reference_index_ranges_in_bounds_on_edge_grids():
     assert r.returncode == 0, r.stderr[-2000:]
     assert "runtime error" not in r.stderr and "AddressSanitizer" not in r.stderr
     assert r.stdout.count("steps 6") == 9
+
+
+def test_halo_update_repeat_is_a_no_op_for_cell_vertex_and_z_face_fields():
+    """update_halo_kernel.f90 applied twice equals applying it once for the
+    cell fields, the vertex velocities and the z-face fluxes, at depth 1 and
+    2, when each axis has at least three cells: the sources of every halo copy
+    then lie inside the chunk along the face normal, and a corner cell that a
+    face pass reads stale is rewritten by a later pass. The native step relies
+    on this to leave out repeats of an update whose fields are unchanged since
+    their last one (density1, energy1 and vol_flux_z in the second pre-sweep
+    update of advection.f90, mass_flux_z after the x and y sweeps). The x- and
+    y-face fluxes are not repeat-safe: the z faces do not reach their far
+    halo columns (j = x_max+2.. for x faces), whose corners keep values a face
+    pass read before a later pass wrote them. On thinner axes a face's high
+    side reads cells its low side writes."""
+    import hydro_harness as H
+    rng = np.random.default_rng(11)
+    lib = O.load()
+    deck = {"initial_timestep": 0.04}
+    safe = ["density0", "density1", "energy0", "energy1", "pressure", "viscosity",
+            "soundspeed", "xvel0", "xvel1", "yvel0", "yvel1", "zvel0", "zvel1", "vol_flux_z",
+            "mass_flux_z"]
+    unsafe = ["vol_flux_x", "mass_flux_x", "vol_flux_y", "mass_flux_y"]
+    for nx, ny, nz in [(3, 3, 3), (5, 4, 6), (7, 3, 9), (4, 8, 3)]:
+        for depth in (1, 2):
+            a = H.new_chunk(nx, ny, nz)
+            for k in H.ARRAYS_3D:
+                a[k][...] = rng.standard_normal(a[k].shape)
+            h = H.Hydro(H.Backend(lib, "oracle_"), a, nx, ny, nz, deck)
+            h.halo(list(range(1, 20)), depth)
+            once = H.clone(a)
+            h.halo(list(range(1, 20)), depth)
+            for k in safe:
+                assert np.array_equal(a[k].view(np.uint64), once[k].view(np.uint64)), \
+                    (nx, ny, nz, depth, k)
+            for k in unsafe:
+                assert not np.array_equal(a[k], once[k]), (nx, ny, nz, depth, k)
+    # a one-cell axis: the repeat changes the far halo layer of a cell field
+    a = H.new_chunk(4, 1, 4)
+    for k in H.ARRAYS_3D:
+        a[k][...] = rng.standard_normal(a[k].shape)
+    h = H.Hydro(H.Backend(lib, "oracle_"), a, 4, 1, 4, deck)
+    h.halo([1], 2)
+    once = H.clone(a)
+    h.halo([1], 2)
+    assert not np.array_equal(a["density0"], once["density0"])
+
+
+def test_depth_two_halo_update_rewrites_every_halo_cell_of_cell_and_vertex_fields():
+    """A depth-2 update_halo_kernel.f90 call leaves the halo of every cell
+    field and vertex velocity (and of vol_flux_z, mass_flux_z) a function of
+    the interior alone, on grids with three or more cells per axis: two
+    states with the same interior and different halos agree after it. The
+    native step's out-of-place sweeps therefore copy no halo shell into their
+    output buffers when such an update of those fields follows before the
+    shell is read."""
+    import hydro_harness as H
+    rng = np.random.default_rng(5)
+    lib = O.load()
+    deck = {"initial_timestep": 0.04}
+    extra = {"cell": (0, 0, 0), "vert": (1, 1, 1), "work": (1, 1, 1), "xface": (1, 0, 0),
+             "yface": (0, 1, 0), "zface": (0, 0, 1)}
+    fields = ["density0", "density1", "energy0", "energy1", "pressure", "viscosity",
+              "soundspeed", "xvel0", "xvel1", "yvel0", "yvel1", "zvel0", "zvel1", "vol_flux_z",
+              "mass_flux_z"]
+    for nx, ny, nz in [(3, 3, 3), (5, 4, 6), (7, 3, 9)]:
+        base = H.new_chunk(nx, ny, nz)
+        for k in H.ARRAYS_3D:
+            base[k][...] = rng.standard_normal(base[k].shape)
+        a, b = H.clone(base), H.clone(base)
+        for k, kind in H.ARRAYS_3D.items():
+            ex = extra[kind]
+            halo = np.ones(b[k].shape, bool)
+            halo[2:2 + nx + ex[0], 2:2 + ny + ex[1], 2:2 + nz + ex[2]] = False
+            b[k][halo] = rng.standard_normal(int(halo.sum()))
+        for arr in (a, b):
+            H.Hydro(H.Backend(lib, "oracle_"), arr, nx, ny, nz, deck).halo(list(range(1, 20)), 2)
+        for k in fields:
+            assert np.array_equal(a[k].view(np.uint64), b[k].view(np.uint64)), (nx, ny, nz, k)
