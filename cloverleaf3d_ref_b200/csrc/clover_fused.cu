@@ -1218,7 +1218,7 @@ void launch_pdv_predict_eos(const Target& tg, cudaStream_t s, const double* dt_p
                             const typename S::cs_t* viscosity, const typename S::vel_t* xvel0,
                             const typename S::vel_t* yvel0, const typename S::vel_t* zvel0) {
   launch_mapped2(tg, s, kKeyPdvPredict, grid_interior, grid_interior_flat, 0, false, kBlk,
-                k_pdv_predict_eos<S, MapSingle>, k_pdv_predict_eos<S, MapBatch>, dt_ptr, ga,
+                k_pdv_predict_eos<S, MapSingle>, k_pdv_predict_eos<S, MapBatchFree>, dt_ptr, ga,
                 density0, energy0, pressure, viscosity, xvel0, yvel0, zvel0);
 }
 
@@ -1233,7 +1233,7 @@ void launch_pdv_flux(const Target& tg, cudaStream_t s, const double* dt_ptr, con
                      typename S::vf_t* vol_flux_x, typename S::vf_t* vol_flux_y,
                      typename S::vf_t* vol_flux_z) {
   launch_mapped2(tg, s, kKeyPdvFlux, grid_nodes, grid_nodes_flat, 0, false, kBlk, k_pdv_flux<S, MapSingle>,
-                k_pdv_flux<S, MapBatch>, dt_ptr, ga, density0, density1, energy0, energy1,
+                k_pdv_flux<S, MapBatchFree>, dt_ptr, ga, density0, density1, energy0, energy1,
                 pressure, viscosity, xvel0, xvel1, yvel0, yvel1, zvel0, zvel1, vol_flux_x,
                 vol_flux_y, vol_flux_z);
 }
@@ -1283,12 +1283,12 @@ void launch_advec_cell_x(const Target& tg, cudaStream_t s, int sweep, const Geom
   // pre_vol variant: 0 on sweep 1 (all three flux differences), 1 on sweep 3
   if (sweep == 1)
     launch_mapped(tg, s, kKeyCellSweepX, grid_cell_sweep_x, 0, false, kBlk,
-                  k_cell_sweep_x<S, 0, MapSingle>, k_cell_sweep_x<S, 0, MapBatch>, ga,
+                  k_cell_sweep_x<S, 0, MapSingle>, k_cell_sweep_x<S, 0, MapBatchFree>, ga,
                   density1_in, energy1_in, density1_out, energy1_out, vol_flux_x, vol_flux_y,
                   vol_flux_z, mass_flux_x);
   else
     launch_mapped(tg, s, kKeyCellSweepX | (1u << 4), grid_cell_sweep_x, 0, false, kBlk,
-                  k_cell_sweep_x<S, 1, MapSingle>, k_cell_sweep_x<S, 1, MapBatch>, ga,
+                  k_cell_sweep_x<S, 1, MapSingle>, k_cell_sweep_x<S, 1, MapBatchFree>, ga,
                   density1_in, energy1_in, density1_out, energy1_out, vol_flux_x, vol_flux_y,
                   vol_flux_z, mass_flux_x);
   // the cells the sweep does not update keep their values in the output pair
@@ -1296,7 +1296,7 @@ void launch_advec_cell_x(const Target& tg, cudaStream_t s, int sweep, const Geom
     using R = typename S::rho_t;
     using En = typename S::ene_t;
     launch_mapped2(tg, s, kKeyCellShell, grid_cell_shell, grid_cell_shell_flat, 0, false, kBlk,
-                   k_cell_shell_copy<R, En, MapSingle>, k_cell_shell_copy<R, En, MapBatch>,
+                   k_cell_shell_copy<R, En, MapSingle>, k_cell_shell_copy<R, En, MapBatchFree>,
                    density1_in, energy1_in, density1_out, energy1_out);
   }
 }
@@ -1323,11 +1323,11 @@ void launch_advec_mom_fused(const Target& tg, cudaStream_t s, int advect_x, int 
     constexpr int D = decltype(dir_c)::value, V = decltype(var)::value;
     // node pass then velocity pass, each marching along the sweep axis in segments
     launch_mapped(tg, s, kKeyMomNode | D | (V << 4), grid_mom_node<D>, kMarchSeg, true, kBlk,
-                  k_mom_node_march<S, D, V, MapSingle>, k_mom_node_march<S, D, V, MapBatch>, ga,
+                  k_mom_node_march<S, D, V, MapSingle>, k_mom_node_march<S, D, V, MapBatchFree>, ga,
                   D == 2 ? mass_flux_y : mass_flux_z, density1, vol_flux_x, vol_flux_y,
                   vol_flux_z, nd_flux, nd_post, nd_pre);
     launch_mapped2(tg, s, kKeyMomVel3 | D, grid_mom_vel<D>, grid_mom_vel_flat<D>, kMarchSeg,
-                   true, kBlk, k_mom_vel3_march<S, D, MapSingle>, k_mom_vel3_march<S, D, MapBatch>,
+                   true, kBlk, k_mom_vel3_march<S, D, MapSingle>, k_mom_vel3_march<S, D, MapBatchFree>,
                    ga, nd_flux, nd_post, nd_pre, vel_in[0], vel_in[1], vel_in[2], vel_out[0],
                    vel_out[1], vel_out[2]);
   };
@@ -1338,7 +1338,7 @@ void launch_advec_mom_fused(const Target& tg, cudaStream_t s, int advect_x, int 
     auto sweep_x = [&](auto var) {
       constexpr int V = decltype(var)::value;
       launch_mapped(tg, s, kKeyMomSweepX | (V << 4), grid_mom_sweep_x, kMarchSeg, true, kBlk,
-                    k_mom_sweep_x<S, V, MapSingle>, k_mom_sweep_x<S, V, MapBatch>, ga,
+                    k_mom_sweep_x<S, V, MapSingle>, k_mom_sweep_x<S, V, MapBatchFree>, ga,
                     mass_flux_x, density1, vol_flux_x, vol_flux_y, vol_flux_z, vel_in[0],
                     vel_in[1], vel_in[2], vel_out[0], vel_out[1], vel_out[2]);
     };
@@ -1355,10 +1355,10 @@ void launch_advec_mom_fused(const Target& tg, cudaStream_t s, int advect_x, int 
   if (copy_shell) {
     using V = typename S::vel_t;
     launch_mapped2(tg, s, kKeyShellCopy, grid_shell_planes, grid_shell_planes_flat, 0, false,
-                   kBlk, k_vert_shell_planes<V, MapSingle>, k_vert_shell_planes<V, MapBatch>,
+                   kBlk, k_vert_shell_planes<V, MapSingle>, k_vert_shell_planes<V, MapBatchFree>,
                    vel_in[0], vel_in[1], vel_in[2], vel_out[0], vel_out[1], vel_out[2]);
     launch_mapped(tg, s, kKeyShellCopy | 1u, grid_shell_ring, 0, false, kBlk,
-                  k_vert_shell_ring<V, MapSingle>, k_vert_shell_ring<V, MapBatch>, vel_in[0],
+                  k_vert_shell_ring<V, MapSingle>, k_vert_shell_ring<V, MapBatchFree>, vel_in[0],
                   vel_in[1], vel_in[2], vel_out[0], vel_out[1], vel_out[2]);
   }
 }

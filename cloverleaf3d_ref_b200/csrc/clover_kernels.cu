@@ -1126,7 +1126,7 @@ void launch_ideal_gas(const Target& tg, cudaStream_t s, const typename S::rho_t*
                       const typename S::ene_t* energy, typename S::cs_t* pressure,
                       typename S::cs_t* soundspeed) {
   launch_mapped2(tg, s, kKeyIdealGas, grid_interior, grid_interior_flat, 0, false, dim3(BX, BY),
-                k_ideal_gas<S, MapSingle>, k_ideal_gas<S, MapBatch>, density, energy, pressure,
+                k_ideal_gas<S, MapSingle>, k_ideal_gas<S, MapBatchFree>, density, energy, pressure,
                 soundspeed);
 }
 
@@ -1181,12 +1181,12 @@ void launch_accelerate(const Target& tg, cudaStream_t s, double dt_val, const do
                        typename S::vel_t* yvel1, typename S::vel_t* zvel1, bool uniform_mesh) {
   if (uniform_mesh)
     launch_mapped2(tg, s, kKeyAccelerate, grid_nodes, grid_nodes_flat, 0, false, dim3(BX, BY),
-                   k_accelerate<S, MapSingle, true>, k_accelerate<S, MapBatch, true>, dt_val,
+                   k_accelerate<S, MapSingle, true>, k_accelerate<S, MapBatchFree, true>, dt_val,
                    dt_ptr, ga, density0, pressure, viscosity, xvel0, yvel0, zvel0, xvel1, yvel1,
                    zvel1);
   else
     launch_mapped2(tg, s, kKeyAccelerate, grid_nodes, grid_nodes_flat, 0, false, dim3(BX, BY),
-                   k_accelerate<S, MapSingle, false>, k_accelerate<S, MapBatch, false>, dt_val,
+                   k_accelerate<S, MapSingle, false>, k_accelerate<S, MapBatchFree, false>, dt_val,
                    dt_ptr, ga, density0, pressure, viscosity, xvel0, yvel0, zvel0, xvel1, yvel1,
                    zvel1);
 }
@@ -1306,7 +1306,7 @@ void launch_reset_field(const Target& tg, cudaStream_t s, typename S::rho_t* den
                         const typename S::vel_t* yvel1, typename S::vel_t* zvel0,
                         const typename S::vel_t* zvel1) {
   launch_mapped2(tg, s, kKeyReset, grid_nodes, grid_nodes_flat, 0, false, dim3(BX, BY), k_reset<S, MapSingle>,
-                k_reset<S, MapBatch>, density0, density1, energy0, energy1, xvel0, xvel1, yvel0,
+                k_reset<S, MapBatchFree>, density0, density1, energy0, energy1, xvel0, xvel1, yvel0,
                 yvel1, zvel0, zvel1);
 }
 
@@ -1380,17 +1380,17 @@ void launch_update_halo(const Target& tg, cudaStream_t s, const HaloFields& f, c
       const unsigned kx = kKeyHaloX | (unsigned)per_row;
       if (depth == 1)
         launch_mapped(tg, s, kx, grid_halo_x<1>, per_row, false, blk, k_halo_x<MapSingle>,
-                      k_halo_x<MapBatch>, h, depth, do_low, do_high);
+                      k_halo_x<MapBatchFree>, h, depth, do_low, do_high);
       else
         launch_mapped(tg, s, kx, grid_halo_x<2>, per_row, false, blk, k_halo_x<MapSingle>,
-                      k_halo_x<MapBatch>, h, depth, do_low, do_high);
+                      k_halo_x<MapBatchFree>, h, depth, do_low, do_high);
     }
     else if (ax == 1)
       launch_mapped2(tg, s, key, grid_halo<1>, grid_halo_flat<1>, depth, false, blk,
-                     k_halo<1, MapSingle>, k_halo<1, MapBatch>, h, depth, do_low, do_high);
+                     k_halo<1, MapSingle>, k_halo<1, MapBatchFree>, h, depth, do_low, do_high);
     else
       launch_mapped2(tg, s, key, grid_halo<2>, grid_halo_flat<2>, depth, false, blk,
-                     k_halo<2, MapSingle>, k_halo<2, MapBatch>, h, depth, do_low, do_high);
+                     k_halo<2, MapSingle>, k_halo<2, MapBatchFree>, h, depth, do_low, do_high);
   }
 }
 

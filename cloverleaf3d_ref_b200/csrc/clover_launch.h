@@ -69,10 +69,10 @@ struct Target {
 
 // Launch kernel ks over one chunk (grid from grid_fn) or kb over the plan's
 // schedule; both get the map first and then args.
-template <class... P, class... A>
+template <class MB, class... P, class... A>
 inline void launch_mapped(const Target& tg, cudaStream_t s, unsigned key, GridFn grid_fn, int aux,
                           bool seg_tunable, dim3 blk, void (*ks)(MapSingle, P...),
-                          void (*kb)(MapBatch, P...), A&&... args) {
+                          void (*kb)(MB, P...), A&&... args) {
   if (!tg.plan) {
     const dim3 gr = grid_fn(tg.g, aux);
     if (gr.x && gr.y && gr.z) ks<<<gr, blk, 0, s>>>(MapSingle{tg.g, aux}, std::forward<A>(args)...);
@@ -82,16 +82,16 @@ inline void launch_mapped(const Target& tg, cudaStream_t s, unsigned key, GridFn
                                       (int)(blk.x * blk.y * blk.z));
   if (bl.grid <= 0) return;
   batch_mark(tg.plan, key, s, true);
-  kb<<<bl.grid, blk, 0, s>>>(MapBatch{bl.items, bl.decks, bl.n, bl.aux}, std::forward<A>(args)...);
+  kb<<<bl.grid, blk, 0, s>>>(MB{bl.items, bl.decks, bl.n, bl.aux}, std::forward<A>(args)...);
   batch_mark(tg.plan, key, s, false);
 }
 
 // The same with another grid function for the batched launch (kernels whose
 // tiles a batch lays out differently, e.g. flattened (j, k) planes).
-template <class... P, class... A>
+template <class MB, class... P, class... A>
 inline void launch_mapped2(const Target& tg, cudaStream_t s, unsigned key, GridFn grid_single,
                            GridFn grid_batch, int aux, bool seg_tunable, dim3 blk,
-                           void (*ks)(MapSingle, P...), void (*kb)(MapBatch, P...),
+                           void (*ks)(MapSingle, P...), void (*kb)(MB, P...),
                            A&&... args) {
   if (!tg.plan) {
     launch_mapped(tg, s, key, grid_single, aux, seg_tunable, blk, ks, kb, std::forward<A>(args)...);

@@ -34,7 +34,11 @@ struct MapSingle {
   }
 };
 
-struct MapBatch {
+// kSync: a barrier after each item, for kernels whose threads share memory
+// within an item (the next item may reuse it only when every thread is done);
+// without it the warps of a block move on to their next item independently.
+template <bool kSync>
+struct MapBatchT {
   // box kernels take 256 consecutive cells of a deck's (j, k) plane per tile,
   // so that decks whose x extent is not a multiple of 32 fill every lane
   static constexpr bool kFlat = true;
@@ -48,10 +52,11 @@ struct MapBatch {
       const int4 it = __ldg(items + w);
       const Geom g = decks[it.x];
       f(g, Tile{it.x, it.y, it.z, it.w});
-      // shared memory of one item is free again only when every thread is done
-      __syncthreads();
+      if (kSync) __syncthreads();
     }
   }
 };
+using MapBatch = MapBatchT<true>;       // kernels with shared memory or block barriers
+using MapBatchFree = MapBatchT<false>;  // kernels whose warps work independently
 
 }  // namespace clover
