@@ -164,24 +164,38 @@ __global__ void __launch_bounds__(BX * BY, 3) k_visc_dt(M m, GeomArrays ga, doub
   int j, k;
   const bool in_jk = tile_jk<M>(b, t, j, k);
   unsigned long long key = ~0ull;
-  // kViscCellsZ cells along z per thread, unrolled so that the loads of one
-  // cell are in flight with the arithmetic of the other
-#pragma unroll
+  // kViscCellsZ cells along z per thread, one after another (not unrolled,
+  // which keeps the FP64 form's spills small); the node values of a cell's
+  // upper plane are the next cell's lower plane
+  A cp[12];
+  bool carried = false;
+#pragma unroll 1
   for (int iz = 0; iz < kViscCellsZ; iz++) {
   const int l = b.l0 + t.z * kViscCellsZ + iz;
   if (in_jk && l <= b.l1) {
-  const A u000 = LA(xvel0, j, k, l), u100 = LA(xvel0, j + 1, k, l);
-  const A u010 = LA(xvel0, j, k + 1, l), u110 = LA(xvel0, j + 1, k + 1, l);
+  A u000, u100, u010, u110, v000, v100, v010, v110, w000, w100, w010, w110;
+  if (carried) {
+    u000 = cp[0]; u100 = cp[1]; u010 = cp[2]; u110 = cp[3];
+    v000 = cp[4]; v100 = cp[5]; v010 = cp[6]; v110 = cp[7];
+    w000 = cp[8]; w100 = cp[9]; w010 = cp[10]; w110 = cp[11];
+  } else {
+    u000 = LA(xvel0, j, k, l); u100 = LA(xvel0, j + 1, k, l);
+    u010 = LA(xvel0, j, k + 1, l); u110 = LA(xvel0, j + 1, k + 1, l);
+    v000 = LA(yvel0, j, k, l); v100 = LA(yvel0, j + 1, k, l);
+    v010 = LA(yvel0, j, k + 1, l); v110 = LA(yvel0, j + 1, k + 1, l);
+    w000 = LA(zvel0, j, k, l); w100 = LA(zvel0, j + 1, k, l);
+    w010 = LA(zvel0, j, k + 1, l); w110 = LA(zvel0, j + 1, k + 1, l);
+  }
   const A u001 = LA(xvel0, j, k, l + 1), u101 = LA(xvel0, j + 1, k, l + 1);
   const A u011 = LA(xvel0, j, k + 1, l + 1), u111 = LA(xvel0, j + 1, k + 1, l + 1);
-  const A v000 = LA(yvel0, j, k, l), v100 = LA(yvel0, j + 1, k, l);
-  const A v010 = LA(yvel0, j, k + 1, l), v110 = LA(yvel0, j + 1, k + 1, l);
   const A v001 = LA(yvel0, j, k, l + 1), v101 = LA(yvel0, j + 1, k, l + 1);
   const A v011 = LA(yvel0, j, k + 1, l + 1), v111 = LA(yvel0, j + 1, k + 1, l + 1);
-  const A w000 = LA(zvel0, j, k, l), w100 = LA(zvel0, j + 1, k, l);
-  const A w010 = LA(zvel0, j, k + 1, l), w110 = LA(zvel0, j + 1, k + 1, l);
   const A w001 = LA(zvel0, j, k, l + 1), w101 = LA(zvel0, j + 1, k, l + 1);
   const A w011 = LA(zvel0, j, k + 1, l + 1), w111 = LA(zvel0, j + 1, k + 1, l + 1);
+  cp[0] = u001; cp[1] = u101; cp[2] = u011; cp[3] = u111;
+  cp[4] = v001; cp[5] = v101; cp[6] = v011; cp[7] = v111;
+  cp[8] = w001; cp[9] = w101; cp[10] = w011; cp[11] = w111;
+  carried = true;
 
   const A ugradx1 = u000 + u010 + u001 + u011;
   const A ugradx2 = u100 + u110 + u101 + u111;
