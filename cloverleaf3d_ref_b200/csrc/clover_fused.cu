@@ -144,7 +144,7 @@ __device__ __forceinline__ A lda(const float* p) { return (A)__ldg(p); }
 // limiter > 0 -> 0, else ..." (the same outcome). The cell minimum folds into
 // deck d's key at min_key[d * kScalarStride] (warp, block, one atomic).
 template <class S, class M>
-__global__ void __launch_bounds__(BX * BY, sizeof(typename S::arith_t) == 4 && !M::kFlat ? 4 : 3) k_visc_dt(M m, GeomArrays ga, double g_small,
+__global__ void __launch_bounds__(BX * BY, sizeof(typename S::arith_t) == 4 || M::kFlat ? 4 : 3) k_visc_dt(M m, GeomArrays ga, double g_small,
     double dtc_safe, double dtu_safe, double dtv_safe, double dtw_safe, double dtdiv_safe,
     const typename S::rho_t* __restrict__ density0, const typename S::cs_t* __restrict__ pressure,
     typename S::cs_t* __restrict__ viscosity, const typename S::cs_t* __restrict__ soundspeed,
@@ -308,7 +308,7 @@ __global__ void __launch_bounds__(BX * BY, sizeof(typename S::arith_t) == 4 && !
 // the predicted density1/energy1; the pressure is stored in place (each
 // thread reads and writes only its own cell).
 template <class S, class M>
-__global__ void __launch_bounds__(BX * BY, M::kFlat ? 1 : 8) k_pdv_predict_eos(M m, const double* dt_ptr,
+__global__ void __launch_bounds__(BX * BY, M::kFlat ? 6 : 8) k_pdv_predict_eos(M m, const double* dt_ptr,
     GeomArrays ga, const typename S::rho_t* __restrict__ density0,
     const typename S::ene_t* __restrict__ energy0, typename S::cs_t* __restrict__ pressure,
     const typename S::cs_t* __restrict__ viscosity, const typename S::vel_t* __restrict__ xvel0,
@@ -495,7 +495,7 @@ __device__ __forceinline__ double cell_limiter(double sig, double sigma3, double
 // fluxes of face c and update cell c from faces c and c+1 into the output
 // arrays, so no thread reads a value another one writes.
 template <class S, int VAR, class M>
-__global__ void __launch_bounds__(BX * BY, M::kFlat ? 1 : 5) k_cell_sweep_x(M m, GeomArrays ga,
+__global__ void __launch_bounds__(BX * BY, M::kFlat ? 4 : 5) k_cell_sweep_x(M m, GeomArrays ga,
     const typename S::rho_t* __restrict__ d_in, const typename S::ene_t* __restrict__ e_in,
     typename S::rho_t* __restrict__ d_out, typename S::ene_t* __restrict__ e_out,
     const typename S::vf_t* __restrict__ vfx, const typename S::vf_t* __restrict__ vfy,
@@ -649,7 +649,7 @@ __device__ __forceinline__ double cell_product(const Geom& g, int variant, const
 // DIR 2: p = k, c = l; DIR 3: p = l, c = k. Sums keep the reference order
 // (advec_mom_kernel.f90:166-190 and the y/z forms).
 template <class S, int DIR, int VAR, class M>
-__global__ void __launch_bounds__(BX * BY, M::kFlat ? 4 : 6) k_mom_node_march(M m, GeomArrays ga,
+__global__ void __launch_bounds__(BX * BY, M::kFlat ? 5 : 6) k_mom_node_march(M m, GeomArrays ga,
     const typename S::mf_t* __restrict__ mf, const typename S::rho_t* __restrict__ density1,
     const typename S::vf_t* __restrict__ vfx, const typename S::vf_t* __restrict__ vfy,
     const typename S::vf_t* __restrict__ vfz, typename S::nd_t* __restrict__ node_flux,
@@ -1005,7 +1005,7 @@ __global__ void __launch_bounds__(BX * BY, 3) k_cell_sweep_march(M m, GeomArrays
 // and the momentum limiter keep the reference order
 // (advec_mom_kernel.f90:166-252).
 template <class S, int VAR, class M>
-__global__ void __launch_bounds__(BX * BY, M::kFlat ? 3 : 4) k_mom_sweep_x(M m,
+__global__ void __launch_bounds__(BX * BY, 4) k_mom_sweep_x(M m,
     GeomArrays ga, const typename S::mf_t* __restrict__ mfx,
     const typename S::rho_t* __restrict__ density1, const typename S::vf_t* __restrict__ vfx,
     const typename S::vf_t* __restrict__ vfy, const typename S::vf_t* __restrict__ vfz,
