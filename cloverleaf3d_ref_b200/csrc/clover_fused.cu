@@ -29,6 +29,7 @@
 //                    velocity pass, each marching along the sweep axis with the
 //                    previous node's values in registers.
 //  Updated velocities go to the other buffer of each velocity pair.
+#include <cfloat>
 #include <type_traits>
 
 #include "clover_launch.h"
@@ -134,6 +135,12 @@ template <class A>
 __device__ __forceinline__ A lda(const double* p) { return (A)__ldg(p); }
 template <class A>
 __device__ __forceinline__ A lda(const float* p) { return (A)__ldg(p); }
+
+// The per-chunk quotients of Geom in the arithmetic type A.
+template <class A>
+__device__ __forceinline__ A geo_rvol(const Geom& g) { return sizeof(A) == 4 ? (A)g.rvol_f : (A)g.rvol; }
+template <class A>
+__device__ __forceinline__ A geo_ds(const Geom& g) { return sizeof(A) == 4 ? (A)g.ds_f : (A)g.ds; }
 
 // ---------------------------------------------------------------------------
 // viscosity_kernel.f90:71-134 followed by calc_dt_kernel.f90:102-149 on the
@@ -254,8 +261,8 @@ __global__ void __launch_bounds__(BX * BY, sizeof(typename S::arith_t) == 4 || M
   // calc_dt_kernel.f90:102-149 (the viscosity as stored)
   const A visc = (A)st<C>((double)q);
   const A d0 = LA(density0, j, k, l);
-  const A mcd = fmin2(fmin2(AG(GX, ga.celldx, j), AG(GY, ga.celldy, k)), AG(GZ, ga.celldz, l));
-  const A ds = A(1.0) / (mcd * mcd);
+  // 1/min(celldx, celldy, celldz)^2 of the chunk's uniform mesh
+  const A ds = geo_ds<A>(g);
   const A ss = LA(soundspeed, j, k, l);
   A cc = ss * ss;
   cc = cc + A(2.0) * visc / d0;
@@ -353,7 +360,7 @@ __global__ void __launch_bounds__(BX * BY, M::kFlat ? 6 : 8) k_pdv_predict_eos(M
   const A total_flux = right_flux - left_flux + top_flux - bottom_flux + front_flux - back_flux;
   const A vol = (A)g.vol;
   const A vol_change_s = vol / (vol + total_flux);
-  const A recip_volume = A(1.0) / vol;
+  const A recip_volume = geo_rvol<A>(g);  // 1/volume
   const A d0 = LA(density0, j, k, l);
   const A energy_change =
       (LA(pressure, j, k, l) / d0 + LA(viscosity, j, k, l) / d0) * total_flux * recip_volume;
@@ -440,7 +447,7 @@ __global__ void __launch_bounds__(BX * BY, M::kFlat ? 5 : 8) k_pdv_flux(M m, con
   const double total_flux = right_flux - left_flux + top_flux - bottom_flux + front_flux - back_flux;
   const double vol = g.vol;
   const double vol_change_s = vol / (vol + total_flux);
-  const double recip_volume = 1.0 / vol;
+  const double recip_volume = g.rvol;  // 1/volume
   const double d0 = L(density0, j, k, l);
   const double energy_change =
       (L(pressure, j, k, l) / d0 + L(viscosity, j, k, l) / d0) * total_flux * recip_volume;
@@ -475,6 +482,12 @@ __device__ __forceinline__ double cell_pre_vol(const Geom& g, int variant, const
     default:
       return vol + L(vfz, j, k, l + 1) - L(vfz, j, k, l);
   }
+}
+
+// vertexd(j) / vertexd(dif) of the limiter: exactly 1 where the two widths
+// are equal (every face of a uniform mesh), without the division
+__device__ __forceinline__ double width_ratio(double a, double b) {
+  return (a == b && a != 0.0 && fabs(a) <= DBL_MAX) ? 1.0 : a / b;
 }
 
 __device__ __forceinline__ double cell_limiter(double sig, double sigma3, double sigma4,
@@ -539,7 +552,7 @@ __global__ void __launch_bounds__(BX * BY, M::kFlat ? 4 : 5) k_cell_sweep_x(M m,
       pv_don = pv; vd_dif = clamp ? vd : vd_p1;
     }
     const double sigmat = fabs(vf) / pv_don;
-    const double sigma3 = (1.0 + sigmat) * (vd / vd_dif);
+    const double sigma3 = (1.0 + sigmat) * width_ratio(vd, vd_dif);
     const double sigma4 = 2.0 - sigmat;
     double diffuw = d_don - d_up;
     double diffdw = d_dn - d_don;
@@ -961,7 +974,7 @@ __global__ void __launch_bounds__(BX * BY, 3) k_cell_sweep_march(M m, GeomArrays
       dif = p + 1 < top ? p + 1 : top;
     }
     const double sigmat = fabs(vf) / pv_don;
-    const double sigma3 = (1.0 + sigmat) * (VD(p) / VD(dif));
+    const double sigma3 = (1.0 + sigmat) * width_ratio(VD(p), VD(dif));
     const double sigma4 = 2.0 - sigmat;
     double diffuw = d_don - d_up;
     double diffdw = d_dn - d_don;

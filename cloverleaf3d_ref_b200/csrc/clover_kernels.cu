@@ -362,7 +362,7 @@ __global__ void __launch_bounds__(BX * BY) k_revert(Geom g, Box b,
 // the chunk's uniform-mesh constants (Geom::vol, xa, ya, za) instead of the
 // arrays.
 template <class S, class M, bool UM>
-__global__ void __launch_bounds__(BX * BY) k_accelerate(M m, double dt_val,
+__global__ void __launch_bounds__(BX * BY, UM ? 5 : 4) k_accelerate(M m, double dt_val,
     const double* dt_ptr, GeomArrays ga, const typename S::rho_t* __restrict__ density0,
     const typename S::cs_t* __restrict__ pressure, const typename S::cs_t* __restrict__ viscosity,
     const typename S::vel_t* __restrict__ xvel0, const typename S::vel_t* __restrict__ yvel0,

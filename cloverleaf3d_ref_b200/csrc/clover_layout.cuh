@@ -33,6 +33,12 @@ struct Geom {
   // kernels read them here instead of streaming four 3D arrays; the drop-in
   // kernels, whose callers own the arrays, read the arrays.
   double vol, xa, ya, za;
+  // Per-chunk quotients of those constants, formed on the host in the
+  // precision the kernels use them in (IEEE division either side): 1/volume
+  // (PdV_kernel.f90:105) and calc_dt's ds = 1/min(dx,dy,dz)^2
+  // (calc_dt_kernel.f90:112), in FP64 and FP32.
+  double rvol, ds;
+  float rvol_f, ds_f;
 };
 
 // Elements per 128 bytes for a storage type.
@@ -54,6 +60,8 @@ inline Geom make_geom(int x_min, int x_max, int y_min, int y_max, int z_min, int
   g.o1 = 0;
   g.o3 = 0;
   g.vol = g.xa = g.ya = g.za = 0.0;
+  g.rvol = g.ds = 0.0;
+  g.rvol_f = g.ds_f = 0.0f;
   return g;
 }
 

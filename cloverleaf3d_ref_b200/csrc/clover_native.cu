@@ -266,6 +266,14 @@ struct Chunk : ChunkBase {
       q.xa = dy * dz;
       q.ya = dx * dz;
       q.za = dx * dy;
+      // the kernels' min(celldx, celldy, celldz) takes b when b < a
+      auto mn = [](auto a, auto b) { return b < a ? b : a; };
+      const double mcd = mn(mn(dx, dy), dz);
+      const float mcd_f = mn(mn((float)dx, (float)dy), (float)dz);
+      q.rvol = 1.0 / q.vol;
+      q.rvol_f = 1.0f / (float)q.vol;
+      q.ds = 1.0 / (mcd * mcd);
+      q.ds_f = 1.0f / (mcd_f * mcd_f);
       q.o3 = total3;
       q.o1 = (int)total1;
       total3 += array_elems(q);
