@@ -512,7 +512,8 @@ __global__ void __launch_bounds__(BX * BY, M::kFlat ? 4 : 5) k_cell_sweep_x(M m,
     const typename S::rho_t* __restrict__ d_in, const typename S::ene_t* __restrict__ e_in,
     typename S::rho_t* __restrict__ d_out, typename S::ene_t* __restrict__ e_out,
     const typename S::vf_t* __restrict__ vfx, const typename S::vf_t* __restrict__ vfy,
-    const typename S::vf_t* __restrict__ vfz, typename S::mf_t* __restrict__ mass_flux) {
+    const typename S::vf_t* __restrict__ vfz, typename S::mf_t* __restrict__ mass_flux,
+    Level0<S> lz) {
   m.run([&](const Geom& g, const Tile& t) {
   const int lane = threadIdx.x;
   const int c = g.x_min - 2 + t.x * 28 + lane;
@@ -577,8 +578,14 @@ __global__ void __launch_bounds__(BX * BY, M::kFlat ? 4 : 5) k_cell_sweep_x(M m,
     const double pom = pm + mf_st - mf_p;
     const double poe = (e * pm + ef - ef_p) / pom;
     const double av = pv + vf - vf_p;
-    E(d_out, c, k, l) = st<typename S::rho_t>(pom / av);
-    E(e_out, c, k, l) = st<typename S::ene_t>(poe);
+    const typename S::rho_t dn = st<typename S::rho_t>(pom / av);
+    const typename S::ene_t en = st<typename S::ene_t>(poe);
+    E(d_out, c, k, l) = dn;
+    E(e_out, c, k, l) = en;
+    if (lz.density0) {  // last sweep of the step: reset_field
+      E(lz.density0, c, k, l) = dn;
+      E(lz.energy0, c, k, l) = en;
+    }
   }
   });
 }
@@ -807,7 +814,7 @@ __global__ void __launch_bounds__(BX * BY, 3) k_mom_vel3_march(M m, GeomArrays g
     const typename S::nd_t* __restrict__ node_mass_pre, const typename S::vel_t* __restrict__ u_in,
     const typename S::vel_t* __restrict__ v_in, const typename S::vel_t* __restrict__ w_in,
     typename S::vel_t* __restrict__ u_out, typename S::vel_t* __restrict__ v_out,
-    typename S::vel_t* __restrict__ w_out) {
+    typename S::vel_t* __restrict__ w_out, Level0<S> lz) {
   m.run([&](const Geom& g, const Tile& t) {
   const MarchRange r = mom_vel_range<DIR>(g);
   const int jlo = r.jlo, jhi = r.jhi, clo = r.clo, chi = r.chi, plo = r.plo, phi = r.phi;
@@ -826,6 +833,7 @@ __global__ void __launch_bounds__(BX * BY, 3) k_mom_vel3_march(M m, GeomArrays g
 #define LA(a, idx) lda<A>(&EI_(a, idx))
   const typename S::vel_t* in[3] = {u_in, v_in, w_in};
   typename S::vel_t* out[3] = {u_out, v_out, w_out};
+  typename S::vel_t* lev0[3] = {lz.xvel0, lz.yvel0, lz.zvel0};
   // window at node p: v(p-2), v(p-1), v(p), v(p+1) ; loaded v(p+2) each step
   A vw[3][4];
   A mf_prev[3];
@@ -858,7 +866,9 @@ __global__ void __launch_bounds__(BX * BY, 3) k_mom_vel3_march(M m, GeomArrays g
     for (int q = 0; q < 3; q++) {
       const A vp2 = vn[q];
       const A mf_0 = mom_flux_v<A>(nt, vw[q][1], vw[q][2], vw[q][3], vp2);
-      EI(out[q], IDX(p)) = st<V>((vw[q][2] * pre_0 + mf_prev[q] - mf_0) / post_0);
+      const V vn1 = st<V>((vw[q][2] * pre_0 + mf_prev[q] - mf_0) / post_0);
+      EI(out[q], IDX(p)) = vn1;
+      if (lz.xvel0) EI(lev0[q], IDX(p)) = vn1;  // last sweep of the step: reset_field
       mf_prev[q] = mf_0;
       vw[q][0] = vw[q][1];
       vw[q][1] = vw[q][2];
@@ -890,7 +900,8 @@ template <class S, int DIR, int VAR, class M>
 __global__ void __launch_bounds__(BX * BY, 3) k_cell_sweep_march(M m, GeomArrays ga,
     typename S::rho_t* __restrict__ density1, typename S::ene_t* __restrict__ energy1,
     const typename S::vf_t* __restrict__ vfx, const typename S::vf_t* __restrict__ vfy,
-    const typename S::vf_t* __restrict__ vfz, typename S::mf_t* __restrict__ mass_flux) {
+    const typename S::vf_t* __restrict__ vfz, typename S::mf_t* __restrict__ mass_flux,
+    Level0<S> lz) {
   // old density/energy of cells c1+1, c1+2 of each thread's segment
   __shared__ double s_end[4][BY][BX];
   m.run([&](const Geom& g, const Tile& t) {
@@ -993,8 +1004,14 @@ __global__ void __launch_bounds__(BX * BY, 3) k_cell_sweep_march(M m, GeomArrays
       const double pom = pm + mf_prev - mf_stored;
       const double poe = (e1 * pm + ef_prev - eflux) / pom;
       const double av = pv_m + vf_prev - vf;
-      EI(density1, IDX(p - 1)) = st<R>(pom / av);
-      EI(energy1, IDX(p - 1)) = st<En>(poe);
+      const R dn = st<R>(pom / av);
+      const En en = st<En>(poe);
+      EI(density1, IDX(p - 1)) = dn;
+      EI(energy1, IDX(p - 1)) = en;
+      if (lz.density0) {  // last sweep of the step: reset_field
+        EI(lz.density0, IDX(p - 1)) = dn;
+        EI(lz.energy0, IDX(p - 1)) = en;
+      }
     }
     vf_prev = vf;
     mf_prev = mf_stored;
@@ -1024,7 +1041,8 @@ __global__ void __launch_bounds__(BX * BY, 4) k_mom_sweep_x(M m,
     const typename S::vf_t* __restrict__ vfy, const typename S::vf_t* __restrict__ vfz,
     const typename S::vel_t* __restrict__ u_in, const typename S::vel_t* __restrict__ v_in,
     const typename S::vel_t* __restrict__ w_in, typename S::vel_t* __restrict__ u_out,
-    typename S::vel_t* __restrict__ v_out, typename S::vel_t* __restrict__ w_out) {
+    typename S::vel_t* __restrict__ v_out, typename S::vel_t* __restrict__ w_out,
+    Level0<S> lz) {
   m.run([&](const Geom& g, const Tile& t) {
   const int seg = m.seg;
   const int lane = threadIdx.x;
@@ -1043,6 +1061,7 @@ __global__ void __launch_bounds__(BX * BY, 4) k_mom_sweep_x(M m,
   using V = typename S::vel_t;
   const typename S::vel_t* in[3] = {u_in, v_in, w_in};
   typename S::vel_t* out[3] = {u_out, v_out, w_out};
+  typename S::vel_t* lev0[3] = {lz.xvel0, lz.yvel0, lz.zvel0};
   const double cd_0 = has_nf ? GX(ga.celldx, j) : 1.0;
   const double cd_m1 = has_mf ? GX(ga.celldx, j - 1) : 1.0;
   const double cd_p1 = has_mf ? GX(ga.celldx, j + 1) : 1.0;
@@ -1084,7 +1103,11 @@ __global__ void __launch_bounds__(BX * BY, 4) k_mom_sweep_x(M m,
         mf = mom_flux_v<A>(nt, vm1, v0, vp1, vp2);
       }
       const A mf_m = __shfl_up_sync(0xffffffffu, mf, 1);
-      if (has_up) E(out[q], j, k, l) = st<V>((v0 * (A)nmpre + mf_m - mf) / (A)nmp);
+      if (has_up) {
+        const V vn1 = st<V>((v0 * (A)nmpre + mf_m - mf) / (A)nmp);
+        E(out[q], j, k, l) = vn1;
+        if (lz.xvel0) E(lev0[q], j, k, l) = vn1;  // last sweep of the step: reset_field
+      }
     }
     fm_a = f_a; fm_b = f_b; fm_c = f_c; fm_d = f_d;
     pm_a = p_a; pm_b = p_b;
@@ -1271,7 +1294,8 @@ void launch_advec_cell_fused(const Target& tg, cudaStream_t s, int advect_x, int
                              typename S::ene_t* energy1, typename S::mf_t* mass_flux_x,
                              const typename S::vf_t* vol_flux_x, typename S::mf_t* mass_flux_y,
                              const typename S::vf_t* vol_flux_y, typename S::mf_t* mass_flux_z,
-                             const typename S::vf_t* vol_flux_z, typename S::wk_t* ener_flux) {
+                             const typename S::vf_t* vol_flux_z, typename S::wk_t* ener_flux,
+                             const Level0<S>& level0) {
   (void)ener_flux;
   // pre_vol variant (the sweep's volume-flux terms) as a kernel template
   // argument: y is sweep 2 (2: after x, 3: after z); z is sweep 1 (4) or 3 (5)
@@ -1281,14 +1305,14 @@ void launch_advec_cell_fused(const Target& tg, cudaStream_t s, int advect_x, int
     launch_mapped2(tg, s, kKeyCellSweep | 2u | (V << 4), grid_cell_sweep<2>,
                    grid_cell_sweep_flat<2>, 0, false, kBlk,
                    k_cell_sweep_march<S, 2, V, MapSingle>, k_cell_sweep_march<S, 2, V, MapBatch>,
-                   ga, density1, energy1, vol_flux_x, vol_flux_y, vol_flux_z, mass_flux_y);
+                   ga, density1, energy1, vol_flux_x, vol_flux_y, vol_flux_z, mass_flux_y, level0);
   };
   auto sweep_z = [&](auto var) {
     constexpr int V = decltype(var)::value;
     launch_mapped2(tg, s, kKeyCellSweep | 3u | (V << 4), grid_cell_sweep<3>,
                    grid_cell_sweep_flat<3>, 0, false, kBlk,
                    k_cell_sweep_march<S, 3, V, MapSingle>, k_cell_sweep_march<S, 3, V, MapBatch>,
-                   ga, density1, energy1, vol_flux_x, vol_flux_y, vol_flux_z, mass_flux_z);
+                   ga, density1, energy1, vol_flux_x, vol_flux_y, vol_flux_z, mass_flux_z, level0);
   };
   // one marching pass, in place
   if (dir == 2) {
@@ -1306,18 +1330,18 @@ void launch_advec_cell_x(const Target& tg, cudaStream_t s, int sweep, const Geom
                          typename S::rho_t* density1_out, typename S::ene_t* energy1_out,
                          const typename S::vf_t* vol_flux_x, const typename S::vf_t* vol_flux_y,
                          const typename S::vf_t* vol_flux_z, typename S::mf_t* mass_flux_x,
-                         bool copy_shell) {
+                         bool copy_shell, const Level0<S>& level0) {
   // pre_vol variant: 0 on sweep 1 (all three flux differences), 1 on sweep 3
   if (sweep == 1)
     launch_mapped(tg, s, kKeyCellSweepX, grid_cell_sweep_x, 0, false, kBlk,
                   k_cell_sweep_x<S, 0, MapSingle>, k_cell_sweep_x<S, 0, MapBatchFree>, ga,
                   density1_in, energy1_in, density1_out, energy1_out, vol_flux_x, vol_flux_y,
-                  vol_flux_z, mass_flux_x);
+                  vol_flux_z, mass_flux_x, level0);
   else
     launch_mapped(tg, s, kKeyCellSweepX | (1u << 4), grid_cell_sweep_x, 0, false, kBlk,
                   k_cell_sweep_x<S, 1, MapSingle>, k_cell_sweep_x<S, 1, MapBatchFree>, ga,
                   density1_in, energy1_in, density1_out, energy1_out, vol_flux_x, vol_flux_y,
-                  vol_flux_z, mass_flux_x);
+                  vol_flux_z, mass_flux_x, level0);
   // the cells the sweep does not update keep their values in the output pair
   if (copy_shell) {
     using R = typename S::rho_t;
@@ -1336,7 +1360,8 @@ void launch_advec_mom_fused(const Target& tg, cudaStream_t s, int advect_x, int 
                             const typename S::vf_t* vol_flux_y, const typename S::vf_t* vol_flux_z,
                             typename S::wk_t* node_flux, typename S::wk_t* node_mass_post,
                             typename S::wk_t* node_mass_pre, typename S::vel_t* const* vel_in,
-                            typename S::vel_t* const* vel_out, bool copy_shell) {
+                            typename S::vel_t* const* vel_out, bool copy_shell,
+                            const Level0<S>& level0) {
   // the node arrays of the y/z sweeps live in three work arrays, as nd_t
   using ND = typename S::nd_t;
   static_assert(sizeof(ND) <= sizeof(typename S::wk_t), "node arrays fit the work arrays");
@@ -1356,7 +1381,7 @@ void launch_advec_mom_fused(const Target& tg, cudaStream_t s, int advect_x, int 
     launch_mapped2(tg, s, kKeyMomVel3 | D, grid_mom_vel<D>, grid_mom_vel_flat<D>, kMarchSeg,
                    true, kBlk, k_mom_vel3_march<S, D, MapSingle>, k_mom_vel3_march<S, D, MapBatchFree>,
                    ga, nd_flux, nd_post, nd_pre, vel_in[0], vel_in[1], vel_in[2], vel_out[0],
-                   vel_out[1], vel_out[2]);
+                   vel_out[1], vel_out[2], level0);
   };
   using I2 = std::integral_constant<int, 2>;
   using I3 = std::integral_constant<int, 3>;
@@ -1367,7 +1392,7 @@ void launch_advec_mom_fused(const Target& tg, cudaStream_t s, int advect_x, int 
       launch_mapped(tg, s, kKeyMomSweepX | (V << 4), grid_mom_sweep_x, kMarchSeg, true, kBlk,
                     k_mom_sweep_x<S, V, MapSingle>, k_mom_sweep_x<S, V, MapBatchFree>, ga,
                     mass_flux_x, density1, vol_flux_x, vol_flux_y, vol_flux_z, vel_in[0],
-                    vel_in[1], vel_in[2], vel_out[0], vel_out[1], vel_out[2]);
+                    vel_in[1], vel_in[2], vel_out[0], vel_out[1], vel_out[2], level0);
     };
     if (sweep == 1) sweep_x(std::integral_constant<int, 0>{});
     else sweep_x(std::integral_constant<int, 4>{});
@@ -1408,16 +1433,17 @@ void launch_advec_mom_fused(const Target& tg, cudaStream_t s, int advect_x, int 
   template void launch_advec_cell_fused<S>(const Target&, cudaStream_t, int, int, int,           \
                                            const GeomArrays&, S::rho_t*, S::ene_t*, S::mf_t*,  \
                                            const S::vf_t*, S::mf_t*, const S::vf_t*, S::mf_t*, \
-                                           const S::vf_t*, S::wk_t*);                          \
+                                           const S::vf_t*, S::wk_t*, const Level0<S>&);        \
   template void launch_advec_cell_x<S>(const Target&, cudaStream_t, int, const GeomArrays&,      \
                                        const S::rho_t*, const S::ene_t*, S::rho_t*, S::ene_t*,  \
                                        const S::vf_t*, const S::vf_t*, const S::vf_t*,          \
-                                       S::mf_t*, bool);                                         \
+                                       S::mf_t*, bool, const Level0<S>&);                       \
   template void launch_advec_mom_fused<S>(const Target&, cudaStream_t, int, int, int, double,    \
                                           const GeomArrays&, const S::rho_t*, const S::mf_t*,  \
                                           const S::mf_t*, const S::mf_t*, const S::vf_t*,      \
                                           const S::vf_t*, const S::vf_t*, S::wk_t*, S::wk_t*,  \
-                                          S::wk_t*, S::vel_t* const*, S::vel_t* const*, bool);
+                                          S::wk_t*, S::vel_t* const*, S::vel_t* const*, bool,  \
+                                          const Level0<S>&);
 
 INSTF(F64)
 INSTF(F32Mixed)

@@ -148,6 +148,19 @@ struct F32Mixed {
   using arith_t = float;  // momentum flux and update, accelerate (node and cell masses stay FP64)
 };
 
+// The time level 0 arrays, which the step's last sweep also writes: the final
+// density1/energy1 of every interior cell and vel1 of every node in
+// [min, max+1]^3, i.e. reset_field_kernel.f90:51-98 folded into the kernels
+// that produce those values. All null in the other sweeps.
+template <class S>
+struct Level0 {
+  typename S::rho_t* density0;
+  typename S::ene_t* energy0;
+  typename S::vel_t* xvel0;
+  typename S::vel_t* yvel0;
+  typename S::vel_t* zvel0;
+};
+
 // Geometry arrays (always FP64).
 struct GeomArrays {
   const double *volume, *xarea, *yarea, *zarea;
@@ -341,7 +354,8 @@ void launch_advec_cell_fused(const Target& tg, cudaStream_t s, int advect_x, int
                              typename S::ene_t* energy1, typename S::mf_t* mass_flux_x,
                              const typename S::vf_t* vol_flux_x, typename S::mf_t* mass_flux_y,
                              const typename S::vf_t* vol_flux_y, typename S::mf_t* mass_flux_z,
-                             const typename S::vf_t* vol_flux_z, typename S::wk_t* ener_flux);
+                             const typename S::vf_t* vol_flux_z, typename S::wk_t* ener_flux,
+                             const Level0<S>& level0);
 // The x cell sweep out of place: density1/energy1 in one buffer pair, the
 // updated values in the other, and with copy_shell a copy of every cell
 // outside the interior (left out where a depth-2 halo update of density1 and
@@ -352,7 +366,7 @@ void launch_advec_cell_x(const Target& tg, cudaStream_t s, int sweep, const Geom
                          typename S::rho_t* density1_out, typename S::ene_t* energy1_out,
                          const typename S::vf_t* vol_flux_x, const typename S::vf_t* vol_flux_y,
                          const typename S::vf_t* vol_flux_z, typename S::mf_t* mass_flux_x,
-                         bool copy_shell);
+                         bool copy_shell, const Level0<S>& level0);
 // All three velocities of one sweep; vel_in/vel_out are the two buffers of
 // each velocity pair, and with copy_shell the shell outside [min,max+1]^3 is
 // copied across (left out where a depth-2 halo update of the velocities
@@ -366,7 +380,8 @@ void launch_advec_mom_fused(const Target& tg, cudaStream_t s, int advect_x, int 
                             const typename S::vf_t* vol_flux_y, const typename S::vf_t* vol_flux_z,
                             typename S::wk_t* node_flux, typename S::wk_t* node_mass_post,
                             typename S::wk_t* node_mass_pre, typename S::vel_t* const* vel_in,
-                            typename S::vel_t* const* vel_out, bool copy_shell);
+                            typename S::vel_t* const* vel_out, bool copy_shell,
+                            const Level0<S>& level0);
 
 // Fill every element of an array (size elems after the pad) with a value.
 template <class T>

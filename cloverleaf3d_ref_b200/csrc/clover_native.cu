@@ -762,9 +762,15 @@ struct Chunk : ChunkBase {
                        viscosity, xvel0, vel1(0, vc), yvel0, vel1(1, vc), zvel0, vel1(2, vc),
                        vol_flux_x, vol_flux_y, vol_flux_z);
     pend("pdv_flux", n * (2 * R8 + 2 * E8 + 2 * C8 + 6 * V8 + 3 * VF8));
-    // advection.f90:43-179
+    // advection.f90:43-179. The last sweep also writes time level 0 (the
+    // interior density/energy and node velocities reset_field copies), so
+    // reset_field needs no pass of its own.
     const int axi = ax ? 1 : 0;
+    const Level0<S> no_level0{nullptr, nullptr, nullptr, nullptr, nullptr};
+    const Level0<S> level0{density0, energy0, xvel0, yvel0, zvel0};
     auto sweep = [&](int sweep_number, int dir, bool pre_halo) {
+      const Level0<S>& l0 = sweep_number == 3 ? level0 : no_level0;
+      const double nl0 = sweep_number == 3 ? 1 : 0;  // level 0 written by this sweep
       if (pre_halo) {
         pbeg();
         // before sweep 2, density1 and energy1 (updated after sweep 1) and
@@ -782,15 +788,15 @@ struct Chunk : ChunkBase {
         // the post-sweep depth-2 halo update rewrites the output pair's shell
         launch_advec_cell_x<S>(tg, stream, sweep_number, ga, rho1(cb), ene1(cb), rho1(cb ^ 1),
                                ene1(cb ^ 1), vol_flux_x, vol_flux_y, vol_flux_z, mass_flux_x,
-                               !halo_repeat_free);
+                               !halo_repeat_free, l0);
         cb ^= 1;
-        pend("advec_cell_x", n * (nvf * VF8 + 2 * R8 + 2 * E8 + MF8));
+        pend("advec_cell_x", n * (nvf * VF8 + (2 + nl0) * (R8 + E8) + MF8));
       } else {
         // one marching pass, in place
         launch_advec_cell_fused<S>(tg, stream, axi, dir, sweep_number, ga, rho1(cb), ene1(cb),
                                    mass_flux_x, vol_flux_x, mass_flux_y, vol_flux_y,
-                                   mass_flux_z, vol_flux_z, work[6]);
-        pend("advec_cell_yz", n * (nvf * VF8 + 2 * R8 + 2 * E8 + MF8));
+                                   mass_flux_z, vol_flux_z, work[6], l0);
+        pend("advec_cell_yz", n * (nvf * VF8 + (2 + nl0) * (R8 + E8) + MF8));
       }
       pbeg();
       // mass_flux_z changes only in the z sweep and is updated right after it
@@ -808,21 +814,18 @@ struct Chunk : ChunkBase {
       launch_advec_mom_fused<S>(tg, stream, axi, sweep_number, dir, cell_volume, ga, rho1(cb),
                                 mass_flux_x, mass_flux_y, mass_flux_z, vol_flux_x, vol_flux_y,
                                 vol_flux_z, work[0], work[1], work[2], vin, vout,
-                                sweep_number == 3 || !halo_repeat_free);
+                                sweep_number == 3 || !halo_repeat_free, l0);
       // x: one pass; y, z: node pass + velocity pass
       if (dir == 1)
-        pend("advec_mom_x", n * (MF8 + R8 + npv * VF8 + 6 * V8));
+        pend("advec_mom_x", n * (MF8 + R8 + npv * VF8 + (6 + 3 * nl0) * V8));
       else  // node pass + velocity pass
-        pend("advec_mom_yz", n * ((MF8 + R8 + npv * VF8 + 3 * N8) + (3 * N8 + 6 * V8)));
+        pend("advec_mom_yz",
+             n * ((MF8 + R8 + npv * VF8 + 3 * N8) + (3 * N8 + (6 + 3 * nl0) * V8)));
       vc ^= 1;
     };
     sweep(1, ax ? 1 : 3, true);
     sweep(2, 2, true);
     sweep(3, ax ? 3 : 1, false);
-    pbeg();
-    launch_reset_field<S>(tg, stream, density0, rho1(cb), energy0, ene1(cb), xvel0, vel1(0, vc),
-                          yvel0, vel1(1, vc), zvel0, vel1(2, vc));
-    pend("reset_field", n * (2 * R8 + 2 * E8 + 6 * V8));
     k_step_end<<<deck_blocks(), 128, 0, stream>>>(sc, nd);
   }
 
