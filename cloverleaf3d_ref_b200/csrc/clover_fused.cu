@@ -153,8 +153,9 @@ __device__ __forceinline__ A geo_ds(const Geom& g) { return sizeof(A) == 4 ? (A)
 template <class S, class M>
 __global__ void __launch_bounds__(BX * BY, sizeof(typename S::arith_t) == 4 || M::kFlat ? 4 : 3) k_visc_dt(M m, GeomArrays ga, double g_small,
     double dtc_safe, double dtu_safe, double dtv_safe, double dtw_safe, double dtdiv_safe,
-    const typename S::rho_t* __restrict__ density0, const typename S::cs_t* __restrict__ pressure,
-    typename S::cs_t* __restrict__ viscosity, const typename S::cs_t* __restrict__ soundspeed,
+    const typename S::rho_t* __restrict__ density0, const typename S::ene_t* __restrict__ energy0,
+    typename S::cs_t* __restrict__ pressure, typename S::cs_t* __restrict__ viscosity,
+    typename S::cs_t* __restrict__ soundspeed,
     const typename S::vel_t* __restrict__ xvel0, const typename S::vel_t* __restrict__ yvel0,
     const typename S::vel_t* __restrict__ zvel0, unsigned long long* __restrict__ min_key) {
   __shared__ unsigned long long wmin[BX * BY / 32];
@@ -234,9 +235,15 @@ __global__ void __launch_bounds__(BX * BY, sizeof(typename S::arith_t) == 4 || M
     const A xy = A(0.25) * (ugrady2 - ugrady1) / cdy + A(0.25) * (vgradx2 - vgradx1) / cdx;
     const A xz = A(0.25) * (ugradz2 - ugradz1) / cdz + A(0.25) * (wgradx2 - wgradx1) / cdx;
     const A yz = A(0.25) * (vgradz2 - vgradz1) / cdz + A(0.25) * (wgrady2 - wgrady1) / cdy;
-    A pgradx = (LA(pressure, j + 1, k, l) - LA(pressure, j - 1, k, l)) / (cdx + AG(GX, ga.celldx, j + 1));
-    A pgrady = (LA(pressure, j, k + 1, l) - LA(pressure, j, k - 1, l)) / (cdy + AG(GY, ga.celldy, k + 1));
-    A pgradz = (LA(pressure, j, k, l + 1) - LA(pressure, j, k, l - 1)) / (cdz + AG(GZ, ga.celldz, l + 1));
+    // the neighbours' pressures as ideal_gas stores them (density0 and
+    // energy0 carry the halo the pressure's would mirror)
+    using C = typename S::cs_t;
+#define PN(jj, kk, ll) \
+  ((A)st<C>((double)((A(1.4) - A(1.0)) * LA(density0, jj, kk, ll) * LA(energy0, jj, kk, ll))))
+    A pgradx = (PN(j + 1, k, l) - PN(j - 1, k, l)) / (cdx + AG(GX, ga.celldx, j + 1));
+    A pgrady = (PN(j, k + 1, l) - PN(j, k - 1, l)) / (cdy + AG(GY, ga.celldy, k + 1));
+    A pgradz = (PN(j, k, l + 1) - PN(j, k, l - 1)) / (cdz + AG(GZ, ga.celldz, l + 1));
+#undef PN
     const A pgradx2 = pgradx * pgradx;
     const A pgrady2 = pgrady * pgrady;
     const A pgradz2 = pgradz * pgradz;
@@ -263,7 +270,19 @@ __global__ void __launch_bounds__(BX * BY, sizeof(typename S::arith_t) == 4 || M
   const A d0 = LA(density0, j, k, l);
   // 1/min(celldx, celldy, celldz)^2 of the chunk's uniform mesh
   const A ds = geo_ds<A>(g);
-  const A ss = LA(soundspeed, j, k, l);
+  // ideal_gas_kernel.f90:47-58 on this cell, stored as ideal_gas stores it
+  A ss;
+  {
+    const A v_eos = A(1.0) / d0;
+    const A p_eos = (A(1.4) - A(1.0)) * d0 * LA(energy0, j, k, l);
+    const A pbe = (A(1.4) - A(1.0)) * d0;
+    const A pbv = -d0 * p_eos;
+    const A ss2 = v_eos * v_eos * (p_eos * pbe - pbv);
+    E(pressure, j, k, l) = st<C>((double)p_eos);
+    const C ss_st = st<C>((double)sqrt(ss2));
+    E(soundspeed, j, k, l) = ss_st;
+    ss = (A)ss_st;
+  }
   A cc = ss * ss;
   cc = cc + A(2.0) * visc / d0;
   A dtct = ds * cc;
@@ -1251,14 +1270,14 @@ template <class S>
 void launch_visc_dt(const Target& tg, cudaStream_t s, const GeomArrays& ga, double g_small,
                     double dtc_safe, double dtu_safe, double dtv_safe, double dtw_safe,
                     double dtdiv_safe, const typename S::rho_t* density0,
-                    const typename S::cs_t* pressure, typename S::cs_t* viscosity,
-                    const typename S::cs_t* soundspeed, const typename S::vel_t* xvel0,
-                    const typename S::vel_t* yvel0, const typename S::vel_t* zvel0,
-                    unsigned long long* min_key) {
+                    const typename S::ene_t* energy0, typename S::cs_t* pressure,
+                    typename S::cs_t* viscosity, typename S::cs_t* soundspeed,
+                    const typename S::vel_t* xvel0, const typename S::vel_t* yvel0,
+                    const typename S::vel_t* zvel0, unsigned long long* min_key) {
   launch_mapped2(tg, s, kKeyTimestepVisc, grid_visc, grid_visc_flat, 0, false, kBlk, k_visc_dt<S, MapSingle>,
                 k_visc_dt<S, MapBatch>, ga, g_small, dtc_safe, dtu_safe, dtv_safe, dtw_safe,
-                dtdiv_safe, density0, pressure, viscosity, soundspeed, xvel0, yvel0, zvel0,
-                min_key);
+                dtdiv_safe, density0, energy0, pressure, viscosity, soundspeed, xvel0, yvel0,
+                zvel0, min_key);
 }
 
 template <class S>
@@ -1418,8 +1437,9 @@ void launch_advec_mom_fused(const Target& tg, cudaStream_t s, int advect_x, int 
 #define INSTF(S)                                                                               \
   template void launch_visc_dt<S>(const Target&, cudaStream_t, const GeomArrays&, double, double,  \
                                   double, double, double, double, const S::rho_t*,             \
-                                  const S::cs_t*, S::cs_t*, const S::cs_t*, const S::vel_t*,    \
-                                  const S::vel_t*, const S::vel_t*, unsigned long long*);      \
+                                  const S::ene_t*, S::cs_t*, S::cs_t*, S::cs_t*,               \
+                                  const S::vel_t*, const S::vel_t*, const S::vel_t*,           \
+                                  unsigned long long*);                                        \
   template void launch_pdv_predict_eos<S>(const Target&, cudaStream_t, const double*,            \
                                           const GeomArrays&, const S::rho_t*, const S::ene_t*, \
                                           S::cs_t*, const S::cs_t*, const S::vel_t*,           \

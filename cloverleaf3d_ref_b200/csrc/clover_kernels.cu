@@ -1377,7 +1377,9 @@ void launch_update_halo(const Target& tg, cudaStream_t s, const HaloFields& f, c
     const unsigned key = kKeyHalo | (unsigned)(ax << 4) | (unsigned)depth;
     if (ax == 0) {
       const int per_row = h.nfields * 2 * depth;
-      const unsigned kx = kKeyHaloX | (unsigned)per_row;
+      // the schedule depends on the depth as well as the tasks per row (a
+      // depth-1 and a depth-2 update can have the same number per row)
+      const unsigned kx = kKeyHaloX | (unsigned)((depth - 1) << 7) | (unsigned)per_row;
       if (depth == 1)
         launch_mapped(tg, s, kx, grid_halo_x<1>, per_row, false, blk, k_halo_x<MapSingle>,
                       k_halo_x<MapBatchFree>, h, depth, do_low, do_high);

@@ -328,10 +328,10 @@ template <class S>
 void launch_visc_dt(const Target& tg, cudaStream_t s, const GeomArrays& ga, double g_small,
                     double dtc_safe, double dtu_safe, double dtv_safe, double dtw_safe,
                     double dtdiv_safe, const typename S::rho_t* density0,
-                    const typename S::cs_t* pressure, typename S::cs_t* viscosity,
-                    const typename S::cs_t* soundspeed, const typename S::vel_t* xvel0,
-                    const typename S::vel_t* yvel0, const typename S::vel_t* zvel0,
-                    unsigned long long* min_key);
+                    const typename S::ene_t* energy0, typename S::cs_t* pressure,
+                    typename S::cs_t* viscosity, typename S::cs_t* soundspeed,
+                    const typename S::vel_t* xvel0, const typename S::vel_t* yvel0,
+                    const typename S::vel_t* zvel0, unsigned long long* min_key);
 template <class S>
 void launch_pdv_predict_eos(const Target& tg, cudaStream_t s, const double* dt_ptr,
                             const GeomArrays& ga, const typename S::rho_t* density0,

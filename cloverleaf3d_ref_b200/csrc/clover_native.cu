@@ -730,18 +730,20 @@ struct Chunk : ChunkBase {
     int cb = ax ? 0 : 1;  // buffer of the density1/energy1 pair at the start of this step
     // timestep.f90:56-126
     k_dt_prepare<<<deck_blocks(), 128, 0, stream>>>(sc, nd, min_key_of(kGBig));
+    // ideal_gas runs inside the viscosity/calc_dt kernel: it stores every
+    // cell's pressure and sound speed and forms the neighbours' pressures
+    // from density0/energy0, whose halo is updated first. The step-start
+    // update of the pressure's halo is left out: the depth-1 update after the
+    // predictor rewrites the same cells before anything reads them.
     pbeg();
-    launch_ideal_gas<S>(tg, stream, density0, energy0, pressure, soundspeed);
-    pend("ideal_gas", n * (R8 + E8 + 2 * C8));
-    pbeg();
-    halo({5, 3, 1, 8, 10}, 1, vc, cb);
+    halo({3, 1, 8, 10}, 1, vc, cb);
     pend("update_halo", 0);
     pbeg();
     launch_visc_dt<S>(tg, stream, ga, kGSmall, deck.dtc_safe, deck.dtu_safe, deck.dtv_safe,
-                      deck.dtw_safe, deck.dtdiv_safe, density0, pressure, viscosity, soundspeed,
-                      xvel0, yvel0, zvel0, &sc->key);
+                      deck.dtw_safe, deck.dtdiv_safe, density0, energy0, pressure, viscosity,
+                      soundspeed, xvel0, yvel0, zvel0, &sc->key);
     k_dt_finalize<<<deck_blocks(), 128, 0, stream>>>(sc, nd, dt_hist);
-    pend("viscosity_calc_dt", n * (3 * V8 + R8 + 3 * C8));
+    pend("eos_viscosity_calc_dt", n * (3 * V8 + R8 + E8 + 3 * C8));
     pbeg();
     halo({6}, 1, vc, cb);  // read by accelerate at its neighbours
     pend("update_halo", 0);

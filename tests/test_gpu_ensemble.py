@@ -61,6 +61,23 @@ def test_ensemble_decks_match_oracle(graphs):
     ens.close()
 
 
+def test_decks_of_three_cells_or_more_match_oracle():
+    """Without a thin deck the batched step leaves out the halo updates that
+    repeat a no-op and the shell copies a depth-2 update overwrites; every
+    field, halos included, still equals the oracle's."""
+    kw = dict(end_step=STEPS, summary_frequency=5)
+    ds = [decks.shock(13, 9, 11, STEPS, states=decks.MIXED_STATES, **kw),
+          decks.shock(16, 16, 16, STEPS, **kw),
+          decks.shock(33, 6, 9, STEPS, initial_timestep=0.01, timestep_rise=1.2, **kw)]
+    ens = C.Ensemble([decks.to_deck(d) for d in ds])
+    assert ens.run() == STEPS
+    for i, d in enumerate(ds):
+        r = O.run(d, want_fields=True)
+        sums, sst = ens.deck_summaries(i)
+        compare(r, ens.deck_dt_history(i), sums, sst, lambda n, i=i: ens.deck_field(i, n))
+    ens.close()
+
+
 def test_one_deck_ensemble_matches_chunk():
     d = decks.to_deck(decks.shock(19, 11, 8, 9, states=decks.MIXED_STATES))
     ens = C.Ensemble([d])
