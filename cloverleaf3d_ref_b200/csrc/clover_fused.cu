@@ -1054,7 +1054,7 @@ __global__ void __launch_bounds__(BX * BY, 3) k_cell_sweep_march(M m, GeomArrays
 // and the momentum limiter keep the reference order
 // (advec_mom_kernel.f90:166-252).
 template <class S, int VAR, class M>
-__global__ void __launch_bounds__(BX * BY, 4) k_mom_sweep_x(M m,
+__global__ void __launch_bounds__(BX * BY, M::kFlat || sizeof(typename S::arith_t) == 8 ? 4 : 6) k_mom_sweep_x(M m,
     GeomArrays ga, const typename S::mf_t* __restrict__ mfx,
     const typename S::rho_t* __restrict__ density1, const typename S::vf_t* __restrict__ vfx,
     const typename S::vf_t* __restrict__ vfy, const typename S::vf_t* __restrict__ vfz,
