@@ -203,6 +203,7 @@ def _declare(L):
     L.clover_gpu_status.restype = ctypes.c_int
     L.clover_gpu_error_string.restype = ctypes.c_char_p
     L.clover_gpu_invalidate.argtypes = [P]
+    L.clover_gpu_invalidate_all.argtypes = []
     abi = L
 
 

@@ -549,6 +549,11 @@ void clover_gpu_invalidate(const void* host_array) {
   if (it != c.mirrors.end()) it->second.planes = 0;
 }
 
+void clover_gpu_invalidate_all(void) {
+  Context& c = ctx();
+  for (auto& kv : c.mirrors) kv.second.planes = 0;
+}
+
 void clover_gpu_synchronize(void) {
   Context& c = ctx();
   if (c.ready) check(cudaStreamSynchronize(c.stream), "synchronize");

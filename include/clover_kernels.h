@@ -218,6 +218,9 @@ void clover_gpu_clear_status(void);
 void clover_gpu_sync_to_host(void);
 /* The host copy of this array changed: upload it again at its next use. */
 void clover_gpu_invalidate(const void *host_array);
+/* Every mirrored host array changed (e.g. the caller restored its state on
+ * the host): each is uploaded again at its next use. */
+void clover_gpu_invalidate_all(void);
 /* Wait for all queued work. */
 void clover_gpu_synchronize(void);
 /* Free every mirror and the library stream. */

@@ -126,6 +126,24 @@ def test_dropin_driver_run_bitwise(case):
     di.close()
 
 
+def test_dropin_state_restored_from_host_arrays():
+    """Copying the state back, marking every mirror stale and carrying on
+    (each array uploaded again from its host copy at its next use) gives the
+    uninterrupted run bit for bit."""
+    d = decks.shock(13, 9, 11, 20, states=decks.MIXED_STATES)
+    r = O.run(d, max_steps=20, want_fields=True)
+    L = C.lib()
+    di = C.DropIn(decks.to_deck(d))
+    assert di.run(7) == 7  # the driver's step count is cumulative
+    L.clover_gpu_sync_to_host()
+    L.clover_gpu_invalidate_all()
+    assert di.run(20) == r["steps"]
+    sums, sst = di.summaries()
+    keep = np.isin(sst, r["summary_steps"])  # drop the summary the first call ended with
+    compare_run(r, di.dt_history(), sums[keep], sst[keep], di.field)
+    di.close()
+
+
 @pytest.mark.parametrize("fused", [True, False])
 @pytest.mark.parametrize("graphs", [True, False])
 @pytest.mark.parametrize("case", ["tp1", "shock16", "mixed", "thin"])
