@@ -35,6 +35,8 @@ struct Context {
   unsigned long long* d_key = nullptr;
   double* d_partials = nullptr;
   double* d_sum = nullptr;
+  double* stage = nullptr;  // contiguous copy of host planes on their way up or down
+  size_t stage_bytes = 0;
   int status = 0;
   std::string err;
   bool pin_host = true;
@@ -100,28 +102,58 @@ bool is_device_pointer(const void* p) {
 
 }  // namespace
 
-// Host <-> device copy of planes [p0,p1) of a 3D mirror.
+// Rows of hx elements between the host's contiguous planes (hy rows each) and
+// the mirror's pitched layout (row pitch px, plane pitch pxy): one block per
+// row, grid-strided.
+__global__ void k_rows_to_pitched(const double* __restrict__ src, double* __restrict__ dst, int hx,
+                                  int hy, long long rows, int px, long long pxy) {
+  for (long long r = blockIdx.x; r < rows; r += gridDim.x) {
+    const double* s = src + r * hx;
+    double* d = dst + (r / hy) * pxy + (r % hy) * px;
+    for (int i = threadIdx.x; i < hx; i += blockDim.x) d[i] = s[i];
+  }
+}
+__global__ void k_pitched_to_rows(const double* __restrict__ src, double* __restrict__ dst, int hx,
+                                  int hy, long long rows, int px, long long pxy) {
+  for (long long r = blockIdx.x; r < rows; r += gridDim.x) {
+    const double* s = src + (r / hy) * pxy + (r % hy) * px;
+    double* d = dst + r * hx;
+    for (int i = threadIdx.x; i < hx; i += blockDim.x) d[i] = s[i];
+  }
+}
+
+// Host <-> device copy of planes [p0,p1) of a 3D mirror: one contiguous DMA
+// of the host planes to or from a staging buffer, and a kernel that moves the
+// rows between the staging buffer and the pitched mirror (a strided copy of
+// ~4 KB rows runs at a fraction of the link's rate).
 static void xfer3d(const void* host, Mirror& m, int p0, int p1, bool up) {
   Context& c = ctx();
   if (p1 <= p0) return;
   const HostShape& s = m.shape;
-  cudaMemcpy3DParms q = {};
   const size_t host_plane = (size_t)s.hx * s.hy * 8;
-  cudaPitchedPtr hp = make_cudaPitchedPtr((char*)host + host_plane * p0, (size_t)s.hx * 8,
-                                          (size_t)s.hx * 8, (size_t)s.hy);
-  cudaPitchedPtr dp = make_cudaPitchedPtr((char*)(m.dev + c.g.pxy * p0), (size_t)c.g.px * 8,
-                                          (size_t)s.hx * 8, (size_t)(c.g.pxy / c.g.px));
-  q.extent = make_cudaExtent((size_t)s.hx * 8, (size_t)s.hy, (size_t)(p1 - p0));
-  if (up) {
-    q.srcPtr = hp;
-    q.dstPtr = dp;
-    q.kind = cudaMemcpyHostToDevice;
-  } else {
-    q.srcPtr = dp;
-    q.dstPtr = hp;
-    q.kind = cudaMemcpyDeviceToHost;
+  const size_t bytes = host_plane * (size_t)(p1 - p0);
+  if (bytes > c.stage_bytes) {
+    cudaStreamSynchronize(c.stream);
+    cudaFree(c.stage);
+    c.stage = nullptr;
+    c.stage_bytes = 0;
+    if (!check(cudaMalloc(&c.stage, bytes), "staging malloc")) return;
+    c.stage_bytes = bytes;
   }
-  check(cudaMemcpy3DAsync(&q, c.stream), up ? "upload" : "download");
+  char* hp = (char*)host + host_plane * p0;
+  double* dp = m.dev + c.g.pxy * p0;
+  const long long rows = (long long)s.hy * (p1 - p0);
+  if (up) {
+    check(cudaMemcpyAsync(c.stage, hp, bytes, cudaMemcpyHostToDevice, c.stream), "upload");
+    k_rows_to_pitched<<<148 * 8, 256, 0, c.stream>>>(c.stage, dp, s.hx, s.hy, rows, c.g.px,
+                                                     c.g.pxy);
+    check_launch("upload rows");
+  } else {
+    k_pitched_to_rows<<<148 * 8, 256, 0, c.stream>>>(dp, c.stage, s.hx, s.hy, rows, c.g.px,
+                                                     c.g.pxy);
+    check_launch("download rows");
+    check(cudaMemcpyAsync(hp, c.stage, bytes, cudaMemcpyDeviceToHost, c.stream), "download");
+  }
 }
 
 // Resolve a 3D array argument to its device copy.
@@ -571,6 +603,9 @@ void clover_gpu_release(void) {
   cudaFree(c.d_key);
   cudaFree(c.d_partials);
   cudaFree(c.d_sum);
+  cudaFree(c.stage);
+  c.stage = nullptr;
+  c.stage_bytes = 0;
   cudaStreamDestroy(c.stream);
   c.ready = false;
 }
