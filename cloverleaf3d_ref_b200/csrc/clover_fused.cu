@@ -466,11 +466,13 @@ __global__ void __launch_bounds__(BX * BY, M::kFlat ? 5 : 8) k_pdv_flux(M m, con
   const double total_flux = right_flux - left_flux + top_flux - bottom_flux + front_flux - back_flux;
   const double vol = g.vol;
   const double vol_change_s = vol / (vol + total_flux);
-  const double recip_volume = g.rvol;  // 1/volume
   const double d0 = L(density0, j, k, l);
-  const double energy_change =
-      (L(pressure, j, k, l) / d0 + L(viscosity, j, k, l) / d0) * total_flux * recip_volume;
-  E(energy1, j, k, l) = st<typename S::ene_t>(L(energy0, j, k, l) - energy_change);
+  // the energy change in the policy's arithmetic (an FP32 stencil in the
+  // mixed path); the density, which carries the mass, stays FP64
+  const A ad0 = (A)d0;
+  const A energy_change = (LA(pressure, j, k, l) / ad0 + LA(viscosity, j, k, l) / ad0) *
+                          (A)total_flux * geo_rvol<A>(g);
+  E(energy1, j, k, l) = st<typename S::ene_t>((double)(LA(energy0, j, k, l) - energy_change));
   E(density1, j, k, l) = st<typename S::rho_t>(d0 * vol_change_s);
 #undef LA
   });
@@ -509,14 +511,18 @@ __device__ __forceinline__ double width_ratio(double a, double b) {
   return (a == b && a != 0.0 && fabs(a) <= DBL_MAX) ? 1.0 : a / b;
 }
 
-__device__ __forceinline__ double cell_limiter(double sig, double sigma3, double sigma4,
-                                               double diffuw, double diffdw) {
-  const double one_by_six = 1.0 / 6.0;
-  if (diffuw * diffdw > 0.0)
-    return (1.0 - sig) * copysign(1.0, diffdw) *
+// advec_cell_kernel.f90:141-151 in the limiter's arithmetic A (FP64, or FP32
+// in the mixed path: the limiter shapes a face flux that both cells of the
+// face take, so its rounding does not touch conservation; the flux itself and
+// the cell update stay FP64)
+template <class A>
+__device__ __forceinline__ A cell_limiter(A sig, A sigma3, A sigma4, A diffuw, A diffdw) {
+  const A one_by_six = A(1.0) / A(6.0);
+  if (diffuw * diffdw > A(0.0))
+    return (A(1.0) - sig) * copysign(A(1.0), diffdw) *
            fmin2(fmin2(fabs(diffuw), fabs(diffdw)),
                  one_by_six * (sigma3 * fabs(diffuw) + sigma4 * fabs(diffdw)));
-  return 0.0;
+  return A(0.0);
 }
 
 // advec_cell x sweep as ONE pass (advec_cell_kernel.f90:125-185), out of
@@ -571,22 +577,23 @@ __global__ void __launch_bounds__(BX * BY, M::kFlat ? 4 : 5) k_cell_sweep_x(M m,
       e_up = clamp ? e : e_p1; e_don = e; e_dn = e_m1;
       pv_don = pv; vd_dif = clamp ? vd : vd_p1;
     }
-    const double sigmat = fabs(vf) / pv_don;
-    const double sigma3 = (1.0 + sigmat) * width_ratio(vd, vd_dif);
-    const double sigma4 = 2.0 - sigmat;
-    double diffuw = d_don - d_up;
-    double diffdw = d_dn - d_don;
-    double limiter = cell_limiter(sigmat, sigma3, sigma4, diffuw, diffdw);
-    const double mflux = vf * (d_don + limiter);
+    using AL = typename S::arith_t;  // the limiters' arithmetic
+    const AL sigmat = (AL)fabs(vf) / (AL)pv_don;
+    const AL sigma3 = (AL(1.0) + sigmat) * (AL)width_ratio(vd, vd_dif);
+    const AL sigma4 = AL(2.0) - sigmat;
+    AL diffuw = (AL)(d_don - d_up);
+    AL diffdw = (AL)(d_dn - d_don);
+    AL limiter = cell_limiter<AL>(sigmat, sigma3, sigma4, diffuw, diffdw);
+    const double mflux = vf * (d_don + (double)limiter);
     // the cell update takes the FP64 face fluxes; the stored mass flux
     // (mf_t) feeds only the momentum sweep
     mf_st = mflux;
     if (lane <= 29) E(mass_flux, c, k, l) = st<MF>(mflux);
-    const double sigmam = fabs(mflux) / (d_don * pv_don);
-    diffuw = e_don - e_up;
-    diffdw = e_dn - e_don;
-    limiter = cell_limiter(sigmam, sigma3, sigma4, diffuw, diffdw);
-    ef = mflux * (e_don + limiter);
+    const AL sigmam = (AL)fabs(mflux) / ((AL)d_don * (AL)pv_don);
+    diffuw = (AL)(e_don - e_up);
+    diffdw = (AL)(e_dn - e_don);
+    limiter = cell_limiter<AL>(sigmam, sigma3, sigma4, diffuw, diffdw);
+    ef = mflux * (e_don + (double)limiter);
   }
   // advec_cell_kernel.f90:173-185 for cell c from faces c and c+1
   const double mf_p = __shfl_down_sync(full, mf_st, 1);
@@ -1003,20 +1010,21 @@ __global__ void __launch_bounds__(BX * BY, 3) k_cell_sweep_march(M m, GeomArrays
       d_up = d3; d_don = d2; d_dn = d1; e_up = e3; e_don = e2; e_dn = e1; pv_don = pv_0;
       dif = p + 1 < top ? p + 1 : top;
     }
-    const double sigmat = fabs(vf) / pv_don;
-    const double sigma3 = (1.0 + sigmat) * width_ratio(VD(p), VD(dif));
-    const double sigma4 = 2.0 - sigmat;
-    double diffuw = d_don - d_up;
-    double diffdw = d_dn - d_don;
-    double limiter = cell_limiter(sigmat, sigma3, sigma4, diffuw, diffdw);
-    const double mflux = vf * (d_don + limiter);
+    using AL = typename S::arith_t;  // the limiters' arithmetic
+    const AL sigmat = (AL)fabs(vf) / (AL)pv_don;
+    const AL sigma3 = (AL(1.0) + sigmat) * (AL)width_ratio(VD(p), VD(dif));
+    const AL sigma4 = AL(2.0) - sigmat;
+    AL diffuw = (AL)(d_don - d_up);
+    AL diffdw = (AL)(d_dn - d_don);
+    AL limiter = cell_limiter<AL>(sigmat, sigma3, sigma4, diffuw, diffdw);
+    const double mflux = vf * (d_don + (double)limiter);
     if (p <= c1 || last) EI(mass_flux, IDX(p)) = st<MF>(mflux);
     const double mf_stored = mflux;  // FP64 in the cell update; mf_t storage feeds the momentum sweep
-    const double sigmam = fabs(mflux) / (d_don * pv_don);
-    diffuw = e_don - e_up;
-    diffdw = e_dn - e_don;
-    limiter = cell_limiter(sigmam, sigma3, sigma4, diffuw, diffdw);
-    const double eflux = mflux * (e_don + limiter);
+    const AL sigmam = (AL)fabs(mflux) / ((AL)d_don * (AL)pv_don);
+    diffuw = (AL)(e_don - e_up);
+    diffdw = (AL)(e_dn - e_don);
+    limiter = cell_limiter<AL>(sigmam, sigma3, sigma4, diffuw, diffdw);
+    const double eflux = mflux * (e_don + (double)limiter);
     // advec_cell_kernel.f90:270-281 (y) / :365-376 (z) for cell p-1
     if (update && p - 1 >= c0 && p - 1 <= c1) {
       const double pm = d1 * pv_m;
