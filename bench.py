@@ -347,24 +347,27 @@ def e2e_dropin(C, args, n, steps):
 
     Set-up (not timed): the reference's start() over host arrays, which
     allocates them (build_field), registers them as pinned memory on their
-    first sight and initialises the chunk; the state is then copied back and
-    every mirror marked stale, so the timed run starts from the host arrays.
+    first sight and initialises the chunk, and the warm-up steps; the state is
+    then copied back and every mirror marked stale, so the timed run starts
+    from the host arrays.
     Timed: the steps of the reference control flow through clover_*_kernel,
     whose first call on each array uploads it from the pinned host array (all
     of the state), the per-step scalar reads (dt, summaries), and the copy of
     every array back to the host at the end."""
     import numpy as np  # noqa: F401
     sys.path.insert(0, os.path.join(ROOT, "tests"))
-    deck = C.Deck.from_values(states=STATES, **deck_values(n, steps))
+    warm = max(args.warmup if args is not None else 3, 1)
+    deck = C.Deck.from_values(states=STATES, **deck_values(n, warm + steps + 1))
     L = C.lib()
     L.clover_gpu_release()
     L.clover_gpu_synchronize()
     ts = time.perf_counter()
     di = C.DropIn(deck)  # start(): first sight of every host array pins and uploads it
+    di.run(warm)  # warm-up steps (the driver's step count is cumulative)
     L.clover_gpu_sync_to_host()
     L.clover_gpu_invalidate_all()
     t0 = time.perf_counter()
-    taken = di.run(steps)
+    taken = di.run(warm + steps) - warm
     L.clover_gpu_sync_to_host()  # every array back to the host
     t1 = time.perf_counter()
     arrays = ctypes.c_int(0)

@@ -533,7 +533,7 @@ __device__ __forceinline__ A cell_limiter(A sig, A sigma3, A sigma4, A diffuw, A
 // fluxes of face c and update cell c from faces c and c+1 into the output
 // arrays, so no thread reads a value another one writes.
 template <class S, int VAR, class M>
-__global__ void __launch_bounds__(BX * BY, M::kFlat ? 4 : 5) k_cell_sweep_x(M m, GeomArrays ga,
+__global__ void __launch_bounds__(BX * BY, M::kFlat ? 4 : (sizeof(typename S::arith_t) == 4 ? 6 : 5)) k_cell_sweep_x(M m, GeomArrays ga,
     const typename S::rho_t* __restrict__ d_in, const typename S::ene_t* __restrict__ e_in,
     typename S::rho_t* __restrict__ d_out, typename S::ene_t* __restrict__ e_out,
     const typename S::vf_t* __restrict__ vfx, const typename S::vf_t* __restrict__ vfy,
@@ -923,7 +923,7 @@ __global__ void __launch_bounds__(BX * BY, 3) k_mom_vel3_march(M m, GeomArrays g
 // in [pmin, pmax] (c <= cmax); face c1+1 is computed by both neighbours and
 // stored by the segment that starts there.
 template <class S, int DIR, int VAR, class M>
-__global__ void __launch_bounds__(BX * BY, 3) k_cell_sweep_march(M m, GeomArrays ga,
+__global__ void __launch_bounds__(BX * BY, sizeof(typename S::arith_t) == 4 ? 4 : 3) k_cell_sweep_march(M m, GeomArrays ga,
     typename S::rho_t* __restrict__ density1, typename S::ene_t* __restrict__ energy1,
     const typename S::vf_t* __restrict__ vfx, const typename S::vf_t* __restrict__ vfy,
     const typename S::vf_t* __restrict__ vfz, typename S::mf_t* __restrict__ mass_flux,
