@@ -128,7 +128,7 @@ __global__ void __launch_bounds__(BX * BY) k_ideal_gas(M m,
 // ---------------------------------------------------------------------------
 // viscosity_kernel.f90:71-134
 template <class S>
-__global__ void __launch_bounds__(BX * BY) k_viscosity(Geom g, Box b, GeomArrays ga,
+__global__ void __launch_bounds__(BX * BY, 4) k_viscosity(Geom g, Box b, GeomArrays ga,
     const typename S::rho_t* __restrict__ density0, const typename S::cs_t* __restrict__ pressure,
     typename S::cs_t* __restrict__ viscosity, const typename S::vel_t* __restrict__ xvel0,
     const typename S::vel_t* __restrict__ yvel0, const typename S::vel_t* __restrict__ zvel0) {
@@ -214,7 +214,7 @@ __global__ void __launch_bounds__(BX * BY) k_viscosity(Geom g, Box b, GeomArrays
 // atomic gives exactly the serial minimum; NaNs never win, as with .LT..
 
 template <class S, class M>
-__global__ void __launch_bounds__(BX * BY) k_calc_dt(M m, GeomArrays ga,
+__global__ void __launch_bounds__(BX * BY, 6) k_calc_dt(M m, GeomArrays ga,
     double g_small, double dtc_safe, double dtu_safe, double dtv_safe, double dtw_safe,
     double dtdiv_safe, const typename S::rho_t* __restrict__ density0,
     const typename S::cs_t* __restrict__ viscosity_a, const typename S::cs_t* __restrict__ soundspeed,
@@ -290,7 +290,7 @@ __global__ void __launch_bounds__(BX * BY) k_calc_dt(M m, GeomArrays ga,
 // ---------------------------------------------------------------------------
 // PdV_kernel.f90:72-166
 template <class S>
-__global__ void __launch_bounds__(BX * BY) k_pdv(Geom g, Box b, int predict, double dt_val,
+__global__ void __launch_bounds__(BX * BY, 8) k_pdv(Geom g, Box b, int predict, double dt_val,
     const double* dt_ptr, GeomArrays ga, const typename S::rho_t* __restrict__ density0,
     typename S::rho_t* __restrict__ density1, const typename S::ene_t* __restrict__ energy0,
     typename S::ene_t* __restrict__ energy1, const typename S::cs_t* __restrict__ pressure,
@@ -507,7 +507,7 @@ __device__ __forceinline__ double cell_limiter(double sig, double sigma3, double
 // advec_cell_kernel.f90 flux pass (:125-171 x, :220-266 y, :315-361 z).
 // DIR is the sweep axis; (dj,dk,dl) its unit offset.
 template <class S, int DIR>
-__global__ void __launch_bounds__(BX * BY) k_cell_flux(Geom g, Box b, GeomArrays ga,
+__global__ void __launch_bounds__(BX * BY, 8) k_cell_flux(Geom g, Box b, GeomArrays ga,
     const typename S::rho_t* __restrict__ density1, const typename S::ene_t* __restrict__ energy1,
     const typename S::vf_t* __restrict__ vol_flux, typename S::mf_t* __restrict__ mass_flux,
     const typename S::wk_t* __restrict__ pre_vol, typename S::wk_t* __restrict__ ener_flux) {
@@ -683,7 +683,7 @@ __device__ __forceinline__ double mom_limiter(double sigma, double width, double
 
 // mom_flux (:211-242 x, :295-327 y, :381-413 z)
 template <class S, int DIR>
-__global__ void __launch_bounds__(BX * BY) k_mom_flux(Geom g, Box b, GeomArrays ga,
+__global__ void __launch_bounds__(BX * BY, 8) k_mom_flux(Geom g, Box b, GeomArrays ga,
     const typename S::vel_t* __restrict__ vel1, const typename S::wk_t* __restrict__ node_flux,
     const typename S::wk_t* __restrict__ node_mass_pre, typename S::wk_t* __restrict__ mom_flux) {
   BOX_THREAD(b);
