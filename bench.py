@@ -26,6 +26,9 @@ ensemble   batched decks (seeded draws of the same problem with drawn sizes,
 cannot be compiled on this image: no Fortran compiler).
 Multi-GPU (--gpus N under torchrun): N independent replicas, one chunk per
 GPU (the single-chunk path does not shard); weak scaling, max time over ranks.
+The ensemble legs partition their decks over the ranks instead (each rank
+its share, balanced by cells, no communication; strong scaling, max time over
+ranks).
 """
 import argparse
 import ctypes
@@ -230,10 +233,7 @@ def mixed_leg(C, torch, deck, args, fp64_ms, fp64_sums, fp64_steps, barrier, wor
     e1.synchronize()
     ms = e0.elapsed_time(e1)
     barrier()
-    if world > 1:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(ms, dist if world > 1 else None, "cuda")
     ch.profile(True)
     ch.step(args.steps)
     groups = ch.profile_report()
@@ -273,18 +273,32 @@ def timed_steps(torch, obj, steps):
     return e0.elapsed_time(e1)
 
 
-def ensemble_leg(C, torch, n_decks, cells, steps, seed, precisions, seq_decks, warm=3):
+def ensemble_leg(C, torch, n_decks, cells, steps, seed, precisions, seq_decks, warm=3,
+                 world=1, rank=0, barrier=None, dist=None):
     """One ensemble configuration: per precision, the batched run (autotuned,
     then warm steps, then the rest of the steps timed); then the same decks
     one after another as single chunks (the first seq_decks of them, the
     rate scaled by their cells), and the per-deck summary error of the mixed
-    run against the FP64 run at every summary step."""
+    run against the FP64 run at every summary step.
+
+    With world > 1 every rank draws the same decks and runs its share of them
+    (replicas.deck_share, balanced by cells) as its own ensemble, with no
+    communication between ranks; the time is the slowest rank's (barrier
+    before, max over ranks after) over the cells of all the decks, and the
+    one-after-another baseline is left to the 1-GPU run."""
     import numpy as np
-    decks = C.draw_decks(n_decks, seed, cells=cells, end_step=steps, summary_frequency=10)
-    total = sum(d.cells for d in decks)
+    from cloverleaf3d_ref_b200.replicas import deck_share, max_over_ranks
+    all_decks = C.draw_decks(n_decks, seed, cells=cells, end_step=steps, summary_frequency=10)
+    total = sum(d.cells for d in all_decks)
+    mine = deck_share([d.cells for d in all_decks], rank, world)
+    decks = [all_decks[i] for i in mine]
     timed = steps - warm
     out = {"decks": n_decks, "cells_per_axis": list(cells), "steps": steps, "seed": seed,
            "total_cells": total}
+    if world > 1:
+        out["partition"] = {"ranks": world, "scaling": "strong",
+                            "rank0_decks": len(decks),
+                            "rank0_cells": sum(d.cells for d in decks)}
     sums = {}
     for prec in precisions:
         key = "fp64" if prec == C.PRECISION_FP64 else "mixed"
@@ -294,10 +308,13 @@ def ensemble_leg(C, torch, n_decks, cells, steps, seed, precisions, seq_decks, w
         tune_s = time.perf_counter() - t0
         ens.step(warm)
         ens.sync()
+        if barrier is not None:
+            barrier()
         ms = timed_steps(torch, ens, timed)
+        ms = max_over_ranks(ms, dist, "cuda")
         assert ens.run() == steps
-        bad = [d for d in range(n_decks) if ens.deck_status(d) != 0]
-        sums[key] = [ens.deck_summaries(d)[0] for d in range(n_decks)]
+        bad = [mine[d] for d in range(len(decks)) if ens.deck_status(d) != 0]
+        sums[key] = [ens.deck_summaries(d)[0] for d in range(len(decks))]
         sched = ens.schedule()
         out[key] = {
             "value": total * timed / (ms / 1000.0), "unit": "cell-updates/s",
@@ -312,6 +329,13 @@ def ensemble_leg(C, torch, n_decks, cells, steps, seed, precisions, seq_decks, w
                          "segs": sorted({x["seg"] for x in sched if x["seg"] > 0})},
         }
         ens.close()
+    if world > 1:
+        if "fp64" in sums and "mixed" in sums:
+            e = max(float(rel_err(a, b)[:, [0, 1, 2, 4]].max())
+                    for a, b in zip(sums["mixed"], sums["fp64"]))
+            out["mixed_rel_err_vs_fp64"] = {
+                "all_summaries_max_over_decks_excluding_ke": max_over_ranks(e, dist, "cuda")}
+        return out
     # the same decks one after another (single chunks, graph replay)
     prec = precisions[0]
     key = "fp64" if prec == C.PRECISION_FP64 else "mixed"
@@ -389,14 +413,15 @@ def e2e_dropin(C, args, n, steps):
                      "per-step dt and summary reads, every array copied back"}
 
 
-def ensembles(C, torch):
+def ensembles(C, torch, world=1, rank=0, barrier=None, dist=None):
     """The two ensemble configurations (64 decks FP64 + mixed; 512 small decks
-    mixed with its FP64 twin)."""
+    mixed with its FP64 twin), partitioned over the ranks when world > 1."""
+    kw = dict(world=world, rank=rank, barrier=barrier, dist=dist)
     return {
         "decks64": ensemble_leg(C, torch, 64, (24, 128), 150, 2024,
-                                [C.PRECISION_FP64, C.PRECISION_MIXED], 64),
+                                [C.PRECISION_FP64, C.PRECISION_MIXED], 64, **kw),
         "decks512": ensemble_leg(C, torch, 512, (16, 48), 100, 4048,
-                                 [C.PRECISION_MIXED, C.PRECISION_FP64], 64),
+                                 [C.PRECISION_MIXED, C.PRECISION_FP64], 64, **kw),
     }
 
 
@@ -426,6 +451,7 @@ def main():
     import torch
     import torch.distributed as dist
     import cloverleaf3d_ref_b200 as C
+    from cloverleaf3d_ref_b200.replicas import max_over_ranks
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -441,8 +467,11 @@ def main():
             dist.barrier()
 
     if args.ensemble_only:
+        ens = ensembles(C, torch, world, rank, barrier, dist)
         if rank == 0:
-            print(json.dumps({"ensemble": ensembles(C, torch)}))
+            print(json.dumps({"ensemble": ens, "n_gpus": world}))
+        if world > 1:
+            dist.destroy_process_group()
         return 0
 
     n = args.cells
@@ -468,10 +497,7 @@ def main():
     ms = e0.elapsed_time(e1)
     torch.cuda.synchronize()
     barrier()
-    if world > 1:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(ms, dist if world > 1 else None, "cuda")
     clocks = clk.summary()
 
     # profiled region B: same steps with events around every kernel group
@@ -516,15 +542,17 @@ def main():
         if not args.no_accuracy and rank == 0:
             mixed["accuracy_200_steps"] = accuracy_leg(C, n, 200)
 
+    # every rank takes part in the partitioned ensemble before rank 0 alone
+    # runs the end-to-end and CPU legs
+    ens = None
+    if not args.no_ensemble:
+        ens = ensembles(C, torch, world, rank, barrier, dist)
     e2e = None
     if not args.no_e2e and rank == 0:
         e2e = e2e_dropin(C, args, n, args.steps)
     cpu = None
     if not args.no_cpu and rank == 0 and world == 1:
         cpu = cpu_baseline(n)
-    ens = None
-    if not args.no_ensemble and rank == 0 and world == 1:
-        ens = ensembles(C, torch)
 
     if rank == 0:
         line = {

@@ -1,0 +1,92 @@
+"""CPU: the multi-rank host logic of the replica / ensemble-partition path,
+run as two gloo ranks on 127.0.0.1 (world size 2).
+
+Each rank draws the same seeded ensemble decks, takes its share with
+deck_share, and the shares are gathered: every deck is taken by exactly one
+rank and the cells are balanced. max_over_ranks gives every rank the
+largest of the ranks' values."""
+import os
+import socket
+
+import pytest
+import torch.multiprocessing as mp
+
+from cloverleaf3d_ref_b200.replicas import deck_share, max_over_ranks
+
+
+def free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def rank_main(rank, world, port, q):
+    import datetime
+    import torch
+    import torch.distributed as dist
+    import cloverleaf3d_ref_b200 as C
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=60))
+    try:
+        decks = C.draw_decks(64, 2024, cells=(24, 128), end_step=150)
+        cells = [d.cells for d in decks]
+        mine = deck_share(cells, rank, world)
+        shares = [None] * world
+        dist.all_gather_object(shares, mine)
+        # a timing that differs per rank: the max must reach every rank
+        t = max_over_ranks(10.0 + 7.5 * rank, dist, "cpu")
+        dist.barrier()
+        q.put((rank, cells, shares, t))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_deck_share_single_rank_takes_all():
+    assert deck_share([5, 1, 3], 0, 1) == [0, 1, 2]
+    assert deck_share([], 0, 3) == []
+    with pytest.raises(ValueError):
+        deck_share([1], 2, 2)
+
+
+def test_deck_share_balances_cells():
+    cells = [100, 90, 80, 10, 10, 10]
+    shares = [deck_share(cells, r, 3) for r in range(3)]
+    assert sorted(i for s in shares for i in s) == list(range(6))
+    loads = [sum(cells[i] for i in s) for s in shares]
+    assert max(loads) - min(loads) <= max(cells)
+
+
+def test_max_over_ranks_without_group():
+    assert max_over_ranks(3.25) == 3.25
+
+
+def test_two_gloo_ranks_partition_decks_and_take_max_time():
+    world = 2
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = free_port()
+    procs = [ctx.Process(target=rank_main, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    try:
+        got = [q.get(timeout=180) for _ in range(world)]
+    finally:
+        for p in procs:
+            p.join(timeout=60)
+            if p.is_alive():
+                p.kill()
+    assert all(p.exitcode == 0 for p in procs)
+    got.sort()
+    cells = got[0][1]
+    for rank, c, shares, t in got:
+        assert c == cells  # every rank drew the same decks
+        assert shares == got[0][2]  # and computed the same partition
+        assert t == 17.5
+    shares = got[0][2]
+    taken = sorted(i for s in shares for i in s)
+    assert taken == list(range(len(cells)))
+    loads = [sum(cells[i] for i in s) for s in shares]
+    assert max(loads) - min(loads) <= max(cells)
+    assert all(len(s) > 0 for s in shares)
