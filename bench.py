@@ -42,6 +42,8 @@ import time
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
+from cloverleaf3d_ref_b200.replicas import deck_share, max_over_ranks  # noqa: E402
+
 STATES = [
     dict(density=0.2, energy=1.0),
     dict(density=1.0, energy=2.5, geometry="cuboid", xmin=0.0, xmax=5.0, ymin=0.0, ymax=2.0,
@@ -213,10 +215,10 @@ def accuracy_leg(C, n, steps):
 
 
 def mixed_leg(C, torch, deck, args, fp64_ms, fp64_sums, fp64_steps, barrier, world, dist):
-    """The same workload with FP32 storage of the stencilled fields (FP64
-    density, volume fluxes, pre/post volumes, cell mass/energy update and
-    node masses): timed the same way, and its field summaries compared with
-    the FP64 run's at the same steps."""
+    """The same workload with FP32 storage of the stencilled fields and the
+    volume and mass fluxes (FP64 density, pre/post volumes, cell mass/energy
+    update and node masses): timed the same way, and its field summaries
+    compared with the FP64 run's at the same steps."""
     import numpy as np
     n = args.cells
     ch = C.Chunk(deck, C.PRECISION_MIXED)
@@ -248,7 +250,7 @@ def mixed_leg(C, torch, deck, args, fp64_ms, fp64_sums, fp64_steps, barrier, wor
     return {
         "value": world * n ** 3 * args.steps / (ms / 1000.0), "unit": "cell-updates/s",
         "ms_per_step": ms / args.steps, "speedup_vs_fp64": fp64_ms / ms,
-        "dtype": "f32 storage and stencils (f64 density, volume fluxes, cell update, node masses)",
+        "dtype": "f32 storage and stencils (f64 density, volumes, cell update, node masses)",
         "device_gb": nbytes / 1e9,
         "step_algorithmic_bytes_per_cell": step_bytes / n ** 3,
         "step_achieved_gbs": step_bytes / (ms / args.steps / 1000.0) / 1e9,
@@ -287,7 +289,6 @@ def ensemble_leg(C, torch, n_decks, cells, steps, seed, precisions, seq_decks, w
     before, max over ranks after) over the cells of all the decks, and the
     one-after-another baseline is left to the 1-GPU run."""
     import numpy as np
-    from cloverleaf3d_ref_b200.replicas import deck_share, max_over_ranks
     all_decks = C.draw_decks(n_decks, seed, cells=cells, end_step=steps, summary_frequency=10)
     total = sum(d.cells for d in all_decks)
     mine = deck_share([d.cells for d in all_decks], rank, world)
@@ -451,7 +452,6 @@ def main():
     import torch
     import torch.distributed as dist
     import cloverleaf3d_ref_b200 as C
-    from cloverleaf3d_ref_b200.replicas import max_over_ranks
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

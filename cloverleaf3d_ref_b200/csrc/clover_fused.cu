@@ -439,13 +439,16 @@ __global__ void __launch_bounds__(BX * BY, M::kFlat ? 5 : 8) k_pdv_flux(M m, con
                     LA(zvel1, j, k + 1, ll) + LA(zvel1, j + 1, k + 1, ll));
   };
   double sx = 0, sy = 0, sz = 0;
+  F vfx0 = F(0), vfy0 = F(0);
   if (kin && lin) {
     sx = xsum(j);
-    E(vol_flux_x, j, k, l) = st<F>(0.125 * dt * g.xa * sx);
+    vfx0 = st<F>(0.125 * dt * g.xa * sx);
+    E(vol_flux_x, j, k, l) = vfx0;
   }
   if (jin && lin) {
     sy = ysum(k);
-    E(vol_flux_y, j, k, l) = st<F>(0.125 * dt * g.ya * sy);
+    vfy0 = st<F>(0.125 * dt * g.ya * sy);
+    E(vol_flux_y, j, k, l) = vfy0;
   }
   if (jin && kin) {
     // flux_calc_kernel.f90:86 repeats zvel0(j+1,k,l) and omits zvel0(j,k+1,l)
@@ -457,12 +460,27 @@ __global__ void __launch_bounds__(BX * BY, M::kFlat ? 5 : 8) k_pdv_flux(M m, con
     sz = zsum(l);
   }
   if (!(jin && kin && lin)) return;
-  const double left_flux = (g.xa * sx) * 0.125 * dt;
-  const double right_flux = (g.xa * xsum(j + 1)) * 0.125 * dt;
-  const double bottom_flux = (g.ya * sy) * 0.125 * dt;
-  const double top_flux = (g.ya * ysum(k + 1)) * 0.125 * dt;
-  const double back_flux = (g.za * sz) * 0.125 * dt;
-  const double front_flux = (g.za * zsum(l + 1)) * 0.125 * dt;
+  double left_flux, right_flux, bottom_flux, top_flux, back_flux, front_flux;
+  if (sizeof(F) == 8) {  // PdV_kernel.f90:120-131 order
+    left_flux = (g.xa * sx) * 0.125 * dt;
+    right_flux = (g.xa * xsum(j + 1)) * 0.125 * dt;
+    bottom_flux = (g.ya * sy) * 0.125 * dt;
+    top_flux = (g.ya * ysum(k + 1)) * 0.125 * dt;
+    back_flux = (g.za * sz) * 0.125 * dt;
+    front_flux = (g.za * zsum(l + 1)) * 0.125 * dt;
+  } else {
+    // FP32 volume fluxes: the corrector's face fluxes as the volume fluxes are
+    // stored (the same expression and rounding; the z faces from the
+    // corrector's own node sums), so that the advection's pre/post volumes
+    // cancel against this volume change
+    auto stored = [&](double area, double s) { return (double)st<F>(0.125 * dt * area * s); };
+    left_flux = (double)vfx0;
+    right_flux = stored(g.xa, xsum(j + 1));
+    bottom_flux = (double)vfy0;
+    top_flux = stored(g.ya, ysum(k + 1));
+    back_flux = stored(g.za, sz);
+    front_flux = stored(g.za, zsum(l + 1));
+  }
   const double total_flux = right_flux - left_flux + top_flux - bottom_flux + front_flux - back_flux;
   const double vol = g.vol;
   const double vol_change_s = vol / (vol + total_flux);
@@ -695,7 +713,7 @@ __device__ __forceinline__ double cell_product(const Geom& g, int variant, const
 // DIR 2: p = k, c = l; DIR 3: p = l, c = k. Sums keep the reference order
 // (advec_mom_kernel.f90:166-190 and the y/z forms).
 template <class S, int DIR, int VAR, class M>
-__global__ void __launch_bounds__(BX * BY, M::kFlat ? 5 : 6) k_mom_node_march(M m, GeomArrays ga,
+__global__ void __launch_bounds__(BX * BY, M::kFlat || sizeof(typename S::arith_t) == 4 ? 5 : 6) k_mom_node_march(M m, GeomArrays ga,
     const typename S::mf_t* __restrict__ mf, const typename S::rho_t* __restrict__ density1,
     const typename S::vf_t* __restrict__ vfx, const typename S::vf_t* __restrict__ vfy,
     const typename S::vf_t* __restrict__ vfz, typename S::nd_t* __restrict__ node_flux,
@@ -835,7 +853,7 @@ __device__ __forceinline__ A mom_flux_at(A nf, A nmpre_i, A nmpre_ip1, A vm1, A 
 // Velocity pass for direction y or z, marching along the sweep axis with the
 // previous momentum fluxes and the velocity window in registers.
 template <class S, int DIR, class M>
-__global__ void __launch_bounds__(BX * BY, 3) k_mom_vel3_march(M m, GeomArrays ga,
+__global__ void __launch_bounds__(BX * BY, sizeof(typename S::arith_t) == 4 && !M::kFlat ? 5 : 3) k_mom_vel3_march(M m, GeomArrays ga,
     const typename S::nd_t* __restrict__ node_flux, const typename S::nd_t* __restrict__ node_mass_post,
     const typename S::nd_t* __restrict__ node_mass_pre, const typename S::vel_t* __restrict__ u_in,
     const typename S::vel_t* __restrict__ v_in, const typename S::vel_t* __restrict__ w_in,
@@ -923,7 +941,7 @@ __global__ void __launch_bounds__(BX * BY, 3) k_mom_vel3_march(M m, GeomArrays g
 // in [pmin, pmax] (c <= cmax); face c1+1 is computed by both neighbours and
 // stored by the segment that starts there.
 template <class S, int DIR, int VAR, class M>
-__global__ void __launch_bounds__(BX * BY, sizeof(typename S::arith_t) == 4 ? 4 : 3) k_cell_sweep_march(M m, GeomArrays ga,
+__global__ void __launch_bounds__(BX * BY, sizeof(typename S::arith_t) == 4 && M::kFlat ? 4 : 3) k_cell_sweep_march(M m, GeomArrays ga,
     typename S::rho_t* __restrict__ density1, typename S::ene_t* __restrict__ energy1,
     const typename S::vf_t* __restrict__ vfx, const typename S::vf_t* __restrict__ vfy,
     const typename S::vf_t* __restrict__ vfz, typename S::mf_t* __restrict__ mass_flux,

@@ -324,13 +324,37 @@ __global__ void __launch_bounds__(BX * BY, 8) k_pdv(Geom g, Box b, int predict, 
     top_flux = YF(k + 1) * 0.125 * dt * 0.5;
     back_flux = ZF(l) * 0.125 * dt * 0.5;
     front_flux = ZF(l + 1) * 0.125 * dt * 0.5;
-  } else {
+  } else if (sizeof(typename S::vf_t) == 8) {
     left_flux = XF(j) * 0.125 * dt;
     right_flux = XF(j + 1) * 0.125 * dt;
     bottom_flux = YF(k) * 0.125 * dt;
     top_flux = YF(k + 1) * 0.125 * dt;
     back_flux = ZF(l) * 0.125 * dt;
     front_flux = ZF(l + 1) * 0.125 * dt;
+  } else {
+    // FP32 volume fluxes (mixed storage): the corrector's face fluxes as
+    // k_flux_calc stores them (its expression and rounding; the z faces from
+    // the corrector's own node sums), so that the advection's pre/post
+    // volumes cancel against this volume change
+    using F = typename S::vf_t;
+#define XS(jj) (0.125 * dt * E(ga.xarea, jj, k, l) *                                              \
+    (L(xvel0, jj, k, l) + L(xvel0, jj, k + 1, l) + L(xvel0, jj, k, l + 1) + L(xvel0, jj, k + 1, l + 1) + \
+     L(xb, jj, k, l) + L(xb, jj, k + 1, l) + L(xb, jj, k, l + 1) + L(xb, jj, k + 1, l + 1)))
+#define YS(kk) (0.125 * dt * E(ga.yarea, j, kk, l) *                                              \
+    (L(yvel0, j, kk, l) + L(yvel0, j + 1, kk, l) + L(yvel0, j, kk, l + 1) + L(yvel0, j + 1, kk, l + 1) + \
+     L(yb, j, kk, l) + L(yb, j + 1, kk, l) + L(yb, j, kk, l + 1) + L(yb, j + 1, kk, l + 1)))
+#define ZS(ll) (0.125 * dt * E(ga.zarea, j, k, ll) *                                              \
+    (L(zvel0, j, k, ll) + L(zvel0, j + 1, k, ll) + L(zvel0, j, k + 1, ll) + L(zvel0, j + 1, k + 1, ll) + \
+     L(zb, j, k, ll) + L(zb, j + 1, k, ll) + L(zb, j, k + 1, ll) + L(zb, j + 1, k + 1, ll)))
+    left_flux = (double)st<F>(XS(j));
+    right_flux = (double)st<F>(XS(j + 1));
+    bottom_flux = (double)st<F>(YS(k));
+    top_flux = (double)st<F>(YS(k + 1));
+    back_flux = (double)st<F>(ZS(l));
+    front_flux = (double)st<F>(ZS(l + 1));
+#undef XS
+#undef YS
+#undef ZS
   }
 #undef XF
 #undef YF

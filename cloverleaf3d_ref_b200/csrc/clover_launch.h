@@ -124,10 +124,13 @@ struct F64 {
 };
 
 // Storage policy of the mixed-precision native path: FP32 storage for the
-// stencilled fields (energy, pressure, viscosity, sound speed, velocities),
-// FP64 kept where conservation needs it: density, the work arrays (pre/post
-// volumes) and the volume fluxes, whose differences form the pre/post volumes
-// and must cancel against the PdV volume change for mass to be conserved.
+// stencilled fields (energy, pressure, viscosity, sound speed, velocities)
+// and the volume fluxes, FP64 kept where conservation needs it: density, the
+// work arrays and all the arithmetic on volumes. The volume fluxes' differences
+// form the advection's pre/post volumes and must cancel against the PdV volume
+// change for mass to be conserved: the PdV corrector takes its face fluxes as
+// they are stored (flux_calc's expression, rounded to FP32), so the two see
+// the same values and the volumes are formed from them in FP64.
 // The cell sweeps update mass and energy from their FP64 face fluxes; the
 // mass flux is stored in FP32 (mf_t) for the momentum sweep, which forms its
 // node fluxes and node masses from it in FP64. The y/z momentum sweeps hand
@@ -135,13 +138,15 @@ struct F64 {
 // arithmetic: they are stored as FP32 (nd_t), the rounding the velocity pass
 // would apply. The momentum advection's flux limiter and velocity update,
 // accelerate's gradients and the EOS/viscosity/dt stencils run in FP32
-// (arith_t); all other arithmetic is FP64.
+// (arith_t), with FP32 division and square root to within 2 ulp and FP32
+// subnormals flushed (the library's single-precision build flags); all other
+// arithmetic is FP64.
 struct F32Mixed {
   using rho_t = double;
   using ene_t = float;
   using cs_t = float;
   using vel_t = float;
-  using vf_t = double;
+  using vf_t = float;
   using mf_t = float;
   using wk_t = double;
   using nd_t = float;

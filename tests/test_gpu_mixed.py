@@ -1,10 +1,11 @@
 """GPU: the FP32-storage mixed-precision path against the FP64 path.
 
-FP32 storage for energy, pressure, viscosity, sound speed, velocities, mass
-fluxes and the momentum sweep's node values, FP32 arithmetic in the EOS,
-viscosity, dt, PdV predictor, accelerate and momentum stencils; FP64 for
-density, volume fluxes, pre/post volumes, the cell mass/energy update and the
-node masses.
+FP32 storage for energy, pressure, viscosity, sound speed, velocities, volume
+and mass fluxes and the momentum sweep's node values, FP32 arithmetic (division
+and square root within 2 ulp) in the EOS, viscosity, dt, PdV predictor,
+accelerate and momentum stencils; FP64 for density, pre/post volumes, the cell
+mass/energy update and the node masses. The PdV corrector takes the volume
+fluxes as stored, so the advection's volumes cancel against its volume change.
 Bar: every field_summary quantity within 1e-5 relative of FP64 at every
 summary step; total mass equal to FP64's to 1e-8 relative, and on a deck
 where FP64 conserves mass, conserved to 1e-12 relative itself.
