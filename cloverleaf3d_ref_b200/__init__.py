@@ -200,6 +200,25 @@ def _declare(L):
     L.clover_dropin_read_field.argtypes = [P, ctypes.c_int, P, ctypes.c_longlong]
     L.clover_dropin_read_field.restype = ctypes.c_int
     L.clover_dropin_destroy.argtypes = [P]
+    I = ctypes.c_int
+    L.clover_decompose.argtypes = [I, I, I, I, P, P, P]
+    L.clover_decompose.restype = I
+    L.clover_bricks_create.argtypes = [P, I]
+    L.clover_bricks_create.restype = P
+    L.clover_bricks_run.argtypes = [P, I]
+    L.clover_bricks_run.restype = I
+    L.clover_bricks_count.argtypes = [P, P]
+    L.clover_bricks_count.restype = I
+    L.clover_bricks_extent.argtypes = [P, I, P, P]
+    L.clover_bricks_extent.restype = I
+    L.clover_bricks_dt_history.argtypes = [P, P, I]
+    L.clover_bricks_dt_history.restype = I
+    L.clover_bricks_summaries.argtypes = [P, P, P, I]
+    L.clover_bricks_summaries.restype = I
+    L.clover_bricks_read_field.argtypes = [P, I, I, P, ctypes.c_longlong]
+    L.clover_bricks_read_field.restype = I
+    L.clover_bricks_destroy.argtypes = [P]
+    L.clover_gpu_face_copy.argtypes = [P, P, P, P, I, I, I]
     L.clover_gpu_status.restype = ctypes.c_int
     L.clover_gpu_error_string.restype = ctypes.c_char_p
     L.clover_gpu_invalidate.argtypes = [P]
@@ -546,6 +565,102 @@ def draw_decks(n, seed, cells=(24, 128), end_step=150, summary_frequency=10):
             zmin=0.0, zmax=10.0, initial_timestep=0.04, timestep_rise=1.5, max_timestep=0.04,
             end_step=end_step, end_time=1.0e6, summary_frequency=summary_frequency))
     return out
+
+
+def decompose(x_cells, y_cells, z_cells, n_chunks):
+    """clover_decompose (clover.f90:108-256): the chunk grid (3,), each chunk's
+    global cell range (n, 6: left, right, bottom, top, back, front) and its
+    neighbours (n, 6; chunk ids from 1, -1 for an external face). Host only."""
+    grid = np.zeros(3, dtype=np.int32)
+    ext = np.zeros((n_chunks, 6), dtype=np.int32)
+    nbr = np.zeros((n_chunks, 6), dtype=np.int32)
+    rc = lib().clover_decompose(x_cells, y_cells, z_cells, n_chunks, grid.ctypes.data,
+                                ext.ctypes.data, nbr.ctypes.data)
+    if rc != 0:
+        raise CloverError("cannot decompose %dx%dx%d cells into %d chunks"
+                          % (x_cells, y_cells, z_cells, n_chunks))
+    return grid, ext, nbr
+
+
+class Bricks:
+    """One deck decomposed into n bricks (``decompose``) and run by the
+    reference's decomposed control flow in this process: the drop-in driver's
+    calls on every brick, halo messages exchanged between the bricks on the
+    device before each update_halo's reflective faces, dt the minimum over the
+    bricks, the summaries their sum."""
+
+    def __init__(self, deck, n_chunks):
+        L = lib()
+        L.clover_gpu_clear_status()
+        self.deck = deck
+        self.h = L.clover_bricks_create(ctypes.byref(deck.s), n_chunks)
+        if not self.h:
+            raise CloverError("bricks start failed: " + L.clover_gpu_error_string().decode())
+        grid = np.zeros(3, dtype=np.int32)
+        self.n = L.clover_bricks_count(self.h, grid.ctypes.data)
+        self.grid = tuple(int(v) for v in grid)
+        self.extents, self.neighbours = [], []
+        for i in range(self.n):
+            e = np.zeros(6, dtype=np.int32)
+            nb = np.zeros(6, dtype=np.int32)
+            L.clover_bricks_extent(self.h, i, e.ctypes.data, nb.ctypes.data)
+            self.extents.append(tuple(int(v) for v in e))
+            self.neighbours.append(tuple(int(v) for v in nb))
+
+    def run(self, max_steps=2 ** 30):
+        n = lib().clover_bricks_run(self.h, max_steps)
+        st = lib().clover_gpu_status()
+        if st & ~0x4:
+            raise CloverError("bricks: " + lib().clover_gpu_error_string().decode())
+        return n
+
+    def dt_history(self, cap=1 << 20):
+        out = np.zeros(cap)
+        n = lib().clover_bricks_dt_history(self.h, out.ctypes.data, cap)
+        return out[:n]
+
+    def summaries(self, cap=100000):
+        out = np.zeros((cap, 5))
+        st = np.zeros(cap, dtype=np.int32)
+        n = lib().clover_bricks_summaries(self.h, out.ctypes.data, st.ctypes.data, cap)
+        return out[:n], st[:n]
+
+    def brick_field(self, i, name):
+        """Field `name` of brick i in its own reference layout."""
+        e = self.extents[i]
+        a = np.zeros(field_shape(name, e[1] - e[0] + 1, e[3] - e[2] + 1, e[5] - e[4] + 1),
+                     order="F")
+        if lib().clover_bricks_read_field(self.h, i, FIELD_IDS[name], a.ctypes.data, a.size) != 0:
+            raise CloverError("bricks read_field failed")
+        return a
+
+    def field(self, name):
+        """Field `name` of the whole deck in the reference layout: each
+        brick's own cells (and nodes / faces up to its upper boundary) at its
+        global place; the halo of the deck left zero."""
+        s = self.deck.s
+        g = np.zeros(field_shape(name, s.x_cells, s.y_cells, s.z_cells), order="F")
+        extra = [g.shape[a] - (n + 4) for a, n in enumerate((s.x_cells, s.y_cells, s.z_cells))]
+        for i, e in enumerate(self.extents):
+            b = self.brick_field(i, name)
+            src, dst = [], []
+            for a in range(3):
+                n_b = e[2 * a + 1] - e[2 * a] + 1 + extra[a]
+                src.append(slice(2, 2 + n_b))  # local index 1.. (array index = index + 1)
+                dst.append(slice(e[2 * a] + 1, e[2 * a] + 1 + n_b))
+            g[tuple(dst)] = b[tuple(src)]
+        return g
+
+    def close(self):
+        if self.h:
+            lib().clover_bricks_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class DropIn:

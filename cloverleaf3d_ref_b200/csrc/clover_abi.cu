@@ -6,6 +6,7 @@
 #include <mutex>
 #include <string>
 #include <unordered_map>
+#include <vector>
 
 #include "../../include/clover_kernels.h"
 #include "clover_launch.h"
@@ -25,6 +26,7 @@ struct Mirror {
   HostShape shape{};        // largest declared shape seen
   int planes = 0;           // host planes copied up so far
   bool pinned = false;
+  Geom g{};                 // the bounds of the chunk the array belongs to (3D arrays)
 };
 
 struct Context {
@@ -32,11 +34,14 @@ struct Context {
   Geom g{};
   cudaStream_t stream = nullptr;
   std::unordered_map<const void*, Mirror> mirrors;
+  std::vector<void*> scratch;  // arrays standing in for mirrors passed with another chunk's bounds
   unsigned long long* d_key = nullptr;
   double* d_partials = nullptr;
   double* d_sum = nullptr;
   double* stage = nullptr;  // contiguous copy of host planes on their way up or down
   size_t stage_bytes = 0;
+  double* msg = nullptr;    // one halo message (pack_kernel.f90) on the device
+  size_t msg_bytes = 0;
   int status = 0;
   std::string err;
   bool pin_host = true;
@@ -61,10 +66,17 @@ bool check(cudaError_t e, const char* what) {
 
 void check_launch(const char* what) { check(cudaGetLastError(), what); }
 
-// Create the context on first use; every call must pass the same bounds.
+// Create the context on first use. Each call's bounds select the geometry of
+// that call: several chunks may share the process (the reference runs one
+// chunk per task; the brick driver runs the bricks of a deck in one process),
+// and every array belongs to the chunk whose bounds it was first passed with.
 bool enter(const int* x_min, const int* x_max, const int* y_min, const int* y_max,
            const int* z_min, const int* z_max) {
   Context& c = ctx();
+  if (*x_max < *x_min || *y_max < *y_min || *z_max < *z_min) {
+    set_error(CLOVER_STATUS_BAD_ARG, "empty chunk bounds");
+    return false;
+  }
   if (!c.ready) {
     int n = 0;
     if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
@@ -84,11 +96,14 @@ bool enter(const int* x_min, const int* x_max, const int* y_min, const int* y_ma
   }
   const Geom& g = c.g;
   if (g.x_min != *x_min || g.x_max != *x_max || g.y_min != *y_min || g.y_max != *y_max ||
-      g.z_min != *z_min || g.z_max != *z_max) {
-    set_error(CLOVER_STATUS_BOUNDS, "call with bounds of another chunk");
-    return false;
-  }
+      g.z_min != *z_min || g.z_max != *z_max)
+    c.g = make_geom(*x_min, *x_max, *y_min, *y_max, *z_min, *z_max);
   return true;
+}
+
+bool same_chunk(const Geom& a, const Geom& b) {
+  return a.x_min == b.x_min && a.x_max == b.x_max && a.y_min == b.y_min && a.y_max == b.y_max &&
+         a.z_min == b.z_min && a.z_max == b.z_max;
 }
 
 bool is_device_pointer(const void* p) {
@@ -141,16 +156,16 @@ static void xfer3d(const void* host, Mirror& m, int p0, int p1, bool up) {
     c.stage_bytes = bytes;
   }
   char* hp = (char*)host + host_plane * p0;
-  double* dp = m.dev + c.g.pxy * p0;
+  double* dp = m.dev + m.g.pxy * p0;
   const long long rows = (long long)s.hy * (p1 - p0);
   if (up) {
     check(cudaMemcpyAsync(c.stage, hp, bytes, cudaMemcpyHostToDevice, c.stream), "upload");
-    k_rows_to_pitched<<<148 * 8, 256, 0, c.stream>>>(c.stage, dp, s.hx, s.hy, rows, c.g.px,
-                                                     c.g.pxy);
+    k_rows_to_pitched<<<148 * 8, 256, 0, c.stream>>>(c.stage, dp, s.hx, s.hy, rows, m.g.px,
+                                                     m.g.pxy);
     check_launch("upload rows");
   } else {
-    k_pitched_to_rows<<<148 * 8, 256, 0, c.stream>>>(dp, c.stage, s.hx, s.hy, rows, c.g.px,
-                                                     c.g.pxy);
+    k_pitched_to_rows<<<148 * 8, 256, 0, c.stream>>>(dp, c.stage, s.hx, s.hy, rows, m.g.px,
+                                                     m.g.pxy);
     check_launch("download rows");
     check(cudaMemcpyAsync(hp, c.stage, bytes, cudaMemcpyDeviceToHost, c.stream), "download");
   }
@@ -164,6 +179,7 @@ static double* dev3(double* host, int hx, int hy, int hz) {
   if (it == c.mirrors.end()) {
     if (is_device_pointer(host)) return host;
     Mirror m;
+    m.g = c.g;
     const long long elems = array_elems(c.g) + kFrontPad<double>;
     if (!check(cudaMalloc(&m.raw, (size_t)elems * 8), "mirror malloc")) return nullptr;
     m.dev = (double*)m.raw + kFrontPad<double>;
@@ -181,6 +197,17 @@ static double* dev3(double* host, int hx, int hy, int hz) {
     it = c.mirrors.emplace(host, m).first;
   }
   Mirror& m = it->second;
+  if (!same_chunk(m.g, c.g)) {
+    // an array of another chunk: the call runs on a zeroed array of this
+    // call's bounds instead (so no access leaves an allocation) and fails
+    set_error(CLOVER_STATUS_BOUNDS, "array passed with the bounds of another chunk");
+    void* raw = nullptr;
+    const long long elems = array_elems(c.g) + kFrontPad<double>;
+    if (!check(cudaMalloc(&raw, (size_t)elems * 8), "scratch malloc")) return nullptr;
+    check(cudaMemsetAsync(raw, 0, (size_t)elems * 8, c.stream), "scratch clear");
+    c.scratch.push_back(raw);
+    return (double*)raw + kFrontPad<double>;
+  }
   if (hz > m.shape.hz) {
     // A later declaration covers more planes (e.g. post_ener is declared to
     // z_max+2, the same work array elsewhere to z_max+3): a copy may not
@@ -211,9 +238,18 @@ static double* dev1(double* host, int n) {
     if (!check(cudaMalloc(&m.raw, (size_t)(n + 32) * 8), "mirror malloc")) return nullptr;
     m.dev = (double*)m.raw;
     m.shape = HostShape{n, 1, 1, true};
+    m.shape.hy = n + 32;  // capacity (1D mirrors)
     it = c.mirrors.emplace(host, m).first;
   }
   Mirror& m = it->second;
+  if (n > m.shape.hy) {  // a 1D array of a smaller chunk passed with larger bounds
+    set_error(CLOVER_STATUS_BOUNDS, "array passed with the bounds of another chunk");
+    void* raw = nullptr;
+    if (!check(cudaMalloc(&raw, (size_t)(n + 32) * 8), "scratch malloc")) return nullptr;
+    check(cudaMemsetAsync(raw, 0, (size_t)(n + 32) * 8, c.stream), "scratch clear");
+    c.scratch.push_back(raw);
+    return (double*)raw;
+  }
   if (m.planes == 0 || n > m.shape.hx) {
     m.shape.hx = n > m.shape.hx ? n : m.shape.hx;
     check(cudaMemcpyAsync(m.dev, host, (size_t)m.shape.hx * 8, cudaMemcpyHostToDevice, c.stream),
@@ -223,6 +259,182 @@ static double* dev1(double* host, int n) {
   return m.dev;
 }
 
+}  // namespace clover
+
+
+namespace clover {
+// ---------------------------------------------------------------------------
+// Halo messages between chunks (pack_kernel.f90). Side 0..5 = left, right,
+// bottom, top, back, front. A message holds `depth` layers of the field next
+// to that side, over the other two axes' full extents including their halos;
+// element (j,k,l) of the loop space goes to the reference's 1-based buffer
+// index of pack_kernel.f90 (:78 left/right, :310 bottom/top, :542 back/front).
+// pack: field -> buf, unpack: buf -> field; buf[0] holds buffer index `lo`.
+struct FaceMsg {
+  int side, depth, xi, yi, zi;  // x_inc, y_inc, z_inc of the field type
+  int off_a, off_b;             // left/right: y, z offsets; bottom/top: x, z; back/front: x, y
+  int gx, gy, gz;               // g_x_max, g_y_max, g_z_max
+  long long base, lo;           // buffer_offset; the first buffer index the message covers
+  int n0, n1, n2;               // extents of the loop space (j, k, l)
+  int j0, k0, l0;               // their first values
+};
+
+__host__ __device__ inline long long face_index(const FaceMsg& f, int j, int k, int l) {
+  const int d = f.depth;
+  if (f.side < 2)
+    return f.base + (j + (long long)(k + f.off_a + d - 1) * d) +
+           (long long)(l + f.off_b + d - 1) * (f.gy + f.yi + 2 * d) * d;
+  const long long rx = f.gx + f.xi + 2 * d;
+  if (f.side < 4)
+    return f.base + (j + f.off_a + d) + (long long)(l + f.off_b - 1 + d) * rx +
+           (long long)(k - 1) * (rx * (f.gz + f.zi + 2 * d));
+  return f.base + (j + f.off_a + d) + (long long)(k + f.off_b - 1 + d) * rx +
+         (long long)(l - 1) * (rx * (f.gy + f.yi + 2 * d));
+}
+
+// The field element a message element comes from (pack) or goes to (unpack).
+__device__ inline void face_cell(const Geom& g, const FaceMsg& f, bool pack, int& j, int& k, int& l) {
+  switch (f.side) {
+    case 0: j = pack ? g.x_min + f.xi - 1 + j : g.x_min - j; break;
+    case 1: j = pack ? g.x_max + 1 - j : g.x_max + f.xi + j; break;
+    case 2: k = pack ? g.y_min + f.yi - 1 + k : g.y_min - k; break;
+    case 3: k = pack ? g.y_max + 1 - k : g.y_max + f.yi + k; break;
+    case 4: l = pack ? g.z_min + f.zi - 1 + l : g.z_min - l; break;
+    default: l = pack ? g.z_max + 1 - l : g.z_max + f.zi + l; break;
+  }
+}
+
+__global__ void k_face_msg(Geom g, FaceMsg f, double* __restrict__ field, double* __restrict__ buf,
+                           int pack) {
+  const long long n = (long long)f.n0 * f.n1 * f.n2;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int a = (int)(i % f.n0), b = (int)((i / f.n0) % f.n1), c = (int)(i / ((long long)f.n0 * f.n1));
+    int j = f.j0 + a, k = f.k0 + b, l = f.l0 + c;
+    const long long q = face_index(f, j, k, l) - f.lo;
+    face_cell(g, f, pack != 0, j, k, l);
+    double* e = field + off3(g, j, k, l);
+    if (pack) buf[q] = *e;
+    else *e = buf[q];
+  }
+}
+
+namespace {
+
+// The loop space of pack_kernel.f90 for one side (j innermost), and the
+// buffer index range it covers (the index grows with every loop variable).
+FaceMsg face_msg(const Geom& g, int side, int depth, int xi, int yi, int zi, int off_a, int off_b,
+                 int gx, int gy, int gz, long long base) {
+  FaceMsg f;
+  f.side = side; f.depth = depth; f.xi = xi; f.yi = yi; f.zi = zi;
+  f.off_a = off_a; f.off_b = off_b; f.gx = gx; f.gy = gy; f.gz = gz; f.base = base;
+  const int d = depth;
+  f.j0 = side < 2 ? 1 : g.x_min - d;
+  f.n0 = side < 2 ? d : (g.x_max + xi + d) - (g.x_min - d) + 1;
+  f.k0 = (side == 2 || side == 3) ? 1 : g.y_min - d;
+  f.n1 = (side == 2 || side == 3) ? d : (g.y_max + yi + d) - (g.y_min - d) + 1;
+  f.l0 = side >= 4 ? 1 : g.z_min - d;
+  f.n2 = side >= 4 ? d : (g.z_max + zi + d) - (g.z_min - d) + 1;
+  f.lo = 0;
+  f.lo = face_index(f, f.j0, f.k0, f.l0);
+  return f;
+}
+
+long long face_len(const FaceMsg& f) {
+  return face_index(f, f.j0 + f.n0 - 1, f.k0 + f.n1 - 1, f.l0 + f.n2 - 1) - f.lo + 1;
+}
+
+// x_inc, y_inc, z_inc of pack_kernel.f90's field types; false if unknown
+bool field_incs(int type, int& xi, int& yi, int& zi) {
+  switch (type) {
+    case 1: xi = 0; yi = 0; zi = 0; return true;  // cell
+    case 2: xi = 1; yi = 1; zi = 1; return true;  // vertex
+    case 3: xi = 1; yi = 0; zi = 0; return true;  // x face
+    case 4: xi = 0; yi = 1; zi = 0; return true;  // y face
+    case 5: xi = 0; yi = 0; zi = 1; return true;  // z face
+  }
+  return false;
+}
+
+// The device copy of a 3D field argument of the given pack_kernel field type.
+double* dev_of_type(double* host, int type) {
+  const Geom& g = ctx().g;
+  const int nx = g.x_max - g.x_min + 1, ny = g.y_max - g.y_min + 1, nz = g.z_max - g.z_min + 1;
+  int xi, yi, zi;
+  field_incs(type, xi, yi, zi);
+  return dev3(host, nx + 4 + xi, ny + 4 + yi, nz + 4 + zi);
+}
+
+double* msg_buffer(long long n) {
+  Context& c = ctx();
+  const size_t bytes = (size_t)n * 8;
+  if (bytes > c.msg_bytes) {
+    cudaStreamSynchronize(c.stream);
+    cudaFree(c.msg);
+    c.msg = nullptr;
+    c.msg_bytes = 0;
+    if (!check(cudaMalloc(&c.msg, bytes), "message malloc")) return nullptr;
+    c.msg_bytes = bytes;
+  }
+  return c.msg;
+}
+
+void launch_face(const Geom& g, const FaceMsg& f, double* field, double* buf, bool pack) {
+  const long long n = (long long)f.n0 * f.n1 * f.n2;
+  const int blocks = (int)((n + 255) / 256 < 148 * 8 ? (n + 255) / 256 : 148 * 8);
+  k_face_msg<<<blocks > 0 ? blocks : 1, 256, 0, ctx().stream>>>(g, f, field, buf, pack ? 1 : 0);
+  check_launch(pack ? "pack" : "unpack");
+}
+
+// clover_pack_message_* / clover_unpack_message_* with a host buffer: the
+// message is formed on the device and copied to (or from) the caller's buffer
+// at its 1-based buffer_offset indices.
+void message(const int* x_min, const int* x_max, const int* y_min, const int* y_max,
+             const int* z_min, const int* z_max, double* field, double* buffer,
+             const int* cell_data, const int* vertex_data, const int* x_face_data,
+             const int* y_face_data, const int* z_face_data, const int* depth,
+             const int* field_type, const int* buffer_offset, const int* off_a, const int* off_b,
+             const int* g_x_max, const int* g_y_max, const int* g_z_max, int side, bool pack) {
+  if (!enter(x_min, x_max, y_min, y_max, z_min, z_max)) return;
+  Context& c = ctx();
+  int type = 0;
+  if (*field_type == *cell_data) type = 1;
+  else if (*field_type == *vertex_data) type = 2;
+  else if (*field_type == *x_face_data) type = 3;
+  else if (*field_type == *y_face_data) type = 4;
+  else if (*field_type == *z_face_data) type = 5;
+  if (type == 0 || *depth < 1 || *depth > 2) {
+    set_error(CLOVER_STATUS_BAD_ARG, "pack/unpack: unknown field type or depth");
+    return;
+  }
+  int xi, yi, zi;
+  field_incs(type, xi, yi, zi);
+  const FaceMsg f = face_msg(c.g, side, *depth, xi, yi, zi, *off_a, *off_b, *g_x_max, *g_y_max,
+                             *g_z_max, *buffer_offset);
+  if (f.lo < 1) {
+    set_error(CLOVER_STATUS_BAD_ARG, "pack/unpack: buffer index below 1");
+    return;
+  }
+  const long long n = face_len(f);
+  double* d_field = dev_of_type(field, type);
+  double* d_buf = msg_buffer(n);
+  if (!d_field || !d_buf) return;
+  double* h = buffer + (f.lo - 1);
+  if (pack) {
+    // the index range can have gaps (tile offsets, g_*_max beyond the tile)
+    // that hold other messages: the range goes up first, so that copying it
+    // back rewrites those entries with their own values
+    check(cudaMemcpyAsync(d_buf, h, (size_t)n * 8, cudaMemcpyHostToDevice, c.stream), "message up");
+    launch_face(c.g, f, d_field, d_buf, true);
+    check(cudaMemcpyAsync(h, d_buf, (size_t)n * 8, cudaMemcpyDeviceToHost, c.stream), "message down");
+    check(cudaStreamSynchronize(c.stream), "message sync");
+  } else {
+    check(cudaMemcpyAsync(d_buf, h, (size_t)n * 8, cudaMemcpyHostToDevice, c.stream), "message up");
+    launch_face(c.g, f, d_field, d_buf, false);
+  }
+}
+
+}  // namespace
 }  // namespace clover
 
 using namespace clover;
@@ -552,6 +764,62 @@ void clover_generate_chunk_kernel(const int* x_min, const int* x_max, const int*
   check_launch("generate_chunk");
 }
 
+
+#define MSG_ARGS                                                                                  \
+  const int *x_min, const int *x_max, const int *y_min, const int *y_max, const int *z_min,      \
+      const int *z_max, double *field, double *buffer, const int *cell_data,                     \
+      const int *vertex_data, const int *x_face_data, const int *y_face_data,                    \
+      const int *z_face_data, const int *depth, const int *field_type, const int *buffer_offset, \
+      const int *off_a, const int *off_b, const int *g_x_max, const int *g_y_max,                \
+      const int *g_z_max
+#define MSG_PASS                                                                                  \
+  x_min, x_max, y_min, y_max, z_min, z_max, field, buffer, cell_data, vertex_data, x_face_data,  \
+      y_face_data, z_face_data, depth, field_type, buffer_offset, off_a, off_b, g_x_max,         \
+      g_y_max, g_z_max
+void clover_pack_message_left(MSG_ARGS) { message(MSG_PASS, 0, true); }
+void clover_unpack_message_left(MSG_ARGS) { message(MSG_PASS, 0, false); }
+void clover_pack_message_right(MSG_ARGS) { message(MSG_PASS, 1, true); }
+void clover_unpack_message_right(MSG_ARGS) { message(MSG_PASS, 1, false); }
+void clover_pack_message_bottom(MSG_ARGS) { message(MSG_PASS, 2, true); }
+void clover_unpack_message_bottom(MSG_ARGS) { message(MSG_PASS, 2, false); }
+void clover_pack_message_top(MSG_ARGS) { message(MSG_PASS, 3, true); }
+void clover_unpack_message_top(MSG_ARGS) { message(MSG_PASS, 3, false); }
+void clover_pack_message_back(MSG_ARGS) { message(MSG_PASS, 4, true); }
+void clover_unpack_message_back(MSG_ARGS) { message(MSG_PASS, 4, false); }
+void clover_pack_message_front(MSG_ARGS) { message(MSG_PASS, 5, true); }
+void clover_unpack_message_front(MSG_ARGS) { message(MSG_PASS, 5, false); }
+#undef MSG_PASS
+#undef MSG_ARGS
+
+void clover_gpu_face_copy(const int* src_bounds, double* src, const int* dst_bounds, double* dst,
+                          int side, int field_type, int depth) {
+  const int* a = src_bounds;
+  const int* b = dst_bounds;
+  int xi, yi, zi;
+  if (side < 0 || side > 5 || depth < 1 || depth > 2 || !field_incs(field_type, xi, yi, zi)) {
+    set_error(CLOVER_STATUS_BAD_ARG, "face_copy: bad side, depth or field type");
+    return;
+  }
+  if (!enter(a, a + 1, a + 2, a + 3, a + 4, a + 5)) return;
+  Context& c = ctx();
+  const Geom gs = c.g;
+  const FaceMsg fs = face_msg(gs, side, depth, xi, yi, zi, 0, 0, gs.x_max, gs.y_max, gs.z_max, 1);
+  double* d_src = dev_of_type(src, field_type);
+  if (!enter(b, b + 1, b + 2, b + 3, b + 4, b + 5)) return;
+  const Geom gd = c.g;
+  const int other = side ^ 1;  // the receiver unpacks on the opposite side
+  const FaceMsg fd = face_msg(gd, other, depth, xi, yi, zi, 0, 0, gd.x_max, gd.y_max, gd.z_max, 1);
+  if (face_len(fs) != face_len(fd)) {
+    set_error(CLOVER_STATUS_BAD_ARG, "face_copy: the two chunks' faces differ in extent");
+    return;
+  }
+  double* d_dst = dev_of_type(dst, field_type);
+  double* d_buf = msg_buffer(face_len(fs));
+  if (!d_src || !d_dst || !d_buf) return;
+  launch_face(gs, fs, d_src, d_buf, true);
+  launch_face(gd, fd, d_dst, d_buf, false);
+}
+
 int clover_gpu_status(void) { return ctx().status; }
 
 const char* clover_gpu_error_string(void) { return ctx().err.c_str(); }
@@ -600,12 +868,17 @@ void clover_gpu_release(void) {
     cudaFree(kv.second.raw);
   }
   c.mirrors.clear();
+  for (void* p : c.scratch) cudaFree(p);
+  c.scratch.clear();
   cudaFree(c.d_key);
   cudaFree(c.d_partials);
   cudaFree(c.d_sum);
   cudaFree(c.stage);
   c.stage = nullptr;
   c.stage_bytes = 0;
+  cudaFree(c.msg);
+  c.msg = nullptr;
+  c.msg_bytes = 0;
   cudaStreamDestroy(c.stream);
   c.ready = false;
 }
@@ -624,7 +897,7 @@ void clover_gpu_mirror_stats(int* arrays, long long* bytes) {
   long long b = 0;
   for (auto& kv : c.mirrors)
     b += kv.second.shape.one_d ? (long long)(kv.second.shape.hx + 32) * 8
-                               : (array_elems(c.g) + kFrontPad<double>) * 8;
+                               : (array_elems(kv.second.g) + kFrontPad<double>) * 8;
   *arrays = (int)c.mirrors.size();
   *bytes = b;
 }

@@ -179,6 +179,33 @@ int clover_dropin_summaries(clover_dropin *d, double *out5, int *steps, int cap)
 int clover_dropin_read_field(clover_dropin *d, int field_id, double *out, long long n);
 void clover_dropin_destroy(clover_dropin *d);
 
+/* ---- Brick decomposition of one deck (clover.f90's MPI layer) ----
+ * clover_decompose, clover.f90:108-256: the chunk grid chunks_xyz[3] for
+ * n_chunks chunks, and per chunk (ids 1..n in x-fastest order) its global
+ * cell range extents[6*i..] = left, right, bottom, top, back, front and its
+ * neighbours[6*i..] (left, right, bottom, top, back, front; -1 = external
+ * face). Host only. Returns 0, or -1 when a chunk would be empty. */
+int clover_decompose(int x_cells, int y_cells, int z_cells, int n_chunks, int *chunks_xyz,
+                     int *extents, int *neighbours);
+/* The decomposed run of the reference over n_chunks bricks of one deck in
+ * this process: the drop-in driver's control flow on every brick, each
+ * update_halo exchanging the bricks' faces on the device (pack_kernel.f90's
+ * messages, x then y then z) before the reflective halos of the external
+ * faces, dt the minimum over the bricks (clover_min), the summaries their sum
+ * (clover_sum). NULL on failure (clover_gpu_error_string). */
+typedef struct clover_bricks clover_bricks;
+clover_bricks *clover_bricks_create(const clover_deck *deck, int n_chunks);
+int clover_bricks_run(clover_bricks *w, int max_steps);
+/* Number of bricks; chunks_xyz gets the chunk grid. */
+int clover_bricks_count(clover_bricks *w, int *chunks_xyz);
+/* Global cell range and neighbours of brick (0-based). */
+int clover_bricks_extent(clover_bricks *w, int brick, int *ext6, int *neighbours6);
+int clover_bricks_dt_history(clover_bricks *w, double *out, int cap);
+int clover_bricks_summaries(clover_bricks *w, double *out5, int *steps, int cap);
+/* Field id 1..19 of a brick in its reference layout (n elements). */
+int clover_bricks_read_field(clover_bricks *w, int brick, int field_id, double *out, long long n);
+void clover_bricks_destroy(clover_bricks *w);
+
 #ifdef __cplusplus
 }
 #endif

@@ -200,6 +200,112 @@ void clover_generate_chunk_kernel(const int *x_min, const int *x_max, const int 
                                   const int *state_geometry, const int *g_rect,
                                   const int *g_circ, const int *g_point);
 
+/* pack_kernel_module (pack_kernel.f90): the halo messages of the reference's
+ * MPI exchange, called per field by clover.f90:715-4457 (clover_pack_left and
+ * the like). pack copies `depth` layers of `field` next to the side into the
+ * caller's buffer at the 1-based indices pack_kernel.f90 forms from
+ * buffer_offset, the two tile offsets and g_x/y/z_max; unpack copies them into
+ * the halo on that side. The field is the device mirror of the host array; the
+ * message is formed on the device and copied to or from `buffer` (host memory)
+ * before the call returns. field_type is compared with the five *_DATA
+ * arguments (data.f90 CELL_DATA..Z_FACE_DATA) as the reference does. */
+/* pack_kernel_module::clover_pack_message_left, pack_kernel.f90:29-85 */
+void clover_pack_message_left(const int *x_min, const int *x_max, const int *y_min, const int *y_max,
+                          const int *z_min, const int *z_max, double *field, double *buffer,
+                          const int *cell_data, const int *vertex_data, const int *x_face_data,
+                          const int *y_face_data, const int *z_face_data, const int *depth,
+                          const int *field_type, const int *buffer_offset, const int *y_offset,
+                          const int *z_offset, const int *g_x_max, const int *g_y_max,
+                          const int *g_z_max);
+/* pack_kernel_module::clover_unpack_message_left, pack_kernel.f90:87-143 */
+void clover_unpack_message_left(const int *x_min, const int *x_max, const int *y_min, const int *y_max,
+                          const int *z_min, const int *z_max, double *field, double *buffer,
+                          const int *cell_data, const int *vertex_data, const int *x_face_data,
+                          const int *y_face_data, const int *z_face_data, const int *depth,
+                          const int *field_type, const int *buffer_offset, const int *y_offset,
+                          const int *z_offset, const int *g_x_max, const int *g_y_max,
+                          const int *g_z_max);
+/* pack_kernel_module::clover_pack_message_right, pack_kernel.f90:145-201 */
+void clover_pack_message_right(const int *x_min, const int *x_max, const int *y_min, const int *y_max,
+                          const int *z_min, const int *z_max, double *field, double *buffer,
+                          const int *cell_data, const int *vertex_data, const int *x_face_data,
+                          const int *y_face_data, const int *z_face_data, const int *depth,
+                          const int *field_type, const int *buffer_offset, const int *y_offset,
+                          const int *z_offset, const int *g_x_max, const int *g_y_max,
+                          const int *g_z_max);
+/* pack_kernel_module::clover_unpack_message_right, pack_kernel.f90:203-259 */
+void clover_unpack_message_right(const int *x_min, const int *x_max, const int *y_min, const int *y_max,
+                          const int *z_min, const int *z_max, double *field, double *buffer,
+                          const int *cell_data, const int *vertex_data, const int *x_face_data,
+                          const int *y_face_data, const int *z_face_data, const int *depth,
+                          const int *field_type, const int *buffer_offset, const int *y_offset,
+                          const int *z_offset, const int *g_x_max, const int *g_y_max,
+                          const int *g_z_max);
+/* pack_kernel_module::clover_pack_message_bottom, pack_kernel.f90:377-433 */
+void clover_pack_message_bottom(const int *x_min, const int *x_max, const int *y_min, const int *y_max,
+                          const int *z_min, const int *z_max, double *field, double *buffer,
+                          const int *cell_data, const int *vertex_data, const int *x_face_data,
+                          const int *y_face_data, const int *z_face_data, const int *depth,
+                          const int *field_type, const int *buffer_offset, const int *x_offset,
+                          const int *z_offset, const int *g_x_max, const int *g_y_max,
+                          const int *g_z_max);
+/* pack_kernel_module::clover_unpack_message_bottom, pack_kernel.f90:435-491 */
+void clover_unpack_message_bottom(const int *x_min, const int *x_max, const int *y_min, const int *y_max,
+                          const int *z_min, const int *z_max, double *field, double *buffer,
+                          const int *cell_data, const int *vertex_data, const int *x_face_data,
+                          const int *y_face_data, const int *z_face_data, const int *depth,
+                          const int *field_type, const int *buffer_offset, const int *x_offset,
+                          const int *z_offset, const int *g_x_max, const int *g_y_max,
+                          const int *g_z_max);
+/* pack_kernel_module::clover_pack_message_top, pack_kernel.f90:261-317 */
+void clover_pack_message_top(const int *x_min, const int *x_max, const int *y_min, const int *y_max,
+                          const int *z_min, const int *z_max, double *field, double *buffer,
+                          const int *cell_data, const int *vertex_data, const int *x_face_data,
+                          const int *y_face_data, const int *z_face_data, const int *depth,
+                          const int *field_type, const int *buffer_offset, const int *x_offset,
+                          const int *z_offset, const int *g_x_max, const int *g_y_max,
+                          const int *g_z_max);
+/* pack_kernel_module::clover_unpack_message_top, pack_kernel.f90:319-375 */
+void clover_unpack_message_top(const int *x_min, const int *x_max, const int *y_min, const int *y_max,
+                          const int *z_min, const int *z_max, double *field, double *buffer,
+                          const int *cell_data, const int *vertex_data, const int *x_face_data,
+                          const int *y_face_data, const int *z_face_data, const int *depth,
+                          const int *field_type, const int *buffer_offset, const int *x_offset,
+                          const int *z_offset, const int *g_x_max, const int *g_y_max,
+                          const int *g_z_max);
+/* pack_kernel_module::clover_pack_message_back, pack_kernel.f90:493-549 */
+void clover_pack_message_back(const int *x_min, const int *x_max, const int *y_min, const int *y_max,
+                          const int *z_min, const int *z_max, double *field, double *buffer,
+                          const int *cell_data, const int *vertex_data, const int *x_face_data,
+                          const int *y_face_data, const int *z_face_data, const int *depth,
+                          const int *field_type, const int *buffer_offset, const int *x_offset,
+                          const int *y_offset, const int *g_x_max, const int *g_y_max,
+                          const int *g_z_max);
+/* pack_kernel_module::clover_unpack_message_back, pack_kernel.f90:551-607 */
+void clover_unpack_message_back(const int *x_min, const int *x_max, const int *y_min, const int *y_max,
+                          const int *z_min, const int *z_max, double *field, double *buffer,
+                          const int *cell_data, const int *vertex_data, const int *x_face_data,
+                          const int *y_face_data, const int *z_face_data, const int *depth,
+                          const int *field_type, const int *buffer_offset, const int *x_offset,
+                          const int *y_offset, const int *g_x_max, const int *g_y_max,
+                          const int *g_z_max);
+/* pack_kernel_module::clover_pack_message_front, pack_kernel.f90:609-664 */
+void clover_pack_message_front(const int *x_min, const int *x_max, const int *y_min, const int *y_max,
+                          const int *z_min, const int *z_max, double *field, double *buffer,
+                          const int *cell_data, const int *vertex_data, const int *x_face_data,
+                          const int *y_face_data, const int *z_face_data, const int *depth,
+                          const int *field_type, const int *buffer_offset, const int *x_offset,
+                          const int *y_offset, const int *g_x_max, const int *g_y_max,
+                          const int *g_z_max);
+/* pack_kernel_module::clover_unpack_message_front, pack_kernel.f90:666-721 */
+void clover_unpack_message_front(const int *x_min, const int *x_max, const int *y_min, const int *y_max,
+                          const int *z_min, const int *z_max, double *field, double *buffer,
+                          const int *cell_data, const int *vertex_data, const int *x_face_data,
+                          const int *y_face_data, const int *z_face_data, const int *depth,
+                          const int *field_type, const int *buffer_offset, const int *x_offset,
+                          const int *y_offset, const int *g_x_max, const int *g_y_max,
+                          const int *g_z_max);
+
 /* ---- mirror management (no counterpart in the reference: the reference
  * arrays live in host memory only) ---- */
 
@@ -232,6 +338,15 @@ void clover_gpu_layout(const int *x_min, const int *x_max, const int *y_min, con
                        long long *elems);
 /* Number of host arrays currently mirrored, and their total device bytes. */
 void clover_gpu_mirror_stats(int *arrays, long long *bytes);
+/* One halo message between two chunks mirrored in this process, on the
+ * device: side's message of `src` (a host array of the chunk with bounds
+ * src_bounds = x_min,x_max,y_min,y_max,z_min,z_max) packed as pack_kernel.f90
+ * packs it and unpacked into the opposite side of `dst` (chunk dst_bounds).
+ * side 0..5 = left, right, bottom, top, back, front; field_type 1 cell,
+ * 2 vertex, 3 x face, 4 y face, 5 z face; depth 1 or 2. The transport of the
+ * brick driver when its bricks share a device. */
+void clover_gpu_face_copy(const int *src_bounds, double *src, const int *dst_bounds, double *dst,
+                          int side, int field_type, int depth);
 
 #ifdef __cplusplus
 }

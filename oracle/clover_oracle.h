@@ -25,6 +25,15 @@
 extern "C" {
 #endif
 
+/* pack_kernel.f90:29-721, the twelve message routines as one (oracle_pack.c):
+ * side 0..5 = left, right, bottom, top, back, front; field_type 1 cell,
+ * 2 vertex, 3 x face, 4 y face, 5 z face. */
+void oracle_pack_message(int side, int pack, const int *x_min, const int *x_max,
+                         const int *y_min, const int *y_max, const int *z_min, const int *z_max,
+                         double *field, double *buffer, const int *depth, const int *field_type,
+                         const int *buffer_offset, const int *off_a, const int *off_b,
+                         const int *g_x_max, const int *g_y_max, const int *g_z_max);
+
 /* ideal_gas_kernel.f90:23-64 */
 void oracle_ideal_gas_kernel(const int *x_min, const int *x_max, const int *y_min,
                              const int *y_max, const int *z_min, const int *z_max,
