@@ -219,6 +219,12 @@ def _declare(L):
     L.clover_bricks_read_field.restype = I
     L.clover_bricks_destroy.argtypes = [P]
     L.clover_gpu_face_copy.argtypes = [P, P, P, P, I, I, I]
+    L.clover_bricks_create_rank.argtypes = [P, I, I, P]
+    L.clover_bricks_create_rank.restype = P
+    L.clover_gpu_message_len.argtypes = [P, I, I, I]
+    L.clover_gpu_message_len.restype = ctypes.c_longlong
+    L.clover_gpu_pack_device.argtypes = [P, P, I, I, I, P, I]
+    L.clover_gpu_pack_device.restype = I
     L.clover_gpu_status.restype = ctypes.c_int
     L.clover_gpu_error_string.restype = ctypes.c_char_p
     L.clover_gpu_invalidate.argtypes = [P]

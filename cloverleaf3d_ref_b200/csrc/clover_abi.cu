@@ -791,6 +791,31 @@ void clover_unpack_message_front(MSG_ARGS) { message(MSG_PASS, 5, false); }
 #undef MSG_PASS
 #undef MSG_ARGS
 
+long long clover_gpu_message_len(const int* bounds, int side, int field_type, int depth) {
+  int xi, yi, zi;
+  if (side < 0 || side > 5 || depth < 1 || depth > 2 || !field_incs(field_type, xi, yi, zi))
+    return -1;
+  const Geom g = make_geom(bounds[0], bounds[1], bounds[2], bounds[3], bounds[4], bounds[5]);
+  return face_len(face_msg(g, side, depth, xi, yi, zi, 0, 0, g.x_max, g.y_max, g.z_max, 1));
+}
+
+int clover_gpu_pack_device(const int* bounds, double* field, int side, int field_type, int depth,
+                           double* dev_msg, int unpack) {
+  int xi, yi, zi;
+  if (side < 0 || side > 5 || depth < 1 || depth > 2 || !field_incs(field_type, xi, yi, zi)) {
+    set_error(CLOVER_STATUS_BAD_ARG, "pack_device: bad side, depth or field type");
+    return -1;
+  }
+  if (!enter(bounds, bounds + 1, bounds + 2, bounds + 3, bounds + 4, bounds + 5)) return -1;
+  Context& c = ctx();
+  const Geom g = c.g;
+  const FaceMsg f = face_msg(g, side, depth, xi, yi, zi, 0, 0, g.x_max, g.y_max, g.z_max, 1);
+  double* d_field = dev_of_type(field, field_type);
+  if (!d_field || !dev_msg) return -1;
+  launch_face(g, f, d_field, dev_msg, unpack == 0);
+  return c.status == 0 ? 0 : -1;
+}
+
 void clover_gpu_face_copy(const int* src_bounds, double* src, const int* dst_bounds, double* dst,
                           int side, int field_type, int depth) {
   const int* a = src_bounds;

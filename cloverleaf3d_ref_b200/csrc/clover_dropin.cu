@@ -4,6 +4,8 @@
 // arrays allocated as build_field.f90 allocates them. This is what the
 // unchanged Fortran drivers do once relinked against the ABI; the arrays
 // stay resident on the GPU and only scalars cross back per step.
+#include <cuda_runtime.h>
+
 #include <cstdlib>
 #include <cstring>
 #include <vector>
@@ -400,14 +402,98 @@ struct clover_bricks {
   bool advect_x = true;
   std::vector<double> dt_hist, sum_hist;
   std::vector<int> sum_steps;
+  // one brick per rank: this rank's chunk (id rank + 1) and the transport of
+  // its messages and reductions; rank < 0: every brick in this process
+  int rank = -1;
+  clover_transport tr{};
+  double* dmsg[4] = {nullptr, nullptr, nullptr, nullptr};  // send lo, recv lo, send hi, recv hi
+  double* hmsg[4] = {nullptr, nullptr, nullptr, nullptr};  // their host copies (host_staged)
+  long long msg_cap = 0;
+  bool failed = false;
 
   ~clover_bricks() {
     for (clover_dropin* d : b) delete d;
+    for (int q = 0; q < 4; q++) {
+      if (dmsg[q]) cudaFree(dmsg[q]);
+      if (hmsg[q]) cudaFreeHost(hmsg[q]);
+    }
+  }
+
+  bool reserve(long long n) {
+    if (n <= msg_cap) return true;
+    for (int q = 0; q < 4; q++) {
+      if (dmsg[q]) cudaFree(dmsg[q]);
+      if (hmsg[q]) cudaFreeHost(hmsg[q]);
+      dmsg[q] = hmsg[q] = nullptr;
+      if (cudaMalloc(&dmsg[q], (size_t)n * 8) != cudaSuccess) return false;
+      if (tr.host_staged && cudaMallocHost(&hmsg[q], (size_t)n * 8) != cudaSuccess) return false;
+    }
+    msg_cap = n;
+    return true;
+  }
+
+  // clover_exchange for this rank's brick: per axis, the messages of every
+  // field of the call packed one after another per side (clover.f90:474-713
+  // packs them into one buffer per side), moved by the transport, unpacked
+  void exchange_ranks(const std::vector<int>& ids, int depth) {
+    clover_dropin* c = b[0];
+    int bnd[6];
+    c->bounds(bnd);
+    for (int axis = 0; axis < 3; axis++) {
+      const int nb[2] = {c->neighbours[2 * axis], c->neighbours[2 * axis + 1]};
+      long long len[2] = {0, 0};
+      for (int s2 = 0; s2 < 2; s2++)
+        if (nb[s2] >= 0)
+          for (int id : ids)
+            len[s2] += clover_gpu_message_len(bnd, 2 * axis + s2, field_type_of(id), depth);
+      if (!reserve(len[0] > len[1] ? len[0] : len[1])) {
+        failed = true;
+        return;
+      }
+      for (int s2 = 0; s2 < 2; s2++) {
+        if (nb[s2] < 0) continue;
+        long long off = 0;
+        for (int id : ids) {
+          const int t = field_type_of(id);
+          clover_gpu_pack_device(bnd, c->field(id), 2 * axis + s2, t, depth, dmsg[2 * s2] + off, 0);
+          off += clover_gpu_message_len(bnd, 2 * axis + s2, t, depth);
+        }
+      }
+      clover_gpu_synchronize();
+      double* io[4];
+      for (int q = 0; q < 4; q++) io[q] = tr.host_staged ? hmsg[q] : dmsg[q];
+      if (tr.host_staged)
+        for (int s2 = 0; s2 < 2; s2++)
+          if (nb[s2] >= 0)
+            cudaMemcpy(hmsg[2 * s2], dmsg[2 * s2], (size_t)len[s2] * 8, cudaMemcpyDeviceToHost);
+      if (tr.exchange(tr.ctx, axis, nb[0], io[0], io[1], len[0], nb[1], io[2], io[3], len[1]) != 0) {
+        failed = true;
+        return;
+      }
+      for (int s2 = 0; s2 < 2; s2++) {
+        if (nb[s2] < 0) continue;
+        if (tr.host_staged)
+          cudaMemcpy(dmsg[2 * s2 + 1], hmsg[2 * s2 + 1], (size_t)len[s2] * 8,
+                     cudaMemcpyHostToDevice);
+        long long off = 0;
+        for (int id : ids) {
+          const int t = field_type_of(id);
+          clover_gpu_pack_device(bnd, c->field(id), 2 * axis + s2, t, depth,
+                                 dmsg[2 * s2 + 1] + off, 1);
+          off += clover_gpu_message_len(bnd, 2 * axis + s2, t, depth);
+        }
+      }
+    }
   }
 
   // clover_exchange (clover.f90:474-713): per axis, both messages of every
   // pair of neighbours along it, then the reflective halos
   void update_halo(const std::vector<int>& ids, int depth) {
+    if (rank >= 0) {
+      exchange_ranks(ids, depth);
+      for (clover_dropin* d : b) d->update_halo(ids, depth);
+      return;
+    }
     for (int axis = 0; axis < 3; axis++) {
       for (size_t i = 0; i < b.size(); i++) {
         const int hi = b[i]->neighbours[2 * axis + 1];
@@ -441,6 +527,7 @@ struct clover_bricks {
       d->summary_kernel(s);
       for (int q = 0; q < 5; q++) t[q] += s[q];
     }
+    if (rank >= 0 && tr.sum(tr.ctx, t, 5) != 0) failed = true;
     sum_hist.insert(sum_hist.end(), t, t + 5);
     sum_steps.push_back(step);
   }
@@ -450,6 +537,7 @@ struct clover_bricks {
     std::vector<int> ext(6 * n), nbr(6 * n);
     decompose(d.x_cells, d.y_cells, d.z_cells, n, grid, ext.data(), nbr.data());
     for (int i = 0; i < n; i++) {
+      if (rank >= 0 && i != rank) continue;
       clover_dropin* c = new clover_dropin;
       b.push_back(c);
       for (int f = 0; f < 6; f++) c->neighbours[f] = nbr[6 * i + f];
@@ -472,6 +560,7 @@ struct clover_bricks {
       const double dtlp = c->calc_dt();
       if (dtlp <= dt) dt = dtlp;
     }
+    if (rank >= 0 && tr.min(tr.ctx, &dt) != 0) failed = true;
     double m = dt;
     const double r = dtold * deck.timestep_rise;
     if (r < m) m = r;
@@ -518,6 +607,7 @@ struct clover_bricks {
     for (;;) {
       step = step + 1;
       if (!timestep()) return -step;
+      if (failed) return -step;
       dt_hist.push_back(dt);
       pdv(true);
       for (clover_dropin* c : b) c->accelerate(dt);
@@ -596,7 +686,24 @@ clover_bricks* clover_bricks_create(const clover_deck* deck, int n_chunks) {
   return w;
 }
 
-int clover_bricks_run(clover_bricks* w, int max_steps) { return w->hydro(max_steps); }
+clover_bricks* clover_bricks_create_rank(const clover_deck* deck, int n_chunks, int rank,
+                                         const clover_transport* t) {
+  if (n_chunks < 1 || rank < 0 || rank >= n_chunks || !t || !t->exchange || !t->min || !t->sum)
+    return nullptr;
+  clover_bricks* w = new clover_bricks;
+  w->rank = rank;
+  w->tr = *t;
+  if (!w->start(*deck, n_chunks) || w->failed) {
+    delete w;
+    return nullptr;
+  }
+  return w;
+}
+
+int clover_bricks_run(clover_bricks* w, int max_steps) {
+  const int n = w->hydro(max_steps);
+  return w->failed ? -1 : n;
+}
 
 int clover_bricks_count(clover_bricks* w, int* chunks_xyz) {
   for (int q = 0; q < 3; q++) chunks_xyz[q] = w->grid[q];

@@ -195,6 +195,28 @@ int clover_decompose(int x_cells, int y_cells, int z_cells, int n_chunks, int *c
  * (clover_sum). NULL on failure (clover_gpu_error_string). */
 typedef struct clover_bricks clover_bricks;
 clover_bricks *clover_bricks_create(const clover_deck *deck, int n_chunks);
+/* The transport of a decomposed run with one brick per rank (the reference's
+ * MPI model): implemented by the caller, e.g. over torch.distributed.
+ * exchange: one axis phase of clover_exchange (axis 0 x, 1 y, 2 z): send
+ * send_lo (n_lo doubles) to chunk lo and receive recv_lo from it, the same
+ * with chunk hi; a chunk of -1 is no neighbour (nothing to move). Chunk ids
+ * are ranks + 1. min: clover_min of one value in place; sum: clover_sum of n
+ * values in place. Each returns 0 on success. host_staged: 1 = the message
+ * buffers are host (pinned) memory, 0 = device memory, filled and drained on
+ * the library's stream, which is idle during the call. */
+typedef struct clover_transport {
+  void *ctx;
+  int host_staged;
+  int (*exchange)(void *ctx, int axis, int lo, double *send_lo, double *recv_lo, long long n_lo,
+                  int hi, double *send_hi, double *recv_hi, long long n_hi);
+  int (*min)(void *ctx, double *v);
+  int (*sum)(void *ctx, double *v, int n);
+} clover_transport;
+/* This rank's brick (chunk rank + 1 of clover_decompose's n_chunks) of the
+ * decomposed run; every rank calls it with the same deck and n_chunks. The
+ * brick queries below then address the one local brick as brick 0. */
+clover_bricks *clover_bricks_create_rank(const clover_deck *deck, int n_chunks, int rank,
+                                         const clover_transport *t);
 int clover_bricks_run(clover_bricks *w, int max_steps);
 /* Number of bricks; chunks_xyz gets the chunk grid. */
 int clover_bricks_count(clover_bricks *w, int *chunks_xyz);

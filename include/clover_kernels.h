@@ -347,6 +347,15 @@ void clover_gpu_mirror_stats(int *arrays, long long *bytes);
  * brick driver when its bricks share a device. */
 void clover_gpu_face_copy(const int *src_bounds, double *src, const int *dst_bounds, double *dst,
                           int side, int field_type, int depth);
+/* Length in doubles of one halo message (pack_kernel.f90 layout, no tile
+ * offsets) of a chunk with bounds x_min..z_max; -1 for a bad argument. */
+long long clover_gpu_message_len(const int *bounds, int side, int field_type, int depth);
+/* Pack (unpack = 0) side's message of `field` (host array of the chunk with
+ * `bounds`, mirrored) into the device buffer dev_msg, or unpack (unpack = 1)
+ * it from there into the halo on that side; queued on the library stream.
+ * Returns 0, or -1 with the status set. */
+int clover_gpu_pack_device(const int *bounds, double *field, int side, int field_type, int depth,
+                           double *dev_msg, int unpack);
 
 #ifdef __cplusplus
 }
