@@ -15,6 +15,9 @@ roofline   dominant kernel group, algorithmic bytes / its event-timed duration
            (a profiled run of the same steps right after the timed one).
 cpu_baseline  the oracle (C restatement of the reference, OpenMP) on the
            host cores over a bounded sample of the same problem.
+bricks_decomposition  the same problem at 256^3 decomposed into 8 bricks
+           (clover_decompose, device-side halo messages) against one chunk, both
+           through the drop-in driver: the exchange's cost per step.
 ensemble   batched decks (seeded draws of the same problem with drawn sizes,
            region, densities and energies): 64 decks of 24..128 cells per
            axis for 150 steps (FP64 and mixed) and 512 decks of 16..48 cells
@@ -414,6 +417,34 @@ def e2e_dropin(C, args, n, steps):
                      "per-step dt and summary reads, every array copied back"}
 
 
+def bricks_leg(C, n=256, n_bricks=8, steps=10):
+    """The decomposed run of one deck (clover_decompose's bricks, halo
+    messages exchanged between them on the device) against the same deck as
+    one chunk, both through the drop-in driver on this GPU, FP64: what the
+    exchange costs per step. The bricks share the GPU here; across GPUs each
+    rank would hold one (ranks.RankBricks)."""
+    deck = C.Deck.from_values(states=STATES, **deck_values(n, steps + 4))
+    L = C.lib()
+    out = {"cells": "%d^3" % n, "bricks": n_bricks, "steps_timed": steps, "precision": "fp64"}
+    for key, make in (("one_chunk", lambda: C.DropIn(deck)),
+                      ("bricks", lambda: C.Bricks(deck, n_bricks))):
+        L.clover_gpu_release()
+        w = make()
+        w.run(2)
+        L.clover_gpu_synchronize()
+        t0 = time.perf_counter()
+        w.run(2 + steps)
+        L.clover_gpu_synchronize()
+        dt = time.perf_counter() - t0
+        out[key] = {"value": n ** 3 * steps / dt, "unit": "cell-updates/s",
+                    "ms_per_step": 1e3 * dt / steps}
+        if key == "bricks":
+            out["grid"] = list(w.grid)
+        w.close()
+    out["bricks_over_one_chunk"] = out["bricks"]["ms_per_step"] / out["one_chunk"]["ms_per_step"]
+    return out
+
+
 def ensembles(C, torch, world=1, rank=0, barrier=None, dist=None):
     """The two ensemble configurations (64 decks FP64 + mixed; 512 small decks
     mixed with its FP64 twin), partitioned over the ranks when world > 1."""
@@ -438,6 +469,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--no-ensemble", action="store_true")
+    ap.add_argument("--no-bricks", action="store_true")
     ap.add_argument("--no-accuracy", action="store_true",
                     help="skip the 200-step FP64 vs mixed comparison")
     ap.add_argument("--ensemble-only", action="store_true",
@@ -553,6 +585,9 @@ def main():
     cpu = None
     if not args.no_cpu and rank == 0 and world == 1:
         cpu = cpu_baseline(n)
+    bricks = None
+    if not args.no_bricks and rank == 0 and world == 1:
+        bricks = bricks_leg(C)
 
     if rank == 0:
         line = {
@@ -578,6 +613,8 @@ def main():
             line["cpu_baseline"] = cpu
         if ens:
             line["ensemble"] = ens
+        if bricks:
+            line["bricks_decomposition"] = bricks
         print(json.dumps(line))
     if world > 1:
         dist.destroy_process_group()

@@ -319,6 +319,32 @@ __global__ void k_face_msg(Geom g, FaceMsg f, double* __restrict__ field, double
   }
 }
 
+// Several halo messages between chunks of this process in one launch, each
+// copied straight from the sender's layers to the receiver's halo: element i
+// of the loop space is message element i on both sides (the two chunks share
+// the extents of the face), so no buffer is needed. blockIdx.y = message.
+struct FaceCopy {
+  Geom gs, gd;
+  FaceMsg fs, fd;
+  const double* src;
+  double* dst;
+};
+
+__global__ void k_face_copy_batch(const FaceCopy* __restrict__ list) {
+  const FaceCopy& c = list[blockIdx.y];
+  const long long n = (long long)c.fs.n0 * c.fs.n1 * c.fs.n2;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int a = (int)(i % c.fs.n0), b = (int)((i / c.fs.n0) % c.fs.n1),
+              e = (int)(i / ((long long)c.fs.n0 * c.fs.n1));
+    int js = c.fs.j0 + a, ks = c.fs.k0 + b, ls = c.fs.l0 + e;
+    int jd = c.fd.j0 + a, kd = c.fd.k0 + b, ld = c.fd.l0 + e;
+    face_cell(c.gs, c.fs, true, js, ks, ls);
+    face_cell(c.gd, c.fd, false, jd, kd, ld);
+    c.dst[off3(c.gd, jd, kd, ld)] = c.src[off3(c.gs, js, ks, ls)];
+  }
+}
+
 namespace {
 
 // The loop space of pack_kernel.f90 for one side (j innermost), and the
@@ -790,6 +816,56 @@ void clover_pack_message_front(MSG_ARGS) { message(MSG_PASS, 5, true); }
 void clover_unpack_message_front(MSG_ARGS) { message(MSG_PASS, 5, false); }
 #undef MSG_PASS
 #undef MSG_ARGS
+
+int clover_gpu_face_copy_many(int n, const int* src_bounds, double* const* src,
+                              const int* dst_bounds, double* const* dst, const int* sides,
+                              const int* field_types, int depth) {
+  if (n <= 0) return 0;
+  if (depth < 1 || depth > 2) {
+    set_error(CLOVER_STATUS_BAD_ARG, "face_copy_many: depth must be 1 or 2");
+    return -1;
+  }
+  std::vector<FaceCopy> list((size_t)n);
+  long long longest = 0;
+  for (int m = 0; m < n; m++) {
+    int xi, yi, zi;
+    const int side = sides[m];
+    if (side < 0 || side > 5 || !field_incs(field_types[m], xi, yi, zi)) {
+      set_error(CLOVER_STATUS_BAD_ARG, "face_copy_many: bad side or field type");
+      return -1;
+    }
+    const int* a = src_bounds + 6 * m;
+    const int* b = dst_bounds + 6 * m;
+    FaceCopy& c = list[m];
+    if (!enter(a, a + 1, a + 2, a + 3, a + 4, a + 5)) return -1;
+    c.gs = ctx().g;
+    c.fs = face_msg(c.gs, side, depth, xi, yi, zi, 0, 0, c.gs.x_max, c.gs.y_max, c.gs.z_max, 1);
+    c.src = dev_of_type(src[m], field_types[m]);
+    if (!enter(b, b + 1, b + 2, b + 3, b + 4, b + 5)) return -1;
+    c.gd = ctx().g;
+    c.fd = face_msg(c.gd, side ^ 1, depth, xi, yi, zi, 0, 0, c.gd.x_max, c.gd.y_max, c.gd.z_max, 1);
+    c.dst = dev_of_type(dst[m], field_types[m]);
+    if (c.fs.n0 != c.fd.n0 || c.fs.n1 != c.fd.n1 || c.fs.n2 != c.fd.n2) {
+      set_error(CLOVER_STATUS_BAD_ARG, "face_copy_many: the two chunks' faces differ in extent");
+      return -1;
+    }
+    if (!c.src || !c.dst) return -1;
+    const long long len = (long long)c.fs.n0 * c.fs.n1 * c.fs.n2;
+    if (len > longest) longest = len;
+  }
+  Context& c = ctx();
+  const size_t bytes = list.size() * sizeof(FaceCopy);
+  double* d_list = msg_buffer((long long)((bytes + 7) / 8));
+  if (!d_list) return -1;
+  check(cudaMemcpyAsync(d_list, list.data(), bytes, cudaMemcpyHostToDevice, c.stream), "face list");
+  // the list is read by the kernel before the next call can change the host copy:
+  // the copy above is from pageable memory, which the runtime stages before returning
+  long long bx = (longest + 255) / 256;
+  if (bx > 64) bx = 64;
+  k_face_copy_batch<<<dim3((unsigned)bx, (unsigned)n), 256, 0, c.stream>>>((const FaceCopy*)d_list);
+  check_launch("face_copy_many");
+  return c.status == 0 ? 0 : -1;
+}
 
 long long clover_gpu_message_len(const int* bounds, int side, int field_type, int depth) {
   int xi, yi, zi;

@@ -494,7 +494,12 @@ struct clover_bricks {
       for (clover_dropin* d : b) d->update_halo(ids, depth);
       return;
     }
+    // one launch per axis phase: every message of the phase (both directions
+    // of every pair of neighbours along the axis, every field of the call)
+    std::vector<int> sb, db, sides, types;
+    std::vector<double*> src, dst;
     for (int axis = 0; axis < 3; axis++) {
+      sb.clear(); db.clear(); sides.clear(); types.clear(); src.clear(); dst.clear();
       for (size_t i = 0; i < b.size(); i++) {
         const int hi = b[i]->neighbours[2 * axis + 1];
         if (hi < 0) continue;
@@ -505,12 +510,21 @@ struct clover_bricks {
         hi_b->bounds(hi_bounds);
         for (int id : ids) {
           const int t = field_type_of(id);
-          clover_gpu_face_copy(lo_bounds, lo_b->field(id), hi_bounds, hi_b->field(id),
-                               2 * axis + 1, t, depth);
-          clover_gpu_face_copy(hi_bounds, hi_b->field(id), lo_bounds, lo_b->field(id),
-                               2 * axis, t, depth);
+          for (int dir = 0; dir < 2; dir++) {  // lo's hi side to hi, hi's lo side to lo
+            const int* from = dir == 0 ? lo_bounds : hi_bounds;
+            const int* to = dir == 0 ? hi_bounds : lo_bounds;
+            sb.insert(sb.end(), from, from + 6);
+            db.insert(db.end(), to, to + 6);
+            src.push_back(dir == 0 ? lo_b->field(id) : hi_b->field(id));
+            dst.push_back(dir == 0 ? hi_b->field(id) : lo_b->field(id));
+            sides.push_back(dir == 0 ? 2 * axis + 1 : 2 * axis);
+            types.push_back(t);
+          }
         }
       }
+      if (!sides.empty())
+        clover_gpu_face_copy_many((int)sides.size(), sb.data(), src.data(), db.data(), dst.data(),
+                                  sides.data(), types.data(), depth);
     }
     for (clover_dropin* d : b) d->update_halo(ids, depth);
   }

@@ -166,8 +166,8 @@ int clover_ensemble_read_field(clover_chunk *c, int deck, int field_id, double *
 /* ---- Host driver over the drop-in ABI ----
  * The reference's own control flow (start.f90, hydro.f90, timestep.f90,
  * PdV.f90, advection.f90) over host arrays allocated as build_field.f90
- * allocates them, every kernel call going through clover_kernels.h. One
- * instance per process (the ABI mirrors one chunk). */
+ * allocates them, every kernel call going through clover_kernels.h. Its
+ * destroy call releases every mirror of the process. */
 typedef struct clover_dropin clover_dropin;
 clover_dropin *clover_dropin_create(const clover_deck *deck);
 /* Run the hydro loop to its end (deck end_step/end_time, or max_steps).

@@ -311,7 +311,7 @@ void clover_unpack_message_front(const int *x_min, const int *x_max, const int *
 
 /* Status bits. */
 #define CLOVER_STATUS_CUDA_ERROR 0x1   /* a CUDA call or launch failed */
-#define CLOVER_STATUS_BOUNDS 0x2       /* a call passed other chunk bounds */
+#define CLOVER_STATUS_BOUNDS 0x2       /* an array passed with another chunk's bounds */
 #define CLOVER_STATUS_SMALL_DT 0x4     /* calc_dt returned small=1 */
 #define CLOVER_STATUS_NO_DEVICE 0x8    /* no CUDA device */
 #define CLOVER_STATUS_BAD_ARG 0x10     /* unsupported argument (e.g. >16 states) */
@@ -347,6 +347,14 @@ void clover_gpu_mirror_stats(int *arrays, long long *bytes);
  * brick driver when its bricks share a device. */
 void clover_gpu_face_copy(const int *src_bounds, double *src, const int *dst_bounds, double *dst,
                           int side, int field_type, int depth);
+/* n halo messages between chunks of this process in one launch, message m
+ * as clover_gpu_face_copy(src_bounds + 6m, src[m], dst_bounds + 6m, dst[m],
+ * sides[m], field_types[m], depth) would move it; the messages must not write
+ * what another of them reads (one axis phase of an exchange). 0, or -1 with
+ * the status set. */
+int clover_gpu_face_copy_many(int n, const int *src_bounds, double *const *src,
+                              const int *dst_bounds, double *const *dst, const int *sides,
+                              const int *field_types, int depth);
 /* Length in doubles of one halo message (pack_kernel.f90 layout, no tile
  * offsets) of a chunk with bounds x_min..z_max; -1 for a bad argument. */
 long long clover_gpu_message_len(const int *bounds, int side, int field_type, int depth);
