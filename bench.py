@@ -411,7 +411,7 @@ def e2e_dropin(C, args, n, steps):
     return {"value": n ** 3 * taken / (t1 - t0), "unit": "cell-updates/s",
             "h2d_bytes_per_step": host_bytes / taken,
             "d2h_bytes_per_step": (host_bytes + 8 * taken + 40 * (taken // 10 + 2)) / taken,
-            "seconds": t1 - t0, "steps": taken, "cells": "%d^3" % n,
+            "seconds": t1 - t0, "steps": taken, "cells": "%d^3" % n, "ranks": 1,
             "setup_seconds_untimed": t0 - ts,
             "timed": "upload of every host array (pinned) at its first use, the steps, "
                      "per-step dt and summary reads, every array copied back"}
@@ -579,6 +579,8 @@ def main():
     ens = None
     if not args.no_ensemble:
         ens = ensembles(C, torch, world, rank, barrier, dist)
+    # the end-to-end leg holds every reference array on the host (~33 GB at
+    # 512^3), so it runs on rank 0 only, as the reference arm does
     e2e = None
     if not args.no_e2e and rank == 0:
         e2e = e2e_dropin(C, args, n, args.steps)
