@@ -42,6 +42,17 @@ struct Context {
   size_t stage_bytes = 0;
   double* msg = nullptr;    // one halo message (pack_kernel.f90) on the device
   size_t msg_bytes = 0;
+  // advec_mom's pre/post volumes (advec_mom_kernel.f90 recomputes them in each
+  // of a sweep's three velocity calls): the call that formed them last, and
+  // the number of library calls made up to it
+  long long calls = 0;
+  struct {
+    long long at = -1;
+    int variant = -1;
+    const void* in[4] = {nullptr, nullptr, nullptr, nullptr};  // vol_flux_x/y/z, volume
+    const void* out[2] = {nullptr, nullptr};                  // pre_vol, post_vol
+    Geom g{};
+  } mom_vol;
   int status = 0;
   std::string err;
   bool pin_host = true;
@@ -73,6 +84,7 @@ void check_launch(const char* what) { check(cudaGetLastError(), what); }
 bool enter(const int* x_min, const int* x_max, const int* y_min, const int* y_max,
            const int* z_min, const int* z_max) {
   Context& c = ctx();
+  c.calls++;
   if (*x_max < *x_min || *y_max < *y_min || *z_max < *z_min) {
     set_error(CLOVER_STATUS_BAD_ARG, "empty chunk bounds");
     return false;
@@ -662,11 +674,33 @@ void clover_advec_mom_kernel(const int* x_min, const int* x_max, const int* y_mi
   ga.celldx = CX(celldx); ga.celldy = CY(celldy); ga.celldz = CZ(celldz);
   double* work[7] = {VERT(node_flux), VERT(node_mass_post), VERT(node_mass_pre),
                      VERT(advec_vel), VERT(mom_flux), VERT(pre_vol), VERT(post_vol)};
+  // The pre/post volumes depend only on the sweep's variant, the volume
+  // fluxes and the volume. They are formed again only if another library call
+  // (or a host change: clover_gpu_invalidate*) came since the advec_mom call
+  // that last formed them, or that call had another variant or other arrays.
+  // A call whose other outputs alias them forms them again too.
+  const int variant = mom_vol_variant(*advect_x != 0, *sweep_number, *direction);
+  const void* in[4] = {vol_flux_x, vol_flux_y, vol_flux_z, volume};
+  const void* out[2] = {pre_vol, post_vol};
+  const void* others[6] = {vel1, node_flux, node_mass_post, node_mass_pre, advec_vel, mom_flux};
+  bool skip = variant >= 0 && c.mom_vol.at == c.calls - 1 && c.mom_vol.variant == variant &&
+              same_chunk(c.mom_vol.g, g);
+  for (int q = 0; q < 4 && skip; q++) skip = c.mom_vol.in[q] == in[q];
+  for (int q = 0; q < 2 && skip; q++) skip = c.mom_vol.out[q] == out[q];
+  bool aliased = pre_vol == post_vol;
+  for (int q = 0; q < 6; q++) aliased = aliased || others[q] == pre_vol || others[q] == post_vol;
+  for (int q = 0; q < 4; q++) aliased = aliased || in[q] == pre_vol || in[q] == post_vol;
+  skip = skip && !aliased;
   launch_advec_mom<F64>(g, c.stream, VERT(vel1), XF(mass_flux_x), XF(vol_flux_x),
                         YF(mass_flux_y), YF(vol_flux_y), ZF(mass_flux_z), ZF(vol_flux_z), ga,
                         CELL(density1), work, *advect_x != 0, *which_vel, *sweep_number,
-                        *direction);
+                        *direction, skip);
   check_launch("advec_mom");
+  c.mom_vol.at = (variant >= 0 && !aliased && c.status == 0) ? c.calls : -1;
+  c.mom_vol.variant = variant;
+  c.mom_vol.g = g;
+  for (int q = 0; q < 4; q++) c.mom_vol.in[q] = in[q];
+  for (int q = 0; q < 2; q++) c.mom_vol.out[q] = out[q];
 }
 
 void clover_reset_field_kernel(const int* x_min, const int* x_max, const int* y_min,
@@ -946,12 +980,14 @@ void clover_gpu_sync_to_host(void) {
 
 void clover_gpu_invalidate(const void* host_array) {
   Context& c = ctx();
+  c.mom_vol.at = -1;
   auto it = c.mirrors.find(host_array);
   if (it != c.mirrors.end()) it->second.planes = 0;
 }
 
 void clover_gpu_invalidate_all(void) {
   Context& c = ctx();
+  c.mom_vol.at = -1;
   for (auto& kv : c.mirrors) kv.second.planes = 0;
 }
 
@@ -969,6 +1005,7 @@ void clover_gpu_release(void) {
     cudaFree(kv.second.raw);
   }
   c.mirrors.clear();
+  c.mom_vol.at = -1;
   for (void* p : c.scratch) cudaFree(p);
   c.scratch.clear();
   cudaFree(c.d_key);

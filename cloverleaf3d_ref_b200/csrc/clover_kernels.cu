@@ -1266,6 +1266,17 @@ static inline Box box_union(const Box& a, const Box& b) {
              a.l0 < b.l0 ? a.l0 : b.l0, a.l1 > b.l1 ? a.l1 : b.l1};
 }
 
+// advec_mom_kernel.f90:106-162: which pre/post volume form a sweep takes
+// (-1: none)
+int mom_vol_variant(int advect_x, int sweep, int direction) {
+  if (sweep == 1 && direction == 1) return 0;
+  if (sweep == 1 && direction == 3) return 1;
+  if (sweep == 2) return advect_x ? 2 : 3;
+  if (sweep == 3 && direction == 1) return 4;
+  if (sweep == 3 && direction == 3) return 5;
+  return -1;
+}
+
 template <class S>
 void launch_advec_mom(const Geom& g, cudaStream_t s, typename S::vel_t* vel1,
                       const typename S::mf_t* mass_flux_x, const typename S::vf_t* vol_flux_x,
@@ -1273,17 +1284,11 @@ void launch_advec_mom(const Geom& g, cudaStream_t s, typename S::vel_t* vel1,
                       const typename S::mf_t* mass_flux_z, const typename S::vf_t* vol_flux_z,
                       const GeomArrays& ga, const typename S::rho_t* density1,
                       typename S::wk_t* const* work, int advect_x, int which_vel, int sweep,
-                      int direction) {
+                      int direction, bool skip_volumes) {
   typename S::wk_t *node_flux = work[0], *node_mass_post = work[1], *node_mass_pre = work[2],
                    *mom_flux = work[4], *pre_vol = work[5], *post_vol = work[6];
-  int variant = -1;
-  if (sweep == 1 && direction == 1) variant = 0;
-  else if (sweep == 1 && direction == 3) variant = 1;
-  else if (sweep == 2 && advect_x) variant = 2;
-  else if (sweep == 2 && !advect_x) variant = 3;
-  else if (sweep == 3 && direction == 1) variant = 4;
-  else if (sweep == 3 && direction == 3) variant = 5;
-  if (variant >= 0)
+  const int variant = mom_vol_variant(advect_x, sweep, direction);
+  if (variant >= 0 && !skip_volumes)
     LAUNCH(k_mom_vol<S>, halo2(g), variant, ga, vol_flux_x, vol_flux_y, vol_flux_z, pre_vol, post_vol);
   const int x0 = g.x_min, x1 = g.x_max, y0 = g.y_min, y1 = g.y_max, z0 = g.z_min, z1 = g.z_max;
   if (direction == 1) {
@@ -1483,7 +1488,8 @@ void launch_fill(cudaStream_t s, T* p, long long elems, T value) {
   template void launch_advec_mom<S>(const Geom&, cudaStream_t, S::vel_t*, const S::mf_t*,        \
                                     const S::vf_t*, const S::mf_t*, const S::vf_t*,            \
                                     const S::mf_t*, const S::vf_t*, const GeomArrays&,         \
-                                    const S::rho_t*, S::wk_t* const*, int, int, int, int);     \
+                                    const S::rho_t*, S::wk_t* const*, int, int, int, int,      \
+                                    bool);                                                     \
   template void launch_reset_field<S>(const Target&, cudaStream_t, S::rho_t*, const S::rho_t*,     \
                                       S::ene_t*, const S::ene_t*, S::vel_t*, const S::vel_t*,  \
                                       S::vel_t*, const S::vel_t*, S::vel_t*, const S::vel_t*); \

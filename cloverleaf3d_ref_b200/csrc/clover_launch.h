@@ -261,7 +261,12 @@ void launch_advec_cell(const Geom& g, cudaStream_t s, int advect_x, int dir, int
                        const typename S::vf_t* vol_flux_y, typename S::mf_t* mass_flux_z,
                        const typename S::vf_t* vol_flux_z, typename S::wk_t* const* work);
 
-// work: the 7 work arrays (advec_mom_driver.f90:51-57 order).
+// advec_mom's pre/post volume form for a sweep (-1: none).
+int mom_vol_variant(int advect_x, int sweep, int direction);
+
+// work: the 7 work arrays (advec_mom_driver.f90:51-57 order). skip_volumes:
+// pre_vol/post_vol already hold this sweep's values (the caller knows that
+// nothing changed them or their inputs since they were formed).
 template <class S>
 void launch_advec_mom(const Geom& g, cudaStream_t s, typename S::vel_t* vel1,
                       const typename S::mf_t* mass_flux_x, const typename S::vf_t* vol_flux_x,
@@ -269,7 +274,7 @@ void launch_advec_mom(const Geom& g, cudaStream_t s, typename S::vel_t* vel1,
                       const typename S::mf_t* mass_flux_z, const typename S::vf_t* vol_flux_z,
                       const GeomArrays& ga, const typename S::rho_t* density1,
                       typename S::wk_t* const* work, int advect_x, int which_vel, int sweep,
-                      int direction);
+                      int direction, bool skip_volumes = false);
 
 template <class S>
 void launch_reset_field(const Target& tg, cudaStream_t s, typename S::rho_t* density0,

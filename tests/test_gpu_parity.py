@@ -198,3 +198,46 @@ def test_native_fused_long_run_bitwise():
     sums, sst = ch.summaries()
     compare_run(r, ch.dt_history(), sums, sst, ch.field)
     ch.close()
+
+
+def test_mom_volumes_formed_again_after_host_change_or_other_call():
+    """advec_mom reuses the pre/post volumes of the previous velocity call of
+    a sweep only while nothing else happened: after the host changes an input
+    (clover_gpu_invalidate) or another library call (here flux_calc, which
+    rewrites the volume fluxes), they are formed again, as the reference
+    forms them in every call."""
+    d = decks.shock(9, 8, 10, 2, states=decks.MIXED_STATES)
+    nx, ny, nz = d["x_cells"], d["y_cells"], d["z_cells"]
+    L = C.lib()
+    a_ref, a_gpu = H.new_chunk(nx, ny, nz), H.new_chunk(nx, ny, nz)
+    hs = [H.Hydro(H.Backend(O.load(), "oracle_"), a_ref, nx, ny, nz, d),
+          H.Hydro(H.Backend(L, "clover_"), a_gpu, nx, ny, nz, d)]
+
+    def check(names):
+        L.clover_gpu_sync_to_host()
+        assert L.clover_gpu_status() in (0, 4), L.clover_gpu_error_string()
+        for k in names:
+            assert np.array_equal(a_gpu[k], a_ref[k]), k
+
+    for h in hs:
+        h.start()
+        h.timestep()
+        h.pdv(True)
+        h.accelerate()
+        h.pdv(False)
+        h.flux_calc()
+        h.halo([4, 2, 14, 15, 16], 2)
+        h.advec_cell(1, 1)
+        h.halo([2, 4, 9, 11, 13, 17, 18, 19], 2)
+        h.advec_mom(1, 1, 1)
+    check(["wa6", "wa7", "xvel1"])
+    for a in (a_ref, a_gpu):  # the host changes an input between two velocity calls
+        a["vol_flux_y"] *= 1.25
+    L.clover_gpu_invalidate(ctypes.c_void_p(a_gpu["vol_flux_y"].ctypes.data))
+    for h in hs:
+        h.advec_mom(2, 1, 1)
+    check(["wa6", "wa7", "yvel1"])
+    for h in hs:  # another library call rewrites the volume fluxes
+        h.flux_calc()
+        h.advec_mom(3, 1, 1)
+    check(["vol_flux_x", "vol_flux_y", "vol_flux_z", "wa6", "wa7", "zvel1"])
