@@ -148,62 +148,62 @@ __global__ void __launch_bounds__(BX * BY, 4) k_viscosity(Geom g, Box b, GeomArr
 
   const double ugradx1 = u000 + u010 + u001 + u011;
   const double ugradx2 = u100 + u110 + u101 + u111;
-  const double ugrady1 = u000 + u100 + u001 + u101;
-  const double ugrady2 = u010 + u110 + u011 + u111;
-  const double ugradz1 = u000 + u100 + u010 + u110;
-  const double ugradz2 = u001 + u101 + u011 + u111;
-
-  const double vgradx1 = v000 + v010 + v001 + v011;
-  const double vgradx2 = v100 + v110 + v101 + v111;
   const double vgrady1 = v000 + v100 + v001 + v101;
   const double vgrady2 = v010 + v110 + v011 + v111;
-  const double vgradz1 = v000 + v100 + v010 + v110;
-  const double vgradz2 = v001 + v101 + v011 + v111;
-
-  const double wgradx1 = w000 + w010 + w001 + w011;
-  const double wgradx2 = w100 + w110 + w101 + w111;
-  const double wgrady1 = w000 + w100 + w001 + w101;
-  const double wgrady2 = w010 + w110 + w011 + w111;
   const double wgradz1 = w000 + w100 + w010 + w110;
   const double wgradz2 = w001 + w101 + w011 + w111;
-
-  const double cdx = GX(ga.celldx, j), cdy = GY(ga.celldy, k), cdz = GZ(ga.celldz, l);
   const double div = (E(ga.xarea, j, k, l) * (ugradx2 - ugradx1) +
                       E(ga.yarea, j, k, l) * (vgrady2 - vgrady1)) +
                      E(ga.zarea, j, k, l) * (wgradz2 - wgradz1);
+  // IF((limiter.GT.0.0).OR.(div.GE.0.0)) q=0: with div >= 0 the limiter
+  // cannot change q, so the strain terms, pressure gradients and limiter are
+  // formed only for compressing cells (a NaN div takes that path too)
+  double q = 0.0;
+  if (!(div >= 0.0)) {
+    const double ugrady1 = u000 + u100 + u001 + u101;
+    const double ugrady2 = u010 + u110 + u011 + u111;
+    const double ugradz1 = u000 + u100 + u010 + u110;
+    const double ugradz2 = u001 + u101 + u011 + u111;
+    const double vgradx1 = v000 + v010 + v001 + v011;
+    const double vgradx2 = v100 + v110 + v101 + v111;
+    const double vgradz1 = v000 + v100 + v010 + v110;
+    const double vgradz2 = v001 + v101 + v011 + v111;
+    const double wgradx1 = w000 + w010 + w001 + w011;
+    const double wgradx2 = w100 + w110 + w101 + w111;
+    const double wgrady1 = w000 + w100 + w001 + w101;
+    const double wgrady2 = w010 + w110 + w011 + w111;
 
-  const double xx = 0.25 * (ugradx2 - ugradx1) / cdx;
-  const double yy = 0.25 * (vgrady2 - vgrady1) / cdy;
-  const double zz = 0.25 * (wgradz2 - wgradz1) / cdz;
-  const double xy = 0.25 * (ugrady2 - ugrady1) / cdy + 0.25 * (vgradx2 - vgradx1) / cdx;
-  const double xz = 0.25 * (ugradz2 - ugradz1) / cdz + 0.25 * (wgradx2 - wgradx1) / cdx;
-  const double yz = 0.25 * (vgradz2 - vgradz1) / cdz + 0.25 * (wgrady2 - wgrady1) / cdy;
+    const double cdx = GX(ga.celldx, j), cdy = GY(ga.celldy, k), cdz = GZ(ga.celldz, l);
+    const double xx = 0.25 * (ugradx2 - ugradx1) / cdx;
+    const double yy = 0.25 * (vgrady2 - vgrady1) / cdy;
+    const double zz = 0.25 * (wgradz2 - wgradz1) / cdz;
+    const double xy = 0.25 * (ugrady2 - ugrady1) / cdy + 0.25 * (vgradx2 - vgradx1) / cdx;
+    const double xz = 0.25 * (ugradz2 - ugradz1) / cdz + 0.25 * (wgradx2 - wgradx1) / cdx;
+    const double yz = 0.25 * (vgradz2 - vgradz1) / cdz + 0.25 * (wgrady2 - wgrady1) / cdy;
 
-  double pgradx = (L(pressure, j + 1, k, l) - L(pressure, j - 1, k, l)) / (cdx + GX(ga.celldx, j + 1));
-  double pgrady = (L(pressure, j, k + 1, l) - L(pressure, j, k - 1, l)) / (cdy + GY(ga.celldy, k + 1));
-  double pgradz = (L(pressure, j, k, l + 1) - L(pressure, j, k, l - 1)) / (cdz + GZ(ga.celldz, l + 1));
+    double pgradx = (L(pressure, j + 1, k, l) - L(pressure, j - 1, k, l)) / (cdx + GX(ga.celldx, j + 1));
+    double pgrady = (L(pressure, j, k + 1, l) - L(pressure, j, k - 1, l)) / (cdy + GY(ga.celldy, k + 1));
+    double pgradz = (L(pressure, j, k, l + 1) - L(pressure, j, k, l - 1)) / (cdz + GZ(ga.celldz, l + 1));
 
-  const double pgradx2 = pgradx * pgradx;
-  const double pgrady2 = pgrady * pgrady;
-  const double pgradz2 = pgradz * pgradz;
+    const double pgradx2 = pgradx * pgradx;
+    const double pgrady2 = pgrady * pgrady;
+    const double pgradz2 = pgradz * pgradz;
 
-  const double limiter = (xx * pgradx2 + yy * pgrady2 + zz * pgradz2 + xy * pgradx * pgrady +
-                          xz * pgradx * pgradz + yz * pgrady * pgradz) /
-                         fmax2(pgradx2 + pgrady2 + pgradz2, 1.0e-16);
-  double q;
-  if ((limiter > 0.0) || (div >= 0.0)) {
-    q = 0.0;
-  } else {
-    pgradx = copysign(fmax2(1.0e-16, fabs(pgradx)), pgradx);
-    pgrady = copysign(fmax2(1.0e-16, fabs(pgrady)), pgrady);
-    pgradz = copysign(fmax2(1.0e-16, fabs(pgradz)), pgradz);
-    const double pgrad = sqrt(pgradx * pgradx + pgrady * pgrady + pgradz * pgradz);
-    const double xgrad = fabs(cdx * pgrad / pgradx);
-    const double ygrad = fabs(cdy * pgrad / pgrady);
-    const double zgrad = fabs(cdz * pgrad / pgradz);
-    const double grad = fmin2(fmin2(xgrad, ygrad), zgrad);
-    const double grad2 = grad * grad;
-    q = 2.0 * L(density0, j, k, l) * grad2 * limiter * limiter;
+    const double limiter = (xx * pgradx2 + yy * pgrady2 + zz * pgradz2 + xy * pgradx * pgrady +
+                            xz * pgradx * pgradz + yz * pgrady * pgradz) /
+                           fmax2(pgradx2 + pgrady2 + pgradz2, 1.0e-16);
+    if (!(limiter > 0.0)) {
+      pgradx = copysign(fmax2(1.0e-16, fabs(pgradx)), pgradx);
+      pgrady = copysign(fmax2(1.0e-16, fabs(pgrady)), pgrady);
+      pgradz = copysign(fmax2(1.0e-16, fabs(pgradz)), pgradz);
+      const double pgrad = sqrt(pgradx * pgradx + pgrady * pgrady + pgradz * pgradz);
+      const double xgrad = fabs(cdx * pgrad / pgradx);
+      const double ygrad = fabs(cdy * pgrad / pgrady);
+      const double zgrad = fabs(cdz * pgrad / pgradz);
+      const double grad = fmin2(fmin2(xgrad, ygrad), zgrad);
+      const double grad2 = grad * grad;
+      q = 2.0 * L(density0, j, k, l) * grad2 * limiter * limiter;
+    }
   }
   E(viscosity, j, k, l) = st<typename S::cs_t>(q);
 }
