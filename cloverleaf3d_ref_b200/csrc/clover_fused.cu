@@ -123,8 +123,10 @@ __device__ __forceinline__ double ld(const float* p) { return (double)__ldg(p); 
 #define EI_(a, jj, kk, ll) (a)[off3(g, (jj), (kk), (ll))]
 #define LI(a, idx) ld(&EI_(a, idx))
 
-template <class T>
-__device__ __forceinline__ T st(double v) { return (T)v; }
+// a value in storage type T, converted once from the arithmetic it was
+// formed in (no detour through double for an FP32 value stored as FP32)
+template <class T, class U>
+__device__ __forceinline__ T st(U v) { return (T)v; }
 
 __device__ __forceinline__ double fmin2(double a, double b) { return b < a ? b : a; }
 __device__ __forceinline__ double fmax2(double a, double b) { return b > a ? b : a; }
@@ -239,7 +241,7 @@ __global__ void __launch_bounds__(BX * BY, sizeof(typename S::arith_t) == 4 || M
     // energy0 carry the halo the pressure's would mirror)
     using C = typename S::cs_t;
 #define PN(jj, kk, ll) \
-  ((A)st<C>((double)((A(1.4) - A(1.0)) * LA(density0, jj, kk, ll) * LA(energy0, jj, kk, ll))))
+  ((A)st<C>(((A(1.4) - A(1.0)) * LA(density0, jj, kk, ll) * LA(energy0, jj, kk, ll))))
     A pgradx = (PN(j + 1, k, l) - PN(j - 1, k, l)) / (cdx + AG(GX, ga.celldx, j + 1));
     A pgrady = (PN(j, k + 1, l) - PN(j, k - 1, l)) / (cdy + AG(GY, ga.celldy, k + 1));
     A pgradz = (PN(j, k, l + 1) - PN(j, k, l - 1)) / (cdz + AG(GZ, ga.celldz, l + 1));
@@ -264,9 +266,9 @@ __global__ void __launch_bounds__(BX * BY, sizeof(typename S::arith_t) == 4 || M
     }
   }
   using C = typename S::cs_t;
-  E(viscosity, j, k, l) = st<C>((double)q);
+  E(viscosity, j, k, l) = st<C>(q);
   // calc_dt_kernel.f90:102-149 (the viscosity as stored)
-  const A visc = (A)st<C>((double)q);
+  const A visc = (A)st<C>(q);
   const A d0 = LA(density0, j, k, l);
   // 1/min(celldx, celldy, celldz)^2 of the chunk's uniform mesh
   const A ds = geo_ds<A>(g);
@@ -278,8 +280,8 @@ __global__ void __launch_bounds__(BX * BY, sizeof(typename S::arith_t) == 4 || M
     const A pbe = (A(1.4) - A(1.0)) * d0;
     const A pbv = -d0 * p_eos;
     const A ss2 = v_eos * v_eos * (p_eos * pbe - pbv);
-    E(pressure, j, k, l) = st<C>((double)p_eos);
-    const C ss_st = st<C>((double)sqrt(ss2));
+    E(pressure, j, k, l) = st<C>(p_eos);
+    const C ss_st = st<C>(sqrt(ss2));
     E(soundspeed, j, k, l) = ss_st;
     ss = (A)ss_st;
   }
@@ -386,9 +388,9 @@ __global__ void __launch_bounds__(BX * BY, M::kFlat ? 6 : 8) k_pdv_predict_eos(M
   using R = typename S::rho_t;
   using En = typename S::ene_t;
   // the predicted state goes through the storage types, as it would in memory
-  const A e1 = (A)st<En>((double)(LA(energy0, j, k, l) - energy_change));
-  const A d1 = (A)st<R>((double)(d0 * vol_change_s));
-  E(pressure, j, k, l) = st<typename S::cs_t>((double)((A(1.4) - A(1.0)) * d1 * e1));
+  const A e1 = (A)st<En>((LA(energy0, j, k, l) - energy_change));
+  const A d1 = (A)st<R>((d0 * vol_change_s));
+  E(pressure, j, k, l) = st<typename S::cs_t>(((A(1.4) - A(1.0)) * d1 * e1));
 #undef EGA
 #undef LA
   });
@@ -490,7 +492,7 @@ __global__ void __launch_bounds__(BX * BY, M::kFlat ? 5 : 8) k_pdv_flux(M m, con
   const A ad0 = (A)d0;
   const A energy_change = (LA(pressure, j, k, l) / ad0 + LA(viscosity, j, k, l) / ad0) *
                           (A)total_flux * geo_rvol<A>(g);
-  E(energy1, j, k, l) = st<typename S::ene_t>((double)(LA(energy0, j, k, l) - energy_change));
+  E(energy1, j, k, l) = st<typename S::ene_t>((LA(energy0, j, k, l) - energy_change));
   E(density1, j, k, l) = st<typename S::rho_t>(d0 * vol_change_s);
 #undef LA
   });

@@ -94,8 +94,10 @@ __device__ __forceinline__ double ld(const double* p) { return __ldg(p); }
 __device__ __forceinline__ double ld(const float* p) { return (double)__ldg(p); }
 #define L(a, jj, kk, ll) ld(&E(a, jj, kk, ll))
 
-template <class T>
-__device__ __forceinline__ T st(double v) { return (T)v; }
+// a value in storage type T, converted once from the arithmetic it was
+// formed in (no detour through double for an FP32 value stored as FP32)
+template <class T, class U>
+__device__ __forceinline__ T st(U v) { return (T)v; }
 
 __device__ __forceinline__ double fmin2(double a, double b) { return b < a ? b : a; }
 __device__ __forceinline__ double fmax2(double a, double b) { return b > a ? b : a; }
@@ -120,8 +122,8 @@ __global__ void __launch_bounds__(BX * BY) k_ideal_gas(M m,
   const A pressurebyvolume = -d * p;
   const A ss2 = v * v * (p * pressurebyenergy - pressurebyvolume);
   using C = typename S::cs_t;
-  E(pressure, j, k, l) = st<C>((double)p);
-  E(soundspeed, j, k, l) = st<C>((double)sqrt(ss2));
+  E(pressure, j, k, l) = st<C>(p);
+  E(soundspeed, j, k, l) = st<C>(sqrt(ss2));
   });
 }
 
