@@ -603,18 +603,18 @@ struct clover_bricks {
     update_halo(pre, 2);
     for (clover_dropin* c : b) c->advec_cell(1, dir);
     update_halo(post, 2);
-    for (int v = 1; v <= 3; v++)
-      for (clover_dropin* c : b) c->advec_mom(v, dir, 1);
+    for (clover_dropin* c : b)  // a brick's three velocity calls back to back
+      for (int v = 1; v <= 3; v++) c->advec_mom(v, dir, 1);
     update_halo(pre, 2);
     for (clover_dropin* c : b) c->advec_cell(2, 2);
     update_halo(post, 2);
-    for (int v = 1; v <= 3; v++)
-      for (clover_dropin* c : b) c->advec_mom(v, 2, 2);
+    for (clover_dropin* c : b)  // a brick's three velocity calls back to back
+      for (int v = 1; v <= 3; v++) c->advec_mom(v, 2, 2);
     dir = advect_x ? 3 : 1;
     for (clover_dropin* c : b) c->advec_cell(3, dir);
     update_halo(post, 2);
-    for (int v = 1; v <= 3; v++)
-      for (clover_dropin* c : b) c->advec_mom(v, dir, 3);
+    for (clover_dropin* c : b)  // a brick's three velocity calls back to back
+      for (int v = 1; v <= 3; v++) c->advec_mom(v, dir, 3);
   }
 
   int hydro(int max_steps) {  // hydro.f90:46-98
