@@ -141,6 +141,59 @@ def cpu_baseline(n_cells, seconds_target=12.0):
                       "OpenMP %d threads, -O3 x86-64-v3)" % (n, steps, cores)}
 
 
+def deck_dict(deck):
+    """A library Deck as the oracle's deck mapping."""
+    s = deck.s
+    geo = {1: "cuboid", 2: "sphere", 3: "point"}
+    states = []
+    for i in range(s.number_of_states):
+        states.append(dict(density=s.state_density[i], energy=s.state_energy[i],
+                           xvel=s.state_xvel[i], yvel=s.state_yvel[i], zvel=s.state_zvel[i],
+                           xmin=s.state_xmin[i], xmax=s.state_xmax[i], ymin=s.state_ymin[i],
+                           ymax=s.state_ymax[i], zmin=s.state_zmin[i], zmax=s.state_zmax[i],
+                           radius=s.state_radius[i], geometry=geo.get(s.state_geometry[i], "cuboid")))
+    return dict(x_cells=s.x_cells, y_cells=s.y_cells, z_cells=s.z_cells, xmin=s.xmin, ymin=s.ymin,
+                zmin=s.zmin, xmax=s.xmax, ymax=s.ymax, zmax=s.zmax,
+                initial_timestep=s.initial_timestep, max_timestep=s.max_timestep,
+                timestep_rise=s.timestep_rise, end_time=s.end_time, end_step=s.end_step,
+                summary_frequency=s.summary_frequency, states=states)
+
+
+def cpu_configs():
+    """The oracle's timing build (OpenMP, all host threads) on the benchmark
+    problem's configurations: 32^3 x 100 and 96^3 x 300 steps in full, 512^3
+    for 3 steps after one, and the two ensembles on samples of their seeded
+    decks run one after another (the rate over the sample's cells)."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_lib as O
+    import cloverleaf3d_ref_b200 as C
+    L = O.load(fast=True)
+    L.oracle_run_timed.restype = ctypes.c_double
+    out = {"cores": os.cpu_count() or 1, "build": "oracle C restatement, -O3 x86-64-v3, OpenMP",
+           "unit": "cell-updates/s"}
+
+    def timed(d, warm, steps):
+        od = O.make_deck(d)
+        return L.oracle_run_timed(ctypes.byref(od), warm, steps)
+
+    for key, n, steps, warm in (("config1_32", 32, 100, 0), ("config2_96", 96, 300, 0),
+                                ("config3_512_sample", 512, 3, 1)):
+        d = dict(deck_values(n, warm + steps + 1), states=STATES)
+        t = timed(d, warm, steps)
+        out[key] = {"value": n ** 3 * steps / t, "steps": steps, "seconds": t}
+    for key, nd, cells, steps, seed, sample in (("config4_64_decks_sample", 64, (24, 128), 150, 2024, 8),
+                                               ("config5_512_decks_sample", 512, (16, 48), 100, 4048, 64)):
+        decks = C.draw_decks(nd, seed, cells=cells, end_step=steps, summary_frequency=10)[:sample]
+        t = 0.0
+        work = 0
+        for dk in decks:
+            d = deck_dict(dk)
+            t += timed(d, 0, steps)
+            work += dk.cells * steps
+        out[key] = {"value": work / t, "decks_timed": sample, "steps": steps, "seconds": t}
+    return out
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -474,12 +527,18 @@ def main():
                     help="skip the 200-step FP64 vs mixed comparison")
     ap.add_argument("--ensemble-only", action="store_true",
                     help="only the ensemble legs (a separate JSON line)")
+    ap.add_argument("--cpu-configs", action="store_true",
+                    help="only the CPU restatement on every configuration (a separate JSON line)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
 
     if args.impl == "reference":
         return run_reference(args)
+    if args.cpu_configs:
+        if int(os.environ.get("RANK", "0")) == 0:
+            print(json.dumps({"cpu_configs": cpu_configs()}))
+        return 0
 
     import torch
     import torch.distributed as dist
