@@ -91,3 +91,44 @@ def test_rank_bricks_match_decomposed_oracle(world):
         np.testing.assert_allclose(o["sums"], np.array(ref.sums), rtol=1e-12, atol=1e-300)
         for f in FIELDS:
             assert np.array_equal(o["fields"][f], ref.h[r].a[f]), (r, f)
+
+
+def test_transport_failure_ends_the_run_with_an_error():
+    """A transport that reports a failure (a peer that is gone, a closed
+    channel) ends the brick driver with an error: the start fails when the
+    first exchange fails, and a run fails at the first reduction that fails.
+    One process, no peer: the callbacks are fakes."""
+    import ctypes
+    import cloverleaf3d_ref_b200 as C
+    from cloverleaf3d_ref_b200.ranks import TransportStruct, _EXCHANGE, _MIN, _SUM
+    L = C.lib()
+    deck = decks.to_deck(deck_dict())
+    calls = {"exchange": 0, "min": 0}
+
+    def exchange_ok(ctx, axis, lo, s_lo, r_lo, n_lo, hi, s_hi, r_hi, n_hi):
+        calls["exchange"] += 1
+        return 0  # leaves the received halo as it was
+
+    def exchange_fail(*a):
+        calls["exchange"] += 1
+        return 1
+
+    def min_fail(ctx, p):
+        calls["min"] += 1
+        return 1
+
+    def ok_sum(ctx, p, n):
+        return 0
+
+    cbs = [_EXCHANGE(exchange_fail), _MIN(min_fail), _SUM(ok_sum)]
+    t = TransportStruct(None, 1, cbs[0], cbs[1], cbs[2])
+    L.clover_gpu_clear_status()
+    h = L.clover_bricks_create_rank(ctypes.byref(deck.s), 2, 0, ctypes.byref(t))
+    assert not h and calls["exchange"] == 1
+    cbs = [_EXCHANGE(exchange_ok), _MIN(min_fail), _SUM(ok_sum)]
+    t = TransportStruct(None, 1, cbs[0], cbs[1], cbs[2])
+    h = L.clover_bricks_create_rank(ctypes.byref(deck.s), 2, 0, ctypes.byref(t))
+    assert h
+    assert L.clover_bricks_run(h, 5) == -1 and calls["min"] == 1
+    L.clover_bricks_destroy(h)
+    L.clover_gpu_clear_status()
