@@ -9,7 +9,7 @@ TWO_STATE = [
 
 
 def shock(nx, ny, nz, steps, states=None, **kw):
-    """The two-state shock on [0,10]^3 (BASELINE config geometry)."""
+    """The two-state shock on [0,10]^3 (the benchmark problem's geometry)."""
     d = dict(x_cells=nx, y_cells=ny, z_cells=nz, xmin=0.0, ymin=0.0, zmin=0.0,
              xmax=10.0, ymax=10.0, zmax=10.0, initial_timestep=0.04, max_timestep=0.04,
              timestep_rise=1.5, end_step=steps, end_time=1000.0, summary_frequency=10,
