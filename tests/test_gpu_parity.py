@@ -241,3 +241,27 @@ def test_mom_volumes_formed_again_after_host_change_or_other_call():
         h.flux_calc()
         h.advec_mom(3, 1, 1)
     check(["vol_flux_x", "vol_flux_y", "vol_flux_z", "wa6", "wa7", "zvel1"])
+
+
+def test_array_passed_with_another_chunks_bounds_is_refused():
+    """An array is the chunk's whose bounds it was first passed with. Passed
+    with other bounds, the call sets CLOVER_STATUS_BOUNDS and runs on a zeroed
+    stand-in (no access outside any allocation); the array keeps its values."""
+    L = C.lib()
+    names = ("density0", "energy0", "pressure", "soundspeed")
+    a = {n: np.zeros(O.shape("cell", 6, 5, 4), order="F") for n in names}
+    a["density0"][:] = 1.0
+    a["energy0"][:] = 2.0
+
+    def call(bounds):
+        L.clover_ideal_gas_kernel(*[ctypes.byref(ctypes.c_int(v)) for v in bounds],
+                                  *[a[n].ctypes.data_as(ctypes.c_void_p) for n in names])
+        L.clover_gpu_synchronize()
+
+    call((1, 6, 1, 5, 1, 4))
+    assert L.clover_gpu_status() == 0
+    call((1, 8, 1, 8, 1, 8))
+    assert L.clover_gpu_status() & 0x2
+    L.clover_gpu_clear_status()
+    L.clover_gpu_sync_to_host()
+    assert np.all(a["pressure"][2:8, 2:7, 2:6] == (1.4 - 1.0) * 1.0 * 2.0)
