@@ -7,10 +7,11 @@ A "step" is one full hydro step (hydro.f90:52-72, summaries included).
 
 value      device-resident chunk (native API), inputs already in HBM, steps
            replayed from CUDA graphs; cells * steps / device time.
-e2e        the same workload through the drop-in C ABI with HOST arrays: the
-           reference control flow calling clover_*_kernel, the first call of
-           each array uploading it and a final copy back of every array, all
-           inside the timed region.
+e2e        the configuration's whole run (200 steps at 512^3, --e2e-steps)
+           through the drop-in C ABI with HOST arrays: the reference control
+           flow calling clover_*_kernel, the first call of each array
+           uploading it and a final copy back of every array, all inside the
+           timed region.
 roofline   dominant kernel group, algorithmic bytes / its event-timed duration
            (a profiled run of the same steps right after the timed one).
 cpu_baseline  the oracle (C restatement of the reference, OpenMP) on the
@@ -58,6 +59,11 @@ def deck_values(n, steps):
     return dict(x_cells=n, y_cells=n, z_cells=n, xmin=0.0, ymin=0.0, zmin=0.0, xmax=10.0,
                 ymax=10.0, zmax=10.0, initial_timestep=0.04, max_timestep=0.04,
                 timestep_rise=1.5, end_step=steps, end_time=1.0e6, summary_frequency=10)
+
+
+def workload_name(n, precision):
+    """The workload both arms run: the benchmark problem at n^3 cells."""
+    return "two-state shock %d^3, %s" % (n, precision)
 
 
 def load_peaks():
@@ -216,8 +222,14 @@ def run_reference(args):
         pass
     if need * 1.5 > avail:
         n = 256
-    steps = max(1, min(args.steps, 5 if n >= 512 else args.steps))
-    warm = min(args.warmup, 1)
+    # K timed steps after W warm-up ones, as the GPU arm; if the host would
+    # need more than about four minutes for them (a calibration step first),
+    # fewer steps, reported in "steps"
+    d1 = O.make_deck(dict(deck_values(n, 3), states=STATES))
+    per_step = L.oracle_run_timed(ctypes.byref(d1), 0, 1)
+    budget = max(1, int(240.0 / max(per_step, 1e-9)))
+    warm = min(args.warmup, max(0, budget - args.steps))
+    steps = max(1, min(args.steps, budget - warm))
     d = O.make_deck(dict(deck_values(n, steps + warm + 1), states=STATES))
     t = L.oracle_run_timed(ctypes.byref(d), warm, steps)
     v = n ** 3 * steps / t
@@ -226,8 +238,10 @@ def run_reference(args):
         "n_gpus": args.gpus, "steps": steps, "warmup": warm, "ms_per_step": 1000.0 * t / steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic: two-state shock deck generated on the host",
-        "config": {"workload": "two-state shock %d^3 FP64 (%s)" % (
-            n, "configured size" if n == args.cells else "reduced from %d^3: host memory" % args.cells)},
+        "config": {"workload": workload_name(n, "fp64"),
+                   "execution": "CPU restatement, OpenMP %d threads" % cores,
+                   "size": "configured" if n == args.cells else
+                           "reduced from %d^3: host memory" % args.cells},
         "cpu_baseline": {"value": v, "unit": "cell-updates/s", "cores": cores, "kind": "port",
                          "sample": "%d^3 cells x %d steps after %d warm-up (oracle C restatement of "
                                    "the reference; the Fortran reference needs a Fortran compiler, "
@@ -466,8 +480,8 @@ def e2e_dropin(C, args, n, steps):
             "d2h_bytes_per_step": (host_bytes + 8 * taken + 40 * (taken // 10 + 2)) / taken,
             "seconds": t1 - t0, "steps": taken, "cells": "%d^3" % n, "ranks": 1,
             "setup_seconds_untimed": t0 - ts,
-            "timed": "upload of every host array (pinned) at its first use, the steps, "
-                     "per-step dt and summary reads, every array copied back"}
+            "timed": "the deck's whole run: upload of every host array (pinned) at its first "
+                     "use, the steps, per-step dt and summary reads, every array copied back"}
 
 
 def bricks_leg(C, n=256, n_bricks=8, steps=10):
@@ -527,6 +541,10 @@ def main():
                     help="skip the 200-step FP64 vs mixed comparison")
     ap.add_argument("--ensemble-only", action="store_true",
                     help="only the ensemble legs (a separate JSON line)")
+    ap.add_argument("--detail", default=None,
+                    help="also write the line with the per-summary accuracy arrays to this file")
+    ap.add_argument("--e2e-steps", type=int, default=200,
+                    help="steps of the end-to-end run (the configuration's full deck: 200)")
     ap.add_argument("--cpu-configs", action="store_true",
                     help="only the CPU restatement on every configuration (a separate JSON line)")
     args = ap.parse_args()
@@ -648,7 +666,7 @@ def main():
     # 512^3), so it runs on rank 0 only, as the reference arm does
     e2e = None
     if not args.no_e2e and rank == 0:
-        e2e = e2e_dropin(C, args, n, args.steps)
+        e2e = e2e_dropin(C, args, n, args.e2e_steps)
     cpu = None
     if not args.no_cpu and rank == 0 and world == 1:
         cpu = cpu_baseline(n)
@@ -665,25 +683,44 @@ def main():
                            "clock": "host wall time"},
             "vs_baseline": None, "dtype": "f64" if prec == C.PRECISION_FP64 else "f32/f64 mixed",
             "data": "synthetic: two-state shock deck generated on the device",
-            "config": {"workload": "two-state shock %d^3, %s, graph-replayed steps" % (
-                n, args.precision), "cells": n ** 3, "parallelism": "replicas only",
-                "l2": "inputs larger than L2 (each field %.2f GB)" % ((n + 5) ** 3 * 8 / 1e9)},
+            "config": {"workload": workload_name(n, args.precision),
+                       "execution": "device-resident chunk, graph-replayed steps",
+                       "cells": n ** 3, "parallelism": "replicas only",
+                       "l2": "inputs larger than L2 (each field %.2f GB)" % ((n + 5) ** 3 * 8 / 1e9)},
             "gpu_launches": launches * args.steps + 2 * (args.steps // 10 + 1),
             "clocks": clocks, "roofline": roofline, "per_kernel": per_kernel,
             "status": status,
             "last_summary": {"step": int(sum_steps[-1]), "vol_mass_ie_ke_press":
                              [float(x) for x in summaries[-1]]},
         }
-        if mixed:
-            line["mixed_fp32"] = mixed
-        if e2e:
-            line["e2e"] = e2e
-        if cpu:
-            line["cpu_baseline"] = cpu
+        # bulky detail first, the headline figures last (a reader that keeps
+        # only the end of the line keeps those)
+        detail = {}
+        if mixed and "accuracy_200_steps" in mixed:
+            detail["mixed_fp32_accuracy_200_steps"] = mixed["accuracy_200_steps"]
+            acc = mixed.pop("accuracy_200_steps")
+            mixed["accuracy_200_steps"] = {k: acc[k] for k in ("steps", "cells", "max_rel_err",
+                                                                "within_1e-5")}
         if ens:
             line["ensemble"] = ens
         if bricks:
             line["bricks_decomposition"] = bricks
+        if mixed:
+            line["mixed_fp32"] = mixed
+        if cpu:
+            line["cpu_baseline"] = cpu
+        if e2e:
+            line["e2e"] = e2e
+        if mixed:
+            line["mixed_fp32_summary"] = {
+                k: mixed[k] for k in ("value", "ms_per_step", "speedup_vs_fp64")}
+            if "accuracy_200_steps" in mixed:
+                line["mixed_fp32_summary"]["max_rel_err_200_steps"] = \
+                    mixed["accuracy_200_steps"]["max_rel_err"]
+        line["roofline"] = line.pop("roofline")
+        if args.detail:
+            with open(args.detail, "w") as f:
+                json.dump(dict(line, **detail), f, indent=1)
         print(json.dumps(line))
     if world > 1:
         dist.destroy_process_group()

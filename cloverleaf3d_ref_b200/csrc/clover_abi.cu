@@ -33,6 +33,7 @@ struct Context {
   bool ready = false;
   Geom g{};
   cudaStream_t stream = nullptr;
+  int device = -1;  // the device current when the context was created
   std::unordered_map<const void*, Mirror> mirrors;
   std::vector<void*> scratch;  // arrays standing in for mirrors passed with another chunk's bounds
   unsigned long long* d_key = nullptr;
@@ -96,6 +97,7 @@ bool enter(const int* x_min, const int* x_max, const int* y_min, const int* y_ma
       return false;
     }
     c.g = make_geom(*x_min, *x_max, *y_min, *y_max, *z_min, *z_max);
+    if (!check(cudaGetDevice(&c.device), "device")) return false;
     if (!check(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking), "stream")) return false;
     if (!check(cudaMalloc(&c.d_key, sizeof(unsigned long long)), "malloc")) return false;
     if (!check(cudaMalloc(&c.d_partials, summary_partials_len() * sizeof(double)), "malloc"))
@@ -128,6 +130,15 @@ bool is_device_pointer(const void* p) {
 }
 
 }  // namespace
+
+// The stream the drop-in entry points queue their kernels on, if the library
+// context exists and was created on device dev; null otherwise. A call that
+// reads arrays those kernels write in place orders itself after them by
+// launching on this stream.
+cudaStream_t abi_stream_on(int dev) {
+  Context& c = ctx();
+  return c.ready && c.device == dev ? c.stream : nullptr;
+}
 
 // Rows of hx elements between the host's contiguous planes (hy rows each) and
 // the mirror's pitched layout (row pitch px, plane pitch pxy): one block per
@@ -1018,6 +1029,8 @@ void clover_gpu_release(void) {
   c.msg = nullptr;
   c.msg_bytes = 0;
   cudaStreamDestroy(c.stream);
+  c.stream = nullptr;
+  c.device = -1;
   c.ready = false;
 }
 

@@ -13,6 +13,7 @@
 #include <cstdio>
 
 #include "clover_launch.h"
+#include "clover_sum.cuh"
 
 namespace clover {
 
@@ -773,30 +774,21 @@ __global__ void __launch_bounds__(BX * BY) k_reset(M m,
 // ---------------------------------------------------------------------------
 // field_summary_kernel.f90:57-77: a fixed grid of SUM_BLOCKS blocks strides
 // over the interior cells in a fixed assignment; each block tree-reduces its
-// five partials; a one-block pass adds the partials in block order. The
-// result is the same on every run.
+// five partials; a one-block pass adds the partials in block order. Every sum
+// carries a Neumaier compensation term through the thread's loop, the block
+// tree and the second stage (clover_sum.cuh). The result is the same on every
+// run.
 constexpr int SUM_THREADS = 256;
 constexpr int SUM_BLOCKS = 148 * 4;
 
-__device__ __forceinline__ void block_sum5(double v[5], double* sh /*5*SUM_THREADS*/) {
-  const int t = threadIdx.x;
-  for (int q = 0; q < 5; q++) sh[q * SUM_THREADS + t] = v[q];
-  __syncthreads();
-  for (int s = SUM_THREADS / 2; s > 0; s >>= 1) {
-    if (t < s)
-      for (int q = 0; q < 5; q++) sh[q * SUM_THREADS + t] += sh[q * SUM_THREADS + t + s];
-    __syncthreads();
-  }
-  for (int q = 0; q < 5; q++) v[q] = sh[q * SUM_THREADS];
-}
-
-// field_summary_kernel.f90:60-75 for cell (j,k,l), added to acc[5]
+// field_summary_kernel.f90:60-75 for cell (j,k,l), added to the compensated
+// sums (s, c)
 template <class S>
 __device__ __forceinline__ void summary_cell(const Geom& g, int j, int k, int l,
     const double* __restrict__ volume, const typename S::rho_t* __restrict__ density0,
     const typename S::ene_t* __restrict__ energy0, const typename S::cs_t* __restrict__ pressure,
     const typename S::vel_t* __restrict__ xvel0, const typename S::vel_t* __restrict__ yvel0,
-    const typename S::vel_t* __restrict__ zvel0, double acc[5]) {
+    const typename S::vel_t* __restrict__ zvel0, double s[kSumQ], double c[kSumQ]) {
   double vsqrd = 0.0;
   for (int lv = l; lv <= l + 1; lv++)
     for (int kv = k; kv <= k + 1; kv++)
@@ -806,11 +798,19 @@ __device__ __forceinline__ void summary_cell(const Geom& g, int j, int k, int l,
       }
   const double cell_vol = E(volume, j, k, l);
   const double cell_mass = cell_vol * L(density0, j, k, l);
-  acc[0] = acc[0] + cell_vol;
-  acc[1] = acc[1] + cell_mass;
-  acc[2] = acc[2] + cell_mass * L(energy0, j, k, l);
-  acc[3] = acc[3] + cell_mass * 0.5 * vsqrd;
-  acc[4] = acc[4] + cell_vol * L(pressure, j, k, l);
+  csum_add(s[0], c[0], cell_vol);
+  csum_add(s[1], c[1], cell_mass);
+  csum_add(s[2], c[2], cell_mass * L(energy0, j, k, l));
+  csum_add(s[3], c[3], cell_mass * 0.5 * vsqrd);
+  csum_add(s[4], c[4], cell_vol * L(pressure, j, k, l));
+}
+
+// partials: per block (or plane) the five sums s then their five compensations c
+__device__ __forceinline__ void store_csum(double* o, const double s[kSumQ], const double c[kSumQ]) {
+  for (int q = 0; q < kSumQ; q++) {
+    o[q] = s[q];
+    o[kSumQ + q] = c[q];
+  }
 }
 
 template <class S>
@@ -819,32 +819,33 @@ __global__ void __launch_bounds__(SUM_THREADS) k_summary(Geom g, const double* _
     const typename S::cs_t* __restrict__ pressure, const typename S::vel_t* __restrict__ xvel0,
     const typename S::vel_t* __restrict__ yvel0, const typename S::vel_t* __restrict__ zvel0,
     double* __restrict__ partials) {
-  __shared__ double sh[5 * SUM_THREADS];
+  __shared__ double sh[2 * kSumQ * SUM_THREADS];
   const int nx = g.x_max - g.x_min + 1, ny = g.y_max - g.y_min + 1, nz = g.z_max - g.z_min + 1;
   const long long n = (long long)nx * ny * nz;
-  double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-  for (long long c = (long long)blockIdx.x * SUM_THREADS + threadIdx.x; c < n;
-       c += (long long)SUM_BLOCKS * SUM_THREADS) {
-    const int j = g.x_min + (int)(c % nx);
-    const long long r = c / nx;
+  double s[kSumQ] = {0.0, 0.0, 0.0, 0.0, 0.0}, c[kSumQ] = {0.0, 0.0, 0.0, 0.0, 0.0};
+  for (long long i = (long long)blockIdx.x * SUM_THREADS + threadIdx.x; i < n;
+       i += (long long)SUM_BLOCKS * SUM_THREADS) {
+    const int j = g.x_min + (int)(i % nx);
+    const long long r = i / nx;
     const int k = g.y_min + (int)(r % ny);
     const int l = g.z_min + (int)(r / ny);
-    summary_cell<S>(g, j, k, l, volume, density0, energy0, pressure, xvel0, yvel0, zvel0, acc);
+    summary_cell<S>(g, j, k, l, volume, density0, energy0, pressure, xvel0, yvel0, zvel0, s, c);
   }
-  block_sum5(acc, sh);
-  if (threadIdx.x == 0)
-    for (int q = 0; q < 5; q++) partials[blockIdx.x * 5 + q] = acc[q];
+  block_csum<SUM_THREADS>(s, c, sh);
+  if (threadIdx.x == 0) store_csum(partials + blockIdx.x * 2 * kSumQ, s, c);
 }
 
+// The block partials merged in a fixed tree; out5 = s + c per quantity.
 __global__ void __launch_bounds__(SUM_THREADS) k_summary_final(const double* __restrict__ partials,
                                                                double* __restrict__ out5) {
-  __shared__ double sh[5 * SUM_THREADS];
-  double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+  __shared__ double sh[2 * kSumQ * SUM_THREADS];
+  double s[kSumQ] = {0.0, 0.0, 0.0, 0.0, 0.0}, c[kSumQ] = {0.0, 0.0, 0.0, 0.0, 0.0};
   for (int i = threadIdx.x; i < SUM_BLOCKS; i += SUM_THREADS)
-    for (int q = 0; q < 5; q++) acc[q] = acc[q] + partials[i * 5 + q];
-  block_sum5(acc, sh);
+    for (int q = 0; q < kSumQ; q++)
+      csum_merge(s[q], c[q], partials[i * 2 * kSumQ + q], partials[i * 2 * kSumQ + kSumQ + q]);
+  block_csum<SUM_THREADS>(s, c, sh);
   if (threadIdx.x == 0)
-    for (int q = 0; q < 5; q++) out5[q] = acc[q];
+    for (int q = 0; q < kSumQ; q++) out5[q] = s[q] + c[q];
 }
 
 // Per-deck summaries of an ensemble: tile z = one z plane of one deck, its
@@ -856,34 +857,32 @@ __global__ void __launch_bounds__(SUM_THREADS) k_summary_plane(M m,
     const typename S::cs_t* __restrict__ pressure, const typename S::vel_t* __restrict__ xvel0,
     const typename S::vel_t* __restrict__ yvel0, const typename S::vel_t* __restrict__ zvel0,
     double* __restrict__ partials) {
-  __shared__ double sh[5 * SUM_THREADS];
+  __shared__ double sh[2 * kSumQ * SUM_THREADS];
   m.run([&](const Geom& g, const Tile& t) {
     const int nx = g.x_max - g.x_min + 1, ny = g.y_max - g.y_min + 1;
     const int l = g.z_min + t.z;
-    double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-    for (int c = threadIdx.x; c < nx * ny; c += SUM_THREADS)
-      summary_cell<S>(g, g.x_min + c % nx, g.y_min + c / nx, l, volume, density0, energy0,
-                      pressure, xvel0, yvel0, zvel0, acc);
-    block_sum5(acc, sh);
-    if (threadIdx.x == 0) {
-      double* o = partials + 5 * ((long long)plane_base[t.d] + t.z);
-      for (int q = 0; q < 5; q++) o[q] = acc[q];
-    }
+    double s[kSumQ] = {0.0, 0.0, 0.0, 0.0, 0.0}, c[kSumQ] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    for (int i = threadIdx.x; i < nx * ny; i += SUM_THREADS)
+      summary_cell<S>(g, g.x_min + i % nx, g.y_min + i / nx, l, volume, density0, energy0,
+                      pressure, xvel0, yvel0, zvel0, s, c);
+    block_csum<SUM_THREADS>(s, c, sh);
+    if (threadIdx.x == 0) store_csum(partials + 2 * kSumQ * ((long long)plane_base[t.d] + t.z), s, c);
   });
 }
 
-// One block per deck: its plane partials added in plane order.
+// One block per deck: its plane partials merged in a fixed tree.
 __global__ void __launch_bounds__(SUM_THREADS) k_summary_decks(const int* __restrict__ plane_base,
     const double* __restrict__ partials, double* __restrict__ out) {
-  __shared__ double sh[5 * SUM_THREADS];
+  __shared__ double sh[2 * kSumQ * SUM_THREADS];
   const int d = blockIdx.x;
   const int p0 = plane_base[d], p1 = plane_base[d + 1];
-  double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+  double s[kSumQ] = {0.0, 0.0, 0.0, 0.0, 0.0}, c[kSumQ] = {0.0, 0.0, 0.0, 0.0, 0.0};
   for (int i = p0 + (int)threadIdx.x; i < p1; i += SUM_THREADS)
-    for (int q = 0; q < 5; q++) acc[q] = acc[q] + partials[i * 5 + q];
-  block_sum5(acc, sh);
+    for (int q = 0; q < kSumQ; q++)
+      csum_merge(s[q], c[q], partials[i * 2 * kSumQ + q], partials[i * 2 * kSumQ + kSumQ + q]);
+  block_csum<SUM_THREADS>(s, c, sh);
   if (threadIdx.x == 0)
-    for (int q = 0; q < 5; q++) out[d * 5 + q] = acc[q];
+    for (int q = 0; q < kSumQ; q++) out[d * kSumQ + q] = s[q] + c[q];
 }
 
 // ---------------------------------------------------------------------------
@@ -1341,7 +1340,7 @@ void launch_reset_field(const Target& tg, cudaStream_t s, typename S::rho_t* den
                 yvel1, zvel0, zvel1);
 }
 
-int summary_partials_len() { return SUM_BLOCKS * 5; }
+int summary_partials_len() { return SUM_BLOCKS * 2 * kSumQ; }
 
 template <class S>
 void launch_field_summary(const Geom& g, cudaStream_t s, const double* volume,

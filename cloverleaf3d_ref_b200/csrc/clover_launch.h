@@ -286,8 +286,9 @@ void launch_reset_field(const Target& tg, cudaStream_t s, typename S::rho_t* den
 
 // Per-deck sums of a plan's decks: out holds 5 doubles per deck. Each deck
 // sums its z planes (one block each, a fixed tree order) into
-// partials[(plane_base[d] + plane) * 5 ...], then one block per deck adds its
-// planes in order. plane_base: device array of the decks' first plane index.
+// partials[(plane_base[d] + plane) * 10 ...] (five compensated sums, then
+// their five compensation terms), then one block per deck merges its planes in
+// a fixed tree. plane_base: device array of the decks' first plane index.
 template <class S>
 void launch_field_summary_batch(BatchPlan* plan, int n_decks, cudaStream_t s,
                                 const int* plane_base, const double* volume,
@@ -296,7 +297,8 @@ void launch_field_summary_batch(BatchPlan* plan, int n_decks, cudaStream_t s,
                                 const typename S::vel_t* yvel0, const typename S::vel_t* zvel0,
                                 double* partials, double* out);
 
-// Sums (vol, mass, ie, ke, press) into out5 (device), deterministic order.
+// Sums (vol, mass, ie, ke, press) into out5 (device), deterministic order,
+// each with a Neumaier compensation term through every stage (clover_sum.cuh).
 // partials: device scratch of summary_partials_len() doubles.
 int summary_partials_len();
 template <class S>

@@ -353,7 +353,8 @@ struct Chunk : ChunkBase {
     dt_hist = (double*)p;
     ok = ok && cudaMalloc(&p, (size_t)nd * sum_cap * 5 * sizeof(double)) == cudaSuccess;
     sum_hist = (double*)p;
-    const size_t np = plan ? (size_t)planes * 5 : (size_t)summary_partials_len();
+    // per plane (ensemble) or per block: five sums and their five compensations
+    const size_t np = plan ? (size_t)planes * 10 : (size_t)summary_partials_len();
     ok = ok && cudaMalloc(&p, np * sizeof(double)) == cudaSuccess;
     partials = (double*)p;
     if (ok && plan) {

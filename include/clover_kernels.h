@@ -137,17 +137,23 @@ void clover_field_summary_kernel(const int *x_min, const int *x_max, const int *
  * memory is all owned by its own pool allocator or held under a fixed budget,
  * where a cudaMalloc made inside the library could fail or fragment that
  * pool. It allocates nothing: the arrays are the caller's DEVICE arrays in
- * the chunk layout of clover_gpu_layout() (host arrays are rejected), the
- * five sums come back in host scalars, and the reduction scratch is a fixed
- * 160 KiB file-scope device array that every GPU loading the library holds
- * until the process exits. At most CLOVER_NOALLOC_MAX_Z_CELLS cells along z
- * (larger grids return CLOVER_STATUS_BAD_ARG with a message on stderr).
- * Runs on the legacy default stream and returns when the sums are on the
- * host; 0 on success, else a CLOVER_STATUS_* bit. The first call on a device
- * looks up the scratch address (once per device); make that first call
- * before any stream capture. All calls share the one scratch array: calls
- * that overlap on the GPU race. Sums agree with clover_field_summary_kernel
- * to rounding (a different, fixed reduction order). */
+ * the chunk layout of clover_gpu_layout(), on the current device (host
+ * arrays and another GPU's arrays are rejected), the five sums come back in
+ * host scalars, and the reduction scratch is a fixed 320 KiB file-scope
+ * device array that every GPU loading the library holds until the process
+ * exits. At most CLOVER_NOALLOC_MAX_Z_CELLS cells along z (larger grids
+ * return CLOVER_STATUS_BAD_ARG with a message on stderr).
+ * It runs on the library's stream when the drop-in context exists on the
+ * current device, so it reads the arrays after every clover_*_kernel call
+ * queued before it (those return without waiting); otherwise on the legacy
+ * default stream. Work the caller queued on its own streams must be finished
+ * first. Returns when the sums are on the host; 0 on success, else a
+ * CLOVER_STATUS_* bit. The first call on a device looks up the scratch
+ * address (once per device; a cudaDeviceReset after it is not supported);
+ * make that first call before any stream capture. All calls share the one
+ * scratch array: calls that overlap on the GPU race. Sums agree with
+ * clover_field_summary_kernel to rounding (both compensated, in different
+ * fixed orders). */
 #define CLOVER_NOALLOC_MAX_Z_CELLS 4096
 int clover_field_summary_kernel_noalloc(const int *x_min, const int *x_max, const int *y_min,
                                         const int *y_max, const int *z_min, const int *z_max,

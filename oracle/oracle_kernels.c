@@ -551,9 +551,17 @@ void oracle_advec_cell_kernel(const int *x_min, const int *x_max, const int *y_m
       }
     }
 
-    /* the y flux pass runs l up to z_max+2 (:220) */
+    /* the y flux pass runs l up to z_max+2 (:220); the test-only
+     * ORACLE_SYMMETRIC_HALO build stops it at z_max, like the x and z passes
+     * (the rotation tests use it to show that this range is what separates a
+     * flow along y from the same flow along x) */
+#ifdef ORACLE_SYMMETRIC_HALO
+    const int y_flux_l_hi = *z_max;
+#else
+    const int y_flux_l_hi = *z_max + 2;
+#endif
 #pragma omp parallel for
-    for (int l = *z_min; l <= *z_max + 2; l++)
+    for (int l = *z_min; l <= y_flux_l_hi; l++)
       for (int k = *y_min; k <= *y_max + 2; k++)
         for (int j = *x_min; j <= *x_max; j++) {
           int upwind, donor, downwind, dif;

@@ -25,6 +25,35 @@ def test_problem_1():
                 end_step=75, states=TWO_STATE)
 
 
+def rotated(d, axis):
+    """The deck with its x axis exchanged for axis 1 (y) or 2 (z): cell
+    counts, domain bounds, and each state's bounds and velocity move with the
+    axis, so a flow along x becomes the same flow along y or z."""
+    if axis == 0:
+        return dict(d, states=[dict(s) for s in d["states"]])
+    a = "xyz"[axis]
+    r = dict(d)
+    for kx, ka in (("x_cells", a + "_cells"), ("xmin", a + "min"), ("xmax", a + "max")):
+        if kx in d or ka in d:
+            r[kx], r[ka] = d.get(ka), d.get(kx)
+    states = []
+    for s in d["states"]:
+        t = {k: v for k, v in s.items() if k not in ("xmin", "xmax", "xvel", a + "min", a + "max", a + "vel")}
+        for kx, ka in (("xmin", a + "min"), ("xmax", a + "max"), ("xvel", a + "vel")):
+            if ka in s:
+                t[kx] = s[ka]
+            if kx in s:
+                t[ka] = s[kx]
+        states.append(t)
+    r["states"] = states
+    return r
+
+
+def test_problem_1_along(axis):
+    """test_problem_1 with its flow along x (0), y (1) or z (2)."""
+    return rotated(test_problem_1(), axis)
+
+
 # A deck with every geometry kind and moving states, on an uneven grid.
 MIXED_STATES = [
     dict(density=0.2, energy=1.0, xvel=0.1),

@@ -15,6 +15,9 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 ORACLE_DIR = os.path.join(ROOT, "oracle")
 LIB_PATH = os.path.join(ORACLE_DIR, "_build", "liboracle.so")
 FAST_LIB_PATH = os.path.join(ORACLE_DIR, "_build", "liboracle_fast.so")
+# parity build with two direction-dependent extents of the reference made
+# symmetric (ORACLE_SYMMETRIC_HALO): only the rotation tests load it
+SYMMETRIC_LIB_PATH = os.path.join(ORACLE_DIR, "_build", "liboracle_symmetric.so")
 
 # Reference field ids (data.f90:55-74), 1-based, in order.
 FIELD_NAMES = [
@@ -73,8 +76,8 @@ def build():
 _LIBS = {}
 
 
-def load(fast=False):
-    path = FAST_LIB_PATH if fast else LIB_PATH
+def load(fast=False, symmetric=False):
+    path = SYMMETRIC_LIB_PATH if symmetric else FAST_LIB_PATH if fast else LIB_PATH
     if path not in _LIBS:
         if not os.path.exists(path):
             build()
@@ -119,9 +122,9 @@ def make_deck(d):
     return od
 
 
-def run(deck, max_steps=None, want_fields=False, fast=False):
+def run(deck, max_steps=None, want_fields=False, fast=False, symmetric=False):
     """Run the oracle hydro loop. Returns dict(dt, summaries, summary_steps, steps, fields)."""
-    lib = load(fast)
+    lib = load(fast, symmetric)
     od = make_deck(deck)
     if max_steps is None:
         max_steps = od.end_step

@@ -5,6 +5,7 @@ import os
 
 import numpy as np
 
+import decks
 import oracle_lib as O
 
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
@@ -135,3 +136,88 @@ def test_depth_two_halo_update_rewrites_every_halo_cell_of_cell_and_vertex_field
             H.Hydro(H.Backend(lib, "oracle_"), arr, nx, ny, nz, deck).halo(list(range(1, 20)), 2)
         for k in fields:
             assert np.array_equal(a[k].view(np.uint64), b[k].view(np.uint64)), (nx, ny, nz, k)
+
+
+# test_problem_1 turned onto y and z: the x axis and each axis it is exchanged
+# with swap places, so arrays of the rotated run transpose onto the x run's.
+_PERM = {1: (1, 0, 2), 2: (2, 1, 0)}
+
+
+def _x_name(n, axis):
+    """The rotated run's name for the x run's array n (velocity and face-flux
+    components move with their axis)."""
+    a = "xyz"[axis]
+    swap = {"x": a, a: "x"}
+    for c in "xyz":
+        for suffix in ("vel0", "vel1"):
+            if n == c + suffix:
+                return swap.get(c, c) + suffix
+        for prefix in ("vol_flux_", "mass_flux_"):
+            if n == prefix + c:
+                return prefix + swap.get(c, c)
+    return n
+
+
+def test_known_answer_with_the_flow_along_y_and_z():
+    """The test_problem_1 shock run along y and along z meets the reference's
+    own criterion (final KE within 0.001% of 3.64560737191257,
+    field_summary.f90:119-136), so the y and z forms of the cell and momentum
+    sweeps, their limiters, the y- and z-face halo rules and flux_calc's z
+    form carry the known answer, not only the x forms."""
+    g = json.load(open(os.path.join(GOLDEN, "test_problem_1.json")))
+    for axis in (1, 2):
+        r = O.run(decks.rotated(g["deck"], axis))
+        assert r["steps"] == 75
+        ke = r["summaries"][-1][3]
+        assert abs(100.0 * (ke / g["final_kinetic_energy"]) - 100.0) < g["tolerance_percent"]
+
+
+def test_rotations_differ_only_by_the_reference_halo_extents():
+    """What separates the x, y and z runs of test_problem_1 is two
+    direction-dependent extents of the reference, nothing in the restated
+    arithmetic:
+    - update_halo_kernel.f90 reflects the x and y face fluxes on the z faces
+      over their face axis up to max+d (:1018-1142, :1156-1280), one node short
+      of the z face fluxes' max+1+d (:1294-1417), so mass_flux_x(x_max+3) and
+      mass_flux_y(y_max+3) in the z halo planes stay stale (the x and y
+      momentum sweeps read them);
+    - the y cell sweep forms fluxes up to z_max+2 (advec_cell_kernel.f90:220),
+      into the z halo planes.
+    The oracle built with both made symmetric (ORACLE_SYMMETRIC_HALO) gives
+    the three rotations' summaries equal to 1e-14 at every step and dt equal
+    bit for bit: the x, y and z forms of every kernel are the same arithmetic.
+    The reference build's x run, with the stale corner, reproduces the known
+    answer to 1e-15, while the symmetric build misses it by 7e-9: the known
+    answer pins the stale corner too."""
+    g = json.load(open(os.path.join(GOLDEN, "test_problem_1.json")))
+    d = dict(g["deck"], summary_frequency=5)
+    sym = [O.run(decks.rotated(d, a), symmetric=True) for a in range(3)]
+    for a in (0, 1):
+        assert np.array_equal(sym[a]["dt"], sym[2]["dt"])
+        np.testing.assert_allclose(sym[a]["summaries"], sym[2]["summaries"], rtol=1e-14, atol=0)
+    ke_ref = O.run(d)["summaries"][-1][3]
+    ke_sym = sym[0]["summaries"][-1][3]
+    assert abs(ke_ref / g["final_kinetic_energy"] - 1.0) < 1e-14
+    assert abs(ke_sym / g["final_kinetic_energy"] - 1.0) > 1e-9
+
+
+def test_rotated_runs_equal_the_x_run_to_rounding():
+    """Before the stale corners reach the flow, every field of the y and z
+    runs, transposed, equals the x run's to a few ulps and the transverse
+    velocities are exactly zero (20 steps). Bit for bit they differ by an ulp
+    from the first step: the cross-direction sweeps of a 1-D flow round
+    (advec_cell's energy update e*m/m, advec_cell_kernel.f90:173-185, and
+    advec_mom's velocity update v*m/m, advec_mom_kernel.f90:244-250, with zero
+    fluxes), and the sweep order alternates (advection.f90:43-179)."""
+    d = dict(decks.test_problem_1(), end_step=20, summary_frequency=5)
+    rx = O.run(d, want_fields=True)
+    for axis in (1, 2):
+        rr = O.run(decks.rotated(d, axis), want_fields=True)
+        assert np.array_equal(rr["dt"], rx["dt"])
+        np.testing.assert_allclose(rr["summaries"], rx["summaries"], rtol=1e-14, atol=0)
+        for c in (c for c in "xyz" if c != "xyz"[axis]):
+            assert not np.any(rr["fields"][c + "vel0"]), (axis, c)
+        for n in O.FIELD_NAMES:
+            a = rx["fields"][n][2:-2, 2:-2, 2:-2]
+            b = rr["fields"][_x_name(n, axis)].transpose(_PERM[axis])[2:-2, 2:-2, 2:-2]
+            assert np.abs(a - b).max() <= 8 * np.spacing(np.abs(a).max()), (axis, n)

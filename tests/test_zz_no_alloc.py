@@ -84,3 +84,54 @@ def test_noalloc_field_summary_matches_regular_entry_point():
     rc = L.clover_field_summary_kernel_noalloc(*B, *hp, *[ctypes.byref(o) for o in got])
     assert rc == 0x10
     L.clover_gpu_release()
+
+
+def test_noalloc_orders_after_queued_library_kernels():
+    """The drop-in entry points queue their kernels and return at once. A
+    no-alloc summary called right after in-place clover_ideal_gas_kernel calls
+    on the caller's device arrays must read the pressure those calls write
+    (it was zero before them): its sums equal the regular entry point's, taken
+    afterwards, and the pressure sum is the ideal-gas one, not zero."""
+    torch = pytest.importorskip("torch")
+    assert torch.cuda.is_available()
+    L = C.lib()
+    L.clover_gpu_release()
+    L.clover_gpu_clear_status()
+    n = (160, 144, 128)
+    b = [ctypes.c_int(v) for v in (1, n[0], 1, n[1], 1, n[2])]
+    B = [ctypes.byref(v) for v in b]
+    px, pxy, elems = ctypes.c_int(0), ctypes.c_longlong(0), ctypes.c_longlong(0)
+    L.clover_gpu_layout(*B, ctypes.byref(px), ctypes.byref(pxy), ctypes.byref(elems))
+    planes = elems.value // pxy.value
+    rng = np.random.default_rng(3)
+    cell = (n[0] + 4, n[1] + 4, n[2] + 4)
+    vert = (n[0] + 5, n[1] + 5, n[2] + 5)
+    host = {
+        "volume": np.full(cell, 0.25), "density0": rng.uniform(0.1, 2.0, cell),
+        "energy0": rng.uniform(0.5, 3.0, cell), "pressure": np.zeros(cell),
+        "soundspeed": np.zeros(cell), "xvel0": rng.uniform(-1, 1, vert),
+        "yvel0": rng.uniform(-1, 1, vert), "zvel0": rng.uniform(-1, 1, vert),
+    }
+    dev = {k: _device_array(torch, np.asfortranarray(v), px.value, pxy.value, planes)
+           for k, v in host.items()}
+    torch.cuda.synchronize()
+    P = {k: ctypes.c_void_p(v.data_ptr()) for k, v in dev.items()}
+    names = ("volume", "density0", "energy0", "pressure", "xvel0", "yvel0", "zvel0")
+
+    def outs():
+        return [ctypes.c_double(0.0) for _ in range(5)]
+
+    L.clover_field_summary_kernel_noalloc.restype = ctypes.c_int
+    for _ in range(3):  # queued, not waited for
+        L.clover_ideal_gas_kernel(*B, P["density0"], P["energy0"], P["pressure"], P["soundspeed"])
+    got = outs()
+    rc = L.clover_field_summary_kernel_noalloc(*B, *[P[k] for k in names],
+                                               *[ctypes.byref(o) for o in got])
+    assert rc == 0
+    ref = outs()
+    L.clover_field_summary_kernel(*B, *[P[k] for k in names], *[ctypes.byref(o) for o in ref])
+    assert L.clover_gpu_status() == 0, L.clover_gpu_error_string()
+    want = np.array([o.value for o in ref])
+    assert want[4] > 0.0
+    np.testing.assert_allclose([o.value for o in got], want, rtol=RTOL, atol=0)
+    L.clover_gpu_release()
