@@ -537,6 +537,9 @@ def main():
     ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--no-ensemble", action="store_true")
     ap.add_argument("--no-bricks", action="store_true")
+    ap.add_argument("--no-tma", action="store_true",
+                    help="the register-marching forms of the stencils that stage their planes "
+                         "by bulk-tensor copies")
     ap.add_argument("--no-accuracy", action="store_true",
                     help="skip the 200-step FP64 vs mixed comparison")
     ap.add_argument("--ensemble-only", action="store_true",
@@ -588,6 +591,7 @@ def main():
     total = args.warmup + 2 * args.steps + 5
     deck = C.Deck.from_values(states=STATES, **deck_values(n, total))
     ch = C.Chunk(deck, prec)
+    tma = ch.use_tma(not args.no_tma)
     stream = torch.cuda.ExternalStream(ch.stream)
     # the first step on its own (hydro.f90 reports it apart): wall time of
     # ch.step(1), which also captures and instantiates the step's CUDA graphs
@@ -684,7 +688,8 @@ def main():
             "vs_baseline": None, "dtype": "f64" if prec == C.PRECISION_FP64 else "f32/f64 mixed",
             "data": "synthetic: two-state shock deck generated on the device",
             "config": {"workload": workload_name(n, args.precision),
-                       "execution": "device-resident chunk, graph-replayed steps",
+                       "execution": "device-resident chunk, graph-replayed steps" +
+                                    (", planes staged by bulk-tensor copies" if tma else ""),
                        "cells": n ** 3, "parallelism": "replicas only",
                        "l2": "inputs larger than L2 (each field %.2f GB)" % ((n + 5) ** 3 * 8 / 1e9)},
             "gpu_launches": launches * args.steps + 2 * (args.steps // 10 + 1),

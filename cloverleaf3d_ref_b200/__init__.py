@@ -142,6 +142,8 @@ def _declare(L):
         getattr(L, n).restype = ctypes.c_int
     L.clover_chunk_use_graphs.argtypes = [P, ctypes.c_int]
     L.clover_chunk_use_fused.argtypes = [P, ctypes.c_int]
+    L.clover_chunk_use_tma.argtypes = [P, ctypes.c_int]
+    L.clover_chunk_use_tma.restype = ctypes.c_int
     L.clover_chunk_time.argtypes = [P]
     L.clover_chunk_time.restype = ctypes.c_double
     L.clover_chunk_dt_history.argtypes = [P, P, ctypes.c_int]
@@ -329,6 +331,12 @@ class Chunk:
         """Fused kernels (default) or one kernel per reference loop nest; only
         before the first step."""
         lib().clover_chunk_use_fused(self.h, 1 if on else 0)
+
+    def use_tma(self, on):
+        """The fused step's stencils staged by bulk-tensor copies (default, one
+        chunk) or their register-marching forms; True if the staged forms are
+        in use."""
+        return lib().clover_chunk_use_tma(self.h, 1 if on else 0) == 1
 
     @property
     def steps(self):

@@ -32,6 +32,7 @@
 #include <cfloat>
 #include <type_traits>
 
+#include "clover_div.cuh"
 #include "clover_launch.h"
 
 namespace clover {
@@ -836,8 +837,9 @@ __device__ __forceinline__ A mom_flux_v(const MomNodeTerms<A>& t, A vm1, A v0, A
     A wind = A(1.0);
     if (vdiffdw <= A(0.0)) wind = A(-1.0);
     const A width = t.width, sigma = t.sigma;
-    limiter = wind * fmin2(fmin2(width * ((A(2.0) - sigma) * adw / width +
-                                          (A(1.0) + sigma) * auw / t.cd_dif) / A(6.0),
+    // ... / 6.0_8 correctly rounded by div6 (clover_div.cuh)
+    limiter = wind * fmin2(fmin2(div6(width * ((A(2.0) - sigma) * adw / width +
+                                               (A(1.0) + sigma) * auw / t.cd_dif)),
                                  auw),
                            adw);
   }

@@ -12,6 +12,7 @@
 #include <cfloat>
 #include <cstdio>
 
+#include "clover_div.cuh"
 #include "clover_launch.h"
 #include "clover_sum.cuh"
 
@@ -700,8 +701,9 @@ __device__ __forceinline__ double mom_limiter(double sigma, double width, double
     const double adw = fabs(vdiffdw);
     double wind = 1.0;
     if (vdiffdw <= 0.0) wind = -1.0;
-    limiter = wind * fmin2(fmin2(width * ((2.0 - sigma) * adw / width +
-                                          (1.0 + sigma) * auw / celld_dif) / 6.0,
+    // ... / 6.0_8 correctly rounded by div6 (clover_div.cuh)
+    limiter = wind * fmin2(fmin2(div6(width * ((2.0 - sigma) * adw / width +
+                                               (1.0 + sigma) * auw / celld_dif)),
                                  auw),
                            adw);
   }

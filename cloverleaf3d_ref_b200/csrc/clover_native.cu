@@ -20,6 +20,7 @@
 
 #include "clover_batch.h"
 #include "clover_launch.h"
+#include "clover_tma.cuh"
 #include "clover_visit.h"
 
 namespace clover {
@@ -151,6 +152,12 @@ struct Chunk : ChunkBase {
   bool advect_x = true;  // start.f90:99
   bool use_graphs = true;
   bool fused = true;  // fused kernels (clover_fused.cu) instead of one kernel per reference pass
+  // one chunk: stencils staged through shared memory by bulk-tensor copies
+  // (clover_tma.cu) where their tensor maps could be made; their
+  // register-marching forms otherwise, and for ensembles
+  bool tma = false;
+  bool use_tma = true;
+  ViscMaps visc_maps;
   // Every axis of every deck has at least three cells. A repeated halo update
   // of a cell field, a vertex velocity or a z-face flux, whose values have
   // not changed since its last update at the same depth, then rewrites every
@@ -336,6 +343,11 @@ struct Chunk : ChunkBase {
     }
     ga = GeomArrays{volume, xarea, yarea, zarea, cellx, celly, cellz, celldx, celldy, celldz,
                     vertexx, vertexy, vertexz, vertexdx, vertexdy, vertexdz};
+    // one chunk: the stencils that stage their planes with bulk-tensor copies
+    // get their tensor maps (the arrays they read never move)
+    if (!batched)
+      tma = visc_dt_tma_prepare<S>() &&
+            visc_dt_tma_maps<S>(g, xvel0, yvel0, zvel0, density0, energy0, &visc_maps);
 
     dt_cap = deck.end_step < (1 << 22) ? deck.end_step + 16 : (1 << 22);
     sum_cap = dt_cap / (deck.summary_frequency > 0 ? deck.summary_frequency : dt_cap) + 8;
@@ -740,9 +752,14 @@ struct Chunk : ChunkBase {
     halo({3, 1, 8, 10}, 1, vc, cb);
     pend("update_halo", 0);
     pbeg();
-    launch_visc_dt<S>(tg, stream, ga, kGSmall, deck.dtc_safe, deck.dtu_safe, deck.dtv_safe,
-                      deck.dtw_safe, deck.dtdiv_safe, density0, energy0, pressure, viscosity,
-                      soundspeed, xvel0, yvel0, zvel0, &sc->key);
+    if (tma && use_tma)
+      launch_visc_dt_tma<S>(g, stream, visc_maps, ga, kGSmall, deck.dtc_safe, deck.dtu_safe,
+                            deck.dtv_safe, deck.dtw_safe, deck.dtdiv_safe, pressure, viscosity,
+                            soundspeed, &sc->key, &sc->status);
+    else
+      launch_visc_dt<S>(tg, stream, ga, kGSmall, deck.dtc_safe, deck.dtu_safe, deck.dtv_safe,
+                        deck.dtw_safe, deck.dtdiv_safe, density0, energy0, pressure, viscosity,
+                        soundspeed, xvel0, yvel0, zvel0, &sc->key);
     k_dt_finalize<<<deck_blocks(), 128, 0, stream>>>(sc, nd, dt_hist);
     pend("eos_viscosity_calc_dt", n * (3 * V8 + R8 + E8 + 3 * C8));
     pbeg();
@@ -1402,6 +1419,17 @@ void clover_chunk_use_fused(clover_chunk* c, int on) {
     c->mixed->fused = on != 0;
     for (auto& gr : c->mixed->graph) if (gr) { cudaGraphExecDestroy(gr); gr = nullptr; }
   }
+}
+
+int clover_chunk_use_tma(clover_chunk* c, int on) {
+  auto set = [&](auto* ch) {
+    if (ch->use_tma != (on != 0)) {
+      ch->use_tma = on != 0;
+      ch->drop_graphs();  // the captured steps hold the other kernels
+    }
+    return ch->tma && ch->use_tma ? 1 : 0;
+  };
+  return c->f64 ? set(c->f64) : set(c->mixed);
 }
 
 void clover_chunk_profile(clover_chunk* c, int on) {

@@ -1,0 +1,360 @@
+// Kernels of the native step whose inputs are staged plane by plane into
+// shared memory with bulk-tensor copies (clover_tma.cuh), and the host-side
+// encoding of their tensor maps.
+//
+//  k_visc_dt_tma  viscosity_kernel.f90:71-134, calc_dt_kernel.f90:102-149
+//                 and ideal_gas_kernel.f90:47-58 on every interior cell, as
+//                 k_visc_dt (clover_fused.cu) forms them, operation for
+//                 operation. A block owns 32 x 8 columns (j, k) and marches
+//                 a segment of planes l; a ring of plane buffers holds, for
+//                 plane p, the node velocities of node plane p (9 rows x
+//                 32+2H columns) and density0 / energy0 of cell plane p (10
+//                 rows x 32+2H columns). Cell l reads node planes l, l+1 and
+//                 cell planes l-1, l, l+1; one thread refills the buffer of
+//                 plane l-1 with plane l-1+R once the block is done with l.
+#include <cfloat>
+#include <cstdio>
+
+#include <cudaTypedefs.h>
+
+#include "../../include/clover_kernels.h"
+#include "clover_launch.h"
+#include "clover_tma.cuh"
+
+namespace clover {
+
+bool encode_plane_map(CUtensorMap* map, const void* base, int elem_bytes, const Geom& g,
+                      int box_rows) {
+  static PFN_cuTensorMapEncodeTiled encode = nullptr;
+  if (!encode) {
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) !=
+            cudaSuccess ||
+        q != cudaDriverEntryPointSuccess || !fn) {
+      cudaGetLastError();
+      return false;
+    }
+    encode = (PFN_cuTensorMapEncodeTiled)fn;
+  }
+  const int halo = 16 / elem_bytes;
+  // the map starts halo columns before x_min (16-byte aligned: x_min is
+  // 128-byte aligned); base points at column x_min - 2
+  const char* start = (const char*)base - (long long)(halo - 2) * elem_bytes;
+  const cuuint64_t dims[3] = {(cuuint64_t)g.px, (cuuint64_t)(g.pxy / g.px),
+                              (cuuint64_t)(g.z_max - g.z_min + 6)};
+  const cuuint64_t strides[2] = {(cuuint64_t)g.px * elem_bytes, (cuuint64_t)g.pxy * elem_bytes};
+  const cuuint32_t box[3] = {(cuuint32_t)(32 + 2 * halo), (cuuint32_t)box_rows, 1};
+  const cuuint32_t estr[3] = {1, 1, 1};
+  const CUresult r =
+      encode(map, elem_bytes == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
+             3, (void*)start, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+             CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS;
+}
+
+namespace {
+
+constexpr int TX = 32, TY = 8;
+
+constexpr int round128(int b) { return (b + 127) / 128 * 128; }
+
+// Byte layout of one plane buffer of the viscosity ring.
+template <class S>
+struct ViscPlane {
+  using V = typename S::vel_t;
+  using R = typename S::rho_t;
+  using En = typename S::ene_t;
+  static constexpr int WV = kTmaWidth<V>, WR = kTmaWidth<R>, WE = kTmaWidth<En>;
+  static constexpr int HV = kTmaHalo<V>, HR = kTmaHalo<R>, HE = kTmaHalo<En>;
+  static constexpr int kNodeRows = TY + 1, kCellRows = TY + 2;
+  static constexpr int kVel = round128(kNodeRows * WV * (int)sizeof(V));
+  static constexpr int kRho = round128(kCellRows * WR * (int)sizeof(R));
+  static constexpr int kEne = round128(kCellRows * WE * (int)sizeof(En));
+  static constexpr int kBytes = 3 * kVel + kRho + kEne;  // one plane buffer
+  // bytes the five boxes of a plane deliver
+  static constexpr unsigned kTx = 3 * box_bytes<V>(kNodeRows) + box_bytes<R>(kCellRows) +
+                                  box_bytes<En>(kCellRows);
+  __device__ static V* vel(unsigned char* p, int q) { return (V*)(p + q * kVel); }
+  __device__ static R* rho(unsigned char* p) { return (R*)(p + 3 * kVel); }
+  __device__ static En* ene(unsigned char* p) { return (En*)(p + 3 * kVel + kRho); }
+};
+
+__device__ __forceinline__ double fmin2(double a, double b) { return b < a ? b : a; }
+__device__ __forceinline__ double fmax2(double a, double b) { return b > a ? b : a; }
+__device__ __forceinline__ float fmin2(float a, float b) { return b < a ? b : a; }
+__device__ __forceinline__ float fmax2(float a, float b) { return b > a ? b : a; }
+
+template <class T, class U>
+__device__ __forceinline__ T st(U v) { return (T)v; }
+
+template <class A>
+__device__ __forceinline__ A geo_ds(const Geom& g) { return sizeof(A) == 4 ? (A)g.ds_f : (A)g.ds; }
+
+template <class S, int RING, int MINB>
+__global__ void __launch_bounds__(TX * TY, MINB)
+k_visc_dt_tma(Geom g, int seg, GeomArrays ga, double g_small, double dtc_safe, double dtu_safe,
+              double dtv_safe, double dtw_safe, double dtdiv_safe,
+              const __grid_constant__ ViscMaps maps, typename S::cs_t* __restrict__ pressure,
+              typename S::cs_t* __restrict__ viscosity, typename S::cs_t* __restrict__ soundspeed,
+              unsigned long long* __restrict__ min_key, int* __restrict__ status) {
+  using P = ViscPlane<S>;
+  using A = typename S::arith_t;
+  using C = typename S::cs_t;
+  extern __shared__ __align__(128) unsigned char ring[];
+  __shared__ unsigned long long full[RING];
+  __shared__ unsigned long long wmin[TX * TY / 32];
+  __shared__ int stop;
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
+  const int j0 = g.x_min + TX * (int)blockIdx.x, k0 = g.y_min + TY * (int)blockIdx.y;
+  const int l0 = g.z_min + seg * (int)blockIdx.z;
+  const int l1 = l0 + seg - 1 < g.z_max ? l0 + seg - 1 : g.z_max;
+  const int j = j0 + tx, k = k0 + ty;
+  const bool in_jk = j <= g.x_max && k <= g.y_max;
+  const int pfirst = l0 - 1, plast = l1 + 1;  // cell planes the segment reads
+  if (tid == 0) {
+    for (int r = 0; r < RING; r++) mbar_init(&full[r], 1);
+    mbar_init_fence();
+    stop = 0;
+  }
+  __syncthreads();
+  int issued_hi = pfirst - 1;  // thread 0: the last plane whose copies it issued
+  // plane p (node plane p and cell plane p) into its buffer
+  auto issue = [&](int p) {
+    issued_hi = p;
+    const int s = (p - pfirst) % RING;
+    unsigned char* b = ring + s * P::kBytes;
+    mbar_arrive_expect_tx(&full[s], P::kTx);
+    const int x = TX * (int)blockIdx.x, z = p - g.z_min + 2;
+    const int yn = k0 - g.y_min + 2, yc = yn - 1;
+    tma_load_box(P::vel(b, 0), &maps.u, &full[s], x, yn, z);
+    tma_load_box(P::vel(b, 1), &maps.v, &full[s], x, yn, z);
+    tma_load_box(P::vel(b, 2), &maps.w, &full[s], x, yn, z);
+    tma_load_box(P::rho(b), &maps.d, &full[s], x, yc, z);
+    tma_load_box(P::ene(b), &maps.e, &full[s], x, yc, z);
+  };
+  if (tid == 0)
+    for (int p = pfirst; p <= plast && p < pfirst + RING; p++) issue(p);
+  auto buf = [&](int p) { return ring + ((p - pfirst) % RING) * P::kBytes; };
+  auto wait = [&](int p) {
+    const int u = p - pfirst;
+    if (!mbar_wait_bounded(&full[u % RING], (unsigned)(u / RING) & 1u)) stop = 1;
+  };
+  const A a_gs = (A)g_small, a_dtc = (A)dtc_safe, a_dtu = (A)dtu_safe, a_dtv = (A)dtv_safe;
+  const A a_dtw = (A)dtw_safe, a_dtdiv = (A)dtdiv_safe;
+  constexpr int WV = P::WV, WR = P::WR, WE = P::WE, HV = P::HV, HR = P::HR, HE = P::HE;
+  unsigned long long key = ~0ull;
+  wait(pfirst);
+  wait(pfirst + 1);
+  int l = l0;
+  for (; l <= l1; l++) {
+    wait(l + 1);
+    if (in_jk && !stop) {
+      unsigned char* bl = buf(l);
+      unsigned char* bu = buf(l + 1);
+      unsigned char* bd = buf(l - 1);
+      // node (j+a, k+b) of a node plane buffer, cell (j+a, k+b) of a cell plane buffer
+#define NV(bb, q, a, b) ((A)P::vel(bb, q)[(ty + (b)) * WV + tx + HV + (a)])
+#define DN(bb, a, b) ((A)P::rho(bb)[(ty + 1 + (b)) * WR + tx + HR + (a)])
+#define EN(bb, a, b) ((A)P::ene(bb)[(ty + 1 + (b)) * WE + tx + HE + (a)])
+      const A u000 = NV(bl, 0, 0, 0), u100 = NV(bl, 0, 1, 0), u010 = NV(bl, 0, 0, 1), u110 = NV(bl, 0, 1, 1);
+      const A v000 = NV(bl, 1, 0, 0), v100 = NV(bl, 1, 1, 0), v010 = NV(bl, 1, 0, 1), v110 = NV(bl, 1, 1, 1);
+      const A w000 = NV(bl, 2, 0, 0), w100 = NV(bl, 2, 1, 0), w010 = NV(bl, 2, 0, 1), w110 = NV(bl, 2, 1, 1);
+      const A u001 = NV(bu, 0, 0, 0), u101 = NV(bu, 0, 1, 0), u011 = NV(bu, 0, 0, 1), u111 = NV(bu, 0, 1, 1);
+      const A v001 = NV(bu, 1, 0, 0), v101 = NV(bu, 1, 1, 0), v011 = NV(bu, 1, 0, 1), v111 = NV(bu, 1, 1, 1);
+      const A w001 = NV(bu, 2, 0, 0), w101 = NV(bu, 2, 1, 0), w011 = NV(bu, 2, 0, 1), w111 = NV(bu, 2, 1, 1);
+      const A ugradx1 = u000 + u010 + u001 + u011;
+      const A ugradx2 = u100 + u110 + u101 + u111;
+      const A vgrady1 = v000 + v100 + v001 + v101;
+      const A vgrady2 = v010 + v110 + v011 + v111;
+      const A wgradz1 = w000 + w100 + w010 + w110;
+      const A wgradz2 = w001 + w101 + w011 + w111;
+      const A xa = (A)g.xa, ya = (A)g.ya, za = (A)g.za;
+      const A div = (xa * (ugradx2 - ugradx1) + ya * (vgrady2 - vgrady1)) + za * (wgradz2 - wgradz1);
+      A q = A(A(0.0));
+      if (!(div >= A(0.0))) {
+        const A ugrady1 = u000 + u100 + u001 + u101;
+        const A ugrady2 = u010 + u110 + u011 + u111;
+        const A ugradz1 = u000 + u100 + u010 + u110;
+        const A ugradz2 = u001 + u101 + u011 + u111;
+        const A vgradx1 = v000 + v010 + v001 + v011;
+        const A vgradx2 = v100 + v110 + v101 + v111;
+        const A vgradz1 = v000 + v100 + v010 + v110;
+        const A vgradz2 = v001 + v101 + v011 + v111;
+        const A wgradx1 = w000 + w010 + w001 + w011;
+        const A wgradx2 = w100 + w110 + w101 + w111;
+        const A wgrady1 = w000 + w100 + w001 + w101;
+        const A wgrady2 = w010 + w110 + w011 + w111;
+        const A cdx = (A)ga.celldx[g.o1 + j - g.x_min + 2];
+        const A cdy = (A)ga.celldy[g.o1 + k - g.y_min + 2];
+        const A cdz = (A)ga.celldz[g.o1 + l - g.z_min + 2];
+        const A xx = A(0.25) * (ugradx2 - ugradx1) / cdx;
+        const A yy = A(0.25) * (vgrady2 - vgrady1) / cdy;
+        const A zz = A(0.25) * (wgradz2 - wgradz1) / cdz;
+        const A xy = A(0.25) * (ugrady2 - ugrady1) / cdy + A(0.25) * (vgradx2 - vgradx1) / cdx;
+        const A xz = A(0.25) * (ugradz2 - ugradz1) / cdz + A(0.25) * (wgradx2 - wgradx1) / cdx;
+        const A yz = A(0.25) * (vgradz2 - vgradz1) / cdz + A(0.25) * (wgrady2 - wgrady1) / cdy;
+        // the neighbours' pressures as ideal_gas stores them
+#define PN(bb, a, b) ((A)st<C>(((A(1.4) - A(1.0)) * DN(bb, a, b) * EN(bb, a, b))))
+        A pgradx = (PN(bl, 1, 0) - PN(bl, -1, 0)) /
+                   (cdx + (A)ga.celldx[g.o1 + j + 1 - g.x_min + 2]);
+        A pgrady = (PN(bl, 0, 1) - PN(bl, 0, -1)) /
+                   (cdy + (A)ga.celldy[g.o1 + k + 1 - g.y_min + 2]);
+        A pgradz = (PN(bu, 0, 0) - PN(bd, 0, 0)) /
+                   (cdz + (A)ga.celldz[g.o1 + l + 1 - g.z_min + 2]);
+#undef PN
+        const A pgradx2 = pgradx * pgradx;
+        const A pgrady2 = pgrady * pgrady;
+        const A pgradz2 = pgradz * pgradz;
+        const A limiter = (xx * pgradx2 + yy * pgrady2 + zz * pgradz2 + xy * pgradx * pgrady +
+                           xz * pgradx * pgradz + yz * pgrady * pgradz) /
+                          fmax2(pgradx2 + pgrady2 + pgradz2, A(1.0e-16));
+        if (!(limiter > A(0.0))) {
+          pgradx = copysign(fmax2(A(1.0e-16), fabs(pgradx)), pgradx);
+          pgrady = copysign(fmax2(A(1.0e-16), fabs(pgrady)), pgrady);
+          pgradz = copysign(fmax2(A(1.0e-16), fabs(pgradz)), pgradz);
+          const A pgrad = sqrt(pgradx * pgradx + pgrady * pgrady + pgradz * pgradz);
+          const A xgrad = fabs(cdx * pgrad / pgradx);
+          const A ygrad = fabs(cdy * pgrad / pgrady);
+          const A zgrad = fabs(cdz * pgrad / pgradz);
+          const A grad = fmin2(fmin2(xgrad, ygrad), zgrad);
+          const A grad2 = grad * grad;
+          q = A(2.0) * DN(bl, 0, 0) * grad2 * limiter * limiter;
+        }
+      }
+      const long long o = off3(g, j, k, l);
+      viscosity[o] = st<C>(q);
+      // calc_dt_kernel.f90:102-149 (the viscosity as stored)
+      const A visc = (A)st<C>(q);
+      const A d0 = DN(bl, 0, 0);
+      const A ds = geo_ds<A>(g);
+      A ss;
+      {
+        const A v_eos = A(1.0) / d0;
+        const A p_eos = (A(1.4) - A(1.0)) * d0 * EN(bl, 0, 0);
+        const A pbe = (A(1.4) - A(1.0)) * d0;
+        const A pbv = -d0 * p_eos;
+        const A ss2 = v_eos * v_eos * (p_eos * pbe - pbv);
+        pressure[o] = st<C>(p_eos);
+        const C ss_st = st<C>(sqrt(ss2));
+        soundspeed[o] = ss_st;
+        ss = (A)ss_st;
+      }
+      A cc = ss * ss;
+      cc = cc + A(2.0) * visc / d0;
+      A dtct = ds * cc;
+      dtct = a_dtc * A(1.0) / fmax2(sqrt(dtct), a_gs);
+      const A vol = (A)g.vol;
+      const A du1 = ugradx1 * xa, du2 = ugradx2 * xa;
+      const A dtut = a_dtu * A(4.0) * vol / fmax2(fmax2(fabs(du1), fabs(du2)), A(1.0e-5) * vol);
+      const A dv1 = vgrady1 * ya, dv2 = vgrady2 * ya;
+      const A dtvt = a_dtv * A(4.0) * vol / fmax2(fmax2(fabs(dv1), fabs(dv2)), A(1.0e-5) * vol);
+      // both z faces use zarea(j,k,l); its sums add (j,k+1) before (j+1,k)
+      const A dw1 = (w000 + w010 + w100 + w110) * za;
+      const A dw2 = (w001 + w011 + w101 + w111) * za;
+      const A dtwt = a_dtw * A(4.0) * vol / fmax2(fmax2(fabs(dw1), fabs(dw2)), A(1.0e-5) * vol);
+      const A dvg = du2 - du1 + dv2 - dv1 + dw2 - dw1;
+      const A dtdivt = a_dtdiv * A(4.0) * vol / fmax2(vol * A(1.0e-05), fabs(dvg));
+      const A mn = fmin2(fmin2(fmin2(fmin2(dtct, dtut), dtvt), dtwt), dtdivt);
+      if (!(mn != mn)) {
+        const unsigned long long kc = key_of(mn);
+        key = kc < key ? kc : key;
+      }
+#undef EN
+#undef DN
+#undef NV
+    }
+    // every thread is done with plane l-1: its buffer takes plane l-1+RING
+    __syncthreads();
+    if (stop) break;
+    if (tid == 0 && l - 1 + RING <= plast) issue(l - 1 + RING);
+  }
+  if (stop) {
+    // a plane's copies did not arrive in time: report it, and give the copies
+    // still in flight (planes from the one waited for last to the last one
+    // issued) a bounded wait before the block's shared memory is released
+    if (tid == 0) {
+      atomicOr(status, CLOVER_STATUS_TIMEOUT);
+      for (int p = (l < l1 ? l : l1) + 1; p <= issued_hi; p++) {
+        const int u = p - pfirst;
+        mbar_wait_bounded(&full[u % RING], (unsigned)(u / RING) & 1u);
+      }
+    }
+    return;
+  }
+  // warp then block minimum, one atomic per block
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    unsigned long long other = __shfl_xor_sync(0xffffffffu, key, o);
+    key = other < key ? other : key;
+  }
+  if (tx == 0) wmin[ty] = key;
+  __syncthreads();
+  if (ty == 0) {
+    key = tx < TY ? wmin[tx] : ~0ull;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      unsigned long long other = __shfl_xor_sync(0xffffffffu, key, o);
+      key = other < key ? other : key;
+    }
+    if (tx == 0 && key != ~0ull) atomicMin(min_key, key);
+  }
+}
+
+constexpr int kViscRing = 4;
+constexpr int kViscSeg = 32;
+
+}  // namespace
+
+template <class S>
+bool visc_dt_tma_maps(const Geom& g, const typename S::vel_t* xvel0, const typename S::vel_t* yvel0,
+                      const typename S::vel_t* zvel0, const typename S::rho_t* density0,
+                      const typename S::ene_t* energy0, ViscMaps* m) {
+  using V = typename S::vel_t;
+  return encode_plane_map(&m->u, xvel0, sizeof(V), g, TY + 1) &&
+         encode_plane_map(&m->v, yvel0, sizeof(V), g, TY + 1) &&
+         encode_plane_map(&m->w, zvel0, sizeof(V), g, TY + 1) &&
+         encode_plane_map(&m->d, density0, sizeof(typename S::rho_t), g, TY + 2) &&
+         encode_plane_map(&m->e, energy0, sizeof(typename S::ene_t), g, TY + 2);
+}
+
+// blocks per SM (measured at 512^3: FP64 2.90 ms at 3 against 3.15 ms at 2,
+// where the FP64 form spills no register)
+template <class S>
+constexpr int kViscMinBlocks = sizeof(typename S::arith_t) == 4 ? 4 : 3;
+
+template <class S>
+bool visc_dt_tma_prepare() {
+  return cudaFuncSetAttribute(k_visc_dt_tma<S, kViscRing, kViscMinBlocks<S>>,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              kViscRing * ViscPlane<S>::kBytes) == cudaSuccess;
+}
+
+template <class S>
+void launch_visc_dt_tma(const Geom& g, cudaStream_t s, const ViscMaps& maps, const GeomArrays& ga,
+                        double g_small, double dtc_safe, double dtu_safe, double dtv_safe,
+                        double dtw_safe, double dtdiv_safe, typename S::cs_t* pressure,
+                        typename S::cs_t* viscosity, typename S::cs_t* soundspeed,
+                        unsigned long long* min_key, int* status) {
+  auto kern = k_visc_dt_tma<S, kViscRing, kViscMinBlocks<S>>;
+  const int smem = kViscRing * ViscPlane<S>::kBytes;
+  const dim3 grid((g.x_max - g.x_min + TX) / TX, (g.y_max - g.y_min + TY) / TY,
+                  (g.z_max - g.z_min + kViscSeg) / kViscSeg);
+  kern<<<grid, dim3(TX, TY), smem, s>>>(g, kViscSeg, ga, g_small, dtc_safe, dtu_safe, dtv_safe,
+                                         dtw_safe, dtdiv_safe, maps, pressure,
+                                         viscosity, soundspeed, min_key, status);
+}
+
+#define INST_TMA(S)                                                                              \
+  template bool visc_dt_tma_maps<S>(const Geom&, const S::vel_t*, const S::vel_t*,              \
+                                    const S::vel_t*, const S::rho_t*, const S::ene_t*,          \
+                                    ViscMaps*);                                                  \
+  template bool visc_dt_tma_prepare<S>();                                                        \
+  template void launch_visc_dt_tma<S>(const Geom&, cudaStream_t, const ViscMaps&, const GeomArrays&, \
+                                      double, double, double, double, double, double, S::cs_t*,  \
+                                      S::cs_t*, S::cs_t*, unsigned long long*, int*);
+INST_TMA(F64)
+INST_TMA(F32Mixed)
+
+}  // namespace clover

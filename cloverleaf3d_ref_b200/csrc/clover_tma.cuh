@@ -1,0 +1,138 @@
+// Bulk-tensor (TMA) staging of chunk-layout planes into shared memory.
+//
+// A z-marching stencil block (32 x 8 columns) needs, per plane of the march,
+// a box of each input array: its 32 columns plus halo columns on both sides,
+// and its 8 rows plus halo rows. One thread issues the box copies of a whole
+// plane (cp.async.bulk.tensor.3d, completion counted in bytes on an
+// mbarrier) a few planes ahead of the plane the block computes, so the loads
+// stay in flight without registers, and the block reads every stencil
+// neighbour from shared memory.
+//
+// Tensor maps describe one array of one chunk in the chunk layout
+// (clover_layout.cuh): dimensions (px, rows, planes), row and plane strides
+// in bytes. A copy must start on a 16-byte boundary along x, so the map's
+// base is the element H = 16 / sizeof(T) columns before x_min (element
+// x_min is 128-byte aligned in every array) and a tile whose first column is
+// x_min + 32 t starts its box at x coordinate 32 t, H columns before it; the
+// box is 32 + 2 H columns wide. Rows and planes have no alignment rule, and a
+// box that runs past the array's end reads zeros there.
+//
+// Only loads (no multicast): each block reads this GPU's own arrays.
+#pragma once
+
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include "clover_launch.h"
+
+namespace clover {
+
+// Columns a box carries on each side of its 32 for element type T.
+template <class T>
+constexpr int kTmaHalo = 16 / (int)sizeof(T);
+template <class T>
+constexpr int kTmaWidth = 32 + 2 * kTmaHalo<T>;
+
+// Encode the map of one chunk-layout array (base: its element
+// (x_min-2, y_min-2, z_min-2), the pointer every kernel indexes with off3)
+// with boxes of kTmaWidth<T> x box_rows x 1. False if the driver refuses it.
+bool encode_plane_map(CUtensorMap* map, const void* base, int elem_bytes, const Geom& g,
+                      int box_rows);
+
+// The tensor maps of the arrays the viscosity/calc_dt stencil reads.
+struct ViscMaps {
+  CUtensorMap u, v, w, d, e;
+};
+
+// The maps of a chunk's velocities (time level 0), density0 and energy0.
+template <class S>
+bool visc_dt_tma_maps(const Geom& g, const typename S::vel_t* xvel0, const typename S::vel_t* yvel0,
+                      const typename S::vel_t* zvel0, const typename S::rho_t* density0,
+                      const typename S::ene_t* energy0, ViscMaps* maps);
+// Once per process before the first launch (outside any stream capture):
+// the kernel's shared-memory size.
+template <class S>
+bool visc_dt_tma_prepare();
+// viscosity + calc_dt (+ ideal_gas) of every interior cell of one chunk, the
+// planes staged by bulk-tensor copies; the cell minimum folds into *min_key,
+// and a block whose copies do not arrive sets CLOVER_STATUS_TIMEOUT in
+// *status.
+template <class S>
+void launch_visc_dt_tma(const Geom& g, cudaStream_t s, const ViscMaps& maps, const GeomArrays& ga,
+                        double g_small, double dtc_safe, double dtu_safe, double dtv_safe,
+                        double dtw_safe, double dtdiv_safe, typename S::cs_t* pressure,
+                        typename S::cs_t* viscosity, typename S::cs_t* soundspeed,
+                        unsigned long long* min_key, int* status);
+
+// Bytes of one box.
+template <class T>
+constexpr unsigned box_bytes(int rows) {
+  return (unsigned)(rows * kTmaWidth<T> * (int)sizeof(T));
+}
+
+#ifdef __CUDACC__
+__device__ __forceinline__ unsigned smem_u32(const void* p) {
+  return (unsigned)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
+               : "memory");
+}
+
+// make the initialised barriers visible to the copy engine
+__device__ __forceinline__ void mbar_init_fence() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+// one arrival that also expects `bytes` of copies to complete this phase
+__device__ __forceinline__ void mbar_arrive_expect_tx(unsigned long long* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned parity) {
+  unsigned done;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(done)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return done != 0;
+}
+
+// Cycles a block waits for a plane's copies before it gives up (about one
+// second at the B200's clocks): the wait then reports failure instead of
+// spinning on.
+constexpr long long kTmaWaitCycles = 2000000000ll;
+
+// Wait for the phase of the given parity; false if it did not complete
+// within kTmaWaitCycles.
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsigned parity) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const long long t0 = clock64();
+  while (!mbar_try_wait(bar, parity))
+    if (clock64() - t0 > kTmaWaitCycles) return false;
+  return true;
+}
+
+// Box (x, y, z) of the map into shared memory (16-byte aligned), completion
+// counted on bar.
+__device__ __forceinline__ void tma_load_box(void* dst, const CUtensorMap* map,
+                                             unsigned long long* bar, int x, int y, int z) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%3, %4, %5}], [%2];" ::"r"(smem_u32(dst)),
+      "l"((unsigned long long)map), "r"(smem_u32(bar)), "r"(x), "r"(y), "r"(z)
+      : "memory");
+}
+
+__device__ __forceinline__ void tma_prefetch_map(const CUtensorMap* map) {
+  asm volatile("prefetch.tensormap [%0];" ::"l"((unsigned long long)map) : "memory");
+}
+#endif
+
+}  // namespace clover

@@ -75,6 +75,12 @@ void clover_chunk_use_graphs(clover_chunk *c, int on);
 /* 1 (default) = the fused kernels, 0 = one kernel per reference loop nest.
  * Both give the same results bit for bit. Only before the first step. */
 void clover_chunk_use_fused(clover_chunk *c, int on);
+/* 1 (default) = the fused step's stencils that stage their input planes in
+ * shared memory with bulk-tensor (TMA) copies, where the chunk could make
+ * their tensor maps; 0 = their register-marching forms. Both give the same
+ * results bit for bit. Returns 1 if the staged forms are in use. Ensembles
+ * always use the register-marching forms. */
+int clover_chunk_use_tma(clover_chunk *c, int on);
 
 /* Host copies of the device records (these synchronise):
  * steps taken, simulated time, dt of each step, field summaries

@@ -144,6 +144,28 @@ def test_dropin_state_restored_from_host_arrays():
     di.close()
 
 
+@pytest.mark.parametrize("case", ["tp1", "shock16", "mixed", "thin", "uneven"])
+def test_native_staged_and_register_forms_bitwise(case):
+    """The fused step with its stencils staged in shared memory by bulk-tensor
+    copies and with their register-marching forms: both equal the oracle bit
+    for bit (tiles that run past the grid on every axis, one-cell and
+    two-cell axes, segments of the march split mid-grid)."""
+    d = {"tp1": decks.test_problem_1(), "shock16": decks.shock(16, 16, 16, 30),
+         "mixed": decks.shock(13, 9, 11, 20, states=decks.MIXED_STATES),
+         "thin": decks.shock(7, 1, 5, 9, states=decks.MIXED_STATES),
+         "uneven": decks.shock(70, 17, 45, 12, states=decks.MIXED_STATES)}[case]
+    r = O.run(d, want_fields=True)
+    for tma in (True, False):
+        ch = C.Chunk(decks.to_deck(d))
+        assert ch.use_tma(tma) == tma
+        n = ch.run()
+        assert n == r["steps"]
+        assert ch.status == 0
+        sums, sst = ch.summaries()
+        compare_run(r, ch.dt_history(), sums, sst, ch.field)
+        ch.close()
+
+
 @pytest.mark.parametrize("fused", [True, False])
 @pytest.mark.parametrize("graphs", [True, False])
 @pytest.mark.parametrize("case", ["tp1", "shock16", "mixed", "thin"])
@@ -265,3 +287,22 @@ def test_array_passed_with_another_chunks_bounds_is_refused():
     L.clover_gpu_clear_status()
     L.clover_gpu_sync_to_host()
     assert np.all(a["pressure"][2:8, 2:7, 2:6] == (1.4 - 1.0) * 1.0 * 2.0)
+
+
+def test_mixed_staged_and_register_forms_identical():
+    """The mixed-precision step gives the same bits with its stencils staged
+    by bulk-tensor copies or in their register-marching forms."""
+    d = decks.shock(70, 17, 45, 12, states=decks.MIXED_STATES)
+    out = []
+    for tma in (True, False):
+        ch = C.Chunk(decks.to_deck(d), precision=C.PRECISION_MIXED)
+        assert ch.use_tma(tma) == tma
+        assert ch.run() == 12
+        assert ch.status == 0
+        out.append((ch.dt_history(), ch.summaries()[0], {n: ch.field(n) for n in O.FIELD_NAMES}))
+        ch.close()
+    (dt_a, s_a, f_a), (dt_b, s_b, f_b) = out
+    assert np.array_equal(dt_a, dt_b)
+    assert np.array_equal(s_a, s_b)
+    for n in O.FIELD_NAMES:
+        assert np.array_equal(f_a[n], f_b[n]), n
