@@ -32,8 +32,9 @@
 #include <cfloat>
 #include <type_traits>
 
-#include "clover_div.cuh"
 #include "clover_launch.h"
+#include "clover_stencil.cuh"
+#include "clover_tma.cuh"
 
 namespace clover {
 namespace {
@@ -123,27 +124,6 @@ __device__ __forceinline__ double ld(const float* p) { return (double)__ldg(p); 
 #define EI(a, idx) EI_(a, idx)
 #define EI_(a, jj, kk, ll) (a)[off3(g, (jj), (kk), (ll))]
 #define LI(a, idx) ld(&EI_(a, idx))
-
-// a value in storage type T, converted once from the arithmetic it was
-// formed in (no detour through double for an FP32 value stored as FP32)
-template <class T, class U>
-__device__ __forceinline__ T st(U v) { return (T)v; }
-
-__device__ __forceinline__ double fmin2(double a, double b) { return b < a ? b : a; }
-__device__ __forceinline__ double fmax2(double a, double b) { return b > a ? b : a; }
-__device__ __forceinline__ float fmin2(float a, float b) { return b < a ? b : a; }
-__device__ __forceinline__ float fmax2(float a, float b) { return b > a ? b : a; }
-// a value of the momentum arithmetic type A from storage
-template <class A>
-__device__ __forceinline__ A lda(const double* p) { return (A)__ldg(p); }
-template <class A>
-__device__ __forceinline__ A lda(const float* p) { return (A)__ldg(p); }
-
-// The per-chunk quotients of Geom in the arithmetic type A.
-template <class A>
-__device__ __forceinline__ A geo_rvol(const Geom& g) { return sizeof(A) == 4 ? (A)g.rvol_f : (A)g.rvol; }
-template <class A>
-__device__ __forceinline__ A geo_ds(const Geom& g) { return sizeof(A) == 4 ? (A)g.ds_f : (A)g.ds; }
 
 // ---------------------------------------------------------------------------
 // viscosity_kernel.f90:71-134 followed by calc_dt_kernel.f90:102-149 on the
@@ -694,13 +674,6 @@ __device__ __forceinline__ double node_flux_at(const Geom& g, const typename S::
                   L(mf, j, k - 1, l + 1));
 }
 
-// Node mass post (reference order of the eight cells) from cell products P.
-__device__ __forceinline__ double node_mass_sum(double p_0m0, double p_000, double p_mm0,
-                                                double p_m00, double p_0mm, double p_00m,
-                                                double p_mmm, double p_m0m) {
-  return 0.125 * (p_0m0 + p_000 + p_mm0 + p_m00 + p_0mm + p_00m + p_mmm + p_m0m);
-}
-
 template <class S>
 __device__ __forceinline__ double cell_product(const Geom& g, int variant, const GeomArrays& ga,
     const typename S::rho_t* density1, const typename S::vf_t* vfx, const typename S::vf_t* vfy,
@@ -799,59 +772,6 @@ __global__ void __launch_bounds__(BX * BY, M::kFlat || sizeof(typename S::arith_
 #undef IDXM
 #undef IDX
   });
-}
-
-// Momentum flux at node i (advec_mom_kernel.f90:211-242 and the y/z forms)
-// from the velocity window v(i-1..i+2). The donor side, the Courant number
-// sigma and the limiter's cell widths depend on the node only, so they are
-// formed once per node (MomNodeTerms) for the three velocity components.
-template <class A>
-struct MomNodeTerms {
-  bool neg;  // node flux < 0: the donor is node i+1
-  A nf, sigma, width, cd_dif;
-};
-
-template <class A>
-__device__ __forceinline__ MomNodeTerms<A> mom_node_terms(A nf, A nmpre_i, A nmpre_ip1, A width,
-                                                          A cd_m1, A cd_p1) {
-  MomNodeTerms<A> t;
-  t.neg = nf < A(0.0);
-  t.nf = nf;
-  t.sigma = fabs(nf) / (t.neg ? nmpre_ip1 : nmpre_i);
-  t.width = width;
-  t.cd_dif = t.neg ? cd_p1 : cd_m1;
-  return t;
-}
-
-template <class A>
-__device__ __forceinline__ A mom_flux_v(const MomNodeTerms<A>& t, A vm1, A v0, A vp1, A vp2) {
-  const A v_upwind = t.neg ? vp2 : vm1;
-  const A v_donor = t.neg ? vp1 : v0;
-  const A v_downwind = t.neg ? v0 : vp1;
-  const A vdiffuw = v_donor - v_upwind;
-  const A vdiffdw = v_downwind - v_donor;
-  A limiter = A(0.0);
-  if (vdiffuw * vdiffdw > A(0.0)) {
-    const A auw = fabs(vdiffuw);
-    const A adw = fabs(vdiffdw);
-    A wind = A(1.0);
-    if (vdiffdw <= A(0.0)) wind = A(-1.0);
-    const A width = t.width, sigma = t.sigma;
-    // ... / 6.0_8 correctly rounded by div6 (clover_div.cuh)
-    limiter = wind * fmin2(fmin2(div6(width * ((A(2.0) - sigma) * adw / width +
-                                               (A(1.0) + sigma) * auw / t.cd_dif)),
-                                 auw),
-                           adw);
-  }
-  const A advec_vel_s = v_donor + (A(1.0) - t.sigma) * limiter;
-  return advec_vel_s * t.nf;
-}
-
-template <class A>
-__device__ __forceinline__ A mom_flux_at(A nf, A nmpre_i, A nmpre_ip1, A vm1, A v0, A vp1, A vp2,
-                                         A width, A cd_m1, A cd_p1) {
-  return mom_flux_v<A>(mom_node_terms<A>(nf, nmpre_i, nmpre_ip1, width, cd_m1, cd_p1), vm1, v0,
-                       vp1, vp2);
 }
 
 // Velocity pass for direction y or z, marching along the sweep axis with the
@@ -1410,7 +1330,7 @@ void launch_advec_mom_fused(const Target& tg, cudaStream_t s, int advect_x, int 
                             typename S::wk_t* node_flux, typename S::wk_t* node_mass_post,
                             typename S::wk_t* node_mass_pre, typename S::vel_t* const* vel_in,
                             typename S::vel_t* const* vel_out, bool copy_shell,
-                            const Level0<S>& level0) {
+                            const Level0<S>& level0, const MomXMaps* x_maps, int* status) {
   // the node arrays of the y/z sweeps live in three work arrays, as nd_t
   using ND = typename S::nd_t;
   static_assert(sizeof(ND) <= sizeof(typename S::wk_t), "node arrays fit the work arrays");
@@ -1434,7 +1354,10 @@ void launch_advec_mom_fused(const Target& tg, cudaStream_t s, int advect_x, int 
   };
   using I2 = std::integral_constant<int, 2>;
   using I3 = std::integral_constant<int, 3>;
-  if (dir == 1) {
+  if (dir == 1 && x_maps && !tg.plan) {
+    // one pass, its planes staged in shared memory
+    launch_mom_x_tma<S>(tg.g, s, sweep, kMarchSeg, *x_maps, ga, vel_out, level0, status);
+  } else if (dir == 1) {
     // one pass for the three velocities
     auto sweep_x = [&](auto var) {
       constexpr int V = decltype(var)::value;
@@ -1493,7 +1416,7 @@ void launch_advec_mom_fused(const Target& tg, cudaStream_t s, int advect_x, int 
                                           const S::mf_t*, const S::mf_t*, const S::vf_t*,      \
                                           const S::vf_t*, const S::vf_t*, S::wk_t*, S::wk_t*,  \
                                           S::wk_t*, S::vel_t* const*, S::vel_t* const*, bool,  \
-                                          const Level0<S>&);
+                                          const Level0<S>&, const MomXMaps*, int*);
 
 INSTF(F64)
 INSTF(F32Mixed)

@@ -384,6 +384,10 @@ void launch_advec_cell_x(const Target& tg, cudaStream_t s, int sweep, const Geom
 // copied across (left out where a depth-2 halo update of the velocities
 // comes before the next read of the shell).
 // vol: the uniform cell volume of the chunk (dx*dy*dz).
+// x_maps (one chunk, x sweep): the tensor maps of the sweep's inputs, to run
+// its shared-memory staged form (clover_tma.cu), which reports a copy that
+// did not arrive in *status; null: the register-marching form.
+struct MomXMaps;
 template <class S>
 void launch_advec_mom_fused(const Target& tg, cudaStream_t s, int advect_x, int sweep, int dir,
                             double vol, const GeomArrays& ga, const typename S::rho_t* density1,
@@ -393,7 +397,8 @@ void launch_advec_mom_fused(const Target& tg, cudaStream_t s, int advect_x, int 
                             typename S::wk_t* node_flux, typename S::wk_t* node_mass_post,
                             typename S::wk_t* node_mass_pre, typename S::vel_t* const* vel_in,
                             typename S::vel_t* const* vel_out, bool copy_shell,
-                            const Level0<S>& level0);
+                            const Level0<S>& level0, const MomXMaps* x_maps = nullptr,
+                            int* status = nullptr);
 
 // Fill every element of an array (size elems after the pad) with a value.
 template <class T>

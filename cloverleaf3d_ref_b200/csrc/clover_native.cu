@@ -158,6 +158,28 @@ struct Chunk : ChunkBase {
   bool tma = false;
   bool use_tma = true;
   ViscMaps visc_maps;
+  // tensor maps of the arrays the staged x momentum sweep reads, by (array,
+  // box rows): both buffers of the density1 and velocity pairs occur
+  std::map<std::pair<const void*, int>, CUtensorMap> tmaps;
+  bool tmap(const void* base, int elem_bytes, int rows, CUtensorMap* out) {
+    const auto key = std::make_pair(base, rows);
+    auto it = tmaps.find(key);
+    if (it == tmaps.end()) {
+      CUtensorMap m;
+      if (!encode_plane_map(&m, base, elem_bytes, g, rows)) return false;
+      it = tmaps.emplace(key, m).first;
+    }
+    *out = it->second;
+    return true;
+  }
+  // the maps of the x momentum sweep reading density1 buffer rho and the
+  // velocity buffers vin
+  bool mom_x_maps(const R* rho, V* const* vin, MomXMaps* m) {
+    return tmap(mass_flux_x, sizeof(MF), 9, &m->mf) && tmap(rho, sizeof(R), 9, &m->d) &&
+           tmap(vol_flux_y, sizeof(VF), 10, &m->vfy) && tmap(vol_flux_z, sizeof(VF), 9, &m->vfz) &&
+           tmap(vin[0], sizeof(V), 8, &m->u) && tmap(vin[1], sizeof(V), 8, &m->v) &&
+           tmap(vin[2], sizeof(V), 8, &m->w);
+  }
   // Every axis of every deck has at least three cells. A repeated halo update
   // of a cell field, a vertex velocity or a z-face flux, whose values have
   // not changed since its last update at the same depth, then rewrites every
@@ -346,7 +368,7 @@ struct Chunk : ChunkBase {
     // one chunk: the stencils that stage their planes with bulk-tensor copies
     // get their tensor maps (the arrays they read never move)
     if (!batched)
-      tma = visc_dt_tma_prepare<S>() &&
+      tma = visc_dt_tma_prepare<S>() && mom_x_tma_prepare<S>() &&
             visc_dt_tma_maps<S>(g, xvel0, yvel0, zvel0, density0, energy0, &visc_maps);
 
     dt_cap = deck.end_step < (1 << 22) ? deck.end_step + 16 : (1 << 22);
@@ -831,10 +853,13 @@ struct Chunk : ChunkBase {
       // after sweeps 1 and 2 the next post-sweep depth-2 halo update rewrites
       // the velocities' shell before anything reads it; after sweep 3 the
       // shell carries the step's final halo values
+      MomXMaps xm;
+      const bool x_tma = dir == 1 && tma && use_tma && mom_x_maps(rho1(cb), vin, &xm);
       launch_advec_mom_fused<S>(tg, stream, axi, sweep_number, dir, cell_volume, ga, rho1(cb),
                                 mass_flux_x, mass_flux_y, mass_flux_z, vol_flux_x, vol_flux_y,
                                 vol_flux_z, work[0], work[1], work[2], vin, vout,
-                                sweep_number == 3 || !halo_repeat_free, l0);
+                                sweep_number == 3 || !halo_repeat_free, l0,
+                                x_tma ? &xm : nullptr, &sc->status);
       // x: one pass; y, z: node pass + velocity pass
       if (dir == 1)
         pend("advec_mom_x", n * (MF8 + R8 + npv * VF8 + (6 + 3 * nl0) * V8));

@@ -19,6 +19,7 @@
 
 #include "../../include/clover_kernels.h"
 #include "clover_launch.h"
+#include "clover_stencil.cuh"
 #include "clover_tma.cuh"
 
 namespace clover {
@@ -80,17 +81,6 @@ struct ViscPlane {
   __device__ static R* rho(unsigned char* p) { return (R*)(p + 3 * kVel); }
   __device__ static En* ene(unsigned char* p) { return (En*)(p + 3 * kVel + kRho); }
 };
-
-__device__ __forceinline__ double fmin2(double a, double b) { return b < a ? b : a; }
-__device__ __forceinline__ double fmax2(double a, double b) { return b > a ? b : a; }
-__device__ __forceinline__ float fmin2(float a, float b) { return b < a ? b : a; }
-__device__ __forceinline__ float fmax2(float a, float b) { return b > a ? b : a; }
-
-template <class T, class U>
-__device__ __forceinline__ T st(U v) { return (T)v; }
-
-template <class A>
-__device__ __forceinline__ A geo_ds(const Geom& g) { return sizeof(A) == 4 ? (A)g.ds_f : (A)g.ds; }
 
 template <class S, int RING, int MINB>
 __global__ void __launch_bounds__(TX * TY, MINB)
@@ -302,6 +292,199 @@ k_visc_dt_tma(Geom g, int seg, GeomArrays ga, double g_small, double dtc_safe, d
   }
 }
 
+// ---------------------------------------------------------------------------
+// The x momentum sweep (advec_mom_kernel.f90:166-252 for the three
+// velocities) of k_mom_sweep_x (clover_fused.cu), with its inputs staged in
+// shared memory. The lane layout stays: lane L of a warp holds node
+// j = x_min-2+29t+L of row k, neighbouring nodes' node values come by
+// shuffles, lanes 1..30 form momentum fluxes and lanes 2..30 update (29
+// nodes per warp), the plane l-1 terms are carried in registers; what
+// changes is where the values come from: every mass flux, density, volume
+// flux and velocity of plane p arrives with plane p's boxes. Box columns
+// start on the 16-byte boundary at or before the block's first node, so a
+// lane's node sits `shift` columns into each box (shift depends on the
+// element type). Plane p holds mass_flux_x and density1 of rows k0-1..k0+7,
+// vol_flux_y of rows k0-1..k0+8 and vol_flux_z of rows k0-1..k0+7 (the post
+// volumes of sweep 1; sweep 3 reads none), and the three velocities of rows
+// k0..k0+7. Node plane l reads planes l and l+1 (vol_flux_z).
+template <class S, int VAR>
+struct MomXPlane {
+  using MF = typename S::mf_t;
+  using R = typename S::rho_t;
+  using VF = typename S::vf_t;
+  using V = typename S::vel_t;
+  static constexpr bool kVf = VAR == 0;
+  static constexpr int kMf = round128(9 * kTmaWidth<MF> * (int)sizeof(MF));
+  static constexpr int kRho = round128(9 * kTmaWidth<R> * (int)sizeof(R));
+  static constexpr int kVfy = kVf ? round128(10 * kTmaWidth<VF> * (int)sizeof(VF)) : 0;
+  static constexpr int kVfz = kVf ? round128(9 * kTmaWidth<VF> * (int)sizeof(VF)) : 0;
+  static constexpr int kVel = round128(8 * kTmaWidth<V> * (int)sizeof(V));
+  static constexpr int kBytes = kMf + kRho + kVfy + kVfz + 3 * kVel;
+  static constexpr unsigned kTx = box_bytes<MF>(9) + box_bytes<R>(9) +
+                                  (kVf ? box_bytes<VF>(10) + box_bytes<VF>(9) : 0u) +
+                                  3 * box_bytes<V>(8);
+  __device__ static MF* mf(unsigned char* p) { return (MF*)p; }
+  __device__ static R* rho(unsigned char* p) { return (R*)(p + kMf); }
+  __device__ static VF* vfy(unsigned char* p) { return (VF*)(p + kMf + kRho); }
+  __device__ static VF* vfz(unsigned char* p) { return (VF*)(p + kMf + kRho + kVfy); }
+  __device__ static V* vel(unsigned char* p, int q) {
+    return (V*)(p + kMf + kRho + kVfy + kVfz + q * kVel);
+  }
+};
+
+// Box x coordinate of element type T for a block whose first node is
+// x_min-2+29t, and the column of that node in the box.
+template <class T>
+__device__ __forceinline__ void x_box(int t, int& x, int& shift) {
+  constexpr int H = kTmaHalo<T>;
+  const int c = 29 * t + H - 2;  // the first node's column, counted from the map's base
+  x = c / H * H;
+  shift = c - x;
+}
+
+template <class S, int VAR, int RING, int MINB>
+__global__ void __launch_bounds__(TX * TY, MINB)
+k_mom_sweep_x_tma(Geom g, int seg, GeomArrays ga, const __grid_constant__ MomXMaps maps,
+                  typename S::vel_t* __restrict__ u_out, typename S::vel_t* __restrict__ v_out,
+                  typename S::vel_t* __restrict__ w_out, Level0<S> lz, int* __restrict__ status) {
+  using P = MomXPlane<S, VAR>;
+  using A = typename S::arith_t;
+  using V = typename S::vel_t;
+  using MF = typename S::mf_t;
+  using R = typename S::rho_t;
+  using VF = typename S::vf_t;
+  extern __shared__ __align__(128) unsigned char ring[];
+  __shared__ unsigned long long full[RING];
+  __shared__ int stop;
+  const int lane = threadIdx.x, ty = threadIdx.y, tid = ty * TX + lane;
+  const unsigned fullmask = 0xffffffffu;
+  const int j = g.x_min - 2 + 29 * (int)blockIdx.x + lane;  // node of this lane
+  const int k0 = g.y_min + TY * (int)blockIdx.y, k = k0 + ty;
+  const int l0 = g.z_min + seg * (int)blockIdx.z;
+  const int l1 = l0 + seg - 1 < g.z_max + 1 ? l0 + seg - 1 : g.z_max + 1;
+  const int pfirst = l0 - 1, plast = l1 + 1;
+  const bool row = k <= g.y_max + 1;              // the whole warp: k depends on the row only
+  const bool has_nf = row && j <= g.x_max + 2;    // node_flux range j in [x_min-2, x_max+2]
+  const bool has_mf = row && lane >= 1 && lane <= 30 && j >= g.x_min - 1 && j <= g.x_max + 1;
+  const bool has_up = row && lane >= 2 && lane <= 30 && j >= g.x_min && j <= g.x_max + 1;
+  int xm, cm, xr, cr, xf, cf, xv, cv;
+  x_box<MF>(blockIdx.x, xm, cm);
+  x_box<R>(blockIdx.x, xr, cr);
+  x_box<VF>(blockIdx.x, xf, cf);
+  x_box<V>(blockIdx.x, xv, cv);
+  cm += lane; cr += lane; cf += lane; cv += lane;  // this lane's node in each box
+  constexpr int WM = kTmaWidth<MF>, WR = kTmaWidth<R>, WF = kTmaWidth<VF>, WV = kTmaWidth<V>;
+  if (tid == 0) {
+    for (int r = 0; r < RING; r++) mbar_init(&full[r], 1);
+    mbar_init_fence();
+    stop = 0;
+  }
+  __syncthreads();
+  int issued_hi = pfirst - 1;
+  auto issue = [&](int p) {
+    issued_hi = p;
+    const int s = (p - pfirst) % RING;
+    unsigned char* b = ring + s * P::kBytes;
+    mbar_arrive_expect_tx(&full[s], P::kTx);
+    const int z = p - g.z_min + 2, y1 = k0 - g.y_min + 1, y0 = y1 + 1;  // rows k0-1.., k0..
+    tma_load_box(P::mf(b), &maps.mf, &full[s], xm, y1, z);
+    tma_load_box(P::rho(b), &maps.d, &full[s], xr, y1, z);
+    if (P::kVf) {
+      tma_load_box(P::vfy(b), &maps.vfy, &full[s], xf, y1, z);
+      tma_load_box(P::vfz(b), &maps.vfz, &full[s], xf, y1, z);
+    }
+    tma_load_box(P::vel(b, 0), &maps.u, &full[s], xv, y0, z);
+    tma_load_box(P::vel(b, 1), &maps.v, &full[s], xv, y0, z);
+    tma_load_box(P::vel(b, 2), &maps.w, &full[s], xv, y0, z);
+  };
+  if (tid == 0)
+    for (int p = pfirst; p <= plast && p < pfirst + RING; p++) issue(p);
+  auto buf = [&](int p) { return ring + ((p - pfirst) % RING) * P::kBytes; };
+  auto wait = [&](int p) {
+    const int u = p - pfirst;
+    if (!mbar_wait_bounded(&full[u % RING], (unsigned)(u / RING) & 1u)) stop = 1;
+  };
+  // values of plane p: mass flux at (j + a, row r) (r = 0 for k-1, 1 for k),
+  // and the cell product density1 * post_vol of cell (j, k-1+r)
+  auto MFv = [&](unsigned char* b, int r, int a) { return (double)P::mf(b)[(ty + r) * WM + cm + a]; };
+  auto prod = [&](unsigned char* b, unsigned char* bz1, int r) {
+    const double d = (double)P::rho(b)[(ty + r) * WR + cr];
+    double pv = g.vol;
+    if (VAR == 0)  // mom_post_vol variant 0, the reference's order
+      pv = pv + (double)P::vfy(b)[(ty + r + 1) * WF + cf] - (double)P::vfy(b)[(ty + r) * WF + cf] +
+           (double)P::vfz(bz1)[(ty + r) * WF + cf] - (double)P::vfz(b)[(ty + r) * WF + cf];
+    return d * pv;
+  };
+  const double cd_0 = has_nf ? ga.celldx[g.o1 + j - g.x_min + 2] : 1.0;
+  const double cd_m1 = has_mf ? ga.celldx[g.o1 + j - 1 - g.x_min + 2] : 1.0;
+  const double cd_p1 = has_mf ? ga.celldx[g.o1 + j + 1 - g.x_min + 2] : 1.0;
+  typename S::vel_t* out[3] = {u_out, v_out, w_out};
+  typename S::vel_t* lev0[3] = {lz.xvel0, lz.yvel0, lz.zvel0};
+  // plane l0-1 terms: mass fluxes at (j, k-1), (j, k), (j+1, k-1), (j+1, k);
+  // cell products at (j, k-1), (j, k)
+  wait(pfirst);
+  wait(pfirst + 1);
+  double fm_a = 0.0, fm_b = 0.0, fm_c = 0.0, fm_d = 0.0, pm_a = 0.0, pm_b = 0.0;
+  if (has_nf && !stop) {
+    unsigned char* b = buf(pfirst);
+    fm_a = MFv(b, 0, 0); fm_b = MFv(b, 1, 0); fm_c = MFv(b, 0, 1); fm_d = MFv(b, 1, 1);
+    pm_a = prod(b, buf(pfirst + 1), 0); pm_b = prod(b, buf(pfirst + 1), 1);
+  }
+  int l = l0;
+  for (; l <= l1; l++) {
+    wait(l + 1);
+    if (row && !stop) {
+      unsigned char* b = buf(l);
+      unsigned char* bz = buf(l + 1);
+      double f_a = 0.0, f_b = 0.0, f_c = 0.0, f_d = 0.0, p_a = 0.0, p_b = 0.0;
+      if (has_nf) {
+        f_a = MFv(b, 0, 0); f_b = MFv(b, 1, 0); f_c = MFv(b, 0, 1); f_d = MFv(b, 1, 1);
+        p_a = prod(b, bz, 0); p_b = prod(b, bz, 1);
+      }
+      const double nf = 0.125 * (f_a + f_b + f_c + f_d + fm_a + fm_b + fm_c + fm_d);
+      const double q_a = __shfl_up_sync(fullmask, p_a, 1);
+      const double q_b = __shfl_up_sync(fullmask, p_b, 1);
+      const double qm_a = __shfl_up_sync(fullmask, pm_a, 1);
+      const double qm_b = __shfl_up_sync(fullmask, pm_b, 1);
+      const double nmp = node_mass_sum(p_a, p_b, q_a, q_b, pm_a, pm_b, qm_a, qm_b);
+      const double nf_m = __shfl_up_sync(fullmask, nf, 1);
+      const double nmpre = nmp - nf_m + nf;
+      const double nmpre_p = __shfl_down_sync(fullmask, nmpre, 1);
+      const MomNodeTerms<A> nt =
+          mom_node_terms<A>((A)nf, (A)nmpre, (A)nmpre_p, (A)cd_0, (A)cd_m1, (A)cd_p1);
+#pragma unroll
+      for (int q = 0; q < 3; q++) {
+        const V* vr = P::vel(b, q) + ty * WV + cv;
+        A mf = A(0.0), v0 = A(0.0);
+        if (has_mf) {
+          v0 = (A)vr[0];
+          mf = mom_flux_v<A>(nt, (A)vr[-1], v0, (A)vr[1], (A)vr[2]);
+        }
+        const A mf_m = __shfl_up_sync(fullmask, mf, 1);
+        if (has_up) {
+          const V vn1 = st<V>((v0 * (A)nmpre + mf_m - mf) / (A)nmp);
+          const long long o = off3(g, j, k, l);
+          out[q][o] = vn1;
+          if (lz.xvel0) lev0[q][o] = vn1;  // last sweep of the step: reset_field
+        }
+      }
+      fm_a = f_a; fm_b = f_b; fm_c = f_c; fm_d = f_d;
+      pm_a = p_a; pm_b = p_b;
+    }
+    // every thread is done with plane l: its buffer takes plane l+RING
+    __syncthreads();
+    if (stop) break;
+    if (tid == 0 && l + RING <= plast) issue(l + RING);
+  }
+  if (stop && tid == 0) {
+    atomicOr(status, CLOVER_STATUS_TIMEOUT);
+    for (int p = (l < l1 ? l : l1) + 1; p <= issued_hi; p++) {
+      const int u = p - pfirst;
+      mbar_wait_bounded(&full[u % RING], (unsigned)(u / RING) & 1u);
+    }
+  }
+}
+
 constexpr int kViscRing = 4;
 constexpr int kViscSeg = 32;
 
@@ -346,11 +529,45 @@ void launch_visc_dt_tma(const Geom& g, cudaStream_t s, const ViscMaps& maps, con
                                          viscosity, soundspeed, min_key, status);
 }
 
+constexpr int kMomXRing = 4;
+template <class S>
+constexpr int kMomXMinBlocks = sizeof(typename S::arith_t) == 4 ? 4 : 3;
+
+template <class S>
+bool mom_x_tma_prepare() {
+  return cudaFuncSetAttribute(k_mom_sweep_x_tma<S, 0, kMomXRing, kMomXMinBlocks<S>>,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              kMomXRing * MomXPlane<S, 0>::kBytes) == cudaSuccess &&
+         cudaFuncSetAttribute(k_mom_sweep_x_tma<S, 4, kMomXRing, kMomXMinBlocks<S>>,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              kMomXRing * MomXPlane<S, 4>::kBytes) == cudaSuccess;
+}
+
+template <class S>
+void launch_mom_x_tma(const Geom& g, cudaStream_t s, int sweep, int seg, const MomXMaps& maps,
+                      const GeomArrays& ga, typename S::vel_t* const* vel_out,
+                      const Level0<S>& level0, int* status) {
+  const dim3 grid((g.x_max + 1 - g.x_min + 1 + 28) / 29, (g.y_max + 1 - g.y_min + 1 + TY - 1) / TY,
+                  (g.z_max + 1 - g.z_min + 1 + seg - 1) / seg);
+  // post_vol variant: 0 on sweep 1, 4 (the cell volume) on sweep 3
+  if (sweep == 1)
+    k_mom_sweep_x_tma<S, 0, kMomXRing, kMomXMinBlocks<S>>
+        <<<grid, dim3(TX, TY), kMomXRing * MomXPlane<S, 0>::kBytes, s>>>(
+            g, seg, ga, maps, vel_out[0], vel_out[1], vel_out[2], level0, status);
+  else
+    k_mom_sweep_x_tma<S, 4, kMomXRing, kMomXMinBlocks<S>>
+        <<<grid, dim3(TX, TY), kMomXRing * MomXPlane<S, 4>::kBytes, s>>>(
+            g, seg, ga, maps, vel_out[0], vel_out[1], vel_out[2], level0, status);
+}
+
 #define INST_TMA(S)                                                                              \
   template bool visc_dt_tma_maps<S>(const Geom&, const S::vel_t*, const S::vel_t*,              \
                                     const S::vel_t*, const S::rho_t*, const S::ene_t*,          \
                                     ViscMaps*);                                                  \
   template bool visc_dt_tma_prepare<S>();                                                        \
+  template bool mom_x_tma_prepare<S>();                                                          \
+  template void launch_mom_x_tma<S>(const Geom&, cudaStream_t, int, int, const MomXMaps&,        \
+                                    const GeomArrays&, S::vel_t* const*, const Level0<S>&, int*); \
   template void launch_visc_dt_tma<S>(const Geom&, cudaStream_t, const ViscMaps&, const GeomArrays&, \
                                       double, double, double, double, double, double, S::cs_t*,  \
                                       S::cs_t*, S::cs_t*, unsigned long long*, int*);

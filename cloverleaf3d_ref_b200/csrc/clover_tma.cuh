@@ -44,6 +44,21 @@ struct ViscMaps {
   CUtensorMap u, v, w, d, e;
 };
 
+// The maps of the arrays the x momentum sweep reads: mass_flux_x, density1,
+// vol_flux_y and vol_flux_z (rows k0-1.., 9 and 10 rows), and the three
+// time-level-1 velocities it advects (rows k0.., 8 rows).
+struct MomXMaps {
+  CUtensorMap mf, d, vfy, vfz, u, v, w;
+};
+template <class S>
+bool mom_x_tma_prepare();
+// The x momentum sweep of one chunk (sweep 1 or 3 of the step), its planes
+// staged by bulk-tensor copies; seg planes per block along z.
+template <class S>
+void launch_mom_x_tma(const Geom& g, cudaStream_t s, int sweep, int seg, const MomXMaps& maps,
+                      const GeomArrays& ga, typename S::vel_t* const* vel_out,
+                      const Level0<S>& level0, int* status);
+
 // The maps of a chunk's velocities (time level 0), density0 and energy0.
 template <class S>
 bool visc_dt_tma_maps(const Geom& g, const typename S::vel_t* xvel0, const typename S::vel_t* yvel0,
