@@ -471,10 +471,11 @@ k_mom_sweep_x_tma(Geom g, int seg, GeomArrays ga, const __grid_constant__ MomXMa
       fm_a = f_a; fm_b = f_b; fm_c = f_c; fm_d = f_d;
       pm_a = p_a; pm_b = p_b;
     }
-    // every thread is done with plane l: its buffer takes plane l+RING
+    // every thread is done with plane l-1 (l0-1: read before the loop): its
+    // buffer takes plane l-1+RING
     __syncthreads();
     if (stop) break;
-    if (tid == 0 && l + RING <= plast) issue(l + RING);
+    if (tid == 0 && l - 1 + RING <= plast) issue(l - 1 + RING);
   }
   if (stop && tid == 0) {
     atomicOr(status, CLOVER_STATUS_TIMEOUT);
