@@ -212,17 +212,12 @@ __global__ void __launch_bounds__(BX * BY, sizeof(typename S::arith_t) == 4 || M
     const A wgrady1 = w000 + w100 + w001 + w101;
     const A wgrady2 = w010 + w110 + w011 + w111;
     const A cdx = AG(GX, ga.celldx, j), cdy = AG(GY, ga.celldy, k), cdz = AG(GZ, ga.celldz, l);
-    // quotients by the widths from their correctly rounded reciprocals
-    const A rx = AG(GX, ga.rcelldx, j), ry = AG(GY, ga.rcelldy, k), rz = AG(GZ, ga.rcelldz, l);
-    const A xx = div_rn(A(0.25) * (ugradx2 - ugradx1), cdx, rx);
-    const A yy = div_rn(A(0.25) * (vgrady2 - vgrady1), cdy, ry);
-    const A zz = div_rn(A(0.25) * (wgradz2 - wgradz1), cdz, rz);
-    const A xy = div_rn(A(0.25) * (ugrady2 - ugrady1), cdy, ry) +
-                 div_rn(A(0.25) * (vgradx2 - vgradx1), cdx, rx);
-    const A xz = div_rn(A(0.25) * (ugradz2 - ugradz1), cdz, rz) +
-                 div_rn(A(0.25) * (wgradx2 - wgradx1), cdx, rx);
-    const A yz = div_rn(A(0.25) * (vgradz2 - vgradz1), cdz, rz) +
-                 div_rn(A(0.25) * (wgrady2 - wgrady1), cdy, ry);
+    const A xx = A(0.25) * (ugradx2 - ugradx1) / cdx;
+    const A yy = A(0.25) * (vgrady2 - vgrady1) / cdy;
+    const A zz = A(0.25) * (wgradz2 - wgradz1) / cdz;
+    const A xy = A(0.25) * (ugrady2 - ugrady1) / cdy + A(0.25) * (vgradx2 - vgradx1) / cdx;
+    const A xz = A(0.25) * (ugradz2 - ugradz1) / cdz + A(0.25) * (wgradx2 - wgradx1) / cdx;
+    const A yz = A(0.25) * (vgradz2 - vgradz1) / cdz + A(0.25) * (wgrady2 - wgrady1) / cdy;
     // the neighbours' pressures as ideal_gas stores them (density0 and
     // energy0 carry the halo the pressure's would mirror)
     using C = typename S::cs_t;
@@ -260,9 +255,8 @@ __global__ void __launch_bounds__(BX * BY, sizeof(typename S::arith_t) == 4 || M
   const A ds = geo_ds<A>(g);
   // ideal_gas_kernel.f90:47-58 on this cell, stored as ideal_gas stores it
   A ss;
-  const A v_eos_r = A(1.0) / d0;
   {
-    const A v_eos = v_eos_r;
+    const A v_eos = A(1.0) / d0;
     const A p_eos = (A(1.4) - A(1.0)) * d0 * LA(energy0, j, k, l);
     const A pbe = (A(1.4) - A(1.0)) * d0;
     const A pbv = -d0 * p_eos;
@@ -273,8 +267,7 @@ __global__ void __launch_bounds__(BX * BY, sizeof(typename S::arith_t) == 4 || M
     ss = (A)ss_st;
   }
   A cc = ss * ss;
-  // v_eos = RN(1/d0): the quotient by d0 without the IEEE division sequence
-  cc = cc + div_rn(A(2.0) * visc, d0, v_eos_r);
+  cc = cc + A(2.0) * visc / d0;
   A dtct = ds * cc;
   dtct = a_dtc * A(1.0) / fmax2(sqrt(dtct), a_gs);
   const A vol = (A)g.vol;
@@ -801,10 +794,8 @@ __global__ void __launch_bounds__(BX * BY, sizeof(typename S::arith_t) == 4 && !
   if (p1 > phi) p1 = phi;
 #define IDX(p) j, (DIR == 2 ? (p) : c), (DIR == 2 ? c : (p))
   const double* cd = DIR == 2 ? ga.celldy : ga.celldz;
-  const double* rcd = DIR == 2 ? ga.rcelldy : ga.rcelldz;
   const int cdlo = DIR == 2 ? g.y_min : g.z_min;
 #define CD(p) cd[g.o1 + (p) - cdlo + 2]
-#define RCD(p) rcd[g.o1 + (p) - cdlo + 2]
   using V = typename S::vel_t;
   using A = typename S::arith_t;  // arithmetic of the flux and update
 #define LA(a, idx) lda<A>(&EI_(a, idx))
@@ -820,8 +811,7 @@ __global__ void __launch_bounds__(BX * BY, sizeof(typename S::arith_t) == 4 && !
   {
     // mom_flux(p0-1)
     const MomNodeTerms<A> nt =
-        mom_node_terms<A>(nf_m, pre_m, pre_0, (A)CD(p0 - 1), (A)CD(p0 - 2), (A)CD(p0),
-                          (A)RCD(p0 - 1), (A)RCD(p0 - 2), (A)RCD(p0));
+        mom_node_terms<A>(nf_m, pre_m, pre_0, (A)CD(p0 - 1), (A)CD(p0 - 2), (A)CD(p0));
 #pragma unroll
     for (int q = 0; q < 3; q++) {
       vw[q][0] = LA(in[q], IDX(p0 - 2));
@@ -839,15 +829,12 @@ __global__ void __launch_bounds__(BX * BY, sizeof(typename S::arith_t) == 4 && !
 #pragma unroll
     for (int q = 0; q < 3; q++) vn[q] = LA(in[q], IDX(p + 2));
     const MomNodeTerms<A> nt =
-        mom_node_terms<A>(nf_0, pre_0, pre_p, (A)CD(p), (A)CD(p - 1), (A)CD(p + 1), (A)RCD(p),
-                          (A)RCD(p - 1), (A)RCD(p + 1));
-    // the three updates divide by the same node mass: one reciprocal
-    const A r_post = A(1.0) / post_0;
+        mom_node_terms<A>(nf_0, pre_0, pre_p, (A)CD(p), (A)CD(p - 1), (A)CD(p + 1));
 #pragma unroll
     for (int q = 0; q < 3; q++) {
       const A vp2 = vn[q];
       const A mf_0 = mom_flux_v<A>(nt, vw[q][1], vw[q][2], vw[q][3], vp2);
-      const V vn1 = st<V>(div_rn(vw[q][2] * pre_0 + mf_prev[q] - mf_0, post_0, r_post));
+      const V vn1 = st<V>((vw[q][2] * pre_0 + mf_prev[q] - mf_0) / post_0);
       EI(out[q], IDX(p)) = vn1;
       if (lz.xvel0) EI(lev0[q], IDX(p)) = vn1;  // last sweep of the step: reset_field
       mf_prev[q] = mf_0;
@@ -859,7 +846,6 @@ __global__ void __launch_bounds__(BX * BY, sizeof(typename S::arith_t) == 4 && !
     pre_0 = pre_p;
   }
 #undef LA
-#undef RCD
 #undef CD
 #undef IDX
   });
@@ -1048,9 +1034,6 @@ __global__ void __launch_bounds__(BX * BY, M::kFlat || sizeof(typename S::arith_
   const double cd_0 = has_nf ? GX(ga.celldx, j) : 1.0;
   const double cd_m1 = has_mf ? GX(ga.celldx, j - 1) : 1.0;
   const double cd_p1 = has_mf ? GX(ga.celldx, j + 1) : 1.0;
-  const double rcd_0 = has_nf ? GX(ga.rcelldx, j) : 1.0;
-  const double rcd_m1 = has_mf ? GX(ga.rcelldx, j - 1) : 1.0;
-  const double rcd_p1 = has_mf ? GX(ga.rcelldx, j + 1) : 1.0;
   // plane l-1 terms: mass fluxes at (j, k-1), (j, k), (j+1, k-1), (j+1, k); cell
   // masses at (j, k-1), (j, k)
   double fm_a = 0.0, fm_b = 0.0, fm_c = 0.0, fm_d = 0.0, pm_a = 0.0, pm_b = 0.0;
@@ -1078,10 +1061,7 @@ __global__ void __launch_bounds__(BX * BY, M::kFlat || sizeof(typename S::arith_
     // flux and update in the momentum arithmetic A (node masses are FP64)
     using A = typename S::arith_t;
     const MomNodeTerms<A> nt =
-        mom_node_terms<A>((A)nf, (A)nmpre, (A)nmpre_p, (A)cd_0, (A)cd_m1, (A)cd_p1, (A)rcd_0,
-                          (A)rcd_m1, (A)rcd_p1);
-    // the three updates divide by the same node mass: one reciprocal
-    const A r_nmp = A(1.0) / (A)nmp;
+        mom_node_terms<A>((A)nf, (A)nmpre, (A)nmpre_p, (A)cd_0, (A)cd_m1, (A)cd_p1);
 #pragma unroll
     for (int q = 0; q < 3; q++) {
       A mf = A(0.0), v0 = A(0.0);
@@ -1093,7 +1073,7 @@ __global__ void __launch_bounds__(BX * BY, M::kFlat || sizeof(typename S::arith_
       }
       const A mf_m = __shfl_up_sync(0xffffffffu, mf, 1);
       if (has_up) {
-        const V vn1 = st<V>(div_rn(v0 * (A)nmpre + mf_m - mf, (A)nmp, r_nmp));
+        const V vn1 = st<V>((v0 * (A)nmpre + mf_m - mf) / (A)nmp);
         E(out[q], j, k, l) = vn1;
         if (lz.xvel0) E(lev0[q], j, k, l) = vn1;  // last sweep of the step: reset_field
       }

@@ -1342,16 +1342,6 @@ void launch_reset_field(const Target& tg, cudaStream_t s, typename S::rho_t* den
                 yvel1, zvel0, zvel1);
 }
 
-__global__ void k_reciprocal(const double* __restrict__ in, double* __restrict__ out, long long n) {
-  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-       i += (long long)gridDim.x * blockDim.x)
-    out[i] = 1.0 / in[i];
-}
-
-void launch_reciprocal(cudaStream_t s, const double* in, double* out, long long n) {
-  if (n > 0) k_reciprocal<<<(unsigned)((n + 255) / 256 < 1024 ? (n + 255) / 256 : 1024), 256, 0, s>>>(in, out, n);
-}
-
 int summary_partials_len() { return SUM_BLOCKS * 2 * kSumQ; }
 
 template <class S>

@@ -173,9 +173,6 @@ struct GeomArrays {
   const double *celldx, *celldy, *celldz;
   const double *vertexx, *vertexy, *vertexz;
   const double *vertexdx, *vertexdy, *vertexdz;
-  // RN(1/celld*) element by element (native chunks; null in the drop-in ABI):
-  // the momentum limiter's divisions by cell widths as div_rn quotients
-  const double *rcelldx = nullptr, *rcelldy = nullptr, *rcelldz = nullptr;
 };
 
 // The 19 halo-exchangeable fields in reference id order (data.f90:55-74).
@@ -402,9 +399,6 @@ void launch_advec_mom_fused(const Target& tg, cudaStream_t s, int advect_x, int 
                             typename S::vel_t* const* vel_out, bool copy_shell,
                             const Level0<S>& level0, const MomXMaps* x_maps = nullptr,
                             int* status = nullptr);
-
-// out[i] = 1 / in[i] (IEEE division) for i < n.
-void launch_reciprocal(cudaStream_t s, const double* in, double* out, long long n);
 
 // Fill every element of an array (size elems after the pad) with a value.
 template <class T>

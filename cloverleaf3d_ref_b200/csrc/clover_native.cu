@@ -136,7 +136,6 @@ struct Chunk : ChunkBase {
   double *volume, *xarea, *yarea, *zarea;
   double *cellx, *celly, *cellz, *celldx, *celldy, *celldz;
   double *vertexx, *vertexy, *vertexz, *vertexdx, *vertexdy, *vertexdz;
-  double *rcelldx, *rcelldy, *rcelldz;  // RN(1/celld*), for the momentum limiter
   GeomArrays ga;
 
   DevScalars* sc = nullptr;
@@ -149,7 +148,6 @@ struct Chunk : ChunkBase {
   int* plane_base = nullptr;  // ensemble: first summary plane of each deck (nd + 1)
 
   double cell_volume = 0.0;  // dx*dy*dz, the volume of every cell (initialise_chunk)
-  long long total1d = 0;     // elements of each shared 1D allocation
   int host_step = 0;     // steps enqueued
   bool advect_x = true;  // start.f90:99
   bool use_graphs = true;
@@ -358,18 +356,15 @@ struct Chunk : ChunkBase {
     chk(xarea = alloc_field<double>(e3, owned, bytes, stream));
     chk(yarea = alloc_field<double>(e3, owned, bytes, stream));
     chk(zarea = alloc_field<double>(e3, owned, bytes, stream));
-    double** one_d[15] = {&cellx, &celly, &cellz, &celldx, &celldy, &celldz,
-                          &vertexx, &vertexy, &vertexz, &vertexdx, &vertexdy, &vertexdz,
-                          &rcelldx, &rcelldy, &rcelldz};
+    double** one_d[12] = {&cellx, &celly, &cellz, &celldx, &celldy, &celldz,
+                          &vertexx, &vertexy, &vertexz, &vertexdx, &vertexdy, &vertexdz};
     for (double** a : one_d) chk(*a = alloc_1d(total1, owned, bytes, stream));
     if (!ok) {
       g_last_error = "device allocation failed";
       return false;
     }
     ga = GeomArrays{volume, xarea, yarea, zarea, cellx, celly, cellz, celldx, celldy, celldz,
-                    vertexx, vertexy, vertexz, vertexdx, vertexdy, vertexdz, rcelldx, rcelldy,
-                    rcelldz};
-    total1d = total1;
+                    vertexx, vertexy, vertexz, vertexdx, vertexdy, vertexdz};
     // one chunk: the stencils that stage their planes with bulk-tensor copies
     // get their tensor maps (the arrays they read never move)
     if (!batched)
@@ -447,11 +442,6 @@ struct Chunk : ChunkBase {
       launch_initialise_chunk(q, stream, xmin, ymin, zmin, dx, dy, dz, vertexx, vertexdx,
                               vertexy, vertexdy, vertexz, vertexdz, cellx, celldx, celly, celldy,
                               cellz, celldz, volume, xarea, yarea, zarea);
-      if (i == nd - 1) {  // every deck's widths are set: their reciprocals
-        launch_reciprocal(stream, celldx, rcelldx, total1d);
-        launch_reciprocal(stream, celldy, rcelldy, total1d);
-        launch_reciprocal(stream, celldz, rcelldz, total1d);
-      }
       // read_input.f90:293-303 nudge, then generate_chunk
       StateTable st;
       st.n = d.number_of_states;

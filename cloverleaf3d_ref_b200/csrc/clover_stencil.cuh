@@ -44,27 +44,21 @@ __device__ __forceinline__ double node_mass_sum(double p_0m0, double p_000, doub
 // from the velocity window v(i-1..i+2). The donor side, the Courant number
 // sigma and the limiter's cell widths depend on the node only, so they are
 // formed once per node (MomNodeTerms) for the three velocity components.
-// The limiter divides by the node's cell width and by the upwind one: rw and
-// rcd_dif are their correctly rounded reciprocals, so those quotients are
-// div_rn's (clover_div.cuh), the same bits as the IEEE division.
 template <class A>
 struct MomNodeTerms {
   bool neg;  // node flux < 0: the donor is node i+1
-  A nf, sigma, width, cd_dif, rw, rcd_dif;
+  A nf, sigma, width, cd_dif;
 };
 
 template <class A>
 __device__ __forceinline__ MomNodeTerms<A> mom_node_terms(A nf, A nmpre_i, A nmpre_ip1, A width,
-                                                          A cd_m1, A cd_p1, A r_width, A r_cd_m1,
-                                                          A r_cd_p1) {
+                                                          A cd_m1, A cd_p1) {
   MomNodeTerms<A> t;
   t.neg = nf < A(0.0);
   t.nf = nf;
   t.sigma = fabs(nf) / (t.neg ? nmpre_ip1 : nmpre_i);
   t.width = width;
   t.cd_dif = t.neg ? cd_p1 : cd_m1;
-  t.rw = r_width;
-  t.rcd_dif = t.neg ? r_cd_p1 : r_cd_m1;
   return t;
 }
 
@@ -82,10 +76,9 @@ __device__ __forceinline__ A mom_flux_v(const MomNodeTerms<A>& t, A vm1, A v0, A
     A wind = A(1.0);
     if (vdiffdw <= A(0.0)) wind = A(-1.0);
     const A width = t.width, sigma = t.sigma;
-    // the quotients by the widths and by 6.0_8 correctly rounded without the
-    // IEEE division sequence (clover_div.cuh)
-    limiter = wind * fmin2(fmin2(div6(width * (div_rn((A(2.0) - sigma) * adw, width, t.rw) +
-                                               div_rn((A(1.0) + sigma) * auw, t.cd_dif, t.rcd_dif))),
+    // ... / 6.0_8 correctly rounded by div6 (clover_div.cuh)
+    limiter = wind * fmin2(fmin2(div6(width * ((A(2.0) - sigma) * adw / width +
+                                               (A(1.0) + sigma) * auw / t.cd_dif)),
                                  auw),
                            adw);
   }
@@ -93,5 +86,11 @@ __device__ __forceinline__ A mom_flux_v(const MomNodeTerms<A>& t, A vm1, A v0, A
   return advec_vel_s * t.nf;
 }
 
+template <class A>
+__device__ __forceinline__ A mom_flux_at(A nf, A nmpre_i, A nmpre_ip1, A vm1, A v0, A vp1, A vp2,
+                                         A width, A cd_m1, A cd_p1) {
+  return mom_flux_v<A>(mom_node_terms<A>(nf, nmpre_i, nmpre_ip1, width, cd_m1, cd_p1), vm1, v0,
+                       vp1, vp2);
+}
 
 }  // namespace clover

@@ -179,19 +179,12 @@ k_visc_dt_tma(Geom g, int seg, GeomArrays ga, double g_small, double dtc_safe, d
         const A cdx = (A)ga.celldx[g.o1 + j - g.x_min + 2];
         const A cdy = (A)ga.celldy[g.o1 + k - g.y_min + 2];
         const A cdz = (A)ga.celldz[g.o1 + l - g.z_min + 2];
-        // quotients by the widths from their correctly rounded reciprocals
-        const A rx = (A)ga.rcelldx[g.o1 + j - g.x_min + 2];
-        const A ry = (A)ga.rcelldy[g.o1 + k - g.y_min + 2];
-        const A rz = (A)ga.rcelldz[g.o1 + l - g.z_min + 2];
-        const A xx = div_rn(A(0.25) * (ugradx2 - ugradx1), cdx, rx);
-        const A yy = div_rn(A(0.25) * (vgrady2 - vgrady1), cdy, ry);
-        const A zz = div_rn(A(0.25) * (wgradz2 - wgradz1), cdz, rz);
-        const A xy = div_rn(A(0.25) * (ugrady2 - ugrady1), cdy, ry) +
-                     div_rn(A(0.25) * (vgradx2 - vgradx1), cdx, rx);
-        const A xz = div_rn(A(0.25) * (ugradz2 - ugradz1), cdz, rz) +
-                     div_rn(A(0.25) * (wgradx2 - wgradx1), cdx, rx);
-        const A yz = div_rn(A(0.25) * (vgradz2 - vgradz1), cdz, rz) +
-                     div_rn(A(0.25) * (wgrady2 - wgrady1), cdy, ry);
+        const A xx = A(0.25) * (ugradx2 - ugradx1) / cdx;
+        const A yy = A(0.25) * (vgrady2 - vgrady1) / cdy;
+        const A zz = A(0.25) * (wgradz2 - wgradz1) / cdz;
+        const A xy = A(0.25) * (ugrady2 - ugrady1) / cdy + A(0.25) * (vgradx2 - vgradx1) / cdx;
+        const A xz = A(0.25) * (ugradz2 - ugradz1) / cdz + A(0.25) * (wgradx2 - wgradx1) / cdx;
+        const A yz = A(0.25) * (vgradz2 - vgradz1) / cdz + A(0.25) * (wgrady2 - wgrady1) / cdy;
         // the neighbours' pressures as ideal_gas stores them
 #define PN(bb, a, b) ((A)st<C>(((A(1.4) - A(1.0)) * DN(bb, a, b) * EN(bb, a, b))))
         A pgradx = (PN(bl, 1, 0) - PN(bl, -1, 0)) /
@@ -227,9 +220,8 @@ k_visc_dt_tma(Geom g, int seg, GeomArrays ga, double g_small, double dtc_safe, d
       const A d0 = DN(bl, 0, 0);
       const A ds = geo_ds<A>(g);
       A ss;
-      const A v_eos_r = A(1.0) / d0;
       {
-        const A v_eos = v_eos_r;
+        const A v_eos = A(1.0) / d0;
         const A p_eos = (A(1.4) - A(1.0)) * d0 * EN(bl, 0, 0);
         const A pbe = (A(1.4) - A(1.0)) * d0;
         const A pbv = -d0 * p_eos;
@@ -240,8 +232,7 @@ k_visc_dt_tma(Geom g, int seg, GeomArrays ga, double g_small, double dtc_safe, d
         ss = (A)ss_st;
       }
       A cc = ss * ss;
-      // v_eos = RN(1/d0): the quotient by d0 without the IEEE division sequence
-      cc = cc + div_rn(A(2.0) * visc, d0, v_eos_r);
+      cc = cc + A(2.0) * visc / d0;
       A dtct = ds * cc;
       dtct = a_dtc * A(1.0) / fmax2(sqrt(dtct), a_gs);
       const A vol = (A)g.vol;
@@ -427,9 +418,6 @@ k_mom_sweep_x_tma(Geom g, int seg, GeomArrays ga, const __grid_constant__ MomXMa
   const double cd_0 = has_nf ? ga.celldx[g.o1 + j - g.x_min + 2] : 1.0;
   const double cd_m1 = has_mf ? ga.celldx[g.o1 + j - 1 - g.x_min + 2] : 1.0;
   const double cd_p1 = has_mf ? ga.celldx[g.o1 + j + 1 - g.x_min + 2] : 1.0;
-  const double rcd_0 = has_nf ? ga.rcelldx[g.o1 + j - g.x_min + 2] : 1.0;
-  const double rcd_m1 = has_mf ? ga.rcelldx[g.o1 + j - 1 - g.x_min + 2] : 1.0;
-  const double rcd_p1 = has_mf ? ga.rcelldx[g.o1 + j + 1 - g.x_min + 2] : 1.0;
   typename S::vel_t* out[3] = {u_out, v_out, w_out};
   typename S::vel_t* lev0[3] = {lz.xvel0, lz.yvel0, lz.zvel0};
   // plane l0-1 terms: mass fluxes at (j, k-1), (j, k), (j+1, k-1), (j+1, k);
@@ -463,10 +451,7 @@ k_mom_sweep_x_tma(Geom g, int seg, GeomArrays ga, const __grid_constant__ MomXMa
       const double nmpre = nmp - nf_m + nf;
       const double nmpre_p = __shfl_down_sync(fullmask, nmpre, 1);
       const MomNodeTerms<A> nt =
-          mom_node_terms<A>((A)nf, (A)nmpre, (A)nmpre_p, (A)cd_0, (A)cd_m1, (A)cd_p1, (A)rcd_0,
-                            (A)rcd_m1, (A)rcd_p1);
-      // the three updates divide by the same node mass: one reciprocal
-      const A r_nmp = A(1.0) / (A)nmp;
+          mom_node_terms<A>((A)nf, (A)nmpre, (A)nmpre_p, (A)cd_0, (A)cd_m1, (A)cd_p1);
 #pragma unroll
       for (int q = 0; q < 3; q++) {
         const V* vr = P::vel(b, q) + ty * WV + cv;
@@ -477,7 +462,7 @@ k_mom_sweep_x_tma(Geom g, int seg, GeomArrays ga, const __grid_constant__ MomXMa
         }
         const A mf_m = __shfl_up_sync(fullmask, mf, 1);
         if (has_up) {
-          const V vn1 = st<V>(div_rn(v0 * (A)nmpre + mf_m - mf, (A)nmp, r_nmp));
+          const V vn1 = st<V>((v0 * (A)nmpre + mf_m - mf) / (A)nmp);
           const long long o = off3(g, j, k, l);
           out[q][o] = vn1;
           if (lz.xvel0) lev0[q][o] = vn1;  // last sweep of the step: reset_field
