@@ -561,6 +561,24 @@ void launch_mom_x_tma(const Geom& g, cudaStream_t s, int sweep, int seg, const M
             g, seg, ga, maps, vel_out[0], vel_out[1], vel_out[2], level0, status);
 }
 
+// The bounded wait of the staged kernels, made to run out: one block arms a
+// barrier phase for 16 bytes of copies that nothing issues, waits with the
+// same mbar_wait_bounded the kernels use (limit `cycles`), and reports the
+// failure as they do. Nothing else happens on the GPU, so the context stays
+// usable.
+__global__ void k_wait_selftest(long long cycles, int* status) {
+  __shared__ unsigned long long bar;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    mbar_init_fence();
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) mbar_arrive_expect_tx(&bar, 16);
+  __syncthreads();
+  const bool done = mbar_wait_bounded(&bar, 0u, cycles);
+  if (!done && threadIdx.x == 0) atomicOr(status, CLOVER_STATUS_TIMEOUT);
+}
+
 #define INST_TMA(S)                                                                              \
   template bool visc_dt_tma_maps<S>(const Geom&, const S::vel_t*, const S::vel_t*,              \
                                     const S::vel_t*, const S::rho_t*, const S::ene_t*,          \
@@ -576,3 +594,21 @@ INST_TMA(F64)
 INST_TMA(F32Mixed)
 
 }  // namespace clover
+
+using namespace clover;
+
+extern "C" int clover_gpu_wait_selftest(long long cycles) {
+  int* d = nullptr;
+  int h = 0;
+  if (cudaMalloc(&d, sizeof(int)) != cudaSuccess) {
+    cudaGetLastError();
+    return CLOVER_STATUS_CUDA_ERROR;
+  }
+  cudaMemset(d, 0, sizeof(int));
+  k_wait_selftest<<<1, 32>>>(cycles, d);
+  const cudaError_t e1 = cudaGetLastError();
+  const cudaError_t e2 = cudaMemcpy(&h, d, sizeof(int), cudaMemcpyDeviceToHost);
+  cudaFree(d);
+  if (e1 != cudaSuccess || e2 != cudaSuccess) return CLOVER_STATUS_CUDA_ERROR;
+  return h;
+}

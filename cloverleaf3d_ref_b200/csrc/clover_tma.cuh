@@ -125,12 +125,13 @@ __device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned 
 constexpr long long kTmaWaitCycles = 2000000000ll;
 
 // Wait for the phase of the given parity; false if it did not complete
-// within kTmaWaitCycles.
-__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsigned parity) {
+// within `limit` cycles.
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsigned parity,
+                                                  long long limit = kTmaWaitCycles) {
   if (mbar_try_wait(bar, parity)) return true;
   const long long t0 = clock64();
   while (!mbar_try_wait(bar, parity))
-    if (clock64() - t0 > kTmaWaitCycles) return false;
+    if (clock64() - t0 > limit) return false;
   return true;
 }
 

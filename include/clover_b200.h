@@ -82,6 +82,14 @@ void clover_chunk_use_fused(clover_chunk *c, int on);
  * always use the register-marching forms. */
 int clover_chunk_use_tma(clover_chunk *c, int on);
 
+/* Self-test of the staged kernels' failure detection (no counterpart in the
+ * reference): a one-block kernel waits, with the bounded wait those kernels
+ * use and a limit of `cycles` SM clocks, for copies that nothing issues, and
+ * reports as they do. Returns CLOVER_STATUS_TIMEOUT when the wait ran out
+ * and was reported (the expected answer), 0 if it did not run out, or
+ * CLOVER_STATUS_CUDA_ERROR. The device stays usable. */
+int clover_gpu_wait_selftest(long long cycles);
+
 /* Host copies of the device records (these synchronise):
  * steps taken, simulated time, dt of each step, field summaries
  * (vol, mass, ie, ke, press) with the step each was taken at. */
