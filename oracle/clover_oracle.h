@@ -217,6 +217,15 @@ int oracle_run(const oracle_deck *deck, int max_steps, double *dt_out, int max_s
                double *summary_out, int *summary_step_out, int *n_summaries,
                double **fields_out);
 
+/* oracle_run keeping the chunk: *steps receives oracle_run's return value;
+ * the handle gives field id 1..19 in its reference shape (oracle_kept_field)
+ * until oracle_kept_free. For comparing a large run array by array. */
+void *oracle_run_keep(const oracle_deck *deck, int max_steps, double *dt_out, int max_summaries,
+                      double *summary_out, int *summary_step_out, int *n_summaries,
+                      int *steps);
+int oracle_kept_field(void *h, int id, double *out);
+void oracle_kept_free(void *h);
+
 /* CPU-baseline timing: run warmup + steps steps of the deck and return the
  * wall seconds of the last `steps` (the step loop including its field
  * summaries, without set-up). */

@@ -227,12 +227,11 @@ static void record(double *summary_out, int *summary_step_out, int *n, int cap, 
   (*n)++;
 }
 
-int oracle_run(const oracle_deck *dk, int max_steps, double *dt_out, int max_summaries,
-               double *summary_out, int *summary_step_out, int *n_summaries,
-               double **fields_out) {
-  tile_t tt, *t = &tt;
+/* The hydro loop on a built chunk t (the body of oracle_run). */
+static int run_chunk(tile_t *t, const oracle_deck *dk, int max_steps, double *dt_out,
+                     int max_summaries, double *summary_out, int *summary_step_out,
+                     int *n_summaries) {
   int nsum = 0;
-  build_field(t, dk->x_cells, dk->y_cells, dk->z_cells);
 
   /* initialise_chunk.f90:38-46 (float() of the cell count is a default REAL) */
   double dx = (dk->xmax - dk->xmin) / (double)(float)dk->x_cells;
@@ -314,20 +313,59 @@ int oracle_run(const oracle_deck *dk, int max_steps, double *dt_out, int max_sum
   }
   timing_t1 = now_s();
   if (n_summaries) *n_summaries = nsum;
+  return step;
+}
 
-  if (fields_out) {
-    double *src[19] = {t->density0, t->density1, t->energy0, t->energy1, t->pressure,
-                       t->viscosity, t->soundspeed, t->xvel0, t->xvel1, t->yvel0,
-                       t->yvel1, t->zvel0, t->zvel1, t->vol_flux_x, t->vol_flux_y,
-                       t->vol_flux_z, t->mass_flux_x, t->mass_flux_y, t->mass_flux_z};
-    long n[19] = {t->ncell, t->ncell, t->ncell, t->ncell, t->ncell, t->ncell, t->ncell,
-                  t->nvert, t->nvert, t->nvert, t->nvert, t->nvert, t->nvert,
-                  t->nxf, t->nyf, t->nzf, t->nxf, t->nyf, t->nzf};
+/* Field id (1..19, data.f90:55-74) of chunk t into out (its reference shape). */
+static void copy_field(const tile_t *t, int id, double *out) {
+  double *src[19] = {t->density0, t->density1, t->energy0, t->energy1, t->pressure,
+                     t->viscosity, t->soundspeed, t->xvel0, t->xvel1, t->yvel0,
+                     t->yvel1, t->zvel0, t->zvel1, t->vol_flux_x, t->vol_flux_y,
+                     t->vol_flux_z, t->mass_flux_x, t->mass_flux_y, t->mass_flux_z};
+  long n[19] = {t->ncell, t->ncell, t->ncell, t->ncell, t->ncell, t->ncell, t->ncell,
+                t->nvert, t->nvert, t->nvert, t->nvert, t->nvert, t->nvert,
+                t->nxf, t->nyf, t->nzf, t->nxf, t->nyf, t->nzf};
+  memcpy(out, src[id - 1], (size_t)n[id - 1] * sizeof(double));
+}
+
+int oracle_run(const oracle_deck *dk, int max_steps, double *dt_out, int max_summaries,
+               double *summary_out, int *summary_step_out, int *n_summaries,
+               double **fields_out) {
+  tile_t tt, *t = &tt;
+  build_field(t, dk->x_cells, dk->y_cells, dk->z_cells);
+  const int step = run_chunk(t, dk, max_steps, dt_out, max_summaries, summary_out,
+                             summary_step_out, n_summaries);
+  if (fields_out)
     for (int i = 0; i < 19; i++)
-      if (fields_out[i]) memcpy(fields_out[i], src[i], (size_t)n[i] * sizeof(double));
-  }
+      if (fields_out[i]) copy_field(t, i + 1, fields_out[i]);
   free_field(t);
   return step;
+}
+
+/* oracle_run keeping the chunk: *steps receives its return value, and the
+ * handle gives the fields one at a time (oracle_kept_field) until
+ * oracle_kept_free, so that a large run is compared array by array. */
+void *oracle_run_keep(const oracle_deck *dk, int max_steps, double *dt_out, int max_summaries,
+                      double *summary_out, int *summary_step_out, int *n_summaries,
+                      int *steps) {
+  tile_t *t = (tile_t *)malloc(sizeof(tile_t));
+  if (!t) return NULL;
+  build_field(t, dk->x_cells, dk->y_cells, dk->z_cells);
+  *steps = run_chunk(t, dk, max_steps, dt_out, max_summaries, summary_out, summary_step_out,
+                     n_summaries);
+  return t;
+}
+
+int oracle_kept_field(void *h, int id, double *out) {
+  if (!h || id < 1 || id > 19) return -1;
+  copy_field((const tile_t *)h, id, out);
+  return 0;
+}
+
+void oracle_kept_free(void *h) {
+  if (!h) return;
+  free_field((tile_t *)h);
+  free(h);
 }
 
 double oracle_run_timed(const oracle_deck *deck, int warmup, int steps) {

@@ -152,6 +152,50 @@ def run(deck, max_steps=None, want_fields=False, fast=False, symmetric=False):
     }
 
 
+class KeptRun:
+    """An oracle run whose chunk stays in host memory: dt, summaries and steps
+    as run() gives them, and each field fetched on demand (for runs too large
+    to hold every field twice)."""
+
+    def __init__(self, deck, max_steps=None):
+        lib = load()
+        lib.oracle_run_keep.restype = ctypes.c_void_p
+        lib.oracle_kept_field.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
+        lib.oracle_kept_free.argtypes = [ctypes.c_void_p]
+        self.lib = lib
+        od = make_deck(deck)
+        if max_steps is None:
+            max_steps = od.end_step
+        nsum_cap = max_steps // max(od.summary_frequency, 1) + 4
+        dts = np.zeros(max_steps, dtype=np.float64)
+        sums = np.zeros((nsum_cap, 5), dtype=np.float64)
+        steps = np.zeros(nsum_cap, dtype=np.int32)
+        nsum, nsteps = ctypes.c_int(0), ctypes.c_int(0)
+        self.h = lib.oracle_run_keep(
+            ctypes.byref(od), ctypes.c_int(max_steps), dts.ctypes.data_as(ctypes.c_void_p),
+            ctypes.c_int(nsum_cap), sums.ctypes.data_as(ctypes.c_void_p),
+            steps.ctypes.data_as(ctypes.c_void_p), ctypes.byref(nsum), ctypes.byref(nsteps))
+        if not self.h:
+            raise MemoryError("oracle chunk allocation failed")
+        n = min(nsum.value, nsum_cap)
+        self.steps = nsteps.value
+        self.dt = dts[:abs(nsteps.value)]
+        self.summaries = sums[:n]
+        self.summary_steps = steps[:n]
+        self.dims = (od.x_cells, od.y_cells, od.z_cells)
+
+    def field(self, name):
+        a = np.zeros(shape(FIELD_KIND[name], *self.dims), order="F")
+        assert self.lib.oracle_kept_field(self.h, FIELD_NAMES.index(name) + 1,
+                                          a.ctypes.data_as(ctypes.c_void_p)) == 0
+        return a
+
+    def close(self):
+        if self.h:
+            self.lib.oracle_kept_free(self.h)
+            self.h = None
+
+
 def ptr(a):
     return a.ctypes.data_as(ctypes.c_void_p)
 
