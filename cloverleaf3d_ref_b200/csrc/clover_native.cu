@@ -368,7 +368,7 @@ struct Chunk : ChunkBase {
     // one chunk: the stencils that stage their planes with bulk-tensor copies
     // get their tensor maps (the arrays they read never move)
     if (!batched)
-      tma = visc_dt_tma_prepare<S>() && mom_x_tma_prepare<S>() &&
+      tma = visc_dt_tma_prepare<S>() && mom_x_tma_prepare<S>() && stencils_tma_prepare<S>() &&
             visc_dt_tma_maps<S>(g, xvel0, yvel0, zvel0, density0, energy0, &visc_maps);
 
     dt_cap = deck.end_step < (1 << 22) ? deck.end_step + 16 : (1 << 22);
@@ -789,20 +789,43 @@ struct Chunk : ChunkBase {
     pend("update_halo", 0);
     // PdV.f90:50-107: predictor + EOS on the predicted state; revert is implied
     pbeg();
-    launch_pdv_predict_eos<S>(tg, stream, dtp, ga, density0, energy0, pressure, viscosity, xvel0,
-                              yvel0, zvel0);
+    PdvMaps pdv_m;
+    if (tma && use_tma && tmap(xvel0, sizeof(V), 9, &pdv_m.u) && tmap(yvel0, sizeof(V), 9, &pdv_m.v) &&
+        tmap(zvel0, sizeof(V), 9, &pdv_m.w) && tmap(density0, sizeof(R), 8, &pdv_m.d) &&
+        tmap(energy0, sizeof(En), 8, &pdv_m.e) && tmap(pressure, sizeof(C), 8, &pdv_m.p) &&
+        tmap(viscosity, sizeof(C), 8, &pdv_m.q))
+      launch_pdv_predict_eos_tma<S>(g, stream, dtp, pdv_m, pressure, &sc->status);
+    else
+      launch_pdv_predict_eos<S>(tg, stream, dtp, ga, density0, energy0, pressure, viscosity, xvel0,
+                                yvel0, zvel0);
     pend("pdv", n * (R8 + E8 + 3 * C8 + 3 * V8));
     pbeg();
     halo({5}, 1, vc, cb);
     pend("update_halo", 0);
     pbeg();
-    launch_accelerate<S>(tg, stream, 0.0, dtp, ga, density0, pressure, viscosity, xvel0, yvel0,
-                         zvel0, vel1(0, vc), vel1(1, vc), vel1(2, vc), true);
+    AccMaps acc_m;
+    if (tma && use_tma && tmap(density0, sizeof(R), 9, &acc_m.d) &&
+        tmap(pressure, sizeof(C), 9, &acc_m.p) && tmap(viscosity, sizeof(C), 9, &acc_m.q) &&
+        tmap(xvel0, sizeof(V), 8, &acc_m.u) && tmap(yvel0, sizeof(V), 8, &acc_m.v) &&
+        tmap(zvel0, sizeof(V), 8, &acc_m.w))
+      launch_accelerate_tma<S>(g, stream, dtp, acc_m, vel1(0, vc), vel1(1, vc), vel1(2, vc),
+                               &sc->status);
+    else
+      launch_accelerate<S>(tg, stream, 0.0, dtp, ga, density0, pressure, viscosity, xvel0, yvel0,
+                           zvel0, vel1(0, vc), vel1(1, vc), vel1(2, vc), true);
     pend("accelerate", n * (R8 + 2 * C8 + 6 * V8));
     pbeg();
-    launch_pdv_flux<S>(tg, stream, dtp, ga, density0, rho1(cb), energy0, ene1(cb), pressure,
-                       viscosity, xvel0, vel1(0, vc), yvel0, vel1(1, vc), zvel0, vel1(2, vc),
-                       vol_flux_x, vol_flux_y, vol_flux_z);
+    FluxMaps flux_m;
+    if (tma && use_tma && tmap(xvel0, sizeof(V), 9, &flux_m.u0) &&
+        tmap(yvel0, sizeof(V), 9, &flux_m.v0) && tmap(zvel0, sizeof(V), 9, &flux_m.w0) &&
+        tmap(vel1(0, vc), sizeof(V), 9, &flux_m.u1) && tmap(vel1(1, vc), sizeof(V), 9, &flux_m.v1) &&
+        tmap(vel1(2, vc), sizeof(V), 9, &flux_m.w1))
+      launch_pdv_flux_tma<S>(g, stream, dtp, flux_m, density0, rho1(cb), energy0, ene1(cb),
+                             pressure, viscosity, vol_flux_x, vol_flux_y, vol_flux_z, &sc->status);
+    else
+      launch_pdv_flux<S>(tg, stream, dtp, ga, density0, rho1(cb), energy0, ene1(cb), pressure,
+                         viscosity, xvel0, vel1(0, vc), yvel0, vel1(1, vc), zvel0, vel1(2, vc),
+                         vol_flux_x, vol_flux_y, vol_flux_z);
     pend("pdv_flux", n * (2 * R8 + 2 * E8 + 2 * C8 + 6 * V8 + 3 * VF8));
     // advection.f90:43-179. The last sweep also writes time level 0 (the
     // interior density/energy and node velocities reset_field copies), so

@@ -486,6 +486,396 @@ k_mom_sweep_x_tma(Geom g, int seg, GeomArrays ga, const __grid_constant__ MomXMa
   }
 }
 
+// ---------------------------------------------------------------------------
+// The march of a staged block over planes l in [l0, l1]: body(l) reads the
+// buffers of planes l-BACK .. l+AHEAD; thread 0 starts plane p's copies with
+// issue(p) (which arms the plane's barrier). Plane l-BACK's buffer takes plane
+// l-BACK+RING once every thread is done with plane l. A wait that runs out
+// stops the block: CLOVER_STATUS_TIMEOUT in *status, and the copies still in
+// flight (the last RING planes issued) get a bounded wait before the block's
+// shared memory is released. full[RING] and *stop are shared memory.
+template <int RING, int BACK, int AHEAD>
+struct PlaneMarch {
+  unsigned char* ring;
+  int bytes;
+  unsigned long long* full;
+  int* stop;
+  int pfirst, plast;
+  __device__ unsigned char* buf(int p) const { return ring + ((p - pfirst) % RING) * bytes; }
+  __device__ unsigned long long* bar(int p) const { return &full[(p - pfirst) % RING]; }
+  __device__ void wait(int p) const {
+    const int u = p - pfirst;
+    if (!mbar_wait_bounded(&full[u % RING], (unsigned)(u / RING) & 1u)) *stop = 1;
+  }
+  template <class Issue, class Body>
+  __device__ void run(int l0, int l1, int* status, Issue issue, Body body) const {
+    const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+    if (tid == 0) {
+      for (int r = 0; r < RING; r++) mbar_init(&full[r], 1);
+      mbar_init_fence();
+      *stop = 0;
+    }
+    __syncthreads();
+    int issued_hi = pfirst - 1;
+    if (tid == 0)
+      for (int p = pfirst; p <= plast && p < pfirst + RING; p++) issue(p), issued_hi = p;
+    for (int p = pfirst; p < l0 + AHEAD; p++) wait(p);
+    for (int l = l0; l <= l1; l++) {
+      wait(l + AHEAD);
+      if (!*stop) body(l);
+      __syncthreads();
+      if (*stop) break;
+      const int np = l - BACK + RING;
+      if (tid == 0 && np <= plast) issue(np), issued_hi = np;
+    }
+    if (*stop && tid == 0) {
+      atomicOr(status, CLOVER_STATUS_TIMEOUT);
+      for (int p = issued_hi - RING + 1 > pfirst ? issued_hi - RING + 1 : pfirst; p <= issued_hi; p++) {
+        const int u = p - pfirst;
+        mbar_wait_bounded(&full[u % RING], (unsigned)(u / RING) & 1u);
+      }
+    }
+  }
+};
+
+// ---------------------------------------------------------------------------
+// PdV_kernel.f90:72-118 (predict) + ideal_gas_kernel.f90:47-58 on the predicted
+// state, as k_pdv_predict_eos (clover_fused.cu) forms them. Plane p: the
+// three node velocities of node plane p (rows k0..k0+8) and density0,
+// energy0, pressure and viscosity of cell plane p (rows k0..k0+7). Cell l
+// reads node planes l, l+1 and cell plane l.
+template <class S>
+struct PdvPlane {
+  using V = typename S::vel_t;
+  using R = typename S::rho_t;
+  using En = typename S::ene_t;
+  using C = typename S::cs_t;
+  static constexpr int kVel = round128(9 * kTmaWidth<V> * (int)sizeof(V));
+  static constexpr int kRho = round128(8 * kTmaWidth<R> * (int)sizeof(R));
+  static constexpr int kEne = round128(8 * kTmaWidth<En> * (int)sizeof(En));
+  static constexpr int kCs = round128(8 * kTmaWidth<C> * (int)sizeof(C));
+  static constexpr int kBytes = 3 * kVel + kRho + kEne + 2 * kCs;
+  static constexpr unsigned kTx = 3 * box_bytes<V>(9) + box_bytes<R>(8) + box_bytes<En>(8) +
+                                  2 * box_bytes<C>(8);
+  __device__ static V* vel(unsigned char* p, int q) { return (V*)(p + q * kVel); }
+  __device__ static R* rho(unsigned char* p) { return (R*)(p + 3 * kVel); }
+  __device__ static En* ene(unsigned char* p) { return (En*)(p + 3 * kVel + kRho); }
+  __device__ static C* cs(unsigned char* p, int q) { return (C*)(p + 3 * kVel + kRho + kEne + q * kCs); }
+};
+
+template <class S, int RING, int MINB>
+__global__ void __launch_bounds__(TX * TY, MINB)
+k_pdv_predict_eos_tma(Geom g, int seg, const double* __restrict__ dt_ptr,
+                      const __grid_constant__ PdvMaps maps, typename S::cs_t* __restrict__ pressure,
+                      int* __restrict__ status) {
+  using P = PdvPlane<S>;
+  using A = typename S::arith_t;
+  using V = typename S::vel_t;
+  using R = typename S::rho_t;
+  using En = typename S::ene_t;
+  using C = typename S::cs_t;
+  extern __shared__ __align__(128) unsigned char ring[];
+  __shared__ unsigned long long full[RING];
+  __shared__ int stop;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int j = g.x_min + TX * (int)blockIdx.x + tx, k0 = g.y_min + TY * (int)blockIdx.y;
+  const int k = k0 + ty;
+  const int l0 = g.z_min + seg * (int)blockIdx.z;
+  const int l1 = l0 + seg - 1 < g.z_max ? l0 + seg - 1 : g.z_max;
+  const bool in_jk = j <= g.x_max && k <= g.y_max;
+  const PlaneMarch<RING, 0, 1> pm{ring, P::kBytes, full, &stop, l0, l1 + 1};
+  const A dt = (A)dt_ptr[0];
+  constexpr int WV = kTmaWidth<V>, HV = kTmaHalo<V>, WR = kTmaWidth<R>, HR = kTmaHalo<R>;
+  constexpr int WE = kTmaWidth<En>, HE = kTmaHalo<En>, WC = kTmaWidth<C>, HC = kTmaHalo<C>;
+  auto issue = [&](int p) {
+    unsigned char* b = pm.buf(p);
+    unsigned long long* bar = pm.bar(p);
+    mbar_arrive_expect_tx(bar, P::kTx);
+    const int x = TX * (int)blockIdx.x, y = k0 - g.y_min + 2, z = p - g.z_min + 2;
+    tma_load_box(P::vel(b, 0), &maps.u, bar, x, y, z);
+    tma_load_box(P::vel(b, 1), &maps.v, bar, x, y, z);
+    tma_load_box(P::vel(b, 2), &maps.w, bar, x, y, z);
+    tma_load_box(P::rho(b), &maps.d, bar, x, y, z);
+    tma_load_box(P::ene(b), &maps.e, bar, x, y, z);
+    tma_load_box(P::cs(b, 0), &maps.p, bar, x, y, z);
+    tma_load_box(P::cs(b, 1), &maps.q, bar, x, y, z);
+  };
+  pm.run(l0, l1, status, issue, [&](int l) {
+    if (!in_jk) return;
+    unsigned char* bl = pm.buf(l);
+    unsigned char* bu = pm.buf(l + 1);
+    // velocity q of node (j+a, k+b) of a node plane buffer
+#define NV(bb, q, a, b) ((A)P::vel(bb, q)[(ty + (b)) * WV + tx + HV + (a)])
+#define XS(a) (NV(bl, 0, a, 0) + NV(bl, 0, a, 1) + NV(bu, 0, a, 0) + NV(bu, 0, a, 1))
+#define YS(b) (NV(bl, 1, 0, b) + NV(bl, 1, 1, b) + NV(bu, 1, 0, b) + NV(bu, 1, 1, b))
+#define ZS(bb) (NV(bb, 2, 0, 0) + NV(bb, 2, 1, 0) + NV(bb, 2, 0, 1) + NV(bb, 2, 1, 1))
+    // the predictor sums the same four node values twice (vel0 + vel0)
+    A sm;
+    sm = XS(0);
+    const A left_flux = ((A)g.xa * (sm + NV(bl, 0, 0, 0) + NV(bl, 0, 0, 1) + NV(bu, 0, 0, 0) +
+                                    NV(bu, 0, 0, 1))) * A(0.125) * dt * A(0.5);
+    sm = XS(1);
+    const A right_flux = ((A)g.xa * (sm + NV(bl, 0, 1, 0) + NV(bl, 0, 1, 1) + NV(bu, 0, 1, 0) +
+                                     NV(bu, 0, 1, 1))) * A(0.125) * dt * A(0.5);
+    sm = YS(0);
+    const A bottom_flux = ((A)g.ya * (sm + NV(bl, 1, 0, 0) + NV(bl, 1, 1, 0) + NV(bu, 1, 0, 0) +
+                                      NV(bu, 1, 1, 0))) * A(0.125) * dt * A(0.5);
+    sm = YS(1);
+    const A top_flux = ((A)g.ya * (sm + NV(bl, 1, 0, 1) + NV(bl, 1, 1, 1) + NV(bu, 1, 0, 1) +
+                                   NV(bu, 1, 1, 1))) * A(0.125) * dt * A(0.5);
+    sm = ZS(bl);
+    const A back_flux = ((A)g.za * (sm + NV(bl, 2, 0, 0) + NV(bl, 2, 1, 0) + NV(bl, 2, 0, 1) +
+                                    NV(bl, 2, 1, 1))) * A(0.125) * dt * A(0.5);
+    sm = ZS(bu);
+    const A front_flux = ((A)g.za * (sm + NV(bu, 2, 0, 0) + NV(bu, 2, 1, 0) + NV(bu, 2, 0, 1) +
+                                     NV(bu, 2, 1, 1))) * A(0.125) * dt * A(0.5);
+#undef ZS
+#undef YS
+#undef XS
+#undef NV
+    const A total_flux = right_flux - left_flux + top_flux - bottom_flux + front_flux - back_flux;
+    const A vol = (A)g.vol;
+    const A vol_change_s = vol / (vol + total_flux);
+    const A recip_volume = geo_rvol<A>(g);  // 1/volume
+    const A d0 = (A)P::rho(bl)[ty * WR + tx + HR];
+    const A energy_change = ((A)P::cs(bl, 0)[ty * WC + tx + HC] / d0 +
+                             (A)P::cs(bl, 1)[ty * WC + tx + HC] / d0) * total_flux * recip_volume;
+    // the predicted state goes through the storage types, as it would in memory
+    const A e1 = (A)st<En>(((A)P::ene(bl)[ty * WE + tx + HE] - energy_change));
+    const A d1 = (A)st<R>((d0 * vol_change_s));
+    pressure[off3(g, j, k, l)] = st<C>(((A(1.4) - A(1.0)) * d1 * e1));
+  });
+}
+
+// ---------------------------------------------------------------------------
+// accelerate_kernel.f90:61-109 on the uniform mesh, as k_accelerate
+// (clover_kernels.cu) forms it. Plane p: density0, pressure and viscosity of
+// cell plane p (rows k0-1..k0+7) and the three node velocities of node plane
+// p (rows k0..k0+7). Node l reads cell planes l-1, l and node plane l.
+template <class S>
+struct AccPlane {
+  using V = typename S::vel_t;
+  using R = typename S::rho_t;
+  using C = typename S::cs_t;
+  static constexpr int kRho = round128(9 * kTmaWidth<R> * (int)sizeof(R));
+  static constexpr int kCs = round128(9 * kTmaWidth<C> * (int)sizeof(C));
+  static constexpr int kVel = round128(8 * kTmaWidth<V> * (int)sizeof(V));
+  static constexpr int kBytes = kRho + 2 * kCs + 3 * kVel;
+  static constexpr unsigned kTx = box_bytes<R>(9) + 2 * box_bytes<C>(9) + 3 * box_bytes<V>(8);
+  __device__ static R* rho(unsigned char* p) { return (R*)p; }
+  __device__ static C* cs(unsigned char* p, int q) { return (C*)(p + kRho + q * kCs); }
+  __device__ static V* vel(unsigned char* p, int q) { return (V*)(p + kRho + 2 * kCs + q * kVel); }
+};
+
+template <class S, int RING, int MINB>
+__global__ void __launch_bounds__(TX * TY, MINB)
+k_accelerate_tma(Geom g, int seg, const double* __restrict__ dt_ptr,
+                 const __grid_constant__ AccMaps maps, typename S::vel_t* __restrict__ xvel1,
+                 typename S::vel_t* __restrict__ yvel1, typename S::vel_t* __restrict__ zvel1,
+                 int* __restrict__ status) {
+  using P = AccPlane<S>;
+  using A = typename S::arith_t;
+  using V = typename S::vel_t;
+  using R = typename S::rho_t;
+  using C = typename S::cs_t;
+  extern __shared__ __align__(128) unsigned char ring[];
+  __shared__ unsigned long long full[RING];
+  __shared__ int stop;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int j = g.x_min + TX * (int)blockIdx.x + tx, k0 = g.y_min + TY * (int)blockIdx.y;
+  const int k = k0 + ty;
+  const int l0 = g.z_min + seg * (int)blockIdx.z;
+  const int l1 = l0 + seg - 1 < g.z_max + 1 ? l0 + seg - 1 : g.z_max + 1;
+  const bool in_jk = j <= g.x_max + 1 && k <= g.y_max + 1;
+  const PlaneMarch<RING, 1, 0> pm{ring, P::kBytes, full, &stop, l0 - 1, l1};
+  const double dt = dt_ptr[0];
+  constexpr int WV = kTmaWidth<V>, HV = kTmaHalo<V>, WR = kTmaWidth<R>, HR = kTmaHalo<R>;
+  constexpr int WC = kTmaWidth<C>, HC = kTmaHalo<C>;
+  auto issue = [&](int p) {
+    unsigned char* b = pm.buf(p);
+    unsigned long long* bar = pm.bar(p);
+    mbar_arrive_expect_tx(bar, P::kTx);
+    const int x = TX * (int)blockIdx.x, y1 = k0 - g.y_min + 1, z = p - g.z_min + 2;
+    tma_load_box(P::rho(b), &maps.d, bar, x, y1, z);
+    tma_load_box(P::cs(b, 0), &maps.p, bar, x, y1, z);
+    tma_load_box(P::cs(b, 1), &maps.q, bar, x, y1, z);
+    tma_load_box(P::vel(b, 0), &maps.u, bar, x, y1 + 1, z);
+    tma_load_box(P::vel(b, 1), &maps.v, bar, x, y1 + 1, z);
+    tma_load_box(P::vel(b, 2), &maps.w, bar, x, y1 + 1, z);
+  };
+  pm.run(l0, l1, status, issue, [&](int l) {
+    if (!in_jk) return;
+    unsigned char* bl = pm.buf(l);
+    unsigned char* bd = pm.buf(l - 1);
+    // cell (j+a, k+b) of the cell plane buffer bb (a, b in {-1, 0})
+#define DC(bb, a, b) ((double)P::rho(bb)[(ty + 1 + (b)) * WR + tx + HR + (a)])
+#define DV(a, b, c) (DC((c) ? bd : bl, a, b) * g.vol)
+    const double nodal_mass = (DV(-1, -1, 0) + DV(0, -1, 0) + DV(0, 0, 0) + DV(-1, 0, 0) +
+                               DV(-1, -1, -1) + DV(0, -1, -1) + DV(0, 0, -1) + DV(-1, 0, -1)) * 0.125;
+#undef DV
+#undef DC
+    const double stepbymass_d = 0.25 * dt / nodal_mass;
+    const A stepbymass_s = (A)stepbymass_d;
+#define CS(bb, q, a, b) ((A)P::cs(bb, q)[(ty + 1 + (b)) * WC + tx + HC + (a)])
+    const A p000 = CS(bl, 0, 0, 0), p100 = CS(bl, 0, -1, 0);
+    const A p010 = CS(bl, 0, 0, -1), p110 = CS(bl, 0, -1, -1);
+    const A p001 = CS(bd, 0, 0, 0), p101 = CS(bd, 0, -1, 0);
+    const A p011 = CS(bd, 0, 0, -1), p111 = CS(bd, 0, -1, -1);
+    const A q000 = CS(bl, 1, 0, 0), q100 = CS(bl, 1, -1, 0);
+    const A q010 = CS(bl, 1, 0, -1), q110 = CS(bl, 1, -1, -1);
+    const A q001 = CS(bd, 1, 0, 0), q101 = CS(bd, 1, -1, 0);
+    const A q011 = CS(bd, 1, 0, -1), q111 = CS(bd, 1, -1, -1);
+#undef CS
+    const A xa0 = (A)g.xa, xa1 = (A)g.xa, xa2 = (A)g.xa, xa3 = (A)g.xa;
+    const A ya0 = (A)g.ya, ya1 = (A)g.ya, ya2 = (A)g.ya, ya3 = (A)g.ya;
+    const A za0 = (A)g.za, za1 = (A)g.za, za2 = (A)g.za, za3 = (A)g.za;
+    const int c = ty * WV + tx + HV;
+    const A xvel1_s = (A)P::vel(bl, 0)[c] -
+        stepbymass_s * (xa0 * (p000 - p100) + xa1 * (p010 - p110) + xa2 * (p001 - p101) +
+                        xa3 * (p011 - p111));
+    const A yvel1_s = (A)P::vel(bl, 1)[c] -
+        stepbymass_s * (ya0 * (p000 - p010) + ya1 * (p100 - p110) + ya2 * (p001 - p011) +
+                        ya3 * (p101 - p111));
+    const A zvel1_s = (A)P::vel(bl, 2)[c] -
+        stepbymass_s * (za0 * (p000 - p001) + za1 * (p010 - p011) + za2 * (p100 - p101) +
+                        za3 * (p110 - p111));
+    const long long o = off3(g, j, k, l);
+    xvel1[o] = st<V>(xvel1_s -
+        stepbymass_s * (xa0 * (q000 - q100) + xa1 * (q010 - q110) + xa2 * (q001 - q101) +
+                        xa3 * (q011 - q111)));
+    yvel1[o] = st<V>(yvel1_s -
+        stepbymass_s * (ya0 * (q000 - q010) + ya1 * (q100 - q110) + ya2 * (q001 - q011) +
+                        ya3 * (q101 - q111)));
+    zvel1[o] = st<V>(zvel1_s -
+        stepbymass_s * (za0 * (q000 - q001) + za1 * (q010 - q011) + za2 * (q100 - q101) +
+                        za3 * (q110 - q111)));
+  });
+}
+
+// ---------------------------------------------------------------------------
+// PdV_kernel.f90:120-166 (corrector) + flux_calc_kernel.f90:58-91 over the
+// node box [min, max+1]^3, as k_pdv_flux (clover_fused.cu) forms them. Plane p:
+// the time level 0 and 1 velocities of node plane p (rows k0..k0+8); the
+// cell's own density0, energy0, pressure and viscosity are read directly.
+template <class S>
+struct FluxPlane {
+  using V = typename S::vel_t;
+  static constexpr int kVel = round128(9 * kTmaWidth<V> * (int)sizeof(V));
+  static constexpr int kBytes = 6 * kVel;
+  static constexpr unsigned kTx = 6 * box_bytes<V>(9);
+  __device__ static V* vel(unsigned char* p, int q) { return (V*)(p + q * kVel); }
+};
+
+template <class S, int RING, int MINB>
+__global__ void __launch_bounds__(TX * TY, MINB)
+k_pdv_flux_tma(Geom g, int seg, const double* __restrict__ dt_ptr,
+               const __grid_constant__ FluxMaps maps, const typename S::rho_t* __restrict__ density0,
+               typename S::rho_t* __restrict__ density1, const typename S::ene_t* __restrict__ energy0,
+               typename S::ene_t* __restrict__ energy1, const typename S::cs_t* __restrict__ pressure,
+               const typename S::cs_t* __restrict__ viscosity, typename S::vf_t* __restrict__ vol_flux_x,
+               typename S::vf_t* __restrict__ vol_flux_y, typename S::vf_t* __restrict__ vol_flux_z,
+               int* __restrict__ status) {
+  using P = FluxPlane<S>;
+  using A = typename S::arith_t;
+  using V = typename S::vel_t;
+  using F = typename S::vf_t;
+  extern __shared__ __align__(128) unsigned char ring[];
+  __shared__ unsigned long long full[RING];
+  __shared__ int stop;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int j = g.x_min + TX * (int)blockIdx.x + tx, k0 = g.y_min + TY * (int)blockIdx.y;
+  const int k = k0 + ty;
+  const int l0 = g.z_min + seg * (int)blockIdx.z;
+  const int l1 = l0 + seg - 1 < g.z_max + 1 ? l0 + seg - 1 : g.z_max + 1;
+  const bool in_jk = j <= g.x_max + 1 && k <= g.y_max + 1;
+  const PlaneMarch<RING, 0, 1> pm{ring, P::kBytes, full, &stop, l0, l1 + 1};
+  const double dt = dt_ptr[0];
+  constexpr int WV = kTmaWidth<V>, HV = kTmaHalo<V>;
+  auto issue = [&](int p) {
+    unsigned char* b = pm.buf(p);
+    unsigned long long* bar = pm.bar(p);
+    mbar_arrive_expect_tx(bar, P::kTx);
+    const int x = TX * (int)blockIdx.x, y = k0 - g.y_min + 2, z = p - g.z_min + 2;
+    tma_load_box(P::vel(b, 0), &maps.u0, bar, x, y, z);
+    tma_load_box(P::vel(b, 1), &maps.v0, bar, x, y, z);
+    tma_load_box(P::vel(b, 2), &maps.w0, bar, x, y, z);
+    tma_load_box(P::vel(b, 3), &maps.u1, bar, x, y, z);
+    tma_load_box(P::vel(b, 4), &maps.v1, bar, x, y, z);
+    tma_load_box(P::vel(b, 5), &maps.w1, bar, x, y, z);
+  };
+  pm.run(l0, l1, status, issue, [&](int l) {
+    if (!in_jk) return;
+    const bool jin = j <= g.x_max, kin = k <= g.y_max, lin = l <= g.z_max;
+    unsigned char* bl = pm.buf(l);
+    unsigned char* bu = pm.buf(l + 1);
+    // velocity q (0-2 time level 0, 3-5 time level 1) of node (j+a, k+b) of buffer bb
+#define NV(bb, q, a, b) ((A)P::vel(bb, q)[(ty + (b)) * WV + tx + HV + (a)])
+    auto xsum = [&](int a) {
+      return (double)(NV(bl, 0, a, 0) + NV(bl, 0, a, 1) + NV(bu, 0, a, 0) + NV(bu, 0, a, 1) +
+                      NV(bl, 3, a, 0) + NV(bl, 3, a, 1) + NV(bu, 3, a, 0) + NV(bu, 3, a, 1));
+    };
+    auto ysum = [&](int b) {
+      return (double)(NV(bl, 1, 0, b) + NV(bl, 1, 1, b) + NV(bu, 1, 0, b) + NV(bu, 1, 1, b) +
+                      NV(bl, 4, 0, b) + NV(bl, 4, 1, b) + NV(bu, 4, 0, b) + NV(bu, 4, 1, b));
+    };
+    auto zsum = [&](unsigned char* bb) {
+      return (double)(NV(bb, 2, 0, 0) + NV(bb, 2, 1, 0) + NV(bb, 2, 0, 1) + NV(bb, 2, 1, 1) +
+                      NV(bb, 5, 0, 0) + NV(bb, 5, 1, 0) + NV(bb, 5, 0, 1) + NV(bb, 5, 1, 1));
+    };
+    const long long o = off3(g, j, k, l);
+    double sx = 0, sy = 0, sz = 0;
+    F vfx0 = F(0), vfy0 = F(0);
+    if (kin && lin) {
+      sx = xsum(0);
+      vfx0 = st<F>(0.125 * dt * g.xa * sx);
+      vol_flux_x[o] = vfx0;
+    }
+    if (jin && lin) {
+      sy = ysum(0);
+      vfy0 = st<F>(0.125 * dt * g.ya * sy);
+      vol_flux_y[o] = vfy0;
+    }
+    if (jin && kin) {
+      // flux_calc_kernel.f90:86 repeats zvel0(j+1,k,l) and omits zvel0(j,k+1,l)
+      const double bz = (double)(NV(bl, 2, 0, 0) + NV(bl, 2, 1, 0) + NV(bl, 2, 1, 0) +
+                                 NV(bl, 2, 1, 1) + NV(bl, 5, 0, 0) + NV(bl, 5, 1, 0) +
+                                 NV(bl, 5, 0, 1) + NV(bl, 5, 1, 1));
+      vol_flux_z[o] = st<F>(0.125 * dt * g.za * bz);
+      sz = zsum(bl);
+    }
+#undef NV
+    if (!(jin && kin && lin)) return;
+    double left_flux, right_flux, bottom_flux, top_flux, back_flux, front_flux;
+    if (sizeof(F) == 8) {  // PdV_kernel.f90:120-131 order
+      left_flux = (g.xa * sx) * 0.125 * dt;
+      right_flux = (g.xa * xsum(1)) * 0.125 * dt;
+      bottom_flux = (g.ya * sy) * 0.125 * dt;
+      top_flux = (g.ya * ysum(1)) * 0.125 * dt;
+      back_flux = (g.za * sz) * 0.125 * dt;
+      front_flux = (g.za * zsum(bu)) * 0.125 * dt;
+    } else {
+      // FP32 volume fluxes: the corrector's face fluxes as the volume fluxes
+      // are stored (the z faces from the corrector's own node sums)
+      auto stored = [&](double area, double s) { return (double)st<F>(0.125 * dt * area * s); };
+      left_flux = (double)vfx0;
+      right_flux = stored(g.xa, xsum(1));
+      bottom_flux = (double)vfy0;
+      top_flux = stored(g.ya, ysum(1));
+      back_flux = stored(g.za, sz);
+      front_flux = stored(g.za, zsum(bu));
+    }
+    const double total_flux = right_flux - left_flux + top_flux - bottom_flux + front_flux - back_flux;
+    const double vol = g.vol;
+    const double vol_change_s = vol / (vol + total_flux);
+    const double d0 = (double)__ldg(&density0[o]);
+    const A ad0 = (A)d0;
+    const A energy_change = ((A)__ldg(&pressure[o]) / ad0 + (A)__ldg(&viscosity[o]) / ad0) *
+                            (A)total_flux * geo_rvol<A>(g);
+    energy1[o] = st<typename S::ene_t>(((A)__ldg(&energy0[o]) - energy_change));
+    density1[o] = st<typename S::rho_t>(d0 * vol_change_s);
+  });
+}
+
 constexpr int kViscRing = 4;
 constexpr int kViscSeg = 32;
 
@@ -579,12 +969,76 @@ __global__ void k_wait_selftest(long long cycles, int* status) {
   if (!done && threadIdx.x == 0) atomicOr(status, CLOVER_STATUS_TIMEOUT);
 }
 
+constexpr int kStencilRing = 4, kStencilSeg = 32;
+// blocks per SM: FP64 holds three (56-72 registers, 60-69 KB of plane
+// buffers), the mixed forms four
+template <class S>
+constexpr int kStencilMinBlocks = sizeof(typename S::arith_t) == 4 ? 4 : 3;
+
+template <class S>
+bool stencils_tma_prepare() {
+  return cudaFuncSetAttribute(k_pdv_predict_eos_tma<S, kStencilRing, kStencilMinBlocks<S>>,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              kStencilRing * PdvPlane<S>::kBytes) == cudaSuccess &&
+         cudaFuncSetAttribute(k_accelerate_tma<S, kStencilRing, kStencilMinBlocks<S>>,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              kStencilRing * AccPlane<S>::kBytes) == cudaSuccess &&
+         cudaFuncSetAttribute(k_pdv_flux_tma<S, kStencilRing, kStencilMinBlocks<S>>,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              kStencilRing * FluxPlane<S>::kBytes) == cudaSuccess;
+}
+
+template <class S>
+void launch_pdv_predict_eos_tma(const Geom& g, cudaStream_t s, const double* dt_ptr,
+                                const PdvMaps& maps, typename S::cs_t* pressure, int* status) {
+  const dim3 grid((g.x_max - g.x_min + TX) / TX, (g.y_max - g.y_min + TY) / TY,
+                  (g.z_max - g.z_min + kStencilSeg) / kStencilSeg);
+  k_pdv_predict_eos_tma<S, kStencilRing, kStencilMinBlocks<S>>
+      <<<grid, dim3(TX, TY), kStencilRing * PdvPlane<S>::kBytes, s>>>(g, kStencilSeg, dt_ptr, maps,
+                                                                       pressure, status);
+}
+
+template <class S>
+void launch_accelerate_tma(const Geom& g, cudaStream_t s, const double* dt_ptr, const AccMaps& maps,
+                           typename S::vel_t* xvel1, typename S::vel_t* yvel1,
+                           typename S::vel_t* zvel1, int* status) {
+  const dim3 grid((g.x_max + 1 - g.x_min + TX) / TX, (g.y_max + 1 - g.y_min + TY) / TY,
+                  (g.z_max + 1 - g.z_min + kStencilSeg) / kStencilSeg);
+  k_accelerate_tma<S, kStencilRing, kStencilMinBlocks<S>>
+      <<<grid, dim3(TX, TY), kStencilRing * AccPlane<S>::kBytes, s>>>(g, kStencilSeg, dt_ptr, maps,
+                                                                      xvel1, yvel1, zvel1, status);
+}
+
+template <class S>
+void launch_pdv_flux_tma(const Geom& g, cudaStream_t s, const double* dt_ptr, const FluxMaps& maps,
+                         const typename S::rho_t* density0, typename S::rho_t* density1,
+                         const typename S::ene_t* energy0, typename S::ene_t* energy1,
+                         const typename S::cs_t* pressure, const typename S::cs_t* viscosity,
+                         typename S::vf_t* vol_flux_x, typename S::vf_t* vol_flux_y,
+                         typename S::vf_t* vol_flux_z, int* status) {
+  const dim3 grid((g.x_max + 1 - g.x_min + TX) / TX, (g.y_max + 1 - g.y_min + TY) / TY,
+                  (g.z_max + 1 - g.z_min + kStencilSeg) / kStencilSeg);
+  k_pdv_flux_tma<S, kStencilRing, kStencilMinBlocks<S>>
+      <<<grid, dim3(TX, TY), kStencilRing * FluxPlane<S>::kBytes, s>>>(
+          g, kStencilSeg, dt_ptr, maps, density0, density1, energy0, energy1, pressure, viscosity,
+          vol_flux_x, vol_flux_y, vol_flux_z, status);
+}
+
 #define INST_TMA(S)                                                                              \
   template bool visc_dt_tma_maps<S>(const Geom&, const S::vel_t*, const S::vel_t*,              \
                                     const S::vel_t*, const S::rho_t*, const S::ene_t*,          \
                                     ViscMaps*);                                                  \
   template bool visc_dt_tma_prepare<S>();                                                        \
   template bool mom_x_tma_prepare<S>();                                                          \
+  template bool stencils_tma_prepare<S>();                                                       \
+  template void launch_pdv_predict_eos_tma<S>(const Geom&, cudaStream_t, const double*,         \
+                                              const PdvMaps&, S::cs_t*, int*);                   \
+  template void launch_accelerate_tma<S>(const Geom&, cudaStream_t, const double*,               \
+                                         const AccMaps&, S::vel_t*, S::vel_t*, S::vel_t*, int*); \
+  template void launch_pdv_flux_tma<S>(const Geom&, cudaStream_t, const double*, const FluxMaps&, \
+                                       const S::rho_t*, S::rho_t*, const S::ene_t*, S::ene_t*,   \
+                                       const S::cs_t*, const S::cs_t*, S::vf_t*, S::vf_t*,       \
+                                       S::vf_t*, int*);                                          \
   template void launch_mom_x_tma<S>(const Geom&, cudaStream_t, int, int, const MomXMaps&,        \
                                     const GeomArrays&, S::vel_t* const*, const Level0<S>&, int*); \
   template void launch_visc_dt_tma<S>(const Geom&, cudaStream_t, const ViscMaps&, const GeomArrays&, \

@@ -59,6 +59,37 @@ void launch_mom_x_tma(const Geom& g, cudaStream_t s, int sweep, int seg, const M
                       const GeomArrays& ga, typename S::vel_t* const* vel_out,
                       const Level0<S>& level0, int* status);
 
+// The maps of the one-cell-per-thread stencils: the PdV predictor + EOS
+// (node velocities 9 rows, density0, energy0, pressure, viscosity 8 rows),
+// accelerate (density0, pressure, viscosity 9 rows from k0-1, node
+// velocities 8 rows) and the PdV corrector + flux_calc (time level 0 and 1
+// velocities, 9 rows).
+struct PdvMaps {
+  CUtensorMap u, v, w, d, e, p, q;
+};
+struct AccMaps {
+  CUtensorMap d, p, q, u, v, w;
+};
+struct FluxMaps {
+  CUtensorMap u0, v0, w0, u1, v1, w1;
+};
+template <class S>
+bool stencils_tma_prepare();
+template <class S>
+void launch_pdv_predict_eos_tma(const Geom& g, cudaStream_t s, const double* dt_ptr,
+                                const PdvMaps& maps, typename S::cs_t* pressure, int* status);
+template <class S>
+void launch_accelerate_tma(const Geom& g, cudaStream_t s, const double* dt_ptr, const AccMaps& maps,
+                           typename S::vel_t* xvel1, typename S::vel_t* yvel1,
+                           typename S::vel_t* zvel1, int* status);
+template <class S>
+void launch_pdv_flux_tma(const Geom& g, cudaStream_t s, const double* dt_ptr, const FluxMaps& maps,
+                         const typename S::rho_t* density0, typename S::rho_t* density1,
+                         const typename S::ene_t* energy0, typename S::ene_t* energy1,
+                         const typename S::cs_t* pressure, const typename S::cs_t* viscosity,
+                         typename S::vf_t* vol_flux_x, typename S::vf_t* vol_flux_y,
+                         typename S::vf_t* vol_flux_z, int* status);
+
 // The maps of a chunk's velocities (time level 0), density0 and energy0.
 template <class S>
 bool visc_dt_tma_maps(const Geom& g, const typename S::vel_t* xvel0, const typename S::vel_t* yvel0,
