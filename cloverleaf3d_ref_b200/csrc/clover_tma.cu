@@ -791,6 +791,25 @@ k_pdv_flux_tma(Geom g, int seg, const double* __restrict__ dt_ptr,
   const PlaneMarch<RING, 0, 1> pm{ring, P::kBytes, full, &stop, l0, l1 + 1};
   const double dt = dt_ptr[0];
   constexpr int WV = kTmaWidth<V>, HV = kTmaHalo<V>;
+  // the cell's own density0, energy0, pressure and viscosity, loaded one plane
+  // ahead (in flight across the block's barrier)
+  using R = typename S::rho_t;
+  using En = typename S::ene_t;
+  using Cs = typename S::cs_t;
+  const bool in_cell = j <= g.x_max && k <= g.y_max;
+  R c_d = R(0);
+  En c_e = En(0);
+  Cs c_p = Cs(0), c_q = Cs(0);
+  auto fetch = [&](int l) {
+    if (in_cell && l <= g.z_max) {
+      const long long o = off3(g, j, k, l);
+      c_d = __ldg(&density0[o]);
+      c_e = __ldg(&energy0[o]);
+      c_p = __ldg(&pressure[o]);
+      c_q = __ldg(&viscosity[o]);
+    }
+  };
+  fetch(l0);
   auto issue = [&](int p) {
     unsigned char* b = pm.buf(p);
     unsigned long long* bar = pm.bar(p);
@@ -805,6 +824,10 @@ k_pdv_flux_tma(Geom g, int seg, const double* __restrict__ dt_ptr,
   };
   pm.run(l0, l1, status, issue, [&](int l) {
     if (!in_jk) return;
+    const R d0_s = c_d;
+    const En e0_s = c_e;
+    const Cs p_s = c_p, q_s = c_q;
+    fetch(l + 1);
     const bool jin = j <= g.x_max, kin = k <= g.y_max, lin = l <= g.z_max;
     unsigned char* bl = pm.buf(l);
     unsigned char* bu = pm.buf(l + 1);
@@ -867,11 +890,10 @@ k_pdv_flux_tma(Geom g, int seg, const double* __restrict__ dt_ptr,
     const double total_flux = right_flux - left_flux + top_flux - bottom_flux + front_flux - back_flux;
     const double vol = g.vol;
     const double vol_change_s = vol / (vol + total_flux);
-    const double d0 = (double)__ldg(&density0[o]);
+    const double d0 = (double)d0_s;
     const A ad0 = (A)d0;
-    const A energy_change = ((A)__ldg(&pressure[o]) / ad0 + (A)__ldg(&viscosity[o]) / ad0) *
-                            (A)total_flux * geo_rvol<A>(g);
-    energy1[o] = st<typename S::ene_t>(((A)__ldg(&energy0[o]) - energy_change));
+    const A energy_change = ((A)p_s / ad0 + (A)q_s / ad0) * (A)total_flux * geo_rvol<A>(g);
+    energy1[o] = st<typename S::ene_t>(((A)e0_s - energy_change));
     density1[o] = st<typename S::rho_t>(d0 * vol_change_s);
   });
 }
