@@ -83,26 +83,6 @@ __host__ __device__ inline Box nodes(const Geom& g) {
   return Box{g.x_min, g.x_max + 1, g.y_min, g.y_max + 1, g.z_min, g.z_max + 1};
 }
 
-// A marching kernel's threads cover j in [jlo, jhi] and the cross axis c in
-// [clo, chi] and walk the sweep axis p over [plo, phi] (cell sweeps: faces
-// from the sweep axis minimum to its maximum+2, cells updated for c <= cmax).
-struct MarchRange {
-  int jlo, jhi, clo, chi, plo, phi, cmax;
-};
-// advec_mom y/z node pass: node fluxes from min-2 to max+2 along the sweep
-template <int DIR>
-__host__ __device__ inline MarchRange mom_node_range(const Geom& g) {
-  const int pmin = DIR == 2 ? g.y_min : g.z_min, pmax = DIR == 2 ? g.y_max : g.z_max;
-  const int cmin = DIR == 2 ? g.z_min : g.y_min, cmx = DIR == 2 ? g.z_max : g.y_max;
-  return MarchRange{g.x_min, g.x_max + 1, cmin, cmx + 1, pmin - 2, pmax + 2, cmx + 1};
-}
-// advec_mom y/z velocity pass: nodes min..max+1 along the sweep
-template <int DIR>
-__host__ __device__ inline MarchRange mom_vel_range(const Geom& g) {
-  const int pmin = DIR == 2 ? g.y_min : g.z_min, pmax = DIR == 2 ? g.y_max : g.z_max;
-  const int cmin = DIR == 2 ? g.z_min : g.y_min, cmx = DIR == 2 ? g.z_max : g.y_max;
-  return MarchRange{g.x_min, g.x_max + 1, cmin, cmx + 1, pmin, pmax + 1, cmx + 1};
-}
 // advec_cell y sweep: columns l in [z_min, z_max+2] (the reference's y face
 // range), cells updated for l <= z_max; z sweep: rows k in [y_min, y_max]
 template <int DIR>
@@ -1330,7 +1310,8 @@ void launch_advec_mom_fused(const Target& tg, cudaStream_t s, int advect_x, int 
                             typename S::wk_t* node_flux, typename S::wk_t* node_mass_post,
                             typename S::wk_t* node_mass_pre, typename S::vel_t* const* vel_in,
                             typename S::vel_t* const* vel_out, bool copy_shell,
-                            const Level0<S>& level0, const MomXMaps* x_maps, int* status) {
+                            const Level0<S>& level0, const MomXMaps* x_maps, int* status,
+                            const NodeMaps* node_maps) {
   // the node arrays of the y/z sweeps live in three work arrays, as nd_t
   using ND = typename S::nd_t;
   static_assert(sizeof(ND) <= sizeof(typename S::wk_t), "node arrays fit the work arrays");
@@ -1343,10 +1324,13 @@ void launch_advec_mom_fused(const Target& tg, cudaStream_t s, int advect_x, int 
   auto node_vel = [&](auto dir_c, auto var) {
     constexpr int D = decltype(dir_c)::value, V = decltype(var)::value;
     // node pass then velocity pass, each marching along the sweep axis in segments
-    launch_mapped(tg, s, kKeyMomNode | D | (V << 4), grid_mom_node<D>, kMarchSeg, true, kBlk,
-                  k_mom_node_march<S, D, V, MapSingle>, k_mom_node_march<S, D, V, MapBatchFree>, ga,
-                  D == 2 ? mass_flux_y : mass_flux_z, density1, vol_flux_x, vol_flux_y,
-                  vol_flux_z, nd_flux, nd_post, nd_pre);
+    if (node_maps && !tg.plan)
+      launch_mom_node_tma<S>(tg.g, s, D, V, *node_maps, nd_flux, nd_post, nd_pre, status);
+    else
+      launch_mapped(tg, s, kKeyMomNode | D | (V << 4), grid_mom_node<D>, kMarchSeg, true, kBlk,
+                    k_mom_node_march<S, D, V, MapSingle>, k_mom_node_march<S, D, V, MapBatchFree>,
+                    ga, D == 2 ? mass_flux_y : mass_flux_z, density1, vol_flux_x, vol_flux_y,
+                    vol_flux_z, nd_flux, nd_post, nd_pre);
     launch_mapped2(tg, s, kKeyMomVel3 | D, grid_mom_vel<D>, grid_mom_vel_flat<D>, kMarchSeg,
                    true, kBlk, k_mom_vel3_march<S, D, MapSingle>, k_mom_vel3_march<S, D, MapBatchFree>,
                    ga, nd_flux, nd_post, nd_pre, vel_in[0], vel_in[1], vel_in[2], vel_out[0],
@@ -1416,7 +1400,8 @@ void launch_advec_mom_fused(const Target& tg, cudaStream_t s, int advect_x, int 
                                           const S::mf_t*, const S::mf_t*, const S::vf_t*,      \
                                           const S::vf_t*, const S::vf_t*, S::wk_t*, S::wk_t*,  \
                                           S::wk_t*, S::vel_t* const*, S::vel_t* const*, bool,  \
-                                          const Level0<S>&, const MomXMaps*, int*);
+                                          const Level0<S>&, const MomXMaps*, int*,            \
+                                          const NodeMaps*);
 
 INSTF(F64)
 INSTF(F32Mixed)

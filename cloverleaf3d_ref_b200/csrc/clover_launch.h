@@ -387,7 +387,10 @@ void launch_advec_cell_x(const Target& tg, cudaStream_t s, int sweep, const Geom
 // x_maps (one chunk, x sweep): the tensor maps of the sweep's inputs, to run
 // its shared-memory staged form (clover_tma.cu), which reports a copy that
 // did not arrive in *status; null: the register-marching form.
+// node_maps (one chunk, y/z sweep): the maps of the node pass's inputs, to run
+// its staged form.
 struct MomXMaps;
+struct NodeMaps;
 template <class S>
 void launch_advec_mom_fused(const Target& tg, cudaStream_t s, int advect_x, int sweep, int dir,
                             double vol, const GeomArrays& ga, const typename S::rho_t* density1,
@@ -398,7 +401,7 @@ void launch_advec_mom_fused(const Target& tg, cudaStream_t s, int advect_x, int 
                             typename S::wk_t* node_mass_pre, typename S::vel_t* const* vel_in,
                             typename S::vel_t* const* vel_out, bool copy_shell,
                             const Level0<S>& level0, const MomXMaps* x_maps = nullptr,
-                            int* status = nullptr);
+                            int* status = nullptr, const NodeMaps* node_maps = nullptr);
 
 // Fill every element of an array (size elems after the pad) with a value.
 template <class T>

@@ -158,15 +158,15 @@ struct Chunk : ChunkBase {
   bool tma = false;
   bool use_tma = true;
   ViscMaps visc_maps;
-  // tensor maps of the arrays the staged x momentum sweep reads, by (array,
-  // box rows): both buffers of the density1 and velocity pairs occur
+  // tensor maps of the arrays the staged kernels read, by (array, box rows
+  // and orientation): both buffers of the density1 and velocity pairs occur
   std::map<std::pair<const void*, int>, CUtensorMap> tmaps;
-  bool tmap(const void* base, int elem_bytes, int rows, CUtensorMap* out) {
-    const auto key = std::make_pair(base, rows);
+  bool tmap(const void* base, int elem_bytes, int rows, CUtensorMap* out, bool zrows = false) {
+    const auto key = std::make_pair(base, 2 * rows + (zrows ? 1 : 0));
     auto it = tmaps.find(key);
     if (it == tmaps.end()) {
       CUtensorMap m;
-      if (!encode_plane_map(&m, base, elem_bytes, g, rows)) return false;
+      if (!encode_plane_map(&m, base, elem_bytes, g, rows, zrows)) return false;
       it = tmaps.emplace(key, m).first;
     }
     *out = it->second;
@@ -174,6 +174,18 @@ struct Chunk : ChunkBase {
   }
   // the maps of the x momentum sweep reading density1 buffer rho and the
   // velocity buffers vin
+  // the maps of the y (dir 2) or z (dir 3) node pass reading density1 buffer
+  // rho, with the post-volume variant of the sweep
+  bool mom_node_maps(int dir, int var, const R* rho, NodeMaps* m) {
+    const bool zr = dir == 2;  // the y sweep's planes are x-z slices
+    bool ok = tmap(dir == 2 ? (const void*)mass_flux_y : (const void*)mass_flux_z, sizeof(MF), 9,
+                   &m->mf, zr) &&
+              tmap(rho, sizeof(R), 9, &m->d, zr);
+    if (ok && (var == 1 || var == 3)) ok = tmap(vol_flux_x, sizeof(VF), 9, &m->vfx, zr);
+    if (ok && var == 1) ok = tmap(vol_flux_y, sizeof(VF), 10, &m->vfr, false);
+    if (ok && var == 2) ok = tmap(vol_flux_z, sizeof(VF), 10, &m->vfr, true);
+    return ok;
+  }
   bool mom_x_maps(const R* rho, V* const* vin, MomXMaps* m) {
     return tmap(mass_flux_x, sizeof(MF), 9, &m->mf) && tmap(rho, sizeof(R), 9, &m->d) &&
            tmap(vol_flux_y, sizeof(VF), 10, &m->vfy) && tmap(vol_flux_z, sizeof(VF), 9, &m->vfz) &&
@@ -369,6 +381,7 @@ struct Chunk : ChunkBase {
     // get their tensor maps (the arrays they read never move)
     if (!batched)
       tma = visc_dt_tma_prepare<S>() && mom_x_tma_prepare<S>() && stencils_tma_prepare<S>() &&
+            mom_node_tma_prepare<S>() &&
             visc_dt_tma_maps<S>(g, xvel0, yvel0, zvel0, density0, energy0, &visc_maps);
 
     dt_cap = deck.end_step < (1 << 22) ? deck.end_step + 16 : (1 << 22);
@@ -877,12 +890,16 @@ struct Chunk : ChunkBase {
       // the velocities' shell before anything reads it; after sweep 3 the
       // shell carries the step's final halo values
       MomXMaps xm;
+      NodeMaps nm;
       const bool x_tma = dir == 1 && tma && use_tma && mom_x_maps(rho1(cb), vin, &xm);
+      const int node_var = dir == 2 ? (axi ? 2 : 3) : (sweep_number == 1 ? 1 : 4);
+      const bool node_tma =
+          dir != 1 && tma && use_tma && mom_node_maps(dir, node_var, rho1(cb), &nm);
       launch_advec_mom_fused<S>(tg, stream, axi, sweep_number, dir, cell_volume, ga, rho1(cb),
                                 mass_flux_x, mass_flux_y, mass_flux_z, vol_flux_x, vol_flux_y,
                                 vol_flux_z, work[0], work[1], work[2], vin, vout,
                                 sweep_number == 3 || !halo_repeat_free, l0,
-                                x_tma ? &xm : nullptr, &sc->status);
+                                x_tma ? &xm : nullptr, &sc->status, node_tma ? &nm : nullptr);
       // x: one pass; y, z: node pass + velocity pass
       if (dir == 1)
         pend("advec_mom_x", n * (MF8 + R8 + npv * VF8 + (6 + 3 * nl0) * V8));

@@ -12,6 +12,26 @@
 
 namespace clover {
 
+// A marching kernel's threads cover j in [jlo, jhi] and the cross axis c in
+// [clo, chi] and walk the sweep axis p over [plo, phi] (cell sweeps: faces
+// from the sweep axis minimum to its maximum+2, cells updated for c <= cmax).
+struct MarchRange {
+  int jlo, jhi, clo, chi, plo, phi, cmax;
+};
+// advec_mom y/z node pass: node fluxes from min-2 to max+2 along the sweep
+template <int DIR>
+__host__ __device__ inline MarchRange mom_node_range(const Geom& g) {
+  const int pmin = DIR == 2 ? g.y_min : g.z_min, pmax = DIR == 2 ? g.y_max : g.z_max;
+  const int cmin = DIR == 2 ? g.z_min : g.y_min, cmx = DIR == 2 ? g.z_max : g.y_max;
+  return MarchRange{g.x_min, g.x_max + 1, cmin, cmx + 1, pmin - 2, pmax + 2, cmx + 1};
+}
+// advec_mom y/z velocity pass: nodes min..max+1 along the sweep
+template <int DIR>
+__host__ __device__ inline MarchRange mom_vel_range(const Geom& g) {
+  const int pmin = DIR == 2 ? g.y_min : g.z_min, pmax = DIR == 2 ? g.y_max : g.z_max;
+  const int cmin = DIR == 2 ? g.z_min : g.y_min, cmx = DIR == 2 ? g.z_max : g.y_max;
+  return MarchRange{g.x_min, g.x_max + 1, cmin, cmx + 1, pmin, pmax + 1, cmx + 1};
+}
 // a value in storage type T, converted once from the arithmetic it was
 // formed in (no detour through double for an FP32 value stored as FP32)
 template <class T, class U>

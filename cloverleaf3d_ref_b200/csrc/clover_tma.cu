@@ -25,7 +25,7 @@
 namespace clover {
 
 bool encode_plane_map(CUtensorMap* map, const void* base, int elem_bytes, const Geom& g,
-                      int box_rows) {
+                      int box_rows, bool rows_along_z) {
   static PFN_cuTensorMapEncodeTiled encode = nullptr;
   if (!encode) {
     void* fn = nullptr;
@@ -45,7 +45,10 @@ bool encode_plane_map(CUtensorMap* map, const void* base, int elem_bytes, const 
   const cuuint64_t dims[3] = {(cuuint64_t)g.px, (cuuint64_t)(g.pxy / g.px),
                               (cuuint64_t)(g.z_max - g.z_min + 6)};
   const cuuint64_t strides[2] = {(cuuint64_t)g.px * elem_bytes, (cuuint64_t)g.pxy * elem_bytes};
-  const cuuint32_t box[3] = {(cuuint32_t)(32 + 2 * halo), (cuuint32_t)box_rows, 1};
+  // a box is one plane of box_rows rows: rows along y (x-y planes), or along
+  // z (x-z slices, for sweeps that march along y)
+  const cuuint32_t box[3] = {(cuuint32_t)(32 + 2 * halo), rows_along_z ? 1u : (cuuint32_t)box_rows,
+                             rows_along_z ? (cuuint32_t)box_rows : 1u};
   const cuuint32_t estr[3] = {1, 1, 1};
   const CUresult r =
       encode(map, elem_bytes == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
@@ -898,6 +901,157 @@ k_pdv_flux_tma(Geom g, int seg, const double* __restrict__ dt_ptr,
   });
 }
 
+// ---------------------------------------------------------------------------
+// The node pass of the y or z momentum sweep (advec_mom_kernel.f90:254-293 for
+// y, :339-379 for z), as k_mom_node_march (clover_fused.cu) forms it, with the
+// inputs staged in shared memory. The lane layout stays: lane L of a warp holds
+// column j = x_min-1+31t+L, the values at column j-1 come from lane L-1 (lane 0
+// only serves lane 1), rows c = c0..c0+7 are the warps; the sweep axis p is
+// marched. Plane p holds the sweep direction's mass flux and density1 of rows
+// c0-1..c0+7 and the volume fluxes of the post volume (variant 1: vol_flux_x
+// and vol_flux_y; 2: vol_flux_z; 3: vol_flux_x; 4: none), rows along y for
+// the z sweep (p = l, c = k) and along z for the y sweep (p = k, c = l). Node p
+// reads planes p-1 (node flux p-1, the cell products below), p and p+1.
+template <class S, int VAR>
+struct NodePlane {
+  using MF = typename S::mf_t;
+  using R = typename S::rho_t;
+  using VF = typename S::vf_t;
+  static constexpr bool kX = VAR == 1 || VAR == 3;  // vol_flux_x, columns j, j+1
+  static constexpr bool kR = VAR == 1 || VAR == 2;  // the row-direction volume flux, rows c, c+1
+  static constexpr int kMf = round128(9 * kTmaWidth<MF> * (int)sizeof(MF));
+  static constexpr int kRho = round128(9 * kTmaWidth<R> * (int)sizeof(R));
+  static constexpr int kVfx = kX ? round128(9 * kTmaWidth<VF> * (int)sizeof(VF)) : 0;
+  static constexpr int kVfr = kR ? round128(10 * kTmaWidth<VF> * (int)sizeof(VF)) : 0;
+  static constexpr int kBytes = kMf + kRho + kVfx + kVfr;
+  static constexpr unsigned kTx = box_bytes<MF>(9) + box_bytes<R>(9) +
+                                  (kX ? box_bytes<VF>(9) : 0u) + (kR ? box_bytes<VF>(10) : 0u);
+  __device__ static MF* mf(unsigned char* p) { return (MF*)p; }
+  __device__ static R* rho(unsigned char* p) { return (R*)(p + kMf); }
+  __device__ static VF* vfx(unsigned char* p) { return (VF*)(p + kMf + kRho); }
+  __device__ static VF* vfr(unsigned char* p) { return (VF*)(p + kMf + kRho + kVfx); }
+};
+
+// Box x coordinate of element type T for a block whose first column is
+// x_min-1+31t, and the column of that node in the box.
+template <class T>
+__device__ __forceinline__ void x_box31(int t, int& x, int& shift) {
+  constexpr int H = kTmaHalo<T>;
+  const int c = 31 * t + H - 1;  // the first column, counted from the map's base
+  x = c / H * H;
+  shift = c - x;
+}
+
+template <class S, int DIR, int VAR, int RING, int MINB>
+__global__ void __launch_bounds__(TX * TY, MINB)
+k_mom_node_tma(Geom g, int seg, const __grid_constant__ NodeMaps maps,
+               typename S::nd_t* __restrict__ node_flux, typename S::nd_t* __restrict__ node_mass_post,
+               typename S::nd_t* __restrict__ node_mass_pre, int* __restrict__ status) {
+  using P = NodePlane<S, VAR>;
+  using MF = typename S::mf_t;
+  using R = typename S::rho_t;
+  using VF = typename S::vf_t;
+  using W = typename S::nd_t;
+  extern __shared__ __align__(128) unsigned char ring[];
+  __shared__ unsigned long long full[RING];
+  __shared__ int stop;
+  const unsigned fullmask = 0xffffffffu;
+  const MarchRange r = mom_node_range<DIR>(g);
+  const int lane = threadIdx.x, ty = threadIdx.y;
+  const int j = r.jlo - 1 + 31 * (int)blockIdx.x + lane;
+  const int c0 = r.clo + TY * (int)blockIdx.y, c = c0 + ty;
+  const bool row = c <= r.chi;      // the whole warp: c depends on the row only
+  const bool lds = row && j <= r.jhi;
+  const bool own = lds && lane >= 1;
+  const int p0 = r.plo + seg * (int)blockIdx.z;
+  const int p1 = p0 + seg - 1 < r.phi ? p0 + seg - 1 : r.phi;
+  const PlaneMarch<RING, 1, 1> pm{ring, P::kBytes, full, &stop, p0 - 1, p1 + 1};
+  int xm, cm, xr, cr, xf, cf;
+  x_box31<MF>(blockIdx.x, xm, cm);
+  x_box31<R>(blockIdx.x, xr, cr);
+  x_box31<VF>(blockIdx.x, xf, cf);
+  cm += lane; cr += lane; cf += lane;
+  constexpr int WM = kTmaWidth<MF>, WR = kTmaWidth<R>, WF = kTmaWidth<VF>;
+  auto issue = [&](int p) {
+    unsigned char* b = pm.buf(p);
+    unsigned long long* bar = pm.bar(p);
+    mbar_arrive_expect_tx(bar, P::kTx);
+    // rows from c0-1: along y (z sweep) or along z (y sweep)
+    const int y = DIR == 3 ? c0 - 1 - g.y_min + 2 : p - g.y_min + 2;
+    const int z = DIR == 3 ? p - g.z_min + 2 : c0 - 1 - g.z_min + 2;
+    tma_load_box(P::mf(b), &maps.mf, bar, xm, y, z);
+    tma_load_box(P::rho(b), &maps.d, bar, xr, y, z);
+    if (P::kX) tma_load_box(P::vfx(b), &maps.vfx, bar, xf, y, z);
+    if (P::kR) tma_load_box(P::vfr(b), &maps.vfr, bar, xf, y, z);
+  };
+  auto up = [&](double v) { return __shfl_up_sync(fullmask, v, 1); };
+  // mass fluxes of plane b at (j, c) and (j, c-1), and of column j-1
+  struct Mf { double a, b, am, bm; };
+  auto mfs = [&](unsigned char* b) {
+    Mf f{0.0, 0.0, 0.0, 0.0};
+    if (lds) {
+      f.a = (double)P::mf(b)[(ty + 1) * WM + cm];
+      f.b = (double)P::mf(b)[ty * WM + cm];
+    }
+    f.am = up(f.a);
+    f.bm = up(f.b);
+    return f;
+  };
+  // the node-flux sum of the reference from the mass fluxes of two planes
+  auto nflux = [](const Mf& lo, const Mf& hi) {
+    return 0.125 * (lo.am + lo.a + hi.am + hi.a + lo.bm + lo.b + hi.bm + hi.b);
+  };
+  // cell product density1 * post_vol of cell (j, box row rr) of plane b
+  auto prod = [&](unsigned char* b, int rr) {
+    const double d = (double)P::rho(b)[rr * WR + cr];
+    double pv = g.vol;
+    if (VAR == 1)
+      pv = pv + (double)P::vfx(b)[rr * WF + cf + 1] - (double)P::vfx(b)[rr * WF + cf] +
+           (double)P::vfr(b)[(rr + 1) * WF + cf] - (double)P::vfr(b)[rr * WF + cf];
+    else if (VAR == 2)
+      pv = pv + (double)P::vfr(b)[(rr + 1) * WF + cf] - (double)P::vfr(b)[rr * WF + cf];
+    else if (VAR == 3)
+      pv = pv + (double)P::vfx(b)[rr * WF + cf + 1] - (double)P::vfx(b)[rr * WF + cf];
+    return d * pv;
+  };
+  // the four products of the node's plane-b cells in the order the node-mass
+  // sum takes them (a, b: this column; c, d: column j-1)
+  struct Pq { double a, b, c, d; };
+  auto prods = [&](unsigned char* b) {
+    Pq u;
+    double x0 = 0.0, x1 = 0.0;
+    if (DIR == 3) {  // plane l: P(j,k-1,l), P(j,k,l), P(j-1,k-1,l), P(j-1,k,l)
+      if (lds) { x0 = prod(b, ty); x1 = prod(b, ty + 1); }
+      u.a = x0; u.b = x1; u.c = up(x0); u.d = up(x1);
+    } else {  // plane k: P(j,k,l), P(j-1,k,l), P(j,k,l-1), P(j-1,k,l-1)
+      if (lds) { x0 = prod(b, ty + 1); x1 = prod(b, ty); }
+      u.a = x0; u.b = up(x0); u.c = x1; u.d = up(x1);
+    }
+    return u;
+  };
+  pm.run(p0, p1, status, issue, [&](int p) {
+    if (!row) return;
+    unsigned char* bm = pm.buf(p - 1);
+    unsigned char* b0 = pm.buf(p);
+    unsigned char* b1 = pm.buf(p + 1);
+    const Mf fm = mfs(bm), f0 = mfs(b0), f1 = mfs(b1);
+    const double nf_prev = nflux(fm, f0);
+    const double nf = nflux(f0, f1);
+    const long long o = DIR == 3 ? off3(g, j, c, p) : off3(g, j, p, c);
+    if (own) node_flux[o] = st<W>(nf);
+    const Pq q = prods(bm), u = prods(b0);
+    double nmp;
+    if (DIR == 3)
+      nmp = node_mass_sum(u.a, u.b, u.c, u.d, q.a, q.b, q.c, q.d);
+    else  // P(j,k-1,l) P(j,k,l) P(j-1,k-1,l) P(j-1,k,l) P(j,k-1,l-1) P(j,k,l-1) P(j-1,k-1,l-1) P(j-1,k,l-1)
+      nmp = node_mass_sum(q.a, u.a, q.b, u.b, q.c, u.c, q.d, u.d);
+    if (own && p >= r.plo + 1) {  // node masses run from one node after the flux range start
+      node_mass_post[o] = st<W>(nmp);
+      node_mass_pre[o] = st<W>(nmp - nf_prev + nf);
+    }
+  });
+}
+
 constexpr int kViscRing = 4;
 constexpr int kViscSeg = 32;
 
@@ -1046,6 +1200,44 @@ void launch_pdv_flux_tma(const Geom& g, cudaStream_t s, const double* dt_ptr, co
           vol_flux_x, vol_flux_y, vol_flux_z, status);
 }
 
+template <class S>
+constexpr int kNodeMinBlocks = sizeof(typename S::arith_t) == 4 ? 5 : 5;
+
+template <class S>
+bool mom_node_tma_prepare() {
+  bool ok = true;
+  auto set = [&](auto kern, int bytes) {
+    ok = ok && cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    kStencilRing * bytes) == cudaSuccess;
+  };
+  set(k_mom_node_tma<S, 3, 1, kStencilRing, kNodeMinBlocks<S>>, NodePlane<S, 1>::kBytes);
+  set(k_mom_node_tma<S, 3, 4, kStencilRing, kNodeMinBlocks<S>>, NodePlane<S, 4>::kBytes);
+  set(k_mom_node_tma<S, 2, 2, kStencilRing, kNodeMinBlocks<S>>, NodePlane<S, 2>::kBytes);
+  set(k_mom_node_tma<S, 2, 3, kStencilRing, kNodeMinBlocks<S>>, NodePlane<S, 3>::kBytes);
+  return ok;
+}
+
+template <class S>
+void launch_mom_node_tma(const Geom& g, cudaStream_t s, int dir, int var, const NodeMaps& maps,
+                         typename S::nd_t* node_flux, typename S::nd_t* node_mass_post,
+                         typename S::nd_t* node_mass_pre, int* status) {
+  auto go = [&](auto kern, int bytes, const MarchRange& r) {
+    const dim3 grid((r.jhi - r.jlo + 1 + 30) / 31, (r.chi - r.clo + 1 + TY - 1) / TY,
+                    (r.phi - r.plo + 1 + kStencilSeg - 1) / kStencilSeg);
+    kern<<<grid, dim3(TX, TY), kStencilRing * bytes, s>>>(g, kStencilSeg, maps, node_flux,
+                                                          node_mass_post, node_mass_pre, status);
+  };
+  if (dir == 3) {
+    const MarchRange r = mom_node_range<3>(g);
+    if (var == 1) go(k_mom_node_tma<S, 3, 1, kStencilRing, kNodeMinBlocks<S>>, NodePlane<S, 1>::kBytes, r);
+    else go(k_mom_node_tma<S, 3, 4, kStencilRing, kNodeMinBlocks<S>>, NodePlane<S, 4>::kBytes, r);
+  } else {
+    const MarchRange r = mom_node_range<2>(g);
+    if (var == 2) go(k_mom_node_tma<S, 2, 2, kStencilRing, kNodeMinBlocks<S>>, NodePlane<S, 2>::kBytes, r);
+    else go(k_mom_node_tma<S, 2, 3, kStencilRing, kNodeMinBlocks<S>>, NodePlane<S, 3>::kBytes, r);
+  }
+}
+
 #define INST_TMA(S)                                                                              \
   template bool visc_dt_tma_maps<S>(const Geom&, const S::vel_t*, const S::vel_t*,              \
                                     const S::vel_t*, const S::rho_t*, const S::ene_t*,          \
@@ -1053,6 +1245,9 @@ void launch_pdv_flux_tma(const Geom& g, cudaStream_t s, const double* dt_ptr, co
   template bool visc_dt_tma_prepare<S>();                                                        \
   template bool mom_x_tma_prepare<S>();                                                          \
   template bool stencils_tma_prepare<S>();                                                       \
+  template bool mom_node_tma_prepare<S>();                                                       \
+  template void launch_mom_node_tma<S>(const Geom&, cudaStream_t, int, int, const NodeMaps&,     \
+                                       S::nd_t*, S::nd_t*, S::nd_t*, int*);                      \
   template void launch_pdv_predict_eos_tma<S>(const Geom&, cudaStream_t, const double*,         \
                                               const PdvMaps&, S::cs_t*, int*);                   \
   template void launch_accelerate_tma<S>(const Geom&, cudaStream_t, const double*,               \

@@ -35,9 +35,10 @@ constexpr int kTmaWidth = 32 + 2 * kTmaHalo<T>;
 
 // Encode the map of one chunk-layout array (base: its element
 // (x_min-2, y_min-2, z_min-2), the pointer every kernel indexes with off3)
-// with boxes of kTmaWidth<T> x box_rows x 1. False if the driver refuses it.
+// with boxes of kTmaWidth<T> x box_rows x 1 (x-y planes), or kTmaWidth<T> x 1
+// x box_rows (x-z slices) with rows_along_z. False if the driver refuses it.
 bool encode_plane_map(CUtensorMap* map, const void* base, int elem_bytes, const Geom& g,
-                      int box_rows);
+                      int box_rows, bool rows_along_z = false);
 
 // The tensor maps of the arrays the viscosity/calc_dt stencil reads.
 struct ViscMaps {
@@ -89,6 +90,23 @@ void launch_pdv_flux_tma(const Geom& g, cudaStream_t s, const double* dt_ptr, co
                          const typename S::cs_t* pressure, const typename S::cs_t* viscosity,
                          typename S::vf_t* vol_flux_x, typename S::vf_t* vol_flux_y,
                          typename S::vf_t* vol_flux_z, int* status);
+
+// The maps of the y/z momentum node pass: mass flux of the sweep direction
+// and density1 (9 rows from c0-1), and the volume fluxes its post volumes
+// take (vol_flux_x 9 rows, the row-direction flux 10 rows: vol_flux_y for
+// the z sweep's variant 1, vol_flux_z for the y sweep's variant 2). Rows run
+// along y for the z sweep and along z for the y sweep.
+struct NodeMaps {
+  CUtensorMap mf, d, vfx, vfr;
+};
+template <class S>
+bool mom_node_tma_prepare();
+// The node pass of the y (dir 2) or z (dir 3) momentum sweep with post-volume
+// variant var, planes staged by bulk-tensor copies.
+template <class S>
+void launch_mom_node_tma(const Geom& g, cudaStream_t s, int dir, int var, const NodeMaps& maps,
+                         typename S::nd_t* node_flux, typename S::nd_t* node_mass_post,
+                         typename S::nd_t* node_mass_pre, int* status);
 
 // The maps of a chunk's velocities (time level 0), density0 and energy0.
 template <class S>
