@@ -1311,13 +1311,13 @@ void launch_advec_mom_fused(const Target& tg, cudaStream_t s, int advect_x, int 
                             typename S::wk_t* node_mass_pre, typename S::vel_t* const* vel_in,
                             typename S::vel_t* const* vel_out, bool copy_shell,
                             const Level0<S>& level0, const MomXMaps* x_maps, int* status,
-                            const NodeMaps* node_maps) {
+                            const NodeMaps* node_maps, const VelMaps* vel_maps) {
   // the node arrays of the y/z sweeps live in three work arrays, as nd_t
   using ND = typename S::nd_t;
   static_assert(sizeof(ND) <= sizeof(typename S::wk_t), "node arrays fit the work arrays");
-  ND* nd_flux = reinterpret_cast<ND*>(node_flux);
-  ND* nd_post = reinterpret_cast<ND*>(node_mass_post);
-  ND* nd_pre = reinterpret_cast<ND*>(node_mass_pre);
+  ND* nd_flux = nd_array<S>(node_flux);
+  ND* nd_post = nd_array<S>(node_mass_post);
+  ND* nd_pre = nd_array<S>(node_mass_pre);
   (void)vol;
   // post_vol variant (mom_post_vol) as a kernel template argument: x is sweep
   // 1 (0) or 3 (4); y is sweep 2 (2: after x, 3: after z); z is sweep 1 (1) or 3 (4)
@@ -1331,10 +1331,14 @@ void launch_advec_mom_fused(const Target& tg, cudaStream_t s, int advect_x, int 
                     k_mom_node_march<S, D, V, MapSingle>, k_mom_node_march<S, D, V, MapBatchFree>,
                     ga, D == 2 ? mass_flux_y : mass_flux_z, density1, vol_flux_x, vol_flux_y,
                     vol_flux_z, nd_flux, nd_post, nd_pre);
-    launch_mapped2(tg, s, kKeyMomVel3 | D, grid_mom_vel<D>, grid_mom_vel_flat<D>, kMarchSeg,
-                   true, kBlk, k_mom_vel3_march<S, D, MapSingle>, k_mom_vel3_march<S, D, MapBatchFree>,
-                   ga, nd_flux, nd_post, nd_pre, vel_in[0], vel_in[1], vel_in[2], vel_out[0],
-                   vel_out[1], vel_out[2], level0);
+    if (vel_maps && !tg.plan)
+      launch_mom_vel_tma<S>(tg.g, s, D, *vel_maps, ga, nd_flux, nd_pre, vel_in, vel_out, level0,
+                            status);
+    else
+      launch_mapped2(tg, s, kKeyMomVel3 | D, grid_mom_vel<D>, grid_mom_vel_flat<D>, kMarchSeg,
+                     true, kBlk, k_mom_vel3_march<S, D, MapSingle>,
+                     k_mom_vel3_march<S, D, MapBatchFree>, ga, nd_flux, nd_post, nd_pre,
+                     vel_in[0], vel_in[1], vel_in[2], vel_out[0], vel_out[1], vel_out[2], level0);
   };
   using I2 = std::integral_constant<int, 2>;
   using I3 = std::integral_constant<int, 3>;
@@ -1401,7 +1405,7 @@ void launch_advec_mom_fused(const Target& tg, cudaStream_t s, int advect_x, int 
                                           const S::vf_t*, const S::vf_t*, S::wk_t*, S::wk_t*,  \
                                           S::wk_t*, S::vel_t* const*, S::vel_t* const*, bool,  \
                                           const Level0<S>&, const MomXMaps*, int*,            \
-                                          const NodeMaps*);
+                                          const NodeMaps*, const VelMaps*);
 
 INSTF(F64)
 INSTF(F32Mixed)

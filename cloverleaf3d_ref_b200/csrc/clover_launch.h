@@ -153,6 +153,16 @@ struct F32Mixed {
   using arith_t = float;  // momentum flux and update, accelerate (node and cell masses stay FP64)
 };
 
+// The node arrays of the y/z momentum sweeps (node flux, node masses) as nd_t
+// views of work arrays of wk_t: an FP32 view of an FP64 work array starts two
+// elements in, so that its column x_min sits on a 128-byte boundary like every
+// other array's (the work array's x_min is 16 bytes after its base).
+template <class S>
+typename S::nd_t* nd_array(typename S::wk_t* w) {
+  using ND = typename S::nd_t;
+  return reinterpret_cast<ND*>(w) + (sizeof(ND) == 4 && sizeof(typename S::wk_t) == 8 ? 2 : 0);
+}
+
 // The time level 0 arrays, which the step's last sweep also writes: the final
 // density1/energy1 of every interior cell and vel1 of every node in
 // [min, max+1]^3, i.e. reset_field_kernel.f90:51-98 folded into the kernels
@@ -387,10 +397,11 @@ void launch_advec_cell_x(const Target& tg, cudaStream_t s, int sweep, const Geom
 // x_maps (one chunk, x sweep): the tensor maps of the sweep's inputs, to run
 // its shared-memory staged form (clover_tma.cu), which reports a copy that
 // did not arrive in *status; null: the register-marching form.
-// node_maps (one chunk, y/z sweep): the maps of the node pass's inputs, to run
-// its staged form.
+// node_maps, vel_maps (one chunk, y/z sweep): the maps of the node pass's and
+// the velocity pass's inputs, to run their staged forms.
 struct MomXMaps;
 struct NodeMaps;
+struct VelMaps;
 template <class S>
 void launch_advec_mom_fused(const Target& tg, cudaStream_t s, int advect_x, int sweep, int dir,
                             double vol, const GeomArrays& ga, const typename S::rho_t* density1,
@@ -401,7 +412,8 @@ void launch_advec_mom_fused(const Target& tg, cudaStream_t s, int advect_x, int 
                             typename S::wk_t* node_mass_pre, typename S::vel_t* const* vel_in,
                             typename S::vel_t* const* vel_out, bool copy_shell,
                             const Level0<S>& level0, const MomXMaps* x_maps = nullptr,
-                            int* status = nullptr, const NodeMaps* node_maps = nullptr);
+                            int* status = nullptr, const NodeMaps* node_maps = nullptr,
+                            const VelMaps* vel_maps = nullptr);
 
 // Fill every element of an array (size elems after the pad) with a value.
 template <class T>

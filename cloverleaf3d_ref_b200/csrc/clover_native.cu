@@ -186,6 +186,16 @@ struct Chunk : ChunkBase {
     if (ok && var == 2) ok = tmap(vol_flux_z, sizeof(VF), 10, &m->vfr, true);
     return ok;
   }
+  // the maps of the y (dir 2) or z (dir 3) velocity pass: the node arrays in
+  // work[0..2] (as nd_t) and the velocity buffers vin
+  bool mom_vel_maps(int dir, V* const* vin, VelMaps* m) {
+    const bool zr = dir == 2;
+    return tmap(nd_array<S>(work[0]), sizeof(ND), 8, &m->nf, zr) &&
+           tmap(nd_array<S>(work[2]), sizeof(ND), 8, &m->pre, zr) &&
+           tmap(nd_array<S>(work[1]), sizeof(ND), 8, &m->post, zr) &&
+           tmap(vin[0], sizeof(V), 8, &m->u, zr) &&
+           tmap(vin[1], sizeof(V), 8, &m->v, zr) && tmap(vin[2], sizeof(V), 8, &m->w, zr);
+  }
   bool mom_x_maps(const R* rho, V* const* vin, MomXMaps* m) {
     return tmap(mass_flux_x, sizeof(MF), 9, &m->mf) && tmap(rho, sizeof(R), 9, &m->d) &&
            tmap(vol_flux_y, sizeof(VF), 10, &m->vfy) && tmap(vol_flux_z, sizeof(VF), 9, &m->vfz) &&
@@ -381,7 +391,7 @@ struct Chunk : ChunkBase {
     // get their tensor maps (the arrays they read never move)
     if (!batched)
       tma = visc_dt_tma_prepare<S>() && mom_x_tma_prepare<S>() && stencils_tma_prepare<S>() &&
-            mom_node_tma_prepare<S>() &&
+            mom_node_tma_prepare<S>() && mom_vel_tma_prepare<S>() &&
             visc_dt_tma_maps<S>(g, xvel0, yvel0, zvel0, density0, energy0, &visc_maps);
 
     dt_cap = deck.end_step < (1 << 22) ? deck.end_step + 16 : (1 << 22);
@@ -895,11 +905,14 @@ struct Chunk : ChunkBase {
       const int node_var = dir == 2 ? (axi ? 2 : 3) : (sweep_number == 1 ? 1 : 4);
       const bool node_tma =
           dir != 1 && tma && use_tma && mom_node_maps(dir, node_var, rho1(cb), &nm);
+      VelMaps vm;
+      const bool vel_tma = dir != 1 && tma && use_tma && mom_vel_maps(dir, vin, &vm);
       launch_advec_mom_fused<S>(tg, stream, axi, sweep_number, dir, cell_volume, ga, rho1(cb),
                                 mass_flux_x, mass_flux_y, mass_flux_z, vol_flux_x, vol_flux_y,
                                 vol_flux_z, work[0], work[1], work[2], vin, vout,
                                 sweep_number == 3 || !halo_repeat_free, l0,
-                                x_tma ? &xm : nullptr, &sc->status, node_tma ? &nm : nullptr);
+                                x_tma ? &xm : nullptr, &sc->status, node_tma ? &nm : nullptr,
+                                vel_tma ? &vm : nullptr);
       // x: one pass; y, z: node pass + velocity pass
       if (dir == 1)
         pend("advec_mom_x", n * (MF8 + R8 + npv * VF8 + (6 + 3 * nl0) * V8));

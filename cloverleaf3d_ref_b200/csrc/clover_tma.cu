@@ -1052,6 +1052,129 @@ k_mom_node_tma(Geom g, int seg, const __grid_constant__ NodeMaps maps,
   });
 }
 
+// ---------------------------------------------------------------------------
+// The velocity pass of the y or z momentum sweep (advec_mom_kernel.f90:295-337
+// for y, :381-423 for z), as k_mom_vel3_march (clover_fused.cu) forms it: each
+// thread walks a segment of its (j, c) column with the velocity window and the
+// previous momentum fluxes in registers. The segment's start (the window
+// v(p0-2..p0+1) and the node values at p0-1, p0) is read from global memory;
+// in the loop, node p reads the node flux and node masses of plane p (and the
+// node mass pre of plane p+1) and the three velocities of plane p+2 from
+// staged planes (rows c0..c0+7, along y for the z sweep, along z for the y
+// sweep).
+template <class S>
+struct VelPlane {
+  using W = typename S::nd_t;
+  using V = typename S::vel_t;
+  static constexpr int kNd = round128(8 * kTmaWidth<W> * (int)sizeof(W));
+  static constexpr int kVel = round128(8 * kTmaWidth<V> * (int)sizeof(V));
+  static constexpr int kBytes = 3 * kNd + 3 * kVel;
+  static constexpr unsigned kTx = 3 * box_bytes<W>(8) + 3 * box_bytes<V>(8);
+  __device__ static W* nd(unsigned char* p, int q) { return (W*)(p + q * kNd); }
+  __device__ static V* vel(unsigned char* p, int q) { return (V*)(p + 3 * kNd + q * kVel); }
+};
+
+template <class S, int DIR, int RING, int MINB>
+__global__ void __launch_bounds__(TX * TY, MINB)
+k_mom_vel_tma(Geom g, int seg, GeomArrays ga, const __grid_constant__ VelMaps maps,
+              const typename S::nd_t* __restrict__ node_flux,
+              const typename S::nd_t* __restrict__ node_mass_pre,
+              const typename S::vel_t* __restrict__ u_in, const typename S::vel_t* __restrict__ v_in,
+              const typename S::vel_t* __restrict__ w_in, typename S::vel_t* __restrict__ u_out,
+              typename S::vel_t* __restrict__ v_out, typename S::vel_t* __restrict__ w_out,
+              Level0<S> lz, int* __restrict__ status) {
+  using P = VelPlane<S>;
+  using W = typename S::nd_t;
+  using V = typename S::vel_t;
+  using A = typename S::arith_t;  // arithmetic of the flux and update
+  extern __shared__ __align__(128) unsigned char ring[];
+  __shared__ unsigned long long full[RING];
+  __shared__ int stop;
+  const MarchRange r = mom_vel_range<DIR>(g);
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int j = r.jlo + TX * (int)blockIdx.x + tx;
+  const int c0 = r.clo + TY * (int)blockIdx.y, c = c0 + ty;
+  const bool in_jc = j <= r.jhi && c <= r.chi;
+  const int p0 = r.plo + seg * (int)blockIdx.z;
+  const int p1 = p0 + seg - 1 < r.phi ? p0 + seg - 1 : r.phi;
+  const PlaneMarch<RING, 0, 2> pm{ring, P::kBytes, full, &stop, p0, p1 + 2};
+  constexpr int WW = kTmaWidth<W>, HW = kTmaHalo<W>, WV = kTmaWidth<V>, HV = kTmaHalo<V>;
+  const int cw = ty * WW + tx + HW, cv = ty * WV + tx + HV;  // this node in the boxes
+#define IDX(p) j, (DIR == 2 ? (p) : c), (DIR == 2 ? c : (p))
+  const double* cd = DIR == 2 ? ga.celldy : ga.celldz;
+  const int cdlo = DIR == 2 ? g.y_min : g.z_min;
+#define CD(p) cd[g.o1 + (p) - cdlo + 2]
+#define LA(a, idx) lda<A>(&EI_(a, idx))
+#define EI_(a, jj, kk, ll) (a)[off3(g, (jj), (kk), (ll))]
+  const typename S::vel_t* in[3] = {u_in, v_in, w_in};
+  typename S::vel_t* out[3] = {u_out, v_out, w_out};
+  typename S::vel_t* lev0[3] = {lz.xvel0, lz.yvel0, lz.zvel0};
+  // window v(p-2), v(p-1), v(p), v(p+1) and the momentum flux of node p-1, from
+  // global memory at the segment's start
+  A vw[3][4];
+  A mf_prev[3];
+  A pre_0 = A(0.0);
+  if (in_jc) {
+    const A nf_m = LA(node_flux, IDX(p0 - 1));
+    const A pre_m = LA(node_mass_pre, IDX(p0 - 1));
+    pre_0 = LA(node_mass_pre, IDX(p0));
+    const MomNodeTerms<A> nt =
+        mom_node_terms<A>(nf_m, pre_m, pre_0, (A)CD(p0 - 1), (A)CD(p0 - 2), (A)CD(p0));
+#pragma unroll
+    for (int q = 0; q < 3; q++) {
+      vw[q][0] = LA(in[q], IDX(p0 - 2));
+      vw[q][1] = LA(in[q], IDX(p0 - 1));
+      vw[q][2] = LA(in[q], IDX(p0));
+      vw[q][3] = LA(in[q], IDX(p0 + 1));
+      mf_prev[q] = mom_flux_v<A>(nt, vw[q][0], vw[q][1], vw[q][2], vw[q][3]);
+    }
+  }
+  auto issue = [&](int p) {
+    unsigned char* b = pm.buf(p);
+    unsigned long long* bar = pm.bar(p);
+    mbar_arrive_expect_tx(bar, P::kTx);
+    const int x = TX * (int)blockIdx.x;
+    const int y = DIR == 3 ? c0 - g.y_min + 2 : p - g.y_min + 2;
+    const int z = DIR == 3 ? p - g.z_min + 2 : c0 - g.z_min + 2;
+    tma_load_box(P::nd(b, 0), &maps.nf, bar, x, y, z);
+    tma_load_box(P::nd(b, 1), &maps.pre, bar, x, y, z);
+    tma_load_box(P::nd(b, 2), &maps.post, bar, x, y, z);
+    tma_load_box(P::vel(b, 0), &maps.u, bar, x, y, z);
+    tma_load_box(P::vel(b, 1), &maps.v, bar, x, y, z);
+    tma_load_box(P::vel(b, 2), &maps.w, bar, x, y, z);
+  };
+  pm.run(p0, p1, status, issue, [&](int p) {
+    if (!in_jc) return;
+    unsigned char* b0 = pm.buf(p);
+    unsigned char* b1 = pm.buf(p + 1);
+    unsigned char* b2 = pm.buf(p + 2);
+    const A nf_0 = (A)P::nd(b0, 0)[cw];
+    const A pre_p = (A)P::nd(b1, 1)[cw];
+    const A post_0 = (A)P::nd(b0, 2)[cw];
+    const MomNodeTerms<A> nt =
+        mom_node_terms<A>(nf_0, pre_0, pre_p, (A)CD(p), (A)CD(p - 1), (A)CD(p + 1));
+    const long long o = off3(g, IDX(p));
+#pragma unroll
+    for (int q = 0; q < 3; q++) {
+      const A vp2 = (A)P::vel(b2, q)[cv];
+      const A mf_0 = mom_flux_v<A>(nt, vw[q][1], vw[q][2], vw[q][3], vp2);
+      const V vn1 = st<V>((vw[q][2] * pre_0 + mf_prev[q] - mf_0) / post_0);
+      out[q][o] = vn1;
+      if (lz.xvel0) lev0[q][o] = vn1;  // last sweep of the step: reset_field
+      mf_prev[q] = mf_0;
+      vw[q][0] = vw[q][1];
+      vw[q][1] = vw[q][2];
+      vw[q][2] = vw[q][3];
+      vw[q][3] = vp2;
+    }
+    pre_0 = pre_p;
+  });
+#undef EI_
+#undef LA
+#undef CD
+#undef IDX
+}
+
 constexpr int kViscRing = 4;
 constexpr int kViscSeg = 32;
 
@@ -1238,6 +1361,35 @@ void launch_mom_node_tma(const Geom& g, cudaStream_t s, int dir, int var, const 
   }
 }
 
+template <class S>
+constexpr int kVelMinBlocks = sizeof(typename S::arith_t) == 4 ? 5 : 3;
+
+template <class S>
+bool mom_vel_tma_prepare() {
+  return cudaFuncSetAttribute(k_mom_vel_tma<S, 2, kStencilRing, kVelMinBlocks<S>>,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              kStencilRing * VelPlane<S>::kBytes) == cudaSuccess &&
+         cudaFuncSetAttribute(k_mom_vel_tma<S, 3, kStencilRing, kVelMinBlocks<S>>,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              kStencilRing * VelPlane<S>::kBytes) == cudaSuccess;
+}
+
+template <class S>
+void launch_mom_vel_tma(const Geom& g, cudaStream_t s, int dir, const VelMaps& maps,
+                        const GeomArrays& ga, const typename S::nd_t* node_flux,
+                        const typename S::nd_t* node_mass_pre, typename S::vel_t* const* vel_in,
+                        typename S::vel_t* const* vel_out, const Level0<S>& level0, int* status) {
+  auto go = [&](auto kern, const MarchRange& r) {
+    const dim3 grid((r.jhi - r.jlo + TX) / TX, (r.chi - r.clo + TY) / TY,
+                    (r.phi - r.plo + kStencilSeg) / kStencilSeg);
+    kern<<<grid, dim3(TX, TY), kStencilRing * VelPlane<S>::kBytes, s>>>(
+        g, kStencilSeg, ga, maps, node_flux, node_mass_pre, vel_in[0], vel_in[1], vel_in[2],
+        vel_out[0], vel_out[1], vel_out[2], level0, status);
+  };
+  if (dir == 2) go(k_mom_vel_tma<S, 2, kStencilRing, kVelMinBlocks<S>>, mom_vel_range<2>(g));
+  else go(k_mom_vel_tma<S, 3, kStencilRing, kVelMinBlocks<S>>, mom_vel_range<3>(g));
+}
+
 #define INST_TMA(S)                                                                              \
   template bool visc_dt_tma_maps<S>(const Geom&, const S::vel_t*, const S::vel_t*,              \
                                     const S::vel_t*, const S::rho_t*, const S::ene_t*,          \
@@ -1246,6 +1398,10 @@ void launch_mom_node_tma(const Geom& g, cudaStream_t s, int dir, int var, const 
   template bool mom_x_tma_prepare<S>();                                                          \
   template bool stencils_tma_prepare<S>();                                                       \
   template bool mom_node_tma_prepare<S>();                                                       \
+  template bool mom_vel_tma_prepare<S>();                                                        \
+  template void launch_mom_vel_tma<S>(const Geom&, cudaStream_t, int, const VelMaps&,            \
+                                      const GeomArrays&, const S::nd_t*, const S::nd_t*,         \
+                                      S::vel_t* const*, S::vel_t* const*, const Level0<S>&, int*); \
   template void launch_mom_node_tma<S>(const Geom&, cudaStream_t, int, int, const NodeMaps&,     \
                                        S::nd_t*, S::nd_t*, S::nd_t*, int*);                      \
   template void launch_pdv_predict_eos_tma<S>(const Geom&, cudaStream_t, const double*,         \

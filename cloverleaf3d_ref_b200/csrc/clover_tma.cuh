@@ -108,6 +108,21 @@ void launch_mom_node_tma(const Geom& g, cudaStream_t s, int dir, int var, const 
                          typename S::nd_t* node_flux, typename S::nd_t* node_mass_post,
                          typename S::nd_t* node_mass_pre, int* status);
 
+// The maps of the y/z momentum velocity pass: node flux, node mass pre and
+// post (the work arrays as the node pass stores them) and the three
+// velocities it advects, 8 rows from c0 (along y for the z sweep, along z for
+// the y sweep).
+struct VelMaps {
+  CUtensorMap nf, pre, post, u, v, w;
+};
+template <class S>
+bool mom_vel_tma_prepare();
+template <class S>
+void launch_mom_vel_tma(const Geom& g, cudaStream_t s, int dir, const VelMaps& maps,
+                        const GeomArrays& ga, const typename S::nd_t* node_flux,
+                        const typename S::nd_t* node_mass_pre, typename S::vel_t* const* vel_in,
+                        typename S::vel_t* const* vel_out, const Level0<S>& level0, int* status);
+
 // The maps of a chunk's velocities (time level 0), density0 and energy0.
 template <class S>
 bool visc_dt_tma_maps(const Geom& g, const typename S::vel_t* xvel0, const typename S::vel_t* yvel0,
