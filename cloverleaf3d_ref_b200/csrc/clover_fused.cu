@@ -83,15 +83,6 @@ __host__ __device__ inline Box nodes(const Geom& g) {
   return Box{g.x_min, g.x_max + 1, g.y_min, g.y_max + 1, g.z_min, g.z_max + 1};
 }
 
-// advec_cell y sweep: columns l in [z_min, z_max+2] (the reference's y face
-// range), cells updated for l <= z_max; z sweep: rows k in [y_min, y_max]
-template <int DIR>
-__host__ __device__ inline MarchRange cell_sweep_range(const Geom& g) {
-  if (DIR == 2)
-    return MarchRange{g.x_min, g.x_max, g.z_min, g.z_max + 2, g.y_min, g.y_max + 2, g.z_max};
-  return MarchRange{g.x_min, g.x_max, g.y_min, g.y_max, g.z_min, g.z_max + 2, g.y_max};
-}
-
 #define E(a, jj, kk, ll) (a)[off3(g, (jj), (kk), (ll))]
 #define GX(a, jj) (a)[g.o1 + (jj) - g.x_min + 2]
 #define GY(a, kk) (a)[g.o1 + (kk) - g.y_min + 2]
@@ -484,26 +475,6 @@ __device__ __forceinline__ double cell_pre_vol(const Geom& g, int variant, const
     default:
       return vol + L(vfz, j, k, l + 1) - L(vfz, j, k, l);
   }
-}
-
-// vertexd(j) / vertexd(dif) of the limiter: exactly 1 where the two widths
-// are equal (every face of a uniform mesh), without the division
-__device__ __forceinline__ double width_ratio(double a, double b) {
-  return (a == b && a != 0.0 && fabs(a) <= DBL_MAX) ? 1.0 : a / b;
-}
-
-// advec_cell_kernel.f90:141-151 in the limiter's arithmetic A (FP64, or FP32
-// in the mixed path: the limiter shapes a face flux that both cells of the
-// face take, so its rounding does not touch conservation; the flux itself and
-// the cell update stay FP64)
-template <class A>
-__device__ __forceinline__ A cell_limiter(A sig, A sigma3, A sigma4, A diffuw, A diffdw) {
-  const A one_by_six = A(1.0) / A(6.0);
-  if (diffuw * diffdw > A(0.0))
-    return (A(1.0) - sig) * copysign(A(1.0), diffdw) *
-           fmin2(fmin2(fabs(diffuw), fabs(diffdw)),
-                 one_by_six * (sigma3 * fabs(diffuw) + sigma4 * fabs(diffdw)));
-  return A(0.0);
 }
 
 // advec_cell x sweep as ONE pass (advec_cell_kernel.f90:125-185), out of

@@ -196,6 +196,18 @@ struct Chunk : ChunkBase {
            tmap(vin[0], sizeof(V), 8, &m->u, zr) &&
            tmap(vin[1], sizeof(V), 8, &m->v, zr) && tmap(vin[2], sizeof(V), 8, &m->w, zr);
   }
+  // the maps of the staged y (dir 2) or z (dir 3) cell sweep reading buffer cb
+  // of the density1/energy1 pair, with pre-volume variant var
+  bool cell_maps(int dir, int var, int cb, CellMaps* m) {
+    const bool zr = dir == 2;
+    bool ok = tmap(rho1(cb), sizeof(R), 8, &m->d, zr) && tmap(ene1(cb), sizeof(En), 8, &m->e, zr) &&
+              tmap(dir == 2 ? (const void*)vol_flux_y : (const void*)vol_flux_z, sizeof(VF), 8,
+                   &m->vfd, zr);
+    if (ok && (var == 3 || var == 4)) ok = tmap(vol_flux_x, sizeof(VF), 8, &m->vfx, zr);
+    if (ok && var == 2) ok = tmap(vol_flux_z, sizeof(VF), 9, &m->vfr, true);
+    if (ok && var == 4) ok = tmap(vol_flux_y, sizeof(VF), 9, &m->vfr, false);
+    return ok;
+  }
   bool mom_x_maps(const R* rho, V* const* vin, MomXMaps* m) {
     return tmap(mass_flux_x, sizeof(MF), 9, &m->mf) && tmap(rho, sizeof(R), 9, &m->d) &&
            tmap(vol_flux_y, sizeof(VF), 10, &m->vfy) && tmap(vol_flux_z, sizeof(VF), 9, &m->vfz) &&
@@ -277,7 +289,8 @@ struct Chunk : ChunkBase {
   // each step flips the pair three times (one per sweep)
   int vel1_buffer(int steps) const { return fused ? steps % 2 : 0; }
   // density1/energy1 pair b, and the buffer holding them after `steps` fused
-  // steps (the x cell sweep flips it once per step)
+  // steps: the out-of-place cell sweeps flip it an odd number of times per
+  // step (the x sweep; with the staged y/z sweeps, all three)
   R* rho1(int b) const { return b ? rho1b : density1; }
   En* ene1(int b) const { return b ? e1b : energy1; }
   int cell_buffer(int steps) const { return fused ? steps % 2 : 0; }
@@ -391,7 +404,7 @@ struct Chunk : ChunkBase {
     // get their tensor maps (the arrays they read never move)
     if (!batched)
       tma = visc_dt_tma_prepare<S>() && mom_x_tma_prepare<S>() && stencils_tma_prepare<S>() &&
-            mom_node_tma_prepare<S>() && mom_vel_tma_prepare<S>() &&
+            mom_node_tma_prepare<S>() && mom_vel_tma_prepare<S>() && cell_sweep_tma_prepare<S>() &&
             visc_dt_tma_maps<S>(g, xvel0, yvel0, zvel0, density0, energy0, &visc_maps);
 
     dt_cap = deck.end_step < (1 << 22) ? deck.end_step + 16 : (1 << 22);
@@ -880,10 +893,21 @@ struct Chunk : ChunkBase {
         cb ^= 1;
         pend("advec_cell_x", n * (nvf * VF8 + (2 + nl0) * (R8 + E8) + MF8));
       } else {
-        // one marching pass, in place
-        launch_advec_cell_fused<S>(tg, stream, axi, dir, sweep_number, ga, rho1(cb), ene1(cb),
-                                   mass_flux_x, vol_flux_x, mass_flux_y, vol_flux_y,
-                                   mass_flux_z, vol_flux_z, work[6], l0);
+        // one marching pass: staged and out of place into the other buffer of
+        // the pair where the depth-2 halo update that follows rewrites the
+        // output's shell, in place otherwise
+        const int cvar = dir == 2 ? (axi ? 2 : 3) : (sweep_number == 1 ? 4 : 5);
+        CellMaps cm;
+        if (tma && use_tma && halo_repeat_free && cell_maps(dir, cvar, cb, &cm)) {
+          launch_cell_sweep_tma<S>(g, stream, dir, cvar, cm, ga, rho1(cb), ene1(cb), rho1(cb ^ 1),
+                                   ene1(cb ^ 1), vol_flux_x, vol_flux_y, vol_flux_z,
+                                   dir == 2 ? mass_flux_y : mass_flux_z, l0, &sc->status);
+          cb ^= 1;
+        } else {
+          launch_advec_cell_fused<S>(tg, stream, axi, dir, sweep_number, ga, rho1(cb), ene1(cb),
+                                     mass_flux_x, vol_flux_x, mass_flux_y, vol_flux_y,
+                                     mass_flux_z, vol_flux_z, work[6], l0);
+        }
         pend("advec_cell_yz", n * (nvf * VF8 + (2 + nl0) * (R8 + E8) + MF8));
       }
       pbeg();

@@ -32,6 +32,15 @@ __host__ __device__ inline MarchRange mom_vel_range(const Geom& g) {
   const int cmin = DIR == 2 ? g.z_min : g.y_min, cmx = DIR == 2 ? g.z_max : g.y_max;
   return MarchRange{g.x_min, g.x_max + 1, cmin, cmx + 1, pmin, pmax + 1, cmx + 1};
 }
+// advec_cell y sweep: columns l in [z_min, z_max+2] (the reference's y face
+// range), cells updated for l <= z_max; z sweep: rows k in [y_min, y_max]
+template <int DIR>
+__host__ __device__ inline MarchRange cell_sweep_range(const Geom& g) {
+  if (DIR == 2)
+    return MarchRange{g.x_min, g.x_max, g.z_min, g.z_max + 2, g.y_min, g.y_max + 2, g.z_max};
+  return MarchRange{g.x_min, g.x_max, g.y_min, g.y_max, g.z_min, g.z_max + 2, g.y_max};
+}
+
 // a value in storage type T, converted once from the arithmetic it was
 // formed in (no detour through double for an FP32 value stored as FP32)
 template <class T, class U>
@@ -46,6 +55,26 @@ template <class A>
 __device__ __forceinline__ A lda(const double* p) { return (A)__ldg(p); }
 template <class A>
 __device__ __forceinline__ A lda(const float* p) { return (A)__ldg(p); }
+
+// vertexd(j) / vertexd(dif) of the limiter: exactly 1 where the two widths
+// are equal (every face of a uniform mesh), without the division
+__device__ __forceinline__ double width_ratio(double a, double b) {
+  return (a == b && a != 0.0 && fabs(a) <= DBL_MAX) ? 1.0 : a / b;
+}
+
+// advec_cell_kernel.f90:141-151 in the limiter's arithmetic A (FP64, or FP32
+// in the mixed path: the limiter shapes a face flux that both cells of the
+// face take, so its rounding does not touch conservation; the flux itself and
+// the cell update stay FP64)
+template <class A>
+__device__ __forceinline__ A cell_limiter(A sig, A sigma3, A sigma4, A diffuw, A diffdw) {
+  const A one_by_six = A(1.0) / A(6.0);
+  if (diffuw * diffdw > A(0.0))
+    return (A(1.0) - sig) * copysign(A(1.0), diffdw) *
+           fmin2(fmin2(fabs(diffuw), fabs(diffdw)),
+                 one_by_six * (sigma3 * fabs(diffuw) + sigma4 * fabs(diffdw)));
+  return A(0.0);
+}
 
 // The per-chunk quotients of Geom in the arithmetic type A.
 template <class A>

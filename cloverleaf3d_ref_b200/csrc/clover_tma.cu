@@ -1175,6 +1175,209 @@ k_mom_vel_tma(Geom g, int seg, GeomArrays ga, const __grid_constant__ VelMaps ma
 #undef IDX
 }
 
+// ---------------------------------------------------------------------------
+// The y or z cell sweep (advec_cell_kernel.f90:190-281 for y, :287-376 for z)
+// out of place, its inputs staged in shared memory: the old density1/energy1
+// come from one buffer of the pair and the updated cells go to the other, so
+// segments of the sweep axis need no ordering between them (every interior
+// cell is written; the depth-2 halo update that follows rewrites the shell).
+// The arithmetic is k_cell_sweep_march's (clover_fused.cu), face by face: the
+// window of old values of cells p-2..p+1 and the pre-volumes of cells p-1, p
+// in registers, face p, then cell p-1. A segment's start (cells q0-2..q0 and
+// the pre-volume of cell q0-1) is read from global memory; at face p the loop
+// reads plane p (the sweep direction's volume flux at face p, the cross fluxes
+// of cell p's pre-volume) and plane p+1 (the volume flux at face p+1, density1
+// and energy1 of cell p+1). Rows c0..c0+7 (c0..c0+8 for the cross flux along
+// the rows) run along y for the z sweep and along z for the y sweep. Pre-volume
+// variants: y sweep 2 (after x: vol_flux_y and vol_flux_z) and 3 (after z:
+// vol_flux_y and vol_flux_x); z sweep 4 (first: all three) and 5 (last:
+// vol_flux_z).
+template <class S, int DIR, int VAR>
+struct CellPlane {
+  using R = typename S::rho_t;
+  using En = typename S::ene_t;
+  using VF = typename S::vf_t;
+  static constexpr bool kX = VAR == 3 || VAR == 4;  // vol_flux_x, columns j, j+1
+  static constexpr bool kR = VAR == 2 || VAR == 4;  // the flux along the rows, rows c, c+1
+  static constexpr int kRho = round128(8 * kTmaWidth<R> * (int)sizeof(R));
+  static constexpr int kEne = round128(8 * kTmaWidth<En> * (int)sizeof(En));
+  static constexpr int kVfd = round128(8 * kTmaWidth<VF> * (int)sizeof(VF));
+  static constexpr int kVfx = kX ? round128(8 * kTmaWidth<VF> * (int)sizeof(VF)) : 0;
+  static constexpr int kVfr = kR ? round128(9 * kTmaWidth<VF> * (int)sizeof(VF)) : 0;
+  static constexpr int kBytes = kRho + kEne + kVfd + kVfx + kVfr;
+  static constexpr unsigned kTx = box_bytes<R>(8) + box_bytes<En>(8) + box_bytes<VF>(8) +
+                                  (kX ? box_bytes<VF>(8) : 0u) + (kR ? box_bytes<VF>(9) : 0u);
+  __device__ static R* rho(unsigned char* p) { return (R*)p; }
+  __device__ static En* ene(unsigned char* p) { return (En*)(p + kRho); }
+  __device__ static VF* vfd(unsigned char* p) { return (VF*)(p + kRho + kEne); }
+  __device__ static VF* vfx(unsigned char* p) { return (VF*)(p + kRho + kEne + kVfd); }
+  __device__ static VF* vfr(unsigned char* p) { return (VF*)(p + kRho + kEne + kVfd + kVfx); }
+};
+
+template <class S, int DIR, int VAR, int RING, int MINB>
+__global__ void __launch_bounds__(TX * TY, MINB)
+k_cell_sweep_tma(Geom g, int seg, GeomArrays ga, const __grid_constant__ CellMaps maps,
+                 const typename S::rho_t* __restrict__ d_in, const typename S::ene_t* __restrict__ e_in,
+                 typename S::rho_t* __restrict__ d_out, typename S::ene_t* __restrict__ e_out,
+                 const typename S::vf_t* __restrict__ vfx, const typename S::vf_t* __restrict__ vfy,
+                 const typename S::vf_t* __restrict__ vfz, typename S::mf_t* __restrict__ mass_flux,
+                 Level0<S> lz, int* __restrict__ status) {
+  using P = CellPlane<S, DIR, VAR>;
+  using R = typename S::rho_t;
+  using En = typename S::ene_t;
+  using VF = typename S::vf_t;
+  using MF = typename S::mf_t;
+  using AL = typename S::arith_t;  // the limiters' arithmetic
+  extern __shared__ __align__(128) unsigned char ring[];
+  __shared__ unsigned long long full[RING];
+  __shared__ int stop;
+  const MarchRange r = cell_sweep_range<DIR>(g);
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int j = r.jlo + TX * (int)blockIdx.x + tx;
+  const int c0 = r.clo + TY * (int)blockIdx.y, c = c0 + ty;
+  const bool col = j <= r.jhi && c <= r.chi;
+  const bool update = c <= r.cmax;
+  const int pmin = DIR == 2 ? g.y_min : g.z_min;
+  const int pmax = DIR == 2 ? g.y_max : g.z_max;
+  const int top = pmax + 2;
+  const int q0 = pmin + seg * (int)blockIdx.z;  // cells of this segment: [q0, q1]
+  const int q1 = q0 + seg - 1 < pmax ? q0 + seg - 1 : pmax;
+  const bool last = q1 == pmax;  // this segment also walks the faces pmax+1, pmax+2
+  const int pend = last ? top : q1 + 1;
+  const PlaneMarch<RING, 0, 1> pm{ring, P::kBytes, full, &stop, q0, pend + 1};
+  constexpr int WR = kTmaWidth<R>, HR = kTmaHalo<R>, WE = kTmaWidth<En>, HE = kTmaHalo<En>;
+  constexpr int WF = kTmaWidth<VF>, HF = kTmaHalo<VF>;
+  const int cr = ty * WR + tx + HR, ce = ty * WE + tx + HE, cf = ty * WF + tx + HF;
+#define IDX(p) j, (DIR == 2 ? (p) : c), (DIR == 2 ? c : (p))
+#define LI(a, p) ((double)__ldg(&(a)[off3(g, IDX(p))]))
+  const typename S::vf_t* vf_d = DIR == 2 ? vfy : vfz;
+  const double* vd = DIR == 2 ? ga.vertexdy : ga.vertexdz;
+#define VD(p) vd[g.o1 + (p) - pmin + 2]
+  // pre_vol of cell p from global memory (the segment's start), the variant's order
+  auto prevol_g = [&](int p) {
+    const double vol = g.vol;
+    const int jj = j, kk = DIR == 2 ? p : c, ll = DIR == 2 ? c : p;
+    auto ld = [&](const VF* a, int dj, int dk, int dl) {
+      return (double)__ldg(&a[off3(g, jj + dj, kk + dk, ll + dl)]);
+    };
+    switch (VAR) {
+      case 4: {
+        const double fx1 = ld(vfx, 1, 0, 0), fx0 = ld(vfx, 0, 0, 0);
+        const double fy1 = ld(vfy, 0, 1, 0), fy0 = ld(vfy, 0, 0, 0);
+        const double fz1 = ld(vfz, 0, 0, 1), fz0 = ld(vfz, 0, 0, 0);
+        return vol + (fx1 - fx0 + fy1 - fy0 + fz1 - fz0);
+      }
+      case 2:
+        return vol + ld(vfy, 0, 1, 0) - ld(vfy, 0, 0, 0) + ld(vfz, 0, 0, 1) - ld(vfz, 0, 0, 0);
+      case 3:
+        return vol + ld(vfy, 0, 1, 0) - ld(vfy, 0, 0, 0) + ld(vfx, 1, 0, 0) - ld(vfx, 0, 0, 0);
+      default:
+        return vol + ld(vfz, 0, 0, 1) - ld(vfz, 0, 0, 0);
+    }
+  };
+  // pre_vol of cell p from the staged planes p (b0) and p+1 (b1), the same order
+  auto prevol_s = [&](unsigned char* b0, unsigned char* b1) {
+    const double vol = g.vol;
+    const double d1 = (double)P::vfd(b1)[cf], d0 = (double)P::vfd(b0)[cf];
+    switch (VAR) {
+      case 4: {  // z sweep: x, y (the rows), z (the sweep)
+        const double fx1 = (double)P::vfx(b0)[cf + 1], fx0 = (double)P::vfx(b0)[cf];
+        const double fy1 = (double)P::vfr(b0)[cf + WF], fy0 = (double)P::vfr(b0)[cf];
+        return vol + (fx1 - fx0 + fy1 - fy0 + d1 - d0);
+      }
+      case 2:  // y sweep: y (the sweep), z (the rows)
+        return vol + d1 - d0 + (double)P::vfr(b0)[cf + WF] - (double)P::vfr(b0)[cf];
+      case 3:  // y sweep: y (the sweep), x
+        return vol + d1 - d0 + (double)P::vfx(b0)[cf + 1] - (double)P::vfx(b0)[cf];
+      default:  // z sweep: z only
+        return vol + d1 - d0;
+    }
+  };
+  // window: d0..d3 = density1(p-2..p+1), e0..e3 = energy1(p-2..p+1), old values
+  double d0 = 0.0, d1 = 0.0, d2 = 0.0, d3 = 0.0, e0 = 0.0, e1 = 0.0, e2 = 0.0, e3 = 0.0;
+  double pv_m = 0.0, pv_0 = 0.0;  // pre_vol(p-1), pre_vol(p)
+  double vf_prev = 0.0, mf_prev = 0.0, ef_prev = 0.0;
+  if (col) {
+    d0 = LI(d_in, q0 - 2); d1 = LI(d_in, q0 - 1); d2 = LI(d_in, q0);
+    e0 = LI(e_in, q0 - 2); e1 = LI(e_in, q0 - 1); e2 = LI(e_in, q0);
+    pv_m = prevol_g(q0 - 1);
+  }
+  auto issue = [&](int p) {
+    unsigned char* b = pm.buf(p);
+    unsigned long long* bar = pm.bar(p);
+    mbar_arrive_expect_tx(bar, P::kTx);
+    const int x = TX * (int)blockIdx.x;
+    const int y = DIR == 3 ? c0 - g.y_min + 2 : p - g.y_min + 2;
+    const int z = DIR == 3 ? p - g.z_min + 2 : c0 - g.z_min + 2;
+    tma_load_box(P::rho(b), &maps.d, bar, x, y, z);
+    tma_load_box(P::ene(b), &maps.e, bar, x, y, z);
+    tma_load_box(P::vfd(b), &maps.vfd, bar, x, y, z);
+    if (P::kX) tma_load_box(P::vfx(b), &maps.vfx, bar, x, y, z);
+    if (P::kR) tma_load_box(P::vfr(b), &maps.vfr, bar, x, y, z);
+  };
+  using MFT = MF;
+  pm.run(q0, pend, status, issue, [&](int p) {
+    if (!col) return;
+    unsigned char* b0 = pm.buf(p);
+    unsigned char* b1 = pm.buf(p + 1);
+    // cell p+1 is read by face p (the upwind index clamps to pmax+2 at the top)
+    unsigned char* bn = p + 1 <= top ? b1 : b0;
+    d3 = (double)P::rho(bn)[cr];
+    e3 = (double)P::ene(bn)[ce];
+    pv_0 = prevol_s(b0, b1);
+    const double vf = (double)P::vfd(b0)[cf];
+    // advec_cell_kernel.f90:226-264 (y) / :321-359 (z) at face p
+    double d_up, d_don, d_dn, e_up, e_don, e_dn, pv_don;
+    int dif;
+    if (vf > 0.0) {  // upwind p-2, donor p-1, downwind p
+      d_up = d0; d_don = d1; d_dn = d2; e_up = e0; e_don = e1; e_dn = e2; pv_don = pv_m;
+      dif = p - 1;
+    } else {  // upwind min(p+1, pmax+2), donor p, downwind p-1
+      d_up = d3; d_don = d2; d_dn = d1; e_up = e3; e_don = e2; e_dn = e1; pv_don = pv_0;
+      dif = p + 1 < top ? p + 1 : top;
+    }
+    const AL sigmat = (AL)fabs(vf) / (AL)pv_don;
+    const AL sigma3 = (AL(1.0) + sigmat) * (AL)width_ratio(VD(p), VD(dif));
+    const AL sigma4 = AL(2.0) - sigmat;
+    AL diffuw = (AL)(d_don - d_up);
+    AL diffdw = (AL)(d_dn - d_don);
+    AL limiter = cell_limiter<AL>(sigmat, sigma3, sigma4, diffuw, diffdw);
+    const double mflux = vf * (d_don + (double)limiter);
+    if (p <= q1 || last) mass_flux[off3(g, IDX(p))] = st<MFT>(mflux);
+    const double mf_stored = mflux;  // FP64 in the cell update; mf_t storage feeds the momentum sweep
+    const AL sigmam = (AL)fabs(mflux) / ((AL)d_don * (AL)pv_don);
+    diffuw = (AL)(e_don - e_up);
+    diffdw = (AL)(e_dn - e_don);
+    limiter = cell_limiter<AL>(sigmam, sigma3, sigma4, diffuw, diffdw);
+    const double eflux = mflux * (e_don + (double)limiter);
+    // advec_cell_kernel.f90:270-281 (y) / :365-376 (z) for cell p-1
+    if (update && p - 1 >= q0 && p - 1 <= q1) {
+      const double pmass = d1 * pv_m;
+      const double pom = pmass + mf_prev - mf_stored;
+      const double poe = (e1 * pmass + ef_prev - eflux) / pom;
+      const double av = pv_m + vf_prev - vf;
+      const R dn = st<R>(pom / av);
+      const En en = st<En>(poe);
+      const long long o = off3(g, IDX(p - 1));
+      d_out[o] = dn;
+      e_out[o] = en;
+      if (lz.density0) {  // last sweep of the step: reset_field
+        lz.density0[o] = dn;
+        lz.energy0[o] = en;
+      }
+    }
+    vf_prev = vf;
+    mf_prev = mf_stored;
+    ef_prev = eflux;
+    d0 = d1; d1 = d2; d2 = d3;
+    e0 = e1; e1 = e2; e2 = e3;
+    pv_m = pv_0;
+  });
+#undef VD
+#undef LI
+#undef IDX
+}
+
 constexpr int kViscRing = 4;
 constexpr int kViscSeg = 32;
 
@@ -1390,6 +1593,49 @@ void launch_mom_vel_tma(const Geom& g, cudaStream_t s, int dir, const VelMaps& m
   else go(k_mom_vel_tma<S, 3, kStencilRing, kVelMinBlocks<S>>, mom_vel_range<3>(g));
 }
 
+template <class S>
+constexpr int kCellMinBlocks = sizeof(typename S::arith_t) == 4 ? 4 : 3;
+
+template <class S>
+bool cell_sweep_tma_prepare() {
+  bool ok = true;
+  auto set = [&](auto kern, int bytes) {
+    ok = ok && cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    kStencilRing * bytes) == cudaSuccess;
+  };
+  set(k_cell_sweep_tma<S, 2, 2, kStencilRing, kCellMinBlocks<S>>, CellPlane<S, 2, 2>::kBytes);
+  set(k_cell_sweep_tma<S, 2, 3, kStencilRing, kCellMinBlocks<S>>, CellPlane<S, 2, 3>::kBytes);
+  set(k_cell_sweep_tma<S, 3, 4, kStencilRing, kCellMinBlocks<S>>, CellPlane<S, 3, 4>::kBytes);
+  set(k_cell_sweep_tma<S, 3, 5, kStencilRing, kCellMinBlocks<S>>, CellPlane<S, 3, 5>::kBytes);
+  return ok;
+}
+
+template <class S>
+void launch_cell_sweep_tma(const Geom& g, cudaStream_t s, int dir, int var, const CellMaps& maps,
+                           const GeomArrays& ga, const typename S::rho_t* d_in,
+                           const typename S::ene_t* e_in, typename S::rho_t* d_out,
+                           typename S::ene_t* e_out, const typename S::vf_t* vfx,
+                           const typename S::vf_t* vfy, const typename S::vf_t* vfz,
+                           typename S::mf_t* mass_flux, const Level0<S>& level0, int* status) {
+  auto go = [&](auto kern, int bytes, const MarchRange& r, int pcells) {
+    const dim3 grid((r.jhi - r.jlo + TX) / TX, (r.chi - r.clo + TY) / TY,
+                    (pcells + kStencilSeg - 1) / kStencilSeg);
+    kern<<<grid, dim3(TX, TY), kStencilRing * bytes, s>>>(g, kStencilSeg, ga, maps, d_in, e_in,
+                                                          d_out, e_out, vfx, vfy, vfz, mass_flux,
+                                                          level0, status);
+  };
+  const int ny = g.y_max - g.y_min + 1, nz = g.z_max - g.z_min + 1;
+  if (dir == 2) {
+    const MarchRange r = cell_sweep_range<2>(g);
+    if (var == 2) go(k_cell_sweep_tma<S, 2, 2, kStencilRing, kCellMinBlocks<S>>, CellPlane<S, 2, 2>::kBytes, r, ny);
+    else go(k_cell_sweep_tma<S, 2, 3, kStencilRing, kCellMinBlocks<S>>, CellPlane<S, 2, 3>::kBytes, r, ny);
+  } else {
+    const MarchRange r = cell_sweep_range<3>(g);
+    if (var == 4) go(k_cell_sweep_tma<S, 3, 4, kStencilRing, kCellMinBlocks<S>>, CellPlane<S, 3, 4>::kBytes, r, nz);
+    else go(k_cell_sweep_tma<S, 3, 5, kStencilRing, kCellMinBlocks<S>>, CellPlane<S, 3, 5>::kBytes, r, nz);
+  }
+}
+
 #define INST_TMA(S)                                                                              \
   template bool visc_dt_tma_maps<S>(const Geom&, const S::vel_t*, const S::vel_t*,              \
                                     const S::vel_t*, const S::rho_t*, const S::ene_t*,          \
@@ -1399,6 +1645,11 @@ void launch_mom_vel_tma(const Geom& g, cudaStream_t s, int dir, const VelMaps& m
   template bool stencils_tma_prepare<S>();                                                       \
   template bool mom_node_tma_prepare<S>();                                                       \
   template bool mom_vel_tma_prepare<S>();                                                        \
+  template bool cell_sweep_tma_prepare<S>();                                                     \
+  template void launch_cell_sweep_tma<S>(const Geom&, cudaStream_t, int, int, const CellMaps&,   \
+                                         const GeomArrays&, const S::rho_t*, const S::ene_t*,    \
+                                         S::rho_t*, S::ene_t*, const S::vf_t*, const S::vf_t*,   \
+                                         const S::vf_t*, S::mf_t*, const Level0<S>&, int*);      \
   template void launch_mom_vel_tma<S>(const Geom&, cudaStream_t, int, const VelMaps&,            \
                                       const GeomArrays&, const S::nd_t*, const S::nd_t*,         \
                                       S::vel_t* const*, S::vel_t* const*, const Level0<S>&, int*); \

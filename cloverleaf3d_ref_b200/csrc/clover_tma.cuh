@@ -123,6 +123,26 @@ void launch_mom_vel_tma(const Geom& g, cudaStream_t s, int dir, const VelMaps& m
                         const typename S::nd_t* node_mass_pre, typename S::vel_t* const* vel_in,
                         typename S::vel_t* const* vel_out, const Level0<S>& level0, int* status);
 
+// The maps of the staged y/z cell sweep: density1 and energy1 of the input
+// buffer, the sweep direction's volume flux (8 rows from c0), vol_flux_x (8
+// rows) and the volume flux along the rows (9 rows: vol_flux_z for the y
+// sweep's variant 2, vol_flux_y for the z sweep's variant 4).
+struct CellMaps {
+  CUtensorMap d, e, vfd, vfx, vfr;
+};
+template <class S>
+bool cell_sweep_tma_prepare();
+// The y (dir 2) or z (dir 3) cell sweep with pre-volume variant var, out of
+// place from (d_in, e_in) into (d_out, e_out), planes staged by bulk-tensor
+// copies. Needs a depth-2 halo update of density1/energy1 after it.
+template <class S>
+void launch_cell_sweep_tma(const Geom& g, cudaStream_t s, int dir, int var, const CellMaps& maps,
+                           const GeomArrays& ga, const typename S::rho_t* d_in,
+                           const typename S::ene_t* e_in, typename S::rho_t* d_out,
+                           typename S::ene_t* e_out, const typename S::vf_t* vfx,
+                           const typename S::vf_t* vfy, const typename S::vf_t* vfz,
+                           typename S::mf_t* mass_flux, const Level0<S>& level0, int* status);
+
 // The maps of a chunk's velocities (time level 0), density0 and energy0.
 template <class S>
 bool visc_dt_tma_maps(const Geom& g, const typename S::vel_t* xvel0, const typename S::vel_t* yvel0,
