@@ -532,73 +532,312 @@ __device__ __forceinline__ double cell_limiter(double sig, double sigma3, double
   return 0.0;
 }
 
-// advec_cell_kernel.f90 flux pass (:125-171 x, :220-266 y, :315-361 z).
-// DIR is the sweep axis; (dj,dk,dl) its unit offset.
-template <class S, int DIR>
-__global__ void __launch_bounds__(BX * BY, 8) k_cell_flux(Geom g, Box b, GeomArrays ga,
-    const typename S::rho_t* __restrict__ density1, const typename S::ene_t* __restrict__ energy1,
-    const typename S::vf_t* __restrict__ vol_flux, typename S::mf_t* __restrict__ mass_flux,
-    const typename S::wk_t* __restrict__ pre_vol, typename S::wk_t* __restrict__ ener_flux) {
-  BOX_THREAD(b);
-  const int i = DIR == 1 ? j : DIR == 2 ? k : l;
-  const int imax = DIR == 1 ? g.x_max : DIR == 2 ? g.y_max : g.z_max;
-  const double* vd = DIR == 1 ? ga.vertexdx : DIR == 2 ? ga.vertexdy : ga.vertexdz;
-  const int vlo = DIR == 1 ? g.x_min : DIR == 2 ? g.y_min : g.z_min;
-  const double vf = L(vol_flux, j, k, l);
-  int upwind, donor, downwind, dif;
-  if (vf > 0.0) {
-    upwind = i - 2; donor = i - 1; downwind = i; dif = donor;
-  } else {
-    upwind = (i + 1 < imax + 2) ? i + 1 : imax + 2;
-    donor = i; downwind = i - 1; dif = upwind;
-  }
-#define AT(a, ii) L(a, DIR == 1 ? (ii) : j, DIR == 2 ? (ii) : k, DIR == 3 ? (ii) : l)
-  const double pv_donor = AT(pre_vol, donor);
-  const double sigmat = fabs(vf) / pv_donor;
-  const double sigma3 = (1.0 + sigmat) * (vd[g.o1 + i - vlo + 2] / vd[g.o1 + dif - vlo + 2]);
-  const double sigma4 = 2.0 - sigmat;
-  const double sigmav = sigmat;
+// Warp-row helpers of the x sweeps: lane m holds element b+m of a row chunk
+// (cur), b+32+m (nxt) and b-32+m (prv).
+constexpr unsigned kFull = 0xffffffffu;
 
-  const double d_donor = AT(density1, donor);
-  double diffuw = d_donor - AT(density1, upwind);
-  double diffdw = AT(density1, downwind) - d_donor;
-  double limiter = cell_limiter(sigmav, sigma3, sigma4, diffuw, diffdw);
-  const double mflux = vf * (d_donor + limiter);
-  E(mass_flux, j, k, l) = st<typename S::mf_t>(mflux);
-
-  const double sigmam = fabs(mflux) / (d_donor * pv_donor);
-  const double e_donor = AT(energy1, donor);
-  diffuw = e_donor - AT(energy1, upwind);
-  diffdw = AT(energy1, downwind) - e_donor;
-  limiter = cell_limiter(sigmam, sigma3, sigma4, diffuw, diffdw);
-  E(ener_flux, j, k, l) = st<typename S::wk_t>(mflux * (e_donor + limiter));
-#undef AT
+// element b+m+s of the row (s = 1, 2): lanes past 31 read the next chunk
+__device__ __forceinline__ double row_dn(double cur, double nxt, int s) {
+  const int m = threadIdx.x & 31;
+  return __shfl_sync(kFull, m >= s ? cur : nxt, (m + s) & 31);
+}
+// element b+m-1: lane 0 reads the previous chunk's last
+__device__ __forceinline__ double row_up(double cur, double prv) {
+  const int m = threadIdx.x & 31;
+  return __shfl_sync(kFull, m == 31 ? prv : cur, (m + 31) & 31);
 }
 
-// advec_cell_kernel.f90 update pass (:175-186 x, :270-281 y, :365-376 z)
-template <class S, int DIR>
-__global__ void __launch_bounds__(BX * BY) k_cell_update(Geom g, Box b,
-    typename S::rho_t* __restrict__ density1, typename S::ene_t* __restrict__ energy1,
-    const typename S::vf_t* __restrict__ vol_flux, const typename S::mf_t* __restrict__ mass_flux,
-    const typename S::wk_t* __restrict__ pre_vol, typename S::wk_t* __restrict__ pre_mass,
-    typename S::wk_t* __restrict__ post_mass, typename S::wk_t* __restrict__ advec_vol,
-    typename S::wk_t* __restrict__ post_ener, const typename S::wk_t* __restrict__ ener_flux) {
-  BOX_THREAD(b);
-  const int j1 = j + (DIR == 1), k1 = k + (DIR == 2), l1 = l + (DIR == 3);
-  const double pv = L(pre_vol, j, k, l);
-  const double pm = L(density1, j, k, l) * pv;
-  const double pom = pm + L(mass_flux, j, k, l) - L(mass_flux, j1, k1, l1);
-  const double poe = (L(energy1, j, k, l) * pm + L(ener_flux, j, k, l) - L(ener_flux, j1, k1, l1)) / pom;
-  const double av = pv + L(vol_flux, j, k, l) - L(vol_flux, j1, k1, l1);
+// A loaded element of an array the kernel also writes (a plain load: the
+// read-only path is for arrays nobody writes during the launch).
+template <class T>
+__device__ __forceinline__ double ldw(const T* p) { return (double)*p; }
+
+// Per-thread prefetch rings of the line marches: each thread copies the
+// elements it will need kLineRing - 1 steps ahead into its own shared-memory
+// slots with cp.async (one commit group per step) and reads back only its own
+// slots after its own cp.async.wait_group, so no barrier orders them. A copy
+// whose element is not wanted zero-fills its slot without reading memory.
+constexpr int kLineRing = 4;
+constexpr int kLineStreams = 4;
+constexpr int kLineSlots = kLineRing * kLineStreams * BX * BY;  // doubles per block
+
+template <class T>
+__device__ __forceinline__ void cp_elem(double* slot, const T* src, bool want) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(slot);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;\n" ::"r"(d), "l"(src),
+               "n"((int)sizeof(T)), "r"(want ? (int)sizeof(T) : 0)
+               : "memory");
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_wait_step() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(kLineRing - 1) : "memory");
+}
+__device__ __forceinline__ void cp_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+template <class T>
+__device__ __forceinline__ double slot_val(const double* slot) {
+  return (double)*(const volatile T*)slot;
+}
+// this thread's slot of stream q for step t
+__device__ __forceinline__ double* line_slot(double* ring, int t, int q) {
+  return ring + ((t & (kLineRing - 1)) * kLineStreams + q) * (BX * BY) + threadIdx.y * BX + threadIdx.x;
+}
+
+// The fluxes at one face of a cell sweep (advec_cell_kernel.f90:125-171 x,
+// :220-266 y, :315-361 z), from the cells' old values: du/dd/dw (density) and
+// eu/ed/ew (energy) at the upwind, donor and downwind cells, pvd the donor's
+// pre_vol, rw = vertexd(i) / vertexd(dif). mf and ef are the mass and energy
+// fluxes as formed (the energy flux takes the mass flux before storage).
+__device__ __forceinline__ void cell_face_flux(double vf, double pvd, double rw, double du,
+                                               double dd, double dw, double eu, double ed,
+                                               double ew, double& mf, double& ef) {
+  const double sigmat = fabs(vf) / pvd;
+  const double sigma3 = (1.0 + sigmat) * rw;
+  const double sigma4 = 2.0 - sigmat;
+  double limiter = cell_limiter(sigmat, sigma3, sigma4, dd - du, dw - dd);
+  mf = vf * (dd + limiter);
+  const double sigmam = fabs(mf) / (dd * pvd);
+  limiter = cell_limiter(sigmam, sigma3, sigma4, ed - eu, ew - ed);
+  ef = mf * (ed + limiter);
+}
+
+// The cell update (advec_cell_kernel.f90:175-186 x, :270-281 y, :365-376 z) of
+// a cell with old density d, energy e, pre_vol pv, from the stored fluxes at
+// its low (ml, el, vl) and high (mh, eh, vh) faces.
+template <class S>
+__device__ __forceinline__ void cell_update(long long at, double d, double e, double pv,
+                                            double ml, double mh, double el, double eh,
+                                            double vl, double vh,
+                                            typename S::rho_t* __restrict__ density1,
+                                            typename S::ene_t* __restrict__ energy1,
+                                            typename S::wk_t* __restrict__ pre_mass,
+                                            typename S::wk_t* __restrict__ post_mass,
+                                            typename S::wk_t* __restrict__ advec_vol,
+                                            typename S::wk_t* __restrict__ post_ener) {
+  const double pm = d * pv;
+  const double pom = pm + ml - mh;
+  const double poe = (e * pm + el - eh) / pom;
+  const double av = pv + vl - vh;
   using W = typename S::wk_t;
   if (pre_mass) {
-    E(pre_mass, j, k, l) = st<W>(pm);
-    E(post_mass, j, k, l) = st<W>(pom);
-    E(post_ener, j, k, l) = st<W>(poe);
-    E(advec_vol, j, k, l) = st<W>(av);
+    pre_mass[at] = st<W>(pm);
+    post_mass[at] = st<W>(pom);
+    post_ener[at] = st<W>(poe);
+    advec_vol[at] = st<W>(av);
   }
-  E(density1, j, k, l) = st<typename S::rho_t>(pom / av);
-  E(energy1, j, k, l) = st<typename S::ene_t>(poe);
+  density1[at] = st<typename S::rho_t>(pom / av);
+  energy1[at] = st<typename S::ene_t>(poe);
+}
+
+// The x cell sweep, flux pass and update in one: a warp per (k, l) row of the
+// interior marches along x in chunks of 32 cells. Lane m of the chunk at b
+// holds the old values of cell b+m, forms the fluxes at face b+m+1 (faces
+// x_min..x_max+2) and updates cell b+m from them and the fluxes lane m-1
+// formed at face b+m (lane 0: lane 31 of the previous chunk). A face reads
+// cells b+m-1 .. b+m+2, all held in registers (this chunk, the next, and the
+// previous chunk's last), and the next chunks are loaded before this one is
+// written: density1 and energy1 are updated in place and no element is read
+// after it has been written.
+template <class S>
+__global__ void __launch_bounds__(BX * BY, 3) k_cell_line_x(Geom g, GeomArrays ga,
+    typename S::rho_t* __restrict__ density1, typename S::ene_t* __restrict__ energy1,
+    const typename S::vf_t* __restrict__ vol_flux, typename S::mf_t* __restrict__ mass_flux,
+    const typename S::wk_t* __restrict__ pre_vol, typename S::wk_t* __restrict__ pre_mass,
+    typename S::wk_t* __restrict__ post_mass, typename S::wk_t* __restrict__ advec_vol,
+    typename S::wk_t* __restrict__ post_ener, typename S::wk_t* __restrict__ ener_flux) {
+  __shared__ double ring[kLineSlots];
+  const int k = g.y_min + blockIdx.x * BY + threadIdx.y;
+  const int l = g.z_min + blockIdx.y;
+  if (k > g.y_max) return;  // the warp's row: every lane leaves together
+  const int m = threadIdx.x;
+  const int x0 = g.x_min, x1 = g.x_max;
+  const long long row = off3(g, 0, k, l);  // element j of the row at row + j
+  const double* vd = ga.vertexdx + g.o1 + 2 - x0;
+  auto in_row = [&](int j) { return j >= x0 - 2 && j <= x1 + 2; };
+  auto lw = [&](const auto* a, int j) { return in_row(j) ? ldw(a + row + j) : 0.0; };
+  auto lr = [&](const auto* a, int j) { return in_row(j) ? ld(a + row + j) : 0.0; };
+  // step t marches the chunk at b = x0-32+32t; its ring entry is the chunk
+  // two ahead (b+64), copied kLineRing-1 steps before it is shifted in
+  const int steps = (x1 + 1 - (x0 - 32)) / 32 + 1;
+  auto issue = [&](int t) {
+    const int j = x0 + 32 + 32 * t + m;
+    const bool want = t < steps && in_row(j);
+    const long long at = row + (want ? j : x0);
+    cp_elem(line_slot(ring, t, 0), density1 + at, want);
+    cp_elem(line_slot(ring, t, 1), energy1 + at, want);
+    cp_elem(line_slot(ring, t, 2), pre_vol + at, want);
+    cp_elem(line_slot(ring, t, 3), vol_flux + at, want);
+    cp_commit();
+  };
+  for (int t = 0; t < kLineRing - 1; t++) issue(t);
+  int b = x0 - 32;
+  double dp = 0.0, dc = lw(density1, b + m), dn = lw(density1, b + 32 + m);
+  double ep = 0.0, ec = lw(energy1, b + m), en = lw(energy1, b + 32 + m);
+  double pc = lr(pre_vol, b + m), pn = lr(pre_vol, b + 32 + m);
+  double fc = lr(vol_flux, b + m), fn = lr(vol_flux, b + 32 + m);
+  double m_last = 0.0, e_last = 0.0;  // this lane's stored fluxes of the previous chunk
+  for (int t = 0; t < steps; t++, b += 32) {
+    issue(t + kLineRing - 1);
+    cp_wait_step();
+    const double dnn = slot_val<typename S::rho_t>(line_slot(ring, t, 0));
+    const double enn = slot_val<typename S::ene_t>(line_slot(ring, t, 1));
+    const double pnn = slot_val<typename S::wk_t>(line_slot(ring, t, 2));
+    const double fnn = slot_val<typename S::vf_t>(line_slot(ring, t, 3));
+    const int c = b + m, i = c + 1;  // this lane's cell and face
+    const double da = row_up(dc, dp), d1 = row_dn(dc, dn, 1), d2 = row_dn(dc, dn, 2);
+    const double ea = row_up(ec, ep), e1 = row_dn(ec, en, 1), e2 = row_dn(ec, en, 2);
+    const double vf = row_dn(fc, fn, 1), pv1 = row_dn(pc, pn, 1);
+    double mflux = 0.0, eflux = 0.0;
+    if (i >= x0 && i <= x1 + 2) {
+      // vf > 0: upwind i-2, donor i-1, downwind i; else upwind MIN(i+1, x_max+2),
+      // donor i, downwind i-1 (the donor's vertexdx over the upwind's)
+      const bool pos = vf > 0.0, clamp = i + 1 > x1 + 2;
+      const int dif = pos ? i - 1 : (clamp ? x1 + 2 : i + 1);
+      double mf, ef;
+      cell_face_flux(vf, pos ? pc : pv1, vd[i] / vd[dif], pos ? da : (clamp ? d1 : d2),
+                     pos ? dc : d1, pos ? d1 : dc, pos ? ea : (clamp ? e1 : e2), pos ? ec : e1,
+                     pos ? e1 : ec, mf, ef);
+      const typename S::mf_t ms = st<typename S::mf_t>(mf);
+      const typename S::wk_t es = st<typename S::wk_t>(ef);
+      mass_flux[row + i] = ms;
+      ener_flux[row + i] = es;
+      mflux = (double)ms;
+      eflux = (double)es;
+    }
+    const double ml = row_up(mflux, m_last), el = row_up(eflux, e_last);
+    if (c >= x0 && c <= x1)
+      cell_update<S>(row + c, dc, ec, pc, ml, mflux, el, eflux, fc, vf, density1, energy1,
+                     pre_mass, post_mass, advec_vol, post_ener);
+    m_last = mflux;
+    e_last = eflux;
+    dp = dc; dc = dn; dn = dnn;
+    ep = ec; ec = en; en = enn;
+    pc = pn; pn = pnn;
+    fc = fn; fn = fnn;
+  }
+  cp_wait_all();
+}
+
+// The y or z cell sweep (DIR 2 or 3), flux pass and update in one. A block
+// holds 32 columns along the sweep axis (consecutive in x, then in the other
+// index: l for y, over z_min..z_max+2 as the reference's y flux range, k for
+// z) and splits the faces min..max+2 into one segment per warp.
+// A warp marches its segment face by face with the old cells i-2..i+1 in
+// registers, stores the fluxes at face i and updates cell i-1. Before the
+// block's barrier each warp reads the old cells it needs that the
+// neighbouring segments will overwrite: the first window (cells f0-3..f0,
+// starting with the face f0-1 below its segment, formed again and not stored)
+// and cells f1 and f1+1 above its last face f1. After the barrier a warp
+// writes only its own cells and reads from memory only its own cells not yet
+// written, so the update is in place.
+template <class S, int DIR>
+__global__ void __launch_bounds__(BX * BY, 3) k_cell_line_yz(Geom g, GeomArrays ga,
+    typename S::rho_t* __restrict__ density1, typename S::ene_t* __restrict__ energy1,
+    const typename S::vf_t* __restrict__ vol_flux, typename S::mf_t* __restrict__ mass_flux,
+    const typename S::wk_t* __restrict__ pre_vol, typename S::wk_t* __restrict__ pre_mass,
+    typename S::wk_t* __restrict__ post_mass, typename S::wk_t* __restrict__ advec_vol,
+    typename S::wk_t* __restrict__ post_ener, typename S::wk_t* __restrict__ ener_flux) {
+  __shared__ double ring[kLineSlots];
+  // columns (j, o) numbered j fastest: lane x of block b holds column 32b+x
+  const int nj = g.x_max - g.x_min + 1;
+  const int no = DIR == 2 ? g.z_max + 3 - g.z_min : g.y_max + 1 - g.y_min;
+  const int col = blockIdx.x * BX + threadIdx.x;
+  const int j = g.x_min + col % nj;
+  const int o = (DIR == 2 ? g.z_min : g.y_min) + col / nj;
+  const int imin = DIR == 2 ? g.y_min : g.z_min, imax = DIR == 2 ? g.y_max : g.z_max;
+  const int top = imax + 2;  // last face, and last cell a face reads
+  // faces imin..top in BY segments
+  const int per = (top - imin + BY) / BY;
+  const int f0 = imin + (int)threadIdx.y * per;
+  const int f1 = f0 + per - 1 < top ? f0 + per - 1 : top;
+  const bool act = col < nj * no && f0 <= f1;
+  const bool upd = DIR == 3 || o <= g.z_max;  // the y sweep's planes z_max+1, z_max+2: fluxes only
+  const long long step = DIR == 2 ? g.px : g.pxy;
+  const long long base = DIR == 2 ? off3(g, j, 0, o) : off3(g, j, o, 0);  // + i * step
+  const double* vd = (DIR == 2 ? ga.vertexdy : ga.vertexdz) + g.o1 + 2 - imin;
+  const int i0 = f0 > imin ? f0 - 1 : f0;  // first face formed
+  const int steps = f1 - i0 + 1;
+  // cells f1 and MIN(f1+1, top) above the segment (the next segment's), read
+  // before the barrier and kept in shared memory until the segment's end
+  __shared__ double edge[4][BX * BY];
+  const int me = threadIdx.y * BX + threadIdx.x;
+  // step t (face i = i0+t) shifts in cell MIN(i+2, top) (below f1; the cells
+  // at and above f1 come from the pre-read pair), pre_vol and vol_flux at
+  // i+1; ia is the element offset of face i0+ti, the next step to issue
+  int ti = 0;
+  long long ia = base + i0 * step;
+  auto issue = [&]() {
+    const int i = i0 + ti;
+    const bool wc = ti < steps && i + 2 < f1, wf = ti < steps && i < f1;
+    const long long ac = wc ? ia + 2 * step : base, af = wf ? ia + step : base;
+    double* sl = line_slot(ring, ti, 0);
+    cp_elem(sl, density1 + ac, wc);
+    cp_elem(sl + BX * BY, energy1 + ac, wc);
+    cp_elem(sl + 2 * BX * BY, pre_vol + af, wf);
+    cp_elem(sl + 3 * BX * BY, vol_flux + af, wf);
+    cp_commit();
+    ia += step;
+    ti++;
+  };
+  double d0 = 0, d1 = 0, d2 = 0, d3 = 0, e0 = 0, e1 = 0, e2 = 0, e3 = 0;  // cells i-2..i+1
+  if (act) {
+    for (int t = 0; t < kLineRing - 1; t++) issue();
+    const int c3 = i0 + 1 < top ? i0 + 1 : top;
+    d0 = ldw(density1 + base + (i0 - 2) * step); e0 = ldw(energy1 + base + (i0 - 2) * step);
+    d1 = ldw(density1 + base + (i0 - 1) * step); e1 = ldw(energy1 + base + (i0 - 1) * step);
+    d2 = ldw(density1 + base + i0 * step);       e2 = ldw(energy1 + base + i0 * step);
+    d3 = ldw(density1 + base + c3 * step);       e3 = ldw(energy1 + base + c3 * step);
+    const int r1 = f1 + 1 < top ? f1 + 1 : top;
+    edge[0][me] = ldw(density1 + base + f1 * step);
+    edge[1][me] = ldw(density1 + base + r1 * step);
+    edge[2][me] = ldw(energy1 + base + f1 * step);
+    edge[3][me] = ldw(energy1 + base + r1 * step);
+  }
+  __syncthreads();
+  if (!act) return;
+  double p0 = ld(pre_vol + base + (i0 - 1) * step), p1 = ld(pre_vol + base + i0 * step);
+  double v0 = ld(vol_flux + base + (i0 - 1) * step), v1 = ld(vol_flux + base + i0 * step);
+  // vertex widths at i-1, i and MIN(i+1, top)
+  double xm = vd[i0 - 1], xc = vd[i0], xp = vd[i0 + 1 < top ? i0 + 1 : top];
+  long long at = base + i0 * step;  // face i
+  double m_last = 0.0, e_last = 0.0;  // stored fluxes at face i-1
+  for (int t = 0; t < steps; t++) {
+    issue();
+    const int i = i0 + t, cn = i + 2 < top ? i + 2 : top;
+    const double xn = vd[cn];
+    cp_wait_step();
+    const double* sl = line_slot(ring, t, 0);
+    // (at the segment's last face cn may be f1+2: that shift-in is never used)
+    const int eg = cn > f1 ? 1 : 0;
+    const double dn = cn < f1 ? slot_val<typename S::rho_t>(sl) : edge[eg][me];
+    const double en = cn < f1 ? slot_val<typename S::ene_t>(sl + BX * BY) : edge[2 + eg][me];
+    const double pn = slot_val<typename S::wk_t>(sl + 2 * BX * BY);
+    const double vn = slot_val<typename S::vf_t>(sl + 3 * BX * BY);
+    // face i: cells d0 (i-2), d1 (i-1), d2 (i), d3 (MIN(i+1, top)); the
+    // donor's width over the upwind's: i-1 for v > 0, else MIN(i+1, top)
+    const bool pos = v1 > 0.0;
+    double mf, ef;
+    cell_face_flux(v1, pos ? p0 : p1, xc / (pos ? xm : xp), pos ? d0 : d3, pos ? d1 : d2,
+                   pos ? d2 : d1, pos ? e0 : e3, pos ? e1 : e2, pos ? e2 : e1, mf, ef);
+    const typename S::mf_t ms = st<typename S::mf_t>(mf);
+    const typename S::wk_t es = st<typename S::wk_t>(ef);
+    if (i >= f0) {
+      mass_flux[at] = ms;
+      ener_flux[at] = es;
+    }
+    const int c = i - 1;
+    if (upd && i > i0 && c >= imin && c <= imax)
+      cell_update<S>(at - step, d1, e1, p0, m_last, (double)ms, e_last, (double)es, v0, v1,
+                     density1, energy1, pre_mass, post_mass, advec_vol, post_ener);
+    m_last = (double)ms;
+    e_last = (double)es;
+    d0 = d1; d1 = d2; d2 = d3; d3 = dn;
+    e0 = e1; e1 = e2; e2 = e3; e3 = en;
+    p0 = p1; p1 = pn;
+    v0 = v1; v1 = vn;
+    xm = xc; xc = xp; xp = xn;
+    at += step;
+  }
+  cp_wait_all();
 }
 
 // ---------------------------------------------------------------------------
@@ -710,45 +949,180 @@ __device__ __forceinline__ double mom_limiter(double sigma, double width, double
   return limiter;
 }
 
-// mom_flux (:211-242 x, :295-327 y, :381-413 z)
-template <class S, int DIR>
-__global__ void __launch_bounds__(BX * BY, 8) k_mom_flux(Geom g, Box b, GeomArrays ga,
-    const typename S::vel_t* __restrict__ vel1, const typename S::wk_t* __restrict__ node_flux,
-    const typename S::wk_t* __restrict__ node_mass_pre, typename S::wk_t* __restrict__ mom_flux) {
-  BOX_THREAD(b);
-  const int i = DIR == 1 ? j : DIR == 2 ? k : l;
-  const double nf = L(node_flux, j, k, l);
-  int upwind, donor, downwind, dif;
-  if (nf < 0.0) {
-    upwind = i + 2; donor = i + 1; downwind = i; dif = donor;
-  } else {
-    upwind = i - 1; donor = i; downwind = i + 1; dif = upwind;
-  }
-#define AT(a, ii) L(a, DIR == 1 ? (ii) : j, DIR == 2 ? (ii) : k, DIR == 3 ? (ii) : l)
-  const double sigma = fabs(nf) / AT(node_mass_pre, donor);
-  const double* cd = DIR == 1 ? ga.celldx : DIR == 2 ? ga.celldy : ga.celldz;
-  const int clo = DIR == 1 ? g.x_min : DIR == 2 ? g.y_min : g.z_min;
-  const double width = cd[g.o1 + i - clo + 2];
-  const double v_donor = AT(vel1, donor);
-  const double vdiffuw = v_donor - AT(vel1, upwind);
-  const double vdiffdw = AT(vel1, downwind) - v_donor;
-  const double limiter = mom_limiter(sigma, width, cd[g.o1 + dif - clo + 2], vdiffuw, vdiffdw);
+// The momentum flux at node i (advec_mom_kernel.f90:211-242 x, :295-327 y,
+// :381-413 z) from the old velocities vm1, v0, vp1, vp2 at i-1..i+2, the node
+// flux nf, node_mass_pre at i and i+1, and the cell widths cd at i-1, i, i+1.
+__device__ __forceinline__ double mom_node_flux(double nf, double vm1, double v0, double vp1,
+                                                double vp2, double nmp0, double nmp1, double cdm,
+                                                double cd0, double cdp) {
+  // nf < 0: upwind i+2, donor i+1, downwind i (width of the donor);
+  // else upwind i-1, donor i, downwind i+1 (width of the upwind)
+  const bool neg = nf < 0.0;
+  const double v_donor = neg ? vp1 : v0;
+  const double sigma = fabs(nf) / (neg ? nmp1 : nmp0);
+  const double vdiffuw = v_donor - (neg ? vp2 : vm1);
+  const double vdiffdw = (neg ? v0 : vp1) - v_donor;
+  const double limiter = mom_limiter(sigma, cd0, neg ? cdp : cdm, vdiffuw, vdiffdw);
   const double advec_vel_s = v_donor + (1.0 - sigma) * limiter;
-  E(mom_flux, j, k, l) = st<typename S::wk_t>(advec_vel_s * nf);
-#undef AT
+  return advec_vel_s * nf;
 }
 
-// velocity update (:245-252 x, :330-337 y, :416-423 z)
+// The x momentum flux and velocity update of one velocity in one pass: a warp
+// per (k, l) node row (nodes y_min..y_max+1, z_min..z_max+1) marches along x
+// in chunks of 32 nodes. Lane m of the chunk at b forms the flux at node b+m
+// (nodes x_min-1..x_max+1) from the old velocities b+m-1..b+m+2 held in
+// registers (this chunk, the next and the previous chunk's last) and updates
+// node b+m (x_min..x_max+1) with the flux lane m-1 formed (lane 0: lane 31 of
+// the previous chunk); the velocity is updated in place.
+template <class S>
+__global__ void __launch_bounds__(BX * BY, 4) k_mom_line_x(Geom g, GeomArrays ga,
+    typename S::vel_t* __restrict__ vel1, const typename S::wk_t* __restrict__ node_flux,
+    const typename S::wk_t* __restrict__ node_mass_pre,
+    const typename S::wk_t* __restrict__ node_mass_post, typename S::wk_t* __restrict__ mom_flux) {
+  __shared__ double ring[kLineSlots];
+  const int k = g.y_min + blockIdx.x * BY + threadIdx.y;
+  const int l = g.z_min + blockIdx.y;
+  if (k > g.y_max + 1) return;  // the warp's row: every lane leaves together
+  const int m = threadIdx.x;
+  const int x0 = g.x_min, x1 = g.x_max;
+  const long long row = off3(g, 0, k, l);
+  const double* cd = ga.celldx + g.o1 + 2 - x0;
+  auto in_row = [&](int j) { return j >= x0 - 2 && j <= x1 + 3; };
+  auto lw = [&](const auto* a, int j) { return in_row(j) ? ldw(a + row + j) : 0.0; };
+  auto lr = [&](const auto* a, int j) { return in_row(j) ? ld(a + row + j) : 0.0; };
+  // step t marches the chunk at b = x0-32+32t: its ring entries are the
+  // velocity and node_mass_pre two chunks ahead (b+64) and the node flux and
+  // node_mass_post of the chunk itself
+  const int steps = (x1 + 1 - (x0 - 32)) / 32 + 1;
+  auto issue = [&](int t) {
+    const int ja = x0 + 32 + 32 * t + m, jc = x0 - 32 + 32 * t + m;
+    const bool wa = t < steps && in_row(ja), wc = t < steps && in_row(jc);
+    const long long aa = row + (wa ? ja : x0), ac = row + (wc ? jc : x0);
+    cp_elem(line_slot(ring, t, 0), vel1 + aa, wa);
+    cp_elem(line_slot(ring, t, 1), node_mass_pre + aa, wa);
+    cp_elem(line_slot(ring, t, 2), node_flux + ac, wc);
+    cp_elem(line_slot(ring, t, 3), node_mass_post + ac, wc);
+    cp_commit();
+  };
+  for (int t = 0; t < kLineRing - 1; t++) issue(t);
+  int b = x0 - 32;
+  double vp = 0.0, vc = lw(vel1, b + m), vn = lw(vel1, b + 32 + m);
+  double qc = lr(node_mass_pre, b + m), qn = lr(node_mass_pre, b + 32 + m);
+  double f_last = 0.0;  // this lane's stored flux of the previous chunk
+  for (int t = 0; t < steps; t++, b += 32) {
+    issue(t + kLineRing - 1);
+    cp_wait_step();
+    const double vnn = slot_val<typename S::vel_t>(line_slot(ring, t, 0));
+    const double qnn = slot_val<typename S::wk_t>(line_slot(ring, t, 1));
+    const double nf = slot_val<typename S::wk_t>(line_slot(ring, t, 2));
+    const double post = slot_val<typename S::wk_t>(line_slot(ring, t, 3));
+    const int i = b + m;
+    const double vm1 = row_up(vc, vp), vp1 = row_dn(vc, vn, 1), vp2 = row_dn(vc, vn, 2);
+    const double q1 = row_dn(qc, qn, 1);
+    double flux = 0.0;
+    if (i >= x0 - 1 && i <= x1 + 1) {
+      const typename S::wk_t fs = st<typename S::wk_t>(
+          mom_node_flux(nf, vm1, vc, vp1, vp2, qc, q1, cd[i - 1], cd[i], cd[i + 1]));
+      mom_flux[row + i] = fs;
+      flux = (double)fs;
+    }
+    const double fl = row_up(flux, f_last);
+    if (i >= x0 && i <= x1 + 1)
+      vel1[row + i] = st<typename S::vel_t>((vc * qc + fl - flux) / post);
+    f_last = flux;
+    vp = vc; vc = vn; vn = vnn;
+    qc = qn; qn = qnn;
+  }
+  cp_wait_all();
+}
+
+// The y or z momentum flux and velocity update of one velocity in one pass
+// (DIR 2 or 3). A block holds 32 node columns along the sweep axis
+// (consecutive in x, then in the other index) and splits the nodes min..max+1
+// into one segment per warp. A warp marches its segment node by node with the
+// old velocities i-1..i+2 in registers, starting at the node below its
+// segment (whose flux only the first segment stores), stores the flux at node
+// i and updates node i. Before the block's barrier each warp reads the old
+// velocities the neighbouring segments will overwrite: n0-2, n0-1 below its
+// first node n0 and n1+1, n1+2 above its last n1; so the update is in place.
 template <class S, int DIR>
-__global__ void __launch_bounds__(BX * BY) k_mom_update(Geom g, Box b,
-    typename S::vel_t* __restrict__ vel1, const typename S::wk_t* __restrict__ node_mass_pre,
-    const typename S::wk_t* __restrict__ node_mass_post, const typename S::wk_t* __restrict__ mom_flux) {
-  BOX_THREAD(b);
-  const double prev = DIR == 1 ? L(mom_flux, j - 1, k, l)
-                    : DIR == 2 ? L(mom_flux, j, k - 1, l) : L(mom_flux, j, k, l - 1);
-  E(vel1, j, k, l) = st<typename S::vel_t>(
-      (L(vel1, j, k, l) * L(node_mass_pre, j, k, l) + prev - L(mom_flux, j, k, l)) /
-      L(node_mass_post, j, k, l));
+__global__ void __launch_bounds__(BX * BY, 4) k_mom_line_yz(Geom g, GeomArrays ga,
+    typename S::vel_t* __restrict__ vel1, const typename S::wk_t* __restrict__ node_flux,
+    const typename S::wk_t* __restrict__ node_mass_pre,
+    const typename S::wk_t* __restrict__ node_mass_post, typename S::wk_t* __restrict__ mom_flux) {
+  __shared__ double ring[kLineSlots];
+  // node columns (j, o) numbered j fastest: lane x of block b holds column 32b+x
+  const int nj = g.x_max + 2 - g.x_min;
+  const int no = DIR == 2 ? g.z_max + 2 - g.z_min : g.y_max + 2 - g.y_min;
+  const int col = blockIdx.x * BX + threadIdx.x;
+  const int j = g.x_min + col % nj;
+  const int o = (DIR == 2 ? g.z_min : g.y_min) + col / nj;
+  const int imin = DIR == 2 ? g.y_min : g.z_min;
+  const int top = (DIR == 2 ? g.y_max : g.z_max) + 1;  // last node
+  const int per = (top - imin + BY) / BY;
+  const int n0 = imin + (int)threadIdx.y * per;
+  const int n1 = n0 + per - 1 < top ? n0 + per - 1 : top;
+  const bool act = col < nj * no && n0 <= n1;
+  const long long step = DIR == 2 ? g.px : g.pxy;
+  const long long base = DIR == 2 ? off3(g, j, 0, o) : off3(g, j, o, 0);
+  const double* cd = (DIR == 2 ? ga.celldy : ga.celldz) + g.o1 + 2 - imin;
+  const int i0 = n0 - 1;  // first node whose flux is formed
+  const int steps = n1 - i0 + 1;
+  // the velocities n1+1, n1+2 above the segment (the next segment's), read
+  // before the barrier and kept in shared memory until the segment's end
+  __shared__ double edge[2][BX * BY];
+  const int me = threadIdx.y * BX + threadIdx.x;
+  // step t (node i = i0+t): the velocity at i+2 (up to n1; above it the
+  // pre-read pair), node_mass_pre at i+1, the node flux and node_mass_post
+  // at i; ia is the element offset of node i0+ti, the next step to issue
+  int ti = 0;
+  long long ia = base + i0 * step;
+  auto issue = [&]() {
+    const bool wn = ti < steps, wv = wn && i0 + ti + 2 <= n1;
+    const long long a = wn ? ia : base;
+    double* sl = line_slot(ring, ti, 0);
+    cp_elem(sl, vel1 + (wv ? ia + 2 * step : base), wv);
+    cp_elem(sl + BX * BY, node_mass_pre + a + (wn ? step : 0), wn);
+    cp_elem(sl + 2 * BX * BY, node_flux + a, wn);
+    cp_elem(sl + 3 * BX * BY, node_mass_post + a, wn);
+    cp_commit();
+    ia += step;
+    ti++;
+  };
+  double w0 = 0, w1 = 0, w2 = 0;  // old velocities i-1..i+1
+  if (act) {
+    for (int t = 0; t < kLineRing - 1; t++) issue();
+    w0 = ldw(vel1 + base + (i0 - 1) * step);
+    w1 = ldw(vel1 + base + i0 * step);
+    w2 = ldw(vel1 + base + (i0 + 1) * step);
+    edge[0][me] = ldw(vel1 + base + (n1 + 1) * step);
+    edge[1][me] = ldw(vel1 + base + (n1 + 2) * step);
+  }
+  __syncthreads();
+  if (!act) return;
+  double q0 = ld(node_mass_pre + base + i0 * step);
+  long long at = base + i0 * step;  // node i
+  double f_last = 0.0;  // stored flux at node i-1
+  for (int t = 0; t < steps; t++) {
+    issue();
+    const int i = i0 + t;
+    cp_wait_step();
+    const double* sl = line_slot(ring, t, 0);
+    // (i + 2 is n1 + 1 or n1 + 2 here)
+    const double w3 = i + 2 <= n1 ? slot_val<typename S::vel_t>(sl) : edge[i + 1 - n1][me];
+    const double q1 = slot_val<typename S::wk_t>(sl + BX * BY);
+    const double nf = slot_val<typename S::wk_t>(sl + 2 * BX * BY);
+    const double post = slot_val<typename S::wk_t>(sl + 3 * BX * BY);
+    const typename S::wk_t fs =
+        st<typename S::wk_t>(mom_node_flux(nf, w0, w1, w2, w3, q0, q1, cd[i - 1], cd[i], cd[i + 1]));
+    if (i >= n0 || n0 == imin) mom_flux[at] = fs;
+    if (i >= n0) vel1[at] = st<typename S::vel_t>((w1 * q0 + f_last - (double)fs) / post);
+    f_last = (double)fs;
+    w0 = w1; w1 = w2; w2 = w3;
+    q0 = q1;
+    at += step;
+  }
+  cp_wait_all();
 }
 
 // ---------------------------------------------------------------------------
@@ -1245,22 +1619,18 @@ void launch_advec_cell(const Geom& g, cudaStream_t s, int advect_x, int dir, int
   else if (dir == 3) variant = sweep == 1 ? 4 : sweep == 3 ? 5 : -1;
   if (variant >= 0)
     LAUNCH(k_cell_vol<S>, halo2(g), variant, ga, vol_flux_x, vol_flux_y, vol_flux_z, pre_vol, post_vol);
-  if (dir == 1) {
-    LAUNCH((k_cell_flux<S, 1>), (Box{g.x_min, g.x_max + 2, g.y_min, g.y_max, g.z_min, g.z_max}),
-           ga, density1, energy1, vol_flux_x, mass_flux_x, pre_vol, ener_flux);
-    LAUNCH((k_cell_update<S, 1>), interior(g), density1, energy1, vol_flux_x, mass_flux_x, pre_vol,
-           pre_mass, post_mass, advec_vol, post_ener, ener_flux);
-  } else if (dir == 2) {
-    LAUNCH((k_cell_flux<S, 2>), (Box{g.x_min, g.x_max, g.y_min, g.y_max + 2, g.z_min, g.z_max + 2}),
-           ga, density1, energy1, vol_flux_y, mass_flux_y, pre_vol, ener_flux);
-    LAUNCH((k_cell_update<S, 2>), interior(g), density1, energy1, vol_flux_y, mass_flux_y, pre_vol,
-           pre_mass, post_mass, advec_vol, post_ener, ener_flux);
-  } else if (dir == 3) {
-    LAUNCH((k_cell_flux<S, 3>), (Box{g.x_min, g.x_max, g.y_min, g.y_max, g.z_min, g.z_max + 2}),
-           ga, density1, energy1, vol_flux_z, mass_flux_z, pre_vol, ener_flux);
-    LAUNCH((k_cell_update<S, 3>), interior(g), density1, energy1, vol_flux_z, mass_flux_z, pre_vol,
-           pre_mass, post_mass, advec_vol, post_ener, ener_flux);
-  }
+  const int nx = g.x_max - g.x_min + 1, ny = g.y_max - g.y_min + 1, nz = g.z_max - g.z_min + 1;
+  const dim3 blk(BX, BY);
+  if (dir == 1)
+    k_cell_line_x<S><<<dim3((ny + BY - 1) / BY, nz), blk, 0, s>>>(g, ga, density1, energy1,
+        vol_flux_x, mass_flux_x, pre_vol, pre_mass, post_mass, advec_vol, post_ener, ener_flux);
+  else if (dir == 2)  // columns on the planes z_min..z_max+2 (the reference's y flux range)
+    k_cell_line_yz<S, 2><<<dim3((nx * (nz + 2) + BX - 1) / BX), blk, 0, s>>>(g, ga, density1,
+        energy1, vol_flux_y, mass_flux_y, pre_vol, pre_mass, post_mass, advec_vol, post_ener,
+        ener_flux);
+  else if (dir == 3)
+    k_cell_line_yz<S, 3><<<dim3((nx * ny + BX - 1) / BX), blk, 0, s>>>(g, ga, density1, energy1,
+        vol_flux_z, mass_flux_z, pre_vol, pre_mass, post_mass, advec_vol, post_ener, ener_flux);
 }
 
 static inline Box box_union(const Box& a, const Box& b) {
@@ -1301,8 +1671,6 @@ void launch_advec_mom(const Geom& g, cudaStream_t s, typename S::vel_t* vel1,
              node_flux, node_mass_post);
       LAUNCH((k_mom_nmpre<S, 1>), bm, node_flux, node_mass_post, node_mass_pre);
     }
-    LAUNCH((k_mom_flux<S, 1>), (Box{x0 - 1, x1 + 1, y0, y1 + 1, z0, z1 + 1}), ga, vel1, node_flux,
-           node_mass_pre, mom_flux);
   } else if (direction == 2) {
     if (which_vel == 1) {
       const Box bf{x0, x1 + 1, y0 - 2, y1 + 2, z0, z1 + 1}, bm{x0, x1 + 1, y0 - 1, y1 + 2, z0, z1 + 1};
@@ -1310,8 +1678,6 @@ void launch_advec_mom(const Geom& g, cudaStream_t s, typename S::vel_t* vel1,
              node_flux, node_mass_post);
       LAUNCH((k_mom_nmpre<S, 2>), bm, node_flux, node_mass_post, node_mass_pre);
     }
-    LAUNCH((k_mom_flux<S, 2>), (Box{x0, x1 + 1, y0 - 1, y1 + 1, z0, z1 + 1}), ga, vel1, node_flux,
-           node_mass_pre, mom_flux);
   } else if (direction == 3) {
     if (which_vel == 1) {
       const Box bf{x0, x1 + 1, y0, y1 + 1, z0 - 2, z1 + 2}, bm{x0, x1 + 1, y0, y1 + 1, z0 - 1, z1 + 2};
@@ -1319,15 +1685,20 @@ void launch_advec_mom(const Geom& g, cudaStream_t s, typename S::vel_t* vel1,
              node_flux, node_mass_post);
       LAUNCH((k_mom_nmpre<S, 3>), bm, node_flux, node_mass_post, node_mass_pre);
     }
-    LAUNCH((k_mom_flux<S, 3>), (Box{x0, x1 + 1, y0, y1 + 1, z0 - 1, z1 + 1}), ga, vel1, node_flux,
-           node_mass_pre, mom_flux);
   }
+  // the flux at nodes min-1..max+1 and the update of nodes min..max+1 along
+  // the sweep, in one pass per velocity
+  const int nx = x1 - x0 + 1, ny = y1 - y0 + 1, nz = z1 - z0 + 1;
+  const dim3 blk(BX, BY);
   if (direction == 1)
-    LAUNCH((k_mom_update<S, 1>), nodes(g), vel1, node_mass_pre, node_mass_post, mom_flux);
+    k_mom_line_x<S><<<dim3((ny + 1 + BY - 1) / BY, nz + 1), blk, 0, s>>>(g, ga, vel1, node_flux,
+        node_mass_pre, node_mass_post, mom_flux);
   else if (direction == 2)
-    LAUNCH((k_mom_update<S, 2>), nodes(g), vel1, node_mass_pre, node_mass_post, mom_flux);
+    k_mom_line_yz<S, 2><<<dim3(((nx + 1) * (nz + 1) + BX - 1) / BX), blk, 0, s>>>(g, ga, vel1,
+        node_flux, node_mass_pre, node_mass_post, mom_flux);
   else if (direction == 3)
-    LAUNCH((k_mom_update<S, 3>), nodes(g), vel1, node_mass_pre, node_mass_post, mom_flux);
+    k_mom_line_yz<S, 3><<<dim3(((nx + 1) * (ny + 1) + BX - 1) / BX), blk, 0, s>>>(g, ga, vel1,
+        node_flux, node_mass_pre, node_mass_post, mom_flux);
 }
 
 template <class S>
