@@ -231,6 +231,7 @@ def _declare(L):
     L.clover_gpu_error_string.restype = ctypes.c_char_p
     L.clover_gpu_invalidate.argtypes = [P]
     L.clover_gpu_invalidate_all.argtypes = []
+    L.clover_gpu_use_staging.argtypes = [ctypes.c_int]
     abi = L
 
 

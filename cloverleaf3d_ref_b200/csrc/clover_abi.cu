@@ -3,13 +3,16 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <string>
+#include <tuple>
 #include <unordered_map>
 #include <vector>
 
 #include "../../include/clover_kernels.h"
 #include "clover_launch.h"
+#include "clover_tma.cuh"
 
 namespace clover {
 namespace {
@@ -57,6 +60,15 @@ struct Context {
   int status = 0;
   std::string err;
   bool pin_host = true;
+  // Bulk-tensor staging of the stencils that have a staged form: allowed
+  // (clover_gpu_use_staging), and whether the staged kernels could be set up
+  // (0 not tried yet, 1 ready, -1 unavailable). Tensor maps are made once per
+  // (array, box rows, layout) and kept until release; a staged kernel whose
+  // bounded wait gives up sets a bit in d_status, read back at the next sync.
+  bool staging = true;
+  int tma_state = 0;
+  std::map<std::tuple<const void*, int, int, long long, int>, CUtensorMap> tmaps;
+  int* d_status = nullptr;
 };
 
 Context& ctx() {
@@ -103,6 +115,8 @@ bool enter(const int* x_min, const int* x_max, const int* y_min, const int* y_ma
     if (!check(cudaMalloc(&c.d_partials, summary_partials_len() * sizeof(double)), "malloc"))
       return false;
     if (!check(cudaMalloc(&c.d_sum, 5 * sizeof(double)), "malloc")) return false;
+    if (!check(cudaMalloc(&c.d_status, sizeof(int)), "malloc")) return false;
+    if (!check(cudaMemsetAsync(c.d_status, 0, sizeof(int), c.stream), "status clear")) return false;
     const char* pin = getenv("CLOVER_GPU_PIN_HOST");
     c.pin_host = !(pin && pin[0] == '0');
     c.ready = true;
@@ -127,6 +141,42 @@ bool is_device_pointer(const void* p) {
     return false;
   }
   return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+// The tensor map of a chunk-layout FP64 array with boxes of `rows` rows, made
+// on first use; null if the array cannot be staged (the driver refuses the
+// map, e.g. a device array passed in place whose base is not 16-byte aligned).
+const CUtensorMap* tmap(Context& c, const double* base, const Geom& g, int rows) {
+  if (!base) return nullptr;
+  const auto key = std::make_tuple((const void*)base, rows, g.px, g.pxy, g.z_max - g.z_min);
+  auto it = c.tmaps.find(key);
+  if (it != c.tmaps.end()) return &it->second;
+  CUtensorMap m;
+  if (!encode_plane_map(&m, base, 8, g, rows)) return nullptr;
+  return &(c.tmaps[key] = m);
+}
+
+// Whether the staged drop-in kernels may run: allowed, and set up once.
+bool staged(Context& c) {
+  if (!c.staging) return false;
+  if (c.tma_state == 0) c.tma_state = pdv_dropin_tma_prepare() ? 1 : -1;
+  if (c.tma_state < 0) cudaGetLastError();
+  return c.tma_state > 0;
+}
+
+// After a synchronisation of the library stream: a staged kernel's bounded
+// wait that gave up left a status bit on the device.
+void poll_device_status(Context& c) {
+  if (!c.d_status) return;
+  int st = 0;
+  if (cudaMemcpy(&st, c.d_status, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) {
+    cudaGetLastError();
+    return;
+  }
+  if (st) {
+    set_error(st, "a staged kernel's wait for its bulk copies gave up");
+    cudaMemset(c.d_status, 0, sizeof(int));
+  }
 }
 
 }  // namespace
@@ -570,6 +620,7 @@ void clover_calc_dt_kernel(const int* x_min, const int* x_max, const int* y_min,
   unsigned long long key = init;
   check(cudaMemcpyAsync(&key, c.d_key, sizeof(key), cudaMemcpyDeviceToHost, c.stream), "key");
   check(cudaStreamSynchronize(c.stream), "calc_dt sync");
+  poll_device_status(c);
   *dt_min_val = min_key_value(key);
   // calc_dt_kernel.f90:154-161: jkl_control is the constant 1.1 (a default
   // REAL), so these outputs never depend on the field.
@@ -602,9 +653,36 @@ void clover_pdv_kernel(const int32_t* predict, const int* x_min, const int* x_ma
   ENTER();
   GeomArrays ga = no_geom();
   ga.xarea = XF(xarea); ga.yarea = YF(yarea); ga.zarea = ZF(zarea); ga.volume = CELL(volume);
-  launch_pdv<F64>(g, c.stream, *predict != 0, *dt, nullptr, ga, CELL(density0), CELL(density1),
-                  CELL(energy0), CELL(energy1), CELL(pressure), CELL(viscosity), VERT(xvel0),
-                  VERT(xvel1), VERT(yvel0), VERT(yvel1), VERT(zvel0), VERT(zvel1));
+  double *d0 = CELL(density0), *d1 = CELL(density1), *e0 = CELL(energy0), *e1 = CELL(energy1);
+  double *pr = CELL(pressure), *vi = CELL(viscosity);
+  double *u0 = VERT(xvel0), *u1 = VERT(xvel1), *v0 = VERT(yvel0), *v1 = VERT(yvel1);
+  double *w0 = VERT(zvel0), *w1 = VERT(zvel1);
+  const bool pred = *predict != 0;
+  // the planes staged by bulk-tensor copies when every staged array has a map
+  // (the corrector's time level 1 velocities too)
+  if (staged(c)) {
+    const CUtensorMap* m[9] = {tmap(c, u0, g, 9), tmap(c, v0, g, 9), tmap(c, w0, g, 9),
+                               pred ? nullptr : tmap(c, u1, g, 9),
+                               pred ? nullptr : tmap(c, v1, g, 9),
+                               pred ? nullptr : tmap(c, w1, g, 9),
+                               tmap(c, ga.xarea, g, 8), tmap(c, ga.yarea, g, 9),
+                               tmap(c, ga.zarea, g, 8)};
+    bool ok = true;
+    for (int q = 0; q < 9; q++) ok = ok && (m[q] || (pred && q >= 3 && q <= 5));
+    if (ok) {
+      PdvDropMaps maps;
+      maps.u0 = *m[0]; maps.v0 = *m[1]; maps.w0 = *m[2];
+      if (!pred) { maps.u1 = *m[3]; maps.v1 = *m[4]; maps.w1 = *m[5]; }
+      else { maps.u1 = *m[0]; maps.v1 = *m[1]; maps.w1 = *m[2]; }
+      maps.xa = *m[6]; maps.ya = *m[7]; maps.za = *m[8];
+      launch_pdv_dropin_tma(g, c.stream, pred, *dt, maps, ga.volume, d0, d1, e0, e1, pr, vi,
+                            c.d_status);
+      check_launch("PdV");
+      return;
+    }
+  }
+  launch_pdv<F64>(g, c.stream, pred, *dt, nullptr, ga, d0, d1, e0, e1, pr, vi, u0, u1, v0, v1, w0,
+                  w1);
   check_launch("PdV");
 }
 
@@ -740,6 +818,7 @@ void clover_field_summary_kernel(const int* x_min, const int* x_max, const int* 
   double s[5] = {0, 0, 0, 0, 0};
   check(cudaMemcpyAsync(s, c.d_sum, sizeof(s), cudaMemcpyDeviceToHost, c.stream), "summary");
   check(cudaStreamSynchronize(c.stream), "summary sync");
+  poll_device_status(c);
   *vol = s[0]; *mass = s[1]; *ie = s[2]; *ke = s[3]; *press = s[4];
 }
 
@@ -968,6 +1047,8 @@ void clover_gpu_face_copy(const int* src_bounds, double* src, const int* dst_bou
 
 int clover_gpu_status(void) { return ctx().status; }
 
+void clover_gpu_use_staging(int on) { ctx().staging = on != 0; }
+
 const char* clover_gpu_error_string(void) { return ctx().err.c_str(); }
 
 void clover_gpu_clear_status(void) {
@@ -987,6 +1068,7 @@ void clover_gpu_sync_to_host(void) {
       xfer3d(kv.first, m, 0, m.planes, false);
   }
   check(cudaStreamSynchronize(c.stream), "sync_to_host");
+  poll_device_status(c);
 }
 
 void clover_gpu_invalidate(const void* host_array) {
@@ -1004,7 +1086,9 @@ void clover_gpu_invalidate_all(void) {
 
 void clover_gpu_synchronize(void) {
   Context& c = ctx();
-  if (c.ready) check(cudaStreamSynchronize(c.stream), "synchronize");
+  if (!c.ready) return;
+  check(cudaStreamSynchronize(c.stream), "synchronize");
+  poll_device_status(c);
 }
 
 void clover_gpu_release(void) {
@@ -1022,6 +1106,10 @@ void clover_gpu_release(void) {
   cudaFree(c.d_key);
   cudaFree(c.d_partials);
   cudaFree(c.d_sum);
+  cudaFree(c.d_status);
+  c.d_status = nullptr;
+  c.tmaps.clear();
+  c.tma_state = 0;
   cudaFree(c.stage);
   c.stage = nullptr;
   c.stage_bytes = 0;

@@ -902,6 +902,132 @@ k_pdv_flux_tma(Geom g, int seg, const double* __restrict__ dt_ptr,
 }
 
 // ---------------------------------------------------------------------------
+// PdV_kernel.f90:72-166 over the drop-in caller's arrays (the face areas and
+// the volume are arrays there, not the uniform mesh's constants), as k_pdv
+// (clover_kernels.cu) forms it. Plane p: the time level 0 node velocities of
+// node plane p (rows k0..k0+8; the corrector also the time level 1
+// velocities), xarea and zarea of plane p (rows k0..k0+7) and yarea (rows
+// k0..k0+8). Cell l reads node and z-face planes l, l+1 and the x/y-face
+// plane l; its own volume, density0, energy0, pressure and viscosity are
+// loaded one plane ahead into registers.
+template <bool PRED>
+struct PdvDropPlane {
+  static constexpr int kNv = PRED ? 3 : 6;
+  static constexpr int W = kTmaWidth<double>;
+  static constexpr int k9 = round128(9 * W * 8);
+  static constexpr int k8 = round128(8 * W * 8);
+  static constexpr int kBytes = kNv * k9 + k9 + 2 * k8;
+  static constexpr unsigned kTx = kNv * box_bytes<double>(9) + box_bytes<double>(9) +
+                                  2 * box_bytes<double>(8);
+  __device__ static double* vel(unsigned char* p, int q) { return (double*)(p + q * k9); }
+  __device__ static double* ya(unsigned char* p) { return (double*)(p + kNv * k9); }
+  __device__ static double* xa(unsigned char* p) { return (double*)(p + (kNv + 1) * k9); }
+  __device__ static double* za(unsigned char* p) { return (double*)(p + (kNv + 1) * k9 + k8); }
+};
+
+template <bool PRED, int RING, int MINB>
+__global__ void __launch_bounds__(TX * TY, MINB)
+k_pdv_dropin_tma(Geom g, int seg, double dt, const __grid_constant__ PdvDropMaps maps,
+                 const double* __restrict__ volume, const double* __restrict__ density0,
+                 double* __restrict__ density1, const double* __restrict__ energy0,
+                 double* __restrict__ energy1, const double* __restrict__ pressure,
+                 const double* __restrict__ viscosity, int* __restrict__ status) {
+  using P = PdvDropPlane<PRED>;
+  extern __shared__ __align__(128) unsigned char ring[];
+  __shared__ unsigned long long full[RING];
+  __shared__ int stop;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int j = g.x_min + TX * (int)blockIdx.x + tx, k0 = g.y_min + TY * (int)blockIdx.y;
+  const int k = k0 + ty;
+  const int l0 = g.z_min + seg * (int)blockIdx.z;
+  const int l1 = l0 + seg - 1 < g.z_max ? l0 + seg - 1 : g.z_max;
+  const bool in_jk = j <= g.x_max && k <= g.y_max;
+  const PlaneMarch<RING, 0, 1> pm{ring, P::kBytes, full, &stop, l0, l1 + 1};
+  constexpr int W = P::W, H = kTmaHalo<double>;
+  double c_v = 0, c_d = 0, c_e = 0, c_p = 0, c_q = 0;
+  auto fetch = [&](int l) {
+    if (in_jk && l <= l1) {
+      const long long o = off3(g, j, k, l);
+      c_v = __ldg(&volume[o]);
+      c_d = __ldg(&density0[o]);
+      c_e = __ldg(&energy0[o]);
+      c_p = __ldg(&pressure[o]);
+      c_q = __ldg(&viscosity[o]);
+    }
+  };
+  fetch(l0);
+  auto issue = [&](int p) {
+    unsigned char* b = pm.buf(p);
+    unsigned long long* bar = pm.bar(p);
+    mbar_arrive_expect_tx(bar, P::kTx);
+    const int x = TX * (int)blockIdx.x, y = k0 - g.y_min + 2, z = p - g.z_min + 2;
+    tma_load_box(P::vel(b, 0), &maps.u0, bar, x, y, z);
+    tma_load_box(P::vel(b, 1), &maps.v0, bar, x, y, z);
+    tma_load_box(P::vel(b, 2), &maps.w0, bar, x, y, z);
+    if (!PRED) {
+      tma_load_box(P::vel(b, 3), &maps.u1, bar, x, y, z);
+      tma_load_box(P::vel(b, 4), &maps.v1, bar, x, y, z);
+      tma_load_box(P::vel(b, 5), &maps.w1, bar, x, y, z);
+    }
+    tma_load_box(P::ya(b), &maps.ya, bar, x, y, z);
+    tma_load_box(P::xa(b), &maps.xa, bar, x, y, z);
+    tma_load_box(P::za(b), &maps.za, bar, x, y, z);
+  };
+  pm.run(l0, l1, status, issue, [&](int l) {
+    if (!in_jk) return;
+    const double vol = c_v, d0 = c_d, e0 = c_e, pr = c_p, vi = c_q;
+    fetch(l + 1);
+    unsigned char* bl = pm.buf(l);
+    unsigned char* bu = pm.buf(l + 1);
+    // velocity q of node (j+a, k+b) of a node plane buffer; the predictor's
+    // second set is time level 0 again
+#define NV(bb, q, a, b) (P::vel(bb, q)[(ty + (b)) * W + tx + H + (a)])
+    constexpr int q1 = PRED ? 0 : 3;
+    auto xsum = [&](int a) {
+      return NV(bl, 0, a, 0) + NV(bl, 0, a, 1) + NV(bu, 0, a, 0) + NV(bu, 0, a, 1) +
+             NV(bl, q1, a, 0) + NV(bl, q1, a, 1) + NV(bu, q1, a, 0) + NV(bu, q1, a, 1);
+    };
+    auto ysum = [&](int b) {
+      return NV(bl, 1, 0, b) + NV(bl, 1, 1, b) + NV(bu, 1, 0, b) + NV(bu, 1, 1, b) +
+             NV(bl, q1 + 1, 0, b) + NV(bl, q1 + 1, 1, b) + NV(bu, q1 + 1, 0, b) +
+             NV(bu, q1 + 1, 1, b);
+    };
+    auto zsum = [&](unsigned char* bb) {
+      return NV(bb, 2, 0, 0) + NV(bb, 2, 1, 0) + NV(bb, 2, 0, 1) + NV(bb, 2, 1, 1) +
+             NV(bb, q1 + 2, 0, 0) + NV(bb, q1 + 2, 1, 0) + NV(bb, q1 + 2, 0, 1) +
+             NV(bb, q1 + 2, 1, 1);
+    };
+#undef NV
+    const double xa0 = P::xa(bl)[ty * W + tx + H], xa1 = P::xa(bl)[ty * W + tx + H + 1];
+    const double ya0 = P::ya(bl)[ty * W + tx + H], ya1 = P::ya(bl)[(ty + 1) * W + tx + H];
+    const double za0 = P::za(bl)[ty * W + tx + H], za1 = P::za(bu)[ty * W + tx + H];
+    double left_flux, right_flux, bottom_flux, top_flux, back_flux, front_flux;
+    if (PRED) {
+      left_flux = (xa0 * xsum(0)) * 0.125 * dt * 0.5;
+      right_flux = (xa1 * xsum(1)) * 0.125 * dt * 0.5;
+      bottom_flux = (ya0 * ysum(0)) * 0.125 * dt * 0.5;
+      top_flux = (ya1 * ysum(1)) * 0.125 * dt * 0.5;
+      back_flux = (za0 * zsum(bl)) * 0.125 * dt * 0.5;
+      front_flux = (za1 * zsum(bu)) * 0.125 * dt * 0.5;
+    } else {
+      left_flux = (xa0 * xsum(0)) * 0.125 * dt;
+      right_flux = (xa1 * xsum(1)) * 0.125 * dt;
+      bottom_flux = (ya0 * ysum(0)) * 0.125 * dt;
+      top_flux = (ya1 * ysum(1)) * 0.125 * dt;
+      back_flux = (za0 * zsum(bl)) * 0.125 * dt;
+      front_flux = (za1 * zsum(bu)) * 0.125 * dt;
+    }
+    const double total_flux = right_flux - left_flux + top_flux - bottom_flux + front_flux - back_flux;
+    const double vol_change_s = vol / (vol + total_flux);
+    const double recip_volume = 1.0 / vol;
+    const double energy_change = (pr / d0 + vi / d0) * total_flux * recip_volume;
+    const long long o = off3(g, j, k, l);
+    energy1[o] = e0 - energy_change;
+    density1[o] = d0 * vol_change_s;
+  });
+}
+
+// ---------------------------------------------------------------------------
 // The node pass of the y or z momentum sweep (advec_mom_kernel.f90:254-293 for
 // y, :339-379 for z), as k_mom_node_march (clover_fused.cu) forms it, with the
 // inputs staged in shared memory. The lane layout stays: lane L of a warp holds
@@ -1488,6 +1614,39 @@ bool stencils_tma_prepare() {
          cudaFuncSetAttribute(k_pdv_flux_tma<S, kStencilRing, kStencilMinBlocks<S>>,
                               cudaFuncAttributeMaxDynamicSharedMemorySize,
                               kStencilRing * FluxPlane<S>::kBytes) == cudaSuccess;
+}
+
+// blocks per SM of the drop-in PdV: the corrector's plane (six velocity
+// boxes and three area boxes, 23 KB) leaves room for two blocks of a
+// four-plane ring, the predictor's for three
+template <bool PRED>
+constexpr int kPdvDropMinBlocks = PRED ? 3 : 2;
+
+bool pdv_dropin_tma_prepare() {
+  return cudaFuncSetAttribute(k_pdv_dropin_tma<true, kStencilRing, kPdvDropMinBlocks<true>>,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              kStencilRing * PdvDropPlane<true>::kBytes) == cudaSuccess &&
+         cudaFuncSetAttribute(k_pdv_dropin_tma<false, kStencilRing, kPdvDropMinBlocks<false>>,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              kStencilRing * PdvDropPlane<false>::kBytes) == cudaSuccess;
+}
+
+void launch_pdv_dropin_tma(const Geom& g, cudaStream_t s, bool predict, double dt,
+                           const PdvDropMaps& maps, const double* volume, const double* density0,
+                           double* density1, const double* energy0, double* energy1,
+                           const double* pressure, const double* viscosity, int* status) {
+  const dim3 grid((g.x_max - g.x_min + TX) / TX, (g.y_max - g.y_min + TY) / TY,
+                  (g.z_max - g.z_min + kStencilSeg) / kStencilSeg);
+  if (predict)
+    k_pdv_dropin_tma<true, kStencilRing, kPdvDropMinBlocks<true>>
+        <<<grid, dim3(TX, TY), kStencilRing * PdvDropPlane<true>::kBytes, s>>>(
+            g, kStencilSeg, dt, maps, volume, density0, density1, energy0, energy1, pressure,
+            viscosity, status);
+  else
+    k_pdv_dropin_tma<false, kStencilRing, kPdvDropMinBlocks<false>>
+        <<<grid, dim3(TX, TY), kStencilRing * PdvDropPlane<false>::kBytes, s>>>(
+            g, kStencilSeg, dt, maps, volume, density0, density1, energy0, energy1, pressure,
+            viscosity, status);
 }
 
 template <class S>

@@ -91,6 +91,20 @@ void launch_pdv_flux_tma(const Geom& g, cudaStream_t s, const double* dt_ptr, co
                          typename S::vf_t* vol_flux_x, typename S::vf_t* vol_flux_y,
                          typename S::vf_t* vol_flux_z, int* status);
 
+// The maps of the drop-in PdV (clover_pdv_kernel over the caller's arrays):
+// time level 0 and (corrector) time level 1 node velocities and yarea, 9
+// rows; xarea and zarea, 8 rows.
+struct PdvDropMaps {
+  CUtensorMap u0, v0, w0, u1, v1, w1, xa, ya, za;
+};
+bool pdv_dropin_tma_prepare();
+// PdV_kernel.f90:72-166 (predict or correct) over the caller's arrays, planes
+// staged by bulk-tensor copies; FP64, one chunk.
+void launch_pdv_dropin_tma(const Geom& g, cudaStream_t s, bool predict, double dt,
+                           const PdvDropMaps& maps, const double* volume, const double* density0,
+                           double* density1, const double* energy0, double* energy1,
+                           const double* pressure, const double* viscosity, int* status);
+
 // The maps of the y/z momentum node pass: mass flux of the sweep direction
 // and density1 (9 rows from c0-1), and the volume fluxes its post volumes
 // take (vol_flux_x 9 rows, the row-direction flux 10 rows: vol_flux_y for

@@ -335,6 +335,11 @@ void clover_gpu_invalidate(const void *host_array);
 void clover_gpu_invalidate_all(void);
 /* Wait for all queued work. */
 void clover_gpu_synchronize(void);
+/* Allow (1, the default) or forbid (0) the staged forms of the kernels that
+ * have one (planes copied into shared memory by bulk-tensor copies): both
+ * forms give the same bits. A staged kernel whose bounded wait for its copies
+ * gives up sets CLOVER_STATUS_TIMEOUT, seen at the next synchronisation. */
+void clover_gpu_use_staging(int on);
 /* Free every mirror and the library stream. */
 void clover_gpu_release(void);
 /* Chunk layout for device pointers passed in place: element (j,k,l) is at

@@ -77,8 +77,19 @@ def gpu_lockstep(d, steps, snaps):
     return scal
 
 
+@pytest.mark.parametrize("staging", [True, False])
 @pytest.mark.parametrize("case", ["shock_11x7x6", "mixed_9x8x10", "thin_5x1x3", "tp1_10x2x2"])
-def test_kernel_by_kernel_bitwise(case):
+def test_kernel_by_kernel_bitwise(case, staging):
+    """Every array after every call, with the staged drop-in forms (planes
+    copied into shared memory by bulk-tensor copies) allowed and forbidden."""
+    C.lib().clover_gpu_use_staging(1 if staging else 0)
+    try:
+        _kernel_by_kernel(case)
+    finally:
+        C.lib().clover_gpu_use_staging(1)
+
+
+def _kernel_by_kernel(case):
     d = {
         "shock_11x7x6": decks.shock(11, 7, 6, 3),
         "mixed_9x8x10": decks.shock(9, 8, 10, 2, states=decks.MIXED_STATES),
