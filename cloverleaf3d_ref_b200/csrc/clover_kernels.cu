@@ -884,52 +884,55 @@ __global__ void __launch_bounds__(BX * BY) k_mom_vol(Geom g, Box b, int variant,
   E(pre_vol, j, k, l) = st<W>(pre);
 }
 
-// node_flux (:166-176 x, :254-263 y, :339-349 z) and node_mass_post
-// (:177-193, :264-279, :350-365) over the union of their ranges.
+// node_flux (:166-176 x, :254-263 y, :339-349 z), node_mass_post
+// (:177-193, :264-279, :350-365) and node_mass_pre (:194-202, :280-288,
+// :366-374) over the union of their ranges, one pass: a node of the mass
+// range forms the node flux of its lower neighbour along the sweep again (the
+// same sum, so the same bits) for its node_mass_pre.
+template <class S, int DIR>
+__device__ __forceinline__ double node_flux_at(const Geom& g, const typename S::mf_t* __restrict__ mf,
+                                               int j, int k, int l) {
+  if (DIR == 1)
+    return 0.125 * (L(mf, j, k - 1, l) + L(mf, j, k, l) + L(mf, j + 1, k - 1, l) + L(mf, j + 1, k, l) +
+                    L(mf, j, k - 1, l - 1) + L(mf, j, k, l - 1) + L(mf, j + 1, k - 1, l - 1) +
+                    L(mf, j + 1, k, l - 1));
+  if (DIR == 2)
+    return 0.125 * (L(mf, j - 1, k, l) + L(mf, j, k, l) + L(mf, j - 1, k + 1, l) + L(mf, j, k + 1, l) +
+                    L(mf, j - 1, k, l - 1) + L(mf, j, k, l - 1) + L(mf, j - 1, k + 1, l - 1) +
+                    L(mf, j, k + 1, l - 1));
+  return 0.125 * (L(mf, j - 1, k, l) + L(mf, j, k, l) + L(mf, j - 1, k, l + 1) + L(mf, j, k, l + 1) +
+                  L(mf, j - 1, k - 1, l) + L(mf, j, k - 1, l) + L(mf, j - 1, k - 1, l + 1) +
+                  L(mf, j, k - 1, l + 1));
+}
+
 template <class S, int DIR>
 __global__ void __launch_bounds__(BX * BY) k_mom_node(Geom g, Box b, Box bflux, Box bmass,
     const typename S::mf_t* __restrict__ mf, const typename S::rho_t* __restrict__ density1,
     const typename S::wk_t* __restrict__ post_vol, typename S::wk_t* __restrict__ node_flux,
-    typename S::wk_t* __restrict__ node_mass_post) {
+    typename S::wk_t* __restrict__ node_mass_post, typename S::wk_t* __restrict__ node_mass_pre) {
   BOX_THREAD(b);
   using W = typename S::wk_t;
-  if (j >= bflux.j0 && j <= bflux.j1 && k >= bflux.k0 && k <= bflux.k1 && l >= bflux.l0 &&
-      l <= bflux.l1) {
-    double nf;
-    if (DIR == 1)
-      nf = 0.125 * (L(mf, j, k - 1, l) + L(mf, j, k, l) + L(mf, j + 1, k - 1, l) + L(mf, j + 1, k, l) +
-                    L(mf, j, k - 1, l - 1) + L(mf, j, k, l - 1) + L(mf, j + 1, k - 1, l - 1) +
-                    L(mf, j + 1, k, l - 1));
-    else if (DIR == 2)
-      nf = 0.125 * (L(mf, j - 1, k, l) + L(mf, j, k, l) + L(mf, j - 1, k + 1, l) + L(mf, j, k + 1, l) +
-                    L(mf, j - 1, k, l - 1) + L(mf, j, k, l - 1) + L(mf, j - 1, k + 1, l - 1) +
-                    L(mf, j, k + 1, l - 1));
-    else
-      nf = 0.125 * (L(mf, j - 1, k, l) + L(mf, j, k, l) + L(mf, j - 1, k, l + 1) + L(mf, j, k, l + 1) +
-                    L(mf, j - 1, k - 1, l) + L(mf, j, k - 1, l) + L(mf, j - 1, k - 1, l + 1) +
-                    L(mf, j, k - 1, l + 1));
-    E(node_flux, j, k, l) = st<W>(nf);
+  const bool in_flux = j >= bflux.j0 && j <= bflux.j1 && k >= bflux.k0 && k <= bflux.k1 &&
+                       l >= bflux.l0 && l <= bflux.l1;
+  const bool in_mass = j >= bmass.j0 && j <= bmass.j1 && k >= bmass.k0 && k <= bmass.k1 &&
+                       l >= bmass.l0 && l <= bmass.l1;
+  double nf = 0.0;
+  if (in_flux || in_mass) {
+    nf = (double)st<W>(node_flux_at<S, DIR>(g, mf, j, k, l));
+    if (in_flux) E(node_flux, j, k, l) = st<W>(nf);
   }
-  if (j >= bmass.j0 && j <= bmass.j1 && k >= bmass.k0 && k <= bmass.k1 && l >= bmass.l0 &&
-      l <= bmass.l1) {
+  if (in_mass) {
 #define DP(a, bb, c) (L(density1, j + (a), k + (bb), l + (c)) * L(post_vol, j + (a), k + (bb), l + (c)))
-    const double nm = 0.125 * (DP(0, -1, 0) + DP(0, 0, 0) + DP(-1, -1, 0) + DP(-1, 0, 0) +
-                               DP(0, -1, -1) + DP(0, 0, -1) + DP(-1, -1, -1) + DP(-1, 0, -1));
+    const double nm = (double)st<W>(0.125 * (DP(0, -1, 0) + DP(0, 0, 0) + DP(-1, -1, 0) + DP(-1, 0, 0) +
+                                             DP(0, -1, -1) + DP(0, 0, -1) + DP(-1, -1, -1) + DP(-1, 0, -1)));
 #undef DP
     E(node_mass_post, j, k, l) = st<W>(nm);
+    // the lower neighbour's node flux (inside the flux range for every mass node)
+    const double prev = (double)st<W>(DIR == 1 ? node_flux_at<S, DIR>(g, mf, j - 1, k, l)
+                                      : DIR == 2 ? node_flux_at<S, DIR>(g, mf, j, k - 1, l)
+                                                 : node_flux_at<S, DIR>(g, mf, j, k, l - 1));
+    E(node_mass_pre, j, k, l) = st<W>(nm - prev + nf);
   }
-}
-
-// node_mass_pre (:194-202 x, :280-288 y, :366-374 z)
-template <class S, int DIR>
-__global__ void __launch_bounds__(BX * BY) k_mom_nmpre(Geom g, Box b,
-    const typename S::wk_t* __restrict__ node_flux, const typename S::wk_t* __restrict__ node_mass_post,
-    typename S::wk_t* __restrict__ node_mass_pre) {
-  BOX_THREAD(b);
-  const double prev = DIR == 1 ? L(node_flux, j - 1, k, l)
-                    : DIR == 2 ? L(node_flux, j, k - 1, l) : L(node_flux, j, k, l - 1);
-  E(node_mass_pre, j, k, l) =
-      st<typename S::wk_t>(L(node_mass_post, j, k, l) - prev + L(node_flux, j, k, l));
 }
 
 __device__ __forceinline__ double mom_limiter(double sigma, double width, double celld_dif,
@@ -1668,22 +1671,19 @@ void launch_advec_mom(const Geom& g, cudaStream_t s, typename S::vel_t* vel1,
     if (which_vel == 1) {
       const Box bf{x0 - 2, x1 + 2, y0, y1 + 1, z0, z1 + 1}, bm{x0 - 1, x1 + 2, y0, y1 + 1, z0, z1 + 1};
       LAUNCH((k_mom_node<S, 1>), box_union(bf, bm), bf, bm, mass_flux_x, density1, post_vol,
-             node_flux, node_mass_post);
-      LAUNCH((k_mom_nmpre<S, 1>), bm, node_flux, node_mass_post, node_mass_pre);
+             node_flux, node_mass_post, node_mass_pre);
     }
   } else if (direction == 2) {
     if (which_vel == 1) {
       const Box bf{x0, x1 + 1, y0 - 2, y1 + 2, z0, z1 + 1}, bm{x0, x1 + 1, y0 - 1, y1 + 2, z0, z1 + 1};
       LAUNCH((k_mom_node<S, 2>), box_union(bf, bm), bf, bm, mass_flux_y, density1, post_vol,
-             node_flux, node_mass_post);
-      LAUNCH((k_mom_nmpre<S, 2>), bm, node_flux, node_mass_post, node_mass_pre);
+             node_flux, node_mass_post, node_mass_pre);
     }
   } else if (direction == 3) {
     if (which_vel == 1) {
       const Box bf{x0, x1 + 1, y0, y1 + 1, z0 - 2, z1 + 2}, bm{x0, x1 + 1, y0, y1 + 1, z0 - 1, z1 + 2};
       LAUNCH((k_mom_node<S, 3>), box_union(bf, bm), bf, bm, mass_flux_z, density1, post_vol,
-             node_flux, node_mass_post);
-      LAUNCH((k_mom_nmpre<S, 3>), bm, node_flux, node_mass_post, node_mass_pre);
+             node_flux, node_mass_post, node_mass_pre);
     }
   }
   // the flux at nodes min-1..max+1 and the update of nodes min..max+1 along
