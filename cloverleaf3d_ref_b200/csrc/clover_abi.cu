@@ -156,10 +156,23 @@ const CUtensorMap* tmap(Context& c, const double* base, const Geom& g, int rows)
   return &(c.tmaps[key] = m);
 }
 
+// The maps of n arrays (base, box rows) into out[], in order; false if any
+// array has none.
+bool tmaps_of(Context& c, const Geom& g, int n, const double* const* base, const int* rows,
+              CUtensorMap* out) {
+  for (int q = 0; q < n; q++) {
+    const CUtensorMap* m = tmap(c, base[q], g, rows[q]);
+    if (!m) return false;
+    out[q] = *m;
+  }
+  return true;
+}
+
 // Whether the staged drop-in kernels may run: allowed, and set up once.
 bool staged(Context& c) {
   if (!c.staging) return false;
-  if (c.tma_state == 0) c.tma_state = pdv_dropin_tma_prepare() ? 1 : -1;
+  if (c.tma_state == 0)
+    c.tma_state = pdv_dropin_tma_prepare() && stencils_dropin_tma_prepare() ? 1 : -1;
   if (c.tma_state < 0) cudaGetLastError();
   return c.tma_state > 0;
 }
@@ -586,8 +599,22 @@ void clover_viscosity_kernel(const int* x_min, const int* x_max, const int* y_mi
   GeomArrays ga = no_geom();
   ga.xarea = XF(xarea); ga.yarea = YF(yarea); ga.zarea = ZF(zarea);
   ga.celldx = CX(celldx); ga.celldy = CY(celldy); ga.celldz = CZ(celldz);
-  launch_viscosity<F64>(g, c.stream, ga, CELL(density0), CELL(pressure), CELL(viscosity),
-                        VERT(xvel0), VERT(yvel0), VERT(zvel0));
+  double *d0 = CELL(density0), *pr = CELL(pressure), *vi = CELL(viscosity);
+  double *u0 = VERT(xvel0), *v0 = VERT(yvel0), *w0 = VERT(zvel0);
+  if (staged(c)) {
+    const double* base[8] = {u0, v0, w0, pr, ga.xarea, ga.yarea, ga.zarea, d0};
+    const int rows[8] = {9, 9, 9, 10, 8, 8, 8, 8};
+    CUtensorMap m[8];
+    if (tmaps_of(c, g, 8, base, rows, m)) {
+      ViscDropMaps maps;
+      maps.u = m[0]; maps.v = m[1]; maps.w = m[2]; maps.p = m[3];
+      maps.xa = m[4]; maps.ya = m[5]; maps.za = m[6]; maps.d = m[7];
+      launch_viscosity_dropin_tma(g, c.stream, ga, maps, vi, c.d_status);
+      check_launch("viscosity");
+      return;
+    }
+  }
+  launch_viscosity<F64>(g, c.stream, ga, d0, pr, vi, u0, v0, w0);
   check_launch("viscosity");
 }
 
@@ -613,9 +640,25 @@ void clover_calc_dt_kernel(const int* x_min, const int* x_max, const int* y_min,
   ga.volume = CELL(volume);
   const unsigned long long init = min_key_of(*g_big);
   check(cudaMemcpyAsync(c.d_key, &init, sizeof(init), cudaMemcpyHostToDevice, c.stream), "key");
-  launch_calc_dt<F64>(g, c.stream, ga, *g_small, *dtc_safe, *dtu_safe, *dtv_safe, *dtw_safe,
-                      *dtdiv_safe, CELL(density0), CELL(viscosity_a), CELL(soundspeed),
-                      VERT(xvel0), VERT(yvel0), VERT(zvel0), VERT(dt_min), c.d_key);
+  double *d0 = CELL(density0), *qa = CELL(viscosity_a), *ss = CELL(soundspeed);
+  double *u0 = VERT(xvel0), *v0 = VERT(yvel0), *w0 = VERT(zvel0), *dtm = VERT(dt_min);
+  bool done = false;
+  if (staged(c)) {
+    const double* base[10] = {u0, v0, w0, ss, qa, d0, ga.volume, ga.xarea, ga.yarea, ga.zarea};
+    const int rows[10] = {9, 9, 9, 8, 8, 8, 8, 8, 8, 8};
+    CUtensorMap m[10];
+    if (tmaps_of(c, g, 10, base, rows, m)) {
+      DtDropMaps maps;
+      maps.u = m[0]; maps.v = m[1]; maps.w = m[2]; maps.ss = m[3]; maps.q = m[4];
+      maps.d = m[5]; maps.vol = m[6]; maps.xa = m[7]; maps.ya = m[8]; maps.za = m[9];
+      launch_calc_dt_dropin_tma(g, c.stream, ga, *g_small, *dtc_safe, *dtu_safe, *dtv_safe,
+                                *dtw_safe, *dtdiv_safe, maps, dtm, c.d_key, c.d_status);
+      done = true;
+    }
+  }
+  if (!done)
+    launch_calc_dt<F64>(g, c.stream, ga, *g_small, *dtc_safe, *dtu_safe, *dtv_safe, *dtw_safe,
+                        *dtdiv_safe, d0, qa, ss, u0, v0, w0, dtm, c.d_key);
   check_launch("calc_dt");
   unsigned long long key = init;
   check(cudaMemcpyAsync(&key, c.d_key, sizeof(key), cudaMemcpyDeviceToHost, c.stream), "key");
@@ -704,9 +747,23 @@ void clover_accelerate_kernel(const int* x_min, const int* x_max, const int* y_m
   ENTER();
   GeomArrays ga = no_geom();
   ga.xarea = XF(xarea); ga.yarea = YF(yarea); ga.zarea = ZF(zarea); ga.volume = CELL(volume);
-  launch_accelerate<F64>(g, c.stream, *dt, nullptr, ga, CELL(density0), CELL(pressure),
-                         CELL(viscosity), VERT(xvel0), VERT(yvel0), VERT(zvel0), VERT(xvel1),
-                         VERT(yvel1), VERT(zvel1));
+  double *d0 = CELL(density0), *pr = CELL(pressure), *vi = CELL(viscosity);
+  double *u0 = VERT(xvel0), *v0 = VERT(yvel0), *w0 = VERT(zvel0);
+  double *u1 = VERT(xvel1), *v1 = VERT(yvel1), *w1 = VERT(zvel1);
+  if (staged(c)) {
+    const double* base[10] = {d0, ga.volume, pr, vi, ga.xarea, ga.zarea, ga.yarea, u0, v0, w0};
+    const int rows[10] = {9, 9, 9, 9, 9, 9, 8, 8, 8, 8};
+    CUtensorMap m[10];
+    if (tmaps_of(c, g, 10, base, rows, m)) {
+      AccDropMaps maps;
+      maps.d = m[0]; maps.vol = m[1]; maps.p = m[2]; maps.q = m[3]; maps.xa = m[4];
+      maps.za = m[5]; maps.ya = m[6]; maps.u = m[7]; maps.v = m[8]; maps.w = m[9];
+      launch_accelerate_dropin_tma(g, c.stream, *dt, maps, u1, v1, w1, c.d_status);
+      check_launch("accelerate");
+      return;
+    }
+  }
+  launch_accelerate<F64>(g, c.stream, *dt, nullptr, ga, d0, pr, vi, u0, v0, w0, u1, v1, w1);
   check_launch("accelerate");
 }
 

@@ -1028,6 +1028,358 @@ k_pdv_dropin_tma(Geom g, int seg, double dt, const __grid_constant__ PdvDropMaps
 }
 
 // ---------------------------------------------------------------------------
+// The other one-cell-per-thread stencils of the drop-in over the caller's
+// arrays, staged the same way (FP64, one chunk): a box per array and plane,
+// the boxes a plane's cells or nodes do not read left out (their bytes are
+// not expected on the plane's barrier).
+constexpr int kDropW = kTmaWidth<double>, kDropH = kTmaHalo<double>;
+constexpr int kBox8 = round128(8 * kDropW * 8), kBox9 = round128(9 * kDropW * 8);
+constexpr int kBox10 = round128(10 * kDropW * 8);
+
+// calc_dt_kernel.f90:102-149 as k_calc_dt forms it. Plane p: the node
+// velocities of node plane p (rows k0..k0+8) and, for cell plane p, the sound
+// speed, viscosity, density0, volume and the three face areas (rows
+// k0..k0+7; not on the last node plane). Cell l reads planes l and l+1.
+struct DtDropPlane {
+  static constexpr int kBytes = 3 * kBox9 + 7 * kBox8;
+  static constexpr unsigned kTxVel = 3 * box_bytes<double>(9);
+  static constexpr unsigned kTxCell = 7 * box_bytes<double>(8);
+  __device__ static double* vel(unsigned char* p, int q) { return (double*)(p + q * kBox9); }
+  // 0 soundspeed, 1 viscosity, 2 density0, 3 volume, 4 xarea, 5 yarea, 6 zarea
+  __device__ static double* cell(unsigned char* p, int q) {
+    return (double*)(p + 3 * kBox9 + q * kBox8);
+  }
+};
+
+template <int RING, int MINB>
+__global__ void __launch_bounds__(TX * TY, MINB)
+k_calc_dt_dropin_tma(Geom g, int seg, GeomArrays ga, double g_small, double dtc_safe,
+                     double dtu_safe, double dtv_safe, double dtw_safe, double dtdiv_safe,
+                     const __grid_constant__ DtDropMaps maps, double* __restrict__ dt_min,
+                     unsigned long long* __restrict__ min_key, int* __restrict__ status) {
+  using P = DtDropPlane;
+  extern __shared__ __align__(128) unsigned char ring[];
+  __shared__ unsigned long long full[RING];
+  __shared__ unsigned long long wmin[TX * TY / 32];
+  __shared__ int stop;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int j = g.x_min + TX * (int)blockIdx.x + tx, k0 = g.y_min + TY * (int)blockIdx.y;
+  const int k = k0 + ty;
+  const int l0 = g.z_min + seg * (int)blockIdx.z;
+  const int l1 = l0 + seg - 1 < g.z_max ? l0 + seg - 1 : g.z_max;
+  const bool in_jk = j <= g.x_max && k <= g.y_max;
+  const PlaneMarch<RING, 0, 1> pm{ring, P::kBytes, full, &stop, l0, l1 + 1};
+  constexpr int W = kDropW, H = kDropH;
+  auto issue = [&](int p) {
+    unsigned char* b = pm.buf(p);
+    unsigned long long* bar = pm.bar(p);
+    const bool cells = p <= l1;
+    mbar_arrive_expect_tx(bar, P::kTxVel + (cells ? P::kTxCell : 0u));
+    const int x = TX * (int)blockIdx.x, y = k0 - g.y_min + 2, z = p - g.z_min + 2;
+    tma_load_box(P::vel(b, 0), &maps.u, bar, x, y, z);
+    tma_load_box(P::vel(b, 1), &maps.v, bar, x, y, z);
+    tma_load_box(P::vel(b, 2), &maps.w, bar, x, y, z);
+    if (cells) {
+      tma_load_box(P::cell(b, 0), &maps.ss, bar, x, y, z);
+      tma_load_box(P::cell(b, 1), &maps.q, bar, x, y, z);
+      tma_load_box(P::cell(b, 2), &maps.d, bar, x, y, z);
+      tma_load_box(P::cell(b, 3), &maps.vol, bar, x, y, z);
+      tma_load_box(P::cell(b, 4), &maps.xa, bar, x, y, z);
+      tma_load_box(P::cell(b, 5), &maps.ya, bar, x, y, z);
+      tma_load_box(P::cell(b, 6), &maps.za, bar, x, y, z);
+    }
+  };
+  unsigned long long key = ~0ull;
+  const double cdx = in_jk ? ga.celldx[g.o1 + j - g.x_min + 2] : 1.0;
+  const double cdy = in_jk ? ga.celldy[g.o1 + k - g.y_min + 2] : 1.0;
+  pm.run(l0, l1, status, issue, [&](int l) {
+    if (!in_jk) return;
+    unsigned char* bl = pm.buf(l);
+    unsigned char* bu = pm.buf(l + 1);
+    const int c = ty * W + tx + H;
+#define NV(bb, q, a, b) (P::vel(bb, q)[(ty + (b)) * W + tx + H + (a)])
+    const double m = fmin2(fmin2(cdx, cdy), ga.celldz[g.o1 + l - g.z_min + 2]);
+    const double ds = 1.0 / (m * m);
+    const double ss = P::cell(bl, 0)[c];
+    double cc = ss * ss;
+    cc = cc + 2.0 * P::cell(bl, 1)[c] / P::cell(bl, 2)[c];
+    double dtct = ds * cc;
+    dtct = dtc_safe * 1.0 / fmax2(sqrt(dtct), g_small);
+    const double vol = P::cell(bl, 3)[c];
+    const double xa = P::cell(bl, 4)[c];
+    const double du1 = (NV(bl, 0, 0, 0) + NV(bl, 0, 0, 1) + NV(bu, 0, 0, 0) + NV(bu, 0, 0, 1)) * xa;
+    const double du2 = (NV(bl, 0, 1, 0) + NV(bl, 0, 1, 1) + NV(bu, 0, 1, 0) + NV(bu, 0, 1, 1)) * xa;
+    const double dtut = dtu_safe * 4.0 * vol / fmax2(fmax2(fabs(du1), fabs(du2)), 1.0e-5 * vol);
+    const double ya = P::cell(bl, 5)[c];
+    const double dv1 = (NV(bl, 1, 0, 0) + NV(bl, 1, 1, 0) + NV(bu, 1, 0, 0) + NV(bu, 1, 1, 0)) * ya;
+    const double dv2 = (NV(bl, 1, 0, 1) + NV(bl, 1, 1, 1) + NV(bu, 1, 0, 1) + NV(bu, 1, 1, 1)) * ya;
+    const double dtvt = dtv_safe * 4.0 * vol / fmax2(fmax2(fabs(dv1), fabs(dv2)), 1.0e-5 * vol);
+    const double za = P::cell(bl, 6)[c];  // both z faces use zarea(j,k,l)
+    const double dw1 = (NV(bl, 2, 0, 0) + NV(bl, 2, 0, 1) + NV(bl, 2, 1, 0) + NV(bl, 2, 1, 1)) * za;
+    const double dw2 = (NV(bu, 2, 0, 0) + NV(bu, 2, 0, 1) + NV(bu, 2, 1, 0) + NV(bu, 2, 1, 1)) * za;
+    const double dtwt = dtw_safe * 4.0 * vol / fmax2(fmax2(fabs(dw1), fabs(dw2)), 1.0e-5 * vol);
+#undef NV
+    const double div = du2 - du1 + dv2 - dv1 + dw2 - dw1;
+    const double dtdivt = dtdiv_safe * 4.0 * vol / fmax2(vol * 1.0e-05, fabs(div));
+    const double mn = fmin2(fmin2(fmin2(fmin2(dtct, dtut), dtvt), dtwt), dtdivt);
+    if (dt_min) dt_min[off3(g, j, k, l)] = mn;
+    if (!(mn != mn)) {
+      const unsigned long long kc = key_of(mn);
+      key = kc < key ? kc : key;
+    }
+  });
+  if (stop) return;
+  // warp then block minimum, one atomic per block
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    unsigned long long other = __shfl_xor_sync(0xffffffffu, key, o);
+    key = other < key ? other : key;
+  }
+  if (tx == 0) wmin[ty] = key;
+  __syncthreads();
+  if (ty == 0) {
+    key = tx < TY ? wmin[tx] : ~0ull;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      unsigned long long other = __shfl_xor_sync(0xffffffffu, key, o);
+      key = other < key ? other : key;
+    }
+    if (tx == 0 && key != ~0ull) atomicMin(min_key, key);
+  }
+}
+
+// viscosity_kernel.f90:71-134 as k_viscosity forms it (the strain terms,
+// pressure gradients and limiter of compressing cells only). Plane p: the node
+// velocities of node plane p (rows k0..k0+8), the pressure of cell plane p
+// (rows k0-1..k0+8), and for cell plane p the three face areas and density0
+// (rows k0..k0+7). Cell l reads node planes l, l+1 and pressure planes
+// l-1..l+1; plane l0-1 carries the pressure only, plane l1+1 no cell boxes.
+struct ViscDropPlane {
+  static constexpr int kBytes = 3 * kBox9 + kBox10 + 4 * kBox8;
+  __device__ static double* vel(unsigned char* p, int q) { return (double*)(p + q * kBox9); }
+  __device__ static double* pres(unsigned char* p) { return (double*)(p + 3 * kBox9); }
+  // 0 xarea, 1 yarea, 2 zarea, 3 density0
+  __device__ static double* cell(unsigned char* p, int q) {
+    return (double*)(p + 3 * kBox9 + kBox10 + q * kBox8);
+  }
+};
+
+template <int RING, int MINB>
+__global__ void __launch_bounds__(TX * TY, MINB)
+k_viscosity_dropin_tma(Geom g, int seg, GeomArrays ga, const __grid_constant__ ViscDropMaps maps,
+                       double* __restrict__ viscosity, int* __restrict__ status) {
+  using P = ViscDropPlane;
+  extern __shared__ __align__(128) unsigned char ring[];
+  __shared__ unsigned long long full[RING];
+  __shared__ int stop;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int j = g.x_min + TX * (int)blockIdx.x + tx, k0 = g.y_min + TY * (int)blockIdx.y;
+  const int k = k0 + ty;
+  const int l0 = g.z_min + seg * (int)blockIdx.z;
+  const int l1 = l0 + seg - 1 < g.z_max ? l0 + seg - 1 : g.z_max;
+  const bool in_jk = j <= g.x_max && k <= g.y_max;
+  const PlaneMarch<RING, 1, 1> pm{ring, P::kBytes, full, &stop, l0 - 1, l1 + 1};
+  constexpr int W = kDropW, H = kDropH;
+  auto issue = [&](int p) {
+    unsigned char* b = pm.buf(p);
+    unsigned long long* bar = pm.bar(p);
+    const bool vel = p >= l0, cells = p >= l0 && p <= l1;
+    mbar_arrive_expect_tx(bar, box_bytes<double>(10) + (vel ? 3 * box_bytes<double>(9) : 0u) +
+                                   (cells ? 4 * box_bytes<double>(8) : 0u));
+    const int x = TX * (int)blockIdx.x, y = k0 - g.y_min + 2, z = p - g.z_min + 2;
+    tma_load_box(P::pres(b), &maps.p, bar, x, y - 1, z);
+    if (vel) {
+      tma_load_box(P::vel(b, 0), &maps.u, bar, x, y, z);
+      tma_load_box(P::vel(b, 1), &maps.v, bar, x, y, z);
+      tma_load_box(P::vel(b, 2), &maps.w, bar, x, y, z);
+    }
+    if (cells) {
+      tma_load_box(P::cell(b, 0), &maps.xa, bar, x, y, z);
+      tma_load_box(P::cell(b, 1), &maps.ya, bar, x, y, z);
+      tma_load_box(P::cell(b, 2), &maps.za, bar, x, y, z);
+      tma_load_box(P::cell(b, 3), &maps.d, bar, x, y, z);
+    }
+  };
+  pm.run(l0, l1, status, issue, [&](int l) {
+    if (!in_jk) return;
+    unsigned char* bd = pm.buf(l - 1);
+    unsigned char* bl = pm.buf(l);
+    unsigned char* bu = pm.buf(l + 1);
+    const int c = ty * W + tx + H;
+#define NV(bb, q, a, b) (P::vel(bb, q)[(ty + (b)) * W + tx + H + (a)])
+    const double u000 = NV(bl, 0, 0, 0), u100 = NV(bl, 0, 1, 0), u010 = NV(bl, 0, 0, 1);
+    const double u110 = NV(bl, 0, 1, 1), u001 = NV(bu, 0, 0, 0), u101 = NV(bu, 0, 1, 0);
+    const double u011 = NV(bu, 0, 0, 1), u111 = NV(bu, 0, 1, 1);
+    const double v000 = NV(bl, 1, 0, 0), v100 = NV(bl, 1, 1, 0), v010 = NV(bl, 1, 0, 1);
+    const double v110 = NV(bl, 1, 1, 1), v001 = NV(bu, 1, 0, 0), v101 = NV(bu, 1, 1, 0);
+    const double v011 = NV(bu, 1, 0, 1), v111 = NV(bu, 1, 1, 1);
+    const double w000 = NV(bl, 2, 0, 0), w100 = NV(bl, 2, 1, 0), w010 = NV(bl, 2, 0, 1);
+    const double w110 = NV(bl, 2, 1, 1), w001 = NV(bu, 2, 0, 0), w101 = NV(bu, 2, 1, 0);
+    const double w011 = NV(bu, 2, 0, 1), w111 = NV(bu, 2, 1, 1);
+#undef NV
+    const double ugradx1 = u000 + u010 + u001 + u011;
+    const double ugradx2 = u100 + u110 + u101 + u111;
+    const double vgrady1 = v000 + v100 + v001 + v101;
+    const double vgrady2 = v010 + v110 + v011 + v111;
+    const double wgradz1 = w000 + w100 + w010 + w110;
+    const double wgradz2 = w001 + w101 + w011 + w111;
+    const double div = (P::cell(bl, 0)[c] * (ugradx2 - ugradx1) +
+                        P::cell(bl, 1)[c] * (vgrady2 - vgrady1)) +
+                       P::cell(bl, 2)[c] * (wgradz2 - wgradz1);
+    double q = 0.0;
+    if (!(div >= 0.0)) {
+      const double ugrady1 = u000 + u100 + u001 + u101;
+      const double ugrady2 = u010 + u110 + u011 + u111;
+      const double ugradz1 = u000 + u100 + u010 + u110;
+      const double ugradz2 = u001 + u101 + u011 + u111;
+      const double vgradx1 = v000 + v010 + v001 + v011;
+      const double vgradx2 = v100 + v110 + v101 + v111;
+      const double vgradz1 = v000 + v100 + v010 + v110;
+      const double vgradz2 = v001 + v101 + v011 + v111;
+      const double wgradx1 = w000 + w010 + w001 + w011;
+      const double wgradx2 = w100 + w110 + w101 + w111;
+      const double wgrady1 = w000 + w100 + w001 + w101;
+      const double wgrady2 = w010 + w110 + w011 + w111;
+      const double* cx = ga.celldx + g.o1 + 2 - g.x_min;
+      const double* cy = ga.celldy + g.o1 + 2 - g.y_min;
+      const double* cz = ga.celldz + g.o1 + 2 - g.z_min;
+      const double cdx = cx[j], cdy = cy[k], cdz = cz[l];
+      const double xx = 0.25 * (ugradx2 - ugradx1) / cdx;
+      const double yy = 0.25 * (vgrady2 - vgrady1) / cdy;
+      const double zz = 0.25 * (wgradz2 - wgradz1) / cdz;
+      const double xy = 0.25 * (ugrady2 - ugrady1) / cdy + 0.25 * (vgradx2 - vgradx1) / cdx;
+      const double xz = 0.25 * (ugradz2 - ugradz1) / cdz + 0.25 * (wgradx2 - wgradx1) / cdx;
+      const double yz = 0.25 * (vgradz2 - vgradz1) / cdz + 0.25 * (wgrady2 - wgrady1) / cdy;
+      // pressure (j+a, k+b) of a pressure buffer (rows from k0-1)
+#define PR(bb, a, b) (P::pres(bb)[(ty + 1 + (b)) * W + tx + H + (a)])
+      double pgradx = (PR(bl, 1, 0) - PR(bl, -1, 0)) / (cdx + cx[j + 1]);
+      double pgrady = (PR(bl, 0, 1) - PR(bl, 0, -1)) / (cdy + cy[k + 1]);
+      double pgradz = (PR(bu, 0, 0) - PR(bd, 0, 0)) / (cdz + cz[l + 1]);
+#undef PR
+      const double pgradx2 = pgradx * pgradx;
+      const double pgrady2 = pgrady * pgrady;
+      const double pgradz2 = pgradz * pgradz;
+      const double limiter = (xx * pgradx2 + yy * pgrady2 + zz * pgradz2 + xy * pgradx * pgrady +
+                              xz * pgradx * pgradz + yz * pgrady * pgradz) /
+                             fmax2(pgradx2 + pgrady2 + pgradz2, 1.0e-16);
+      if (!(limiter > 0.0)) {
+        pgradx = copysign(fmax2(1.0e-16, fabs(pgradx)), pgradx);
+        pgrady = copysign(fmax2(1.0e-16, fabs(pgrady)), pgrady);
+        pgradz = copysign(fmax2(1.0e-16, fabs(pgradz)), pgradz);
+        const double pgrad = sqrt(pgradx * pgradx + pgrady * pgrady + pgradz * pgradz);
+        const double xgrad = fabs(cdx * pgrad / pgradx);
+        const double ygrad = fabs(cdy * pgrad / pgrady);
+        const double zgrad = fabs(cdz * pgrad / pgradz);
+        const double grad = fmin2(fmin2(xgrad, ygrad), zgrad);
+        const double grad2 = grad * grad;
+        q = 2.0 * P::cell(bl, 3)[c] * grad2 * limiter * limiter;
+      }
+    }
+    viscosity[off3(g, j, k, l)] = q;
+  });
+}
+
+// accelerate_kernel.f90:61-109 as k_accelerate forms it over the caller's
+// arrays. Plane p: density0, volume, pressure, viscosity, xarea and zarea of
+// cell plane p (rows k0-1..k0+7), yarea (rows k0..k0+7) and the node
+// velocities of node plane p (rows k0..k0+7). Node l reads cell planes l-1
+// and l (zarea and the velocities of plane l only).
+struct AccDropPlane {
+  static constexpr int kBytes = 6 * kBox9 + 4 * kBox8;
+  // 0 density0, 1 volume, 2 pressure, 3 viscosity, 4 xarea, 5 zarea
+  __device__ static double* c9(unsigned char* p, int q) { return (double*)(p + q * kBox9); }
+  __device__ static double* ya(unsigned char* p) { return (double*)(p + 6 * kBox9); }
+  __device__ static double* vel(unsigned char* p, int q) {
+    return (double*)(p + 6 * kBox9 + (1 + q) * kBox8);
+  }
+};
+
+template <int RING, int MINB>
+__global__ void __launch_bounds__(TX * TY, MINB)
+k_accelerate_dropin_tma(Geom g, int seg, double dt, const __grid_constant__ AccDropMaps maps,
+                        double* __restrict__ xvel1, double* __restrict__ yvel1,
+                        double* __restrict__ zvel1, int* __restrict__ status) {
+  using P = AccDropPlane;
+  extern __shared__ __align__(128) unsigned char ring[];
+  __shared__ unsigned long long full[RING];
+  __shared__ int stop;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int j = g.x_min + TX * (int)blockIdx.x + tx, k0 = g.y_min + TY * (int)blockIdx.y;
+  const int k = k0 + ty;
+  const int l0 = g.z_min + seg * (int)blockIdx.z;
+  const int l1 = l0 + seg - 1 < g.z_max + 1 ? l0 + seg - 1 : g.z_max + 1;
+  const bool in_jk = j <= g.x_max + 1 && k <= g.y_max + 1;
+  const PlaneMarch<RING, 1, 0> pm{ring, P::kBytes, full, &stop, l0 - 1, l1};
+  constexpr int W = kDropW, H = kDropH;
+  auto issue = [&](int p) {
+    unsigned char* b = pm.buf(p);
+    unsigned long long* bar = pm.bar(p);
+    const bool node = p >= l0;  // zarea and the velocities: the nodes' own plane only
+    mbar_arrive_expect_tx(bar, 5 * box_bytes<double>(9) + box_bytes<double>(8) +
+                                   (node ? box_bytes<double>(9) + 3 * box_bytes<double>(8) : 0u));
+    const int x = TX * (int)blockIdx.x, y = k0 - g.y_min + 2, z = p - g.z_min + 2;
+    tma_load_box(P::c9(b, 0), &maps.d, bar, x, y - 1, z);
+    tma_load_box(P::c9(b, 1), &maps.vol, bar, x, y - 1, z);
+    tma_load_box(P::c9(b, 2), &maps.p, bar, x, y - 1, z);
+    tma_load_box(P::c9(b, 3), &maps.q, bar, x, y - 1, z);
+    tma_load_box(P::c9(b, 4), &maps.xa, bar, x, y - 1, z);
+    tma_load_box(P::ya(b), &maps.ya, bar, x, y, z);
+    if (node) {
+      tma_load_box(P::c9(b, 5), &maps.za, bar, x, y - 1, z);
+      tma_load_box(P::vel(b, 0), &maps.u, bar, x, y, z);
+      tma_load_box(P::vel(b, 1), &maps.v, bar, x, y, z);
+      tma_load_box(P::vel(b, 2), &maps.w, bar, x, y, z);
+    }
+  };
+  pm.run(l0, l1, status, issue, [&](int l) {
+    if (!in_jk) return;
+    unsigned char* bd = pm.buf(l - 1);
+    unsigned char* bl = pm.buf(l);
+    // cell (j+a, k+b) of a 9-row buffer (rows from k0-1), of yarea (rows from k0)
+#define C9(bb, q, a, b) (P::c9(bb, q)[(ty + 1 + (b)) * W + tx + H + (a)])
+#define YA(bb, a) (P::ya(bb)[ty * W + tx + H + (a)])
+#define DV(bb, a, b) (C9(bb, 0, a, b) * C9(bb, 1, a, b))
+    const double nodal_mass = (DV(bl, -1, -1) + DV(bl, 0, -1) + DV(bl, 0, 0) + DV(bl, -1, 0) +
+                               DV(bd, -1, -1) + DV(bd, 0, -1) + DV(bd, 0, 0) + DV(bd, -1, 0)) * 0.125;
+#undef DV
+    const double stepbymass_s = 0.25 * dt / nodal_mass;
+    const double p000 = C9(bl, 2, 0, 0), p100 = C9(bl, 2, -1, 0);
+    const double p010 = C9(bl, 2, 0, -1), p110 = C9(bl, 2, -1, -1);
+    const double p001 = C9(bd, 2, 0, 0), p101 = C9(bd, 2, -1, 0);
+    const double p011 = C9(bd, 2, 0, -1), p111 = C9(bd, 2, -1, -1);
+    const double q000 = C9(bl, 3, 0, 0), q100 = C9(bl, 3, -1, 0);
+    const double q010 = C9(bl, 3, 0, -1), q110 = C9(bl, 3, -1, -1);
+    const double q001 = C9(bd, 3, 0, 0), q101 = C9(bd, 3, -1, 0);
+    const double q011 = C9(bd, 3, 0, -1), q111 = C9(bd, 3, -1, -1);
+    const double xa0 = C9(bl, 4, 0, 0), xa1 = C9(bl, 4, 0, -1);
+    const double xa2 = C9(bd, 4, 0, 0), xa3 = C9(bd, 4, 0, -1);
+    const double ya0 = YA(bl, 0), ya1 = YA(bl, -1);
+    const double ya2 = YA(bd, 0), ya3 = YA(bd, -1);
+    const double za0 = C9(bl, 5, 0, 0), za1 = C9(bl, 5, 0, -1);
+    const double za2 = C9(bl, 5, -1, 0), za3 = C9(bl, 5, -1, -1);
+#undef YA
+#undef C9
+    const int c = ty * W + tx + H;
+    const double xvel1_s = P::vel(bl, 0)[c] -
+        stepbymass_s * (xa0 * (p000 - p100) + xa1 * (p010 - p110) + xa2 * (p001 - p101) +
+                        xa3 * (p011 - p111));
+    const double yvel1_s = P::vel(bl, 1)[c] -
+        stepbymass_s * (ya0 * (p000 - p010) + ya1 * (p100 - p110) + ya2 * (p001 - p011) +
+                        ya3 * (p101 - p111));
+    const double zvel1_s = P::vel(bl, 2)[c] -
+        stepbymass_s * (za0 * (p000 - p001) + za1 * (p010 - p011) + za2 * (p100 - p101) +
+                        za3 * (p110 - p111));
+    const long long o = off3(g, j, k, l);
+    xvel1[o] = xvel1_s - stepbymass_s * (xa0 * (q000 - q100) + xa1 * (q010 - q110) +
+                                         xa2 * (q001 - q101) + xa3 * (q011 - q111));
+    yvel1[o] = yvel1_s - stepbymass_s * (ya0 * (q000 - q010) + ya1 * (q100 - q110) +
+                                         ya2 * (q001 - q011) + ya3 * (q101 - q111));
+    zvel1[o] = zvel1_s - stepbymass_s * (za0 * (q000 - q001) + za1 * (q010 - q011) +
+                                         za2 * (q100 - q101) + za3 * (q110 - q111));
+  });
+}
+
+// ---------------------------------------------------------------------------
 // The node pass of the y or z momentum sweep (advec_mom_kernel.f90:254-293 for
 // y, :339-379 for z), as k_mom_node_march (clover_fused.cu) forms it, with the
 // inputs staged in shared memory. The lane layout stays: lane L of a warp holds
@@ -1647,6 +1999,51 @@ void launch_pdv_dropin_tma(const Geom& g, cudaStream_t s, bool predict, double d
         <<<grid, dim3(TX, TY), kStencilRing * PdvDropPlane<false>::kBytes, s>>>(
             g, kStencilSeg, dt, maps, volume, density0, density1, energy0, energy1, pressure,
             viscosity, status);
+}
+
+constexpr int kDropMinBlocks = 2;
+
+bool stencils_dropin_tma_prepare() {
+  return cudaFuncSetAttribute(k_calc_dt_dropin_tma<kStencilRing, kDropMinBlocks>,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              kStencilRing * DtDropPlane::kBytes) == cudaSuccess &&
+         cudaFuncSetAttribute(k_viscosity_dropin_tma<kStencilRing, kDropMinBlocks>,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              kStencilRing * ViscDropPlane::kBytes) == cudaSuccess &&
+         cudaFuncSetAttribute(k_accelerate_dropin_tma<kStencilRing, kDropMinBlocks>,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              kStencilRing * AccDropPlane::kBytes) == cudaSuccess;
+}
+
+void launch_calc_dt_dropin_tma(const Geom& g, cudaStream_t s, const GeomArrays& ga, double g_small,
+                               double dtc_safe, double dtu_safe, double dtv_safe, double dtw_safe,
+                               double dtdiv_safe, const DtDropMaps& maps, double* dt_min,
+                               unsigned long long* min_key, int* status) {
+  const dim3 grid((g.x_max - g.x_min + TX) / TX, (g.y_max - g.y_min + TY) / TY,
+                  (g.z_max - g.z_min + kStencilSeg) / kStencilSeg);
+  k_calc_dt_dropin_tma<kStencilRing, kDropMinBlocks>
+      <<<grid, dim3(TX, TY), kStencilRing * DtDropPlane::kBytes, s>>>(
+          g, kStencilSeg, ga, g_small, dtc_safe, dtu_safe, dtv_safe, dtw_safe, dtdiv_safe, maps,
+          dt_min, min_key, status);
+}
+
+void launch_viscosity_dropin_tma(const Geom& g, cudaStream_t s, const GeomArrays& ga,
+                                 const ViscDropMaps& maps, double* viscosity, int* status) {
+  const dim3 grid((g.x_max - g.x_min + TX) / TX, (g.y_max - g.y_min + TY) / TY,
+                  (g.z_max - g.z_min + kStencilSeg) / kStencilSeg);
+  k_viscosity_dropin_tma<kStencilRing, kDropMinBlocks>
+      <<<grid, dim3(TX, TY), kStencilRing * ViscDropPlane::kBytes, s>>>(g, kStencilSeg, ga, maps,
+                                                                         viscosity, status);
+}
+
+void launch_accelerate_dropin_tma(const Geom& g, cudaStream_t s, double dt,
+                                  const AccDropMaps& maps, double* xvel1, double* yvel1,
+                                  double* zvel1, int* status) {
+  const dim3 grid((g.x_max + 1 - g.x_min + TX) / TX, (g.y_max + 1 - g.y_min + TY) / TY,
+                  (g.z_max + 1 - g.z_min + kStencilSeg) / kStencilSeg);
+  k_accelerate_dropin_tma<kStencilRing, kDropMinBlocks>
+      <<<grid, dim3(TX, TY), kStencilRing * AccDropPlane::kBytes, s>>>(g, kStencilSeg, dt, maps,
+                                                                        xvel1, yvel1, zvel1, status);
 }
 
 template <class S>

@@ -105,6 +105,31 @@ void launch_pdv_dropin_tma(const Geom& g, cudaStream_t s, bool predict, double d
                            double* density1, const double* energy0, double* energy1,
                            const double* pressure, const double* viscosity, int* status);
 
+// The maps of the drop-in calc_dt (node velocities 9 rows; sound speed,
+// viscosity, density0, volume and the face areas 8 rows), viscosity (node
+// velocities 9 rows, pressure 10 rows from k0-1, face areas and density0 8
+// rows) and accelerate (density0, volume, pressure, viscosity, xarea and
+// zarea 9 rows from k0-1, yarea and the node velocities 8 rows).
+struct DtDropMaps {
+  CUtensorMap u, v, w, ss, q, d, vol, xa, ya, za;
+};
+struct ViscDropMaps {
+  CUtensorMap u, v, w, p, xa, ya, za, d;
+};
+struct AccDropMaps {
+  CUtensorMap d, vol, p, q, xa, za, ya, u, v, w;
+};
+bool stencils_dropin_tma_prepare();
+void launch_calc_dt_dropin_tma(const Geom& g, cudaStream_t s, const GeomArrays& ga, double g_small,
+                               double dtc_safe, double dtu_safe, double dtv_safe, double dtw_safe,
+                               double dtdiv_safe, const DtDropMaps& maps, double* dt_min,
+                               unsigned long long* min_key, int* status);
+void launch_viscosity_dropin_tma(const Geom& g, cudaStream_t s, const GeomArrays& ga,
+                                 const ViscDropMaps& maps, double* viscosity, int* status);
+void launch_accelerate_dropin_tma(const Geom& g, cudaStream_t s, double dt,
+                                  const AccDropMaps& maps, double* xvel1, double* yvel1,
+                                  double* zvel1, int* status);
+
 // The maps of the y/z momentum node pass: mass flux of the sweep direction
 // and density1 (9 rows from c0-1), and the volume fluxes its post volumes
 // take (vol_flux_x 9 rows, the row-direction flux 10 rows: vol_flux_y for
