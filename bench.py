@@ -633,10 +633,12 @@ def main():
     top = max(groups, key=lambda g: g["ms"])
     # DRAM bytes per launch of the dominant group, from an ncu capture of its
     # kernels at 256^3 (dram__bytes_read.sum + dram__bytes_write.sum of one
-    # direction's node pass and velocity pass), scaled by the cells to 512^3
+    # direction's staged node pass and velocity pass, the mean over the five
+    # of each in profiles/hydro_step_fused_fp64_256_launches.md: 2.356 GB),
+    # scaled by the cells to 512^3
     traffic = None
-    if top["name"] == "advec_mom_yz" and n == 512:
-        traffic = (0.485 + 0.380 + 0.898 + 0.388) * 1e9 * 8
+    if top["name"] == "advec_mom_yz" and n == 512 and tma and prec == C.PRECISION_FP64:
+        traffic = 2.356e9 * 8
     prof_total_ms = sum(g["ms"] for g in groups)
     achieved = top["bytes"] / (top["ms"] / 1000.0) / 1e9
     step_bytes = sum(g["bytes"] for g in groups) / args.steps

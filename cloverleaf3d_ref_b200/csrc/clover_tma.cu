@@ -1968,6 +1968,18 @@ bool stencils_tma_prepare() {
                               kStencilRing * FluxPlane<S>::kBytes) == cudaSuccess;
 }
 
+// Planes per block of a staged drop-in stencil over nz planes with xy blocks
+// per plane: 32 where that leaves at least eight blocks per SM (148 SMs),
+// fewer on small chunks (down to 4), whose blocks would otherwise each march
+// a long column of planes with most SMs idle.
+int drop_seg(int nz, int xy) {
+  const long long want = 148LL * 8;
+  long long seg = ((long long)nz * xy + want - 1) / want;
+  if (seg > kStencilSeg) seg = kStencilSeg;
+  if (seg < 4) seg = 4;
+  return (int)seg;
+}
+
 // blocks per SM of the drop-in PdV: the corrector's plane (six velocity
 // boxes and three area boxes, 23 KB) leaves room for two blocks of a
 // four-plane ring, the predictor's for three
@@ -1987,21 +1999,23 @@ void launch_pdv_dropin_tma(const Geom& g, cudaStream_t s, bool predict, double d
                            const PdvDropMaps& maps, const double* volume, const double* density0,
                            double* density1, const double* energy0, double* energy1,
                            const double* pressure, const double* viscosity, int* status) {
-  const dim3 grid((g.x_max - g.x_min + TX) / TX, (g.y_max - g.y_min + TY) / TY,
-                  (g.z_max - g.z_min + kStencilSeg) / kStencilSeg);
+  const int gx = (g.x_max - g.x_min + TX) / TX, gy = (g.y_max - g.y_min + TY) / TY;
+  const int nz = g.z_max - g.z_min + 1, seg = drop_seg(nz, gx * gy);
+  const dim3 grid(gx, gy, (nz + seg - 1) / seg);
   if (predict)
     k_pdv_dropin_tma<true, kStencilRing, kPdvDropMinBlocks<true>>
         <<<grid, dim3(TX, TY), kStencilRing * PdvDropPlane<true>::kBytes, s>>>(
-            g, kStencilSeg, dt, maps, volume, density0, density1, energy0, energy1, pressure,
-            viscosity, status);
+            g, seg, dt, maps, volume, density0, density1, energy0, energy1, pressure, viscosity,
+            status);
   else
     k_pdv_dropin_tma<false, kStencilRing, kPdvDropMinBlocks<false>>
         <<<grid, dim3(TX, TY), kStencilRing * PdvDropPlane<false>::kBytes, s>>>(
-            g, kStencilSeg, dt, maps, volume, density0, density1, energy0, energy1, pressure,
-            viscosity, status);
+            g, seg, dt, maps, volume, density0, density1, energy0, energy1, pressure, viscosity,
+            status);
 }
 
 constexpr int kDropMinBlocks = 2;
+
 
 bool stencils_dropin_tma_prepare() {
   return cudaFuncSetAttribute(k_calc_dt_dropin_tma<kStencilRing, kDropMinBlocks>,
@@ -2019,31 +2033,34 @@ void launch_calc_dt_dropin_tma(const Geom& g, cudaStream_t s, const GeomArrays& 
                                double dtc_safe, double dtu_safe, double dtv_safe, double dtw_safe,
                                double dtdiv_safe, const DtDropMaps& maps, double* dt_min,
                                unsigned long long* min_key, int* status) {
-  const dim3 grid((g.x_max - g.x_min + TX) / TX, (g.y_max - g.y_min + TY) / TY,
-                  (g.z_max - g.z_min + kStencilSeg) / kStencilSeg);
+  const int gx = (g.x_max - g.x_min + TX) / TX, gy = (g.y_max - g.y_min + TY) / TY;
+  const int nz = g.z_max - g.z_min + 1, seg = drop_seg(nz, gx * gy);
+  const dim3 grid(gx, gy, (nz + seg - 1) / seg);
   k_calc_dt_dropin_tma<kStencilRing, kDropMinBlocks>
       <<<grid, dim3(TX, TY), kStencilRing * DtDropPlane::kBytes, s>>>(
-          g, kStencilSeg, ga, g_small, dtc_safe, dtu_safe, dtv_safe, dtw_safe, dtdiv_safe, maps,
+          g, seg, ga, g_small, dtc_safe, dtu_safe, dtv_safe, dtw_safe, dtdiv_safe, maps,
           dt_min, min_key, status);
 }
 
 void launch_viscosity_dropin_tma(const Geom& g, cudaStream_t s, const GeomArrays& ga,
                                  const ViscDropMaps& maps, double* viscosity, int* status) {
-  const dim3 grid((g.x_max - g.x_min + TX) / TX, (g.y_max - g.y_min + TY) / TY,
-                  (g.z_max - g.z_min + kStencilSeg) / kStencilSeg);
+  const int gx = (g.x_max - g.x_min + TX) / TX, gy = (g.y_max - g.y_min + TY) / TY;
+  const int nz = g.z_max - g.z_min + 1, seg = drop_seg(nz, gx * gy);
+  const dim3 grid(gx, gy, (nz + seg - 1) / seg);
   k_viscosity_dropin_tma<kStencilRing, kDropMinBlocks>
-      <<<grid, dim3(TX, TY), kStencilRing * ViscDropPlane::kBytes, s>>>(g, kStencilSeg, ga, maps,
+      <<<grid, dim3(TX, TY), kStencilRing * ViscDropPlane::kBytes, s>>>(g, seg, ga, maps,
                                                                          viscosity, status);
 }
 
 void launch_accelerate_dropin_tma(const Geom& g, cudaStream_t s, double dt,
                                   const AccDropMaps& maps, double* xvel1, double* yvel1,
                                   double* zvel1, int* status) {
-  const dim3 grid((g.x_max + 1 - g.x_min + TX) / TX, (g.y_max + 1 - g.y_min + TY) / TY,
-                  (g.z_max + 1 - g.z_min + kStencilSeg) / kStencilSeg);
+  const int gx = (g.x_max + 1 - g.x_min + TX) / TX, gy = (g.y_max + 1 - g.y_min + TY) / TY;
+  const int nz = g.z_max - g.z_min + 2, seg = drop_seg(nz, gx * gy);
+  const dim3 grid(gx, gy, (nz + seg - 1) / seg);
   k_accelerate_dropin_tma<kStencilRing, kDropMinBlocks>
-      <<<grid, dim3(TX, TY), kStencilRing * AccDropPlane::kBytes, s>>>(g, kStencilSeg, dt, maps,
-                                                                        xvel1, yvel1, zvel1, status);
+      <<<grid, dim3(TX, TY), kStencilRing * AccDropPlane::kBytes, s>>>(g, seg, dt, maps, xvel1,
+                                                                        yvel1, zvel1, status);
 }
 
 template <class S>
