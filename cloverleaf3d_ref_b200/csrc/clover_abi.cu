@@ -146,22 +146,25 @@ bool is_device_pointer(const void* p) {
 // The tensor map of a chunk-layout FP64 array with boxes of `rows` rows, made
 // on first use; null if the array cannot be staged (the driver refuses the
 // map, e.g. a device array passed in place whose base is not 16-byte aligned).
-const CUtensorMap* tmap(Context& c, const double* base, const Geom& g, int rows) {
+const CUtensorMap* tmap(Context& c, const double* base, const Geom& g, int rows,
+                        bool rows_along_z = false) {
   if (!base) return nullptr;
-  const auto key = std::make_tuple((const void*)base, rows, g.px, g.pxy, g.z_max - g.z_min);
+  // box rows along z are keyed as negative row counts
+  const auto key = std::make_tuple((const void*)base, rows_along_z ? -rows : rows, g.px, g.pxy,
+                                   g.z_max - g.z_min);
   auto it = c.tmaps.find(key);
   if (it != c.tmaps.end()) return &it->second;
   CUtensorMap m;
-  if (!encode_plane_map(&m, base, 8, g, rows)) return nullptr;
+  if (!encode_plane_map(&m, base, 8, g, rows, rows_along_z)) return nullptr;
   return &(c.tmaps[key] = m);
 }
 
 // The maps of n arrays (base, box rows) into out[], in order; false if any
 // array has none.
 bool tmaps_of(Context& c, const Geom& g, int n, const double* const* base, const int* rows,
-              CUtensorMap* out) {
+              CUtensorMap* out, bool rows_along_z = false) {
   for (int q = 0; q < n; q++) {
-    const CUtensorMap* m = tmap(c, base[q], g, rows[q]);
+    const CUtensorMap* m = tmap(c, base[q], g, rows[q], rows_along_z);
     if (!m) return false;
     out[q] = *m;
   }
@@ -172,7 +175,10 @@ bool tmaps_of(Context& c, const Geom& g, int n, const double* const* base, const
 bool staged(Context& c) {
   if (!c.staging) return false;
   if (c.tma_state == 0)
-    c.tma_state = pdv_dropin_tma_prepare() && stencils_dropin_tma_prepare() ? 1 : -1;
+    c.tma_state = pdv_dropin_tma_prepare() && stencils_dropin_tma_prepare() &&
+                          mom_node_dropin_tma_prepare()
+                      ? 1
+                      : -1;
   if (c.tma_state < 0) cudaGetLastError();
   return c.tma_state > 0;
 }
@@ -837,10 +843,33 @@ void clover_advec_mom_kernel(const int* x_min, const int* x_max, const int* y_mi
   for (int q = 0; q < 6; q++) aliased = aliased || others[q] == pre_vol || others[q] == post_vol;
   for (int q = 0; q < 4; q++) aliased = aliased || in[q] == pre_vol || in[q] == post_vol;
   skip = skip && !aliased;
-  launch_advec_mom<F64>(g, c.stream, VERT(vel1), XF(mass_flux_x), XF(vol_flux_x),
-                        YF(mass_flux_y), YF(vol_flux_y), ZF(mass_flux_z), ZF(vol_flux_z), ga,
-                        CELL(density1), work, *advect_x != 0, *which_vel, *sweep_number,
-                        *direction, skip);
+  double *v1 = VERT(vel1), *mfx = XF(mass_flux_x), *vfx = XF(vol_flux_x);
+  double *mfy = YF(mass_flux_y), *vfy = YF(vol_flux_y), *mfz = ZF(mass_flux_z);
+  double *vfz = ZF(vol_flux_z), *d1 = CELL(density1);
+  // the y/z node pass staged by bulk-tensor copies, between the volumes it
+  // reads and the flux + update
+  bool staged_node = false;
+  NodeDropMaps nmaps;
+  const int dir = *direction;
+  if (*which_vel == 1 && (dir == 2 || dir == 3) && staged(c)) {
+    const double* base[3] = {dir == 2 ? mfy : mfz, d1, work[6]};
+    const int rows[3] = {9, 9, 9};
+    CUtensorMap m[3];
+    if (tmaps_of(c, g, 3, base, rows, m, dir == 2)) {
+      nmaps.mf = m[0]; nmaps.d = m[1]; nmaps.pv = m[2];
+      staged_node = true;
+    }
+  }
+  if (staged_node) {
+    launch_advec_mom<F64>(g, c.stream, v1, mfx, vfx, mfy, vfy, mfz, vfz, ga, d1, work,
+                          *advect_x != 0, *which_vel, *sweep_number, dir, skip, kMomVolumes);
+    launch_mom_node_dropin_tma(g, c.stream, dir, nmaps, work[0], work[1], work[2], c.d_status);
+    launch_advec_mom<F64>(g, c.stream, v1, mfx, vfx, mfy, vfy, mfz, vfz, ga, d1, work,
+                          *advect_x != 0, *which_vel, *sweep_number, dir, true, kMomFluxUpdate);
+  } else {
+    launch_advec_mom<F64>(g, c.stream, v1, mfx, vfx, mfy, vfy, mfz, vfz, ga, d1, work,
+                          *advect_x != 0, *which_vel, *sweep_number, dir, skip);
+  }
   check_launch("advec_mom");
   c.mom_vol.at = (variant >= 0 && !aliased && c.status == 0) ? c.calls : -1;
   c.mom_vol.variant = variant;

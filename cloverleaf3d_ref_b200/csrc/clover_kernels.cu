@@ -1660,14 +1660,15 @@ void launch_advec_mom(const Geom& g, cudaStream_t s, typename S::vel_t* vel1,
                       const typename S::mf_t* mass_flux_z, const typename S::vf_t* vol_flux_z,
                       const GeomArrays& ga, const typename S::rho_t* density1,
                       typename S::wk_t* const* work, int advect_x, int which_vel, int sweep,
-                      int direction, bool skip_volumes) {
+                      int direction, bool skip_volumes, int parts) {
   typename S::wk_t *node_flux = work[0], *node_mass_post = work[1], *node_mass_pre = work[2],
                    *mom_flux = work[4], *pre_vol = work[5], *post_vol = work[6];
   const int variant = mom_vol_variant(advect_x, sweep, direction);
-  if (variant >= 0 && !skip_volumes)
+  if (variant >= 0 && !skip_volumes && (parts & kMomVolumes))
     LAUNCH(k_mom_vol<S>, halo2(g), variant, ga, vol_flux_x, vol_flux_y, vol_flux_z, pre_vol, post_vol);
   const int x0 = g.x_min, x1 = g.x_max, y0 = g.y_min, y1 = g.y_max, z0 = g.z_min, z1 = g.z_max;
-  if (direction == 1) {
+  if (!(parts & kMomNodePass)) {
+  } else if (direction == 1) {
     if (which_vel == 1) {
       const Box bf{x0 - 2, x1 + 2, y0, y1 + 1, z0, z1 + 1}, bm{x0 - 1, x1 + 2, y0, y1 + 1, z0, z1 + 1};
       LAUNCH((k_mom_node<S, 1>), box_union(bf, bm), bf, bm, mass_flux_x, density1, post_vol,
@@ -1686,6 +1687,7 @@ void launch_advec_mom(const Geom& g, cudaStream_t s, typename S::vel_t* vel1,
              node_flux, node_mass_post, node_mass_pre);
     }
   }
+  if (!(parts & kMomFluxUpdate)) return;
   // the flux at nodes min-1..max+1 and the update of nodes min..max+1 along
   // the sweep, in one pass per velocity
   const int nx = x1 - x0 + 1, ny = y1 - y0 + 1, nz = z1 - z0 + 1;
@@ -1863,7 +1865,7 @@ void launch_fill(cudaStream_t s, T* p, long long elems, T value) {
                                     const S::vf_t*, const S::mf_t*, const S::vf_t*,            \
                                     const S::mf_t*, const S::vf_t*, const GeomArrays&,         \
                                     const S::rho_t*, S::wk_t* const*, int, int, int, int,      \
-                                    bool);                                                     \
+                                    bool, int);                                                \
   template void launch_reset_field<S>(const Target&, cudaStream_t, S::rho_t*, const S::rho_t*,     \
                                       S::ene_t*, const S::ene_t*, S::vel_t*, const S::vel_t*,  \
                                       S::vel_t*, const S::vel_t*, S::vel_t*, const S::vel_t*); \

@@ -277,6 +277,12 @@ int mom_vol_variant(int advect_x, int sweep, int direction);
 // work: the 7 work arrays (advec_mom_driver.f90:51-57 order). skip_volumes:
 // pre_vol/post_vol already hold this sweep's values (the caller knows that
 // nothing changed them or their inputs since they were formed).
+// The parts of one advec_mom call: the pre/post volumes, the node pass
+// (which_vel 1) and the momentum flux + velocity update; a caller that runs
+// the node pass itself launches the first and the last part around it.
+constexpr int kMomVolumes = 1, kMomNodePass = 2, kMomFluxUpdate = 4;
+constexpr int kMomAllParts = kMomVolumes | kMomNodePass | kMomFluxUpdate;
+
 template <class S>
 void launch_advec_mom(const Geom& g, cudaStream_t s, typename S::vel_t* vel1,
                       const typename S::mf_t* mass_flux_x, const typename S::vf_t* vol_flux_x,
@@ -284,7 +290,7 @@ void launch_advec_mom(const Geom& g, cudaStream_t s, typename S::vel_t* vel1,
                       const typename S::mf_t* mass_flux_z, const typename S::vf_t* vol_flux_z,
                       const GeomArrays& ga, const typename S::rho_t* density1,
                       typename S::wk_t* const* work, int advect_x, int which_vel, int sweep,
-                      int direction, bool skip_volumes = false);
+                      int direction, bool skip_volumes = false, int parts = kMomAllParts);
 
 template <class S>
 void launch_reset_field(const Target& tg, cudaStream_t s, typename S::rho_t* density0,

@@ -1380,6 +1380,90 @@ k_accelerate_dropin_tma(Geom g, int seg, double dt, const __grid_constant__ AccD
 }
 
 // ---------------------------------------------------------------------------
+// The drop-in advec_mom node pass of the y (DIR 2) or z (DIR 3) sweep
+// (advec_mom_kernel.f90:254-288 y, :339-374 z, as k_mom_node forms it over
+// the caller's arrays): node flux over nodes min-2..max+2 along the sweep,
+// node_mass_post and node_mass_pre (the lower neighbour's node flux formed
+// again) over min-1..max+2. The block marches the sweep axis p (z for the z
+// sweep; y for the y sweep, whose boxes are x-z slices) over rows r (y; z).
+// Plane p: the sweep's mass flux, density1 and post_vol, rows r0-1..r0+7.
+// Node p reads planes p-1..p+1 (mass flux) and p-1, p (cells); the mass-flux
+// plane below min-2 lies outside the array, reads as zeros and is not used.
+struct NodeDropPlane {
+  static constexpr int kBytes = 3 * kBox9;
+  static constexpr unsigned kTx = 3 * box_bytes<double>(9);
+  __device__ static double* arr(unsigned char* p, int q) { return (double*)(p + q * kBox9); }
+};
+
+template <int DIR, int RING, int MINB>
+__global__ void __launch_bounds__(TX * TY, MINB)
+k_mom_node_dropin_tma(Geom g, int seg, const __grid_constant__ NodeDropMaps maps,
+                      double* __restrict__ node_flux, double* __restrict__ node_mass_post,
+                      double* __restrict__ node_mass_pre, int* __restrict__ status) {
+  using P = NodeDropPlane;
+  extern __shared__ __align__(128) unsigned char ring[];
+  __shared__ unsigned long long full[RING];
+  __shared__ int stop;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int pmin = DIR == 2 ? g.y_min : g.z_min, pmax = DIR == 2 ? g.y_max : g.z_max;
+  const int rmin = DIR == 2 ? g.z_min : g.y_min, rmax = DIR == 2 ? g.z_max : g.y_max;
+  const int j = g.x_min + TX * (int)blockIdx.x + tx, r0 = rmin + TY * (int)blockIdx.y;
+  const int r = r0 + ty;
+  const int q0 = pmin - 2 + seg * (int)blockIdx.z;
+  const int q1 = q0 + seg - 1 < pmax + 2 ? q0 + seg - 1 : pmax + 2;
+  const bool in_jr = j <= g.x_max + 1 && r <= rmax + 1;
+  const PlaneMarch<RING, 1, 1> pm{ring, P::kBytes, full, &stop, q0 - 1, q1 + 1};
+  constexpr int W = kDropW, H = kDropH;
+  auto issue = [&](int p) {
+    unsigned char* b = pm.buf(p);
+    unsigned long long* bar = pm.bar(p);
+    mbar_arrive_expect_tx(bar, P::kTx);
+    const int x = TX * (int)blockIdx.x;
+    const int rr = r0 - 1 - rmin + 2, pp = p - pmin + 2;
+    const int y = DIR == 2 ? pp : rr, z = DIR == 2 ? rr : pp;
+    tma_load_box(P::arr(b, 0), &maps.mf, bar, x, y, z);
+    tma_load_box(P::arr(b, 1), &maps.d, bar, x, y, z);
+    tma_load_box(P::arr(b, 2), &maps.pv, bar, x, y, z);
+  };
+  pm.run(q0, q1, status, issue, [&](int p) {
+    if (!in_jr) return;
+    unsigned char* bd = pm.buf(p - 1);
+    unsigned char* bl = pm.buf(p);
+    unsigned char* bu = pm.buf(p + 1);
+    // array q at column j+a, row r+b of a plane buffer (rows from r0-1)
+#define AT(bb, q, a, b) (P::arr(bb, q)[(ty + 1 + (b)) * W + tx + H + (a)])
+    // the node flux of node (j, r, p) from mass-flux planes lo (p) and hi (p+1)
+    auto nflux = [&](unsigned char* lo, unsigned char* hi) {
+      if (DIR == 3)  // mf(j-1,k,l) + mf(j,k,l) + mf(j-1,k,l+1) + mf(j,k,l+1) + the k-1 row
+        return 0.125 * (AT(lo, 0, -1, 0) + AT(lo, 0, 0, 0) + AT(hi, 0, -1, 0) + AT(hi, 0, 0, 0) +
+                        AT(lo, 0, -1, -1) + AT(lo, 0, 0, -1) + AT(hi, 0, -1, -1) + AT(hi, 0, 0, -1));
+      // mf(j-1,k,l) + mf(j,k,l) + mf(j-1,k+1,l) + mf(j,k+1,l) + the l-1 row
+      return 0.125 * (AT(lo, 0, -1, 0) + AT(lo, 0, 0, 0) + AT(hi, 0, -1, 0) + AT(hi, 0, 0, 0) +
+                      AT(lo, 0, -1, -1) + AT(lo, 0, 0, -1) + AT(hi, 0, -1, -1) + AT(hi, 0, 0, -1));
+    };
+    const double nf = nflux(bl, bu);
+    const long long o = DIR == 2 ? off3(g, j, p, r) : off3(g, j, r, p);
+    node_flux[o] = nf;
+    if (p >= pmin - 1) {
+      // cell (j+a, r+b) of cell plane p+c: the reference's order of the eight
+      // cells, (a, p-offset, r-offset) in DIR 3's (j, k, l) terms
+#define DP(a, b, bb) (AT(bb, 1, a, b) * AT(bb, 2, a, b))
+      double nm;
+      if (DIR == 3)  // DP(0,-1,0) DP(0,0,0) DP(-1,-1,0) DP(-1,0,0) then the l-1 plane
+        nm = 0.125 * (DP(0, -1, bl) + DP(0, 0, bl) + DP(-1, -1, bl) + DP(-1, 0, bl) +
+                      DP(0, -1, bd) + DP(0, 0, bd) + DP(-1, -1, bd) + DP(-1, 0, bd));
+      else  // (j, k-1, l) (j, k, l) (j-1, k-1, l) (j-1, k, l) then the l-1 row
+        nm = 0.125 * (DP(0, 0, bd) + DP(0, 0, bl) + DP(-1, 0, bd) + DP(-1, 0, bl) +
+                      DP(0, -1, bd) + DP(0, -1, bl) + DP(-1, -1, bd) + DP(-1, -1, bl));
+#undef DP
+      node_mass_post[o] = nm;
+      node_mass_pre[o] = nm - nflux(bd, bl) + nf;
+    }
+#undef AT
+  });
+}
+
+// ---------------------------------------------------------------------------
 // The node pass of the y or z momentum sweep (advec_mom_kernel.f90:254-293 for
 // y, :339-379 for z), as k_mom_node_march (clover_fused.cu) forms it, with the
 // inputs staged in shared memory. The lane layout stays: lane L of a warp holds
@@ -2061,6 +2145,32 @@ void launch_accelerate_dropin_tma(const Geom& g, cudaStream_t s, double dt,
   k_accelerate_dropin_tma<kStencilRing, kDropMinBlocks>
       <<<grid, dim3(TX, TY), kStencilRing * AccDropPlane::kBytes, s>>>(g, seg, dt, maps, xvel1,
                                                                         yvel1, zvel1, status);
+}
+
+bool mom_node_dropin_tma_prepare() {
+  return cudaFuncSetAttribute(k_mom_node_dropin_tma<2, kStencilRing, 4>,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              kStencilRing * NodeDropPlane::kBytes) == cudaSuccess &&
+         cudaFuncSetAttribute(k_mom_node_dropin_tma<3, kStencilRing, 4>,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              kStencilRing * NodeDropPlane::kBytes) == cudaSuccess;
+}
+
+void launch_mom_node_dropin_tma(const Geom& g, cudaStream_t s, int dir, const NodeDropMaps& maps,
+                                double* node_flux, double* node_mass_post, double* node_mass_pre,
+                                int* status) {
+  const int nr = (dir == 2 ? g.z_max - g.z_min : g.y_max - g.y_min) + 2;
+  const int np = (dir == 2 ? g.y_max - g.y_min : g.z_max - g.z_min) + 5;
+  const int gx = (g.x_max + 1 - g.x_min + TX) / TX, gy = (nr + TY - 1) / TY;
+  const int seg = drop_seg(np, gx * gy);
+  const dim3 grid(gx, gy, (np + seg - 1) / seg);
+  const int smem = kStencilRing * NodeDropPlane::kBytes;
+  if (dir == 2)
+    k_mom_node_dropin_tma<2, kStencilRing, 4><<<grid, dim3(TX, TY), smem, s>>>(
+        g, seg, maps, node_flux, node_mass_post, node_mass_pre, status);
+  else
+    k_mom_node_dropin_tma<3, kStencilRing, 4><<<grid, dim3(TX, TY), smem, s>>>(
+        g, seg, maps, node_flux, node_mass_post, node_mass_pre, status);
 }
 
 template <class S>

@@ -130,6 +130,16 @@ void launch_accelerate_dropin_tma(const Geom& g, cudaStream_t s, double dt,
                                   const AccDropMaps& maps, double* xvel1, double* yvel1,
                                   double* zvel1, int* status);
 
+// The maps of the drop-in y/z momentum node pass: the sweep's mass flux,
+// density1 and post_vol, 9 rows (x-z slices for the y sweep).
+struct NodeDropMaps {
+  CUtensorMap mf, d, pv;
+};
+bool mom_node_dropin_tma_prepare();
+void launch_mom_node_dropin_tma(const Geom& g, cudaStream_t s, int dir, const NodeDropMaps& maps,
+                                double* node_flux, double* node_mass_post, double* node_mass_pre,
+                                int* status);
+
 // The maps of the y/z momentum node pass: mass flux of the sweep direction
 // and density1 (9 rows from c0-1), and the volume fluxes its post volumes
 // take (vol_flux_x 9 rows, the row-direction flux 10 rows: vol_flux_y for
