@@ -136,6 +136,14 @@ k_visc_dt_tma(Geom g, int seg, GeomArrays ga, double g_small, double dtc_safe, d
   };
   const A a_gs = (A)g_small, a_dtc = (A)dtc_safe, a_dtu = (A)dtu_safe, a_dtv = (A)dtv_safe;
   const A a_dtw = (A)dtw_safe, a_dtdiv = (A)dtdiv_safe;
+  // calc_dt's four velocity quotients where the denominator is its floor
+  // (1.0e-5 * volume: every cell at rest), formed once: the same operands give
+  // the same quotient, so those cells skip the division (FP64 only: the FP32
+  // division of the mixed path costs less than the test, measured)
+  constexpr bool kFloor = sizeof(A) == 8;
+  const A a_vol = (A)g.vol, a_flo = A(1.0e-5) * a_vol, a_flo_div = a_vol * A(1.0e-05);
+  const A q_u = a_dtu * A(4.0) * a_vol / a_flo, q_v = a_dtv * A(4.0) * a_vol / a_flo;
+  const A q_w = a_dtw * A(4.0) * a_vol / a_flo, q_div = a_dtdiv * A(4.0) * a_vol / a_flo_div;
   constexpr int WV = P::WV, WR = P::WR, WE = P::WE, HV = P::HV, HR = P::HR, HE = P::HE;
   unsigned long long key = ~0ull;
   wait(pfirst);
@@ -235,20 +243,26 @@ k_visc_dt_tma(Geom g, int seg, GeomArrays ga, double g_small, double dtc_safe, d
         ss = (A)ss_st;
       }
       A cc = ss * ss;
-      cc = cc + A(2.0) * visc / d0;
+      // a zero viscosity over a positive density adds a zero to ss*ss (>= +0):
+      // cc is unchanged, without the division
+      if (!kFloor || visc != A(0.0) || !(d0 > A(0.0))) cc = cc + A(2.0) * visc / d0;
       A dtct = ds * cc;
       dtct = a_dtc * A(1.0) / fmax2(sqrt(dtct), a_gs);
-      const A vol = (A)g.vol;
+      const A vol = a_vol;
       const A du1 = ugradx1 * xa, du2 = ugradx2 * xa;
-      const A dtut = a_dtu * A(4.0) * vol / fmax2(fmax2(fabs(du1), fabs(du2)), A(1.0e-5) * vol);
+      const A mu = fmax2(fmax2(fabs(du1), fabs(du2)), a_flo);
+      const A dtut = kFloor && mu == a_flo ? q_u : a_dtu * A(4.0) * vol / mu;
       const A dv1 = vgrady1 * ya, dv2 = vgrady2 * ya;
-      const A dtvt = a_dtv * A(4.0) * vol / fmax2(fmax2(fabs(dv1), fabs(dv2)), A(1.0e-5) * vol);
+      const A mv = fmax2(fmax2(fabs(dv1), fabs(dv2)), a_flo);
+      const A dtvt = kFloor && mv == a_flo ? q_v : a_dtv * A(4.0) * vol / mv;
       // both z faces use zarea(j,k,l); its sums add (j,k+1) before (j+1,k)
       const A dw1 = (w000 + w010 + w100 + w110) * za;
       const A dw2 = (w001 + w011 + w101 + w111) * za;
-      const A dtwt = a_dtw * A(4.0) * vol / fmax2(fmax2(fabs(dw1), fabs(dw2)), A(1.0e-5) * vol);
+      const A mw = fmax2(fmax2(fabs(dw1), fabs(dw2)), a_flo);
+      const A dtwt = kFloor && mw == a_flo ? q_w : a_dtw * A(4.0) * vol / mw;
       const A dvg = du2 - du1 + dv2 - dv1 + dw2 - dw1;
-      const A dtdivt = a_dtdiv * A(4.0) * vol / fmax2(vol * A(1.0e-05), fabs(dvg));
+      const A mdv = fmax2(a_flo_div, fabs(dvg));
+      const A dtdivt = kFloor && mdv == a_flo_div ? q_div : a_dtdiv * A(4.0) * vol / mdv;
       const A mn = fmin2(fmin2(fmin2(fmin2(dtct, dtut), dtvt), dtwt), dtdivt);
       if (!(mn != mn)) {
         const unsigned long long kc = key_of(mn);
