@@ -411,16 +411,25 @@ void oracle_flux_calc_kernel(const int *x_min, const int *x_max, const int *y_mi
             (V3(yvel0, j, k, l) + V3(yvel0, j + 1, k, l) + V3(yvel0, j, k, l + 1) +
              V3(yvel0, j + 1, k, l + 1) + V3(yvel1, j, k, l) + V3(yvel1, j + 1, k, l) +
              V3(yvel1, j, k, l + 1) + V3(yvel1, j + 1, k, l + 1));
-  /* the zvel0 sum repeats zvel0(j+1,k,l) and omits zvel0(j,k+1,l) (:86) */
+  /* the zvel0 sum repeats zvel0(j+1,k,l) and omits zvel0(j,k+1,l) (:86).
+   * ORACLE_FLUX_Z_PDV (a test-only build, never the checker of a parity
+   * test) takes the four nodes PdV_kernel.f90 sums instead, to show that the
+   * FP64 run's mass drift comes from this sum alone. */
+#ifdef ORACLE_FLUX_Z_PDV
+#define FLUX_Z_NODE3 V3(zvel0, j, k + 1, l)
+#else
+#define FLUX_Z_NODE3 V3(zvel0, j + 1, k, l)
+#endif
 #pragma omp parallel for
   for (int l = *z_min; l <= *z_max + 1; l++)
     for (int k = *y_min; k <= *y_max; k++)
       for (int j = *x_min; j <= *x_max; j++)
         Z3(vol_flux_z, j, k, l) =
             0.125 * dtv * Z3(zarea, j, k, l) *
-            (V3(zvel0, j, k, l) + V3(zvel0, j + 1, k, l) + V3(zvel0, j + 1, k, l) +
+            (V3(zvel0, j, k, l) + V3(zvel0, j + 1, k, l) + FLUX_Z_NODE3 +
              V3(zvel0, j + 1, k + 1, l) + V3(zvel1, j, k, l) + V3(zvel1, j + 1, k, l) +
              V3(zvel1, j, k + 1, l) + V3(zvel1, j + 1, k + 1, l));
+#undef FLUX_Z_NODE3
 }
 
 /* Van Leer limited face flux, shared by the three directions of

@@ -18,6 +18,9 @@ FAST_LIB_PATH = os.path.join(ORACLE_DIR, "_build", "liboracle_fast.so")
 # parity build with two direction-dependent extents of the reference made
 # symmetric (ORACLE_SYMMETRIC_HALO): only the rotation tests load it
 SYMMETRIC_LIB_PATH = os.path.join(ORACLE_DIR, "_build", "liboracle_symmetric.so")
+# parity build whose flux_calc z sum takes PdV's four nodes (ORACLE_FLUX_Z_PDV):
+# only the mass-drift test loads it
+FLUXZ_LIB_PATH = os.path.join(ORACLE_DIR, "_build", "liboracle_fluxz.so")
 
 # Reference field ids (data.f90:55-74), 1-based, in order.
 FIELD_NAMES = [
@@ -76,8 +79,9 @@ def build():
 _LIBS = {}
 
 
-def load(fast=False, symmetric=False):
-    path = SYMMETRIC_LIB_PATH if symmetric else FAST_LIB_PATH if fast else LIB_PATH
+def load(fast=False, symmetric=False, fluxz=False):
+    path = (FLUXZ_LIB_PATH if fluxz else SYMMETRIC_LIB_PATH if symmetric
+            else FAST_LIB_PATH if fast else LIB_PATH)
     if path not in _LIBS:
         if not os.path.exists(path):
             build()
@@ -122,9 +126,9 @@ def make_deck(d):
     return od
 
 
-def run(deck, max_steps=None, want_fields=False, fast=False, symmetric=False):
+def run(deck, max_steps=None, want_fields=False, fast=False, symmetric=False, fluxz=False):
     """Run the oracle hydro loop. Returns dict(dt, summaries, summary_steps, steps, fields)."""
-    lib = load(fast, symmetric)
+    lib = load(fast, symmetric, fluxz)
     od = make_deck(deck)
     if max_steps is None:
         max_steps = od.end_step

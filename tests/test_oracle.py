@@ -221,3 +221,18 @@ def test_rotated_runs_equal_the_x_run_to_rounding():
             a = rx["fields"][n][2:-2, 2:-2, 2:-2]
             b = rr["fields"][_x_name(n, axis)].transpose(_PERM[axis])[2:-2, 2:-2, 2:-2]
             assert np.abs(a - b).max() <= 8 * np.spacing(np.abs(a).max()), (axis, n)
+
+
+def test_fp64_mass_drift_is_the_flux_calc_z_sum():
+    """On the benchmark's two-state problem the reference (FP64) does not
+    conserve mass: 1e-4 relative over 40 steps at 24^3. flux_calc_kernel.f90:86
+    sums zvel0 over nodes (j,k), (j+1,k), (j+1,k), (j+1,k+1) where the PdV
+    kernel sums (j,k), (j+1,k), (j,k+1), (j+1,k+1), so the advection's z volume
+    fluxes do not cancel the PdV volume change. A test-only build of the oracle
+    whose z sum takes PdV's four nodes (ORACLE_FLUX_Z_PDV) conserves mass to
+    rounding on the same deck: the drift is that sum's alone."""
+    d = decks.shock(24, 24, 24, 40)
+    ref = np.array(O.run(d)["summaries"])[:, 1]
+    pdv = np.array(O.run(d, fluxz=True)["summaries"])[:, 1]
+    assert np.abs(ref / ref[0] - 1).max() > 1e-5
+    assert np.abs(pdv / pdv[0] - 1).max() < 1e-14
