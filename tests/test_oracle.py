@@ -236,3 +236,35 @@ def test_fp64_mass_drift_is_the_flux_calc_z_sum():
     pdv = np.array(O.run(d, fluxz=True)["summaries"])[:, 1]
     assert np.abs(ref / ref[0] - 1).max() > 1e-5
     assert np.abs(pdv / pdv[0] - 1).max() < 1e-14
+
+
+def _deck_of(struct, region_energy_scale=1.0):
+    """A drawn ensemble deck (cloverleaf3d_ref_b200.draw_decks) as the oracle's
+    mapping, the region's energy scaled."""
+    s = struct
+    d = {k: getattr(s, k) for k in ("x_cells", "y_cells", "z_cells", "xmin", "ymin", "zmin",
+                                     "xmax", "ymax", "zmax", "initial_timestep", "max_timestep",
+                                     "timestep_rise", "end_time", "end_step", "summary_frequency")}
+    states = [dict(density=s.state_density[0], energy=s.state_energy[0])]
+    states.append(dict(density=s.state_density[1], energy=s.state_energy[1] * region_energy_scale,
+                       geometry="cuboid", xmin=s.state_xmin[1], xmax=s.state_xmax[1],
+                       ymin=s.state_ymin[1], ymax=s.state_ymax[1], zmin=s.state_zmin[1],
+                       zmax=s.state_zmax[1]))
+    d["states"] = states
+    return d
+
+
+def test_drawn_ensemble_deck_is_ill_conditioned_in_fp64():
+    """Deck 20 of the 64-deck ensemble (seed 2024; 35x111x96 cells on the
+    [0,10]^3 cube): a 1e-7 relative change of the region's energy, FP64 alone,
+    moves the internal energy by 4.9e-5 and the kinetic energy by 6.0e-5 (more
+    than 1e-5 and 3e-5) within the configuration's 150 steps. A storage precision that
+    rounds at 1e-7 every step cannot meet 1e-5 against FP64 on such decks."""
+    import cloverleaf3d_ref_b200 as C
+    s = C.draw_decks(64, 2024)[20].s
+    assert (s.x_cells, s.y_cells, s.z_cells, s.end_step) == (35, 111, 96, 150)
+    a = np.array(O.run(_deck_of(s), fast=True)["summaries"])
+    b = np.array(O.run(_deck_of(s, 1.0 + 1e-7), fast=True)["summaries"])
+    moving = a[:, 3] > 0
+    assert np.abs(b[:, 2] / a[:, 2] - 1).max() > 1e-5
+    assert np.abs(b[moving, 3] / a[moving, 3] - 1).max() > 3e-5
