@@ -1250,9 +1250,13 @@ void launch_advec_cell_x(const Target& tg, cudaStream_t s, int sweep, const Geom
                          typename S::rho_t* density1_out, typename S::ene_t* energy1_out,
                          const typename S::vf_t* vol_flux_x, const typename S::vf_t* vol_flux_y,
                          const typename S::vf_t* vol_flux_z, typename S::mf_t* mass_flux_x,
-                         bool copy_shell, const Level0<S>& level0) {
+                         bool copy_shell, const Level0<S>& level0, const CellXMaps* maps,
+                         int* status) {
   // pre_vol variant: 0 on sweep 1 (all three flux differences), 1 on sweep 3
-  if (sweep == 1)
+  if (maps && !tg.plan)  // one chunk: planes staged by bulk-tensor copies
+    launch_cell_sweep_x_tma<S>(tg.g, s, sweep, *maps, ga, density1_out, energy1_out, mass_flux_x,
+                               level0, status);
+  else if (sweep == 1)
     launch_mapped(tg, s, kKeyCellSweepX, grid_cell_sweep_x, 0, false, kBlk,
                   k_cell_sweep_x<S, 0, MapSingle>, k_cell_sweep_x<S, 0, MapBatchFree>, ga,
                   density1_in, energy1_in, density1_out, energy1_out, vol_flux_x, vol_flux_y,
@@ -1369,7 +1373,7 @@ void launch_advec_mom_fused(const Target& tg, cudaStream_t s, int advect_x, int 
   template void launch_advec_cell_x<S>(const Target&, cudaStream_t, int, const GeomArrays&,      \
                                        const S::rho_t*, const S::ene_t*, S::rho_t*, S::ene_t*,  \
                                        const S::vf_t*, const S::vf_t*, const S::vf_t*,          \
-                                       S::mf_t*, bool, const Level0<S>&);                       \
+                                       S::mf_t*, bool, const Level0<S>&, const CellXMaps*, int*); \
   template void launch_advec_mom_fused<S>(const Target&, cudaStream_t, int, int, int, double,    \
                                           const GeomArrays&, const S::rho_t*, const S::mf_t*,  \
                                           const S::mf_t*, const S::mf_t*, const S::vf_t*,      \

@@ -388,13 +388,15 @@ void launch_advec_cell_fused(const Target& tg, cudaStream_t s, int advect_x, int
 // updated values in the other, and with copy_shell a copy of every cell
 // outside the interior (left out where a depth-2 halo update of density1 and
 // energy1 follows, which rewrites all of them from the interior).
+struct CellXMaps;  // clover_tma.cuh
 template <class S>
 void launch_advec_cell_x(const Target& tg, cudaStream_t s, int sweep, const GeomArrays& ga,
                          const typename S::rho_t* density1_in, const typename S::ene_t* energy1_in,
                          typename S::rho_t* density1_out, typename S::ene_t* energy1_out,
                          const typename S::vf_t* vol_flux_x, const typename S::vf_t* vol_flux_y,
                          const typename S::vf_t* vol_flux_z, typename S::mf_t* mass_flux_x,
-                         bool copy_shell, const Level0<S>& level0);
+                         bool copy_shell, const Level0<S>& level0,
+                         const CellXMaps* maps = nullptr, int* status = nullptr);
 // All three velocities of one sweep; vel_in/vel_out are the two buffers of
 // each velocity pair, and with copy_shell the shell outside [min,max+1]^3 is
 // copied across (left out where a depth-2 halo update of the velocities

@@ -198,6 +198,15 @@ struct Chunk : ChunkBase {
   }
   // the maps of the staged y (dir 2) or z (dir 3) cell sweep reading buffer cb
   // of the density1/energy1 pair, with pre-volume variant var
+  // the maps of the staged x cell sweep of sweep 1 or 3 reading buffer cb of
+  // the density1/energy1 pair
+  bool cell_x_maps(int sweep, int cb, CellXMaps* m) {
+    bool ok = tmap(rho1(cb), sizeof(R), 8, &m->d) && tmap(ene1(cb), sizeof(En), 8, &m->e) &&
+              tmap(vol_flux_x, sizeof(VF), 8, &m->vfx);
+    if (ok && sweep == 1)
+      ok = tmap(vol_flux_y, sizeof(VF), 9, &m->vfy) && tmap(vol_flux_z, sizeof(VF), 8, &m->vfz);
+    return ok;
+  }
   bool cell_maps(int dir, int var, int cb, CellMaps* m) {
     const bool zr = dir == 2;
     bool ok = tmap(rho1(cb), sizeof(R), 8, &m->d, zr) && tmap(ene1(cb), sizeof(En), 8, &m->e, zr) &&
@@ -405,6 +414,7 @@ struct Chunk : ChunkBase {
     if (!batched)
       tma = visc_dt_tma_prepare<S>() && mom_x_tma_prepare<S>() && stencils_tma_prepare<S>() &&
             mom_node_tma_prepare<S>() && mom_vel_tma_prepare<S>() && cell_sweep_tma_prepare<S>() &&
+            cell_sweep_x_tma_prepare<S>() &&
             visc_dt_tma_maps<S>(g, xvel0, yvel0, zvel0, density0, energy0, &visc_maps);
 
     dt_cap = deck.end_step < (1 << 22) ? deck.end_step + 16 : (1 << 22);
@@ -887,9 +897,11 @@ struct Chunk : ChunkBase {
       if (dir == 1) {
         // one pass, out of place into the other buffer of the pair
         // the post-sweep depth-2 halo update rewrites the output pair's shell
+        CellXMaps xm;
+        const bool x_tma = tma && use_tma && cell_x_maps(sweep_number, cb, &xm);
         launch_advec_cell_x<S>(tg, stream, sweep_number, ga, rho1(cb), ene1(cb), rho1(cb ^ 1),
                                ene1(cb ^ 1), vol_flux_x, vol_flux_y, vol_flux_z, mass_flux_x,
-                               !halo_repeat_free, l0);
+                               !halo_repeat_free, l0, x_tma ? &xm : nullptr, &sc->status);
         cb ^= 1;
         pend("advec_cell_x", n * (nvf * VF8 + (2 + nl0) * (R8 + E8) + MF8));
       } else {

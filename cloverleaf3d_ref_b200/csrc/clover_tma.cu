@@ -1954,6 +1954,173 @@ k_cell_sweep_tma(Geom g, int seg, GeomArrays ga, const __grid_constant__ CellMap
 #undef IDX
 }
 
+// The x cell sweep (advec_cell_kernel.f90:97-186) out of place, its inputs
+// staged in shared memory, as k_cell_sweep_x (clover_fused.cu) forms it. Lane
+// m of a warp takes face and cell c = x_min+31t+m of one row: it forms the
+// fluxes at face c from cells c-2..c+1 of the row's box, and lanes 0..30
+// update cell c from faces c and c+1 (lane m+1's) into the output pair, so
+// 31 cells per warp and no thread reads what another writes. Plane p:
+// density1, energy1 and vol_flux_x (rows k0..k0+7) and, for pre-volume
+// variant 0, vol_flux_y (rows k0..k0+8) and vol_flux_z (rows k0..k0+7);
+// cell l reads planes l and l+1 (vol_flux_z).
+constexpr int kCellXLanes = 31;
+
+// The box x coordinate (from the map's base, H columns before x_min) of tile
+// t and the column of the tile's first cell x_min+31t in the box: the box
+// starts two cells before it, rounded down to 16 bytes.
+template <class T>
+__device__ __forceinline__ void cell_x_box(int t, int& x, int& col) {
+  constexpr int H = kTmaHalo<T>;
+  const int c = kCellXLanes * t + H - 2;  // the column of cell x_min+31t-2
+  x = c / H * H;
+  col = c - x + 2;
+}
+
+template <class S, int VAR>
+struct CellXPlane {
+  using R = typename S::rho_t;
+  using En = typename S::ene_t;
+  using VF = typename S::vf_t;
+  static constexpr bool kVf = VAR == 0;
+  static constexpr int kRho = round128(8 * kTmaWidth<R> * (int)sizeof(R));
+  static constexpr int kEne = round128(8 * kTmaWidth<En> * (int)sizeof(En));
+  static constexpr int kVf8 = round128(8 * kTmaWidth<VF> * (int)sizeof(VF));
+  static constexpr int kVf9 = round128(9 * kTmaWidth<VF> * (int)sizeof(VF));
+  static constexpr int kBytes = kRho + kEne + kVf8 + (kVf ? kVf9 + kVf8 : 0);
+  static constexpr unsigned kTx = box_bytes<R>(8) + box_bytes<En>(8) + box_bytes<VF>(8) +
+                                  (kVf ? box_bytes<VF>(9) + box_bytes<VF>(8) : 0u);
+  __device__ static R* rho(unsigned char* p) { return (R*)p; }
+  __device__ static En* ene(unsigned char* p) { return (En*)(p + kRho); }
+  __device__ static VF* vfx(unsigned char* p) { return (VF*)(p + kRho + kEne); }
+  __device__ static VF* vfy(unsigned char* p) { return (VF*)(p + kRho + kEne + kVf8); }
+  __device__ static VF* vfz(unsigned char* p) { return (VF*)(p + kRho + kEne + kVf8 + kVf9); }
+};
+
+template <class S, int VAR, int RING, int MINB>
+__global__ void __launch_bounds__(TX * TY, MINB)
+k_cell_sweep_x_tma(Geom g, int seg, GeomArrays ga, const __grid_constant__ CellXMaps maps,
+                   typename S::rho_t* __restrict__ d_out, typename S::ene_t* __restrict__ e_out,
+                   typename S::mf_t* __restrict__ mass_flux, Level0<S> lz,
+                   int* __restrict__ status) {
+  using P = CellXPlane<S, VAR>;
+  using R = typename S::rho_t;
+  using En = typename S::ene_t;
+  using VF = typename S::vf_t;
+  using MF = typename S::mf_t;
+  using AL = typename S::arith_t;  // the limiters' arithmetic
+  extern __shared__ __align__(128) unsigned char ring[];
+  __shared__ unsigned long long full[RING];
+  __shared__ int stop;
+  const int lane = threadIdx.x, ty = threadIdx.y;
+  const int c = g.x_min + kCellXLanes * (int)blockIdx.x + lane;  // this lane's face and cell
+  const int k0 = g.y_min + TY * (int)blockIdx.y, k = k0 + ty;
+  const int l0 = g.z_min + seg * (int)blockIdx.z;
+  const int l1 = l0 + seg - 1 < g.z_max ? l0 + seg - 1 : g.z_max;
+  const bool row = k <= g.y_max;  // the whole warp: k is the row's
+  const int top = g.x_max + 2;
+  const bool face = row && c <= top;
+  const bool upd = row && lane < kCellXLanes && c <= g.x_max;
+  const PlaneMarch<RING, 0, 1> pm{ring, P::kBytes, full, &stop, l0, l1 + 1};
+  int xr, cr, xe, ce, xf, cf;
+  cell_x_box<R>(blockIdx.x, xr, cr);
+  cell_x_box<En>(blockIdx.x, xe, ce);
+  cell_x_box<VF>(blockIdx.x, xf, cf);
+  cr += lane; ce += lane; cf += lane;  // cell c in each box
+  constexpr int WR = kTmaWidth<R>, WE = kTmaWidth<En>, WF = kTmaWidth<VF>;
+  // vertexdx at c-1, c and MIN(c+1, x_max+2)
+  const double* vdx = ga.vertexdx + g.o1 + 2 - g.x_min;
+  const double vd_0 = face ? vdx[c] : 1.0;
+  const double vd_m1 = face ? vdx[c - 1] : 1.0;
+  const double vd_p1 = face && c + 1 <= top ? vdx[c + 1] : vd_0;
+  auto issue = [&](int p) {
+    unsigned char* b = pm.buf(p);
+    unsigned long long* bar = pm.bar(p);
+    mbar_arrive_expect_tx(bar, P::kTx);
+    const int y = k0 - g.y_min + 2, z = p - g.z_min + 2;
+    tma_load_box(P::rho(b), &maps.d, bar, xr, y, z);
+    tma_load_box(P::ene(b), &maps.e, bar, xe, y, z);
+    tma_load_box(P::vfx(b), &maps.vfx, bar, xf, y, z);
+    if (P::kVf) {
+      tma_load_box(P::vfy(b), &maps.vfy, bar, xf, y, z);
+      tma_load_box(P::vfz(b), &maps.vfz, bar, xf, y, z);
+    }
+  };
+  pm.run(l0, l1, status, issue, [&](int l) {
+    if (!row) return;
+    unsigned char* b = pm.buf(l);
+    unsigned char* bz = pm.buf(l + 1);
+    const R* dr = P::rho(b) + ty * WR + cr;
+    const En* er = P::ene(b) + ty * WE + ce;
+    const VF* fx = P::vfx(b) + ty * WF + cf;
+    // the pre-volume of cell c+a (a = -1, 0): cell_pre_vol's variants 0 and 1
+    auto pre_vol = [&](int a) {
+      const double vol = g.vol;
+      const double fx1 = (double)fx[a + 1], fx0 = (double)fx[a];
+      if (VAR == 0) {
+        const VF* fy = P::vfy(b) + ty * WF + cf + a;
+        const double fy1 = (double)fy[WF], fy0 = (double)fy[0];
+        const double fz1 = (double)(P::vfz(bz) + ty * WF + cf)[a];
+        const double fz0 = (double)(P::vfz(b) + ty * WF + cf)[a];
+        return vol + (fx1 - fx0 + fy1 - fy0 + fz1 - fz0);
+      }
+      return vol + fx1 - fx0;
+    };
+    double mf_st = 0.0, ef = 0.0;
+    const double d = (double)dr[0], e = (double)er[0], vf = (double)fx[0];
+    const double pv = pre_vol(0);
+    if (face && c >= g.x_min) {
+      // advec_cell_kernel.f90:131-169 at face c; the upwind index clamps to x_max+2
+      const double d_m2 = (double)dr[-2], d_m1 = (double)dr[-1];
+      const double e_m2 = (double)er[-2], e_m1 = (double)er[-1];
+      double d_up, d_don, d_dn, e_up, e_don, e_dn, pv_don, vd_dif;
+      if (vf > 0.0) {  // upwind c-2, donor c-1, downwind c
+        d_up = d_m2; d_don = d_m1; d_dn = d; e_up = e_m2; e_don = e_m1; e_dn = e;
+        pv_don = pre_vol(-1); vd_dif = vd_m1;
+      } else {  // upwind min(c+1, x_max+2), donor c, downwind c-1
+        const bool clamp = c + 1 > top;
+        d_up = clamp ? d : (double)dr[1]; d_don = d; d_dn = d_m1;
+        e_up = clamp ? e : (double)er[1]; e_don = e; e_dn = e_m1;
+        pv_don = pv; vd_dif = clamp ? vd_0 : vd_p1;
+      }
+      const AL sigmat = (AL)fabs(vf) / (AL)pv_don;
+      const AL sigma3 = (AL(1.0) + sigmat) * (AL)width_ratio(vd_0, vd_dif);
+      const AL sigma4 = AL(2.0) - sigmat;
+      AL diffuw = (AL)(d_don - d_up);
+      AL diffdw = (AL)(d_dn - d_don);
+      AL limiter = cell_limiter<AL>(sigmat, sigma3, sigma4, diffuw, diffdw);
+      const double mflux = vf * (d_don + (double)limiter);
+      // the cell update takes the FP64 face fluxes; the stored mass flux
+      // (mf_t) feeds only the momentum sweep
+      mf_st = mflux;
+      if (lane < kCellXLanes) mass_flux[off3(g, c, k, l)] = st<MF>(mflux);
+      const AL sigmam = (AL)fabs(mflux) / ((AL)d_don * (AL)pv_don);
+      diffuw = (AL)(e_don - e_up);
+      diffdw = (AL)(e_dn - e_don);
+      limiter = cell_limiter<AL>(sigmam, sigma3, sigma4, diffuw, diffdw);
+      ef = mflux * (e_don + (double)limiter);
+    }
+    // advec_cell_kernel.f90:173-185 for cell c from faces c and c+1
+    const double mf_p = __shfl_down_sync(0xffffffffu, mf_st, 1);
+    const double ef_p = __shfl_down_sync(0xffffffffu, ef, 1);
+    if (upd) {
+      const double vf_p = (double)fx[1];
+      const double pm_ = d * pv;
+      const double pom = pm_ + mf_st - mf_p;
+      const double poe = (e * pm_ + ef - ef_p) / pom;
+      const double av = pv + vf - vf_p;
+      const R dn = st<R>(pom / av);
+      const En en = st<En>(poe);
+      const long long o = off3(g, c, k, l);
+      d_out[o] = dn;
+      e_out[o] = en;
+      if (lz.density0) {  // last sweep of the step: reset_field
+        lz.density0[o] = dn;
+        lz.energy0[o] = en;
+      }
+    }
+  });
+}
+
 constexpr int kViscRing = 4;
 constexpr int kViscSeg = 32;
 
@@ -2188,6 +2355,37 @@ void launch_mom_node_dropin_tma(const Geom& g, cudaStream_t s, int dir, const No
 }
 
 template <class S>
+constexpr int kCellXMinBlocks = sizeof(typename S::arith_t) == 4 ? 4 : 3;
+
+template <class S>
+bool cell_sweep_x_tma_prepare() {
+  return cudaFuncSetAttribute(k_cell_sweep_x_tma<S, 0, kStencilRing, kCellXMinBlocks<S>>,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              kStencilRing * CellXPlane<S, 0>::kBytes) == cudaSuccess &&
+         cudaFuncSetAttribute(k_cell_sweep_x_tma<S, 1, kStencilRing, kCellXMinBlocks<S>>,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              kStencilRing * CellXPlane<S, 1>::kBytes) == cudaSuccess;
+}
+
+template <class S>
+void launch_cell_sweep_x_tma(const Geom& g, cudaStream_t s, int sweep, const CellXMaps& maps,
+                             const GeomArrays& ga, typename S::rho_t* d_out,
+                             typename S::ene_t* e_out, typename S::mf_t* mass_flux_x,
+                             const Level0<S>& level0, int* status) {
+  // faces x_min..x_max+2, 31 per warp
+  const dim3 grid((g.x_max - g.x_min + 3 + kCellXLanes - 1) / kCellXLanes,
+                  (g.y_max - g.y_min + TY) / TY, (g.z_max - g.z_min + kStencilSeg) / kStencilSeg);
+  if (sweep == 1)
+    k_cell_sweep_x_tma<S, 0, kStencilRing, kCellXMinBlocks<S>>
+        <<<grid, dim3(TX, TY), kStencilRing * CellXPlane<S, 0>::kBytes, s>>>(
+            g, kStencilSeg, ga, maps, d_out, e_out, mass_flux_x, level0, status);
+  else
+    k_cell_sweep_x_tma<S, 1, kStencilRing, kCellXMinBlocks<S>>
+        <<<grid, dim3(TX, TY), kStencilRing * CellXPlane<S, 1>::kBytes, s>>>(
+            g, kStencilSeg, ga, maps, d_out, e_out, mass_flux_x, level0, status);
+}
+
+template <class S>
 void launch_pdv_predict_eos_tma(const Geom& g, cudaStream_t s, const double* dt_ptr,
                                 const PdvMaps& maps, typename S::cs_t* pressure, int* status) {
   const dim3 grid((g.x_max - g.x_min + TX) / TX, (g.y_max - g.y_min + TY) / TY,
@@ -2352,6 +2550,10 @@ void launch_cell_sweep_tma(const Geom& g, cudaStream_t s, int dir, int var, cons
                                       S::vel_t* const*, S::vel_t* const*, const Level0<S>&, int*); \
   template void launch_mom_node_tma<S>(const Geom&, cudaStream_t, int, int, const NodeMaps&,     \
                                        S::nd_t*, S::nd_t*, S::nd_t*, int*);                      \
+  template bool cell_sweep_x_tma_prepare<S>();                                                   \
+  template void launch_cell_sweep_x_tma<S>(const Geom&, cudaStream_t, int, const CellXMaps&,     \
+                                           const GeomArrays&, S::rho_t*, S::ene_t*, S::mf_t*,    \
+                                           const Level0<S>&, int*);                              \
   template void launch_pdv_predict_eos_tma<S>(const Geom&, cudaStream_t, const double*,         \
                                               const PdvMaps&, S::cs_t*, int*);                   \
   template void launch_accelerate_tma<S>(const Geom&, cudaStream_t, const double*,               \

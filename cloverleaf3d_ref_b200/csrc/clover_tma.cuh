@@ -140,6 +140,22 @@ void launch_mom_node_dropin_tma(const Geom& g, cudaStream_t s, int dir, const No
                                 double* node_flux, double* node_mass_post, double* node_mass_pre,
                                 int* status);
 
+// The maps of the x cell sweep reading one buffer of the density1/energy1
+// pair: density1, energy1, vol_flux_x and vol_flux_z (8 rows), vol_flux_y
+// (9 rows).
+struct CellXMaps {
+  CUtensorMap d, e, vfx, vfy, vfz;
+};
+template <class S>
+bool cell_sweep_x_tma_prepare();
+// The x cell sweep of the step's sweep 1 or 3, out of place into (d_out,
+// e_out), planes staged by bulk-tensor copies (interior cells only).
+template <class S>
+void launch_cell_sweep_x_tma(const Geom& g, cudaStream_t s, int sweep, const CellXMaps& maps,
+                             const GeomArrays& ga, typename S::rho_t* d_out,
+                             typename S::ene_t* e_out, typename S::mf_t* mass_flux_x,
+                             const Level0<S>& level0, int* status);
+
 // The maps of the y/z momentum node pass: mass flux of the sweep direction
 // and density1 (9 rows from c0-1), and the volume fluxes its post volumes
 // take (vol_flux_x 9 rows, the row-direction flux 10 rows: vol_flux_y for
