@@ -846,13 +846,13 @@ void clover_advec_mom_kernel(const int* x_min, const int* x_max, const int* y_mi
   double *v1 = VERT(vel1), *mfx = XF(mass_flux_x), *vfx = XF(vol_flux_x);
   double *mfy = YF(mass_flux_y), *vfy = YF(vol_flux_y), *mfz = ZF(mass_flux_z);
   double *vfz = ZF(vol_flux_z), *d1 = CELL(density1);
-  // the y/z node pass staged by bulk-tensor copies, between the volumes it
-  // reads and the flux + update
+  // the node pass staged by bulk-tensor copies, between the volumes it reads
+  // and the flux + update
   bool staged_node = false;
   NodeDropMaps nmaps;
   const int dir = *direction;
-  if (*which_vel == 1 && (dir == 2 || dir == 3) && staged(c)) {
-    const double* base[3] = {dir == 2 ? mfy : mfz, d1, work[6]};
+  if (*which_vel == 1 && staged(c)) {
+    const double* base[3] = {dir == 1 ? mfx : dir == 2 ? mfy : mfz, d1, work[6]};
     const int rows[3] = {9, 9, 9};
     CUtensorMap m[3];
     if (tmaps_of(c, g, 3, base, rows, m, dir == 2)) {

@@ -1478,6 +1478,68 @@ k_mom_node_dropin_tma(Geom g, int seg, const __grid_constant__ NodeDropMaps maps
 }
 
 // ---------------------------------------------------------------------------
+// The drop-in advec_mom node pass of the x sweep (advec_mom_kernel.f90:166-202
+// as k_mom_node forms it over the caller's arrays): node flux over nodes
+// x_min-2..x_max+2, node_mass_post and node_mass_pre (the left neighbour's
+// node flux formed again) over x_min-1..x_max+2, rows y_min..y_max+1, planes
+// z_min..z_max+1. Lane m of tile t takes node x_min-2+32t+m, whose box
+// starts two columns before it. Plane p: mass_flux_x, density1 and post_vol,
+// rows k0-1..k0+7; node l reads planes l-1 and l.
+template <int RING, int MINB>
+__global__ void __launch_bounds__(TX * TY, MINB)
+k_mom_node_x_dropin_tma(Geom g, int seg, const __grid_constant__ NodeDropMaps maps,
+                        double* __restrict__ node_flux, double* __restrict__ node_mass_post,
+                        double* __restrict__ node_mass_pre, int* __restrict__ status) {
+  using P = NodeDropPlane;
+  extern __shared__ __align__(128) unsigned char ring[];
+  __shared__ unsigned long long full[RING];
+  __shared__ int stop;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int j = g.x_min - 2 + TX * (int)blockIdx.x + tx, k0 = g.y_min + TY * (int)blockIdx.y;
+  const int k = k0 + ty;
+  const int l0 = g.z_min + seg * (int)blockIdx.z;
+  const int l1 = l0 + seg - 1 < g.z_max + 1 ? l0 + seg - 1 : g.z_max + 1;
+  const bool in_jk = j <= g.x_max + 2 && k <= g.y_max + 1;
+  const PlaneMarch<RING, 1, 0> pm{ring, P::kBytes, full, &stop, l0 - 1, l1};
+  constexpr int W = kDropW, H = kDropH;
+  auto issue = [&](int p) {
+    unsigned char* b = pm.buf(p);
+    unsigned long long* bar = pm.bar(p);
+    mbar_arrive_expect_tx(bar, P::kTx);
+    const int x = TX * (int)blockIdx.x - H, y = k0 - 1 - g.y_min + 2, z = p - g.z_min + 2;
+    tma_load_box(P::arr(b, 0), &maps.mf, bar, x, y, z);
+    tma_load_box(P::arr(b, 1), &maps.d, bar, x, y, z);
+    tma_load_box(P::arr(b, 2), &maps.pv, bar, x, y, z);
+  };
+  pm.run(l0, l1, status, issue, [&](int l) {
+    if (!in_jk) return;
+    unsigned char* bd = pm.buf(l - 1);
+    unsigned char* bl = pm.buf(l);
+    // array q at column j+a, row k+b of a plane buffer (rows from k0-1; the
+    // box starts H columns before this tile's first node)
+#define AT(bb, q, a, b) (P::arr(bb, q)[(ty + 1 + (b)) * W + tx + H + (a)])
+    // mf(j,k-1,l) + mf(j,k,l) + mf(j+1,k-1,l) + mf(j+1,k,l) + the l-1 plane, at node j+a
+    auto nflux = [&](int a) {
+      return 0.125 * (AT(bl, 0, a, -1) + AT(bl, 0, a, 0) + AT(bl, 0, a + 1, -1) + AT(bl, 0, a + 1, 0) +
+                      AT(bd, 0, a, -1) + AT(bd, 0, a, 0) + AT(bd, 0, a + 1, -1) + AT(bd, 0, a + 1, 0));
+    };
+    const double nf = nflux(0);
+    const long long o = off3(g, j, k, l);
+    node_flux[o] = nf;
+    if (j >= g.x_min - 1) {
+#define DP(a, b, bb) (AT(bb, 1, a, b) * AT(bb, 2, a, b))
+      // the reference's order: (j,k-1,l) (j,k,l) (j-1,k-1,l) (j-1,k,l), then plane l-1
+      const double nm = 0.125 * (DP(0, -1, bl) + DP(0, 0, bl) + DP(-1, -1, bl) + DP(-1, 0, bl) +
+                                 DP(0, -1, bd) + DP(0, 0, bd) + DP(-1, -1, bd) + DP(-1, 0, bd));
+#undef DP
+      node_mass_post[o] = nm;
+      node_mass_pre[o] = nm - nflux(-1) + nf;
+    }
+#undef AT
+  });
+}
+
+// ---------------------------------------------------------------------------
 // The node pass of the y or z momentum sweep (advec_mom_kernel.f90:254-293 for
 // y, :339-379 for z), as k_mom_node_march (clover_fused.cu) forms it, with the
 // inputs staged in shared memory. The lane layout stays: lane L of a warp holds
@@ -2329,7 +2391,10 @@ void launch_accelerate_dropin_tma(const Geom& g, cudaStream_t s, double dt,
 }
 
 bool mom_node_dropin_tma_prepare() {
-  return cudaFuncSetAttribute(k_mom_node_dropin_tma<2, kStencilRing, 4>,
+  return cudaFuncSetAttribute(k_mom_node_x_dropin_tma<kStencilRing, 4>,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              kStencilRing * NodeDropPlane::kBytes) == cudaSuccess &&
+         cudaFuncSetAttribute(k_mom_node_dropin_tma<2, kStencilRing, 4>,
                               cudaFuncAttributeMaxDynamicSharedMemorySize,
                               kStencilRing * NodeDropPlane::kBytes) == cudaSuccess &&
          cudaFuncSetAttribute(k_mom_node_dropin_tma<3, kStencilRing, 4>,
@@ -2340,12 +2405,20 @@ bool mom_node_dropin_tma_prepare() {
 void launch_mom_node_dropin_tma(const Geom& g, cudaStream_t s, int dir, const NodeDropMaps& maps,
                                 double* node_flux, double* node_mass_post, double* node_mass_pre,
                                 int* status) {
+  const int smem = kStencilRing * NodeDropPlane::kBytes;
+  if (dir == 1) {  // nodes x_min-2..x_max+2, 32 per tile
+    const int gx = (g.x_max - g.x_min + 5 + TX - 1) / TX, gy = (g.y_max - g.y_min + 2 + TY - 1) / TY;
+    const int nz = g.z_max - g.z_min + 2, seg = drop_seg(nz, gx * gy);
+    k_mom_node_x_dropin_tma<kStencilRing, 4><<<dim3(gx, gy, (nz + seg - 1) / seg), dim3(TX, TY),
+                                               smem, s>>>(g, seg, maps, node_flux, node_mass_post,
+                                                          node_mass_pre, status);
+    return;
+  }
   const int nr = (dir == 2 ? g.z_max - g.z_min : g.y_max - g.y_min) + 2;
   const int np = (dir == 2 ? g.y_max - g.y_min : g.z_max - g.z_min) + 5;
   const int gx = (g.x_max + 1 - g.x_min + TX) / TX, gy = (nr + TY - 1) / TY;
   const int seg = drop_seg(np, gx * gy);
   const dim3 grid(gx, gy, (np + seg - 1) / seg);
-  const int smem = kStencilRing * NodeDropPlane::kBytes;
   if (dir == 2)
     k_mom_node_dropin_tma<2, kStencilRing, 4><<<grid, dim3(TX, TY), smem, s>>>(
         g, seg, maps, node_flux, node_mass_post, node_mass_pre, status);

@@ -130,7 +130,7 @@ void launch_accelerate_dropin_tma(const Geom& g, cudaStream_t s, double dt,
                                   const AccDropMaps& maps, double* xvel1, double* yvel1,
                                   double* zvel1, int* status);
 
-// The maps of the drop-in y/z momentum node pass: the sweep's mass flux,
+// The maps of the drop-in momentum node pass: the sweep's mass flux,
 // density1 and post_vol, 9 rows (x-z slices for the y sweep).
 struct NodeDropMaps {
   CUtensorMap mf, d, pv;
