@@ -1135,6 +1135,13 @@ int clover_gpu_status(void) { return ctx().status; }
 
 void clover_gpu_use_staging(int on) { ctx().staging = on != 0; }
 
+int clover_gpu_wait_selftest_queued(long long cycles) {
+  Context& c = ctx();
+  if (!c.ready) return CLOVER_STATUS_NO_DEVICE;
+  launch_wait_selftest(c.stream, cycles, c.d_status);
+  return check(cudaGetLastError(), "wait selftest") ? 0 : CLOVER_STATUS_CUDA_ERROR;
+}
+
 const char* clover_gpu_error_string(void) { return ctx().err.c_str(); }
 
 void clover_gpu_clear_status(void) {

@@ -2643,6 +2643,10 @@ void launch_cell_sweep_tma(const Geom& g, cudaStream_t s, int dir, int var, cons
 INST_TMA(F64)
 INST_TMA(F32Mixed)
 
+void launch_wait_selftest(cudaStream_t s, long long cycles, int* status) {
+  k_wait_selftest<<<1, 32, 0, s>>>(cycles, status);
+}
+
 }  // namespace clover
 
 using namespace clover;

@@ -156,6 +156,11 @@ void launch_cell_sweep_x_tma(const Geom& g, cudaStream_t s, int sweep, const Cel
                              typename S::ene_t* e_out, typename S::mf_t* mass_flux_x,
                              const Level0<S>& level0, int* status);
 
+// The bounded wait of the staged kernels made to run out (a barrier phase
+// nothing completes, cycles SM clocks at most), CLOVER_STATUS_TIMEOUT or'd
+// into *status on the device, queued on stream s.
+void launch_wait_selftest(cudaStream_t s, long long cycles, int* status);
+
 // The maps of the y/z momentum node pass: mass flux of the sweep direction
 // and density1 (9 rows from c0-1), and the volume fluxes its post volumes
 // take (vol_flux_x 9 rows, the row-direction flux 10 rows: vol_flux_y for

@@ -340,6 +340,12 @@ void clover_gpu_synchronize(void);
  * forms give the same bits. A staged kernel whose bounded wait for its copies
  * gives up sets CLOVER_STATUS_TIMEOUT, seen at the next synchronisation. */
 void clover_gpu_use_staging(int on);
+/* Failure-path check of the above: queue on the library stream a bounded wait
+ * that runs out (cycles SM clocks at most) and reports through the library's
+ * device status word, as a staged kernel whose copies do not arrive would; the
+ * next synchronisation sets CLOVER_STATUS_TIMEOUT. 0, or a status bit if no
+ * library context exists yet or the launch failed. */
+int clover_gpu_wait_selftest_queued(long long cycles);
 /* Free every mirror and the library stream. */
 void clover_gpu_release(void);
 /* Chunk layout for device pointers passed in place: element (j,k,l) is at

@@ -41,3 +41,34 @@ def test_bounded_wait_runs_out_and_reports_timeout():
         assert np.array_equal(ch.field("density0"), r["fields"]["density0"])
     finally:
         ch.close()
+
+
+def test_abi_reports_a_staged_wait_that_ran_out():
+    """The drop-in ABI's staged kernels report a bounded wait that gave up
+    through the library's device status word, read back at the next
+    synchronisation: CLOVER_STATUS_TIMEOUT with a message, and the calls that
+    follow (status cleared) still match the oracle bit for bit."""
+    L = C.lib()
+    L.clover_gpu_wait_selftest_queued.argtypes = [ctypes.c_longlong]
+    L.clover_gpu_wait_selftest_queued.restype = ctypes.c_int
+    L.clover_gpu_release()
+    L.clover_gpu_clear_status()
+    d = decks.shock(12, 10, 8, 6, states=decks.MIXED_STATES)
+    r = O.run(d, max_steps=6, want_fields=True)
+    di = C.DropIn(decks.to_deck(d))
+    try:
+        assert di.run(2) == 2
+        assert L.clover_gpu_status() == 0
+        assert L.clover_gpu_wait_selftest_queued(10_000_000) == 0  # ~5 ms of SM clocks
+        L.clover_gpu_synchronize()
+        assert L.clover_gpu_status() & STATUS_TIMEOUT
+        assert b"gave up" in L.clover_gpu_error_string()
+        L.clover_gpu_clear_status()
+        assert di.run(6) == r["steps"]
+        assert L.clover_gpu_status() == 0
+        assert np.array_equal(di.dt_history(), r["dt"])
+        assert np.array_equal(di.field("density0"), r["fields"]["density0"])
+    finally:
+        di.close()
+        L.clover_gpu_release()
+        L.clover_gpu_clear_status()
