@@ -416,6 +416,15 @@ struct Chunk : ChunkBase {
             mom_node_tma_prepare<S>() && mom_vel_tma_prepare<S>() && cell_sweep_tma_prepare<S>() &&
             cell_sweep_x_tma_prepare<S>() &&
             visc_dt_tma_maps<S>(g, xvel0, yvel0, zvel0, density0, energy0, &visc_maps);
+    // by default the staged forms only where a launch has blocks to fill the
+    // GPU (32 x 8 columns by 32 planes each: at least four per SM); on smaller
+    // chunks (the measured 24..128-cell decks) the register-marching forms are
+    // faster. clover_chunk_use_tma chooses either way; both give the same bits.
+    {
+      const long long blocks = (long long)((g.x_max - g.x_min + 32) / 32) *
+                               ((g.y_max - g.y_min + 8) / 8) * ((g.z_max - g.z_min + 32) / 32);
+      use_tma = blocks >= 4 * 148;
+    }
 
     dt_cap = deck.end_step < (1 << 22) ? deck.end_step + 16 : (1 << 22);
     sum_cap = dt_cap / (deck.summary_frequency > 0 ? deck.summary_frequency : dt_cap) + 8;

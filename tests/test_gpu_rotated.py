@@ -50,14 +50,18 @@ def _compare(r, dts, sums, sum_steps, field):
             raise AssertionError("%s differs at %d elements, first %s" % (n, len(bad), bad[0]))
 
 
-@pytest.mark.parametrize("fused", [True, False])
+@pytest.mark.parametrize("form", ["staged", "register", "unfused"])
 @pytest.mark.parametrize("axis", [1, 2])
 @pytest.mark.parametrize("case", ["tp1", "tp1_40x8x8"])
-def test_native_rotated_bitwise(case, axis, fused):
+def test_native_rotated_bitwise(case, axis, form):
+    """The fused step with its stencils staged by bulk-tensor copies or in
+    their register-marching forms, and the unfused step."""
     d = _deck(case, axis)
     r = O.run(d, want_fields=True)
     ch = C.Chunk(decks.to_deck(d))
-    ch.use_fused(fused)
+    ch.use_fused(form != "unfused")
+    if form != "unfused":
+        assert ch.use_tma(form == "staged") == (form == "staged")
     try:
         assert ch.run() == r["steps"]
         assert ch.status == 0
