@@ -332,11 +332,11 @@ __global__ void __launch_bounds__(BX * BY, M::kFlat ? 6 : 8) k_pdv_predict_eos(M
 #undef ZS
   const A total_flux = right_flux - left_flux + top_flux - bottom_flux + front_flux - back_flux;
   const A vol = (A)g.vol;
-  const A vol_change_s = vol / (vol + total_flux);
+  const A vol_change_s = div_rn(vol, vol + total_flux);
   const A recip_volume = geo_rvol<A>(g);  // 1/volume
   const A d0 = LA(density0, j, k, l);
   const A energy_change =
-      (LA(pressure, j, k, l) / d0 + LA(viscosity, j, k, l) / d0) * total_flux * recip_volume;
+      quot_pair_sum(LA(pressure, j, k, l), LA(viscosity, j, k, l), d0) * total_flux * recip_volume;
   using R = typename S::rho_t;
   using En = typename S::ene_t;
   // the predicted state goes through the storage types, as it would in memory
@@ -530,7 +530,7 @@ __global__ void __launch_bounds__(BX * BY, M::kFlat ? 4 : (sizeof(typename S::ar
       pv_don = pv; vd_dif = clamp ? vd : vd_p1;
     }
     using AL = typename S::arith_t;  // the limiters' arithmetic
-    const AL sigmat = (AL)fabs(vf) / (AL)pv_don;
+    const AL sigmat = div_rn((AL)fabs(vf), (AL)pv_don);
     const AL sigma3 = (AL(1.0) + sigmat) * (AL)width_ratio(vd, vd_dif);
     const AL sigma4 = AL(2.0) - sigmat;
     AL diffuw = (AL)(d_don - d_up);
@@ -541,7 +541,7 @@ __global__ void __launch_bounds__(BX * BY, M::kFlat ? 4 : (sizeof(typename S::ar
     // (mf_t) feeds only the momentum sweep
     mf_st = mflux;
     if (lane <= 29) E(mass_flux, c, k, l) = st<MF>(mflux);
-    const AL sigmam = (AL)fabs(mflux) / ((AL)d_don * (AL)pv_don);
+    const AL sigmam = div_rn((AL)fabs(mflux), (AL)d_don * (AL)pv_don);
     diffuw = (AL)(e_don - e_up);
     diffdw = (AL)(e_dn - e_don);
     limiter = cell_limiter<AL>(sigmam, sigma3, sigma4, diffuw, diffdw);
@@ -785,14 +785,19 @@ __global__ void __launch_bounds__(BX * BY, sizeof(typename S::arith_t) == 4 && !
     for (int q = 0; q < 3; q++) {
       const A vp2 = vn[q];
       const A mf_0 = mom_flux_v<A>(nt, vw[q][1], vw[q][2], vw[q][3], vp2);
-      const V vn1 = st<V>((vw[q][2] * pre_0 + mf_prev[q] - mf_0) / post_0);
-      EI(out[q], IDX(p)) = vn1;
-      if (lz.xvel0) EI(lev0[q], IDX(p)) = vn1;  // last sweep of the step: reset_field
+      vn[q] = vw[q][2] * pre_0 + mf_prev[q] - mf_0;
       mf_prev[q] = mf_0;
       vw[q][0] = vw[q][1];
       vw[q][1] = vw[q][2];
       vw[q][2] = vw[q][3];
       vw[q][3] = vp2;
+    }
+    div3_rn(vn, post_0);  // the three updates share node_mass_post
+#pragma unroll
+    for (int q = 0; q < 3; q++) {
+      const V vn1 = st<V>(vn[q]);
+      EI(out[q], IDX(p)) = vn1;
+      if (lz.xvel0) EI(lev0[q], IDX(p)) = vn1;  // last sweep of the step: reset_field
     }
     pre_0 = pre_p;
   }
@@ -904,7 +909,7 @@ __global__ void __launch_bounds__(BX * BY, sizeof(typename S::arith_t) == 4 && M
       dif = p + 1 < top ? p + 1 : top;
     }
     using AL = typename S::arith_t;  // the limiters' arithmetic
-    const AL sigmat = (AL)fabs(vf) / (AL)pv_don;
+    const AL sigmat = div_rn((AL)fabs(vf), (AL)pv_don);
     const AL sigma3 = (AL(1.0) + sigmat) * (AL)width_ratio(VD(p), VD(dif));
     const AL sigma4 = AL(2.0) - sigmat;
     AL diffuw = (AL)(d_don - d_up);
@@ -913,7 +918,7 @@ __global__ void __launch_bounds__(BX * BY, sizeof(typename S::arith_t) == 4 && M
     const double mflux = vf * (d_don + (double)limiter);
     if (p <= c1 || last) EI(mass_flux, IDX(p)) = st<MF>(mflux);
     const double mf_stored = mflux;  // FP64 in the cell update; mf_t storage feeds the momentum sweep
-    const AL sigmam = (AL)fabs(mflux) / ((AL)d_don * (AL)pv_don);
+    const AL sigmam = div_rn((AL)fabs(mflux), (AL)d_don * (AL)pv_don);
     diffuw = (AL)(e_don - e_up);
     diffdw = (AL)(e_dn - e_don);
     limiter = cell_limiter<AL>(sigmam, sigma3, sigma4, diffuw, diffdw);
@@ -1013,6 +1018,7 @@ __global__ void __launch_bounds__(BX * BY, M::kFlat || sizeof(typename S::arith_
     using A = typename S::arith_t;
     const MomNodeTerms<A> nt =
         mom_node_terms<A>((A)nf, (A)nmpre, (A)nmpre_p, (A)cd_0, (A)cd_m1, (A)cd_p1);
+    A vn[3];
 #pragma unroll
     for (int q = 0; q < 3; q++) {
       A mf = A(0.0), v0 = A(0.0);
@@ -1023,8 +1029,13 @@ __global__ void __launch_bounds__(BX * BY, M::kFlat || sizeof(typename S::arith_
         mf = mom_flux_v<A>(nt, vm1, v0, vp1, vp2);
       }
       const A mf_m = __shfl_up_sync(0xffffffffu, mf, 1);
-      if (has_up) {
-        const V vn1 = st<V>((v0 * (A)nmpre + mf_m - mf) / (A)nmp);
+      vn[q] = v0 * (A)nmpre + mf_m - mf;
+    }
+    if (has_up) {
+      div3_rn(vn, (A)nmp);  // the three updates share node_mass_post
+#pragma unroll
+      for (int q = 0; q < 3; q++) {
+        const V vn1 = st<V>(vn[q]);
         E(out[q], j, k, l) = vn1;
         if (lz.xvel0) E(lev0[q], j, k, l) = vn1;  // last sweep of the step: reset_field
       }

@@ -12,6 +12,8 @@
 #include <cfloat>
 #include <cstdio>
 
+#include "../../include/clover_b200.h"
+#include "../../include/clover_kernels.h"
 #include "clover_div.cuh"
 #include "clover_launch.h"
 #include "clover_sum.cuh"
@@ -118,7 +120,7 @@ __global__ void __launch_bounds__(BX * BY) k_ideal_gas(M m,
   // are stored in FP32)
   using A = typename S::arith_t;
   const A d = (A)L(density, j, k, l);
-  const A v = A(1.0) / d;
+  const A v = div_rn(A(1.0), d);
   const A p = (A(1.4) - A(1.0)) * d * (A)L(energy, j, k, l);
   const A pressurebyenergy = (A(1.4) - A(1.0)) * d;
   const A pressurebyvolume = -d * p;
@@ -365,11 +367,11 @@ __global__ void __launch_bounds__(BX * BY, 8) k_pdv(Geom g, Box b, int predict, 
 #undef ZF
   const double total_flux = right_flux - left_flux + top_flux - bottom_flux + front_flux - back_flux;
   const double vol = E(ga.volume, j, k, l);
-  const double vol_change_s = vol / (vol + total_flux);
-  const double recip_volume = 1.0 / vol;
+  const double vol_change_s = div_rn(vol, vol + total_flux);
+  const double recip_volume = div_rn(1.0, vol);
   const double d0 = L(density0, j, k, l);
   const double energy_change =
-      (L(pressure, j, k, l) / d0 + L(viscosity, j, k, l) / d0) * total_flux * recip_volume;
+      quot_pair_sum(L(pressure, j, k, l), L(viscosity, j, k, l), d0) * total_flux * recip_volume;
   E(energy1, j, k, l) = st<typename S::ene_t>(L(energy0, j, k, l) - energy_change);
   E(density1, j, k, l) = st<typename S::rho_t>(d0 * vol_change_s);
 }
@@ -590,12 +592,12 @@ __device__ __forceinline__ double* line_slot(double* ring, int t, int q) {
 __device__ __forceinline__ void cell_face_flux(double vf, double pvd, double rw, double du,
                                                double dd, double dw, double eu, double ed,
                                                double ew, double& mf, double& ef) {
-  const double sigmat = fabs(vf) / pvd;
+  const double sigmat = div_rn(fabs(vf), pvd);
   const double sigma3 = (1.0 + sigmat) * rw;
   const double sigma4 = 2.0 - sigmat;
   double limiter = cell_limiter(sigmat, sigma3, sigma4, dd - du, dw - dd);
   mf = vf * (dd + limiter);
-  const double sigmam = fabs(mf) / (dd * pvd);
+  const double sigmam = div_rn(fabs(mf), dd * pvd);
   limiter = cell_limiter(sigmam, sigma3, sigma4, ed - eu, ew - ed);
   ef = mf * (ed + limiter);
 }
@@ -962,7 +964,7 @@ __device__ __forceinline__ double mom_node_flux(double nf, double vm1, double v0
   // else upwind i-1, donor i, downwind i+1 (width of the upwind)
   const bool neg = nf < 0.0;
   const double v_donor = neg ? vp1 : v0;
-  const double sigma = fabs(nf) / (neg ? nmp1 : nmp0);
+  const double sigma = div_rn(fabs(nf), neg ? nmp1 : nmp0);
   const double vdiffuw = v_donor - (neg ? vp2 : vm1);
   const double vdiffdw = (neg ? v0 : vp1) - v_donor;
   const double limiter = mom_limiter(sigma, cd0, neg ? cdp : cdm, vdiffuw, vdiffdw);
@@ -1031,7 +1033,7 @@ __global__ void __launch_bounds__(BX * BY, 4) k_mom_line_x(Geom g, GeomArrays ga
     }
     const double fl = row_up(flux, f_last);
     if (i >= x0 && i <= x1 + 1)
-      vel1[row + i] = st<typename S::vel_t>((vc * qc + fl - flux) / post);
+      vel1[row + i] = st<typename S::vel_t>(div_rn(vc * qc + fl - flux, post));
     f_last = flux;
     vp = vc; vc = vn; vn = vnn;
     qc = qn; qn = qnn;
@@ -1119,7 +1121,7 @@ __global__ void __launch_bounds__(BX * BY, 4) k_mom_line_yz(Geom g, GeomArrays g
     const typename S::wk_t fs =
         st<typename S::wk_t>(mom_node_flux(nf, w0, w1, w2, w3, q0, q1, cd[i - 1], cd[i], cd[i + 1]));
     if (i >= n0 || n0 == imin) mom_flux[at] = fs;
-    if (i >= n0) vel1[at] = st<typename S::vel_t>((w1 * q0 + f_last - (double)fs) / post);
+    if (i >= n0) vel1[at] = st<typename S::vel_t>(div_rn(w1 * q0 + f_last - (double)fs, post));
     f_last = (double)fs;
     w0 = w1; w1 = w2; w2 = w3;
     q0 = q1;
@@ -1890,3 +1892,48 @@ template void launch_fill<double>(cudaStream_t, double*, long long, double);
 template void launch_fill<float>(cudaStream_t, float*, long long, float);
 
 }  // namespace clover
+
+// ---------------------------------------------------------------------------
+// Self-test of the shared-reciprocal quotient (clover_div.cuh): q[i] = x[i] /
+// b[i] through recip_for + quot_rn where both lie in its range (fast[i] = 1),
+// else by IEEE division (fast[i] = 0).
+namespace clover {
+namespace {
+__global__ void k_quotient_selftest(const double* __restrict__ x, const double* __restrict__ b,
+                                    double* __restrict__ q, int* __restrict__ fast, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const Recip r = recip_for(b[i]);
+    const bool ok = r.ok && quot_in_range(x[i]);
+    q[i] = ok ? quot_rn(x[i], r) : x[i] / b[i];
+    fast[i] = ok ? 1 : 0;
+  }
+}
+}  // namespace
+}  // namespace clover
+
+extern "C" int clover_gpu_quotient_selftest(const double* x, const double* b, double* q, int* fast,
+                                            long long n) {
+  using namespace clover;
+  if (n <= 0) return 0;
+  double *dx = nullptr, *db = nullptr, *dq = nullptr;
+  int* df = nullptr;
+  const size_t bytes = (size_t)n * sizeof(double);
+  bool ok = cudaMalloc(&dx, bytes) == cudaSuccess && cudaMalloc(&db, bytes) == cudaSuccess &&
+            cudaMalloc(&dq, bytes) == cudaSuccess &&
+            cudaMalloc(&df, (size_t)n * sizeof(int)) == cudaSuccess;
+  ok = ok && cudaMemcpy(dx, x, bytes, cudaMemcpyHostToDevice) == cudaSuccess &&
+       cudaMemcpy(db, b, bytes, cudaMemcpyHostToDevice) == cudaSuccess;
+  if (ok) {
+    k_quotient_selftest<<<4 * 148, 256>>>(dx, db, dq, df, n);
+    ok = cudaGetLastError() == cudaSuccess &&
+         cudaMemcpy(q, dq, bytes, cudaMemcpyDeviceToHost) == cudaSuccess &&
+         cudaMemcpy(fast, df, (size_t)n * sizeof(int), cudaMemcpyDeviceToHost) == cudaSuccess;
+  }
+  cudaFree(dx);
+  cudaFree(db);
+  cudaFree(dq);
+  cudaFree(df);
+  if (!ok) cudaGetLastError();
+  return ok ? 0 : CLOVER_STATUS_CUDA_ERROR;
+}

@@ -105,7 +105,7 @@ __device__ __forceinline__ MomNodeTerms<A> mom_node_terms(A nf, A nmpre_i, A nmp
   MomNodeTerms<A> t;
   t.neg = nf < A(0.0);
   t.nf = nf;
-  t.sigma = fabs(nf) / (t.neg ? nmpre_ip1 : nmpre_i);
+  t.sigma = div_rn(fabs(nf), t.neg ? nmpre_ip1 : nmpre_i);
   t.width = width;
   t.cd_dif = t.neg ? cd_p1 : cd_m1;
   return t;

@@ -469,6 +469,7 @@ k_mom_sweep_x_tma(Geom g, int seg, GeomArrays ga, const __grid_constant__ MomXMa
       const double nmpre_p = __shfl_down_sync(fullmask, nmpre, 1);
       const MomNodeTerms<A> nt =
           mom_node_terms<A>((A)nf, (A)nmpre, (A)nmpre_p, (A)cd_0, (A)cd_m1, (A)cd_p1);
+      A vn[3];
 #pragma unroll
       for (int q = 0; q < 3; q++) {
         const V* vr = P::vel(b, q) + ty * WV + cv;
@@ -478,9 +479,14 @@ k_mom_sweep_x_tma(Geom g, int seg, GeomArrays ga, const __grid_constant__ MomXMa
           mf = mom_flux_v<A>(nt, (A)vr[-1], v0, (A)vr[1], (A)vr[2]);
         }
         const A mf_m = __shfl_up_sync(fullmask, mf, 1);
-        if (has_up) {
-          const V vn1 = st<V>((v0 * (A)nmpre + mf_m - mf) / (A)nmp);
-          const long long o = off3(g, j, k, l);
+        vn[q] = v0 * (A)nmpre + mf_m - mf;
+      }
+      if (has_up) {
+        div3_rn(vn, (A)nmp);  // the three updates share node_mass_post
+        const long long o = off3(g, j, k, l);
+#pragma unroll
+        for (int q = 0; q < 3; q++) {
+          const V vn1 = st<V>(vn[q]);
           out[q][o] = vn1;
           if (lz.xvel0) lev0[q][o] = vn1;  // last sweep of the step: reset_field
         }
@@ -652,11 +658,12 @@ k_pdv_predict_eos_tma(Geom g, int seg, const double* __restrict__ dt_ptr,
 #undef NV
     const A total_flux = right_flux - left_flux + top_flux - bottom_flux + front_flux - back_flux;
     const A vol = (A)g.vol;
-    const A vol_change_s = vol / (vol + total_flux);
+    const A vol_change_s = div_rn(vol, vol + total_flux);
     const A recip_volume = geo_rvol<A>(g);  // 1/volume
     const A d0 = (A)P::rho(bl)[ty * WR + tx + HR];
-    const A energy_change = ((A)P::cs(bl, 0)[ty * WC + tx + HC] / d0 +
-                             (A)P::cs(bl, 1)[ty * WC + tx + HC] / d0) * total_flux * recip_volume;
+    const A energy_change = quot_pair_sum((A)P::cs(bl, 0)[ty * WC + tx + HC],
+                                          (A)P::cs(bl, 1)[ty * WC + tx + HC], d0) *
+                            total_flux * recip_volume;
     // the predicted state goes through the storage types, as it would in memory
     const A e1 = (A)st<En>(((A)P::ene(bl)[ty * WE + tx + HE] - energy_change));
     const A d1 = (A)st<R>((d0 * vol_change_s));
@@ -1032,9 +1039,9 @@ k_pdv_dropin_tma(Geom g, int seg, double dt, const __grid_constant__ PdvDropMaps
       front_flux = (za1 * zsum(bu)) * 0.125 * dt;
     }
     const double total_flux = right_flux - left_flux + top_flux - bottom_flux + front_flux - back_flux;
-    const double vol_change_s = vol / (vol + total_flux);
-    const double recip_volume = 1.0 / vol;
-    const double energy_change = (pr / d0 + vi / d0) * total_flux * recip_volume;
+    const double vol_change_s = div_rn(vol, vol + total_flux);
+    const double recip_volume = div_rn(1.0, vol);
+    const double energy_change = quot_pair_sum(pr, vi, d0) * total_flux * recip_volume;
     const long long o = off3(g, j, k, l);
     energy1[o] = e0 - energy_change;
     density1[o] = d0 * vol_change_s;
@@ -1792,18 +1799,24 @@ k_mom_vel_tma(Geom g, int seg, GeomArrays ga, const __grid_constant__ VelMaps ma
     const MomNodeTerms<A> nt =
         mom_node_terms<A>(nf_0, pre_0, pre_p, (A)CD(p), (A)CD(p - 1), (A)CD(p + 1));
     const long long o = off3(g, IDX(p));
+    A vn[3];
 #pragma unroll
     for (int q = 0; q < 3; q++) {
       const A vp2 = (A)P::vel(b2, q)[cv];
       const A mf_0 = mom_flux_v<A>(nt, vw[q][1], vw[q][2], vw[q][3], vp2);
-      const V vn1 = st<V>((vw[q][2] * pre_0 + mf_prev[q] - mf_0) / post_0);
-      out[q][o] = vn1;
-      if (lz.xvel0) lev0[q][o] = vn1;  // last sweep of the step: reset_field
+      vn[q] = vw[q][2] * pre_0 + mf_prev[q] - mf_0;
       mf_prev[q] = mf_0;
       vw[q][0] = vw[q][1];
       vw[q][1] = vw[q][2];
       vw[q][2] = vw[q][3];
       vw[q][3] = vp2;
+    }
+    div3_rn(vn, post_0);  // the three updates share node_mass_post
+#pragma unroll
+    for (int q = 0; q < 3; q++) {
+      const V vn1 = st<V>(vn[q]);
+      out[q][o] = vn1;
+      if (lz.xvel0) lev0[q][o] = vn1;  // last sweep of the step: reset_field
     }
     pre_0 = pre_p;
   });
@@ -1974,7 +1987,7 @@ k_cell_sweep_tma(Geom g, int seg, GeomArrays ga, const __grid_constant__ CellMap
       d_up = d3; d_don = d2; d_dn = d1; e_up = e3; e_don = e2; e_dn = e1; pv_don = pv_0;
       dif = p + 1 < top ? p + 1 : top;
     }
-    const AL sigmat = (AL)fabs(vf) / (AL)pv_don;
+    const AL sigmat = div_rn((AL)fabs(vf), (AL)pv_don);
     const AL sigma3 = (AL(1.0) + sigmat) * (AL)width_ratio(VD(p), VD(dif));
     const AL sigma4 = AL(2.0) - sigmat;
     AL diffuw = (AL)(d_don - d_up);
@@ -1983,7 +1996,7 @@ k_cell_sweep_tma(Geom g, int seg, GeomArrays ga, const __grid_constant__ CellMap
     const double mflux = vf * (d_don + (double)limiter);
     if (p <= q1 || last) mass_flux[off3(g, IDX(p))] = st<MFT>(mflux);
     const double mf_stored = mflux;  // FP64 in the cell update; mf_t storage feeds the momentum sweep
-    const AL sigmam = (AL)fabs(mflux) / ((AL)d_don * (AL)pv_don);
+    const AL sigmam = div_rn((AL)fabs(mflux), (AL)d_don * (AL)pv_don);
     diffuw = (AL)(e_don - e_up);
     diffdw = (AL)(e_dn - e_don);
     limiter = cell_limiter<AL>(sigmam, sigma3, sigma4, diffuw, diffdw);
@@ -2144,7 +2157,7 @@ k_cell_sweep_x_tma(Geom g, int seg, GeomArrays ga, const __grid_constant__ CellX
         e_up = clamp ? e : (double)er[1]; e_don = e; e_dn = e_m1;
         pv_don = pv; vd_dif = clamp ? vd_0 : vd_p1;
       }
-      const AL sigmat = (AL)fabs(vf) / (AL)pv_don;
+      const AL sigmat = div_rn((AL)fabs(vf), (AL)pv_don);
       const AL sigma3 = (AL(1.0) + sigmat) * (AL)width_ratio(vd_0, vd_dif);
       const AL sigma4 = AL(2.0) - sigmat;
       AL diffuw = (AL)(d_don - d_up);
@@ -2155,7 +2168,7 @@ k_cell_sweep_x_tma(Geom g, int seg, GeomArrays ga, const __grid_constant__ CellX
       // (mf_t) feeds only the momentum sweep
       mf_st = mflux;
       if (lane < kCellXLanes) mass_flux[off3(g, c, k, l)] = st<MF>(mflux);
-      const AL sigmam = (AL)fabs(mflux) / ((AL)d_don * (AL)pv_don);
+      const AL sigmam = div_rn((AL)fabs(mflux), (AL)d_don * (AL)pv_don);
       diffuw = (AL)(e_don - e_up);
       diffdw = (AL)(e_dn - e_don);
       limiter = cell_limiter<AL>(sigmam, sigma3, sigma4, diffuw, diffdw);

@@ -90,6 +90,15 @@ int clover_chunk_use_tma(clover_chunk *c, int on);
  * CLOVER_STATUS_CUDA_ERROR. The device stays usable. */
 int clover_gpu_wait_selftest(long long cycles);
 
+/* Self-test of the correctly rounded FP64 quotient the step kernels form from
+ * one approximate reciprocal per divisor (no counterpart in the reference,
+ * whose divisions are IEEE divisions): q[i] = x[i] / b[i] for n host values,
+ * through that quotient where x[i] and b[i] lie in its range (fast[i] = 1)
+ * and by IEEE division elsewhere (fast[i] = 0). Either way q[i] must equal
+ * the IEEE quotient bit for bit. Returns 0 or CLOVER_STATUS_CUDA_ERROR. */
+int clover_gpu_quotient_selftest(const double *x, const double *b, double *q, int *fast,
+                                 long long n);
+
 /* Host copies of the device records (these synchronise):
  * steps taken, simulated time, dt of each step, field summaries
  * (vol, mass, ie, ke, press) with the step each was taken at. */
