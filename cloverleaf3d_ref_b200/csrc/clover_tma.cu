@@ -2440,7 +2440,7 @@ void launch_mom_node_dropin_tma(const Geom& g, cudaStream_t s, int dir, const No
         g, seg, maps, node_flux, node_mass_post, node_mass_pre, status);
 }
 
-// four blocks per SM in both precisions (FP64 at 64 registers: 1.85 -> 1.76 ms at 512^3
+// four blocks per SM in both precisions (FP64 at 64 registers, 4 bytes spilled: 1.85 -> 1.76 ms at 512^3
 // against three; the y/z cell sweeps measured slower at four)
 template <class S>
 constexpr int kCellXMinBlocks = 4;
