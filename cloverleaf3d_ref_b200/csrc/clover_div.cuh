@@ -26,6 +26,8 @@
 
 #include <cfloat>
 #include <cmath>
+#include <cstdint>
+#include <cstring>
 
 #ifdef __CUDACC__
 #define CLOVER_HD __host__ __device__ __forceinline__
@@ -82,37 +84,46 @@ CLOVER_HD float div6(float x) { return x / 6.0f; }
 // fused; the library's other operations stay uncontracted. The kernels use it
 // where it measured faster than the IEEE division sequence (the momentum
 // updates and Courant numbers, the cell Courant numbers, the PdV predictor and
-// the equation of state); elsewhere they divide.
-#ifdef __CUDACC__
+// the equation of state); elsewhere they divide. The host form (for tests on
+// the CPU) takes its seed from the correctly rounded FP32 reciprocal, which
+// lies within the same 1 ulp.
 struct Recip {
   double b, y;
   bool ok;  // b lies in the range above
 };
 
-__device__ __forceinline__ Recip recip_for(double b) {
+CLOVER_HD Recip recip_for(double b) {
   Recip r;
   r.b = b;
+#ifdef __CUDA_ARCH__
   const float bf = __double2float_rn(b);
   float yf;
   asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(yf) : "f"(bf));
+  const unsigned hi = (unsigned)__double2hiint(b);
+#else
+  const float yf = 1.0f / (float)b;
+  std::uint64_t bits;
+  std::memcpy(&bits, &b, sizeof bits);
+  const unsigned hi = (unsigned)(bits >> 32);
+#endif
   double y = (double)yf;
   double e = fma(-b, y, 1.0);
   y = fma(y, e, y);
   e = fma(-b, y, 1.0);
   r.y = fma(y, e, y);
   const double ab = fabs(b);
-  r.ok = ab >= 0x1p-100 && ab <= 0x1p100 && (__double2hiint(b) & 0xFFFFF) != 0xFFFFF;
+  r.ok = ab >= 0x1p-100 && ab <= 0x1p100 && (hi & 0xFFFFFu) != 0xFFFFFu;
   return r;
 }
 
 // x lies in the range above
-__device__ __forceinline__ bool quot_in_range(double x) {
+CLOVER_HD bool quot_in_range(double x) {
   const double ax = fabs(x);
   return (ax >= 0x1p-800 && ax <= 0x1p800) || x == 0.0;
 }
 
 // RN(x / r.b) when r.ok and quot_in_range(x)
-__device__ __forceinline__ double quot_rn(double x, const Recip& r) {
+CLOVER_HD double quot_rn(double x, const Recip& r) {
   const double q0 = x * r.y;
   const double r0 = fma(-r.b, q0, x);
   const double q1 = fma(r0, r.y, q0);
@@ -120,6 +131,8 @@ __device__ __forceinline__ double quot_rn(double x, const Recip& r) {
   const double q = fma(r1, r.y, q1);
   return x == 0.0 ? q0 : q;  // q0 = x * y: a zero with the IEEE quotient's sign
 }
+
+#ifdef __CUDACC__
 
 // x / b correctly rounded: in FP64 through quot_rn where x and b lie in its
 // range, else by IEEE division; in FP32 by division.

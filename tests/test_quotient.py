@@ -1,9 +1,16 @@
-"""CPU: the shared-reciprocal FP64 quotient (clover_div.cuh) restated in exact
-arithmetic (tests/quotient_cases.py) gives the IEEE quotient bit for bit on
+"""CPU: the shared-reciprocal FP64 quotient (clover_div.cuh) gives the IEEE
+quotient bit for bit. Restated in exact arithmetic (tests/quotient_cases.py) on
 random inputs and on quotients within a few 2^-53 ulp of a midpoint, where the
-product with the reciprocal alone often rounds the wrong way."""
+product with the reciprocal alone often rounds the wrong way; and the header
+itself, compiled for the host (tests/quotient_host.cpp), on millions of them."""
+import ctypes
 import math
+import os
+import shutil
+import subprocess
 from fractions import Fraction
+
+import pytest
 
 import numpy as np
 
@@ -62,3 +69,44 @@ def test_range_flags():
     assert not Q.recip_for(2.0 ** 101)[1] and Q.recip_for(-(2.0 ** 100))[1]
     assert Q.quot_in_range(-0.0) and not Q.quot_in_range(math.inf)
     assert not Q.quot_in_range(math.nan) and not Q.quot_in_range(2.0 ** -801)
+
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+@pytest.fixture(scope="module")
+def host_quotient(tmp_path_factory):
+    cxx = shutil.which("g++")
+    if cxx is None:
+        pytest.skip("no host C++ compiler")
+    so = str(tmp_path_factory.mktemp("quot") / "libquot.so")
+    subprocess.run([cxx, "-std=c++17", "-O2", "-ffp-contract=off", "-shared", "-fPIC", "-o", so,
+                    os.path.join(HERE, "quotient_host.cpp")], check=True)
+    f = ctypes.CDLL(so).quotient_batch
+    f.argtypes = [ctypes.c_void_p] * 4 + [ctypes.c_longlong]
+    f.restype = None
+
+    def run(x, b):
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        q = np.empty_like(x)
+        fast = np.empty(len(x), dtype=np.int32)
+        f(x.ctypes.data, b.ctypes.data, q.ctypes.data, fast.ctypes.data, len(x))
+        with np.errstate(all="ignore"):
+            ref = x / b
+        nan = np.isnan(ref)
+        assert np.array_equal(np.isnan(q), nan)
+        bad = np.flatnonzero((q.view(np.uint64) != ref.view(np.uint64)) & ~nan)
+        assert len(bad) == 0, [(x[i], b[i], q[i], ref[i]) for i in bad[:5]]
+        return fast
+    return run
+
+
+def test_header_on_the_host_equals_ieee_division(host_quotient):
+    assert host_quotient(*Q.random_cases(4_000_000, 31)).mean() > 0.999
+    host_quotient(*Q.random_cases(1_000_000, 32, span=1000))
+    assert host_quotient(*Q.hard_cases(20_000, 33)).all()
+    assert host_quotient(*Q.hard_cases(5_000, 34, top_divisors=True)).all()
+    xs, bs = Q.special_cases()
+    fast = host_quotient(xs, bs)
+    assert 0 < fast.sum() < len(fast)
